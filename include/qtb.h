@@ -1,0 +1,193 @@
+/*
+ * qtb.h -- C ABI of the qtensor_b200 bucket-elimination engine (libqtb.so).
+ *
+ * Plain pointers, sizes and integer status codes (0 = ok); no exception or
+ * device trap crosses this boundary.  Device buffers are caller-owned (any
+ * allocator, e.g. torch tensors' data_ptr()); the CUDA stream is passed
+ * explicitly as a void* (cudaStream_t; NULL = legacy default stream).
+ *
+ * Reference interfaces replaced (paths within DaniloZZZ/QTensor):
+ *   qtb_bucket_c64      <- BucketBackend.process_bucket
+ *                          qtensor/ProcessingFrameworks.py:14-15 (NumpyBackend :29-31,
+ *                          semantics restated by CMKLExtendedBackend :45-147,
+ *                          tcontract.mkl_contract_complex/_sum call sites :65-66, :129-130)
+ *   qtb_plan_*          <- the per-edge host graph work of
+ *                          QtreeSimulator.simulate_batch qtensor/Simulate.py:66-94
+ *                          (circ2buckets, OrderingOptimizer.optimize
+ *                          qtensor/optimisation/Optimizer.py:65-87, reorder_buckets,
+ *                          slicing) and of the DefaultQAOAComposer simplifier
+ *                          qtensor/simplify_circuit/simplify_circuit.py:78-138
+ *   qtb_plan_run        <- qtree.optimizer.bucket_elimination driven by
+ *                          BucketBackend.process_bucket (Simulate.py:90-94), for
+ *                          every edge of QAOASimulator.energy_expectation
+ *                          qtensor/QAOASimulator.py:44-66 (+ _post_process_energy :27-41)
+ *   qtb_last_error      <- Python exceptions raised by the reference backends
+ */
+#ifndef QTB_H
+#define QTB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QTB_OK 0
+#define QTB_ERR_ARG 1        /* invalid argument (sizes, masks, pointers) */
+#define QTB_ERR_CUDA 2       /* a CUDA runtime call failed */
+#define QTB_ERR_UNSUPPORTED 3
+#define QTB_ERR_DEVICE 4     /* a kernel reported an error status */
+
+#define QTB_MAX_BUCKET_INPUTS 16
+#define QTB_MAX_BUCKET_VARS 31
+
+/* ---------------------------------------------------------------- misc */
+/* Library version string. */
+const char* qtb_version(void);
+/* Select/initialise a CUDA device; safe to call repeatedly. */
+int qtb_init(int device);
+/* Copy the last error message of the calling thread into buf (NUL-terminated). */
+int qtb_last_error(char* buf, size_t len);
+
+/* ------------------------------------------------- K1: one bucket (plain path)
+ * All variables are binary.  The bucket's union of variables is sorted by
+ * variable id; union variable 0 (the bucket variable, smallest id) is the
+ * most significant bit of a row-major union index, union variable n_vars-1
+ * the least significant.  Input t holds the union variables whose bits are
+ * set in masks[t] (bit (n_vars-1-v) <-> union variable v), row-major in
+ * increasing variable id.  The output is the product of all inputs over the
+ * union, summed over union variable 0 when sum_first != 0 (then it has
+ * n_vars-1 variables), row-major complex64.                               */
+typedef struct {
+    int32_t n_inputs;                        /* 1..QTB_MAX_BUCKET_INPUTS */
+    int32_t n_vars;                          /* 0..QTB_MAX_BUCKET_VARS */
+    int32_t sum_first;                       /* 0/1; needs n_vars >= 1 */
+    uint32_t masks[QTB_MAX_BUCKET_INPUTS];
+} qtb_bucket_desc;
+
+/* inputs: n_inputs device pointers to complex64 arrays; output: device
+ * complex64 array of 2^(n_vars - sum_first) elements. Asynchronous on stream. */
+int qtb_bucket_c64(const qtb_bucket_desc* desc, const void* const* inputs,
+                   void* output, void* stream);
+
+/* ------------------------------------------------- plan compiler (host C++) */
+/* Gate kinds of a circuit given to the plan compiler. */
+enum {
+    QTB_GATE_M = 0, QTB_GATE_H = 1, QTB_GATE_Z = 2, QTB_GATE_X = 3,
+    QTB_GATE_Y = 4, QTB_GATE_CX = 5, QTB_GATE_CZ = 6, QTB_GATE_ZPHASE = 7,
+    QTB_GATE_XPHASE = 8, QTB_GATE_YPHASE = 9, QTB_GATE_ZZ = 10, QTB_GATE_T = 11
+};
+
+/* One gate.  Parametric gates have alpha = coef * params[param]; a daggered
+ * parametric gate is passed with coef negated (ZZ, XPhase, YPhase, ZPhase
+ * satisfy G(alpha)^+ = G(-alpha)); the other gates are their own inverse.   */
+typedef struct {
+    int32_t kind;
+    int32_t q0;
+    int32_t q1;        /* second qubit of CX/CZ/ZZ, else -1 */
+    int32_t param;     /* -1 for non-parametric gates */
+    double coef;
+} qtb_gate;
+
+typedef struct qtb_plan qtb_plan;   /* opaque: a set of compiled networks */
+
+/* Per-network statistics filled by qtb_plan_network_info. */
+typedef struct {
+    int32_t n_qubits;
+    int32_t n_vars;           /* variables of the bucket network */
+    int32_t treewidth;        /* greedy width (max neighbour count), Optimizer.py:78 */
+    int32_t max_rank;         /* largest tensor rank built (incl. the summed var) */
+    int32_t n_ops;            /* bucket kernels executed */
+    int32_t n_phases;         /* dependency levels (barriers) */
+    int32_t arena_elems;      /* complex64 scratch elements */
+    int32_t angle_specific;   /* 1: simplifier decisions depend on the angles */
+    double alg_bytes;         /* sum over ops of 8*(sum_t 2^rank_t + 2^w) */
+    double alg_flops;         /* sum over ops of 6*(k-1)*2^u + 2*2^w*sum */
+    double ref_flops;         /* PerfBackend._perfect_bucket_flop summed */
+} qtb_network_info;
+
+/* Create an empty plan for circuits with n_params angle parameters. */
+int qtb_plan_create(int32_t n_params, qtb_plan** out);
+int qtb_plan_destroy(qtb_plan* plan);
+
+/* Compile <0|circuit|0> (all qubits in and out fixed to 0) as one network:
+ * simplify_passes rounds of the commutation simplifier, qtree bucket layout,
+ * greedy min-degree order (ket + bra variables first), reorder, slicing and
+ * symbolic bucket elimination.  params (n_params doubles) are the angles the
+ * simplifier's |alpha1+alpha2| < 1e-5 cancellation test sees; decisions that
+ * are not structural mark the network angle-specific.  Returns its index. */
+int qtb_plan_add_circuit(qtb_plan* plan, int32_t n_qubits, const qtb_gate* gates,
+                         int32_t n_gates, int32_t simplify_passes,
+                         const double* params, int32_t* net_index);
+
+/* Same, building the QAOA lightcone circuit of edge (u, v) of a graph given
+ * in CSR form (node ids 0..n_nodes-1): the qubits are the nodes within p hops
+ * of the edge in increasing node id; layer l = 1..p acts on the radius p+1-l
+ * subgraph with ZZ(2*gamma_l) on its edges (increasing (a, b), a < b) and
+ * XPhase(2*beta_l) on its nodes, then Z_u Z_v, then the inverse.
+ * composer: 0 = ZZ gates + simplifier run twice (DefaultQAOAComposer),
+ * 1 = ZZ gates, 2 = CX-ZPhase-CX (QtreeQAOAComposer).  params = gamma[0..p),
+ * beta[0..p).                                                            */
+int qtb_plan_add_lightcone(qtb_plan* plan, int32_t n_nodes, const int64_t* indptr,
+                           const int32_t* indices, int32_t u, int32_t v, int32_t p,
+                           int32_t composer, const double* params, int32_t* net_index);
+
+/* Compile all edges of a graph with n_threads host threads (0 = all cores);
+ * edges is 2*n_edges node ids.  Network i of the call is edge i.          */
+int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indptr,
+                            const int32_t* indices, const int32_t* edges, int32_t n_edges,
+                            int32_t p, int32_t composer, const double* params,
+                            int32_t n_threads, int32_t* first_net_index);
+
+int qtb_plan_n_networks(const qtb_plan* plan, int32_t* n);
+int qtb_plan_network_info(const qtb_plan* plan, int32_t net, qtb_network_info* info);
+/* Elimination order of a network as variable ids of the qtree layout
+ * (bra 0..nq-1, then variables in creation order), ket+bra first. */
+int qtb_plan_network_peo(const qtb_plan* plan, int32_t net, int32_t* peo, int32_t cap,
+                         int32_t* n);
+/* Check that params keep every angle-dependent simplifier decision of the
+ * plan; *valid = 0 means the plan must be recompiled for these angles.    */
+int qtb_plan_check_params(const qtb_plan* plan, const double* params, int32_t* valid);
+
+/* Host copies of the flattened plan (the arrays qtb_plan_upload sends to the
+ * device), for inspection and CPU-side verification of the compiler.
+ * which: 0 networks (8 x u32 each), 1 ops (16 B each), 2 operands (8 B),
+ * 3 phases (16 B), 4 gate-table entries (24 B), 5 angle terms (16 B).
+ * Writes min(cap, size) bytes to buf (may be NULL) and the full size.     */
+int qtb_plan_export(qtb_plan* plan, int32_t which, void* buf, size_t cap, size_t* size);
+/* Complex64 elements of the gate table. */
+int qtb_plan_table_elems(const qtb_plan* plan, int64_t* n);
+
+/* Copy the plan to the current device (synchronous; allocates device memory
+ * owned by the plan).  Must precede qtb_plan_run.                         */
+int qtb_plan_upload(qtb_plan* plan);
+
+/* Contract networks [first, first+count) of an uploaded plan on stream:
+ *   params_dev  device doubles (n_params) -- the angles of this request;
+ *   terms_dev   device complex64 per network (the amplitude <0|U|0>);
+ *   energy_dev  device double: (count - sum Re terms) / 2 with a compensated
+ *               (Neumaier) fp64 sum -- the MaxCut energy when the networks are
+ *               the edge terms of one graph; may be NULL;
+ *   scratch_dev device memory of qtb_plan_scratch_bytes(); may be NULL when
+ *               that size is 0.
+ * The gate table is generated on the device from params_dev.             */
+int qtb_plan_scratch_bytes(const qtb_plan* plan, int32_t first, int32_t count,
+                           size_t* bytes);
+int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* params_dev,
+                 void* terms_dev, double* energy_dev, void* scratch_dev, void* stream);
+
+/* Device error word of the last run on this plan (0 = ok); synchronises. */
+int qtb_plan_device_status(qtb_plan* plan, int32_t* status);
+
+/* CUDA-event timing of the network-executor launches of qtb_plan_run, on
+ * the run's stream.  set_timing resets the totals; collect_timing waits for
+ * the recorded events and returns the accumulated milliseconds and launch
+ * count.                                                                  */
+int qtb_plan_set_timing(qtb_plan* plan, int32_t enable);
+int qtb_plan_collect_timing(qtb_plan* plan, double* total_ms, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QTB_H */

@@ -1,0 +1,968 @@
+// Host plan compiler: circuit -> bucket network -> elimination order ->
+// device plan (ops, dependency phases, arena offsets, gate-table entries).
+//
+// Follows, per step (paths within DaniloZZZ/QTensor):
+//   simplify()       qtensor/simplify_circuit/simplify_circuit.py:30-138 and
+//                    simplify_circuit_api.py:74-106 (pairs of equal kind on
+//                    equal qubits, visited by distance; merge if every gate
+//                    in between commutes with the first; cancel below 1e-5)
+//   build_network()  qtree circ2buckets as used by TensorNet.py:60-68 (bra
+//                    variables first, gates placed from the bra side, ket
+//                    measurement tensors last; tensor -> bucket of its
+//                    smallest variable)
+//   greedy_order()   qtensor/utils.py:12-44,77-87 + Optimizer.py:65-87 (first
+//                    node of least distinct-neighbour count, clique fill-in;
+//                    peo = ket + bra + greedy)
+//   eliminate()      qtree reorder_buckets / get_sliced_np_buckets /
+//                    bucket_elimination as driven by Simulate.py:47-94, with
+//                    the bucket arithmetic of ProcessingFrameworks.py:45-147
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <thread>
+#include <tuple>
+
+#include "plan.h"
+
+namespace qtb {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string& msg) { g_err = msg; }
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+bool EntryKey::operator<(const EntryKey& o) const {
+    return std::tie(kind, expr, rank_in, sliced_mask, perm) <
+           std::tie(o.kind, o.expr, o.rank_in, o.sliced_mask, o.perm);
+}
+
+int rank_of_kind(int32_t kind) {
+    switch (kind) {
+        case QTB_GATE_Z: case QTB_GATE_T: case QTB_GATE_ZPHASE: return 1;
+        case QTB_GATE_CX: return 3;
+        default: return 2;
+    }
+}
+
+static int qubits_of_kind(int32_t kind) {
+    return (kind == QTB_GATE_CX || kind == QTB_GATE_CZ || kind == QTB_GATE_ZZ) ? 2 : 1;
+}
+
+static bool is_parametric(int32_t kind) {
+    return kind == QTB_GATE_ZPHASE || kind == QTB_GATE_XPHASE || kind == QTB_GATE_YPHASE ||
+           kind == QTB_GATE_ZZ;
+}
+
+// Position (in the gate's qubit list) of the qubit that gets a new variable,
+// or -1 for gates diagonal on all their qubits.
+static int changed_position(int32_t kind) {
+    switch (kind) {
+        case QTB_GATE_M: case QTB_GATE_H: case QTB_GATE_X: case QTB_GATE_Y:
+        case QTB_GATE_XPHASE: case QTB_GATE_YPHASE: return 0;
+        case QTB_GATE_CX: return 1;
+        default: return -1;
+    }
+}
+
+static Expr expr_add(const Expr& a, const Expr& b) {
+    Expr out;
+    size_t i = 0, j = 0;
+    while (i < a.size() || j < b.size()) {
+        if (j == b.size() || (i < a.size() && a[i].first < b[j].first)) {
+            out.push_back(a[i++]);
+        } else if (i == a.size() || b[j].first < a[i].first) {
+            out.push_back(b[j++]);
+        } else {
+            double c = a[i].second + b[j].second;
+            if (c != 0.0) out.emplace_back(a[i].first, c);
+            ++i;
+            ++j;
+        }
+    }
+    return out;
+}
+
+// ------------------------------------------------------------- simplifier
+namespace {
+
+enum SKind { SK_ZZ, SK_X, SK_Y, SK_ZP, SK_H, SK_CX, SK_Z, SK_ID };
+enum SBasis { SB_Z = 1, SB_X, SB_Y, SB_XY, SB_CA, SB_CB };
+
+struct SGate {
+    int kind = SK_ID;
+    int nq = 0;
+    int q[2] = {-1, -1};
+    int basis[2] = {0, 0};
+    double angle = 0.0;
+    Expr expr;
+};
+
+SGate make_sgate(int kind, const int* qs, double angle, const Expr& expr) {
+    SGate g;
+    g.kind = kind;
+    g.angle = angle;
+    g.expr = expr;
+    switch (kind) {
+        case SK_ZZ:
+            g.nq = 2;
+            g.q[0] = std::min(qs[0], qs[1]);
+            g.q[1] = std::max(qs[0], qs[1]);
+            g.basis[0] = g.basis[1] = SB_Z;
+            break;
+        case SK_CX:
+            g.nq = 2;
+            g.q[0] = qs[0];
+            g.q[1] = qs[1];
+            g.basis[0] = SB_CA;
+            g.basis[1] = SB_CB;
+            g.angle = 0.0;
+            g.expr.clear();
+            break;
+        case SK_H:
+            g.nq = 1;
+            g.q[0] = qs[0];
+            g.basis[0] = SB_XY;
+            g.angle = M_PI / 2.0 / std::sqrt(2.0);   // fixed, gates.py hadamard
+            g.expr.clear();
+            break;
+        case SK_Z:
+            g.nq = 1;
+            g.q[0] = qs[0];
+            g.basis[0] = SB_Z;
+            g.angle = 0.0;
+            g.expr.clear();
+            break;
+        case SK_X: case SK_Y: case SK_ZP:
+            g.nq = 1;
+            g.q[0] = qs[0];
+            g.basis[0] = kind == SK_X ? SB_X : (kind == SK_Y ? SB_Y : SB_Z);
+            break;
+        default:
+            g.kind = SK_ID;
+            g.nq = 0;
+            g.angle = 0.0;
+            g.expr.clear();
+    }
+    return g;
+}
+
+bool commute(const SGate& a, const SGate& b) {
+    for (int i = 0; i < a.nq; ++i)
+        for (int j = 0; j < b.nq; ++j)
+            if (a.q[i] == b.q[j] && a.basis[i] != b.basis[j]) return false;
+    return true;
+}
+
+bool same_site(const SGate& a, const SGate& b) {
+    if (a.kind != b.kind || a.nq != b.nq) return false;
+    for (int i = 0; i < a.nq; ++i)
+        if (a.q[i] != b.q[i]) return false;
+    return true;
+}
+
+struct Gate {
+    int32_t kind;
+    int32_t q[2];
+    double angle;   // numeric alpha (parametric gates)
+    Expr expr;      // symbolic alpha
+};
+
+int skind_of(int32_t kind) {
+    switch (kind) {
+        case QTB_GATE_ZZ: return SK_ZZ;
+        case QTB_GATE_XPHASE: return SK_X;
+        case QTB_GATE_YPHASE: return SK_Y;
+        case QTB_GATE_ZPHASE: return SK_ZP;
+        case QTB_GATE_H: return SK_H;
+        case QTB_GATE_CX: return SK_CX;
+        case QTB_GATE_Z: return SK_Z;
+        default: return -1;
+    }
+}
+
+int32_t kind_of_skind(int sk) {
+    switch (sk) {
+        case SK_ZZ: return QTB_GATE_ZZ;
+        case SK_X: return QTB_GATE_XPHASE;
+        case SK_Y: return QTB_GATE_YPHASE;
+        case SK_ZP: return QTB_GATE_ZPHASE;
+        case SK_H: return QTB_GATE_H;
+        case SK_CX: return QTB_GATE_CX;
+        default: return QTB_GATE_Z;
+    }
+}
+
+// One pass of the commutation simplifier over a gate list.
+int simplify(std::vector<Gate>* gates, std::vector<AngleCheck>* checks, bool* angle_specific,
+             std::string* err) {
+    const int n = (int)gates->size();
+    if (n == 0) return QTB_OK;
+    std::vector<SGate> cir(n);
+    for (int i = 0; i < n; ++i) {
+        const Gate& g = (*gates)[i];
+        int sk = skind_of(g.kind);
+        if (sk < 0) {
+            *err = "simplifier: gate kind " + std::to_string(g.kind) + " has no commutation record";
+            return QTB_ERR_UNSUPPORTED;
+        }
+        cir[i] = make_sgate(sk, g.q, g.angle, g.expr);
+    }
+    std::vector<std::pair<int, int>> pairs;
+    for (int i = 0; i + 1 < n; ++i)
+        for (int j = i + 1; j < n; ++j)
+            if (same_site(cir[i], cir[j])) pairs.emplace_back(i, j);
+    if (pairs.empty()) return QTB_OK;
+    std::vector<int> order(pairs.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return pairs[x].second - pairs[x].first < pairs[y].second - pairs[y].first;
+    });
+    for (int idx : order) {
+        const int a = pairs[idx].first, b = pairs[idx].second;
+        if (cir[a].kind == SK_ID || cir[b].kind == SK_ID) continue;
+        bool ok = true;
+        for (int m = a + 1; m < b && ok; ++m) ok = commute(cir[a], cir[m]);
+        if (!ok) continue;
+        const double total = cir[a].angle + cir[b].angle;
+        const Expr sym = expr_add(cir[a].expr, cir[b].expr);
+        const bool param = cir[a].kind == SK_ZZ || cir[a].kind == SK_X || cir[a].kind == SK_Y ||
+                           cir[a].kind == SK_ZP;
+        if (std::fabs(total) < 1e-5) {
+            if (param && !sym.empty()) {
+                checks->push_back({sym, true});
+                *angle_specific = true;
+            }
+            cir[a] = SGate();
+            cir[b] = SGate();
+        } else {
+            if (param) checks->push_back({sym, false});
+            SGate merged = make_sgate(cir[a].kind, cir[a].q, total, sym);
+            cir[a] = SGate();
+            cir[b] = merged;
+        }
+    }
+    std::vector<Gate> out;
+    for (const SGate& s : cir) {
+        if (s.kind == SK_ID) continue;
+        Gate g;
+        g.kind = kind_of_skind(s.kind);
+        g.q[0] = s.q[0];
+        g.q[1] = s.nq > 1 ? s.q[1] : -1;
+        g.angle = s.angle;
+        g.expr = s.expr;
+        out.push_back(std::move(g));
+    }
+    gates->swap(out);
+    return QTB_OK;
+}
+
+// ------------------------------------------------------ bucket network
+struct TRec {
+    int32_t kind;
+    Expr expr;
+    std::vector<int32_t> vars;   // native axis order
+};
+
+struct Ref {
+    bool table = false;
+    int32_t id = -1;                // local entry id or op id
+    std::vector<int32_t> vars;      // sorted new ids, sliced ones included
+};
+
+struct OpRec {
+    int32_t u = 0, sum = 0, w = 0;
+    std::vector<Ref> inputs;
+    std::vector<uint32_t> masks;
+    int32_t level = 0;
+    int32_t consumer_level = 0;
+    uint32_t dst = 0;
+};
+
+}  // namespace
+
+// Greedy min-degree order over the line graph (nodes in first-appearance
+// order); returns the order and the degree of every eliminated node.
+static void greedy_order(int V, const std::vector<std::vector<int32_t>>& cliques,
+                         std::vector<int32_t>* order, std::vector<int32_t>* degrees) {
+    const int W = (V + 63) / 64;
+    std::vector<uint64_t> adj((size_t)V * W, 0);
+    auto test = [&](int a, int b) { return (adj[(size_t)a * W + (b >> 6)] >> (b & 63)) & 1; };
+    auto set = [&](int a, int b) { adj[(size_t)a * W + (b >> 6)] |= 1ull << (b & 63); };
+    auto clr = [&](int a, int b) { adj[(size_t)a * W + (b >> 6)] &= ~(1ull << (b & 63)); };
+    std::vector<int32_t> deg(V, 0);
+    for (const auto& c : cliques)
+        for (size_t i = 0; i < c.size(); ++i)
+            for (size_t j = i + 1; j < c.size(); ++j) {
+                int a = c[i], b = c[j];
+                if (a != b && !test(a, b)) {
+                    set(a, b);
+                    set(b, a);
+                    ++deg[a];
+                    ++deg[b];
+                }
+            }
+    std::vector<int32_t> alive(V);
+    std::iota(alive.begin(), alive.end(), 0);
+    std::vector<int32_t> nbrs;
+    order->clear();
+    degrees->clear();
+    while (!alive.empty()) {
+        size_t best = 0;
+        for (size_t i = 1; i < alive.size(); ++i)
+            if (deg[alive[i]] < deg[alive[best]]) best = i;
+        const int x = alive[best];
+        alive.erase(alive.begin() + best);
+        nbrs.clear();
+        for (int w = 0; w < W; ++w) {
+            uint64_t bits = adj[(size_t)x * W + w];
+            while (bits) {
+                int b = __builtin_ctzll(bits);
+                nbrs.push_back(w * 64 + b);
+                bits &= bits - 1;
+            }
+        }
+        order->push_back(x);
+        degrees->push_back((int32_t)nbrs.size());
+        for (int a : nbrs) {
+            clr(a, x);
+            --deg[a];
+        }
+        for (size_t i = 0; i < nbrs.size(); ++i)
+            for (size_t j = i + 1; j < nbrs.size(); ++j) {
+                int a = nbrs[i], b = nbrs[j];
+                if (!test(a, b)) {
+                    set(a, b);
+                    set(b, a);
+                    ++deg[a];
+                    ++deg[b];
+                }
+            }
+    }
+}
+
+int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
+                    int32_t simplify_passes, const double* params, int32_t n_params,
+                    Network* out, std::string* err) {
+    if (n_qubits <= 0 || n_gates < 0 || (n_gates > 0 && in_gates == nullptr)) {
+        *err = "compile: invalid circuit arguments";
+        return QTB_ERR_ARG;
+    }
+    // ---- gates with numeric and symbolic angles
+    std::vector<Gate> gates(n_gates);
+    for (int i = 0; i < n_gates; ++i) {
+        const qtb_gate& g = in_gates[i];
+        if (g.kind < QTB_GATE_M || g.kind > QTB_GATE_T) {
+            *err = "compile: unknown gate kind " + std::to_string(g.kind);
+            return QTB_ERR_ARG;
+        }
+        const int nq = qubits_of_kind(g.kind);
+        if (g.q0 < 0 || g.q0 >= n_qubits || (nq == 2 && (g.q1 < 0 || g.q1 >= n_qubits || g.q1 == g.q0))) {
+            *err = "compile: gate " + std::to_string(i) + " has qubits out of range";
+            return QTB_ERR_ARG;
+        }
+        Gate& o = gates[i];
+        o.kind = g.kind;
+        o.q[0] = g.q0;
+        o.q[1] = nq == 2 ? g.q1 : -1;
+        o.angle = 0.0;
+        if (is_parametric(g.kind)) {
+            if (g.param < 0 || g.param >= n_params || params == nullptr) {
+                *err = "compile: parametric gate " + std::to_string(i) + " has no parameter";
+                return QTB_ERR_ARG;
+            }
+            o.angle = g.coef * params[g.param];
+            if (g.coef != 0.0) o.expr.emplace_back(g.param, g.coef);
+        }
+    }
+    bool angle_specific = false;
+    for (int pass = 0; pass < simplify_passes; ++pass) {
+        int rc = simplify(&gates, &out->checks, &angle_specific, err);
+        if (rc) return rc;
+    }
+    // every qubit must keep a gate (n_qubits counts qubits that appear)
+    {
+        std::vector<char> seen(n_qubits, 0);
+        for (const Gate& g : gates) {
+            seen[g.q[0]] = 1;
+            if (g.q[1] >= 0) seen[g.q[1]] = 1;
+        }
+        for (int q = 0; q < n_qubits; ++q)
+            if (!seen[q]) {
+                *err = "compile: qubit " + std::to_string(q) + " has no gate";
+                return QTB_ERR_ARG;
+            }
+    }
+
+    // ---- qtree layout: bra vars 0..nq-1, gates from the bra side
+    const int nq = n_qubits;
+    std::vector<TRec> tensors;
+    std::vector<std::vector<int32_t>> buckets(nq);
+    std::vector<int32_t> frame(nq);
+    std::iota(frame.begin(), frame.end(), 0);
+    int32_t next_id = nq;
+    auto place = [&](int32_t kind, const Expr& expr, const int* qs, int nqub) {
+        TRec t;
+        t.kind = kind;
+        t.expr = expr;
+        const int cp = changed_position(kind);
+        int32_t new_id = next_id;
+        for (int i = 0; i < nqub; ++i) {
+            t.vars.push_back(frame[qs[i]]);
+            if (i == cp) t.vars.push_back(new_id++);
+        }
+        const int32_t smallest = *std::min_element(t.vars.begin(), t.vars.end());
+        buckets[smallest].push_back((int32_t)tensors.size());
+        tensors.push_back(std::move(t));
+        if (cp >= 0) {
+            frame[qs[cp]] = next_id++;
+            buckets.emplace_back();
+        }
+    };
+    const Expr none;
+    for (int q = 0; q < nq; ++q) place(QTB_GATE_M, none, &q, 1);
+    for (int i = (int)gates.size() - 1; i >= 0; --i)
+        place(gates[i].kind, gates[i].expr, gates[i].q, qubits_of_kind(gates[i].kind));
+    const int32_t ket_start = next_id;
+    for (int q = 0; q < nq; ++q) {
+        TRec t;
+        t.kind = QTB_GATE_M;
+        t.vars = {frame[q], next_id};
+        buckets[frame[q]].push_back((int32_t)tensors.size());
+        tensors.push_back(std::move(t));
+        buckets.emplace_back();
+        frame[q] = next_id++;
+    }
+    const int32_t n_vars = next_id;
+    auto ignored = [&](int32_t v) { return v < nq || v >= ket_start; };
+
+    // ---- line graph (first-appearance node order) and greedy order
+    std::vector<int32_t> node_of(n_vars, -1), var_of;
+    std::vector<std::vector<int32_t>> cliques;
+    for (const auto& b : buckets)
+        for (int32_t ti : b) {
+            std::vector<int32_t> c;
+            for (int32_t v : tensors[ti].vars) {
+                if (ignored(v)) continue;
+                if (node_of[v] < 0) {
+                    node_of[v] = (int32_t)var_of.size();
+                    var_of.push_back(v);
+                }
+                c.push_back(node_of[v]);
+            }
+            if (c.size() > 1) cliques.push_back(std::move(c));
+        }
+    std::vector<int32_t> gorder, gdeg;
+    greedy_order((int)var_of.size(), cliques, &gorder, &gdeg);
+    std::vector<int32_t>& peo = out->peo;
+    peo.clear();
+    for (int q = 0; q < nq; ++q) peo.push_back(ket_start + q);
+    for (int q = 0; q < nq; ++q) peo.push_back(q);
+    for (int32_t x : gorder) peo.push_back(var_of[x]);
+    if ((int32_t)peo.size() != n_vars) {
+        *err = "compile: elimination order does not cover every variable";
+        return QTB_ERR_ARG;
+    }
+    std::vector<int32_t> perm(n_vars);
+    for (int32_t i = 0; i < n_vars; ++i) perm[peo[i]] = i;
+    const int32_t n_sliced = 2 * nq;
+
+    // ---- reorder + slice: tensors become references to gate-table entries
+    std::vector<std::vector<Ref>> nb(n_vars);
+    std::map<EntryKey, int32_t> local;
+    for (const auto& b : buckets)
+        for (int32_t ti : b) {
+            const TRec& t = tensors[ti];
+            const int r = (int)t.vars.size();
+            std::vector<int> axes(r);
+            std::iota(axes.begin(), axes.end(), 0);
+            std::sort(axes.begin(), axes.end(),
+                      [&](int x, int y) { return perm[t.vars[x]] < perm[t.vars[y]]; });
+            EntryKey key;
+            key.kind = t.kind;
+            key.expr = t.expr;
+            key.rank_in = (int8_t)r;
+            key.sliced_mask = 0;
+            Ref ref;
+            ref.table = true;
+            for (int a : axes) {
+                const int32_t nv = perm[t.vars[a]];
+                ref.vars.push_back(nv);
+                if (nv < n_sliced) key.sliced_mask |= (uint8_t)(1u << a);
+                else key.perm.push_back((int8_t)a);
+            }
+            auto it = local.find(key);
+            if (it == local.end()) {
+                it = local.emplace(key, (int32_t)out->entries.size()).first;
+                out->entries.push_back(key);
+            }
+            ref.id = it->second;
+            nb[ref.vars[0]].push_back(std::move(ref));
+        }
+
+    // ---- symbolic bucket elimination
+    std::vector<OpRec> ops;
+    std::vector<Ref> scalars;
+    double ref_flops = 0.0;
+    int32_t max_rank = 0;
+    auto live_count = [&](const std::vector<int32_t>& vs) {
+        int c = 0;
+        for (int32_t v : vs) c += v >= n_sliced;
+        return c;
+    };
+    for (int32_t n = 0; n < n_vars; ++n) {
+        std::vector<Ref>& b = nb[n];
+        if (b.empty()) continue;
+        std::vector<int32_t> U;
+        for (const Ref& r : b) U.insert(U.end(), r.vars.begin(), r.vars.end());
+        std::sort(U.begin(), U.end());
+        U.erase(std::unique(U.begin(), U.end()), U.end());
+        if (U.empty() || U[0] != n) {
+            *err = "compile: bucket " + std::to_string(n) + " holds a tensor without its variable";
+            return QTB_ERR_ARG;
+        }
+        ref_flops += std::ldexp(1.0, (int)U.size() - 1) * (double)(1 + b.size());
+        std::vector<int32_t> outv(U.begin() + 1, U.end());
+        Ref res;
+        const bool live = n >= n_sliced;
+        if (b.size() == 1 && !live) {
+            res = b[0];      // product of one tensor over a size-1 variable: a copy
+            res.vars = outv;
+        } else {
+            OpRec op;
+            std::vector<int32_t> liveU;
+            for (int32_t v : U)
+                if (v >= n_sliced) liveU.push_back(v);
+            op.u = (int32_t)liveU.size();
+            op.sum = live ? 1 : 0;
+            op.w = op.u - op.sum;
+            if (op.u > QTB_MAX_BUCKET_VARS) {
+                *err = "compile: bucket of " + std::to_string(op.u) + " variables exceeds the limit";
+                return QTB_ERR_UNSUPPORTED;
+            }
+            max_rank = std::max(max_rank, op.u);
+            for (const Ref& r : b) {
+                uint32_t m = 0;
+                for (int32_t v : r.vars) {
+                    if (v < n_sliced) continue;
+                    const int pos = (int)(std::lower_bound(liveU.begin(), liveU.end(), v) - liveU.begin());
+                    m |= 1u << (op.u - 1 - pos);
+                }
+                op.masks.push_back(m);
+                op.inputs.push_back(r);
+            }
+            res.table = false;
+            res.id = (int32_t)ops.size();
+            res.vars = outv;
+            ops.push_back(std::move(op));
+        }
+        if (outv.empty()) scalars.push_back(std::move(res));
+        else nb[outv[0]].push_back(std::move(res));
+        b.clear();
+        b.shrink_to_fit();
+    }
+    if (scalars.empty()) {
+        *err = "compile: network has no scalar result";
+        return QTB_ERR_ARG;
+    }
+    Ref result;
+    if (scalars.size() == 1) {
+        result = scalars[0];
+    } else {
+        OpRec op;
+        op.u = op.sum = op.w = 0;
+        for (const Ref& r : scalars) {
+            op.inputs.push_back(r);
+            op.masks.push_back(0);
+        }
+        result.table = false;
+        result.id = (int32_t)ops.size();
+        ops.push_back(std::move(op));
+    }
+
+    // ---- dependency levels, arena intervals
+    int32_t max_level = 0;
+    for (OpRec& op : ops) {
+        int32_t lv = 0;
+        for (const Ref& r : op.inputs)
+            if (!r.table) lv = std::max(lv, ops[r.id].level);
+        op.level = lv + 1;
+        max_level = std::max(max_level, op.level);
+    }
+    for (OpRec& op : ops)
+        for (const Ref& r : op.inputs)
+            if (!r.table) ops[r.id].consumer_level = op.level;
+    if (!result.table) ops[result.id].consumer_level = max_level + 1;
+    std::vector<int32_t> by_level(ops.size());
+    std::iota(by_level.begin(), by_level.end(), 0);
+    std::stable_sort(by_level.begin(), by_level.end(),
+                     [&](int32_t x, int32_t y) { return ops[x].level < ops[y].level; });
+    struct Live { uint32_t off, size; int32_t end; };
+    std::vector<Live> active;
+    uint32_t arena = 0, max_elems = 1;
+    for (int32_t oi : by_level) {
+        OpRec& op = ops[oi];
+        active.erase(std::remove_if(active.begin(), active.end(),
+                                    [&](const Live& l) { return l.end < op.level; }),
+                     active.end());
+        const uint32_t size = 1u << op.w;
+        max_elems = std::max(max_elems, size);
+        const uint32_t need = (size + 3u) & ~3u;
+        std::sort(active.begin(), active.end(), [](const Live& a, const Live& b) { return a.off < b.off; });
+        uint32_t off = 0;
+        for (const Live& l : active) {
+            if (off + need <= l.off) break;
+            off = std::max(off, l.off + l.size);
+        }
+        op.dst = off;
+        active.push_back({off, need, op.consumer_level});
+        arena = std::max(arena, off + need);
+    }
+
+    // ---- device images: ops in phase order
+    out->ops.clear();
+    out->ins.clear();
+    out->phases.clear();
+    double alg_bytes = 0.0, alg_flops = 0.0;
+    size_t cursor = 0;
+    for (int32_t lv = 1; lv <= max_level; ++lv) {
+        DevPhase ph{};
+        ph.op_first = (uint32_t)out->ops.size();
+        uint32_t elems = 0;
+        while (cursor < by_level.size() && ops[by_level[cursor]].level == lv) {
+            const OpRec& op = ops[by_level[cursor++]];
+            DevOp d{};
+            d.u = (uint8_t)op.u;
+            d.sum = (uint8_t)op.sum;
+            d.k = (uint8_t)op.inputs.size();
+            d.dst = op.dst;
+            d.elem_begin = elems;
+            d.in_begin = (uint32_t)out->ins.size();
+            for (size_t t = 0; t < op.inputs.size(); ++t) {
+                const Ref& r = op.inputs[t];
+                DevIn in{};
+                in.mask = op.masks[t];
+                in.src = r.table ? (kSrcTable | (uint32_t)r.id) : ops[r.id].dst;
+                out->ins.push_back(in);
+                alg_bytes += 8.0 * std::ldexp(1.0, __builtin_popcount(in.mask));
+            }
+            alg_bytes += 8.0 * std::ldexp(1.0, op.w);
+            alg_flops += 6.0 * (double)(op.inputs.size() - 1) * std::ldexp(1.0, op.u) +
+                         (op.sum ? 2.0 * std::ldexp(1.0, op.w) : 0.0);
+            elems += 1u << op.w;
+            out->ops.push_back(d);
+        }
+        ph.op_count = (uint32_t)out->ops.size() - ph.op_first;
+        ph.total_elems = elems;
+        out->phases.push_back(ph);
+    }
+    out->result_src = result.table ? (kSrcTable | (uint32_t)result.id) : ops[result.id].dst;
+    out->max_elems = max_elems;
+    qtb_network_info& info = out->info;
+    info.n_qubits = nq;
+    info.n_vars = n_vars;
+    info.treewidth = gdeg.empty() ? 0 : *std::max_element(gdeg.begin(), gdeg.end());
+    info.max_rank = max_rank;
+    info.n_ops = (int32_t)out->ops.size();
+    info.n_phases = (int32_t)out->phases.size();
+    info.arena_elems = (int32_t)arena;
+    info.angle_specific = angle_specific ? 1 : 0;
+    info.alg_bytes = alg_bytes;
+    info.alg_flops = alg_flops;
+    info.ref_flops = ref_flops;
+    return QTB_OK;
+}
+
+// ------------------------------------------------------ native lightcone
+int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indices, int32_t u,
+                    int32_t v, int32_t p, int32_t composer, std::vector<qtb_gate>* gates,
+                    int32_t* n_qubits, std::string* err) {
+    if (n_nodes <= 0 || !indptr || !indices || u < 0 || v < 0 || u >= n_nodes || v >= n_nodes ||
+        u == v || p < 1 || composer < 0 || composer > 2) {
+        *err = "lightcone: invalid arguments";
+        return QTB_ERR_ARG;
+    }
+    // BFS from the edge, radius p
+    std::vector<int32_t> frontier = {u, v}, cone = {u, v};
+    std::map<int32_t, int32_t> dist = {{u, 0}, {v, 0}};
+    for (int d = 1; d <= p; ++d) {
+        std::vector<int32_t> next;
+        for (int32_t x : frontier)
+            for (int64_t e = indptr[x]; e < indptr[x + 1]; ++e) {
+                const int32_t y = indices[e];
+                if (y < 0 || y >= n_nodes) {
+                    *err = "lightcone: neighbour id out of range";
+                    return QTB_ERR_ARG;
+                }
+                if (dist.emplace(y, d).second) {
+                    next.push_back(y);
+                    cone.push_back(y);
+                }
+            }
+        frontier.swap(next);
+    }
+    std::sort(cone.begin(), cone.end());
+    std::map<int32_t, int32_t> qubit;
+    for (size_t i = 0; i < cone.size(); ++i) qubit[cone[i]] = (int32_t)i;
+    const int32_t nq = (int32_t)cone.size();
+    std::vector<qtb_gate> ansatz;
+    auto add = [&](int32_t kind, int32_t a, int32_t b, int32_t param, double coef) {
+        ansatz.push_back(qtb_gate{kind, a, b, param, coef});
+    };
+    for (int32_t q = 0; q < nq; ++q) add(QTB_GATE_H, q, -1, -1, 0.0);
+    for (int32_t l = 0; l < p; ++l) {
+        const int32_t radius = p - l;
+        for (int32_t x : cone) {
+            if (dist[x] > radius) continue;
+            std::vector<int32_t> nb;
+            for (int64_t e = indptr[x]; e < indptr[x + 1]; ++e) {
+                const int32_t y = indices[e];
+                if (y > x && dist.count(y) && dist[y] <= radius) nb.push_back(y);
+            }
+            std::sort(nb.begin(), nb.end());
+            nb.erase(std::unique(nb.begin(), nb.end()), nb.end());
+            for (int32_t y : nb) {
+                const int32_t a = qubit[x], b = qubit[y];
+                if (composer == 2) {
+                    add(QTB_GATE_CX, a, b, -1, 0.0);
+                    add(QTB_GATE_ZPHASE, b, -1, l, 2.0);
+                    add(QTB_GATE_CX, a, b, -1, 0.0);
+                } else {
+                    add(QTB_GATE_ZZ, a, b, l, 2.0);
+                }
+            }
+        }
+        for (int32_t x : cone)
+            if (dist[x] <= radius) add(QTB_GATE_XPHASE, qubit[x], -1, p + l, 2.0);
+    }
+    gates->clear();
+    gates->insert(gates->end(), ansatz.begin(), ansatz.end());
+    gates->push_back(qtb_gate{QTB_GATE_Z, qubit[u], -1, -1, 0.0});
+    gates->push_back(qtb_gate{QTB_GATE_Z, qubit[v], -1, -1, 0.0});
+    for (auto it = ansatz.rbegin(); it != ansatz.rend(); ++it) {
+        qtb_gate g = *it;
+        g.coef = -g.coef;   // G(alpha)^+ = G(-alpha) for ZZ / XPhase / ZPhase
+        gates->push_back(g);
+    }
+    *n_qubits = nq;
+    return QTB_OK;
+}
+
+// ------------------------------------------------------ plan assembly
+void merge_network(qtb_plan* plan, Network&& net) {
+    std::vector<uint32_t> table_off(net.entries.size());
+    for (size_t i = 0; i < net.entries.size(); ++i) {
+        const EntryKey& key = net.entries[i];
+        auto it = plan->entry_index.find(key);
+        if (it == plan->entry_index.end()) {
+            DevEntry e{};
+            e.kind = key.kind;
+            e.expr_begin = (int32_t)plan->terms.size();
+            e.expr_count = (int32_t)key.expr.size();
+            for (const auto& t : key.expr) plan->terms.push_back(DevTerm{t.first, 0, t.second});
+            e.off = plan->table_elems;
+            e.rank_in = key.rank_in;
+            e.rank_out = (int8_t)key.perm.size();
+            e.sliced_mask = key.sliced_mask;
+            for (int a = 0; a < 5; ++a) e.perm[a] = a < (int)key.perm.size() ? key.perm[a] : -1;
+            plan->table_elems += 1u << e.rank_out;
+            it = plan->entry_index.emplace(key, (int32_t)plan->entries.size()).first;
+            plan->entries.push_back(e);
+        }
+        table_off[i] = plan->entries[it->second].off;
+    }
+    for (DevIn& in : net.ins)
+        if (in.src & kSrcTable) in.src = kSrcTable | table_off[in.src & ~kSrcTable];
+    if (net.result_src & kSrcTable) net.result_src = kSrcTable | table_off[net.result_src & ~kSrcTable];
+    for (AngleCheck& c : net.checks) plan->checks.push_back(c);
+    net.entries.clear();
+    net.entries.shrink_to_fit();
+    plan->nets.push_back(std::move(net));
+    plan->uploaded = false;
+}
+
+void flatten_plan(qtb_plan* plan) {
+    plan->dnets.clear();
+    plan->dops.clear();
+    plan->dins.clear();
+    plan->dphases.clear();
+    for (const Network& n : plan->nets) {
+        DevNet d{};
+        d.op_begin = (uint32_t)plan->dops.size();
+        d.n_ops = (uint32_t)n.ops.size();
+        d.phase_begin = (uint32_t)plan->dphases.size();
+        d.n_phases = (uint32_t)n.phases.size();
+        d.arena_elems = (uint32_t)n.info.arena_elems;
+        d.result_src = n.result_src;
+        d.max_elems = n.max_elems;
+        const uint32_t in_base = (uint32_t)plan->dins.size();
+        for (DevOp op : n.ops) {
+            op.in_begin += in_base;
+            plan->dops.push_back(op);
+        }
+        plan->dins.insert(plan->dins.end(), n.ins.begin(), n.ins.end());
+        for (DevPhase ph : n.phases) {
+            ph.op_first += d.op_begin;
+            plan->dphases.push_back(ph);
+        }
+        plan->dnets.push_back(d);
+    }
+}
+
+}  // namespace qtb
+
+// =================================================================== C ABI
+using namespace qtb;
+
+extern "C" {
+
+int qtb_last_error(char* buf, size_t len) {
+    if (!buf || len == 0) return QTB_ERR_ARG;
+    std::strncpy(buf, g_err.c_str(), len - 1);
+    buf[len - 1] = '\0';
+    return QTB_OK;
+}
+
+int qtb_plan_create(int32_t n_params, qtb_plan** out) {
+    if (!out || n_params < 0) return fail(QTB_ERR_ARG, "plan_create: bad arguments");
+    qtb_plan* p = new qtb_plan();
+    p->n_params = n_params;
+    *out = p;
+    return QTB_OK;
+}
+
+int qtb_plan_add_circuit(qtb_plan* plan, int32_t n_qubits, const qtb_gate* gates, int32_t n_gates,
+                         int32_t simplify_passes, const double* params, int32_t* net_index) {
+    if (!plan) return fail(QTB_ERR_ARG, "plan_add_circuit: null plan");
+    Network net;
+    std::string err;
+    int rc = compile_circuit(n_qubits, gates, n_gates, simplify_passes, params, plan->n_params,
+                             &net, &err);
+    if (rc) return fail(rc, err);
+    std::lock_guard<std::mutex> lock(plan->mu);
+    if (net_index) *net_index = (int32_t)plan->nets.size();
+    merge_network(plan, std::move(net));
+    return QTB_OK;
+}
+
+int qtb_plan_add_lightcone(qtb_plan* plan, int32_t n_nodes, const int64_t* indptr,
+                           const int32_t* indices, int32_t u, int32_t v, int32_t p,
+                           int32_t composer, const double* params, int32_t* net_index) {
+    if (!plan) return fail(QTB_ERR_ARG, "plan_add_lightcone: null plan");
+    if (plan->n_params != 2 * p) return fail(QTB_ERR_ARG, "plan_add_lightcone: plan needs 2*p params");
+    std::vector<qtb_gate> gates;
+    int32_t nq = 0;
+    std::string err;
+    int rc = build_lightcone(n_nodes, indptr, indices, u, v, p, composer, &gates, &nq, &err);
+    if (rc) return fail(rc, err);
+    return qtb_plan_add_circuit(plan, nq, gates.data(), (int32_t)gates.size(),
+                                composer == 0 ? 2 : 0, params, net_index);
+}
+
+int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indptr,
+                            const int32_t* indices, const int32_t* edges, int32_t n_edges,
+                            int32_t p, int32_t composer, const double* params, int32_t n_threads,
+                            int32_t* first_net_index) {
+    if (!plan || !edges || n_edges < 0) return fail(QTB_ERR_ARG, "plan_add_lightcones: bad arguments");
+    if (plan->n_params != 2 * p) return fail(QTB_ERR_ARG, "plan_add_lightcones: plan needs 2*p params");
+    std::vector<Network> nets(n_edges);
+    std::vector<int> codes(n_edges, 0);
+    std::vector<std::string> errs(n_edges);
+    std::atomic<int32_t> next{0};
+    auto worker = [&]() {
+        std::vector<qtb_gate> gates;
+        for (;;) {
+            const int32_t i = next.fetch_add(1);
+            if (i >= n_edges) break;
+            int32_t nq = 0;
+            int rc = build_lightcone(n_nodes, indptr, indices, edges[2 * i], edges[2 * i + 1], p,
+                                     composer, &gates, &nq, &errs[i]);
+            if (!rc)
+                rc = compile_circuit(nq, gates.data(), (int32_t)gates.size(), composer == 0 ? 2 : 0,
+                                     params, plan->n_params, &nets[i], &errs[i]);
+            codes[i] = rc;
+        }
+    };
+    int nt = n_threads > 0 ? n_threads : (int)std::thread::hardware_concurrency();
+    nt = std::max(1, std::min(nt, std::max(1, n_edges)));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& t : pool) t.join();
+    for (int32_t i = 0; i < n_edges; ++i)
+        if (codes[i]) return fail(codes[i], "edge " + std::to_string(i) + ": " + errs[i]);
+    std::lock_guard<std::mutex> lock(plan->mu);
+    if (first_net_index) *first_net_index = (int32_t)plan->nets.size();
+    for (auto& n : nets) merge_network(plan, std::move(n));
+    return QTB_OK;
+}
+
+int qtb_plan_n_networks(const qtb_plan* plan, int32_t* n) {
+    if (!plan || !n) return fail(QTB_ERR_ARG, "plan_n_networks: bad arguments");
+    *n = (int32_t)plan->nets.size();
+    return QTB_OK;
+}
+
+int qtb_plan_network_info(const qtb_plan* plan, int32_t net, qtb_network_info* info) {
+    if (!plan || !info || net < 0 || net >= (int32_t)plan->nets.size())
+        return fail(QTB_ERR_ARG, "plan_network_info: bad arguments");
+    *info = plan->nets[net].info;
+    return QTB_OK;
+}
+
+int qtb_plan_network_peo(const qtb_plan* plan, int32_t net, int32_t* peo, int32_t cap, int32_t* n) {
+    if (!plan || !n || net < 0 || net >= (int32_t)plan->nets.size())
+        return fail(QTB_ERR_ARG, "plan_network_peo: bad arguments");
+    const auto& src = plan->nets[net].peo;
+    *n = (int32_t)src.size();
+    if (peo) std::copy(src.begin(), src.begin() + std::min<size_t>(src.size(), (size_t)std::max(cap, 0)), peo);
+    return QTB_OK;
+}
+
+int qtb_plan_check_params(const qtb_plan* plan, const double* params, int32_t* valid) {
+    if (!plan || !valid || (plan->n_params > 0 && !params))
+        return fail(QTB_ERR_ARG, "plan_check_params: bad arguments");
+    *valid = 1;
+    for (const AngleCheck& c : plan->checks) {
+        double x = 0.0;
+        for (const auto& t : c.expr) x += t.second * params[t.first];
+        const bool small = std::fabs(x) < 1e-5;
+        if (small != c.must_be_small) {
+            *valid = 0;
+            break;
+        }
+    }
+    return QTB_OK;
+}
+
+int qtb_plan_export(qtb_plan* plan, int32_t which, void* buf, size_t cap, size_t* size) {
+    if (!plan || !size) return fail(QTB_ERR_ARG, "plan_export: bad arguments");
+    std::lock_guard<std::mutex> lock(plan->mu);
+    flatten_plan(plan);
+    const void* src = nullptr;
+    size_t n = 0;
+    switch (which) {
+        case 0: src = plan->dnets.data(); n = plan->dnets.size() * sizeof(DevNet); break;
+        case 1: src = plan->dops.data(); n = plan->dops.size() * sizeof(DevOp); break;
+        case 2: src = plan->dins.data(); n = plan->dins.size() * sizeof(DevIn); break;
+        case 3: src = plan->dphases.data(); n = plan->dphases.size() * sizeof(DevPhase); break;
+        case 4: src = plan->entries.data(); n = plan->entries.size() * sizeof(DevEntry); break;
+        case 5: src = plan->terms.data(); n = plan->terms.size() * sizeof(DevTerm); break;
+        default: return fail(QTB_ERR_ARG, "plan_export: unknown array");
+    }
+    *size = n;
+    if (buf && n) std::memcpy(buf, src, std::min(cap, n));
+    return QTB_OK;
+}
+
+int qtb_plan_table_elems(const qtb_plan* plan, int64_t* n) {
+    if (!plan || !n) return fail(QTB_ERR_ARG, "plan_table_elems: bad arguments");
+    *n = plan->table_elems;
+    return QTB_OK;
+}
+
+}  // extern "C"

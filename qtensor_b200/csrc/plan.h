@@ -1,0 +1,159 @@
+// Internal plan structures shared by the host plan compiler (plan.cpp) and
+// the device executor (qtb.cu).  Not part of the public C ABI.
+#pragma once
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/qtb.h"
+
+namespace qtb {
+
+// Flag on DevIn::src / DevNet::result_src: the operand lives in the gate
+// table, not in the network's arena.
+constexpr uint32_t kSrcTable = 0x80000000u;
+
+// One bucket kernel of a network (device layout, 16 bytes).
+struct DevOp {
+    uint8_t u;          // live (binary) variables in the bucket's union
+    uint8_t sum;        // 1: sum over union variable 0 (the bucket variable)
+    uint8_t k;          // number of input tensors
+    uint8_t pad;
+    uint32_t dst;       // arena offset of the output (complex64 elements)
+    uint32_t elem_begin;  // first flattened element of this op within its phase
+    uint32_t in_begin;  // index of the first DevIn of this op
+};
+
+// One operand of an op: which union bits it holds, where it lives.
+struct DevIn {
+    uint32_t mask;      // bit (u-1-v) set <=> union variable v is an axis
+    uint32_t src;       // arena offset, or kSrcTable | gate-table offset
+};
+
+// Ops of one dependency level; a barrier follows every phase.
+struct DevPhase {
+    uint32_t op_first;
+    uint32_t op_count;
+    uint32_t total_elems;
+    uint32_t pad;
+};
+
+// One network (edge term).
+struct DevNet {
+    uint32_t op_begin;
+    uint32_t n_ops;
+    uint32_t phase_begin;
+    uint32_t n_phases;
+    uint32_t arena_elems;
+    uint32_t result_src;   // arena offset or kSrcTable | offset of the scalar
+    uint32_t max_elems;    // largest op output (elements)
+    uint32_t pad;
+};
+
+// Gate-table entry: the tensor of a gate, sliced and transposed into the
+// sorted-variable layout the network reads (device layout).
+struct DevEntry {
+    int32_t kind;
+    int32_t expr_begin;    // into the DevTerm array
+    int32_t expr_count;
+    uint32_t off;          // complex64 offset in the gate table
+    int8_t rank_in;        // axes of the gate tensor as generated
+    int8_t rank_out;       // axes kept (not sliced)
+    uint8_t sliced_mask;   // native axes fixed to index 0
+    int8_t perm[5];        // output axis a <- native axis perm[a]
+};
+
+struct DevTerm {
+    int32_t param;
+    int32_t pad;
+    double coef;
+};
+
+static_assert(sizeof(DevOp) == 16, "DevOp layout");
+static_assert(sizeof(DevIn) == 8, "DevIn layout");
+static_assert(sizeof(DevPhase) == 16, "DevPhase layout");
+static_assert(sizeof(DevNet) == 32, "DevNet layout");
+static_assert(sizeof(DevEntry) == 24, "DevEntry layout");
+static_assert(sizeof(DevTerm) == 16, "DevTerm layout");
+
+// Linear angle expression: sum coef_i * params[param_i], sorted by param.
+using Expr = std::vector<std::pair<int32_t, double>>;
+
+struct EntryKey {
+    int32_t kind;
+    Expr expr;
+    int8_t rank_in;
+    uint8_t sliced_mask;
+    std::vector<int8_t> perm;
+    bool operator<(const EntryKey& o) const;
+};
+
+// A simplifier decision that holds only for some angles.
+struct AngleCheck {
+    Expr expr;
+    bool must_be_small;   // true: |expr| < 1e-5 (cancelled); false: >= 1e-5 (merged)
+};
+
+struct Network {
+    qtb_network_info info{};
+    std::vector<int32_t> peo;          // qtree-layout variable ids
+    std::vector<DevOp> ops;
+    std::vector<DevIn> ins;            // src of table operands: kSrcTable | local entry id
+    std::vector<DevPhase> phases;
+    std::vector<EntryKey> entries;     // local gate-table entries
+    std::vector<AngleCheck> checks;
+    uint32_t result_src = 0;
+    uint32_t max_elems = 1;
+};
+
+struct DeviceBuffers {
+    void* nets = nullptr;
+    void* ops = nullptr;
+    void* ins = nullptr;
+    void* phases = nullptr;
+    void* entries = nullptr;
+    void* terms = nullptr;
+    void* table = nullptr;        // complex64 gate table
+    void* status = nullptr;       // int error word
+    void* partials = nullptr;     // per-block fp64 partial sums
+    size_t partials_cap = 0;
+};
+
+}  // namespace qtb
+
+struct qtb_plan {
+    int32_t n_params = 0;
+    std::vector<qtb::Network> nets;
+    // global gate table, built from the networks' local entries
+    std::map<qtb::EntryKey, int32_t> entry_index;
+    std::vector<qtb::DevEntry> entries;
+    std::vector<qtb::DevTerm> terms;
+    uint32_t table_elems = 0;
+    std::vector<qtb::AngleCheck> checks;
+    // flattened device images
+    std::vector<qtb::DevNet> dnets;
+    std::vector<qtb::DevOp> dops;
+    std::vector<qtb::DevIn> dins;
+    std::vector<qtb::DevPhase> dphases;
+    bool uploaded = false;
+    int device = -1;
+    qtb::DeviceBuffers dev;
+    std::mutex mu;
+};
+
+namespace qtb {
+// plan.cpp
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int compile_circuit(int32_t n_qubits, const qtb_gate* gates, int32_t n_gates,
+                    int32_t simplify_passes, const double* params, int32_t n_params,
+                    Network* out, std::string* err);
+int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indices,
+                    int32_t u, int32_t v, int32_t p, int32_t composer,
+                    std::vector<qtb_gate>* gates, int32_t* n_qubits, std::string* err);
+void merge_network(qtb_plan* plan, Network&& net);
+void flatten_plan(qtb_plan* plan);
+int rank_of_kind(int32_t kind);
+}  // namespace qtb

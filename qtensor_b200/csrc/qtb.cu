@@ -1,0 +1,578 @@
+// Device code and the device-facing C ABI of libqtb.so (sm_100a).
+//
+//   K1  qtb_bucket_kernel    one bucket of BucketBackend.process_bucket
+//                            (qtensor/ProcessingFrameworks.py:29-31,45-147):
+//                            product of the bucket's tensors over the sorted
+//                            union of their variables, summed over variable 0
+//   K0  qtb_table_kernel     gate tensors of a request generated from its
+//                            angles (qtree gate tensors, OpFactory.py:44-58)
+//   K3  qtb_network_kernel   a whole edge network (bucket_elimination,
+//                            Simulate.py:90-94) per CTA: its buckets run in
+//                            dependency phases, intermediates in shared
+//                            memory (or a per-CTA global arena)
+//   K4  qtb_energy_kernel    fp64 Neumaier sum of the edge terms and the
+//                            MaxCut post-processing (QAOASimulator.py:27-41)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "plan.h"
+
+namespace qtb {
+
+// ----------------------------------------------------------------- helpers
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// Parallel bit extract: the bits of x selected by m, packed from bit 0 up.
+__device__ __forceinline__ uint32_t pext32(uint32_t x, uint32_t m) {
+    uint32_t r = 0;
+    for (uint32_t bit = 1; m; bit <<= 1) {
+        const uint32_t low = m & (0u - m);
+        if (x & low) r |= bit;
+        m ^= low;
+    }
+    return r;
+}
+
+// ----------------------------------------------------------------- K1
+struct BucketArgs {
+    const float2* in[QTB_MAX_BUCKET_INPUTS];
+    uint32_t mask[QTB_MAX_BUCKET_INPUTS];
+    float2* out;
+    int32_t k;
+    int32_t w;     // output variables
+    int32_t sum;
+};
+
+__global__ void __launch_bounds__(256) qtb_bucket_kernel(const BucketArgs a) {
+    const uint64_t n_out = 1ull << a.w;
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n_out;
+         j += (uint64_t)gridDim.x * blockDim.x) {
+        float2 acc = make_float2(0.f, 0.f);
+        for (int s = 0; s <= a.sum; ++s) {
+            const uint32_t idx = (uint32_t)j | ((uint32_t)s << a.w);
+            float2 prod = a.in[0][pext32(idx, a.mask[0])];
+            for (int t = 1; t < a.k; ++t) prod = cmul(prod, a.in[t][pext32(idx, a.mask[t])]);
+            acc = s == 0 ? prod : make_float2(acc.x + prod.x, acc.y + prod.y);
+        }
+        a.out[j] = acc;
+    }
+}
+
+// ----------------------------------------------------------------- K0
+__device__ double2 gate_value(int kind, double alpha, const int* ix) {
+    const double r2 = 0.70710678118654752440;
+    double s, c;
+    switch (kind) {
+        case QTB_GATE_M: return make_double2(ix[0] == ix[1] ? 1.0 : 0.0, 0.0);
+        case QTB_GATE_H: return make_double2((ix[0] & ix[1]) ? -r2 : r2, 0.0);
+        case QTB_GATE_X: return make_double2(ix[0] != ix[1] ? 1.0 : 0.0, 0.0);
+        case QTB_GATE_Y:
+            if (ix[0] == ix[1]) return make_double2(0.0, 0.0);
+            return make_double2(0.0, ix[0] == 0 ? -1.0 : 1.0);
+        case QTB_GATE_Z: return make_double2(ix[0] ? -1.0 : 1.0, 0.0);
+        case QTB_GATE_T: return ix[0] ? make_double2(r2, r2) : make_double2(1.0, 0.0);
+        case QTB_GATE_CX: {
+            const bool on = ix[0] ? (ix[1] != ix[2]) : (ix[1] == ix[2]);
+            return make_double2(on ? 1.0 : 0.0, 0.0);
+        }
+        case QTB_GATE_CZ: return make_double2((ix[0] & ix[1]) ? -1.0 : 1.0, 0.0);
+        case QTB_GATE_ZPHASE:
+            if (!ix[0]) return make_double2(1.0, 0.0);
+            sincospi(alpha, &s, &c);
+            return make_double2(c, s);
+        case QTB_GATE_ZZ:
+            sincospi(alpha * 0.5, &s, &c);
+            return ix[0] == ix[1] ? make_double2(c, -s) : make_double2(c, s);
+        case QTB_GATE_XPHASE:
+        case QTB_GATE_YPHASE: {
+            double gs, gc;
+            sincospi(alpha * 0.5, &s, &c);   // cos/sin(pi alpha / 2); also the phase g
+            gc = c;
+            gs = s;
+            double2 m;
+            if (kind == QTB_GATE_XPHASE) {
+                m = ix[0] == ix[1] ? make_double2(c, 0.0) : make_double2(0.0, -s);
+            } else {
+                m = ix[0] == ix[1] ? make_double2(c, 0.0)
+                                   : make_double2(ix[0] == 0 ? -s : s, 0.0);
+            }
+            return make_double2(gc * m.x - gs * m.y, gc * m.y + gs * m.x);
+        }
+        default: return make_double2(0.0, 0.0);
+    }
+}
+
+__global__ void qtb_table_kernel(const DevEntry* entries, int n_entries, const DevTerm* terms,
+                                 const double* params, float2* table) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_entries; e += gridDim.x * blockDim.x) {
+        const DevEntry en = entries[e];
+        double alpha = 0.0;
+        for (int t = 0; t < en.expr_count; ++t)
+            alpha += terms[en.expr_begin + t].coef * params[terms[en.expr_begin + t].param];
+        const int n = 1 << en.rank_out;
+        for (int o = 0; o < n; ++o) {
+            int ix[5] = {0, 0, 0, 0, 0};
+            for (int a = 0; a < en.rank_out; ++a) ix[en.perm[a]] = (o >> (en.rank_out - 1 - a)) & 1;
+            const double2 v = gate_value(en.kind, alpha, ix);
+            table[en.off + o] = make_float2((float)v.x, (float)v.y);
+        }
+    }
+}
+
+// ----------------------------------------------------------------- K3
+struct Job {
+    const DevNet* net;
+    const DevOp* ops;
+    const DevIn* ins;
+    const DevPhase* phases;
+    const float2* table;
+    float2* term;
+};
+
+constexpr int kStatusArena = 1;
+
+template <bool kSmemArena>
+__global__ void __launch_bounds__(512) qtb_network_kernel(const Job* __restrict__ jobs,
+                                                          float2* __restrict__ gscratch,
+                                                          uint32_t arena_capacity,
+                                                          int* __restrict__ status) {
+    extern __shared__ float2 sarena[];
+    const Job job = jobs[blockIdx.x];
+    const DevNet net = *job.net;
+    if (net.arena_elems > arena_capacity) {
+        if (threadIdx.x == 0) atomicOr(status, kStatusArena);
+        return;
+    }
+    float2* arena = kSmemArena ? sarena : gscratch + (size_t)blockIdx.x * arena_capacity;
+    const DevPhase* phases = job.phases + net.phase_begin;
+    for (uint32_t p = 0; p < net.n_phases; ++p) {
+        const DevPhase ph = phases[p];
+        uint32_t oi = ph.op_first;
+        DevOp op = job.ops[oi];
+        uint32_t op_end = op.elem_begin + (1u << (op.u - op.sum));
+        for (uint32_t g = threadIdx.x; g < ph.total_elems; g += blockDim.x) {
+            while (g >= op_end) {
+                op = job.ops[++oi];
+                op_end = op.elem_begin + (1u << (op.u - op.sum));
+            }
+            const uint32_t w = op.u - op.sum;
+            const uint32_t j = g - op.elem_begin;
+            const DevIn* in = job.ins + op.in_begin;
+            float2 acc = make_float2(0.f, 0.f);
+            for (uint32_t s = 0; s <= op.sum; ++s) {
+                const uint32_t idx = j | (s << w);
+                float2 prod = make_float2(1.f, 0.f);
+                for (uint32_t t = 0; t < op.k; ++t) {
+                    const DevIn d = in[t];
+                    const uint32_t off = pext32(idx, d.mask);
+                    const float2 x = (d.src & kSrcTable) ? __ldg(job.table + (d.src & ~kSrcTable) + off)
+                                                         : arena[d.src + off];
+                    prod = t == 0 ? x : cmul(prod, x);
+                }
+                acc = s == 0 ? prod : make_float2(acc.x + prod.x, acc.y + prod.y);
+            }
+            arena[op.dst + j] = acc;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        *job.term = (net.result_src & kSrcTable) ? job.table[net.result_src & ~kSrcTable]
+                                                 : arena[net.result_src];
+    }
+}
+
+// ----------------------------------------------------------------- K4
+__device__ __forceinline__ void neumaier_add(double& sum, double& comp, double x) {
+    const double t = sum + x;
+    comp += fabs(sum) >= fabs(x) ? (sum - t) + x : (x - t) + sum;
+    sum = t;
+}
+
+__global__ void __launch_bounds__(256) qtb_energy_kernel(const float2* __restrict__ terms, int n,
+                                                         double* __restrict__ energy) {
+    __shared__ double ssum[256], scomp[256];
+    double s = 0.0, c = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) neumaier_add(s, c, (double)terms[i].x);
+    ssum[threadIdx.x] = s;
+    scomp[threadIdx.x] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ts = 0.0, tc = 0.0;
+        for (int i = 0; i < (int)blockDim.x; ++i) {
+            neumaier_add(ts, tc, ssum[i]);
+            neumaier_add(ts, tc, scomp[i]);
+        }
+        const double total = ts + tc;
+        *energy = ((double)n - total) * 0.5;
+    }
+}
+
+// ----------------------------------------------------------------- host
+static int cuda_fail(cudaError_t e, const char* what) {
+    return fail(QTB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define QTB_CUDA(call)                                     \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+constexpr uint32_t kSmemArenaLimitBytes = 200 * 1024;
+
+struct LaunchClass {
+    bool smem;
+    uint32_t capacity;     // arena elements per CTA
+    int threads;
+    int n_jobs;
+    size_t job_offset;     // into the job buffer
+    size_t scratch_offset; // elements into scratch (global class)
+};
+
+struct RunCache {
+    Job* jobs = nullptr;
+    std::vector<LaunchClass> classes;
+    size_t scratch_elems = 0;
+};
+
+}  // namespace qtb
+
+// plan-side device state kept outside the public struct
+struct qtb_plan_device {
+    std::map<std::tuple<int32_t, int32_t, uintptr_t>, qtb::RunCache> runs;
+    bool timing = false;
+    double kernel_ms = 0.0;
+    int64_t kernel_launches = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending, spare;
+};
+
+namespace qtb {
+static std::map<const qtb_plan*, qtb_plan_device*> g_dev;
+static std::mutex g_dev_mu;
+
+static qtb_plan_device* dev_state(const qtb_plan* p) {
+    std::lock_guard<std::mutex> lock(g_dev_mu);
+    auto it = g_dev.find(p);
+    if (it == g_dev.end()) it = g_dev.emplace(p, new qtb_plan_device()).first;
+    return it->second;
+}
+
+static void free_device(qtb_plan* plan) {
+    DeviceBuffers& d = plan->dev;
+    void* ptrs[] = {d.nets, d.ops, d.ins, d.phases, d.entries, d.terms, d.table, d.status, d.partials};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    d = DeviceBuffers();
+    qtb_plan_device* s = dev_state(plan);
+    for (auto& kv : s->runs)
+        if (kv.second.jobs) cudaFree(kv.second.jobs);
+    s->runs.clear();
+    plan->uploaded = false;
+}
+
+static void destroy_events(qtb_plan_device* s) {
+    for (auto* v : {&s->pending, &s->spare})
+        for (auto& e : *v) {
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+    s->pending.clear();
+    s->spare.clear();
+}
+
+template <typename T>
+static int upload_vec(const std::vector<T>& v, void** dst) {
+    const size_t bytes = std::max<size_t>(sizeof(T), v.size() * sizeof(T));
+    QTB_CUDA(cudaMalloc(dst, bytes));
+    if (!v.empty()) QTB_CUDA(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return QTB_OK;
+}
+
+static int threads_for(uint32_t max_elems) {
+    if (max_elems <= 128) return 64;
+    if (max_elems <= 1024) return 128;
+    if (max_elems <= 8192) return 256;
+    return 512;
+}
+
+static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms, RunCache* rc) {
+    // classes: smem arenas bucketed by size (4 KB, 16 KB, 64 KB, 200 KB), then global
+    const uint32_t bounds[] = {512, 2048, 8192, kSmemArenaLimitBytes / 8};
+    std::vector<std::vector<int32_t>> members(5);
+    for (int32_t i = first; i < first + count; ++i) {
+        const uint32_t a = plan->dnets[i].arena_elems;
+        int c = 4;
+        for (int b = 0; b < 4; ++b)
+            if (a <= bounds[b]) {
+                c = b;
+                break;
+            }
+        members[c].push_back(i);
+    }
+    std::vector<Job> jobs;
+    const auto* dn = static_cast<const DevNet*>(plan->dev.nets);
+    rc->classes.clear();
+    rc->scratch_elems = 0;
+    for (int c = 0; c < 5; ++c) {
+        if (members[c].empty()) continue;
+        LaunchClass lc{};
+        lc.smem = c < 4;
+        lc.job_offset = jobs.size();
+        lc.n_jobs = (int)members[c].size();
+        uint32_t cap = 4, maxe = 1;
+        for (int32_t i : members[c]) {
+            cap = std::max(cap, plan->dnets[i].arena_elems);
+            maxe = std::max(maxe, plan->dnets[i].max_elems);
+            Job j;
+            j.net = dn + i;
+            j.ops = static_cast<const DevOp*>(plan->dev.ops);
+            j.ins = static_cast<const DevIn*>(plan->dev.ins);
+            j.phases = static_cast<const DevPhase*>(plan->dev.phases);
+            j.table = static_cast<const float2*>(plan->dev.table);
+            j.term = terms + (i - first);
+            jobs.push_back(j);
+        }
+        lc.capacity = (cap + 3u) & ~3u;
+        lc.threads = threads_for(maxe);
+        if (!lc.smem) {
+            lc.scratch_offset = rc->scratch_elems;
+            rc->scratch_elems += (size_t)lc.capacity * lc.n_jobs;
+        }
+        rc->classes.push_back(lc);
+    }
+    void* buf = nullptr;
+    int r = upload_vec(jobs, &buf);
+    if (r) return r;
+    rc->jobs = static_cast<Job*>(buf);
+    return QTB_OK;
+}
+
+}  // namespace qtb
+
+using namespace qtb;
+
+extern "C" {
+
+const char* qtb_version(void) { return "qtensor_b200 0.1 (sm_100a)"; }
+
+int qtb_init(int device) {
+    int n = 0;
+    QTB_CUDA(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) return fail(QTB_ERR_ARG, "qtb_init: no such device");
+    QTB_CUDA(cudaSetDevice(device));
+    QTB_CUDA(cudaFuncSetAttribute(qtb_network_kernel<true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kSmemArenaLimitBytes));
+    return QTB_OK;
+}
+
+int qtb_bucket_c64(const qtb_bucket_desc* d, const void* const* inputs, void* output, void* stream) {
+    if (!d || !inputs || !output) return fail(QTB_ERR_ARG, "bucket: null argument");
+    if (d->n_inputs < 1 || d->n_inputs > QTB_MAX_BUCKET_INPUTS)
+        return fail(QTB_ERR_ARG, "bucket: n_inputs out of range");
+    if (d->n_vars < 0 || d->n_vars > QTB_MAX_BUCKET_VARS)
+        return fail(QTB_ERR_ARG, "bucket: n_vars out of range");
+    if ((d->sum_first != 0 && d->sum_first != 1) || (d->sum_first && d->n_vars < 1))
+        return fail(QTB_ERR_ARG, "bucket: sum_first needs at least one variable");
+    const uint32_t all = d->n_vars >= 32 ? 0xffffffffu : ((1u << d->n_vars) - 1u);
+    BucketArgs a{};
+    for (int t = 0; t < d->n_inputs; ++t) {
+        if (!inputs[t]) return fail(QTB_ERR_ARG, "bucket: null input pointer");
+        if (d->masks[t] & ~all) return fail(QTB_ERR_ARG, "bucket: mask names a variable outside the union");
+        a.in[t] = static_cast<const float2*>(inputs[t]);
+        a.mask[t] = d->masks[t];
+    }
+    a.out = static_cast<float2*>(output);
+    a.k = d->n_inputs;
+    a.sum = d->sum_first;
+    a.w = d->n_vars - d->sum_first;
+    const uint64_t n_out = 1ull << a.w;
+    const int threads = 256;
+    const uint64_t blocks = std::min<uint64_t>((n_out + threads - 1) / threads, 148ull * 16);
+    qtb_bucket_kernel<<<(unsigned)blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(a);
+    QTB_CUDA(cudaGetLastError());
+    return QTB_OK;
+}
+
+int qtb_plan_upload(qtb_plan* plan) {
+    if (!plan) return fail(QTB_ERR_ARG, "plan_upload: null plan");
+    std::lock_guard<std::mutex> lock(plan->mu);
+    free_device(plan);
+    flatten_plan(plan);
+    int r;
+    if ((r = upload_vec(plan->dnets, &plan->dev.nets))) return r;
+    if ((r = upload_vec(plan->dops, &plan->dev.ops))) return r;
+    if ((r = upload_vec(plan->dins, &plan->dev.ins))) return r;
+    if ((r = upload_vec(plan->dphases, &plan->dev.phases))) return r;
+    if ((r = upload_vec(plan->entries, &plan->dev.entries))) return r;
+    if ((r = upload_vec(plan->terms, &plan->dev.terms))) return r;
+    QTB_CUDA(cudaMalloc(&plan->dev.table, std::max<size_t>(8, (size_t)plan->table_elems * 8)));
+    QTB_CUDA(cudaMalloc(&plan->dev.status, sizeof(int)));
+    QTB_CUDA(cudaMemset(plan->dev.status, 0, sizeof(int)));
+    QTB_CUDA(cudaGetDevice(&plan->device));
+    plan->uploaded = true;
+    return QTB_OK;
+}
+
+static int get_run(qtb_plan* plan, int32_t first, int32_t count, void* terms, RunCache** out) {
+    qtb_plan_device* s = dev_state(plan);
+    auto key = std::make_tuple(first, count, reinterpret_cast<uintptr_t>(terms));
+    auto it = s->runs.find(key);
+    if (it == s->runs.end()) {
+        if (s->runs.size() >= 64) {   // callers cycling through many output buffers
+            cudaDeviceSynchronize();
+            for (auto& kv : s->runs)
+                if (kv.second.jobs) cudaFree(kv.second.jobs);
+            s->runs.clear();
+        }
+        RunCache rc;
+        int r = build_run(plan, first, count, static_cast<float2*>(terms), &rc);
+        if (r) return r;
+        it = s->runs.emplace(key, rc).first;
+    }
+    *out = &it->second;
+    return QTB_OK;
+}
+
+int qtb_plan_scratch_bytes(const qtb_plan* plan_c, int32_t first, int32_t count, size_t* bytes) {
+    qtb_plan* plan = const_cast<qtb_plan*>(plan_c);
+    if (!plan || !bytes) return fail(QTB_ERR_ARG, "plan_scratch_bytes: bad arguments");
+    if (!plan->uploaded) return fail(QTB_ERR_ARG, "plan_scratch_bytes: plan not uploaded");
+    if (first < 0 || count < 0 || first + count > (int32_t)plan->dnets.size())
+        return fail(QTB_ERR_ARG, "plan_scratch_bytes: range out of bounds");
+    // the global-arena class gives every CTA the largest arena of its members
+    uint32_t cap = 0;
+    int n = 0;
+    for (int32_t i = first; i < first + count; ++i)
+        if (plan->dnets[i].arena_elems > kSmemArenaLimitBytes / 8) {
+            cap = std::max(cap, plan->dnets[i].arena_elems);
+            ++n;
+        }
+    *bytes = (size_t)((cap + 3u) & ~3u) * n * sizeof(float2);
+    return QTB_OK;
+}
+
+int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* params_dev,
+                 void* terms_dev, double* energy_dev, void* scratch_dev, void* stream) {
+    if (!plan || !terms_dev || (plan->n_params > 0 && !params_dev))
+        return fail(QTB_ERR_ARG, "plan_run: null argument");
+    if (!plan->uploaded) return fail(QTB_ERR_ARG, "plan_run: plan not uploaded");
+    if (first < 0 || count < 1 || first + count > (int32_t)plan->dnets.size())
+        return fail(QTB_ERR_ARG, "plan_run: network range out of bounds");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    RunCache* rc = nullptr;
+    int r = get_run(plan, first, count, terms_dev, &rc);
+    if (r) return r;
+    if (rc->scratch_elems && !scratch_dev)
+        return fail(QTB_ERR_ARG, "plan_run: this range needs scratch memory (qtb_plan_scratch_bytes)");
+    const int n_entries = (int)plan->entries.size();
+    if (n_entries > 0) {
+        qtb_table_kernel<<<(n_entries + 127) / 128, 128, 0, st>>>(
+            static_cast<const DevEntry*>(plan->dev.entries), n_entries,
+            static_cast<const DevTerm*>(plan->dev.terms), params_dev,
+            static_cast<float2*>(plan->dev.table));
+        QTB_CUDA(cudaGetLastError());
+    }
+    qtb_plan_device* s = dev_state(plan);
+    std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+    if (s->timing) {
+        if (!s->spare.empty()) {
+            ev = s->spare.back();
+            s->spare.pop_back();
+        } else {
+            QTB_CUDA(cudaEventCreate(&ev.first));
+            QTB_CUDA(cudaEventCreate(&ev.second));
+        }
+        QTB_CUDA(cudaEventRecord(ev.first, st));
+    }
+    for (const LaunchClass& lc : rc->classes) {
+        if (lc.smem) {
+            qtb_network_kernel<true><<<lc.n_jobs, lc.threads, lc.capacity * sizeof(float2), st>>>(
+                rc->jobs + lc.job_offset, nullptr, lc.capacity, static_cast<int*>(plan->dev.status));
+        } else {
+            qtb_network_kernel<false><<<lc.n_jobs, lc.threads, 0, st>>>(
+                rc->jobs + lc.job_offset, static_cast<float2*>(scratch_dev) + lc.scratch_offset,
+                lc.capacity, static_cast<int*>(plan->dev.status));
+        }
+        QTB_CUDA(cudaGetLastError());
+    }
+    if (s->timing) {
+        QTB_CUDA(cudaEventRecord(ev.second, st));
+        s->pending.push_back(ev);
+        s->kernel_launches += (int64_t)rc->classes.size();
+    }
+    if (energy_dev) {
+        qtb_energy_kernel<<<1, 256, 0, st>>>(static_cast<const float2*>(terms_dev), count, energy_dev);
+        QTB_CUDA(cudaGetLastError());
+    }
+    return QTB_OK;
+}
+
+int qtb_plan_device_status(qtb_plan* plan, int32_t* status) {
+    if (!plan || !status) return fail(QTB_ERR_ARG, "plan_device_status: bad arguments");
+    if (!plan->uploaded) {
+        *status = 0;
+        return QTB_OK;
+    }
+    int v = 0;
+    QTB_CUDA(cudaMemcpy(&v, plan->dev.status, sizeof(int), cudaMemcpyDeviceToHost));
+    *status = v;
+    return QTB_OK;
+}
+
+// Kernel timing of the network executor launches (CUDA events on the run's
+// stream): enable, then read the accumulated milliseconds after each run.
+int qtb_plan_set_timing(qtb_plan* plan, int32_t enable) {
+    if (!plan) return fail(QTB_ERR_ARG, "plan_set_timing: null plan");
+    qtb_plan_device* s = dev_state(plan);
+    for (auto& e : s->pending) {
+        cudaEventSynchronize(e.second);
+        s->spare.push_back(e);
+    }
+    s->pending.clear();
+    s->timing = enable != 0;
+    s->kernel_ms = 0.0;
+    s->kernel_launches = 0;
+    return QTB_OK;
+}
+
+int qtb_plan_collect_timing(qtb_plan* plan, double* total_ms, int64_t* launches) {
+    if (!plan || !total_ms || !launches) return fail(QTB_ERR_ARG, "plan_collect_timing: bad arguments");
+    qtb_plan_device* s = dev_state(plan);
+    for (auto& e : s->pending) {
+        QTB_CUDA(cudaEventSynchronize(e.second));
+        float ms = 0.f;
+        QTB_CUDA(cudaEventElapsedTime(&ms, e.first, e.second));
+        s->kernel_ms += ms;
+        s->spare.push_back(e);
+    }
+    s->pending.clear();
+    *total_ms = s->kernel_ms;
+    *launches = s->kernel_launches;
+    return QTB_OK;
+}
+
+int qtb_plan_destroy(qtb_plan* plan) {
+    if (!plan) return QTB_OK;
+    free_device(plan);
+    {
+        std::lock_guard<std::mutex> lock(g_dev_mu);
+        auto it = g_dev.find(plan);
+        if (it != g_dev.end()) {
+            destroy_events(it->second);
+            delete it->second;
+            g_dev.erase(it);
+        }
+    }
+    delete plan;
+    return QTB_OK;
+}
+
+}  // extern "C"

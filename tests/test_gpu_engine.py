@@ -1,0 +1,92 @@
+"""Batched engine (gate-table kernel + whole-network executor + fp64 energy
+reduction, through the C ABI) against the reference fixtures."""
+import numpy as np
+import pytest
+import torch
+
+import graphs
+import statevector as sv
+from conftest import golden_graph
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def _engine(**kw):
+    from qtensor_b200.engine import QAOAEnergyEngine
+    return QAOAEnergyEngine(**kw)
+
+
+def _check(engine, name):
+    G, w = golden_graph(name)
+    terms = engine.edge_terms(G, w['gamma'], w['beta'])
+    ref = np.array([complex(*t) for t in w['terms']])
+    assert np.max(np.abs(terms - ref)) < TOL, name
+    E = engine.energy_expectation(G, w['gamma'], w['beta'])
+    assert abs(E - w['energy']) <= TOL * abs(w['energy']), (E, w['energy'])
+    return E
+
+
+@pytest.mark.parametrize('comp', ['default', 'cx', 'zz'])
+def test_engine_reference_order_cfg1(cuda_device, comp):
+    _check(_engine(composer=comp, ordering='reference'), 'cfg1_' + comp)
+
+
+@pytest.mark.parametrize('name', ['test_random_n4_p4_d3', 'test_random_n10_p5_d2',
+                                  'test_random_n14_p1_d3', 'test_grid2d_n3_p3_d0',
+                                  'test_line_n8_p4_d0', 'petersen_p9'])
+def test_engine_families(cuda_device, name):
+    E = _check(_engine(ordering='reference'), name)
+    if name == 'petersen_p9':
+        assert abs(E - 12.0) < 1e-2       # qtensor/tests/qiskit_qaoa_energy.py:123
+
+
+@pytest.mark.parametrize('name', ['cfg2', 'cfg3', 'cfg4'])
+def test_engine_native_order_large(cuda_device, name):
+    _check(_engine(ordering='native'), name)
+
+
+def test_engine_full_size_p1_closed_form(cuda_device):
+    """Size-independent pin at the full N=1000 size: p=1 edge terms equal the
+    closed-form expectation of every edge."""
+    G = graphs.regular(1000)
+    gamma, beta = graphs.angles(1, seed=5)
+    terms = _engine().edge_terms(G, gamma, beta)
+    exact = np.array([sv.qaoa_p1_edge_term(G, e, gamma[0], beta[0]) for e in G.edges()])
+    assert np.max(np.abs(terms - exact)) < TOL
+
+
+def test_engine_plan_reuse_across_angles(cuda_device):
+    """A cached plan with new angles equals a fresh compile with those angles."""
+    G = graphs.regular(100)
+    eng = _engine()
+    g1, b1 = graphs.angles(3, seed=1)
+    g2, b2 = graphs.angles(3, seed=2)
+    eng.energy_expectation(G, g1, b1)
+    reused = eng.edge_terms(G, g2, b2)
+    fresh = _engine().edge_terms(G, g2, b2)
+    assert np.array_equal(reused, fresh)
+    assert len(eng._cache) == 1
+
+
+def test_engine_deterministic_and_status_clean(cuda_device):
+    G, w = golden_graph('cfg2')
+    eng = _engine()
+    a = eng.energy_expectation(G, w['gamma'], w['beta'])
+    b = eng.energy_expectation(G, w['gamma'], w['beta'])
+    assert a == b
+    cg = eng.compile(G, 3, w['gamma'], w['beta'])
+    assert cg.plan.device_status() == 0
+
+
+def test_engine_rejects_bad_angles(cuda_device):
+    with pytest.raises(ValueError):
+        _engine().energy_expectation(graphs.regular(10), [0.1, 0.2], [0.3])
+
+
+def test_engine_needs_cuda_loudly(monkeypatch):
+    from qtensor_b200 import engine
+    monkeypatch.setattr(torch.cuda, 'is_available', lambda: False)
+    with pytest.raises(RuntimeError, match='no CPU fallback'):
+        engine.QAOAEnergyEngine()

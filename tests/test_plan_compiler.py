@@ -1,0 +1,153 @@
+"""The C++ plan compiler and the C ABI, checked on the CPU (no GPU needed):
+elimination orders against the reference fixtures, and the compiled device
+plans executed by a numpy interpreter against the reference amplitudes."""
+import ctypes
+import re
+
+import numpy as np
+import pytest
+
+import graphs
+import plan_interp
+import qtensor_port as port
+from conftest import ROOT, golden_graph
+from qtensor_b200 import _lib
+from qtensor_b200.lightcone import composer_id, reference_lightcone, simplify_passes
+from qtensor_b200.plan import NetworkPlan, graph_csr
+
+
+def _params(w):
+    return np.concatenate([w['gamma'], w['beta']])
+
+
+def _ref_plan(G, w, comp='default'):
+    p = len(w['gamma'])
+    plan = NetworkPlan(2 * p)
+    for edge in G.edges():
+        nq, gates = reference_lightcone(G, edge, p, comp)
+        plan.add_circuit(nq, gates, _params(w), simplify_passes(comp))
+    return plan
+
+
+def test_library_exports_every_header_symbol():
+    with open(f'{ROOT}/include/qtb.h') as f:
+        header = f.read()
+    declared = set(re.findall(r'\b(qtb_[a-z0-9_]+)\s*\(', header))
+    lib = _lib.lib()
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert declared == set(_lib.EXPORTS)
+    assert b'sm_100a' in lib.qtb_version()
+
+
+@pytest.mark.parametrize('comp', ['default', 'cx', 'zz'])
+def test_reference_order_matches_fixture(comp):
+    """Same greedy elimination order and width as the reference, edge by edge."""
+    G, w = golden_graph('cfg1_' + comp)
+    plan = _ref_plan(G, w, comp)
+    for k in range(len(w['terms'])):
+        assert plan.peo(k) == w['peo'][k]
+        assert plan.info(k)['treewidth'] == w['widths'][k]
+
+
+@pytest.mark.parametrize('name', ['cfg1_default', 'cfg1_cx', 'cfg1_zz', 'test_random_n4_p4_d3',
+                                  'test_grid2d_n3_p3_d0', 'test_line_n8_p4_d0', 'petersen_p9'])
+def test_interpreted_plan_matches_reference(name):
+    G, w = golden_graph(name)
+    plan = _ref_plan(G, w, w['composer'])
+    vals = plan_interp.run_plan(plan, _params(w))
+    ref = np.array([complex(*t) for t in w['terms']])
+    assert np.max(np.abs(vals - ref)) < 1e-12
+
+
+@pytest.mark.parametrize('comp', ['default', 'cx'])
+def test_native_order_plan_matches_reference(comp):
+    """Native (C++ lightcone) ordering: different numbering, same amplitudes."""
+    G, w = golden_graph('cfg1_default')
+    p = len(w['gamma'])
+    plan = NetworkPlan(2 * p)
+    csr = graph_csr(G)
+    plan.add_lightcones(csr, np.array(list(G.edges())), p, composer_id(comp), _params(w))
+    vals = plan_interp.run_plan(plan, _params(w))
+    ref = np.array([complex(*t) for t in w['terms']])
+    assert np.max(np.abs(vals - ref)) < 1e-12
+
+
+def test_native_plan_cfg2_sample():
+    G, w = golden_graph('cfg2')
+    edges = list(G.edges())[::10]
+    plan = NetworkPlan(6)
+    plan.add_lightcones(graph_csr(G), np.array(edges), 3, 0, _params(w), threads=4)
+    vals = plan_interp.run_plan(plan, _params(w))
+    ref = np.array([complex(*w['terms'][k]) for k in range(0, len(w['edges']), 10)])
+    assert np.max(np.abs(vals - ref)) < 1e-12
+
+
+def test_native_plan_cfg3_shape():
+    """All 1500 edge networks of the N=1000 p=3 workload compile; their
+    widths are the reference's (same cones, greedy order up to numbering)."""
+    G, w = golden_graph('cfg3')
+    plan = NetworkPlan(6)
+    plan.add_lightcones(graph_csr(G), np.array(list(G.edges())), 3, 0, _params(w))
+    infos = plan.infos()
+    assert len(infos) == 1500
+    assert max(i['treewidth'] for i in infos) <= max(w['widths']) + 2
+    assert all(i['arena_elems'] * 8 <= 200 * 1024 for i in infos)
+    assert all(i['angle_specific'] == 0 for i in infos)
+
+
+def test_simplifier_keeps_reference_hadamard_merge():
+    """The reference simplifier turns H.H on one qubit into a single H
+    (simplify_circuit.py:69-70 with gates.py hadamard); the plan does too."""
+    gates = np.array([(_lib.GATE_H, 0, -1, -1, 0.0), (_lib.GATE_H, 0, -1, -1, 0.0)],
+                     dtype=_lib.GATE_DTYPE)
+    plan = NetworkPlan(0)
+    plan.add_circuit(1, gates, np.zeros(0), simplify_passes=1)
+    val = plan_interp.run_plan(plan, np.zeros(0))[0]
+    assert abs(val - 1 / np.sqrt(2)) < 1e-15
+    qops = __import__('qtree').operators
+    amp = port.simulate_amplitude(port.simplify_qtree_circuit([qops.H(0), qops.H(0)]))
+    assert abs(amp[0] - val) < 1e-15
+
+
+def test_angle_dependent_cancellation_is_flagged():
+    """Two X rotations whose angles cancel numerically but not structurally."""
+    gates = np.array([(_lib.GATE_H, 0, -1, -1, 0.0), (_lib.GATE_XPHASE, 0, -1, 0, 2.0),
+                      (_lib.GATE_XPHASE, 0, -1, 1, 2.0), (_lib.GATE_Z, 0, -1, -1, 0.0)],
+                     dtype=_lib.GATE_DTYPE)
+    plan = NetworkPlan(2)
+    plan.add_circuit(1, gates, np.array([0.25, -0.25]), simplify_passes=1)
+    assert plan.info(0)['angle_specific'] == 1
+    assert plan.params_valid(np.array([0.1, -0.1]))
+    assert not plan.params_valid(np.array([0.1, 0.2]))
+
+
+def test_invalid_circuits_raise():
+    plan = NetworkPlan(1)
+    bad_kind = np.array([(99, 0, -1, -1, 0.0)], dtype=_lib.GATE_DTYPE)
+    with pytest.raises(_lib.QtbError):
+        plan.add_circuit(1, bad_kind, np.zeros(1))
+    bad_qubit = np.array([(_lib.GATE_H, 3, -1, -1, 0.0)], dtype=_lib.GATE_DTYPE)
+    with pytest.raises(_lib.QtbError):
+        plan.add_circuit(2, bad_qubit, np.zeros(1))
+    no_param = np.array([(_lib.GATE_XPHASE, 0, -1, 5, 2.0)], dtype=_lib.GATE_DTYPE)
+    with pytest.raises(_lib.QtbError):
+        plan.add_circuit(1, no_param, np.zeros(1))
+    G = graphs.regular(10)
+    with pytest.raises(_lib.QtbError):
+        plan.add_lightcones(graph_csr(G), np.array([[0, 1]]), 2, 0, np.zeros(4))   # 2p != 1
+    assert len(plan) == 0
+
+
+def test_bucket_desc_validation_without_device():
+    """Argument checks of qtb_bucket_c64 run before any CUDA call."""
+    lib = _lib.lib()
+    desc = _lib.BucketDesc()
+    desc.n_inputs = 0
+    ptrs = (ctypes.c_void_p * 1)()
+    assert lib.qtb_bucket_c64(ctypes.byref(desc), ptrs, ctypes.c_void_p(8), None) == 1
+    desc.n_inputs, desc.n_vars, desc.sum_first = 1, 2, 1
+    desc.masks[0] = 0b100          # names a variable outside the union
+    ptrs[0] = 16
+    assert lib.qtb_bucket_c64(ctypes.byref(desc), ptrs, ctypes.c_void_p(8), None) == 1
+    assert 'outside the union' in _lib.last_error()
