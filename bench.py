@@ -1,0 +1,327 @@
+"""QAOA edge-term throughput on B200 -- one JSON line on rank 0.
+
+Workload (default): QAOA MaxCut energy, random 3-regular graph N=1000
+(networkx seed 0 + rank), p=3, angles U[0, pi) drawn per step, default
+composer (ZZ gates + commutation simplifier), greedy elimination order --
+1500 edge-term networks per step.  One step = one full energy: gate tensors
+generated from the step's 6 angles, all 1500 lightcone networks contracted,
+fp64 compensated reduction to the energy.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+* ``value``: device-resident throughput (plans and angles already in HBM),
+  CUDA events around each step on the launching stream, L2 flushed between
+  steps (256 MiB write, outside the events); max over ranks.
+* ``e2e``: the public API ``QAOAEnergyEngine.energy_expectation(G, gamma,
+  beta)`` per step with host angles: pinned H2D of the angles and D2H of the
+  energy inside the events; plans cached from the warm-up (a new graph's plan
+  compile is reported separately as ``compile_s``).
+* ``--impl reference``: the reference algorithm (the oracle port of QTensor's
+  ``energy_expectation_parallel`` with its NumpyBackend, complex128 einsum)
+  on all host cores, rank 0 only.
+Multi-GPU (torchrun): every rank contracts its own graph (weak scaling); no
+collective on the data path.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, 'tests'))
+
+import numpy as np  # noqa: E402
+
+import graphs  # noqa: E402
+
+METRIC = 'QAOA edge terms/s (3-regular N=1000 p=3)'
+UNIT = 'edge terms/s'
+PUBLISHED_TERMS_PER_S = 1500 / 4.89   # N=1000 p=3, 4.89 s, 56 processes
+WORKLOAD = {'workload': 'qaoa-maxcut energy, random 3-regular N=1000 (seed 0+rank), p=3, '
+                        'default composer, greedy order; 1500 edge-term networks per step',
+            'graph_nodes': 1000, 'p': 3, 'edges': 1500, 'composer': 'default',
+            'ordering': 'native'}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--nodes', type=int, default=1000)
+    ap.add_argument('--p', type=int, default=3)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get('RANK', 0))
+    world = int(os.environ.get('WORLD_SIZE', 1))
+    local = int(os.environ.get('LOCAL_RANK', 0))
+    return rank, world, local
+
+
+# ------------------------------------------------------------------ CPU arm
+def cpu_reference(G, p, n_edges, seed, start_method):
+    """Time the oracle port of the reference path on the host cores over the
+    first ``n_edges`` edges.  Returns (terms/s, cores, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import qtensor_port as port
+    cores = os.cpu_count() or 1
+    gamma, beta = graphs.angles(p, seed)
+    edges = list(G.edges())[:n_edges]
+    t0 = time.perf_counter()
+    port.energy_expectation_parallel(G, gamma, beta, n_processes=cores, edges=edges,
+                                     start_method=start_method)
+    dt = time.perf_counter() - t0
+    return len(edges) / dt, cores, dt
+
+
+def cpu_sample_edges(total):
+    cores = os.cpu_count() or 1
+    # about 0.03 s of single-core work per N=1000 p=3 edge: aim at ~15 s of work
+    return int(min(total, max(64, 500 * cores)))
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    G = graphs.regular(args.nodes, seed=0)
+    n_edges = cpu_sample_edges(G.number_of_edges())
+    times = []
+    for step in range(args.warmup + args.steps):
+        rate, cores, dt = cpu_reference(G, args.p, n_edges, seed=step, start_method='fork')
+        if step >= args.warmup:
+            times.append(dt)
+    mean = sum(times) / len(times)
+    value = n_edges / mean
+    sample = '{} of {} edges per step, oracle port of energy_expectation_parallel ' \
+             '(NumpyBackend einsum, complex128), fork pool of {} processes'.format(
+                 n_edges, G.number_of_edges(), cores)
+    line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': args.gpus,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': mean * 1e3,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': value / PUBLISHED_TERMS_PER_S,
+            'dtype': 'c128', 'data': 'synthetic', 'impl': 'reference',
+            'config': dict(WORKLOAD, ordering='reference greedy', cpu_sample=sample),
+            'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': cores, 'kind': 'port',
+                             'sample': sample},
+            'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0,
+                    'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', str(self.gpu), '--query-gpu=' + self.FIELDS,
+                 '--format=csv,noheader,nounits', '-lms', '200'],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sms, maxes, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(',')]
+            if len(parts) < 9:
+                continue
+            try:
+                sms.append(float(parts[1]))
+                maxes.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == 'active':
+                    reasons.add(name)
+        return {'sm_mhz': statistics.median(sms) if sms else None,
+                'sm_max_mhz': max(maxes) if maxes else None,
+                'reasons': sorted(reasons), 'samples': len(sms)}
+
+
+# ------------------------------------------------------------------ GPU arm
+def measured_peak_hbm():
+    path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    try:
+        with open(path) as f:
+            return float(json.load(f)['hbm_gbs']), 'measured'
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 'fallback'
+
+
+def profiled_traffic():
+    """DRAM bytes per executor launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, 'profiles', 'network_kernel_cfg3.json')
+    try:
+        with open(path) as f:
+            return json.load(f).get('dram_bytes_per_launch')
+    except (OSError, ValueError):
+        return None
+
+
+def run_b200(args):
+    rank, world, local = dist_env()
+    G = graphs.regular(args.nodes, seed=rank)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # timed before CUDA is initialised, so the pool may fork
+        n_sample = cpu_sample_edges(G.number_of_edges())
+        rate, cores, dt = cpu_reference(G, args.p, n_sample, seed=0, start_method='fork')
+        cpu = {'value': rate, 'unit': UNIT, 'cores': cores, 'kind': 'port',
+               'sample': '{} of {} edges of the workload through the oracle port of '
+                         'energy_expectation_parallel (NumpyBackend einsum, complex128), '
+                         '{} processes, {:.1f} s'.format(n_sample, G.number_of_edges(), cores, dt)}
+
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group('nccl', timeout=timedelta(seconds=120), device_id=dev)
+        pg = dist
+
+    from qtensor_b200.engine import QAOAEnergyEngine
+    eng = QAOAEnergyEngine(composer='default', ordering='native', device=local)
+    p = args.p
+    gamma0, beta0 = graphs.angles(p, seed=0)
+    t0 = time.perf_counter()
+    cg = eng.compile(G, p, gamma0, beta0)
+    compile_s = time.perf_counter() - t0
+    stats = cg.stats()
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    angle_sets = [np.concatenate(graphs.angles(p, seed=100 + i)) for i in range(args.warmup + args.steps)]
+    params_dev = [torch.from_numpy(a).to(dev) for a in angle_sets]
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+
+    # ---- device-resident steps
+    for i in range(args.warmup):
+        cg.launch(params_dev[i], stream)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    cg.plan.set_timing(True)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier()
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        starts[i].record(stream)
+        cg.launch(params_dev[args.warmup + i], stream)
+        ends[i].record(stream)
+    barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    kernel_ms, kernel_launches = cg.plan.collect_timing()
+    cg.plan.set_timing(False)
+    status = cg.plan.device_status()
+    if status:
+        raise RuntimeError('device status {:#x}'.format(status))
+
+    # ---- end-to-end through the public API (host angles in, energy out)
+    e2e_ms = []
+    for i in range(args.warmup):
+        eng.energy_expectation(G, *graphs.angles(p, seed=200 + i))
+    barrier()
+    for i in range(args.steps):
+        gamma, beta = graphs.angles(p, seed=300 + i)
+        flush.fill_(float(i))
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        eng.energy_expectation(G, gamma, beta)
+        e.record(stream)
+        e.synchronize()
+        e2e_ms.append(s.elapsed_time(e))
+    barrier()
+    clk = clocks.stop()
+
+    total_ms = sum(step_ms)
+    e2e_total = sum(e2e_ms)
+    if pg:
+        t = torch.tensor([total_ms, e2e_total], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms, e2e_total = t.tolist()
+    ms_per_step = total_ms / args.steps
+    value = world * stats['edges'] / (ms_per_step / 1e3)
+    e2e_value = world * stats['edges'] / (e2e_total / args.steps / 1e3)
+    kernel_avg_ms = kernel_ms / max(1, kernel_launches)
+    launches_per_step = kernel_launches / args.steps
+    per_launch_bytes = stats['alg_bytes'] / launches_per_step
+    peak, peak_kind = measured_peak_hbm()
+    achieved = per_launch_bytes / (kernel_avg_ms / 1e3) / 1e9
+    if rank == 0:
+        line = {
+            'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms_per_step,
+            'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': value / PUBLISHED_TERMS_PER_S, 'dtype': 'c64', 'data': 'synthetic',
+            'impl': 'b200',
+            'config': dict(WORKLOAD, l2='flushed between steps (256 MiB write outside the events)',
+                           parallelism='one graph per rank' if world > 1 else 'single GPU',
+                           width_max=stats['width_max'], ops_per_step=stats['ops'],
+                           compile_s=compile_s, alg_bytes_per_step=stats['alg_bytes'],
+                           alg_flops_per_step=stats['alg_flops']),
+            'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                         'frac': achieved / peak, 'traffic': profiled_traffic(),
+                         'kernel': 'qtb_network_kernel', 'peak_source': peak_kind,
+                         'kernel_ms_per_launch': kernel_avg_ms,
+                         'alg_bytes_per_launch': per_launch_bytes},
+            'cpu_baseline': cpu,
+            'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': 8 * 2 * p,
+                    'd2h_bytes_per_step': 8, 'ms_per_step': e2e_total / args.steps},
+            'clocks': clk,
+            'gpu_launches': int(round(kernel_launches + 2 * args.steps)),
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == 'reference':
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == '__main__':
+    main()

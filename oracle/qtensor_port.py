@@ -302,14 +302,15 @@ def _edge_task(args):
 
 
 def energy_expectation_parallel(G, gamma, beta, n_processes=None, composer='default',
-                                edges=None):
-    """Process-pool variant (``QAOASimulator.py:72-88``); a ``spawn`` pool so
-    it is safe in a process that already initialised CUDA.  ``edges`` limits
-    the work to a subset (returns the raw sum of edge terms in that case)."""
+                                edges=None, start_method='spawn'):
+    """Process-pool variant (``QAOASimulator.py:72-88``).  The default
+    ``spawn`` pool is safe in a process that already initialised CUDA; pass
+    ``'fork'`` only before any GPU call.  ``edges`` limits the work to a
+    subset (returns the raw sum of edge terms in that case)."""
     n_processes = n_processes or os.cpu_count()
     todo = list(G.edges()) if edges is None else list(edges)
     args = [(G, gamma, beta, e, composer) for e in todo]
-    with get_context('spawn').Pool(n_processes) as pool:
+    with get_context(start_method).Pool(n_processes) as pool:
         terms = pool.map(_edge_task, args, chunksize=max(1, len(args) // (4 * n_processes)))
     total = sum(terms)
     if edges is not None:
