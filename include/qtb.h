@@ -140,6 +140,13 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
                             int32_t p, int32_t composer, const double* params,
                             int32_t n_threads, int32_t* first_net_index);
 
+/* Elimination-order search for networks added afterwards: 0 (default) keeps
+ * the reference's greedy rule (first node of least degree); trials > 0 also
+ * runs that many seeded greedy orders with random tie-breaking and keeps
+ * the one of least sum over eliminations of 2^degree (the zero-temperature
+ * RGreedyOptimizer, qtensor/optimisation/RGreedy.py:15-77).               */
+int qtb_plan_set_order_trials(qtb_plan* plan, int32_t trials);
+
 int qtb_plan_n_networks(const qtb_plan* plan, int32_t* n);
 int qtb_plan_network_info(const qtb_plan* plan, int32_t net, qtb_network_info* info);
 /* Elimination order of a network as variable ids of the qtree layout
@@ -153,7 +160,9 @@ int qtb_plan_check_params(const qtb_plan* plan, const double* params, int32_t* v
 /* Host copies of the flattened plan (the arrays qtb_plan_upload sends to the
  * device), for inspection and CPU-side verification of the compiler.
  * which: 0 networks (8 x u32 each), 1 ops (16 B each), 2 operands (8 B),
- * 3 phases (16 B), 4 gate-table entries (24 B), 5 angle terms (16 B).
+ * 3 phases (16 B), 4 gate-table entries (24 B), 5 angle terms (16 B),
+ * 6 per-network executor records (8 x u32), 7 the per-network plan blobs
+ * (phases, ops, operands with network-local indices) the executor stages.
  * Writes min(cap, size) bytes to buf (may be NULL) and the full size.     */
 int qtb_plan_export(qtb_plan* plan, int32_t which, void* buf, size_t cap, size_t* size);
 /* Complex64 elements of the gate table. */

@@ -12,6 +12,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, 'libqtb.so')
 
+QTB_OK, QTB_ERR_ARG, QTB_ERR_CUDA, QTB_ERR_UNSUPPORTED, QTB_ERR_DEVICE = range(5)
 QTB_MAX_BUCKET_INPUTS = 16
 QTB_MAX_BUCKET_VARS = 31
 
@@ -24,7 +25,8 @@ COMPOSER_DEFAULT, COMPOSER_ZZ, COMPOSER_CX = 0, 1, 2
 EXPORTS = (
     'qtb_version', 'qtb_init', 'qtb_last_error', 'qtb_bucket_c64',
     'qtb_plan_create', 'qtb_plan_destroy', 'qtb_plan_add_circuit',
-    'qtb_plan_add_lightcone', 'qtb_plan_add_lightcones', 'qtb_plan_n_networks',
+    'qtb_plan_add_lightcone', 'qtb_plan_add_lightcones', 'qtb_plan_set_order_trials',
+    'qtb_plan_n_networks',
     'qtb_plan_network_info', 'qtb_plan_network_peo', 'qtb_plan_check_params',
     'qtb_plan_export', 'qtb_plan_table_elems', 'qtb_plan_upload',
     'qtb_plan_scratch_bytes', 'qtb_plan_run', 'qtb_plan_device_status',
@@ -73,13 +75,16 @@ NET_DTYPE = np.dtype([('op_begin', '<u4'), ('n_ops', '<u4'), ('phase_begin', '<u
                       ('max_elems', '<u4'), ('pad', '<u4')])
 OP_DTYPE = np.dtype([('u', 'u1'), ('sum', 'u1'), ('k', 'u1'), ('pad', 'u1'), ('dst', '<u4'),
                      ('elem_begin', '<u4'), ('in_begin', '<u4')])
-IN_DTYPE = np.dtype([('mask', '<u4'), ('src', '<u4')])
+IN_DTYPE = np.dtype([('mask', '<u4'), ('src', '<u4'), ('runs', '<u8')])
 PHASE_DTYPE = np.dtype([('op_first', '<u4'), ('op_count', '<u4'), ('total_elems', '<u4'),
                         ('pad', '<u4')])
 ENTRY_DTYPE = np.dtype([('kind', '<i4'), ('expr_begin', '<i4'), ('expr_count', '<i4'),
                         ('off', '<u4'), ('rank_in', 'i1'), ('rank_out', 'i1'),
                         ('sliced_mask', 'u1'), ('perm', 'i1', (5,))])
 TERM_DTYPE = np.dtype([('param', '<i4'), ('pad', '<i4'), ('coef', '<f8')])
+RUN_DTYPE = np.dtype([('blob_off16', '<u4'), ('blob_bytes', '<u4'), ('n_phases', '<u4'),
+                      ('ins_off', '<u4'), ('arena_elems', '<u4'), ('result_src', '<u4'),
+                      ('max_elems', '<u4'), ('pad', '<u4')])
 SRC_TABLE = 0x80000000
 
 _lib = None
@@ -101,6 +106,7 @@ def _declare(lib):
                                              c.c_int32, c.c_int32, P, c.POINTER(c.c_int32)]),
         'qtb_plan_add_lightcones': (c.c_int, [P, c.c_int32, P, P, P, c.c_int32, c.c_int32,
                                               c.c_int32, P, c.c_int32, c.POINTER(c.c_int32)]),
+        'qtb_plan_set_order_trials': (c.c_int, [P, c.c_int32]),
         'qtb_plan_n_networks': (c.c_int, [P, c.POINTER(c.c_int32)]),
         'qtb_plan_network_info': (c.c_int, [P, c.c_int32, c.POINTER(NetworkInfo)]),
         'qtb_plan_network_peo': (c.c_int, [P, c.c_int32, P, c.c_int32, c.POINTER(c.c_int32)]),

@@ -87,6 +87,28 @@ static Expr expr_add(const Expr& a, const Expr& b) {
     return out;
 }
 
+// Runs of the operand bits below the summed bit (see DevIn).
+uint64_t encode_runs(uint32_t mask, uint32_t w) {
+    const uint32_t low = w >= 32 ? mask : (mask & ((1u << w) - 1u));
+    uint64_t runs = 0;
+    uint64_t n = 0;
+    uint32_t dst = 0;
+    for (uint32_t bit = 0; bit < 32;) {
+        if (!((low >> bit) & 1u)) {
+            ++bit;
+            continue;
+        }
+        uint32_t len = 0;
+        while (bit + len < 32 && ((low >> (bit + len)) & 1u)) ++len;
+        if (n == (uint64_t)kMaxRuns) return kRunsFallback << 60;
+        runs |= (uint64_t)(bit | (len << 5) | (dst << 10)) << (15 * n);
+        ++n;
+        dst += len;
+        bit += len;
+    }
+    return runs | (n << 60);
+}
+
 // ------------------------------------------------------------- simplifier
 namespace {
 
@@ -286,9 +308,13 @@ struct OpRec {
 }  // namespace
 
 // Greedy min-degree order over the line graph (nodes in first-appearance
-// order); returns the order and the degree of every eliminated node.
-static void greedy_order(int V, const std::vector<std::vector<int32_t>>& cliques,
-                         std::vector<int32_t>* order, std::vector<int32_t>* degrees) {
+// order); returns the order and the degree of every eliminated node.  With
+// seed == 0 ties go to the first node in order (the reference's rule,
+// qtensor/utils.py:30-32); otherwise a deterministic xorshift stream picks
+// uniformly among the tied nodes (the zero-temperature limit of
+// RGreedyOptimizer, qtensor/optimisation/RGreedy.py:36-62).
+static double greedy_order(int V, const std::vector<std::vector<int32_t>>& cliques, uint64_t seed,
+                           std::vector<int32_t>* order, std::vector<int32_t>* degrees) {
     const int W = (V + 63) / 64;
     std::vector<uint64_t> adj((size_t)V * W, 0);
     auto test = [&](int a, int b) { return (adj[(size_t)a * W + (b >> 6)] >> (b & 63)) & 1; };
@@ -308,13 +334,27 @@ static void greedy_order(int V, const std::vector<std::vector<int32_t>>& cliques
             }
     std::vector<int32_t> alive(V);
     std::iota(alive.begin(), alive.end(), 0);
-    std::vector<int32_t> nbrs;
+    std::vector<int32_t> nbrs, ties;
+    uint64_t rng = seed;
+    double cost = 0.0;
     order->clear();
     degrees->clear();
     while (!alive.empty()) {
         size_t best = 0;
-        for (size_t i = 1; i < alive.size(); ++i)
-            if (deg[alive[i]] < deg[alive[best]]) best = i;
+        if (seed == 0) {
+            for (size_t i = 1; i < alive.size(); ++i)
+                if (deg[alive[i]] < deg[alive[best]]) best = i;
+        } else {
+            int32_t dmin = deg[alive[0]];
+            for (size_t i = 1; i < alive.size(); ++i) dmin = std::min(dmin, deg[alive[i]]);
+            ties.clear();
+            for (size_t i = 0; i < alive.size(); ++i)
+                if (deg[alive[i]] == dmin) ties.push_back((int32_t)i);
+            rng ^= rng << 13;
+            rng ^= rng >> 7;
+            rng ^= rng << 17;
+            best = (size_t)ties[rng % ties.size()];
+        }
         const int x = alive[best];
         alive.erase(alive.begin() + best);
         nbrs.clear();
@@ -328,6 +368,7 @@ static void greedy_order(int V, const std::vector<std::vector<int32_t>>& cliques
         }
         order->push_back(x);
         degrees->push_back((int32_t)nbrs.size());
+        cost += std::ldexp(1.0, (int)nbrs.size());
         for (int a : nbrs) {
             clr(a, x);
             --deg[a];
@@ -343,11 +384,12 @@ static void greedy_order(int V, const std::vector<std::vector<int32_t>>& cliques
                 }
             }
     }
+    return cost;
 }
 
 int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
                     int32_t simplify_passes, const double* params, int32_t n_params,
-                    Network* out, std::string* err) {
+                    int32_t order_trials, Network* out, std::string* err) {
     if (n_qubits <= 0 || n_gates < 0 || (n_gates > 0 && in_gates == nullptr)) {
         *err = "compile: invalid circuit arguments";
         return QTB_ERR_ARG;
@@ -456,8 +498,19 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
             }
             if (c.size() > 1) cliques.push_back(std::move(c));
         }
-    std::vector<int32_t> gorder, gdeg;
-    greedy_order((int)var_of.size(), cliques, &gorder, &gdeg);
+    // trial 0: the reference's greedy rule; trials 1..order_trials: seeded
+    // random tie-breaking; the cheapest order (sum of 2^degree) wins
+    std::vector<int32_t> gorder, gdeg, torder, tdeg;
+    double best_cost = greedy_order((int)var_of.size(), cliques, 0, &gorder, &gdeg);
+    for (int32_t t = 1; t <= order_trials; ++t) {
+        const uint64_t seed = 0x9E3779B97F4A7C15ull * (uint64_t)t + (uint64_t)var_of.size();
+        const double c = greedy_order((int)var_of.size(), cliques, seed, &torder, &tdeg);
+        if (c < best_cost) {
+            best_cost = c;
+            gorder.swap(torder);
+            gdeg.swap(tdeg);
+        }
+    }
     std::vector<int32_t>& peo = out->peo;
     peo.clear();
     for (int q = 0; q < nq; ++q) peo.push_back(ket_start + q);
@@ -647,6 +700,7 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
                 DevIn in{};
                 in.mask = op.masks[t];
                 in.src = r.table ? (kSrcTable | (uint32_t)r.id) : ops[r.id].dst;
+                in.runs = encode_runs(in.mask, (uint32_t)op.w);
                 out->ins.push_back(in);
                 alg_bytes += 8.0 * std::ldexp(1.0, __builtin_popcount(in.mask));
             }
@@ -813,6 +867,33 @@ void flatten_plan(qtb_plan* plan) {
     }
 }
 
+// Per-network blobs with network-local indices (see DevNetRun).
+void build_blobs(qtb_plan* plan) {
+    plan->druns.clear();
+    plan->dblobs.clear();
+    for (const Network& n : plan->nets) {
+        DevNetRun r{};
+        r.blob_off16 = (uint32_t)(plan->dblobs.size() / 16);
+        r.n_phases = (uint32_t)n.phases.size();
+        r.arena_elems = (uint32_t)n.info.arena_elems;
+        r.result_src = n.result_src;
+        r.max_elems = n.max_elems;
+        const size_t ph_bytes = n.phases.size() * sizeof(DevPhase);
+        const size_t op_bytes = n.ops.size() * sizeof(DevOp);
+        const size_t in_bytes = n.ins.size() * sizeof(DevIn);
+        r.ins_off = (uint32_t)(ph_bytes + op_bytes);
+        const size_t total = (ph_bytes + op_bytes + in_bytes + 15) & ~size_t(15);
+        r.blob_bytes = (uint32_t)total;
+        const size_t base = plan->dblobs.size();
+        plan->dblobs.resize(base + total, 0);
+        uint8_t* dst = plan->dblobs.data() + base;
+        std::memcpy(dst, n.phases.data(), ph_bytes);     // op_first already network-local
+        std::memcpy(dst + ph_bytes, n.ops.data(), op_bytes);   // in_begin network-local
+        std::memcpy(dst + ph_bytes + op_bytes, n.ins.data(), in_bytes);
+        plan->druns.push_back(r);
+    }
+}
+
 }  // namespace qtb
 
 // =================================================================== C ABI
@@ -841,7 +922,7 @@ int qtb_plan_add_circuit(qtb_plan* plan, int32_t n_qubits, const qtb_gate* gates
     Network net;
     std::string err;
     int rc = compile_circuit(n_qubits, gates, n_gates, simplify_passes, params, plan->n_params,
-                             &net, &err);
+                             plan->order_trials, &net, &err);
     if (rc) return fail(rc, err);
     std::lock_guard<std::mutex> lock(plan->mu);
     if (net_index) *net_index = (int32_t)plan->nets.size();
@@ -883,7 +964,7 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
                                      composer, &gates, &nq, &errs[i]);
             if (!rc)
                 rc = compile_circuit(nq, gates.data(), (int32_t)gates.size(), composer == 0 ? 2 : 0,
-                                     params, plan->n_params, &nets[i], &errs[i]);
+                                     params, plan->n_params, plan->order_trials, &nets[i], &errs[i]);
             codes[i] = rc;
         }
     };
@@ -898,6 +979,12 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
     std::lock_guard<std::mutex> lock(plan->mu);
     if (first_net_index) *first_net_index = (int32_t)plan->nets.size();
     for (auto& n : nets) merge_network(plan, std::move(n));
+    return QTB_OK;
+}
+
+int qtb_plan_set_order_trials(qtb_plan* plan, int32_t trials) {
+    if (!plan || trials < 0) return fail(QTB_ERR_ARG, "plan_set_order_trials: bad arguments");
+    plan->order_trials = trials;
     return QTB_OK;
 }
 
@@ -943,6 +1030,7 @@ int qtb_plan_export(qtb_plan* plan, int32_t which, void* buf, size_t cap, size_t
     if (!plan || !size) return fail(QTB_ERR_ARG, "plan_export: bad arguments");
     std::lock_guard<std::mutex> lock(plan->mu);
     flatten_plan(plan);
+    build_blobs(plan);
     const void* src = nullptr;
     size_t n = 0;
     switch (which) {
@@ -952,6 +1040,8 @@ int qtb_plan_export(qtb_plan* plan, int32_t which, void* buf, size_t cap, size_t
         case 3: src = plan->dphases.data(); n = plan->dphases.size() * sizeof(DevPhase); break;
         case 4: src = plan->entries.data(); n = plan->entries.size() * sizeof(DevEntry); break;
         case 5: src = plan->terms.data(); n = plan->terms.size() * sizeof(DevTerm); break;
+        case 6: src = plan->druns.data(); n = plan->druns.size() * sizeof(DevNetRun); break;
+        case 7: src = plan->dblobs.data(); n = plan->dblobs.size(); break;
         default: return fail(QTB_ERR_ARG, "plan_export: unknown array");
     }
     *size = n;

@@ -26,11 +26,18 @@ struct DevOp {
     uint32_t in_begin;  // index of the first DevIn of this op
 };
 
-// One operand of an op: which union bits it holds, where it lives.
+// One operand of an op: which union bits it holds, where it lives, and the
+// bit gather from an output index to the operand's index precompiled as at
+// most kMaxRuns contiguous runs: run r (15 bits at 15*r) = start | len << 5 |
+// dst << 10 moves bits [start, start+len) of the output index to [dst, ...);
+// bits 60..62 hold the run count, kRunsFallback when the mask needs more.
 struct DevIn {
     uint32_t mask;      // bit (u-1-v) set <=> union variable v is an axis
     uint32_t src;       // arena offset, or kSrcTable | gate-table offset
+    uint64_t runs;
 };
+constexpr int kMaxRuns = 4;
+constexpr uint64_t kRunsFallback = 7;
 
 // Ops of one dependency level; a barrier follows every phase.
 struct DevPhase {
@@ -49,6 +56,21 @@ struct DevNet {
     uint32_t arena_elems;
     uint32_t result_src;   // arena offset or kSrcTable | offset of the scalar
     uint32_t max_elems;    // largest op output (elements)
+    uint32_t pad;
+};
+
+// One network as the executor reads it: its phases, ops and operands are
+// one contiguous 16-byte-aligned blob [DevPhase x n_phases][DevOp x n_ops]
+// [DevIn x n_ins, padded to 16 bytes] with network-local indices, staged
+// into shared memory by one bulk copy.
+struct DevNetRun {
+    uint32_t blob_off16;   // blob offset in 16-byte units
+    uint32_t blob_bytes;   // multiple of 16
+    uint32_t n_phases;
+    uint32_t ins_off;      // byte offset of the DevIn array within the blob
+    uint32_t arena_elems;
+    uint32_t result_src;
+    uint32_t max_elems;
     uint32_t pad;
 };
 
@@ -72,9 +94,10 @@ struct DevTerm {
 };
 
 static_assert(sizeof(DevOp) == 16, "DevOp layout");
-static_assert(sizeof(DevIn) == 8, "DevIn layout");
+static_assert(sizeof(DevIn) == 16, "DevIn layout");
 static_assert(sizeof(DevPhase) == 16, "DevPhase layout");
 static_assert(sizeof(DevNet) == 32, "DevNet layout");
+static_assert(sizeof(DevNetRun) == 32, "DevNetRun layout");
 static_assert(sizeof(DevEntry) == 24, "DevEntry layout");
 static_assert(sizeof(DevTerm) == 16, "DevTerm layout");
 
@@ -109,22 +132,19 @@ struct Network {
 };
 
 struct DeviceBuffers {
-    void* nets = nullptr;
-    void* ops = nullptr;
-    void* ins = nullptr;
-    void* phases = nullptr;
+    void* runs = nullptr;         // DevNetRun per network
+    void* blobs = nullptr;        // concatenated network blobs
     void* entries = nullptr;
     void* terms = nullptr;
     void* table = nullptr;        // complex64 gate table
     void* status = nullptr;       // int error word
-    void* partials = nullptr;     // per-block fp64 partial sums
-    size_t partials_cap = 0;
 };
 
 }  // namespace qtb
 
 struct qtb_plan {
     int32_t n_params = 0;
+    int32_t order_trials = 0;   // extra randomized greedy orders per network
     std::vector<qtb::Network> nets;
     // global gate table, built from the networks' local entries
     std::map<qtb::EntryKey, int32_t> entry_index;
@@ -137,6 +157,8 @@ struct qtb_plan {
     std::vector<qtb::DevOp> dops;
     std::vector<qtb::DevIn> dins;
     std::vector<qtb::DevPhase> dphases;
+    std::vector<qtb::DevNetRun> druns;
+    std::vector<uint8_t> dblobs;
     bool uploaded = false;
     int device = -1;
     qtb::DeviceBuffers dev;
@@ -149,11 +171,13 @@ void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int compile_circuit(int32_t n_qubits, const qtb_gate* gates, int32_t n_gates,
                     int32_t simplify_passes, const double* params, int32_t n_params,
-                    Network* out, std::string* err);
+                    int32_t order_trials, Network* out, std::string* err);
 int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indices,
                     int32_t u, int32_t v, int32_t p, int32_t composer,
                     std::vector<qtb_gate>* gates, int32_t* n_qubits, std::string* err);
 void merge_network(qtb_plan* plan, Network&& net);
 void flatten_plan(qtb_plan* plan);
+uint64_t encode_runs(uint32_t mask, uint32_t w);
+void build_blobs(qtb_plan* plan);
 int rank_of_kind(int32_t kind);
 }  // namespace qtb

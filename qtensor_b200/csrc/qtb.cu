@@ -41,6 +41,24 @@ __device__ __forceinline__ uint32_t pext32(uint32_t x, uint32_t m) {
     return r;
 }
 
+// Operand offset of output index j (bits below the summed bit) from the
+// precompiled runs of DevIn; falls back to the bit loop for masks of more
+// than kMaxRuns runs.
+__device__ __forceinline__ uint32_t gather_bits(uint32_t j, const DevIn& d, uint32_t low_mask) {
+    const uint32_t n = (uint32_t)(d.runs >> 60);
+    if (n == (uint32_t)kRunsFallback) return pext32(j, d.mask & low_mask);
+    uint32_t off = 0;
+#pragma unroll
+    for (uint32_t r = 0; r < (uint32_t)kMaxRuns; ++r) {
+        if (r < n) {
+            const uint32_t rr = (uint32_t)(d.runs >> (15 * r)) & 0x7fffu;
+            const uint32_t start = rr & 31u, len = (rr >> 5) & 31u, dst = rr >> 10;
+            off |= ((j >> start) & ((1u << len) - 1u)) << dst;
+        }
+    }
+    return off;
+}
+
 // ----------------------------------------------------------------- K1
 struct BucketArgs {
     const float2* in[QTB_MAX_BUCKET_INPUTS];
@@ -129,62 +147,118 @@ __global__ void qtb_table_kernel(const DevEntry* entries, int n_entries, const D
 
 // ----------------------------------------------------------------- K3
 struct Job {
-    const DevNet* net;
-    const DevOp* ops;
-    const DevIn* ins;
-    const DevPhase* phases;
+    const DevNetRun* net;
+    const uint4* blobs;      // base of all network blobs (16-byte units)
     const float2* table;
     float2* term;
 };
 
-constexpr int kStatusArena = 1;
+constexpr int kStatusArena = 1;        // network arena larger than the launch's capacity
+constexpr int kStatusStageTimeout = 2; // the plan blob copy did not complete in time
+constexpr int kStatusBlob = 4;         // network blob larger than the launch's capacity
+constexpr uint32_t kStageSpinLimit = 1u << 26;
 
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Copy the network's plan blob global -> shared with one bulk (TMA) copy
+// completing on an mbarrier; every thread waits with a bounded spin.
+// Returns false (and sets the status word) if the copy did not land.
+__device__ bool stage_blob(void* dst, const void* src, uint32_t bytes, uint64_t* bar, int* status) {
+    const uint32_t bar_a = smem_addr(bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+                "r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(bar_a)
+            : "memory");
+    }
+    uint32_t done = 0;
+    for (uint32_t it = 0; it < kStageSpinLimit; ++it) {
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+            " selp.u32 %0, 1, 0, p;\n}" : "=r"(done) : "r"(bar_a) : "memory");
+        if (done) break;
+        if (it > 64) __nanosleep(32);
+    }
+    if (!done && threadIdx.x == 0) atomicOr(status, kStatusStageTimeout);
+    return __syncthreads_and(done) != 0;
+}
+
+// One CTA contracts one network.  Shared memory: [mbarrier | plan blob |
+// arena]; with kSmemArena == false the arena is this CTA's slice of gscratch.
+// Phases run in order with a barrier after each; inside a phase the
+// elements of all its ops are spread over the threads.
 template <bool kSmemArena>
-__global__ void __launch_bounds__(512) qtb_network_kernel(const Job* __restrict__ jobs,
-                                                          float2* __restrict__ gscratch,
-                                                          uint32_t arena_capacity,
-                                                          int* __restrict__ status) {
-    extern __shared__ float2 sarena[];
+__global__ void __launch_bounds__(1024) qtb_network_kernel(const Job* __restrict__ jobs,
+                                                           float2* __restrict__ gscratch,
+                                                           uint32_t arena_capacity,
+                                                           uint32_t blob_capacity,
+                                                           int* __restrict__ status) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+    unsigned char* blob = smem + 16;
     const Job job = jobs[blockIdx.x];
-    const DevNet net = *job.net;
-    if (net.arena_elems > arena_capacity) {
-        if (threadIdx.x == 0) atomicOr(status, kStatusArena);
+    const DevNetRun net = *job.net;
+    if (net.arena_elems > arena_capacity || net.blob_bytes > blob_capacity) {
+        if (threadIdx.x == 0)
+            atomicOr(status, net.arena_elems > arena_capacity ? kStatusArena : kStatusBlob);
         return;
     }
-    float2* arena = kSmemArena ? sarena : gscratch + (size_t)blockIdx.x * arena_capacity;
-    const DevPhase* phases = job.phases + net.phase_begin;
+    if (!stage_blob(blob, job.blobs + net.blob_off16, net.blob_bytes, bar, status)) return;
+    float2* arena = kSmemArena ? reinterpret_cast<float2*>(blob + blob_capacity)
+                               : gscratch + (size_t)blockIdx.x * arena_capacity;
+    const DevPhase* phases = reinterpret_cast<const DevPhase*>(blob);
+    const DevOp* ops = reinterpret_cast<const DevOp*>(blob + net.n_phases * sizeof(DevPhase));
+    const DevIn* ins = reinterpret_cast<const DevIn*>(blob + net.ins_off);
+    const float2* __restrict__ table = job.table;
+
     for (uint32_t p = 0; p < net.n_phases; ++p) {
         const DevPhase ph = phases[p];
         uint32_t oi = ph.op_first;
-        DevOp op = job.ops[oi];
-        uint32_t op_end = op.elem_begin + (1u << (op.u - op.sum));
+        DevOp op = ops[oi];
+        uint32_t w = op.u - op.sum;
+        uint32_t op_end = op.elem_begin + (1u << w);
         for (uint32_t g = threadIdx.x; g < ph.total_elems; g += blockDim.x) {
             while (g >= op_end) {
-                op = job.ops[++oi];
-                op_end = op.elem_begin + (1u << (op.u - op.sum));
+                op = ops[++oi];
+                w = op.u - op.sum;
+                op_end = op.elem_begin + (1u << w);
             }
-            const uint32_t w = op.u - op.sum;
             const uint32_t j = g - op.elem_begin;
-            const DevIn* in = job.ins + op.in_begin;
-            float2 acc = make_float2(0.f, 0.f);
-            for (uint32_t s = 0; s <= op.sum; ++s) {
-                const uint32_t idx = j | (s << w);
-                float2 prod = make_float2(1.f, 0.f);
-                for (uint32_t t = 0; t < op.k; ++t) {
-                    const DevIn d = in[t];
-                    const uint32_t off = pext32(idx, d.mask);
-                    const float2 x = (d.src & kSrcTable) ? __ldg(job.table + (d.src & ~kSrcTable) + off)
-                                                         : arena[d.src + off];
-                    prod = t == 0 ? x : cmul(prod, x);
+            const DevIn* in = ins + op.in_begin;
+            // the summed variable is union bit w and, in an operand that has
+            // it, that operand's most significant axis: a fixed stride
+            float2 p0 = make_float2(1.f, 0.f), p1 = make_float2(1.f, 0.f);
+            for (uint32_t t = 0; t < op.k; ++t) {
+                const DevIn d = in[t];
+                const uint32_t off = gather_bits(j, d, (1u << w) - 1u);
+                const bool tab = d.src & kSrcTable;
+                const float2* base = tab ? table + (d.src & ~kSrcTable) : arena + d.src;
+                const float2 x0 = tab ? __ldg(base + off) : base[off];
+                p0 = t == 0 ? x0 : cmul(p0, x0);
+                if (op.sum) {
+                    float2 x1 = x0;
+                    if ((d.mask >> w) & 1u) {
+                        const uint32_t stride = 1u << (__popc(d.mask) - 1);
+                        x1 = tab ? __ldg(base + off + stride) : base[off + stride];
+                    }
+                    p1 = t == 0 ? x1 : cmul(p1, x1);
                 }
-                acc = s == 0 ? prod : make_float2(acc.x + prod.x, acc.y + prod.y);
             }
-            arena[op.dst + j] = acc;
+            arena[op.dst + j] = op.sum ? make_float2(p0.x + p1.x, p0.y + p1.y) : p0;
         }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        *job.term = (net.result_src & kSrcTable) ? job.table[net.result_src & ~kSrcTable]
+        *job.term = (net.result_src & kSrcTable) ? table[net.result_src & ~kSrcTable]
                                                  : arena[net.result_src];
     }
 }
@@ -225,20 +299,24 @@ static int cuda_fail(cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
     } while (0)
 
-constexpr uint32_t kSmemArenaLimitBytes = 200 * 1024;
+// Dynamic shared memory a CTA may use (B200: 227 KB per block).
+constexpr uint32_t kSmemLimitBytes = 224 * 1024;
+constexpr int kMaxClasses = 5;
 
 struct LaunchClass {
     bool smem;
-    uint32_t capacity;     // arena elements per CTA
+    uint32_t capacity;      // arena elements per CTA
+    uint32_t blob_capacity; // plan-blob bytes per CTA
     int threads;
     int n_jobs;
-    size_t job_offset;     // into the job buffer
-    size_t scratch_offset; // elements into scratch (global class)
+    size_t job_offset;      // into the job buffer
+    size_t scratch_offset;  // elements into scratch (global-arena class)
+    size_t smem_bytes;
 };
 
 struct RunCache {
     Job* jobs = nullptr;
-    std::vector<LaunchClass> classes;
+    std::vector<LaunchClass> classes;   // widest first
     size_t scratch_elems = 0;
 };
 
@@ -251,6 +329,8 @@ struct qtb_plan_device {
     double kernel_ms = 0.0;
     int64_t kernel_launches = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending, spare;
+    cudaStream_t aux[qtb::kMaxClasses] = {};
+    cudaEvent_t fork = nullptr, join[qtb::kMaxClasses] = {};
 };
 
 namespace qtb {
@@ -266,7 +346,7 @@ static qtb_plan_device* dev_state(const qtb_plan* p) {
 
 static void free_device(qtb_plan* plan) {
     DeviceBuffers& d = plan->dev;
-    void* ptrs[] = {d.nets, d.ops, d.ins, d.phases, d.entries, d.terms, d.table, d.status, d.partials};
+    void* ptrs[] = {d.runs, d.blobs, d.entries, d.terms, d.table, d.status};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     d = DeviceBuffers();
@@ -277,7 +357,7 @@ static void free_device(qtb_plan* plan) {
     plan->uploaded = false;
 }
 
-static void destroy_events(qtb_plan_device* s) {
+static void destroy_streams(qtb_plan_device* s) {
     for (auto* v : {&s->pending, &s->spare})
         for (auto& e : *v) {
             cudaEventDestroy(e.first);
@@ -285,11 +365,19 @@ static void destroy_events(qtb_plan_device* s) {
         }
     s->pending.clear();
     s->spare.clear();
+    for (int i = 0; i < kMaxClasses; ++i) {
+        if (s->aux[i]) cudaStreamDestroy(s->aux[i]);
+        if (s->join[i]) cudaEventDestroy(s->join[i]);
+        s->aux[i] = nullptr;
+        s->join[i] = nullptr;
+    }
+    if (s->fork) cudaEventDestroy(s->fork);
+    s->fork = nullptr;
 }
 
 template <typename T>
 static int upload_vec(const std::vector<T>& v, void** dst) {
-    const size_t bytes = std::max<size_t>(sizeof(T), v.size() * sizeof(T));
+    const size_t bytes = std::max<size_t>(16, v.size() * sizeof(T));
     QTB_CUDA(cudaMalloc(dst, bytes));
     if (!v.empty()) QTB_CUDA(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
     return QTB_OK;
@@ -298,49 +386,56 @@ static int upload_vec(const std::vector<T>& v, void** dst) {
 static int threads_for(uint32_t max_elems) {
     if (max_elems <= 128) return 64;
     if (max_elems <= 1024) return 128;
-    if (max_elems <= 8192) return 256;
-    return 512;
+    if (max_elems <= 4096) return 256;
+    if (max_elems <= 16384) return 512;
+    return 1024;
 }
 
+// Launch classes of a run: networks bucketed by the shared memory they need
+// (16 KB, 48 KB, 112 KB, 224 KB; larger arenas go to global scratch), the
+// widest class first so its long critical path starts early.
 static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms, RunCache* rc) {
-    // classes: smem arenas bucketed by size (4 KB, 16 KB, 64 KB, 200 KB), then global
-    const uint32_t bounds[] = {512, 2048, 8192, kSmemArenaLimitBytes / 8};
-    std::vector<std::vector<int32_t>> members(5);
+    const uint32_t bounds[4] = {16 * 1024, 48 * 1024, 112 * 1024, kSmemLimitBytes};
+    std::vector<std::vector<int32_t>> members(kMaxClasses);
     for (int32_t i = first; i < first + count; ++i) {
-        const uint32_t a = plan->dnets[i].arena_elems;
+        const DevNetRun& r = plan->druns[i];
+        const size_t need = 16 + (size_t)r.blob_bytes + 8 * (size_t)((r.arena_elems + 3u) & ~3u);
         int c = 4;
         for (int b = 0; b < 4; ++b)
-            if (a <= bounds[b]) {
+            if (need <= bounds[b]) {
                 c = b;
                 break;
             }
+        if (c == 4 && 16 + (size_t)r.blob_bytes > kSmemLimitBytes)
+            return fail(QTB_ERR_UNSUPPORTED, "network plan blob exceeds shared memory");
         members[c].push_back(i);
     }
     std::vector<Job> jobs;
-    const auto* dn = static_cast<const DevNet*>(plan->dev.nets);
+    const auto* runs = static_cast<const DevNetRun*>(plan->dev.runs);
     rc->classes.clear();
     rc->scratch_elems = 0;
-    for (int c = 0; c < 5; ++c) {
+    for (int c = kMaxClasses - 1; c >= 0; --c) {
         if (members[c].empty()) continue;
         LaunchClass lc{};
         lc.smem = c < 4;
         lc.job_offset = jobs.size();
         lc.n_jobs = (int)members[c].size();
-        uint32_t cap = 4, maxe = 1;
+        uint32_t cap = 4, blob = 16, maxe = 1;
         for (int32_t i : members[c]) {
-            cap = std::max(cap, plan->dnets[i].arena_elems);
-            maxe = std::max(maxe, plan->dnets[i].max_elems);
+            cap = std::max(cap, plan->druns[i].arena_elems);
+            blob = std::max(blob, plan->druns[i].blob_bytes);
+            maxe = std::max(maxe, plan->druns[i].max_elems);
             Job j;
-            j.net = dn + i;
-            j.ops = static_cast<const DevOp*>(plan->dev.ops);
-            j.ins = static_cast<const DevIn*>(plan->dev.ins);
-            j.phases = static_cast<const DevPhase*>(plan->dev.phases);
+            j.net = runs + i;
+            j.blobs = static_cast<const uint4*>(plan->dev.blobs);
             j.table = static_cast<const float2*>(plan->dev.table);
             j.term = terms + (i - first);
             jobs.push_back(j);
         }
         lc.capacity = (cap + 3u) & ~3u;
+        lc.blob_capacity = blob;
         lc.threads = threads_for(maxe);
+        lc.smem_bytes = 16 + (size_t)blob + (lc.smem ? 8 * (size_t)lc.capacity : 0);
         if (!lc.smem) {
             lc.scratch_offset = rc->scratch_elems;
             rc->scratch_elems += (size_t)lc.capacity * lc.n_jobs;
@@ -360,7 +455,7 @@ using namespace qtb;
 
 extern "C" {
 
-const char* qtb_version(void) { return "qtensor_b200 0.1 (sm_100a)"; }
+const char* qtb_version(void) { return "qtensor_b200 0.2 (sm_100a)"; }
 
 int qtb_init(int device) {
     int n = 0;
@@ -368,8 +463,9 @@ int qtb_init(int device) {
     if (device < 0 || device >= n) return fail(QTB_ERR_ARG, "qtb_init: no such device");
     QTB_CUDA(cudaSetDevice(device));
     QTB_CUDA(cudaFuncSetAttribute(qtb_network_kernel<true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kSmemArenaLimitBytes));
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimitBytes));
+    QTB_CUDA(cudaFuncSetAttribute(qtb_network_kernel<false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimitBytes));
     return QTB_OK;
 }
 
@@ -406,14 +502,13 @@ int qtb_plan_upload(qtb_plan* plan) {
     std::lock_guard<std::mutex> lock(plan->mu);
     free_device(plan);
     flatten_plan(plan);
+    build_blobs(plan);
     int r;
-    if ((r = upload_vec(plan->dnets, &plan->dev.nets))) return r;
-    if ((r = upload_vec(plan->dops, &plan->dev.ops))) return r;
-    if ((r = upload_vec(plan->dins, &plan->dev.ins))) return r;
-    if ((r = upload_vec(plan->dphases, &plan->dev.phases))) return r;
+    if ((r = upload_vec(plan->druns, &plan->dev.runs))) return r;
+    if ((r = upload_vec(plan->dblobs, &plan->dev.blobs))) return r;
     if ((r = upload_vec(plan->entries, &plan->dev.entries))) return r;
     if ((r = upload_vec(plan->terms, &plan->dev.terms))) return r;
-    QTB_CUDA(cudaMalloc(&plan->dev.table, std::max<size_t>(8, (size_t)plan->table_elems * 8)));
+    QTB_CUDA(cudaMalloc(&plan->dev.table, std::max<size_t>(16, (size_t)plan->table_elems * 8)));
     QTB_CUDA(cudaMalloc(&plan->dev.status, sizeof(int)));
     QTB_CUDA(cudaMemset(plan->dev.status, 0, sizeof(int)));
     QTB_CUDA(cudaGetDevice(&plan->device));
@@ -427,7 +522,7 @@ static int get_run(qtb_plan* plan, int32_t first, int32_t count, void* terms, Ru
     auto it = s->runs.find(key);
     if (it == s->runs.end()) {
         if (s->runs.size() >= 64) {   // callers cycling through many output buffers
-            cudaDeviceSynchronize();
+            QTB_CUDA(cudaDeviceSynchronize());
             for (auto& kv : s->runs)
                 if (kv.second.jobs) cudaFree(kv.second.jobs);
             s->runs.clear();
@@ -445,17 +540,30 @@ int qtb_plan_scratch_bytes(const qtb_plan* plan_c, int32_t first, int32_t count,
     qtb_plan* plan = const_cast<qtb_plan*>(plan_c);
     if (!plan || !bytes) return fail(QTB_ERR_ARG, "plan_scratch_bytes: bad arguments");
     if (!plan->uploaded) return fail(QTB_ERR_ARG, "plan_scratch_bytes: plan not uploaded");
-    if (first < 0 || count < 0 || first + count > (int32_t)plan->dnets.size())
+    if (first < 0 || count < 0 || first + count > (int32_t)plan->druns.size())
         return fail(QTB_ERR_ARG, "plan_scratch_bytes: range out of bounds");
     // the global-arena class gives every CTA the largest arena of its members
     uint32_t cap = 0;
     int n = 0;
-    for (int32_t i = first; i < first + count; ++i)
-        if (plan->dnets[i].arena_elems > kSmemArenaLimitBytes / 8) {
-            cap = std::max(cap, plan->dnets[i].arena_elems);
+    for (int32_t i = first; i < first + count; ++i) {
+        const DevNetRun& r = plan->druns[i];
+        const size_t need = 16 + (size_t)r.blob_bytes + 8 * (size_t)((r.arena_elems + 3u) & ~3u);
+        if (need > kSmemLimitBytes) {
+            cap = std::max(cap, r.arena_elems);
             ++n;
         }
+    }
     *bytes = (size_t)((cap + 3u) & ~3u) * n * sizeof(float2);
+    return QTB_OK;
+}
+
+static int ensure_streams(qtb_plan_device* s) {
+    if (s->fork) return QTB_OK;
+    QTB_CUDA(cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming));
+    for (int i = 0; i < kMaxClasses; ++i) {
+        QTB_CUDA(cudaStreamCreateWithFlags(&s->aux[i], cudaStreamNonBlocking));
+        QTB_CUDA(cudaEventCreateWithFlags(&s->join[i], cudaEventDisableTiming));
+    }
     return QTB_OK;
 }
 
@@ -464,7 +572,7 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
     if (!plan || !terms_dev || (plan->n_params > 0 && !params_dev))
         return fail(QTB_ERR_ARG, "plan_run: null argument");
     if (!plan->uploaded) return fail(QTB_ERR_ARG, "plan_run: plan not uploaded");
-    if (first < 0 || count < 1 || first + count > (int32_t)plan->dnets.size())
+    if (first < 0 || count < 1 || first + count > (int32_t)plan->druns.size())
         return fail(QTB_ERR_ARG, "plan_run: network range out of bounds");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     RunCache* rc = nullptr;
@@ -472,6 +580,8 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
     if (r) return r;
     if (rc->scratch_elems && !scratch_dev)
         return fail(QTB_ERR_ARG, "plan_run: this range needs scratch memory (qtb_plan_scratch_bytes)");
+    qtb_plan_device* s = dev_state(plan);
+    if ((r = ensure_streams(s))) return r;
     const int n_entries = (int)plan->entries.size();
     if (n_entries > 0) {
         qtb_table_kernel<<<(n_entries + 127) / 128, 128, 0, st>>>(
@@ -480,7 +590,6 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
             static_cast<float2*>(plan->dev.table));
         QTB_CUDA(cudaGetLastError());
     }
-    qtb_plan_device* s = dev_state(plan);
     std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
     if (s->timing) {
         if (!s->spare.empty()) {
@@ -492,16 +601,27 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
         }
         QTB_CUDA(cudaEventRecord(ev.first, st));
     }
-    for (const LaunchClass& lc : rc->classes) {
+    // size classes run concurrently on forked streams, joined back into st
+    const bool forked = rc->classes.size() > 1;
+    if (forked) QTB_CUDA(cudaEventRecord(s->fork, st));
+    for (size_t c = 0; c < rc->classes.size(); ++c) {
+        const LaunchClass& lc = rc->classes[c];
+        cudaStream_t cs = forked ? s->aux[c] : st;
+        if (forked) QTB_CUDA(cudaStreamWaitEvent(cs, s->fork, 0));
         if (lc.smem) {
-            qtb_network_kernel<true><<<lc.n_jobs, lc.threads, lc.capacity * sizeof(float2), st>>>(
-                rc->jobs + lc.job_offset, nullptr, lc.capacity, static_cast<int*>(plan->dev.status));
+            qtb_network_kernel<true><<<lc.n_jobs, lc.threads, lc.smem_bytes, cs>>>(
+                rc->jobs + lc.job_offset, nullptr, lc.capacity, lc.blob_capacity,
+                static_cast<int*>(plan->dev.status));
         } else {
-            qtb_network_kernel<false><<<lc.n_jobs, lc.threads, 0, st>>>(
+            qtb_network_kernel<false><<<lc.n_jobs, lc.threads, lc.smem_bytes, cs>>>(
                 rc->jobs + lc.job_offset, static_cast<float2*>(scratch_dev) + lc.scratch_offset,
-                lc.capacity, static_cast<int*>(plan->dev.status));
+                lc.capacity, lc.blob_capacity, static_cast<int*>(plan->dev.status));
         }
         QTB_CUDA(cudaGetLastError());
+        if (forked) {
+            QTB_CUDA(cudaEventRecord(s->join[c], cs));
+            QTB_CUDA(cudaStreamWaitEvent(st, s->join[c], 0));
+        }
     }
     if (s->timing) {
         QTB_CUDA(cudaEventRecord(ev.second, st));
@@ -566,7 +686,7 @@ int qtb_plan_destroy(qtb_plan* plan) {
         std::lock_guard<std::mutex> lock(g_dev_mu);
         auto it = g_dev.find(plan);
         if (it != g_dev.end()) {
-            destroy_events(it->second);
+            destroy_streams(it->second);
             delete it->second;
             g_dev.erase(it);
         }

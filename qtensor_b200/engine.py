@@ -9,10 +9,11 @@ Every edge's lightcone network is compiled once per (graph, p, composer,
 ordering) by the C++ plan compiler and kept on the device; a call uploads
 the 2p angles, generates the gate tensors on the device, contracts all edge
 networks (one CTA per network, intermediates in shared memory) and reduces
-the edge terms in fp64 -- three kernels, one 8-byte read-back.
+the edge terms in fp64 -- one CUDA-graph replay, one 8-byte read-back.
 """
 import hashlib
 import threading
+import weakref
 
 import numpy as np
 import torch
@@ -27,9 +28,9 @@ def _require_cuda():
         raise RuntimeError('qtensor_b200 needs a CUDA device; there is no CPU fallback')
 
 
-def graph_key(G, p, composer, ordering):
+def graph_key(G, p, composer, ordering, trials=0):
     h = hashlib.sha1()
-    h.update(repr((p, composer, ordering, G.number_of_nodes())).encode())
+    h.update(repr((p, composer, ordering, trials, G.number_of_nodes())).encode())
     h.update(repr(list(G.nodes())).encode())
     h.update(repr(list(G.edges())).encode())
     return h.hexdigest()
@@ -52,6 +53,10 @@ class CompiledGraph:
         self.scratch = (torch.empty(max(nbytes, 8), dtype=torch.uint8, device=device)
                         if nbytes else None)
         self._infos = None
+        # host side of the captured call: pinned angles in, pinned energy out
+        self.host_params = torch.zeros(2 * p, dtype=torch.float64, pin_memory=True)
+        self.host_energy = torch.zeros(1, dtype=torch.float64, pin_memory=True)
+        self._graph = None
 
     @property
     def infos(self):
@@ -80,18 +85,43 @@ class CompiledGraph:
         self.plan.run(0, self.n_edges, self.params if params_dev is None else params_dev,
                       self.terms, self.energy, self.scratch, stream.cuda_stream)
 
+    def _capture(self):
+        """CUDA graph of one call: pinned angles -> device, gate table,
+        executor classes (forked streams), energy, energy -> pinned host."""
+        with torch.cuda.device(self.device):
+            self.launch()                      # builds the run's job arrays outside capture
+            torch.cuda.synchronize(self.device)
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph):
+                stream = torch.cuda.current_stream(self.device)
+                self.params.copy_(self.host_params, non_blocking=True)
+                self.launch(stream=stream)
+                self.host_energy.copy_(self.energy, non_blocking=True)
+            self._graph = graph
+
+    def energy_of(self, params):
+        """MaxCut energy for ``params = gamma[0..p) + beta[0..p)`` (host
+        doubles) by one graph replay and one synchronisation."""
+        if self._graph is None:
+            self._capture()
+        self.host_params.numpy()[:] = params
+        self._graph.replay()
+        torch.cuda.current_stream(self.device).synchronize()
+        return float(self.host_energy.numpy()[0])
+
 
 class QAOAEnergyEngine:
     """QAOA energy expectations contracted on the GPU.
 
     composer: ``'default'`` (ZZ gates + commutation simplifier, QTensor's
     ``DefaultQAOAComposer``), ``'zz'`` or ``'cx'``.
-    ordering: ``'native'`` (C++ lightcones, multithreaded) or ``'reference'``
-    (QTensor's exact qubit numbering, hence its greedy elimination order).
+    ordering: ``'native'`` (C++ lightcones, multithreaded, and the cheapest of
+    ``order_trials`` randomized greedy orders per network) or ``'reference'``
+    (QTensor's exact qubit numbering and greedy elimination order).
     """
 
     def __init__(self, composer='default', ordering='native', device=None, threads=0,
-                 cache_size=16):
+                 cache_size=16, order_trials=16):
         _require_cuda()
         if ordering not in ('native', 'reference'):
             raise ValueError('ordering must be "native" or "reference"')
@@ -101,11 +131,11 @@ class QAOAEnergyEngine:
         self.device = torch.device('cuda', torch.cuda.current_device() if device is None else device)
         self.threads = threads
         self.cache_size = cache_size
+        self.order_trials = order_trials if ordering == 'native' else 0
         self._cache = {}
+        self._by_id = {}        # id(G) -> (weakref, nodes, edges, p, key)
         self._lock = threading.Lock()
         _lib.check(_lib.lib().qtb_init(self.device.index))
-        self._host_energy = torch.empty(1, dtype=torch.float64, pin_memory=True)
-        self._host_params = {}
 
     # ------------------------------------------------------------ compile
     def compile(self, G, p, gamma=None, beta=None):
@@ -114,13 +144,14 @@ class QAOAEnergyEngine:
         The angles only steer the simplifier's near-zero cancellation test;
         a plan whose decisions depend on them is recompiled when they change."""
         params = self._params(p, gamma, beta)
-        key = graph_key(G, p, self.composer, self.ordering)
+        key = self._key(G, p)
         with self._lock:
             cg = self._cache.get(key)
             if cg is not None and cg.plan.params_valid(params):
                 return cg
         edges = list(G.edges())
         plan = NetworkPlan(2 * p)
+        plan.set_order_trials(self.order_trials)
         if self.ordering == 'native':
             csr = graph_csr(G)
             index = {v: i for i, v in enumerate(csr[0])}
@@ -139,6 +170,29 @@ class QAOAEnergyEngine:
             self._cache[key] = cg
         return cg
 
+    def _key(self, G, p):
+        """Plan-cache key of ``G``.  The full key hashes every edge; a graph
+        object seen before with the same node and edge counts reuses its key
+        (call ``invalidate(G)`` after mutating a graph in place)."""
+        hit = self._by_id.get(id(G))
+        if hit is not None:
+            ref, n, m, hp, key = hit
+            if ref() is G and hp == p and n == G.number_of_nodes() and m == G.number_of_edges():
+                return key
+        key = graph_key(G, p, self.composer, self.ordering, self.order_trials)
+        try:
+            self._by_id[id(G)] = (weakref.ref(G), G.number_of_nodes(), G.number_of_edges(), p, key)
+        except TypeError:
+            pass
+        return key
+
+    def invalidate(self, G):
+        """Forget cached plans of ``G`` (after changing it in place)."""
+        hit = self._by_id.pop(id(G), None)
+        if hit is not None:
+            with self._lock:
+                self._cache.pop(hit[4], None)
+
     @staticmethod
     def _params(p, gamma, beta):
         if gamma is None or beta is None:
@@ -150,27 +204,12 @@ class QAOAEnergyEngine:
         return np.concatenate([gamma, beta])
 
     # ------------------------------------------------------------ run
-    def _pinned_params(self, n):
-        buf = self._host_params.get(n)
-        if buf is None:
-            buf = torch.empty(n, dtype=torch.float64, pin_memory=True)
-            self._host_params[n] = buf
-        return buf
-
     def energy_expectation(self, G, gamma, beta):
         """Expected MaxCut value of the depth-p QAOA state (p = len(gamma))."""
         gamma = np.asarray(gamma, dtype=np.float64).ravel()
         p = len(gamma)
         cg = self.compile(G, p, gamma, beta)
-        params = self._params(p, gamma, beta)
-        host = self._pinned_params(2 * p)
-        host.numpy()[:] = params
-        stream = torch.cuda.current_stream(self.device)
-        cg.params.copy_(host, non_blocking=True)
-        cg.launch(stream=stream)
-        self._host_energy.copy_(cg.energy, non_blocking=True)
-        stream.synchronize()
-        return float(self._host_energy[0])
+        return cg.energy_of(self._params(p, gamma, beta))
 
     def edge_terms(self, G, gamma, beta):
         """``<Z_u Z_v>`` of every edge (complex64 numpy array, edge order of ``G.edges()``)."""
@@ -182,7 +221,7 @@ class QAOAEnergyEngine:
         return cg.terms.cpu().numpy()
 
     def check_device(self, cg):
+        """Raise if a kernel of ``cg`` reported an error status (synchronises)."""
         status = cg.plan.device_status()
         if status:
-            raise _lib.QtbError(_lib.QTB_ERR_DEVICE if hasattr(_lib, 'QTB_ERR_DEVICE') else 4,
-                                'device status word {:#x}'.format(status))
+            raise _lib.QtbError(_lib.QTB_ERR_DEVICE, 'device status word {:#x}'.format(status))

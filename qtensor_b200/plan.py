@@ -37,6 +37,11 @@ class NetworkPlan:
         self.uploaded = False
 
     # ------------------------------------------------------------ compile
+    def set_order_trials(self, trials):
+        """Randomized greedy orders tried per network added afterwards (0 =
+        the reference's greedy order only)."""
+        check(self._lib.qtb_plan_set_order_trials(self._h, int(trials)))
+
     def add_circuit(self, n_qubits, gates, params, simplify_passes=0):
         gates = np.ascontiguousarray(gates, dtype=_lib.GATE_DTYPE)
         params = np.ascontiguousarray(params, dtype=np.float64)
@@ -91,7 +96,9 @@ class NetworkPlan:
         for which, (name, dtype) in enumerate([('nets', _lib.NET_DTYPE), ('ops', _lib.OP_DTYPE),
                                                ('ins', _lib.IN_DTYPE), ('phases', _lib.PHASE_DTYPE),
                                                ('entries', _lib.ENTRY_DTYPE),
-                                               ('terms', _lib.TERM_DTYPE)]):
+                                               ('terms', _lib.TERM_DTYPE),
+                                               ('runs', _lib.RUN_DTYPE),
+                                               ('blobs', np.dtype('u1'))]):
             size = ctypes.c_size_t()
             check(self._lib.qtb_plan_export(self._h, which, None, 0, ctypes.byref(size)))
             buf = np.zeros(size.value // dtype.itemsize, dtype=dtype)

@@ -62,29 +62,64 @@ def gate_table(exported, params):
 
 
 def _pext(x, m):
-    r, bit = 0, 1
-    while m:
-        low = m & -m
-        if x & low:
-            r |= bit
-        bit <<= 1
-        m ^= low
+    """Bit gather on an integer array: the bits of x selected by mask m."""
+    x = np.asarray(x, dtype=np.int64)
+    r = np.zeros_like(x)
+    bit = 0
+    for b in range(32):
+        if (m >> b) & 1:
+            r |= ((x >> b) & 1) << bit
+            bit += 1
     return r
 
 
+def _gather_runs(j, runs):
+    """The executor's bit gather from its precompiled runs (None: fallback)."""
+    runs = int(runs)
+    n = runs >> 60
+    if n == 7:
+        return None
+    off = np.zeros_like(j)
+    for r in range(n):
+        rr = (runs >> (15 * r)) & 0x7fff
+        start, length, dst = rr & 31, (rr >> 5) & 31, rr >> 10
+        off |= ((j >> start) & ((1 << length) - 1)) << dst
+    return off
+
+
+def network_views(exported, net_index):
+    """Phases, ops and operands of one network, decoded from its executor
+    blob exactly as the device kernel addresses them (network-local)."""
+    run = exported['runs'][net_index]
+    base = int(run['blob_off16']) * 16
+    blob = exported['blobs'][base:base + int(run['blob_bytes'])]
+    assert int(run['blob_bytes']) % 16 == 0
+    n_ph = int(run['n_phases'])
+    ph_bytes = n_ph * _lib.PHASE_DTYPE.itemsize
+    phases = blob[:ph_bytes].view(_lib.PHASE_DTYPE)
+    ins_off = int(run['ins_off'])
+    ops = blob[ph_bytes:ins_off].view(_lib.OP_DTYPE)
+    n_ins = int(max([o['in_begin'] + o['k'] for o in ops], default=0))
+    ins = blob[ins_off:ins_off + n_ins * _lib.IN_DTYPE.itemsize].view(_lib.IN_DTYPE)
+    assert ins_off + n_ins * _lib.IN_DTYPE.itemsize <= len(blob)
+    return run, phases, ops, ins
+
+
 def run_network(exported, table, net_index):
-    net = exported['nets'][net_index]
-    ops, ins, phases = exported['ops'], exported['ins'], exported['phases']
+    net, phases, ops, ins = network_views(exported, net_index)
     arena = np.full(int(net['arena_elems']) + 4, np.nan + 0j, dtype=np.complex128)
 
     def load(src, off):
         if src & _lib.SRC_TABLE:
-            return table[(src & ~_lib.SRC_TABLE) + off]
+            base = src & ~_lib.SRC_TABLE
+            assert base + off.max() < len(table)
+            return table[base + off]
+        assert src + off.max() <= int(net['arena_elems'])
         v = arena[src + off]
-        assert not np.isnan(v.real), 'read of an arena element nobody wrote'
+        assert not np.isnan(v.real).any(), 'read of an arena element nobody wrote'
         return v
 
-    for p in range(int(net['phase_begin']), int(net['phase_begin'] + net['n_phases'])):
+    for p in range(int(net['n_phases'])):
         ph = phases[p]
         writes = []
         elem = 0
@@ -95,18 +130,27 @@ def run_network(exported, table, net_index):
             assert op['elem_begin'] == elem
             elem += 1 << w
             operands = ins[int(op['in_begin']):int(op['in_begin']) + k]
-            for j in range(1 << w):
-                acc = 0j
-                for sv in range(s + 1):
-                    idx = j | (sv << w)
-                    prod = 1 + 0j
-                    for d in operands:
-                        prod *= load(int(d['src']), _pext(idx, int(d['mask'])))
-                    acc += prod
-                writes.append((int(op['dst']) + j, acc))
+            j = np.arange(1 << w, dtype=np.int64)
+            acc = np.zeros(1 << w, dtype=np.complex128)
+            for sv in range(s + 1):
+                prod = np.ones(1 << w, dtype=np.complex128)
+                for d in operands:
+                    mask = int(d['mask'])
+                    off = _pext(j | (sv << w), mask)
+                    low = _gather_runs(j, d['runs'])
+                    if low is not None:
+                        # runs cover the bits below the summed one; the summed
+                        # bit is the operand's most significant axis
+                        top = (mask >> w) & 1 if s else 0
+                        stride = 1 << (bin(mask).count('1') - 1) if top else 0
+                        assert np.array_equal(off, low + sv * stride)
+                    prod = prod * load(int(d['src']), off)
+                acc = acc + prod
+            writes.append((int(op['dst']), acc))
         assert elem == ph['total_elems']
         for off, val in writes:          # all reads of a phase precede its writes
-            arena[off] = val
+            assert off + len(val) <= int(net['arena_elems'])
+            arena[off:off + len(val)] = val
     res = int(net['result_src'])
     return table[res & ~_lib.SRC_TABLE] if res & _lib.SRC_TABLE else arena[res]
 
@@ -114,4 +158,4 @@ def run_network(exported, table, net_index):
 def run_plan(plan, params):
     ex = plan.export()
     table = gate_table(ex, np.asarray(params, dtype=np.float64))
-    return np.array([run_network(ex, table, i) for i in range(len(ex['nets']))])
+    return np.array([run_network(ex, table, i) for i in range(len(ex['runs']))])

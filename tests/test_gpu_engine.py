@@ -70,6 +70,20 @@ def test_engine_plan_reuse_across_angles(cuda_device):
     assert len(eng._cache) == 1
 
 
+def test_engine_graph_replay_matches_direct_launch(cuda_device):
+    """energy_expectation replays a captured CUDA graph; interleaved angle
+    sets give the energy of a direct launch + host fp64 sum every time."""
+    G = graphs.regular(200, seed=2)
+    eng = _engine()
+    sets = [graphs.angles(2, seed=s) for s in (1, 2, 1, 3)]
+    for gamma, beta in sets:
+        E = eng.energy_expectation(G, gamma, beta)
+        terms = eng.edge_terms(G, gamma, beta).astype(np.complex128)
+        direct = (G.number_of_edges() - np.sum(terms.real)) / 2
+        assert abs(E - direct) < 1e-9 * G.number_of_edges()
+    assert eng.energy_expectation(G, *sets[0]) == eng.energy_expectation(G, *sets[2])
+
+
 def test_engine_deterministic_and_status_clean(cuda_device):
     G, w = golden_graph('cfg2')
     eng = _engine()
