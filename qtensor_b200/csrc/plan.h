@@ -134,8 +134,8 @@ struct Network {
 struct DeviceBuffers {
     void* runs = nullptr;         // DevNetRun per network
     void* blobs = nullptr;        // concatenated network blobs
-    void* entries = nullptr;
-    void* terms = nullptr;
+    void* entries = nullptr;      // common image: gate entries then angle terms
+    void* terms = nullptr;        // inside the entries allocation
     void* table = nullptr;        // complex64 gate table
     void* status = nullptr;       // int error word
 };
@@ -159,6 +159,8 @@ struct qtb_plan {
     std::vector<qtb::DevPhase> dphases;
     std::vector<qtb::DevNetRun> druns;
     std::vector<uint8_t> dblobs;
+    uint32_t common_bytes = 0;       // staged gate entries + angle terms
+    uint32_t common_terms_off = 0;
     bool uploaded = false;
     int device = -1;
     qtb::DeviceBuffers dev;

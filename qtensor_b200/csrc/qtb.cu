@@ -4,14 +4,17 @@
 //                            (qtensor/ProcessingFrameworks.py:29-31,45-147):
 //                            product of the bucket's tensors over the sorted
 //                            union of their variables, summed over variable 0
-//   K0  qtb_table_kernel     gate tensors of a request generated from its
-//                            angles (qtree gate tensors, OpFactory.py:44-58)
 //   K3  qtb_network_kernel   a whole edge network (bucket_elimination,
-//                            Simulate.py:90-94) per CTA: its buckets run in
-//                            dependency phases, intermediates in shared
-//                            memory (or a per-CTA global arena)
-//   K4  qtb_energy_kernel    fp64 Neumaier sum of the edge terms and the
-//                            MaxCut post-processing (QAOASimulator.py:27-41)
+//                            Simulate.py:90-94) per CTA: the gate tensors
+//                            generated from the request's angles (qtree gate
+//                            tensors, OpFactory.py:44-58), the buckets in
+//                            dependency phases with intermediates in shared
+//                            memory (or a per-CTA global arena), and in the
+//                            last CTA to finish the fp64 Neumaier sum of the
+//                            edge terms with the MaxCut post-processing
+//                            (QAOASimulator.py:27-41)
+//   K0  qtb_table_kernel     the gate table in global memory, for plans whose
+//                            table does not fit in shared memory
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -85,8 +88,10 @@ __global__ void __launch_bounds__(256) qtb_bucket_kernel(const BucketArgs a) {
 }
 
 // ----------------------------------------------------------------- K0
-__device__ double2 gate_value(int kind, double alpha, const int* ix) {
+// Element of a gate tensor at native index bits: axis a <-> bit a of ixb.
+__device__ double2 gate_value(int kind, double alpha, uint32_t ixb) {
     const double r2 = 0.70710678118654752440;
+    const int ix[3] = {(int)(ixb & 1u), (int)((ixb >> 1) & 1u), (int)((ixb >> 2) & 1u)};
     double s, c;
     switch (kind) {
         case QTB_GATE_M: return make_double2(ix[0] == ix[1] ? 1.0 : 0.0, 0.0);
@@ -128,44 +133,77 @@ __device__ double2 gate_value(int kind, double alpha, const int* ix) {
     }
 }
 
+// Fill one gate-table entry: the gate tensor for alpha = sum coef*param,
+// with its sliced axes fixed to 0 and the rest transposed to sorted order.
+__device__ void table_entry(const DevEntry& en, const DevTerm* terms, const double* params,
+                            float2* table) {
+    double alpha = 0.0;
+    for (int t = 0; t < en.expr_count; ++t)
+        alpha += terms[en.expr_begin + t].coef * params[terms[en.expr_begin + t].param];
+    const int n = 1 << en.rank_out;
+    for (int o = 0; o < n; ++o) {
+        uint32_t ixb = 0;   // sliced axes stay 0
+        for (int a = 0; a < en.rank_out; ++a)
+            ixb |= (uint32_t)((o >> (en.rank_out - 1 - a)) & 1) << en.perm[a];
+        const double2 v = gate_value(en.kind, alpha, ixb);
+        table[en.off + o] = make_float2((float)v.x, (float)v.y);
+    }
+}
+
 __global__ void qtb_table_kernel(const DevEntry* entries, int n_entries, const DevTerm* terms,
                                  const double* params, float2* table) {
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_entries; e += gridDim.x * blockDim.x) {
-        const DevEntry en = entries[e];
-        double alpha = 0.0;
-        for (int t = 0; t < en.expr_count; ++t)
-            alpha += terms[en.expr_begin + t].coef * params[terms[en.expr_begin + t].param];
-        const int n = 1 << en.rank_out;
-        for (int o = 0; o < n; ++o) {
-            int ix[5] = {0, 0, 0, 0, 0};
-            for (int a = 0; a < en.rank_out; ++a) ix[en.perm[a]] = (o >> (en.rank_out - 1 - a)) & 1;
-            const double2 v = gate_value(en.kind, alpha, ix);
-            table[en.off + o] = make_float2((float)v.x, (float)v.y);
-        }
-    }
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_entries; e += gridDim.x * blockDim.x)
+        table_entry(entries[e], terms, params, table);
 }
 
 // ----------------------------------------------------------------- K3
 struct Job {
     const DevNetRun* net;
-    const uint4* blobs;      // base of all network blobs (16-byte units)
-    const float2* table;
     float2* term;
 };
 
+// Arguments shared by every CTA of one run (all size classes).
+struct RunArgs {
+    const uint4* blobs;           // network blobs
+    const uint4* common;          // [DevEntry x n_entries, padded to 16 B][DevTerm ...]
+    uint32_t common_bytes;        // multiple of 16
+    uint32_t n_entries;
+    uint32_t terms_off;           // byte offset of the DevTerm array in common
+    uint32_t table_elems;
+    const double* params;
+    const float2* gtable;         // global gate table (kernels without a shared table)
+    float2* gscratch;             // global arenas (kernels without a shared arena)
+    uint32_t arena_capacity;      // elements per CTA
+    uint32_t blob_capacity;       // bytes per CTA
+    int* status;
+    unsigned int* done;           // CTAs finished in this run (reset by the last one)
+    uint32_t total_jobs;          // CTAs of the run over all its launches
+    const float2* terms;          // the run's edge terms, [total_jobs]
+    double* energy;               // MaxCut energy of the run, or null
+};
+
 constexpr int kStatusArena = 1;        // network arena larger than the launch's capacity
-constexpr int kStatusStageTimeout = 2; // the plan blob copy did not complete in time
+constexpr int kStatusStageTimeout = 2; // a staging copy did not complete in time
 constexpr int kStatusBlob = 4;         // network blob larger than the launch's capacity
 constexpr uint32_t kStageSpinLimit = 1u << 26;
+constexpr uint32_t kSmemTableLimitElems = 2048;   // 16 KB of gate table per CTA
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// Copy the network's plan blob global -> shared with one bulk (TMA) copy
-// completing on an mbarrier; every thread waits with a bounded spin.
-// Returns false (and sets the status word) if the copy did not land.
-__device__ bool stage_blob(void* dst, const void* src, uint32_t bytes, uint64_t* bar, int* status) {
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+
+// Bulk (TMA) copies global -> shared completing on one mbarrier; every
+// thread waits with a bounded spin.  Returns false (status word set) if the
+// copies did not land.
+__device__ bool stage(void* dst0, const void* src0, uint32_t bytes0, void* dst1, const void* src1,
+                      uint32_t bytes1, uint64_t* bar, int* status) {
     const uint32_t bar_a = smem_addr(bar);
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a));
@@ -173,12 +211,11 @@ __device__ bool stage_blob(void* dst, const void* src, uint32_t bytes, uint64_t*
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a),
+                     "r"(bytes0 + bytes1)
                      : "memory");
-        asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-                "r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(bar_a)
-            : "memory");
+        if (bytes0) bulk_copy(dst0, src0, bytes0, bar_a);
+        if (bytes1) bulk_copy(dst1, src1, bytes1, bar_a);
     }
     uint32_t done = 0;
     for (uint32_t it = 0; it < kStageSpinLimit; ++it) {
@@ -192,33 +229,79 @@ __device__ bool stage_blob(void* dst, const void* src, uint32_t bytes, uint64_t*
     return __syncthreads_and(done) != 0;
 }
 
-// One CTA contracts one network.  Shared memory: [mbarrier | plan blob |
-// arena]; with kSmemArena == false the arena is this CTA's slice of gscratch.
+__device__ __forceinline__ void neumaier_add(double& sum, double& comp, double x) {
+    const double t = sum + x;
+    comp += fabs(sum) >= fabs(x) ? (sum - t) + x : (x - t) + sum;
+    sum = t;
+}
+
+// Compensated fp64 sum of Re(terms) by one CTA in a fixed order, then
+// energy = (n - sum) / 2.
+__device__ void reduce_energy(const float2* terms, uint32_t n, double* energy) {
+    __shared__ double ws[32], wc[32];
+    double s = 0.0, c = 0.0;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) neumaier_add(s, c, (double)__ldcg(terms + i).x);
+    for (int off = 16; off > 0; off >>= 1) {
+        const double os = __shfl_xor_sync(0xffffffffu, s, off);
+        const double oc = __shfl_xor_sync(0xffffffffu, c, off);
+        neumaier_add(s, c, os);
+        neumaier_add(s, c, oc);
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        ws[warp] = s;
+        wc[warp] = c;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ts = 0.0, tc = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+            neumaier_add(ts, tc, ws[i]);
+            neumaier_add(ts, tc, wc[i]);
+        }
+        *energy = ((double)n - (ts + tc)) * 0.5;
+    }
+}
+
+// One CTA contracts one network.  Shared memory, in order: mbarrier (16 B),
+// [plan-wide gate entries + angle terms], the network's plan blob, [gate
+// table], [arena]; the bracketed parts exist when kSmemTable / kSmemArena.
 // Phases run in order with a barrier after each; inside a phase the
 // elements of all its ops are spread over the threads.
-template <bool kSmemArena>
+template <bool kSmemArena, bool kSmemTable>
 __global__ void __launch_bounds__(1024) qtb_network_kernel(const Job* __restrict__ jobs,
-                                                           float2* __restrict__ gscratch,
-                                                           uint32_t arena_capacity,
-                                                           uint32_t blob_capacity,
-                                                           int* __restrict__ status) {
+                                                           const RunArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
-    unsigned char* blob = smem + 16;
+    unsigned char* common = smem + 16;
+    unsigned char* blob = common + (kSmemTable ? a.common_bytes : 0);
+    float2* stable = reinterpret_cast<float2*>(blob + a.blob_capacity);
+    unsigned char* after_table =
+        blob + a.blob_capacity + (kSmemTable ? ((a.table_elems * 8u + 15u) & ~15u) : 0u);
     const Job job = jobs[blockIdx.x];
     const DevNetRun net = *job.net;
-    if (net.arena_elems > arena_capacity || net.blob_bytes > blob_capacity) {
+    if (net.arena_elems > a.arena_capacity || net.blob_bytes > a.blob_capacity) {
         if (threadIdx.x == 0)
-            atomicOr(status, net.arena_elems > arena_capacity ? kStatusArena : kStatusBlob);
+            atomicOr(a.status, net.arena_elems > a.arena_capacity ? kStatusArena : kStatusBlob);
         return;
     }
-    if (!stage_blob(blob, job.blobs + net.blob_off16, net.blob_bytes, bar, status)) return;
-    float2* arena = kSmemArena ? reinterpret_cast<float2*>(blob + blob_capacity)
-                               : gscratch + (size_t)blockIdx.x * arena_capacity;
+    if (!stage(blob, a.blobs + net.blob_off16, net.blob_bytes, common, a.common,
+               kSmemTable ? a.common_bytes : 0u, bar, a.status))
+        return;
+    const float2* __restrict__ table = a.gtable;
+    if (kSmemTable) {
+        const DevEntry* entries = reinterpret_cast<const DevEntry*>(common);
+        const DevTerm* terms = reinterpret_cast<const DevTerm*>(common + a.terms_off);
+        for (uint32_t e = threadIdx.x; e < a.n_entries; e += blockDim.x)
+            table_entry(entries[e], terms, a.params, stable);
+        __syncthreads();
+        table = stable;
+    }
+    float2* arena = kSmemArena ? reinterpret_cast<float2*>(after_table)
+                               : a.gscratch + (size_t)blockIdx.x * a.arena_capacity;
     const DevPhase* phases = reinterpret_cast<const DevPhase*>(blob);
     const DevOp* ops = reinterpret_cast<const DevOp*>(blob + net.n_phases * sizeof(DevPhase));
     const DevIn* ins = reinterpret_cast<const DevIn*>(blob + net.ins_off);
-    const float2* __restrict__ table = job.table;
 
     for (uint32_t p = 0; p < net.n_phases; ++p) {
         const DevPhase ph = phases[p];
@@ -242,13 +325,13 @@ __global__ void __launch_bounds__(1024) qtb_network_kernel(const Job* __restrict
                 const uint32_t off = gather_bits(j, d, (1u << w) - 1u);
                 const bool tab = d.src & kSrcTable;
                 const float2* base = tab ? table + (d.src & ~kSrcTable) : arena + d.src;
-                const float2 x0 = tab ? __ldg(base + off) : base[off];
+                const float2 x0 = (tab && !kSmemTable) ? __ldg(base + off) : base[off];
                 p0 = t == 0 ? x0 : cmul(p0, x0);
                 if (op.sum) {
                     float2 x1 = x0;
                     if ((d.mask >> w) & 1u) {
                         const uint32_t stride = 1u << (__popc(d.mask) - 1);
-                        x1 = tab ? __ldg(base + off + stride) : base[off + stride];
+                        x1 = (tab && !kSmemTable) ? __ldg(base + off + stride) : base[off + stride];
                     }
                     p1 = t == 0 ? x1 : cmul(p1, x1);
                 }
@@ -257,35 +340,21 @@ __global__ void __launch_bounds__(1024) qtb_network_kernel(const Job* __restrict
         }
         __syncthreads();
     }
+    __shared__ unsigned int is_last;
     if (threadIdx.x == 0) {
         *job.term = (net.result_src & kSrcTable) ? table[net.result_src & ~kSrcTable]
                                                  : arena[net.result_src];
-    }
-}
-
-// ----------------------------------------------------------------- K4
-__device__ __forceinline__ void neumaier_add(double& sum, double& comp, double x) {
-    const double t = sum + x;
-    comp += fabs(sum) >= fabs(x) ? (sum - t) + x : (x - t) + sum;
-    sum = t;
-}
-
-__global__ void __launch_bounds__(256) qtb_energy_kernel(const float2* __restrict__ terms, int n,
-                                                         double* __restrict__ energy) {
-    __shared__ double ssum[256], scomp[256];
-    double s = 0.0, c = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) neumaier_add(s, c, (double)terms[i].x);
-    ssum[threadIdx.x] = s;
-    scomp[threadIdx.x] = c;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double ts = 0.0, tc = 0.0;
-        for (int i = 0; i < (int)blockDim.x; ++i) {
-            neumaier_add(ts, tc, ssum[i]);
-            neumaier_add(ts, tc, scomp[i]);
+        if (a.energy) {
+            __threadfence();
+            is_last = atomicAdd(a.done, 1u) == a.total_jobs - 1u;
         }
-        const double total = ts + tc;
-        *energy = ((double)n - total) * 0.5;
+    }
+    if (!a.energy) return;
+    __syncthreads();
+    if (is_last) {
+        __threadfence();
+        reduce_energy(a.terms, a.total_jobs, a.energy);
+        if (threadIdx.x == 0) *a.done = 0u;   // ready for the next run
     }
 }
 
@@ -301,7 +370,14 @@ static int cuda_fail(cudaError_t e, const char* what) {
 
 // Dynamic shared memory a CTA may use (B200: 227 KB per block).
 constexpr uint32_t kSmemLimitBytes = 224 * 1024;
-constexpr int kMaxClasses = 5;
+// Shared memory of one SM available to CTAs, and the per-CTA reserve.
+constexpr uint32_t kSmemPerSm = 228 * 1024;
+constexpr uint32_t kSmemReservePerCta = 1024;
+// Resident CTAs per SM that define the shared-memory size classes (a network
+// goes to the class of the most CTAs per SM its staging + arena allows).
+constexpr int kClassCtas[] = {16, 12, 10, 8, 6, 5, 4, 3, 2, 1};
+constexpr int kSmemClasses = (int)(sizeof(kClassCtas) / sizeof(kClassCtas[0]));
+constexpr int kMaxClasses = kSmemClasses + 1;   // + the global-arena class
 
 struct LaunchClass {
     bool smem;
@@ -314,10 +390,31 @@ struct LaunchClass {
     size_t smem_bytes;
 };
 
+// Plan-wide staging image: gate entries, padded to 16 bytes, then the angle
+// terms; small enough to stage into every CTA next to its network blob.
+struct CommonImage {
+    std::vector<uint8_t> bytes;
+    uint32_t terms_off = 0;
+};
+
+static CommonImage common_image(const qtb_plan* plan) {
+    CommonImage c;
+    const size_t e_bytes = plan->entries.size() * sizeof(DevEntry);
+    c.terms_off = (uint32_t)((e_bytes + 15) & ~size_t(15));
+    const size_t total = (c.terms_off + plan->terms.size() * sizeof(DevTerm) + 15) & ~size_t(15);
+    c.bytes.assign(std::max<size_t>(total, 16), 0);
+    if (e_bytes) std::memcpy(c.bytes.data(), plan->entries.data(), e_bytes);
+    if (!plan->terms.empty())
+        std::memcpy(c.bytes.data() + c.terms_off, plan->terms.data(), plan->terms.size() * sizeof(DevTerm));
+    return c;
+}
+
 struct RunCache {
-    Job* jobs = nullptr;
+    Job* jobs = nullptr;                // jobs of all classes, then the done counter
+    unsigned int* done = nullptr;
     std::vector<LaunchClass> classes;   // widest first
     size_t scratch_elems = 0;
+    bool smem_table = true;
 };
 
 }  // namespace qtb
@@ -346,7 +443,7 @@ static qtb_plan_device* dev_state(const qtb_plan* p) {
 
 static void free_device(qtb_plan* plan) {
     DeviceBuffers& d = plan->dev;
-    void* ptrs[] = {d.runs, d.blobs, d.entries, d.terms, d.table, d.status};
+    void* ptrs[] = {d.runs, d.blobs, d.entries, d.table, d.status};   // terms lives in entries
     for (void* p : ptrs)
         if (p) cudaFree(p);
     d = DeviceBuffers();
@@ -355,6 +452,22 @@ static void free_device(qtb_plan* plan) {
         if (kv.second.jobs) cudaFree(kv.second.jobs);
     s->runs.clear();
     plan->uploaded = false;
+}
+
+// Kernel instantiation for a launch class.
+static void launch_class(const LaunchClass& lc, bool smem_table, const Job* jobs, const RunArgs& a,
+                         cudaStream_t st) {
+    if (lc.smem) {
+        if (smem_table)
+            qtb_network_kernel<true, true><<<lc.n_jobs, lc.threads, lc.smem_bytes, st>>>(jobs, a);
+        else
+            qtb_network_kernel<true, false><<<lc.n_jobs, lc.threads, lc.smem_bytes, st>>>(jobs, a);
+    } else {
+        if (smem_table)
+            qtb_network_kernel<false, true><<<lc.n_jobs, lc.threads, lc.smem_bytes, st>>>(jobs, a);
+        else
+            qtb_network_kernel<false, false><<<lc.n_jobs, lc.threads, lc.smem_bytes, st>>>(jobs, a);
+    }
 }
 
 static void destroy_streams(qtb_plan_device* s) {
@@ -394,21 +507,59 @@ static int threads_for(uint32_t max_elems) {
 // Launch classes of a run: networks bucketed by the shared memory they need
 // (16 KB, 48 KB, 112 KB, 224 KB; larger arenas go to global scratch), the
 // widest class first so its long critical path starts early.
+static size_t fixed_smem(const qtb_plan* plan, bool smem_table) {
+    if (!smem_table) return 16;
+    const size_t table = ((size_t)plan->table_elems * 8 + 15) & ~size_t(15);
+    return 16 + plan->common_bytes + table;
+}
+
+static uint32_t class_bound(int c) {
+    const uint32_t b = kSmemPerSm / (uint32_t)kClassCtas[c] - kSmemReservePerCta;
+    return std::min(b, kSmemLimitBytes);
+}
+
+static size_t net_need(const DevNetRun& r, size_t fixed) {
+    return fixed + (size_t)r.blob_bytes + 8 * (size_t)((r.arena_elems + 3u) & ~3u);
+}
+
+// Launch classes of a run: each network goes to the shared-memory class of
+// the most resident CTAs per SM its staging + arena allows (networks too
+// large for shared memory use a global arena), the largest class launched
+// first so its long critical path starts early.
 static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms, RunCache* rc) {
-    const uint32_t bounds[4] = {16 * 1024, 48 * 1024, 112 * 1024, kSmemLimitBytes};
+    rc->smem_table = plan->table_elems <= kSmemTableLimitElems;
+    const size_t fixed = fixed_smem(plan, rc->smem_table);
     std::vector<std::vector<int32_t>> members(kMaxClasses);
     for (int32_t i = first; i < first + count; ++i) {
         const DevNetRun& r = plan->druns[i];
-        const size_t need = 16 + (size_t)r.blob_bytes + 8 * (size_t)((r.arena_elems + 3u) & ~3u);
-        int c = 4;
-        for (int b = 0; b < 4; ++b)
-            if (need <= bounds[b]) {
+        const size_t need = net_need(r, fixed);
+        int c = kSmemClasses;   // global arena
+        for (int b = 0; b < kSmemClasses; ++b)
+            if (need <= class_bound(b)) {
                 c = b;
                 break;
             }
-        if (c == 4 && 16 + (size_t)r.blob_bytes > kSmemLimitBytes)
+        if (c == kSmemClasses && fixed + (size_t)r.blob_bytes > kSmemLimitBytes)
             return fail(QTB_ERR_UNSUPPORTED, "network plan blob exceeds shared memory");
         members[c].push_back(i);
+    }
+    // a class holds the largest blob and the largest arena of its members;
+    // move members to the global class while that exceeds the CTA limit
+    for (int c = 0; c < kSmemClasses; ++c) {
+        auto& m = members[c];
+        for (;;) {
+            uint32_t blob = 0, arena = 0;
+            for (int32_t i : m) {
+                blob = std::max(blob, plan->druns[i].blob_bytes);
+                arena = std::max(arena, (plan->druns[i].arena_elems + 3u) & ~3u);
+            }
+            if (m.empty() || fixed + blob + 8 * (size_t)arena <= kSmemLimitBytes) break;
+            auto big = std::max_element(m.begin(), m.end(), [&](int32_t x, int32_t y) {
+                return net_need(plan->druns[x], fixed) < net_need(plan->druns[y], fixed);
+            });
+            members[kSmemClasses].push_back(*big);
+            m.erase(big);
+        }
     }
     std::vector<Job> jobs;
     const auto* runs = static_cast<const DevNetRun*>(plan->dev.runs);
@@ -417,7 +568,7 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
     for (int c = kMaxClasses - 1; c >= 0; --c) {
         if (members[c].empty()) continue;
         LaunchClass lc{};
-        lc.smem = c < 4;
+        lc.smem = c < kSmemClasses;
         lc.job_offset = jobs.size();
         lc.n_jobs = (int)members[c].size();
         uint32_t cap = 4, blob = 16, maxe = 1;
@@ -427,25 +578,27 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
             maxe = std::max(maxe, plan->druns[i].max_elems);
             Job j;
             j.net = runs + i;
-            j.blobs = static_cast<const uint4*>(plan->dev.blobs);
-            j.table = static_cast<const float2*>(plan->dev.table);
             j.term = terms + (i - first);
             jobs.push_back(j);
         }
         lc.capacity = (cap + 3u) & ~3u;
         lc.blob_capacity = blob;
         lc.threads = threads_for(maxe);
-        lc.smem_bytes = 16 + (size_t)blob + (lc.smem ? 8 * (size_t)lc.capacity : 0);
+        lc.smem_bytes = fixed + (size_t)blob + (lc.smem ? 8 * (size_t)lc.capacity : 0);
         if (!lc.smem) {
             lc.scratch_offset = rc->scratch_elems;
             rc->scratch_elems += (size_t)lc.capacity * lc.n_jobs;
         }
         rc->classes.push_back(lc);
     }
+    // jobs, then one 16-byte slot for the done counter (zeroed)
+    const size_t job_bytes = jobs.size() * sizeof(Job);
     void* buf = nullptr;
-    int r = upload_vec(jobs, &buf);
-    if (r) return r;
+    QTB_CUDA(cudaMalloc(&buf, job_bytes + 16));
+    QTB_CUDA(cudaMemcpy(buf, jobs.data(), job_bytes, cudaMemcpyHostToDevice));
+    QTB_CUDA(cudaMemset(static_cast<char*>(buf) + job_bytes, 0, 16));
     rc->jobs = static_cast<Job*>(buf);
+    rc->done = reinterpret_cast<unsigned int*>(static_cast<char*>(buf) + job_bytes);
     return QTB_OK;
 }
 
@@ -462,9 +615,13 @@ int qtb_init(int device) {
     QTB_CUDA(cudaGetDeviceCount(&n));
     if (device < 0 || device >= n) return fail(QTB_ERR_ARG, "qtb_init: no such device");
     QTB_CUDA(cudaSetDevice(device));
-    QTB_CUDA(cudaFuncSetAttribute(qtb_network_kernel<true>,
+    QTB_CUDA(cudaFuncSetAttribute(qtb_network_kernel<true, true>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimitBytes));
-    QTB_CUDA(cudaFuncSetAttribute(qtb_network_kernel<false>,
+    QTB_CUDA(cudaFuncSetAttribute(qtb_network_kernel<false, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimitBytes));
+    QTB_CUDA(cudaFuncSetAttribute(qtb_network_kernel<true, false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimitBytes));
+    QTB_CUDA(cudaFuncSetAttribute(qtb_network_kernel<false, false>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimitBytes));
     return QTB_OK;
 }
@@ -506,8 +663,13 @@ int qtb_plan_upload(qtb_plan* plan) {
     int r;
     if ((r = upload_vec(plan->druns, &plan->dev.runs))) return r;
     if ((r = upload_vec(plan->dblobs, &plan->dev.blobs))) return r;
-    if ((r = upload_vec(plan->entries, &plan->dev.entries))) return r;
-    if ((r = upload_vec(plan->terms, &plan->dev.terms))) return r;
+    {
+        const CommonImage c = common_image(plan);
+        plan->common_bytes = (uint32_t)c.bytes.size();
+        plan->common_terms_off = c.terms_off;
+        if ((r = upload_vec(c.bytes, &plan->dev.entries))) return r;
+        plan->dev.terms = static_cast<char*>(plan->dev.entries) + c.terms_off;
+    }
     QTB_CUDA(cudaMalloc(&plan->dev.table, std::max<size_t>(16, (size_t)plan->table_elems * 8)));
     QTB_CUDA(cudaMalloc(&plan->dev.status, sizeof(int)));
     QTB_CUDA(cudaMemset(plan->dev.status, 0, sizeof(int)));
@@ -542,18 +704,14 @@ int qtb_plan_scratch_bytes(const qtb_plan* plan_c, int32_t first, int32_t count,
     if (!plan->uploaded) return fail(QTB_ERR_ARG, "plan_scratch_bytes: plan not uploaded");
     if (first < 0 || count < 0 || first + count > (int32_t)plan->druns.size())
         return fail(QTB_ERR_ARG, "plan_scratch_bytes: range out of bounds");
-    // the global-arena class gives every CTA the largest arena of its members
-    uint32_t cap = 0;
-    int n = 0;
-    for (int32_t i = first; i < first + count; ++i) {
-        const DevNetRun& r = plan->druns[i];
-        const size_t need = 16 + (size_t)r.blob_bytes + 8 * (size_t)((r.arena_elems + 3u) & ~3u);
-        if (need > kSmemLimitBytes) {
-            cap = std::max(cap, r.arena_elems);
-            ++n;
-        }
-    }
-    *bytes = (size_t)((cap + 3u) & ~3u) * n * sizeof(float2);
+    *bytes = 0;
+    if (count == 0) return QTB_OK;
+    // the exact class split of this range (the same one qtb_plan_run uses)
+    RunCache rc;
+    int r = build_run(plan, first, count, nullptr, &rc);
+    if (r) return r;
+    if (rc.jobs) cudaFree(rc.jobs);
+    *bytes = rc.scratch_elems * sizeof(float2);
     return QTB_OK;
 }
 
@@ -582,8 +740,22 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
         return fail(QTB_ERR_ARG, "plan_run: this range needs scratch memory (qtb_plan_scratch_bytes)");
     qtb_plan_device* s = dev_state(plan);
     if ((r = ensure_streams(s))) return r;
+    RunArgs a{};
+    a.blobs = static_cast<const uint4*>(plan->dev.blobs);
+    a.common = static_cast<const uint4*>(plan->dev.entries);
+    a.common_bytes = plan->common_bytes;
+    a.n_entries = (uint32_t)plan->entries.size();
+    a.terms_off = plan->common_terms_off;
+    a.table_elems = plan->table_elems;
+    a.params = params_dev;
+    a.gtable = static_cast<const float2*>(plan->dev.table);
+    a.status = static_cast<int*>(plan->dev.status);
+    a.done = rc->done;
+    a.total_jobs = (uint32_t)count;
+    a.terms = static_cast<const float2*>(terms_dev);
+    a.energy = energy_dev;
     const int n_entries = (int)plan->entries.size();
-    if (n_entries > 0) {
+    if (!rc->smem_table && n_entries > 0) {
         qtb_table_kernel<<<(n_entries + 127) / 128, 128, 0, st>>>(
             static_cast<const DevEntry*>(plan->dev.entries), n_entries,
             static_cast<const DevTerm*>(plan->dev.terms), params_dev,
@@ -608,15 +780,11 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
         const LaunchClass& lc = rc->classes[c];
         cudaStream_t cs = forked ? s->aux[c] : st;
         if (forked) QTB_CUDA(cudaStreamWaitEvent(cs, s->fork, 0));
-        if (lc.smem) {
-            qtb_network_kernel<true><<<lc.n_jobs, lc.threads, lc.smem_bytes, cs>>>(
-                rc->jobs + lc.job_offset, nullptr, lc.capacity, lc.blob_capacity,
-                static_cast<int*>(plan->dev.status));
-        } else {
-            qtb_network_kernel<false><<<lc.n_jobs, lc.threads, lc.smem_bytes, cs>>>(
-                rc->jobs + lc.job_offset, static_cast<float2*>(scratch_dev) + lc.scratch_offset,
-                lc.capacity, lc.blob_capacity, static_cast<int*>(plan->dev.status));
-        }
+        RunArgs ac = a;
+        ac.arena_capacity = lc.capacity;
+        ac.blob_capacity = lc.blob_capacity;
+        ac.gscratch = lc.smem ? nullptr : static_cast<float2*>(scratch_dev) + lc.scratch_offset;
+        launch_class(lc, rc->smem_table, rc->jobs + lc.job_offset, ac, cs);
         QTB_CUDA(cudaGetLastError());
         if (forked) {
             QTB_CUDA(cudaEventRecord(s->join[c], cs));
@@ -627,10 +795,6 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
         QTB_CUDA(cudaEventRecord(ev.second, st));
         s->pending.push_back(ev);
         s->kernel_launches += (int64_t)rc->classes.size();
-    }
-    if (energy_dev) {
-        qtb_energy_kernel<<<1, 256, 0, st>>>(static_cast<const float2*>(terms_dev), count, energy_dev);
-        QTB_CUDA(cudaGetLastError());
     }
     return QTB_OK;
 }
