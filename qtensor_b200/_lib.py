@@ -30,8 +30,9 @@ EXPORTS = (
     'qtb_plan_network_info', 'qtb_plan_network_peo', 'qtb_plan_check_params',
     'qtb_plan_export', 'qtb_plan_table_elems', 'qtb_plan_upload',
     'qtb_plan_scratch_bytes', 'qtb_plan_run', 'qtb_plan_device_status',
-    'qtb_plan_set_timing', 'qtb_plan_collect_timing',
+    'qtb_plan_set_timing', 'qtb_plan_collect_timing', 'qtb_plan_run_noalloc',
 )
+NOALLOC_SCRATCH_BYTES = 64 << 20
 
 
 class QtbError(RuntimeError):
@@ -119,6 +120,7 @@ def _declare(lib):
         'qtb_plan_device_status': (c.c_int, [P, c.POINTER(c.c_int32)]),
         'qtb_plan_set_timing': (c.c_int, [P, c.c_int32]),
         'qtb_plan_collect_timing': (c.c_int, [P, c.POINTER(c.c_double), c.POINTER(c.c_int64)]),
+        'qtb_plan_run_noalloc': (c.c_int, [P, c.c_int32, c.c_int32, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -799,6 +799,134 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
     return QTB_OK;
 }
 
+// ------------------------------------------------- allocation-free run
+}  // extern "C"
+
+namespace qtb {
+
+// Library-owned scratch of qtb_plan_run_noalloc: [completion counter, 256 B]
+// [unused, 256 B][jobs, 16 B each, rounded to 256 B][arenas].  Host code
+// must not take this symbol's address as a device pointer; the device
+// address comes from cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[QTB_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kNoallocMaxDevices = 64;
+static void* g_noalloc_addr[kNoallocMaxDevices] = {};
+static std::mutex g_noalloc_mu;
+
+// Jobs of a contiguous network range, written on the device.
+__global__ void qtb_noalloc_jobs_kernel(Job* jobs, const DevNetRun* runs, int32_t first,
+                                        int32_t count, float2* terms) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) {
+        jobs[i].net = runs + first + i;
+        jobs[i].term = terms + i;
+    }
+}
+
+// Once per device, with that device current: the scratch array's device
+// address and the kernels' shared-memory limits.
+static int noalloc_setup(int device, unsigned char** out) {
+    if (device < 0 || device >= kNoallocMaxDevices)
+        return fail(QTB_ERR_UNSUPPORTED, "run_noalloc: device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void* ptr = nullptr;
+        QTB_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+        QTB_CUDA(cudaFuncSetAttribute(qtb_network_kernel<false, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kSmemLimitBytes));
+        QTB_CUDA(cudaFuncSetAttribute(qtb_network_kernel<false, false>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kSmemLimitBytes));
+        g_noalloc_addr[device] = ptr;
+    }
+    *out = static_cast<unsigned char*>(g_noalloc_addr[device]);
+    return QTB_OK;
+}
+
+}  // namespace qtb
+
+extern "C" {
+
+int qtb_plan_run_noalloc(qtb_plan* plan, int32_t first, int32_t count, const double* params_dev,
+                         void* terms_dev, double* energy_dev, void* stream) {
+    if (!plan || !terms_dev || (plan->n_params > 0 && !params_dev))
+        return fail(QTB_ERR_ARG, "run_noalloc: null argument");
+    if (!plan->uploaded) return fail(QTB_ERR_ARG, "run_noalloc: plan not uploaded");
+    if (first < 0 || count < 1 || first + count > (int32_t)plan->druns.size())
+        return fail(QTB_ERR_ARG, "run_noalloc: network range out of bounds");
+    int device = 0;
+    QTB_CUDA(cudaGetDevice(&device));
+    if (device != plan->device) return fail(QTB_ERR_ARG, "run_noalloc: plan uploaded to another device");
+    unsigned char* scratch = nullptr;
+    int r = noalloc_setup(device, &scratch);
+    if (r) return r;
+    // one launch: every network of the range in a global arena slice
+    const bool smem_table = plan->table_elems <= kSmemTableLimitElems;
+    const size_t fixed = fixed_smem(plan, smem_table);
+    uint32_t cap = 4, blob = 16, maxe = 1;
+    for (int32_t i = first; i < first + count; ++i) {
+        cap = std::max(cap, plan->druns[i].arena_elems);
+        blob = std::max(blob, plan->druns[i].blob_bytes);
+        maxe = std::max(maxe, plan->druns[i].max_elems);
+    }
+    cap = (cap + 3u) & ~3u;
+    const size_t smem_bytes = fixed + blob;
+    if (smem_bytes > kSmemLimitBytes)
+        return fail(QTB_ERR_UNSUPPORTED, "run_noalloc: network plan blob exceeds shared memory");
+    const size_t jobs_off = 512;
+    const size_t arenas_off = jobs_off + (((size_t)count * sizeof(Job) + 255) & ~size_t(255));
+    const size_t need = arenas_off + (size_t)count * cap * sizeof(float2);
+    if (need > QTB_NOALLOC_SCRATCH_BYTES)
+        return fail(QTB_ERR_UNSUPPORTED,
+                    "run_noalloc: " + std::to_string(count) + " networks of arena " +
+                        std::to_string(cap) + " need " + std::to_string(need) +
+                        " bytes of scratch, more than the static " +
+                        std::to_string((size_t)QTB_NOALLOC_SCRATCH_BYTES) + "; split the range");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned int* done = reinterpret_cast<unsigned int*>(scratch);
+    Job* jobs = reinterpret_cast<Job*>(scratch + jobs_off);
+    float2* arenas = reinterpret_cast<float2*>(scratch + arenas_off);
+    QTB_CUDA(cudaMemsetAsync(done, 0, 256, st));
+    qtb_noalloc_jobs_kernel<<<(count + 255) / 256, 256, 0, st>>>(
+        jobs, static_cast<const DevNetRun*>(plan->dev.runs), first, count,
+        static_cast<float2*>(terms_dev));
+    QTB_CUDA(cudaGetLastError());
+    const int n_entries = (int)plan->entries.size();
+    if (!smem_table && n_entries > 0) {
+        qtb_table_kernel<<<(n_entries + 127) / 128, 128, 0, st>>>(
+            static_cast<const DevEntry*>(plan->dev.entries), n_entries,
+            static_cast<const DevTerm*>(plan->dev.terms), params_dev,
+            static_cast<float2*>(plan->dev.table));
+        QTB_CUDA(cudaGetLastError());
+    }
+    RunArgs a{};
+    a.blobs = static_cast<const uint4*>(plan->dev.blobs);
+    a.common = static_cast<const uint4*>(plan->dev.entries);
+    a.common_bytes = plan->common_bytes;
+    a.n_entries = (uint32_t)n_entries;
+    a.terms_off = plan->common_terms_off;
+    a.table_elems = plan->table_elems;
+    a.params = params_dev;
+    a.gtable = static_cast<const float2*>(plan->dev.table);
+    a.gscratch = arenas;
+    a.arena_capacity = cap;
+    a.blob_capacity = blob;
+    a.status = static_cast<int*>(plan->dev.status);
+    a.done = done;
+    a.total_jobs = (uint32_t)count;
+    a.terms = static_cast<const float2*>(terms_dev);
+    a.energy = energy_dev;
+    const int threads = threads_for(maxe);
+    if (smem_table)
+        qtb_network_kernel<false, true><<<count, threads, smem_bytes, st>>>(jobs, a);
+    else
+        qtb_network_kernel<false, false><<<count, threads, smem_bytes, st>>>(jobs, a);
+    QTB_CUDA(cudaGetLastError());
+    return QTB_OK;
+}
+
 int qtb_plan_device_status(qtb_plan* plan, int32_t* status) {
     if (!plan || !status) return fail(QTB_ERR_ARG, "plan_device_status: bad arguments");
     if (!plan->uploaded) {
