@@ -300,6 +300,9 @@ def run_b200(args):
                            parallelism='one graph per rank' if world > 1 else 'single GPU',
                            width_max=stats['width_max'], ops_per_step=stats['ops'],
                            compile_s=compile_s, alg_bytes_per_step=stats['alg_bytes'],
+                           launch_classes=[dict(zip(('networks', 'threads', 'smem_bytes',
+                                                     'smem_arena'), c))
+                                           for c in cg.plan.last_launch_config()],
                            alg_flops_per_step=stats['alg_flops']),
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                          'frac': achieved / peak, 'traffic': profiled_traffic(),

@@ -186,6 +186,14 @@ int qtb_plan_scratch_bytes(const qtb_plan* plan, int32_t first, int32_t count,
 int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* params_dev,
                  void* terms_dev, double* energy_dev, void* scratch_dev, void* stream);
 
+/* Block-size autotuning: when enabled, the first qtb_plan_run of a network
+ * range (outside stream capture) times every launch class with 64..1024
+ * threads per CTA and keeps the fastest; later runs reuse the choice.     */
+int qtb_plan_set_autotune(qtb_plan* plan, int32_t enable);
+/* Launch classes of the plan's most recent run: 4 ints per class (networks,
+ * threads per CTA, dynamic shared memory bytes, 1 = shared-memory arena). */
+int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32_t* n_classes);
+
 /* Device error word of the last run on this plan (0 = ok); synchronises. */
 int qtb_plan_device_status(qtb_plan* plan, int32_t* status);
 

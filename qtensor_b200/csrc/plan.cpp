@@ -92,7 +92,7 @@ uint64_t encode_runs(uint32_t mask, uint32_t w) {
     const uint32_t low = w >= 32 ? mask : (mask & ((1u << w) - 1u));
     uint64_t runs = 0;
     uint64_t n = 0;
-    uint32_t dst = 0;
+    uint32_t dst = 0, first_start = 0, first_len = 0;
     for (uint32_t bit = 0; bit < 32;) {
         if (!((low >> bit) & 1u)) {
             ++bit;
@@ -101,10 +101,18 @@ uint64_t encode_runs(uint32_t mask, uint32_t w) {
         uint32_t len = 0;
         while (bit + len < 32 && ((low >> (bit + len)) & 1u)) ++len;
         if (n == (uint64_t)kMaxRuns) return kRunsFallback << 60;
+        if (n == 0) {
+            first_start = bit;
+            first_len = len;
+        }
         runs |= (uint64_t)(bit | (len << 5) | (dst << 10)) << (15 * n);
         ++n;
         dst += len;
         bit += len;
+    }
+    if (n <= 1) {   // pre-decoded single run
+        const uint64_t lenmask = first_len >= 32 ? 0xffffffffull : ((1ull << first_len) - 1ull);
+        return (n == 0 ? 0ull : (lenmask | ((uint64_t)first_start << 32))) | (n << 60);
     }
     return runs | (n << 60);
 }

@@ -27,10 +27,13 @@ struct DevOp {
 };
 
 // One operand of an op: which union bits it holds, where it lives, and the
-// bit gather from an output index to the operand's index precompiled as at
-// most kMaxRuns contiguous runs: run r (15 bits at 15*r) = start | len << 5 |
-// dst << 10 moves bits [start, start+len) of the output index to [dst, ...);
-// bits 60..62 hold the run count, kRunsFallback when the mask needs more.
+// bit gather from an output index to the operand's index precompiled as
+// contiguous runs; bits 60..62 of `runs` hold the run count n.
+//   n <= 1: bits 0..31 = length mask of the run, bits 32..36 = its start
+//           (the gather is (j >> start) & lenmask; 0 when n == 0);
+//   2 <= n <= kMaxRuns: run r (15 bits at 15*r) = start | len << 5 |
+//           dst << 10 moves bits [start, start+len) of j to [dst, ...);
+//   n == kRunsFallback: more runs than kMaxRuns, gather bit by bit.
 struct DevIn {
     uint32_t mask;      // bit (u-1-v) set <=> union variable v is an axis
     uint32_t src;       // arena offset, or kSrcTable | gate-table offset

@@ -49,6 +49,7 @@ __device__ __forceinline__ uint32_t pext32(uint32_t x, uint32_t m) {
 // than kMaxRuns runs.
 __device__ __forceinline__ uint32_t gather_bits(uint32_t j, const DevIn& d, uint32_t low_mask) {
     const uint32_t n = (uint32_t)(d.runs >> 60);
+    if (n <= 1u) return (j >> ((uint32_t)(d.runs >> 32) & 31u)) & (uint32_t)d.runs;
     if (n == (uint32_t)kRunsFallback) return pext32(j, d.mask & low_mask);
     uint32_t off = 0;
 #pragma unroll
@@ -305,13 +306,22 @@ __global__ void __launch_bounds__(1024) qtb_network_kernel(const Job* __restrict
 
     for (uint32_t p = 0; p < net.n_phases; ++p) {
         const DevPhase ph = phases[p];
+        const uint32_t last = ph.op_first + ph.op_count - 1u;
         uint32_t oi = ph.op_first;
         DevOp op = ops[oi];
         uint32_t w = op.u - op.sum;
         uint32_t op_end = op.elem_begin + (1u << w);
         for (uint32_t g = threadIdx.x; g < ph.total_elems; g += blockDim.x) {
-            while (g >= op_end) {
-                op = ops[++oi];
+            if (g >= op_end) {
+                // binary search: the last op of the phase starting at or before g
+                uint32_t lo = oi + 1u, hi = last;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi + 1u) >> 1;
+                    if (ops[mid].elem_begin <= g) lo = mid;
+                    else hi = mid - 1u;
+                }
+                oi = lo;
+                op = ops[oi];
                 w = op.u - op.sum;
                 op_end = op.elem_begin + (1u << w);
             }
@@ -412,6 +422,7 @@ static CommonImage common_image(const qtb_plan* plan) {
 struct RunCache {
     Job* jobs = nullptr;                // jobs of all classes, then the done counter
     unsigned int* done = nullptr;
+    bool tuned = false;                 // block sizes chosen by the autotuner
     std::vector<LaunchClass> classes;   // widest first
     size_t scratch_elems = 0;
     bool smem_table = true;
@@ -422,6 +433,8 @@ struct RunCache {
 // plan-side device state kept outside the public struct
 struct qtb_plan_device {
     std::map<std::tuple<int32_t, int32_t, uintptr_t>, qtb::RunCache> runs;
+    const qtb::RunCache* last = nullptr;
+    bool autotune = false;
     bool timing = false;
     double kernel_ms = 0.0;
     int64_t kernel_launches = 0;
@@ -715,6 +728,48 @@ int qtb_plan_scratch_bytes(const qtb_plan* plan_c, int32_t first, int32_t count,
     return QTB_OK;
 }
 
+// Block-size autotuner: on the first run of a range, every launch class is
+// timed alone (energy reduction off) with each candidate block size; the
+// fastest of three timed launches per candidate is kept.
+static int autotune_run(RunCache* rc, const RunArgs& base, void* scratch_dev, cudaStream_t st) {
+    static const int kCandidates[] = {64, 128, 256, 512, 1024};
+    cudaEvent_t e0, e1;
+    QTB_CUDA(cudaEventCreate(&e0));
+    QTB_CUDA(cudaEventCreate(&e1));
+    RunArgs a = base;
+    a.energy = nullptr;
+    for (LaunchClass& lc : rc->classes) {
+        a.arena_capacity = lc.capacity;
+        a.blob_capacity = lc.blob_capacity;
+        a.gscratch = lc.smem ? nullptr : static_cast<float2*>(scratch_dev) + lc.scratch_offset;
+        int best_t = lc.threads;
+        float best_ms = 1e30f;
+        for (int t : kCandidates) {
+            LaunchClass trial = lc;
+            trial.threads = t;
+            launch_class(trial, rc->smem_table, rc->jobs + lc.job_offset, a, st);   // warm-up
+            for (int rep = 0; rep < 3; ++rep) {
+                QTB_CUDA(cudaEventRecord(e0, st));
+                launch_class(trial, rc->smem_table, rc->jobs + lc.job_offset, a, st);
+                QTB_CUDA(cudaEventRecord(e1, st));
+                QTB_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                QTB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best_t = t;
+                }
+            }
+            QTB_CUDA(cudaGetLastError());
+        }
+        lc.threads = best_t;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    rc->tuned = true;
+    return QTB_OK;
+}
+
 static int ensure_streams(qtb_plan_device* s) {
     if (s->fork) return QTB_OK;
     QTB_CUDA(cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming));
@@ -762,6 +817,12 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
             static_cast<float2*>(plan->dev.table));
         QTB_CUDA(cudaGetLastError());
     }
+    if (s->autotune && !rc->tuned) {
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        QTB_CUDA(cudaStreamIsCapturing(st, &cap));
+        if (cap == cudaStreamCaptureStatusNone && (r = autotune_run(rc, a, scratch_dev, st))) return r;
+    }
+    s->last = rc;
     std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
     if (s->timing) {
         if (!s->spare.empty()) {
@@ -924,6 +985,27 @@ int qtb_plan_run_noalloc(qtb_plan* plan, int32_t first, int32_t count, const dou
     else
         qtb_network_kernel<false, false><<<count, threads, smem_bytes, st>>>(jobs, a);
     QTB_CUDA(cudaGetLastError());
+    return QTB_OK;
+}
+
+int qtb_plan_set_autotune(qtb_plan* plan, int32_t enable) {
+    if (!plan) return fail(QTB_ERR_ARG, "plan_set_autotune: null plan");
+    dev_state(plan)->autotune = enable != 0;
+    return QTB_OK;
+}
+
+int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32_t* n_classes) {
+    if (!plan || !n_classes) return fail(QTB_ERR_ARG, "plan_last_launch_config: bad arguments");
+    const RunCache* rc = dev_state(plan)->last;
+    *n_classes = rc ? (int32_t)rc->classes.size() : 0;
+    if (!rc || !out) return QTB_OK;
+    for (int32_t c = 0; c < *n_classes && 4 * c + 3 < cap; ++c) {
+        const LaunchClass& lc = rc->classes[c];
+        out[4 * c] = lc.n_jobs;
+        out[4 * c + 1] = lc.threads;
+        out[4 * c + 2] = (int32_t)lc.smem_bytes;
+        out[4 * c + 3] = lc.smem ? 1 : 0;
+    }
     return QTB_OK;
 }
 

@@ -121,7 +121,7 @@ class QAOAEnergyEngine:
     """
 
     def __init__(self, composer='default', ordering='native', device=None, threads=0,
-                 cache_size=16, order_trials=16):
+                 cache_size=16, order_trials=16, autotune=True):
         _require_cuda()
         if ordering not in ('native', 'reference'):
             raise ValueError('ordering must be "native" or "reference"')
@@ -132,6 +132,7 @@ class QAOAEnergyEngine:
         self.threads = threads
         self.cache_size = cache_size
         self.order_trials = order_trials if ordering == 'native' else 0
+        self.autotune = autotune
         self._cache = {}
         self._by_id = {}        # id(G) -> (weakref, nodes, edges, p, key)
         self._lock = threading.Lock()
@@ -163,6 +164,7 @@ class QAOAEnergyEngine:
                 nq, gates = reference_lightcone(G, edge, p, self.cid)
                 plan.add_circuit(nq, gates, params, passes)
         plan.upload()
+        plan.set_autotune(self.autotune)
         cg = CompiledGraph(plan, edges, p, self.composer, self.device)
         with self._lock:
             if len(self._cache) >= self.cache_size:

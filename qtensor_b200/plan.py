@@ -127,6 +127,18 @@ class NetworkPlan:
                                      ptr(terms_dev), ptr(energy_dev), ptr(scratch_dev),
                                      ctypes.c_void_p(int(stream))))
 
+    def set_autotune(self, enable):
+        """Time every launch class with 64..1024 threads per CTA on the first
+        run of a range and keep the fastest."""
+        check(self._lib.qtb_plan_set_autotune(self._h, 1 if enable else 0))
+
+    def last_launch_config(self):
+        """[(networks, threads, smem bytes, smem arena?)] of the latest run."""
+        n = ctypes.c_int32()
+        out = np.zeros(4 * 16, dtype=np.int32)
+        check(self._lib.qtb_plan_last_launch_config(self._h, ptr(out), len(out), ctypes.byref(n)))
+        return [tuple(int(x) for x in out[4 * c:4 * c + 4]) for c in range(min(n.value, 16))]
+
     def device_status(self):
         s = ctypes.c_int32()
         check(self._lib.qtb_plan_device_status(self._h, ctypes.byref(s)))

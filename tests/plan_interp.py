@@ -79,6 +79,8 @@ def _gather_runs(j, runs):
     n = runs >> 60
     if n == 7:
         return None
+    if n <= 1:                       # pre-decoded single run
+        return (j >> ((runs >> 32) & 31)) & (runs & 0xffffffff)
     off = np.zeros_like(j)
     for r in range(n):
         rr = (runs >> (15 * r)) & 0x7fff
