@@ -18,6 +18,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -291,10 +293,28 @@ __global__ void __launch_bounds__(1024) qtb_network_kernel(const Job* __restrict
         return;
     const float2* __restrict__ table = a.gtable;
     if (kSmemTable) {
+        // one thread per table element: find its entry (entries are laid out
+        // in increasing offset), evaluate the gate tensor there
         const DevEntry* entries = reinterpret_cast<const DevEntry*>(common);
         const DevTerm* terms = reinterpret_cast<const DevTerm*>(common + a.terms_off);
-        for (uint32_t e = threadIdx.x; e < a.n_entries; e += blockDim.x)
-            table_entry(entries[e], terms, a.params, stable);
+        for (uint32_t i = threadIdx.x; i < a.table_elems; i += blockDim.x) {
+            uint32_t lo = 0, hi = a.n_entries - 1u;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1u) >> 1;
+                if (entries[mid].off <= i) lo = mid;
+                else hi = mid - 1u;
+            }
+            const DevEntry en = entries[lo];
+            double alpha = 0.0;
+            for (int t = 0; t < en.expr_count; ++t)
+                alpha += terms[en.expr_begin + t].coef * __ldg(a.params + terms[en.expr_begin + t].param);
+            const int o = (int)(i - en.off);
+            uint32_t ixb = 0;
+            for (int ax = 0; ax < en.rank_out; ++ax)
+                ixb |= (uint32_t)((o >> (en.rank_out - 1 - ax)) & 1) << en.perm[ax];
+            const double2 v = gate_value(en.kind, alpha, ixb);
+            stable[i] = make_float2((float)v.x, (float)v.y);
+        }
         __syncthreads();
         table = stable;
     }
@@ -738,6 +758,7 @@ static int autotune_run(RunCache* rc, const RunArgs& base, void* scratch_dev, cu
     QTB_CUDA(cudaEventCreate(&e1));
     RunArgs a = base;
     a.energy = nullptr;
+    const bool log = std::getenv("QTB_AUTOTUNE_LOG") != nullptr;
     for (LaunchClass& lc : rc->classes) {
         a.arena_capacity = lc.capacity;
         a.blob_capacity = lc.blob_capacity;
@@ -759,9 +780,15 @@ static int autotune_run(RunCache* rc, const RunArgs& base, void* scratch_dev, cu
                     best_ms = ms;
                     best_t = t;
                 }
+                if (log && rep == 2)
+                    std::fprintf(stderr, "qtb autotune: class of %d networks (smem %zu B) %4d threads %.1f us\n",
+                                 lc.n_jobs, lc.smem_bytes, t, 1e3 * ms);
             }
             QTB_CUDA(cudaGetLastError());
         }
+        if (log)
+            std::fprintf(stderr, "qtb autotune: class of %d networks -> %d threads (%.1f us)\n", lc.n_jobs,
+                         best_t, 1e3 * best_ms);
         lc.threads = best_t;
     }
     cudaEventDestroy(e0);

@@ -99,6 +99,19 @@ class CompiledGraph:
                 self.host_energy.copy_(self.energy, non_blocking=True)
             self._graph = graph
 
+    def device_graph(self):
+        """CUDA graph of one contraction from the device-resident angles in
+        ``self.params`` (no host copies); energy lands in ``self.energy``."""
+        if getattr(self, '_dgraph', None) is None:
+            with torch.cuda.device(self.device):
+                self.launch()
+                torch.cuda.synchronize(self.device)
+                graph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(graph):
+                    self.launch(stream=torch.cuda.current_stream(self.device))
+                self._dgraph = graph
+        return self._dgraph
+
     def energy_of(self, params):
         """MaxCut energy for ``params = gamma[0..p) + beta[0..p)`` (host
         doubles) by one graph replay and one synchronisation."""
