@@ -321,8 +321,9 @@ def run_b200(args):
                            parallelism='one graph per rank' if world > 1 else 'single GPU',
                            width_max=stats['width_max'], ops_per_step=stats['ops'],
                            compile_s=compile_s, alg_bytes_per_step=stats['alg_bytes'],
-                           launch_classes=[dict(zip(('networks', 'threads', 'smem_bytes',
-                                                     'smem_arena'), c))
+                           launch_classes=[{'networks': c[0], 'threads': c[1], 'smem_bytes': c[2],
+                                            'smem_arena': bool(c[3] & 1),
+                                            'persistent': bool(c[3] & 2)}
                                            for c in cg.plan.last_launch_config()],
                            alg_flops_per_step=stats['alg_flops']),
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',

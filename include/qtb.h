@@ -186,12 +186,18 @@ int qtb_plan_scratch_bytes(const qtb_plan* plan, int32_t first, int32_t count,
 int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* params_dev,
                  void* terms_dev, double* energy_dev, void* scratch_dev, void* stream);
 
-/* Block-size autotuning: when enabled, the first qtb_plan_run of a network
- * range (outside stream capture) times every launch class with 64..1024
- * threads per CTA and keeps the fastest; later runs reuse the choice.     */
+/* Schedule and block-size autotuning: when enabled, the first qtb_plan_run
+ * of a network range (outside stream capture) times every launch class of
+ * the class schedule (one CTA per network, networks grouped by shared
+ * memory, classes concurrent) with 64..1024 threads per CTA, then the whole
+ * class schedule against the persistent schedule (CTAs resident on every
+ * SM take networks widest-first from a queue), and keeps the faster; later
+ * runs reuse the choice.
+ * QTB_AUTOTUNE=0 in the environment keeps the default block sizes.        */
 int qtb_plan_set_autotune(qtb_plan* plan, int32_t enable);
 /* Launch classes of the plan's most recent run: 4 ints per class (networks,
- * threads per CTA, dynamic shared memory bytes, 1 = shared-memory arena). */
+ * threads per CTA, dynamic shared memory bytes, flags: 1 = shared-memory
+ * arena, 2 = persistent launch taking networks from a queue).             */
 int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32_t* n_classes);
 
 /* Device error word of the last run on this plan (0 = ok); synchronises. */

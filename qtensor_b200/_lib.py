@@ -74,12 +74,12 @@ class NetworkInfo(ctypes.Structure):
 # numpy views of the exported plan arrays (plan.h)
 NET_DTYPE = np.dtype([('op_begin', '<u4'), ('n_ops', '<u4'), ('phase_begin', '<u4'),
                       ('n_phases', '<u4'), ('arena_elems', '<u4'), ('result_src', '<u4'),
-                      ('max_elems', '<u4'), ('pad', '<u4')])
+                      ('max_elems', '<u4'), ('tail_start', '<u4')])
 OP_DTYPE = np.dtype([('u', 'u1'), ('sum', 'u1'), ('k', 'u1'), ('pad', 'u1'), ('dst', '<u4'),
                      ('elem_begin', '<u4'), ('in_begin', '<u4')])
 IN_DTYPE = np.dtype([('mask', '<u4'), ('src', '<u4'), ('runs', '<u8')])
 PHASE_DTYPE = np.dtype([('op_first', '<u4'), ('op_count', '<u4'), ('total_elems', '<u4'),
-                        ('pad', '<u4')])
+                        ('chunk_off', '<u4')])
 ENTRY_DTYPE = np.dtype([('kind', '<i4'), ('expr_begin', '<i4'), ('expr_count', '<i4'),
                         ('off', '<u4'), ('rank_in', 'i1'), ('rank_out', 'i1'),
                         ('sliced_mask', 'u1'), ('perm', 'i1', (5,))])

@@ -606,6 +606,10 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
                 return QTB_ERR_UNSUPPORTED;
             }
             max_rank = std::max(max_rank, op.u);
+            if (ops.size() >= 65535) {
+                *err = "compile: network has more than 65535 bucket operations";
+                return QTB_ERR_UNSUPPORTED;
+            }
             for (const Ref& r : b) {
                 uint32_t m = 0;
                 for (int32_t v : r.vars) {
@@ -886,18 +890,34 @@ void build_blobs(qtb_plan* plan) {
         r.arena_elems = (uint32_t)n.info.arena_elems;
         r.result_src = n.result_src;
         r.max_elems = n.max_elems;
+        r.tail_start = (uint32_t)n.phases.size();
+        while (r.tail_start > 0 && n.phases[r.tail_start - 1].total_elems <= 32) --r.tail_start;
         const size_t ph_bytes = n.phases.size() * sizeof(DevPhase);
         const size_t op_bytes = n.ops.size() * sizeof(DevOp);
         const size_t in_bytes = n.ins.size() * sizeof(DevIn);
         r.ins_off = (uint32_t)(ph_bytes + op_bytes);
-        const size_t total = (ph_bytes + op_bytes + in_bytes + 15) & ~size_t(15);
+        // chunk tables: op of every kChunkElems-th flattened element
+        std::vector<DevPhase> phases = n.phases;
+        std::vector<uint16_t> chunks;
+        size_t chunk_base = ph_bytes + op_bytes + in_bytes;
+        for (DevPhase& ph : phases) {
+            ph.chunk_off = (uint32_t)(chunk_base + chunks.size() * sizeof(uint16_t));
+            uint32_t oi = ph.op_first;
+            for (uint32_t e = 0; e < ph.total_elems; e += kChunkElems) {
+                while (oi + 1 < ph.op_first + ph.op_count && n.ops[oi + 1].elem_begin <= e) ++oi;
+                chunks.push_back((uint16_t)oi);
+            }
+        }
+        const size_t total = (chunk_base + chunks.size() * sizeof(uint16_t) + 15) & ~size_t(15);
         r.blob_bytes = (uint32_t)total;
         const size_t base = plan->dblobs.size();
         plan->dblobs.resize(base + total, 0);
         uint8_t* dst = plan->dblobs.data() + base;
-        std::memcpy(dst, n.phases.data(), ph_bytes);     // op_first already network-local
+        std::memcpy(dst, phases.data(), ph_bytes);     // op_first already network-local
         std::memcpy(dst + ph_bytes, n.ops.data(), op_bytes);   // in_begin network-local
         std::memcpy(dst + ph_bytes + op_bytes, n.ins.data(), in_bytes);
+        if (!chunks.empty())
+            std::memcpy(dst + chunk_base, chunks.data(), chunks.size() * sizeof(uint16_t));
         plan->druns.push_back(r);
     }
 }

@@ -42,12 +42,15 @@ struct DevIn {
 constexpr int kMaxRuns = 4;
 constexpr uint64_t kRunsFallback = 7;
 
-// Ops of one dependency level; a barrier follows every phase.
+// Ops of one dependency level; a barrier follows every phase.  In a network
+// blob, chunk_off is the byte offset of the phase's chunk table: for every
+// 32 flattened elements, the (network-local) index of the op holding the
+// chunk's first element.
 struct DevPhase {
     uint32_t op_first;
     uint32_t op_count;
     uint32_t total_elems;
-    uint32_t pad;
+    uint32_t chunk_off;
 };
 
 // One network (edge term).
@@ -64,8 +67,8 @@ struct DevNet {
 
 // One network as the executor reads it: its phases, ops and operands are
 // one contiguous 16-byte-aligned blob [DevPhase x n_phases][DevOp x n_ops]
-// [DevIn x n_ins, padded to 16 bytes] with network-local indices, staged
-// into shared memory by one bulk copy.
+// [DevIn x n_ins][uint16 chunk tables of all phases, padded to 16 bytes]
+// with network-local indices, staged into shared memory by one bulk copy.
 struct DevNetRun {
     uint32_t blob_off16;   // blob offset in 16-byte units
     uint32_t blob_bytes;   // multiple of 16
@@ -74,7 +77,7 @@ struct DevNetRun {
     uint32_t arena_elems;
     uint32_t result_src;
     uint32_t max_elems;
-    uint32_t pad;
+    uint32_t tail_start;   // phases from here on have <= 32 elements each
 };
 
 // Gate-table entry: the tensor of a gate, sliced and transposed into the
@@ -101,6 +104,7 @@ static_assert(sizeof(DevIn) == 16, "DevIn layout");
 static_assert(sizeof(DevPhase) == 16, "DevPhase layout");
 static_assert(sizeof(DevNet) == 32, "DevNet layout");
 static_assert(sizeof(DevNetRun) == 32, "DevNetRun layout");
+constexpr uint32_t kChunkElems = 32;
 static_assert(sizeof(DevEntry) == 24, "DevEntry layout");
 static_assert(sizeof(DevTerm) == 16, "DevTerm layout");
 

@@ -179,8 +179,10 @@ struct RunArgs {
     uint32_t arena_capacity;      // elements per CTA
     uint32_t blob_capacity;       // bytes per CTA
     int* status;
-    unsigned int* done;           // CTAs finished in this run (reset by the last one)
-    uint32_t total_jobs;          // CTAs of the run over all its launches
+    unsigned int* done;           // networks finished in this run (reset by the last one)
+    unsigned int* queue;          // next job of a persistent launch (zeroed before it)
+    uint32_t n_jobs;              // jobs of this launch
+    uint32_t total_jobs;          // networks of the run over all its launches
     const float2* terms;          // the run's edge terms, [total_jobs]
     double* energy;               // MaxCut energy of the run, or null
 };
@@ -188,6 +190,7 @@ struct RunArgs {
 constexpr int kStatusArena = 1;        // network arena larger than the launch's capacity
 constexpr int kStatusStageTimeout = 2; // a staging copy did not complete in time
 constexpr int kStatusBlob = 4;         // network blob larger than the launch's capacity
+constexpr int kStatusQueue = 8;        // persistent launch without a job queue
 constexpr uint32_t kStageSpinLimit = 1u << 26;
 constexpr uint32_t kSmemTableLimitElems = 2048;   // 16 KB of gate table per CTA
 
@@ -202,17 +205,20 @@ __device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t b
         : "memory");
 }
 
-// Bulk (TMA) copies global -> shared completing on one mbarrier; every
-// thread waits with a bounded spin.  Returns false (status word set) if the
-// copies did not land.
-__device__ bool stage(void* dst0, const void* src0, uint32_t bytes0, void* dst1, const void* src1,
-                      uint32_t bytes1, uint64_t* bar, int* status) {
-    const uint32_t bar_a = smem_addr(bar);
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+}
+
+// Bulk (TMA) copies global -> shared completing on the mbarrier's current
+// phase (`parity`); every thread waits with a bounded spin.  Returns false
+// (status word set) if the copies did not land.
+__device__ bool stage(void* dst0, const void* src0, uint32_t bytes0, void* dst1, const void* src1,
+                      uint32_t bytes1, uint64_t* bar, uint32_t parity, int* status) {
+    const uint32_t bar_a = smem_addr(bar);
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a),
                      "r"(bytes0 + bytes1)
@@ -223,8 +229,8 @@ __device__ bool stage(void* dst0, const void* src0, uint32_t bytes0, void* dst1,
     uint32_t done = 0;
     for (uint32_t it = 0; it < kStageSpinLimit; ++it) {
         asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
-            " selp.u32 %0, 1, 0, p;\n}" : "=r"(done) : "r"(bar_a) : "memory");
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}" : "=r"(done) : "r"(bar_a), "r"(parity) : "memory");
         if (done) break;
         if (it > 64) __nanosleep(32);
     }
@@ -266,14 +272,141 @@ __device__ void reduce_energy(const float2* terms, uint32_t n, double* energy) {
     }
 }
 
-// One CTA contracts one network.  Shared memory, in order: mbarrier (16 B),
-// [plan-wide gate entries + angle terms], the network's plan blob, [gate
-// table], [arena]; the bracketed parts exist when kSmemTable / kSmemArena.
-// Phases run in order with a barrier after each; inside a phase the
-// elements of all its ops are spread over the threads.
-template <bool kSmemArena, bool kSmemTable>
-__global__ void __launch_bounds__(1024) qtb_network_kernel(const Job* __restrict__ jobs,
-                                                           const RunArgs a) {
+// One output element j of op: the product of its operands gathered at j
+// (and at j with the summed bit set), summed over the bucket variable.
+// Operands are handled in groups of four so their descriptor and value
+// loads issue together instead of as one dependent chain per operand.
+template <bool kSmemTable>
+__device__ __forceinline__ void compute_element(const DevOp& op, uint32_t j, const DevIn* ins,
+                                                const float2* __restrict__ table,
+                                                float2* __restrict__ arena) {
+    const uint32_t w = op.u - op.sum;
+    const uint32_t low = (1u << w) - 1u;
+    const DevIn* in = ins + op.in_begin;
+    float2 p0 = make_float2(1.f, 0.f), p1 = make_float2(1.f, 0.f);
+    for (uint32_t t0 = 0; t0 < op.k; t0 += 4) {
+        DevIn d[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+            if (t0 + t < op.k) d[t] = in[t0 + t];
+        float2 x0[4], x1[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            if (t0 + t < op.k) {
+                const uint32_t off = gather_bits(j, d[t], low);
+                const bool tab = d[t].src & kSrcTable;
+                const float2* base = tab ? table + (d[t].src & ~kSrcTable) : arena + d[t].src;
+                x0[t] = (tab && !kSmemTable) ? __ldg(base + off) : base[off];
+                x1[t] = x0[t];
+                // the summed variable is union bit w and, in an operand that
+                // has it, that operand's most significant axis: a fixed stride
+                if (op.sum && ((d[t].mask >> w) & 1u)) {
+                    const uint32_t stride = 1u << (__popc(d[t].mask) - 1);
+                    x1[t] = (tab && !kSmemTable) ? __ldg(base + off + stride) : base[off + stride];
+                }
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            if (t0 + t < op.k) {
+                p0 = (t0 + t == 0) ? x0[t] : cmul(p0, x0[t]);
+                p1 = (t0 + t == 0) ? x1[t] : cmul(p1, x1[t]);
+            }
+        }
+    }
+    arena[op.dst + j] = op.sum ? make_float2(p0.x + p1.x, p0.y + p1.y) : p0;
+}
+
+// Gate table for the run's angles into shared memory: one thread per table
+// element; the element's entry is found by binary search over the entries'
+// offsets, the gate tensor evaluated in fp64 and rounded to complex64.
+__device__ void build_table(const unsigned char* common, const RunArgs& a, float2* stable) {
+    const DevEntry* entries = reinterpret_cast<const DevEntry*>(common);
+    const DevTerm* terms = reinterpret_cast<const DevTerm*>(common + a.terms_off);
+    for (uint32_t i = threadIdx.x; i < a.table_elems; i += blockDim.x) {
+        uint32_t lo = 0, hi = a.n_entries - 1u;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1u) >> 1;
+            if (entries[mid].off <= i) lo = mid;
+            else hi = mid - 1u;
+        }
+        const DevEntry en = entries[lo];
+        double alpha = 0.0;
+        for (int t = 0; t < en.expr_count; ++t)
+            alpha += terms[en.expr_begin + t].coef * __ldg(a.params + terms[en.expr_begin + t].param);
+        const int o = (int)(i - en.off);
+        uint32_t ixb = 0;
+        for (int ax = 0; ax < en.rank_out; ++ax)
+            ixb |= (uint32_t)((o >> (en.rank_out - 1 - ax)) & 1) << en.perm[ax];
+        const double2 v = gate_value(en.kind, alpha, ixb);
+        stable[i] = make_float2((float)v.x, (float)v.y);
+    }
+    __syncthreads();
+}
+
+// The phases of one staged network; its scalar result is returned to thread 0.
+template <bool kSmemTable>
+__device__ float2 contract_network(const DevNetRun& net, const unsigned char* blob,
+                                   const float2* __restrict__ table, float2* __restrict__ arena) {
+    const DevPhase* phases = reinterpret_cast<const DevPhase*>(blob);
+    const DevOp* ops = reinterpret_cast<const DevOp*>(blob + net.n_phases * sizeof(DevPhase));
+    const DevIn* ins = reinterpret_cast<const DevIn*>(blob + net.ins_off);
+    // phases with more than 32 elements: all threads, a block barrier each
+    for (uint32_t p = 0; p < net.tail_start; ++p) {
+        const DevPhase ph = phases[p];
+        const uint16_t* chunk = reinterpret_cast<const uint16_t*>(blob + ph.chunk_off);
+        uint32_t oi = ph.op_first;
+        DevOp op = ops[oi];
+        uint32_t op_end = op.elem_begin + (1u << (op.u - op.sum));
+        for (uint32_t g = threadIdx.x; g < ph.total_elems; g += blockDim.x) {
+            if (g >= op_end) {
+                // the chunk table names the op of g's 32-element chunk; small
+                // ops may share a chunk, so step forward to the one holding g
+                oi = chunk[g / kChunkElems];
+                op = ops[oi];
+                op_end = op.elem_begin + (1u << (op.u - op.sum));
+                while (g >= op_end) {
+                    op = ops[++oi];
+                    op_end = op.elem_begin + (1u << (op.u - op.sum));
+                }
+            }
+            compute_element<kSmemTable>(op, g - op.elem_begin, ins, table, arena);
+        }
+        __syncthreads();
+    }
+    // the tail (every phase <= 32 elements): warp 0 alone, warp barriers
+    if (threadIdx.x < 32) {
+        for (uint32_t p = net.tail_start; p < net.n_phases; ++p) {
+            const DevPhase ph = phases[p];
+            const uint32_t g = threadIdx.x;
+            if (g < ph.total_elems) {
+                uint32_t oi = ph.op_first;
+                DevOp op = ops[oi];
+                while (g >= op.elem_begin + (1u << (op.u - op.sum))) op = ops[++oi];
+                compute_element<kSmemTable>(op, g - op.elem_begin, ins, table, arena);
+            }
+            __syncwarp();
+        }
+    }
+    float2 result = make_float2(0.f, 0.f);
+    if (threadIdx.x == 0)
+        result = (net.result_src & kSrcTable) ? table[net.result_src & ~kSrcTable] : arena[net.result_src];
+    return result;
+}
+
+// Network executor.  Shared memory, in order: mbarrier (16 B), [plan-wide
+// gate entries + angle terms], the network's plan blob, [gate table],
+// [arena]; the bracketed parts exist when kSmemTable / kSmemArena.
+//   class launch (kPersistent = false): CTA b contracts jobs[b];
+//   persistent launch: every CTA builds the gate table once, then takes
+//   networks from the run's queue (jobs in descending width) until it is
+//   empty.
+// After each network thread 0 writes its term; with a.energy set, the CTA
+// that finishes the run's last network sums Re(terms) in fp64 and writes
+// the energy.
+template <bool kSmemArena, bool kSmemTable, bool kPersistent>
+__global__ void __launch_bounds__(kPersistent ? 512 : 1024) qtb_network_kernel(
+    const Job* __restrict__ jobs, const RunArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
     unsigned char* common = smem + 16;
@@ -281,110 +414,57 @@ __global__ void __launch_bounds__(1024) qtb_network_kernel(const Job* __restrict
     float2* stable = reinterpret_cast<float2*>(blob + a.blob_capacity);
     unsigned char* after_table =
         blob + a.blob_capacity + (kSmemTable ? ((a.table_elems * 8u + 15u) & ~15u) : 0u);
-    const Job job = jobs[blockIdx.x];
-    const DevNetRun net = *job.net;
-    if (net.arena_elems > a.arena_capacity || net.blob_bytes > a.blob_capacity) {
-        if (threadIdx.x == 0)
-            atomicOr(a.status, net.arena_elems > a.arena_capacity ? kStatusArena : kStatusBlob);
-        return;
-    }
-    if (!stage(blob, a.blobs + net.blob_off16, net.blob_bytes, common, a.common,
-               kSmemTable ? a.common_bytes : 0u, bar, a.status))
-        return;
-    const float2* __restrict__ table = a.gtable;
-    if (kSmemTable) {
-        // one thread per table element: find its entry (entries are laid out
-        // in increasing offset), evaluate the gate tensor there
-        const DevEntry* entries = reinterpret_cast<const DevEntry*>(common);
-        const DevTerm* terms = reinterpret_cast<const DevTerm*>(common + a.terms_off);
-        for (uint32_t i = threadIdx.x; i < a.table_elems; i += blockDim.x) {
-            uint32_t lo = 0, hi = a.n_entries - 1u;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi + 1u) >> 1;
-                if (entries[mid].off <= i) lo = mid;
-                else hi = mid - 1u;
-            }
-            const DevEntry en = entries[lo];
-            double alpha = 0.0;
-            for (int t = 0; t < en.expr_count; ++t)
-                alpha += terms[en.expr_begin + t].coef * __ldg(a.params + terms[en.expr_begin + t].param);
-            const int o = (int)(i - en.off);
-            uint32_t ixb = 0;
-            for (int ax = 0; ax < en.rank_out; ++ax)
-                ixb |= (uint32_t)((o >> (en.rank_out - 1 - ax)) & 1) << en.perm[ax];
-            const double2 v = gate_value(en.kind, alpha, ixb);
-            stable[i] = make_float2((float)v.x, (float)v.y);
-        }
-        __syncthreads();
-        table = stable;
-    }
     float2* arena = kSmemArena ? reinterpret_cast<float2*>(after_table)
                                : a.gscratch + (size_t)blockIdx.x * a.arena_capacity;
-    const DevPhase* phases = reinterpret_cast<const DevPhase*>(blob);
-    const DevOp* ops = reinterpret_cast<const DevOp*>(blob + net.n_phases * sizeof(DevPhase));
-    const DevIn* ins = reinterpret_cast<const DevIn*>(blob + net.ins_off);
-
-    for (uint32_t p = 0; p < net.n_phases; ++p) {
-        const DevPhase ph = phases[p];
-        const uint32_t last = ph.op_first + ph.op_count - 1u;
-        uint32_t oi = ph.op_first;
-        DevOp op = ops[oi];
-        uint32_t w = op.u - op.sum;
-        uint32_t op_end = op.elem_begin + (1u << w);
-        for (uint32_t g = threadIdx.x; g < ph.total_elems; g += blockDim.x) {
-            if (g >= op_end) {
-                // binary search: the last op of the phase starting at or before g
-                uint32_t lo = oi + 1u, hi = last;
-                while (lo < hi) {
-                    const uint32_t mid = (lo + hi + 1u) >> 1;
-                    if (ops[mid].elem_begin <= g) lo = mid;
-                    else hi = mid - 1u;
-                }
-                oi = lo;
-                op = ops[oi];
-                w = op.u - op.sum;
-                op_end = op.elem_begin + (1u << w);
-            }
-            const uint32_t j = g - op.elem_begin;
-            const DevIn* in = ins + op.in_begin;
-            // the summed variable is union bit w and, in an operand that has
-            // it, that operand's most significant axis: a fixed stride
-            float2 p0 = make_float2(1.f, 0.f), p1 = make_float2(1.f, 0.f);
-            for (uint32_t t = 0; t < op.k; ++t) {
-                const DevIn d = in[t];
-                const uint32_t off = gather_bits(j, d, (1u << w) - 1u);
-                const bool tab = d.src & kSrcTable;
-                const float2* base = tab ? table + (d.src & ~kSrcTable) : arena + d.src;
-                const float2 x0 = (tab && !kSmemTable) ? __ldg(base + off) : base[off];
-                p0 = t == 0 ? x0 : cmul(p0, x0);
-                if (op.sum) {
-                    float2 x1 = x0;
-                    if ((d.mask >> w) & 1u) {
-                        const uint32_t stride = 1u << (__popc(d.mask) - 1);
-                        x1 = (tab && !kSmemTable) ? __ldg(base + off + stride) : base[off + stride];
-                    }
-                    p1 = t == 0 ? x1 : cmul(p1, x1);
-                }
-            }
-            arena[op.dst + j] = op.sum ? make_float2(p0.x + p1.x, p0.y + p1.y) : p0;
-        }
-        __syncthreads();
+    __shared__ unsigned int s_job, is_last;
+    if (kPersistent && a.queue == nullptr) {   // a persistent launch needs its queue
+        if (threadIdx.x == 0) atomicOr(a.status, kStatusQueue);
+        return;
     }
-    __shared__ unsigned int is_last;
-    if (threadIdx.x == 0) {
-        *job.term = (net.result_src & kSrcTable) ? table[net.result_src & ~kSrcTable]
-                                                 : arena[net.result_src];
-        if (a.energy) {
+    mbar_init(bar);
+    uint32_t parity = 0;
+    const float2* __restrict__ table = kSmemTable ? stable : a.gtable;
+    bool table_ready = !kSmemTable;
+    for (uint32_t iter = 0;; ++iter) {
+        if (kPersistent) {
+            if (threadIdx.x == 0) s_job = atomicAdd(a.queue, 1u);
+            __syncthreads();
+            if (s_job >= a.n_jobs) break;
+        } else if (iter > 0) {
+            break;
+        }
+        const Job job = jobs[kPersistent ? s_job : blockIdx.x];
+        const DevNetRun net = *job.net;
+        if (net.arena_elems > a.arena_capacity || net.blob_bytes > a.blob_capacity) {
+            if (threadIdx.x == 0)
+                atomicOr(a.status, net.arena_elems > a.arena_capacity ? kStatusArena : kStatusBlob);
+            return;
+        }
+        // the first staging of a CTA also brings the plan-wide gate entries
+        const bool with_common = kSmemTable && !table_ready;
+        if (!stage(blob, a.blobs + net.blob_off16, net.blob_bytes, common, a.common,
+                   with_common ? a.common_bytes : 0u, bar, parity, a.status))
+            return;
+        parity ^= 1u;
+        if (!table_ready) {
+            build_table(common, a, stable);
+            table_ready = true;
+        }
+        const float2 term = contract_network<kSmemTable>(net, blob, table, arena);
+        if (threadIdx.x == 0) {
+            *job.term = term;
+            if (a.energy) {
+                __threadfence();
+                is_last = atomicAdd(a.done, 1u) == a.total_jobs - 1u;
+            }
+        }
+        __syncthreads();   // blob and arena are reused by the next network
+        if (a.energy && is_last) {
             __threadfence();
-            is_last = atomicAdd(a.done, 1u) == a.total_jobs - 1u;
+            reduce_energy(a.terms, a.total_jobs, a.energy);
+            if (threadIdx.x == 0) *a.done = 0u;   // ready for the next run
+            __syncthreads();
         }
-    }
-    if (!a.energy) return;
-    __syncthreads();
-    if (is_last) {
-        __threadfence();
-        reduce_energy(a.terms, a.total_jobs, a.energy);
-        if (threadIdx.x == 0) *a.done = 0u;   // ready for the next run
     }
 }
 
@@ -411,6 +491,8 @@ constexpr int kMaxClasses = kSmemClasses + 1;   // + the global-arena class
 
 struct LaunchClass {
     bool smem;
+    bool persistent;        // CTAs take networks from the run's queue
+    int grid;               // CTAs (= n_jobs unless persistent)
     uint32_t capacity;      // arena elements per CTA
     uint32_t blob_capacity; // plan-blob bytes per CTA
     int threads;
@@ -440,10 +522,13 @@ static CommonImage common_image(const qtb_plan* plan) {
 }
 
 struct RunCache {
-    Job* jobs = nullptr;                // jobs of all classes, then the done counter
+    Job* jobs = nullptr;                // class-mode jobs, persistent-mode jobs, counters
     unsigned int* done = nullptr;
-    bool tuned = false;                 // block sizes chosen by the autotuner
-    std::vector<LaunchClass> classes;   // widest first
+    unsigned int* queue = nullptr;
+    bool tuned = false;                 // schedule and block sizes chosen by the autotuner
+    bool persistent = false;            // the schedule in use
+    std::vector<LaunchClass> classes;   // class schedule, widest first
+    std::vector<LaunchClass> pclasses;  // persistent schedule (+ global-arena class)
     size_t scratch_elems = 0;
     bool smem_table = true;
 };
@@ -488,19 +573,60 @@ static void free_device(qtb_plan* plan) {
 }
 
 // Kernel instantiation for a launch class.
+template <bool kA, bool kT>
+static void launch_one(const LaunchClass& lc, const Job* jobs, const RunArgs& a, cudaStream_t st) {
+    if (lc.persistent)
+        qtb_network_kernel<kA, kT, true><<<lc.grid, lc.threads, lc.smem_bytes, st>>>(jobs, a);
+    else
+        qtb_network_kernel<kA, kT, false><<<lc.grid, lc.threads, lc.smem_bytes, st>>>(jobs, a);
+}
+
 static void launch_class(const LaunchClass& lc, bool smem_table, const Job* jobs, const RunArgs& a,
                          cudaStream_t st) {
     if (lc.smem) {
-        if (smem_table)
-            qtb_network_kernel<true, true><<<lc.n_jobs, lc.threads, lc.smem_bytes, st>>>(jobs, a);
-        else
-            qtb_network_kernel<true, false><<<lc.n_jobs, lc.threads, lc.smem_bytes, st>>>(jobs, a);
+        if (smem_table) launch_one<true, true>(lc, jobs, a, st);
+        else launch_one<true, false>(lc, jobs, a, st);
     } else {
-        if (smem_table)
-            qtb_network_kernel<false, true><<<lc.n_jobs, lc.threads, lc.smem_bytes, st>>>(jobs, a);
-        else
-            qtb_network_kernel<false, false><<<lc.n_jobs, lc.threads, lc.smem_bytes, st>>>(jobs, a);
+        if (smem_table) launch_one<false, true>(lc, jobs, a, st);
+        else launch_one<false, false>(lc, jobs, a, st);
     }
+}
+
+template <bool kA, bool kT, bool kP>
+static cudaError_t allow_smem() {
+    return cudaFuncSetAttribute(qtb_network_kernel<kA, kT, kP>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimitBytes);
+}
+
+static int allow_all_smem() {
+    QTB_CUDA((allow_smem<true, true, false>()));
+    QTB_CUDA((allow_smem<true, false, false>()));
+    QTB_CUDA((allow_smem<false, true, false>()));
+    QTB_CUDA((allow_smem<false, false, false>()));
+    QTB_CUDA((allow_smem<true, true, true>()));
+    QTB_CUDA((allow_smem<true, false, true>()));
+    QTB_CUDA((allow_smem<false, true, true>()));
+    QTB_CUDA((allow_smem<false, false, true>()));
+    return QTB_OK;
+}
+
+// Resident CTAs of a persistent launch class on the whole GPU.
+static int persistent_grid(const LaunchClass& lc, bool smem_table, int* grid) {
+    int per_sm = 0, sms = 0, dev = 0;
+    QTB_CUDA(cudaGetDevice(&dev));
+    QTB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (lc.smem) {
+        if (smem_table)
+            QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, qtb_network_kernel<true, true, true>, lc.threads, lc.smem_bytes));
+        else
+            QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, qtb_network_kernel<true, false, true>, lc.threads, lc.smem_bytes));
+    } else {
+        per_sm = 1;
+    }
+    *grid = std::max(1, std::min(lc.n_jobs, std::max(1, per_sm) * sms));
+    return QTB_OK;
 }
 
 static void destroy_streams(qtb_plan_device* s) {
@@ -535,6 +661,15 @@ static int threads_for(uint32_t max_elems) {
     if (max_elems <= 4096) return 256;
     if (max_elems <= 16384) return 512;
     return 1024;
+}
+
+// Default block size of a launch class (the autotuner may replace it):
+// classes too small to fill the GPU trade occupancy for per-network latency.
+static int class_threads(uint32_t max_elems, int n_jobs) {
+    const int t = threads_for(max_elems);
+    if (n_jobs <= 148) return std::max(t, max_elems >= 512 ? 1024 : 512);
+    if (n_jobs <= 4 * 148) return std::max(t, 256);
+    return t;
 }
 
 // Launch classes of a run: networks bucketed by the shared memory they need
@@ -596,16 +731,15 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
     }
     std::vector<Job> jobs;
     const auto* runs = static_cast<const DevNetRun*>(plan->dev.runs);
-    rc->classes.clear();
-    rc->scratch_elems = 0;
-    for (int c = kMaxClasses - 1; c >= 0; --c) {
-        if (members[c].empty()) continue;
+    auto make_class = [&](const std::vector<int32_t>& m, bool smem, bool persistent) {
         LaunchClass lc{};
-        lc.smem = c < kSmemClasses;
+        lc.smem = smem;
+        lc.persistent = persistent;
         lc.job_offset = jobs.size();
-        lc.n_jobs = (int)members[c].size();
+        lc.n_jobs = (int)m.size();
+        lc.grid = lc.n_jobs;
         uint32_t cap = 4, blob = 16, maxe = 1;
-        for (int32_t i : members[c]) {
+        for (int32_t i : m) {
             cap = std::max(cap, plan->druns[i].arena_elems);
             blob = std::max(blob, plan->druns[i].blob_bytes);
             maxe = std::max(maxe, plan->druns[i].max_elems);
@@ -616,15 +750,47 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
         }
         lc.capacity = (cap + 3u) & ~3u;
         lc.blob_capacity = blob;
-        lc.threads = threads_for(maxe);
-        lc.smem_bytes = fixed + (size_t)blob + (lc.smem ? 8 * (size_t)lc.capacity : 0);
+        lc.threads = persistent ? 256 : class_threads(maxe, lc.n_jobs);
+        lc.smem_bytes = fixed + (size_t)blob + (smem ? 8 * (size_t)lc.capacity : 0);
+        return lc;
+    };
+    rc->classes.clear();
+    rc->pclasses.clear();
+    rc->scratch_elems = 0;
+    // class schedule
+    for (int c = kMaxClasses - 1; c >= 0; --c) {
+        if (members[c].empty()) continue;
+        LaunchClass lc = make_class(members[c], c < kSmemClasses, false);
         if (!lc.smem) {
             lc.scratch_offset = rc->scratch_elems;
             rc->scratch_elems += (size_t)lc.capacity * lc.n_jobs;
         }
         rc->classes.push_back(lc);
     }
-    // jobs, then one 16-byte slot for the done counter (zeroed)
+    // persistent schedule: every shared-memory network in one queue, widest
+    // (largest arena, then most phases) first; the global-arena class as is
+    {
+        std::vector<int32_t> all;
+        for (int c = 0; c < kSmemClasses; ++c) all.insert(all.end(), members[c].begin(), members[c].end());
+        std::stable_sort(all.begin(), all.end(), [&](int32_t x, int32_t y) {
+            const DevNetRun& rx = plan->druns[x];
+            const DevNetRun& ry = plan->druns[y];
+            return rx.arena_elems != ry.arena_elems ? rx.arena_elems > ry.arena_elems
+                                                    : rx.n_phases > ry.n_phases;
+        });
+        if (!members[kSmemClasses].empty()) {
+            for (const LaunchClass& lc : rc->classes)
+                if (!lc.smem) rc->pclasses.push_back(lc);   // same jobs, same scratch
+        }
+        if (!all.empty()) {
+            LaunchClass lc = make_class(all, true, true);
+            if (fixed + lc.blob_capacity + 8 * (size_t)lc.capacity <= kSmemLimitBytes)
+                rc->pclasses.insert(rc->pclasses.begin(), lc);
+            else
+                rc->pclasses.clear();   // no single shared-memory size fits all: class schedule only
+        }
+    }
+    // jobs of both schedules, then 16 bytes of counters (done, queue), zeroed
     const size_t job_bytes = jobs.size() * sizeof(Job);
     void* buf = nullptr;
     QTB_CUDA(cudaMalloc(&buf, job_bytes + 16));
@@ -632,6 +798,12 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
     QTB_CUDA(cudaMemset(static_cast<char*>(buf) + job_bytes, 0, 16));
     rc->jobs = static_cast<Job*>(buf);
     rc->done = reinterpret_cast<unsigned int*>(static_cast<char*>(buf) + job_bytes);
+    rc->queue = rc->done + 1;
+    for (LaunchClass& lc : rc->pclasses)
+        if (lc.persistent) {
+            int r = persistent_grid(lc, rc->smem_table, &lc.grid);
+            if (r) return r;
+        }
     return QTB_OK;
 }
 
@@ -648,14 +820,8 @@ int qtb_init(int device) {
     QTB_CUDA(cudaGetDeviceCount(&n));
     if (device < 0 || device >= n) return fail(QTB_ERR_ARG, "qtb_init: no such device");
     QTB_CUDA(cudaSetDevice(device));
-    QTB_CUDA(cudaFuncSetAttribute(qtb_network_kernel<true, true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimitBytes));
-    QTB_CUDA(cudaFuncSetAttribute(qtb_network_kernel<false, true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimitBytes));
-    QTB_CUDA(cudaFuncSetAttribute(qtb_network_kernel<true, false>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimitBytes));
-    QTB_CUDA(cudaFuncSetAttribute(qtb_network_kernel<false, false>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimitBytes));
+    int r = allow_all_smem();
+    if (r) return r;
     return QTB_OK;
 }
 
@@ -748,10 +914,47 @@ int qtb_plan_scratch_bytes(const qtb_plan* plan_c, int32_t first, int32_t count,
     return QTB_OK;
 }
 
-// Block-size autotuner: on the first run of a range, every launch class is
-// timed alone (energy reduction off) with each candidate block size; the
-// fastest of three timed launches per candidate is kept.
-static int autotune_run(RunCache* rc, const RunArgs& base, void* scratch_dev, cudaStream_t st) {
+static int ensure_streams(qtb_plan_device* s);
+
+// Launch a schedule on st: a persistent class needs its queue zeroed first
+// (a memset node when captured); several classes run concurrently on
+// forked streams joined back into st.
+static int launch_schedule(qtb_plan_device* s, const RunCache* rc,
+                           const std::vector<LaunchClass>& sched, const RunArgs& base,
+                           void* scratch_dev, cudaStream_t st) {
+    int r = ensure_streams(s);
+    if (r) return r;
+    for (const LaunchClass& lc : sched)
+        if (lc.persistent) QTB_CUDA(cudaMemsetAsync(rc->queue, 0, sizeof(unsigned int), st));
+    const bool forked = sched.size() > 1;
+    if (forked) QTB_CUDA(cudaEventRecord(s->fork, st));
+    for (size_t c = 0; c < sched.size(); ++c) {
+        const LaunchClass& lc = sched[c];
+        cudaStream_t cs = forked ? s->aux[c] : st;
+        if (forked) QTB_CUDA(cudaStreamWaitEvent(cs, s->fork, 0));
+        RunArgs ac = base;
+        ac.queue = rc->queue;
+        ac.arena_capacity = lc.capacity;
+        ac.blob_capacity = lc.blob_capacity;
+        ac.n_jobs = (uint32_t)lc.n_jobs;
+        ac.gscratch = lc.smem ? nullptr : static_cast<float2*>(scratch_dev) + lc.scratch_offset;
+        launch_class(lc, rc->smem_table, rc->jobs + lc.job_offset, ac, cs);
+        QTB_CUDA(cudaGetLastError());
+        if (forked) {
+            QTB_CUDA(cudaEventRecord(s->join[c], cs));
+            QTB_CUDA(cudaStreamWaitEvent(st, s->join[c], 0));
+        }
+    }
+    return QTB_OK;
+}
+
+// Autotuner, on the first run of a range (energy reduction off while it
+// times): each class of the class schedule is timed alone with 64..1024
+// threads per CTA; then the whole class schedule and the persistent
+// schedule (128/256/512 threads) are timed end to end and the faster
+// schedule is kept.  Each measurement is the fastest of three launches.
+static int autotune_run(qtb_plan_device* s, RunCache* rc, const RunArgs& base, void* scratch_dev,
+                        cudaStream_t st) {
     static const int kCandidates[] = {64, 128, 256, 512, 1024};
     cudaEvent_t e0, e1;
     QTB_CUDA(cudaEventCreate(&e0));
@@ -759,38 +962,76 @@ static int autotune_run(RunCache* rc, const RunArgs& base, void* scratch_dev, cu
     RunArgs a = base;
     a.energy = nullptr;
     const bool log = std::getenv("QTB_AUTOTUNE_LOG") != nullptr;
+    auto time_it = [&](auto&& launch, float* best) -> int {
+        int r = launch();   // warm-up
+        if (r) return r;
+        for (int rep = 0; rep < 3; ++rep) {
+            QTB_CUDA(cudaEventRecord(e0, st));
+            if ((r = launch())) return r;
+            QTB_CUDA(cudaEventRecord(e1, st));
+            QTB_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            QTB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            *best = std::min(*best, ms);
+        }
+        return QTB_OK;
+    };
+    int r;
     for (LaunchClass& lc : rc->classes) {
-        a.arena_capacity = lc.capacity;
-        a.blob_capacity = lc.blob_capacity;
-        a.gscratch = lc.smem ? nullptr : static_cast<float2*>(scratch_dev) + lc.scratch_offset;
         int best_t = lc.threads;
         float best_ms = 1e30f;
         for (int t : kCandidates) {
-            LaunchClass trial = lc;
-            trial.threads = t;
-            launch_class(trial, rc->smem_table, rc->jobs + lc.job_offset, a, st);   // warm-up
-            for (int rep = 0; rep < 3; ++rep) {
-                QTB_CUDA(cudaEventRecord(e0, st));
-                launch_class(trial, rc->smem_table, rc->jobs + lc.job_offset, a, st);
-                QTB_CUDA(cudaEventRecord(e1, st));
-                QTB_CUDA(cudaEventSynchronize(e1));
-                float ms = 0.f;
-                QTB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-                if (ms < best_ms) {
-                    best_ms = ms;
+            std::vector<LaunchClass> one(1, lc);
+            one[0].threads = t;
+            float ms = 1e30f;
+            if ((r = time_it([&] { return launch_schedule(s, rc, one, a, scratch_dev, st); }, &ms))) return r;
+            if (log)
+                std::fprintf(stderr, "qtb autotune: class of %d networks (smem %zu B) %4d threads %.1f us\n",
+                             lc.n_jobs, lc.smem_bytes, t, 1e3 * ms);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_t = t;
+            }
+        }
+        lc.threads = best_t;
+        for (LaunchClass& pc : rc->pclasses)   // the global class is shared
+            if (!pc.persistent && pc.job_offset == lc.job_offset) pc.threads = best_t;
+    }
+    float class_ms = 1e30f;
+    if ((r = time_it([&] { return launch_schedule(s, rc, rc->classes, a, scratch_dev, st); }, &class_ms)))
+        return r;
+    float pers_ms = 1e30f;
+    if (!rc->pclasses.empty()) {
+        for (LaunchClass& pc : rc->pclasses) {
+            if (!pc.persistent) continue;
+            int best_t = pc.threads;
+            float best = 1e30f;
+            for (int t : {128, 256, 512}) {
+                std::vector<LaunchClass> sched = rc->pclasses;
+                for (LaunchClass& q : sched)
+                    if (q.persistent) {
+                        q.threads = t;
+                        if ((r = persistent_grid(q, rc->smem_table, &q.grid))) return r;
+                    }
+                float ms = 1e30f;
+                if ((r = time_it([&] { return launch_schedule(s, rc, sched, a, scratch_dev, st); }, &ms)))
+                    return r;
+                if (log)
+                    std::fprintf(stderr, "qtb autotune: persistent schedule %4d threads %.1f us\n", t, 1e3 * ms);
+                if (ms < best) {
+                    best = ms;
                     best_t = t;
                 }
-                if (log && rep == 2)
-                    std::fprintf(stderr, "qtb autotune: class of %d networks (smem %zu B) %4d threads %.1f us\n",
-                                 lc.n_jobs, lc.smem_bytes, t, 1e3 * ms);
             }
-            QTB_CUDA(cudaGetLastError());
+            pc.threads = best_t;
+            if ((r = persistent_grid(pc, rc->smem_table, &pc.grid))) return r;
+            pers_ms = best;
         }
-        if (log)
-            std::fprintf(stderr, "qtb autotune: class of %d networks -> %d threads (%.1f us)\n", lc.n_jobs,
-                         best_t, 1e3 * best_ms);
-        lc.threads = best_t;
     }
+    rc->persistent = pers_ms < class_ms;
+    if (log)
+        std::fprintf(stderr, "qtb autotune: class schedule %.1f us, persistent %.1f us -> %s\n",
+                     1e3 * class_ms, 1e3 * pers_ms, rc->persistent ? "persistent" : "classes");
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     rc->tuned = true;
@@ -844,12 +1085,14 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
             static_cast<float2*>(plan->dev.table));
         QTB_CUDA(cudaGetLastError());
     }
+    a.queue = rc->queue;
     if (s->autotune && !rc->tuned) {
         cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
         QTB_CUDA(cudaStreamIsCapturing(st, &cap));
-        if (cap == cudaStreamCaptureStatusNone && (r = autotune_run(rc, a, scratch_dev, st))) return r;
+        if (cap == cudaStreamCaptureStatusNone && (r = autotune_run(s, rc, a, scratch_dev, st))) return r;
     }
     s->last = rc;
+    const std::vector<LaunchClass>& sched = rc->persistent ? rc->pclasses : rc->classes;
     std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
     if (s->timing) {
         if (!s->spare.empty()) {
@@ -861,28 +1104,11 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
         }
         QTB_CUDA(cudaEventRecord(ev.first, st));
     }
-    // size classes run concurrently on forked streams, joined back into st
-    const bool forked = rc->classes.size() > 1;
-    if (forked) QTB_CUDA(cudaEventRecord(s->fork, st));
-    for (size_t c = 0; c < rc->classes.size(); ++c) {
-        const LaunchClass& lc = rc->classes[c];
-        cudaStream_t cs = forked ? s->aux[c] : st;
-        if (forked) QTB_CUDA(cudaStreamWaitEvent(cs, s->fork, 0));
-        RunArgs ac = a;
-        ac.arena_capacity = lc.capacity;
-        ac.blob_capacity = lc.blob_capacity;
-        ac.gscratch = lc.smem ? nullptr : static_cast<float2*>(scratch_dev) + lc.scratch_offset;
-        launch_class(lc, rc->smem_table, rc->jobs + lc.job_offset, ac, cs);
-        QTB_CUDA(cudaGetLastError());
-        if (forked) {
-            QTB_CUDA(cudaEventRecord(s->join[c], cs));
-            QTB_CUDA(cudaStreamWaitEvent(st, s->join[c], 0));
-        }
-    }
+    if ((r = launch_schedule(s, rc, sched, a, scratch_dev, st))) return r;
     if (s->timing) {
         QTB_CUDA(cudaEventRecord(ev.second, st));
         s->pending.push_back(ev);
-        s->kernel_launches += (int64_t)rc->classes.size();
+        s->kernel_launches += (int64_t)sched.size();
     }
     return QTB_OK;
 }
@@ -921,12 +1147,8 @@ static int noalloc_setup(int device, unsigned char** out) {
     if (!g_noalloc_addr[device]) {
         void* ptr = nullptr;
         QTB_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-        QTB_CUDA(cudaFuncSetAttribute(qtb_network_kernel<false, true>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kSmemLimitBytes));
-        QTB_CUDA(cudaFuncSetAttribute(qtb_network_kernel<false, false>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kSmemLimitBytes));
+        QTB_CUDA((allow_smem<false, true, false>()));
+        QTB_CUDA((allow_smem<false, false, false>()));
         g_noalloc_addr[device] = ptr;
     }
     *out = static_cast<unsigned char*>(g_noalloc_addr[device]);
@@ -1003,35 +1225,45 @@ int qtb_plan_run_noalloc(qtb_plan* plan, int32_t first, int32_t count, const dou
     a.blob_capacity = blob;
     a.status = static_cast<int*>(plan->dev.status);
     a.done = done;
+    a.queue = nullptr;
+    a.n_jobs = (uint32_t)count;
     a.total_jobs = (uint32_t)count;
     a.terms = static_cast<const float2*>(terms_dev);
     a.energy = energy_dev;
     const int threads = threads_for(maxe);
     if (smem_table)
-        qtb_network_kernel<false, true><<<count, threads, smem_bytes, st>>>(jobs, a);
+        qtb_network_kernel<false, true, false><<<count, threads, smem_bytes, st>>>(jobs, a);
     else
-        qtb_network_kernel<false, false><<<count, threads, smem_bytes, st>>>(jobs, a);
+        qtb_network_kernel<false, false, false><<<count, threads, smem_bytes, st>>>(jobs, a);
     QTB_CUDA(cudaGetLastError());
     return QTB_OK;
 }
 
 int qtb_plan_set_autotune(qtb_plan* plan, int32_t enable) {
     if (!plan) return fail(QTB_ERR_ARG, "plan_set_autotune: null plan");
-    dev_state(plan)->autotune = enable != 0;
+    // QTB_AUTOTUNE=0 in the environment keeps the default block sizes (e.g.
+    // under a profiler, whose serialised replays would mislead the timing)
+    const char* env = std::getenv("QTB_AUTOTUNE");
+    dev_state(plan)->autotune = enable != 0 && !(env && env[0] == '0');
     return QTB_OK;
 }
 
 int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32_t* n_classes) {
     if (!plan || !n_classes) return fail(QTB_ERR_ARG, "plan_last_launch_config: bad arguments");
     const RunCache* rc = dev_state(plan)->last;
-    *n_classes = rc ? (int32_t)rc->classes.size() : 0;
-    if (!rc || !out) return QTB_OK;
+    if (!rc) {
+        *n_classes = 0;
+        return QTB_OK;
+    }
+    const std::vector<LaunchClass>& sched = rc->persistent ? rc->pclasses : rc->classes;
+    *n_classes = (int32_t)sched.size();
+    if (!out) return QTB_OK;
     for (int32_t c = 0; c < *n_classes && 4 * c + 3 < cap; ++c) {
-        const LaunchClass& lc = rc->classes[c];
+        const LaunchClass& lc = sched[c];
         out[4 * c] = lc.n_jobs;
         out[4 * c + 1] = lc.threads;
         out[4 * c + 2] = (int32_t)lc.smem_bytes;
-        out[4 * c + 3] = lc.smem ? 1 : 0;
+        out[4 * c + 3] = (lc.smem ? 1 : 0) | (lc.persistent ? 2 : 0);
     }
     return QTB_OK;
 }

@@ -133,7 +133,8 @@ class NetworkPlan:
         check(self._lib.qtb_plan_set_autotune(self._h, 1 if enable else 0))
 
     def last_launch_config(self):
-        """[(networks, threads, smem bytes, smem arena?)] of the latest run."""
+        """[(networks, threads, smem bytes, flags)] of the latest run's
+        schedule; flags: 1 shared-memory arena, 2 persistent launch."""
         n = ctypes.c_int32()
         out = np.zeros(4 * 16, dtype=np.int32)
         check(self._lib.qtb_plan_last_launch_config(self._h, ptr(out), len(out), ctypes.byref(n)))

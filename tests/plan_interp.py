@@ -121,8 +121,21 @@ def run_network(exported, table, net_index):
         assert not np.isnan(v.real).any(), 'read of an arena element nobody wrote'
         return v
 
+    blob = exported['blobs'][int(net['blob_off16']) * 16:
+                             int(net['blob_off16']) * 16 + int(net['blob_bytes'])]
     for p in range(int(net['n_phases'])):
         ph = phases[p]
+        # the chunk table names the op holding the first element of every
+        # 32-element chunk of the phase
+        n_chunks = (int(ph['total_elems']) + 31) // 32
+        co = int(ph['chunk_off'])
+        assert co + 2 * n_chunks <= len(blob)
+        chunks = blob[co:co + 2 * n_chunks].view('<u2')
+        starts = ops['elem_begin']
+        for c, oi in enumerate(chunks):
+            assert int(ph['op_first']) <= oi < int(ph['op_first'] + ph['op_count'])
+            e = 32 * c
+            assert starts[oi] <= e < starts[oi] + (1 << int(ops[oi]['u'] - ops[oi]['sum']))
         writes = []
         elem = 0
         for o in range(int(ph['op_first']), int(ph['op_first'] + ph['op_count'])):
