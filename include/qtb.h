@@ -105,6 +105,8 @@ typedef struct {
     double alg_bytes;         /* sum over ops of 8*(sum_t 2^rank_t + 2^w) */
     double alg_flops;         /* sum over ops of 6*(k-1)*2^u + 2*2^w*sum */
     double ref_flops;         /* PerfBackend._perfect_bucket_flop summed */
+    int32_t n_slices;         /* networks of its circuit (2^sliced variables) */
+    int32_t group;            /* the circuit: networks of one circuit share it */
 } qtb_network_info;
 
 /* Create an empty plan for circuits with n_params angle parameters. */
@@ -134,11 +136,22 @@ int qtb_plan_add_lightcone(qtb_plan* plan, int32_t n_nodes, const int64_t* indpt
                            int32_t composer, const double* params, int32_t* net_index);
 
 /* Compile all edges of a graph with n_threads host threads (0 = all cores);
- * edges is 2*n_edges node ids.  Network i of the call is edge i.          */
+ * edges is 2*n_edges node ids.  Edge i of the call becomes the networks of
+ * group (the plan's group count before the call) + i, in edge order.     */
 int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indptr,
                             const int32_t* indices, const int32_t* edges, int32_t n_edges,
                             int32_t p, int32_t composer, const double* params,
                             int32_t n_threads, int32_t* first_net_index);
+
+/* Slicing of circuits added afterwards (qtensor/FeynmanSimulator.py:49-84,
+ * SlicesOptimizer qtensor/optimisation/Optimizer.py:90-159): when the
+ * greedy width reaches max_width, variables of highest degree are removed
+ * from the line graph (GreedyParvars, Greedy.py:78-91) until it drops
+ * below; the circuit then becomes 2^k networks, one per assignment of the
+ * k sliced variables, whose amplitudes sum to the circuit's.  Networks of a
+ * circuit are contiguous and share qtb_network_info.group; qtb_plan_run's
+ * energy counts groups, not networks.  0 (default) never slices.         */
+int qtb_plan_set_max_width(qtb_plan* plan, int32_t max_width);
 
 /* Elimination-order search for networks added afterwards: 0 (default) keeps
  * the reference's greedy rule (first node of least degree); trials > 0 also
@@ -175,9 +188,10 @@ int qtb_plan_upload(qtb_plan* plan);
 /* Contract networks [first, first+count) of an uploaded plan on stream:
  *   params_dev  device doubles (n_params) -- the angles of this request;
  *   terms_dev   device complex64 per network (the amplitude <0|U|0>);
- *   energy_dev  device double: (count - sum Re terms) / 2 with a compensated
- *               (Neumaier) fp64 sum -- the MaxCut energy when the networks are
- *               the edge terms of one graph; may be NULL;
+ *   energy_dev  device double: (groups - sum Re terms) / 2 with a compensated
+ *               (Neumaier) fp64 sum over the range's networks, groups = the
+ *               circuits they belong to -- the MaxCut energy when the
+ *               circuits are the edge terms of one graph; may be NULL;
  *   scratch_dev device memory of qtb_plan_scratch_bytes(); may be NULL when
  *               that size is 0.
  * The gate table is generated on the device from params_dev.             */
@@ -199,6 +213,10 @@ int qtb_plan_set_autotune(qtb_plan* plan, int32_t enable);
  * threads per CTA, dynamic shared memory bytes, flags: 1 = shared-memory
  * arena, 2 = persistent launch taking networks from a queue).             */
 int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32_t* n_classes);
+
+/* Device memory the plan holds once uploaded (images, gate table, job
+ * lists), excluding the caller's terms/energy/scratch buffers.            */
+int qtb_plan_device_bytes(const qtb_plan* plan, size_t* bytes);
 
 /* Device error word of the last run on this plan (0 = ok); synchronises. */
 int qtb_plan_device_status(qtb_plan* plan, int32_t* status);

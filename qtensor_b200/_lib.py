@@ -25,12 +25,13 @@ COMPOSER_DEFAULT, COMPOSER_ZZ, COMPOSER_CX = 0, 1, 2
 EXPORTS = (
     'qtb_version', 'qtb_init', 'qtb_last_error', 'qtb_bucket_c64',
     'qtb_plan_create', 'qtb_plan_destroy', 'qtb_plan_add_circuit',
-    'qtb_plan_add_lightcone', 'qtb_plan_add_lightcones', 'qtb_plan_set_order_trials',
+    'qtb_plan_add_lightcone', 'qtb_plan_add_lightcones', 'qtb_plan_set_max_width',
+    'qtb_plan_set_order_trials',
     'qtb_plan_n_networks',
     'qtb_plan_network_info', 'qtb_plan_network_peo', 'qtb_plan_check_params',
     'qtb_plan_export', 'qtb_plan_table_elems', 'qtb_plan_upload',
     'qtb_plan_scratch_bytes', 'qtb_plan_run', 'qtb_plan_set_autotune',
-    'qtb_plan_last_launch_config', 'qtb_plan_device_status',
+    'qtb_plan_last_launch_config', 'qtb_plan_device_bytes', 'qtb_plan_device_status',
     'qtb_plan_set_timing', 'qtb_plan_collect_timing', 'qtb_plan_run_noalloc',
 )
 NOALLOC_SCRATCH_BYTES = 64 << 20
@@ -65,7 +66,8 @@ class NetworkInfo(ctypes.Structure):
                 ('n_ops', ctypes.c_int32), ('n_phases', ctypes.c_int32),
                 ('arena_elems', ctypes.c_int32), ('angle_specific', ctypes.c_int32),
                 ('alg_bytes', ctypes.c_double), ('alg_flops', ctypes.c_double),
-                ('ref_flops', ctypes.c_double)]
+                ('ref_flops', ctypes.c_double), ('n_slices', ctypes.c_int32),
+                ('group', ctypes.c_int32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -82,7 +84,7 @@ PHASE_DTYPE = np.dtype([('op_first', '<u4'), ('op_count', '<u4'), ('total_elems'
                         ('chunk_off', '<u4')])
 ENTRY_DTYPE = np.dtype([('kind', '<i4'), ('expr_begin', '<i4'), ('expr_count', '<i4'),
                         ('off', '<u4'), ('rank_in', 'i1'), ('rank_out', 'i1'),
-                        ('sliced_mask', 'u1'), ('perm', 'i1', (5,))])
+                        ('sliced_mask', 'u1'), ('perm', 'i1', (4,)), ('sliced_value', 'u1')])
 TERM_DTYPE = np.dtype([('param', '<i4'), ('pad', '<i4'), ('coef', '<f8')])
 RUN_DTYPE = np.dtype([('blob_off16', '<u4'), ('blob_bytes', '<u4'), ('n_phases', '<u4'),
                       ('ins_off', '<u4'), ('arena_elems', '<u4'), ('result_src', '<u4'),
@@ -108,6 +110,7 @@ def _declare(lib):
                                              c.c_int32, c.c_int32, P, c.POINTER(c.c_int32)]),
         'qtb_plan_add_lightcones': (c.c_int, [P, c.c_int32, P, P, P, c.c_int32, c.c_int32,
                                               c.c_int32, P, c.c_int32, c.POINTER(c.c_int32)]),
+        'qtb_plan_set_max_width': (c.c_int, [P, c.c_int32]),
         'qtb_plan_set_order_trials': (c.c_int, [P, c.c_int32]),
         'qtb_plan_n_networks': (c.c_int, [P, c.POINTER(c.c_int32)]),
         'qtb_plan_network_info': (c.c_int, [P, c.c_int32, c.POINTER(NetworkInfo)]),
@@ -120,6 +123,7 @@ def _declare(lib):
         'qtb_plan_run': (c.c_int, [P, c.c_int32, c.c_int32, P, P, P, P, P]),
         'qtb_plan_set_autotune': (c.c_int, [P, c.c_int32]),
         'qtb_plan_last_launch_config': (c.c_int, [P, P, c.c_int32, c.POINTER(c.c_int32)]),
+        'qtb_plan_device_bytes': (c.c_int, [P, c.POINTER(c.c_size_t)]),
         'qtb_plan_device_status': (c.c_int, [P, c.POINTER(c.c_int32)]),
         'qtb_plan_set_timing': (c.c_int, [P, c.c_int32]),
         'qtb_plan_collect_timing': (c.c_int, [P, c.POINTER(c.c_double), c.POINTER(c.c_int64)]),

@@ -37,8 +37,8 @@ int fail(int code, const std::string& msg) {
 }
 
 bool EntryKey::operator<(const EntryKey& o) const {
-    return std::tie(kind, expr, rank_in, sliced_mask, perm) <
-           std::tie(o.kind, o.expr, o.rank_in, o.sliced_mask, o.perm);
+    return std::tie(kind, expr, rank_in, sliced_mask, sliced_value, perm) <
+           std::tie(o.kind, o.expr, o.rank_in, o.sliced_mask, o.sliced_value, o.perm);
 }
 
 int rank_of_kind(int32_t kind) {
@@ -322,26 +322,29 @@ struct OpRec {
 // uniformly among the tied nodes (the zero-temperature limit of
 // RGreedyOptimizer, qtensor/optimisation/RGreedy.py:36-62).
 static double greedy_order(int V, const std::vector<std::vector<int32_t>>& cliques, uint64_t seed,
-                           std::vector<int32_t>* order, std::vector<int32_t>* degrees) {
+                           std::vector<int32_t>* order, std::vector<int32_t>* degrees,
+                           const std::vector<char>* removed = nullptr) {
     const int W = (V + 63) / 64;
     std::vector<uint64_t> adj((size_t)V * W, 0);
     auto test = [&](int a, int b) { return (adj[(size_t)a * W + (b >> 6)] >> (b & 63)) & 1; };
     auto set = [&](int a, int b) { adj[(size_t)a * W + (b >> 6)] |= 1ull << (b & 63); };
     auto clr = [&](int a, int b) { adj[(size_t)a * W + (b >> 6)] &= ~(1ull << (b & 63)); };
     std::vector<int32_t> deg(V, 0);
+    auto gone = [&](int x) { return removed && (*removed)[x]; };
     for (const auto& c : cliques)
         for (size_t i = 0; i < c.size(); ++i)
             for (size_t j = i + 1; j < c.size(); ++j) {
                 int a = c[i], b = c[j];
-                if (a != b && !test(a, b)) {
+                if (a != b && !gone(a) && !gone(b) && !test(a, b)) {
                     set(a, b);
                     set(b, a);
                     ++deg[a];
                     ++deg[b];
                 }
             }
-    std::vector<int32_t> alive(V);
-    std::iota(alive.begin(), alive.end(), 0);
+    std::vector<int32_t> alive;
+    for (int x = 0; x < V; ++x)
+        if (!gone(x)) alive.push_back(x);
     std::vector<int32_t> nbrs, ties;
     uint64_t rng = seed;
     double cost = 0.0;
@@ -397,7 +400,10 @@ static double greedy_order(int V, const std::vector<std::vector<int32_t>>& cliqu
 
 int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
                     int32_t simplify_passes, const double* params, int32_t n_params,
-                    int32_t order_trials, Network* out, std::string* err) {
+                    int32_t order_trials, int32_t max_width, std::vector<Network>* outs,
+                    std::string* err) {
+    outs->clear();
+    std::vector<AngleCheck> checks;
     if (n_qubits <= 0 || n_gates < 0 || (n_gates > 0 && in_gates == nullptr)) {
         *err = "compile: invalid circuit arguments";
         return QTB_ERR_ARG;
@@ -431,7 +437,7 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
     }
     bool angle_specific = false;
     for (int pass = 0; pass < simplify_passes; ++pass) {
-        int rc = simplify(&gates, &out->checks, &angle_specific, err);
+        int rc = simplify(&gates, &checks, &angle_specific, err);
         if (rc) return rc;
     }
     // every qubit must keep a gate (n_qubits counts qubits that appear)
@@ -507,242 +513,298 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
             if (c.size() > 1) cliques.push_back(std::move(c));
         }
     // trial 0: the reference's greedy rule; trials 1..order_trials: seeded
-    // random tie-breaking; the cheapest order (sum of 2^degree) wins
+    // random tie-breaking; the cheapest order (sum of 2^degree) wins.  With
+    // max_width > 0, variables of highest degree are sliced (removed from
+    // the line graph, reference GreedyParvars, qtensor/optimisation/
+    // Greedy.py:78-91 driven by Optimizer.py:109-129) until the order's
+    // width drops below max_width.
+    const int V = (int)var_of.size();
+    std::vector<char> removed(V, 0);
+    std::vector<int32_t> par;   // sliced line-graph nodes, in slicing order
     std::vector<int32_t> gorder, gdeg, torder, tdeg;
-    double best_cost = greedy_order((int)var_of.size(), cliques, 0, &gorder, &gdeg);
-    for (int32_t t = 1; t <= order_trials; ++t) {
-        const uint64_t seed = 0x9E3779B97F4A7C15ull * (uint64_t)t + (uint64_t)var_of.size();
-        const double c = greedy_order((int)var_of.size(), cliques, seed, &torder, &tdeg);
-        if (c < best_cost) {
-            best_cost = c;
-            gorder.swap(torder);
-            gdeg.swap(tdeg);
+    auto best_order = [&]() {
+        double best_cost = greedy_order(V, cliques, 0, &gorder, &gdeg, &removed);
+        for (int32_t t = 1; t <= order_trials; ++t) {
+            const uint64_t seed = 0x9E3779B97F4A7C15ull * (uint64_t)t + (uint64_t)V;
+            const double c = greedy_order(V, cliques, seed, &torder, &tdeg, &removed);
+            if (c < best_cost) {
+                best_cost = c;
+                gorder.swap(torder);
+                gdeg.swap(tdeg);
+            }
         }
+    };
+    best_order();
+    auto width = [&]() { return gdeg.empty() ? 0 : *std::max_element(gdeg.begin(), gdeg.end()); };
+    while (max_width > 0 && width() >= max_width) {
+        if ((int)par.size() >= kMaxSlicedVars) {
+            *err = "compile: width " + std::to_string(width()) + " still >= " + std::to_string(max_width) +
+                   " after slicing " + std::to_string(kMaxSlicedVars) + " variables";
+            return QTB_ERR_UNSUPPORTED;
+        }
+        // distinct-neighbour degree in the graph with the sliced nodes removed
+        std::vector<std::vector<char>> adj(V, std::vector<char>(V, 0));
+        for (const auto& c : cliques)
+            for (size_t i = 0; i < c.size(); ++i)
+                for (size_t j = i + 1; j < c.size(); ++j)
+                    if (!removed[c[i]] && !removed[c[j]] && c[i] != c[j]) adj[c[i]][c[j]] = adj[c[j]][c[i]] = 1;
+        int best = -1, best_deg = -1;
+        for (int x = 0; x < V; ++x) {
+            if (removed[x]) continue;
+            int d = 0;
+            for (int y = 0; y < V; ++y) d += adj[x][y];
+            if (d > best_deg) {
+                best_deg = d;
+                best = x;
+            }
+        }
+        if (best < 0) break;
+        removed[best] = 1;
+        par.push_back(best);
+        best_order();
     }
-    std::vector<int32_t>& peo = out->peo;
-    peo.clear();
+    std::vector<int32_t> peo;
     for (int q = 0; q < nq; ++q) peo.push_back(ket_start + q);
     for (int q = 0; q < nq; ++q) peo.push_back(q);
     for (int32_t x : gorder) peo.push_back(var_of[x]);
+    for (int32_t x : par) peo.push_back(var_of[x]);
     if ((int32_t)peo.size() != n_vars) {
         *err = "compile: elimination order does not cover every variable";
         return QTB_ERR_ARG;
     }
     std::vector<int32_t> perm(n_vars);
     for (int32_t i = 0; i < n_vars; ++i) perm[peo[i]] = i;
-    const int32_t n_sliced = 2 * nq;
+    // sliced variables (new ids): ket and bra fixed to 0, sliced ones per slice
+    std::vector<char> sliced(n_vars, 0);
+    for (int32_t i = 0; i < 2 * nq; ++i) sliced[i] = 1;
+    for (size_t i = 0; i < par.size(); ++i) sliced[perm[var_of[par[i]]]] = 1;
 
-    // ---- reorder + slice: tensors become references to gate-table entries
-    std::vector<std::vector<Ref>> nb(n_vars);
-    std::map<EntryKey, int32_t> local;
-    for (const auto& b : buckets)
-        for (int32_t ti : b) {
-            const TRec& t = tensors[ti];
-            const int r = (int)t.vars.size();
-            std::vector<int> axes(r);
-            std::iota(axes.begin(), axes.end(), 0);
-            std::sort(axes.begin(), axes.end(),
-                      [&](int x, int y) { return perm[t.vars[x]] < perm[t.vars[y]]; });
-            EntryKey key;
-            key.kind = t.kind;
-            key.expr = t.expr;
-            key.rank_in = (int8_t)r;
-            key.sliced_mask = 0;
-            Ref ref;
-            ref.table = true;
-            for (int a : axes) {
-                const int32_t nv = perm[t.vars[a]];
-                ref.vars.push_back(nv);
-                if (nv < n_sliced) key.sliced_mask |= (uint8_t)(1u << a);
-                else key.perm.push_back((int8_t)a);
+    // one network per assignment of the sliced (parallel) variables
+    auto build = [&](uint64_t slice_bits, Network* out) -> int {
+        std::vector<char> value(n_vars, 0);
+        for (size_t i = 0; i < par.size(); ++i)
+            value[perm[var_of[par[i]]]] = (char)((slice_bits >> (par.size() - 1 - i)) & 1u);
+        // ---- reorder + slice: tensors become references to gate-table entries
+        std::vector<std::vector<Ref>> nb(n_vars);
+        std::map<EntryKey, int32_t> local;
+        out->checks = checks;
+        out->peo = peo;
+        for (const auto& b : buckets)
+            for (int32_t ti : b) {
+                const TRec& t = tensors[ti];
+                const int r = (int)t.vars.size();
+                std::vector<int> axes(r);
+                std::iota(axes.begin(), axes.end(), 0);
+                std::sort(axes.begin(), axes.end(),
+                          [&](int x, int y) { return perm[t.vars[x]] < perm[t.vars[y]]; });
+                EntryKey key;
+                key.kind = t.kind;
+                key.expr = t.expr;
+                key.rank_in = (int8_t)r;
+                key.sliced_mask = 0;
+                key.sliced_value = 0;
+                Ref ref;
+                ref.table = true;
+                for (int a : axes) {
+                    const int32_t nv = perm[t.vars[a]];
+                    ref.vars.push_back(nv);
+                    if (sliced[nv]) {
+                        key.sliced_mask |= (uint8_t)(1u << a);
+                        if (value[nv]) key.sliced_value |= (uint8_t)(1u << a);
+                    } else {
+                        key.perm.push_back((int8_t)a);
+                    }
+                }
+                auto it = local.find(key);
+                if (it == local.end()) {
+                    it = local.emplace(key, (int32_t)out->entries.size()).first;
+                    out->entries.push_back(key);
+                }
+                ref.id = it->second;
+                nb[ref.vars[0]].push_back(std::move(ref));
             }
-            auto it = local.find(key);
-            if (it == local.end()) {
-                it = local.emplace(key, (int32_t)out->entries.size()).first;
-                out->entries.push_back(key);
+
+        // ---- symbolic bucket elimination
+        std::vector<OpRec> ops;
+        std::vector<Ref> scalars;
+        double ref_flops = 0.0;
+        int32_t max_rank = 0;
+        for (int32_t n = 0; n < n_vars; ++n) {
+            std::vector<Ref>& b = nb[n];
+            if (b.empty()) continue;
+            std::vector<int32_t> U;
+            for (const Ref& r : b) U.insert(U.end(), r.vars.begin(), r.vars.end());
+            std::sort(U.begin(), U.end());
+            U.erase(std::unique(U.begin(), U.end()), U.end());
+            if (U.empty() || U[0] != n) {
+                *err = "compile: bucket " + std::to_string(n) + " holds a tensor without its variable";
+                return QTB_ERR_ARG;
             }
-            ref.id = it->second;
-            nb[ref.vars[0]].push_back(std::move(ref));
+            ref_flops += std::ldexp(1.0, (int)U.size() - 1) * (double)(1 + b.size());
+            std::vector<int32_t> outv(U.begin() + 1, U.end());
+            Ref res;
+            const bool live = !sliced[n];
+            if (b.size() == 1 && !live) {
+                res = b[0];      // product of one tensor over a size-1 variable: a copy
+                res.vars = outv;
+            } else {
+                OpRec op;
+                std::vector<int32_t> liveU;
+                for (int32_t v : U)
+                    if (!sliced[v]) liveU.push_back(v);
+                op.u = (int32_t)liveU.size();
+                op.sum = live ? 1 : 0;
+                op.w = op.u - op.sum;
+                if (op.u > QTB_MAX_BUCKET_VARS) {
+                    *err = "compile: bucket of " + std::to_string(op.u) + " variables exceeds the limit";
+                    return QTB_ERR_UNSUPPORTED;
+                }
+                max_rank = std::max(max_rank, op.u);
+                if (ops.size() >= 65535) {
+                    *err = "compile: network has more than 65535 bucket operations";
+                    return QTB_ERR_UNSUPPORTED;
+                }
+                for (const Ref& r : b) {
+                    uint32_t m = 0;
+                    for (int32_t v : r.vars) {
+                        if (sliced[v]) continue;
+                        const int pos = (int)(std::lower_bound(liveU.begin(), liveU.end(), v) - liveU.begin());
+                        m |= 1u << (op.u - 1 - pos);
+                    }
+                    op.masks.push_back(m);
+                    op.inputs.push_back(r);
+                }
+                res.table = false;
+                res.id = (int32_t)ops.size();
+                res.vars = outv;
+                ops.push_back(std::move(op));
+            }
+            if (outv.empty()) scalars.push_back(std::move(res));
+            else nb[outv[0]].push_back(std::move(res));
+            b.clear();
+            b.shrink_to_fit();
         }
-
-    // ---- symbolic bucket elimination
-    std::vector<OpRec> ops;
-    std::vector<Ref> scalars;
-    double ref_flops = 0.0;
-    int32_t max_rank = 0;
-    auto live_count = [&](const std::vector<int32_t>& vs) {
-        int c = 0;
-        for (int32_t v : vs) c += v >= n_sliced;
-        return c;
-    };
-    for (int32_t n = 0; n < n_vars; ++n) {
-        std::vector<Ref>& b = nb[n];
-        if (b.empty()) continue;
-        std::vector<int32_t> U;
-        for (const Ref& r : b) U.insert(U.end(), r.vars.begin(), r.vars.end());
-        std::sort(U.begin(), U.end());
-        U.erase(std::unique(U.begin(), U.end()), U.end());
-        if (U.empty() || U[0] != n) {
-            *err = "compile: bucket " + std::to_string(n) + " holds a tensor without its variable";
+        if (scalars.empty()) {
+            *err = "compile: network has no scalar result";
             return QTB_ERR_ARG;
         }
-        ref_flops += std::ldexp(1.0, (int)U.size() - 1) * (double)(1 + b.size());
-        std::vector<int32_t> outv(U.begin() + 1, U.end());
-        Ref res;
-        const bool live = n >= n_sliced;
-        if (b.size() == 1 && !live) {
-            res = b[0];      // product of one tensor over a size-1 variable: a copy
-            res.vars = outv;
+        Ref result;
+        if (scalars.size() == 1) {
+            result = scalars[0];
         } else {
             OpRec op;
-            std::vector<int32_t> liveU;
-            for (int32_t v : U)
-                if (v >= n_sliced) liveU.push_back(v);
-            op.u = (int32_t)liveU.size();
-            op.sum = live ? 1 : 0;
-            op.w = op.u - op.sum;
-            if (op.u > QTB_MAX_BUCKET_VARS) {
-                *err = "compile: bucket of " + std::to_string(op.u) + " variables exceeds the limit";
-                return QTB_ERR_UNSUPPORTED;
-            }
-            max_rank = std::max(max_rank, op.u);
-            if (ops.size() >= 65535) {
-                *err = "compile: network has more than 65535 bucket operations";
-                return QTB_ERR_UNSUPPORTED;
-            }
-            for (const Ref& r : b) {
-                uint32_t m = 0;
-                for (int32_t v : r.vars) {
-                    if (v < n_sliced) continue;
-                    const int pos = (int)(std::lower_bound(liveU.begin(), liveU.end(), v) - liveU.begin());
-                    m |= 1u << (op.u - 1 - pos);
-                }
-                op.masks.push_back(m);
+            op.u = op.sum = op.w = 0;
+            for (const Ref& r : scalars) {
                 op.inputs.push_back(r);
+                op.masks.push_back(0);
             }
-            res.table = false;
-            res.id = (int32_t)ops.size();
-            res.vars = outv;
+            result.table = false;
+            result.id = (int32_t)ops.size();
             ops.push_back(std::move(op));
         }
-        if (outv.empty()) scalars.push_back(std::move(res));
-        else nb[outv[0]].push_back(std::move(res));
-        b.clear();
-        b.shrink_to_fit();
-    }
-    if (scalars.empty()) {
-        *err = "compile: network has no scalar result";
-        return QTB_ERR_ARG;
-    }
-    Ref result;
-    if (scalars.size() == 1) {
-        result = scalars[0];
-    } else {
-        OpRec op;
-        op.u = op.sum = op.w = 0;
-        for (const Ref& r : scalars) {
-            op.inputs.push_back(r);
-            op.masks.push_back(0);
-        }
-        result.table = false;
-        result.id = (int32_t)ops.size();
-        ops.push_back(std::move(op));
-    }
 
-    // ---- dependency levels, arena intervals
-    int32_t max_level = 0;
-    for (OpRec& op : ops) {
-        int32_t lv = 0;
-        for (const Ref& r : op.inputs)
-            if (!r.table) lv = std::max(lv, ops[r.id].level);
-        op.level = lv + 1;
-        max_level = std::max(max_level, op.level);
-    }
-    for (OpRec& op : ops)
-        for (const Ref& r : op.inputs)
-            if (!r.table) ops[r.id].consumer_level = op.level;
-    if (!result.table) ops[result.id].consumer_level = max_level + 1;
-    std::vector<int32_t> by_level(ops.size());
-    std::iota(by_level.begin(), by_level.end(), 0);
-    std::stable_sort(by_level.begin(), by_level.end(),
-                     [&](int32_t x, int32_t y) { return ops[x].level < ops[y].level; });
-    struct Live { uint32_t off, size; int32_t end; };
-    std::vector<Live> active;
-    uint32_t arena = 0, max_elems = 1;
-    for (int32_t oi : by_level) {
-        OpRec& op = ops[oi];
-        active.erase(std::remove_if(active.begin(), active.end(),
-                                    [&](const Live& l) { return l.end < op.level; }),
-                     active.end());
-        const uint32_t size = 1u << op.w;
-        max_elems = std::max(max_elems, size);
-        const uint32_t need = (size + 3u) & ~3u;
-        std::sort(active.begin(), active.end(), [](const Live& a, const Live& b) { return a.off < b.off; });
-        uint32_t off = 0;
-        for (const Live& l : active) {
-            if (off + need <= l.off) break;
-            off = std::max(off, l.off + l.size);
+        // ---- dependency levels, arena intervals
+        int32_t max_level = 0;
+        for (OpRec& op : ops) {
+            int32_t lv = 0;
+            for (const Ref& r : op.inputs)
+                if (!r.table) lv = std::max(lv, ops[r.id].level);
+            op.level = lv + 1;
+            max_level = std::max(max_level, op.level);
         }
-        op.dst = off;
-        active.push_back({off, need, op.consumer_level});
-        arena = std::max(arena, off + need);
-    }
-
-    // ---- device images: ops in phase order
-    out->ops.clear();
-    out->ins.clear();
-    out->phases.clear();
-    double alg_bytes = 0.0, alg_flops = 0.0;
-    size_t cursor = 0;
-    for (int32_t lv = 1; lv <= max_level; ++lv) {
-        DevPhase ph{};
-        ph.op_first = (uint32_t)out->ops.size();
-        uint32_t elems = 0;
-        while (cursor < by_level.size() && ops[by_level[cursor]].level == lv) {
-            const OpRec& op = ops[by_level[cursor++]];
-            DevOp d{};
-            d.u = (uint8_t)op.u;
-            d.sum = (uint8_t)op.sum;
-            d.k = (uint8_t)op.inputs.size();
-            d.dst = op.dst;
-            d.elem_begin = elems;
-            d.in_begin = (uint32_t)out->ins.size();
-            for (size_t t = 0; t < op.inputs.size(); ++t) {
-                const Ref& r = op.inputs[t];
-                DevIn in{};
-                in.mask = op.masks[t];
-                in.src = r.table ? (kSrcTable | (uint32_t)r.id) : ops[r.id].dst;
-                in.runs = encode_runs(in.mask, (uint32_t)op.w);
-                out->ins.push_back(in);
-                alg_bytes += 8.0 * std::ldexp(1.0, __builtin_popcount(in.mask));
+        for (OpRec& op : ops)
+            for (const Ref& r : op.inputs)
+                if (!r.table) ops[r.id].consumer_level = op.level;
+        if (!result.table) ops[result.id].consumer_level = max_level + 1;
+        std::vector<int32_t> by_level(ops.size());
+        std::iota(by_level.begin(), by_level.end(), 0);
+        std::stable_sort(by_level.begin(), by_level.end(),
+                         [&](int32_t x, int32_t y) { return ops[x].level < ops[y].level; });
+        struct Live { uint32_t off, size; int32_t end; };
+        std::vector<Live> active;
+        uint32_t arena = 0, max_elems = 1;
+        for (int32_t oi : by_level) {
+            OpRec& op = ops[oi];
+            active.erase(std::remove_if(active.begin(), active.end(),
+                                        [&](const Live& l) { return l.end < op.level; }),
+                         active.end());
+            const uint32_t size = 1u << op.w;
+            max_elems = std::max(max_elems, size);
+            const uint32_t need = (size + 3u) & ~3u;
+            std::sort(active.begin(), active.end(), [](const Live& a, const Live& b) { return a.off < b.off; });
+            uint32_t off = 0;
+            for (const Live& l : active) {
+                if (off + need <= l.off) break;
+                off = std::max(off, l.off + l.size);
             }
-            alg_bytes += 8.0 * std::ldexp(1.0, op.w);
-            alg_flops += 6.0 * (double)(op.inputs.size() - 1) * std::ldexp(1.0, op.u) +
-                         (op.sum ? 2.0 * std::ldexp(1.0, op.w) : 0.0);
-            elems += 1u << op.w;
-            out->ops.push_back(d);
+            op.dst = off;
+            active.push_back({off, need, op.consumer_level});
+            arena = std::max(arena, off + need);
         }
-        ph.op_count = (uint32_t)out->ops.size() - ph.op_first;
-        ph.total_elems = elems;
-        out->phases.push_back(ph);
+
+        // ---- device images: ops in phase order
+        out->ops.clear();
+        out->ins.clear();
+        out->phases.clear();
+        double alg_bytes = 0.0, alg_flops = 0.0;
+        size_t cursor = 0;
+        for (int32_t lv = 1; lv <= max_level; ++lv) {
+            DevPhase ph{};
+            ph.op_first = (uint32_t)out->ops.size();
+            uint32_t elems = 0;
+            while (cursor < by_level.size() && ops[by_level[cursor]].level == lv) {
+                const OpRec& op = ops[by_level[cursor++]];
+                DevOp d{};
+                d.u = (uint8_t)op.u;
+                d.sum = (uint8_t)op.sum;
+                d.k = (uint8_t)op.inputs.size();
+                d.dst = op.dst;
+                d.elem_begin = elems;
+                d.in_begin = (uint32_t)out->ins.size();
+                for (size_t t = 0; t < op.inputs.size(); ++t) {
+                    const Ref& r = op.inputs[t];
+                    DevIn in{};
+                    in.mask = op.masks[t];
+                    in.src = r.table ? (kSrcTable | (uint32_t)r.id) : ops[r.id].dst;
+                    in.runs = encode_runs(in.mask, (uint32_t)op.w);
+                    out->ins.push_back(in);
+                    alg_bytes += 8.0 * std::ldexp(1.0, __builtin_popcount(in.mask));
+                }
+                alg_bytes += 8.0 * std::ldexp(1.0, op.w);
+                alg_flops += 6.0 * (double)(op.inputs.size() - 1) * std::ldexp(1.0, op.u) +
+                             (op.sum ? 2.0 * std::ldexp(1.0, op.w) : 0.0);
+                elems += 1u << op.w;
+                out->ops.push_back(d);
+            }
+            ph.op_count = (uint32_t)out->ops.size() - ph.op_first;
+            ph.total_elems = elems;
+            out->phases.push_back(ph);
+        }
+        out->result_src = result.table ? (kSrcTable | (uint32_t)result.id) : ops[result.id].dst;
+        out->max_elems = max_elems;
+        qtb_network_info& info = out->info;
+        info.n_qubits = nq;
+        info.n_vars = n_vars;
+        info.treewidth = gdeg.empty() ? 0 : *std::max_element(gdeg.begin(), gdeg.end());
+        info.n_slices = 1 << (int)par.size();
+        info.max_rank = max_rank;
+        info.n_ops = (int32_t)out->ops.size();
+        info.n_phases = (int32_t)out->phases.size();
+        info.arena_elems = (int32_t)arena;
+        info.angle_specific = angle_specific ? 1 : 0;
+        info.alg_bytes = alg_bytes;
+        info.alg_flops = alg_flops;
+        info.ref_flops = ref_flops;
+        return QTB_OK;
+    };
+    const uint64_t n_slices = 1ull << par.size();
+    outs->resize(n_slices);
+    for (uint64_t sl = 0; sl < n_slices; ++sl) {
+        int rc = build(sl, &(*outs)[sl]);
+        if (rc) return rc;
     }
-    out->result_src = result.table ? (kSrcTable | (uint32_t)result.id) : ops[result.id].dst;
-    out->max_elems = max_elems;
-    qtb_network_info& info = out->info;
-    info.n_qubits = nq;
-    info.n_vars = n_vars;
-    info.treewidth = gdeg.empty() ? 0 : *std::max_element(gdeg.begin(), gdeg.end());
-    info.max_rank = max_rank;
-    info.n_ops = (int32_t)out->ops.size();
-    info.n_phases = (int32_t)out->phases.size();
-    info.arena_elems = (int32_t)arena;
-    info.angle_specific = angle_specific ? 1 : 0;
-    info.alg_bytes = alg_bytes;
-    info.alg_flops = alg_flops;
-    info.ref_flops = ref_flops;
     return QTB_OK;
 }
-
 // ------------------------------------------------------ native lightcone
 int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indices, int32_t u,
                     int32_t v, int32_t p, int32_t composer, std::vector<qtb_gate>* gates,
@@ -819,7 +881,8 @@ int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indic
 }
 
 // ------------------------------------------------------ plan assembly
-void merge_network(qtb_plan* plan, Network&& net) {
+void merge_network(qtb_plan* plan, Network&& net, int32_t group) {
+    net.info.group = group;
     std::vector<uint32_t> table_off(net.entries.size());
     for (size_t i = 0; i < net.entries.size(); ++i) {
         const EntryKey& key = net.entries[i];
@@ -834,7 +897,8 @@ void merge_network(qtb_plan* plan, Network&& net) {
             e.rank_in = key.rank_in;
             e.rank_out = (int8_t)key.perm.size();
             e.sliced_mask = key.sliced_mask;
-            for (int a = 0; a < 5; ++a) e.perm[a] = a < (int)key.perm.size() ? key.perm[a] : -1;
+            e.sliced_value = key.sliced_value;
+            for (int a = 0; a < 4; ++a) e.perm[a] = a < (int)key.perm.size() ? key.perm[a] : -1;
             plan->table_elems += 1u << e.rank_out;
             it = plan->entry_index.emplace(key, (int32_t)plan->entries.size()).first;
             plan->entries.push_back(e);
@@ -947,14 +1011,15 @@ int qtb_plan_create(int32_t n_params, qtb_plan** out) {
 int qtb_plan_add_circuit(qtb_plan* plan, int32_t n_qubits, const qtb_gate* gates, int32_t n_gates,
                          int32_t simplify_passes, const double* params, int32_t* net_index) {
     if (!plan) return fail(QTB_ERR_ARG, "plan_add_circuit: null plan");
-    Network net;
+    std::vector<Network> nets;
     std::string err;
     int rc = compile_circuit(n_qubits, gates, n_gates, simplify_passes, params, plan->n_params,
-                             plan->order_trials, &net, &err);
+                             plan->order_trials, plan->max_width, &nets, &err);
     if (rc) return fail(rc, err);
     std::lock_guard<std::mutex> lock(plan->mu);
     if (net_index) *net_index = (int32_t)plan->nets.size();
-    merge_network(plan, std::move(net));
+    const int32_t group = plan->n_groups++;
+    for (auto& n : nets) merge_network(plan, std::move(n), group);
     return QTB_OK;
 }
 
@@ -978,7 +1043,7 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
                             int32_t* first_net_index) {
     if (!plan || !edges || n_edges < 0) return fail(QTB_ERR_ARG, "plan_add_lightcones: bad arguments");
     if (plan->n_params != 2 * p) return fail(QTB_ERR_ARG, "plan_add_lightcones: plan needs 2*p params");
-    std::vector<Network> nets(n_edges);
+    std::vector<std::vector<Network>> nets(n_edges);
     std::vector<int> codes(n_edges, 0);
     std::vector<std::string> errs(n_edges);
     std::atomic<int32_t> next{0};
@@ -992,7 +1057,8 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
                                      composer, &gates, &nq, &errs[i]);
             if (!rc)
                 rc = compile_circuit(nq, gates.data(), (int32_t)gates.size(), composer == 0 ? 2 : 0,
-                                     params, plan->n_params, plan->order_trials, &nets[i], &errs[i]);
+                                     params, plan->n_params, plan->order_trials, plan->max_width,
+                                     &nets[i], &errs[i]);
             codes[i] = rc;
         }
     };
@@ -1006,7 +1072,16 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
         if (codes[i]) return fail(codes[i], "edge " + std::to_string(i) + ": " + errs[i]);
     std::lock_guard<std::mutex> lock(plan->mu);
     if (first_net_index) *first_net_index = (int32_t)plan->nets.size();
-    for (auto& n : nets) merge_network(plan, std::move(n));
+    for (auto& circuit : nets) {
+        const int32_t group = plan->n_groups++;
+        for (auto& n : circuit) merge_network(plan, std::move(n), group);
+    }
+    return QTB_OK;
+}
+
+int qtb_plan_set_max_width(qtb_plan* plan, int32_t max_width) {
+    if (!plan || max_width < 0) return fail(QTB_ERR_ARG, "plan_set_max_width: bad arguments");
+    plan->max_width = max_width;
     return QTB_OK;
 }
 

@@ -89,8 +89,9 @@ struct DevEntry {
     uint32_t off;          // complex64 offset in the gate table
     int8_t rank_in;        // axes of the gate tensor as generated
     int8_t rank_out;       // axes kept (not sliced)
-    uint8_t sliced_mask;   // native axes fixed to index 0
-    int8_t perm[5];        // output axis a <- native axis perm[a]
+    uint8_t sliced_mask;   // native axes fixed to a value
+    int8_t perm[4];        // output axis a <- native axis perm[a]
+    uint8_t sliced_value;  // the values of the sliced axes (bit per native axis)
 };
 
 struct DevTerm {
@@ -116,6 +117,7 @@ struct EntryKey {
     Expr expr;
     int8_t rank_in;
     uint8_t sliced_mask;
+    uint8_t sliced_value;
     std::vector<int8_t> perm;
     bool operator<(const EntryKey& o) const;
 };
@@ -125,6 +127,9 @@ struct AngleCheck {
     Expr expr;
     bool must_be_small;   // true: |expr| < 1e-5 (cancelled); false: >= 1e-5 (merged)
 };
+
+// Most variables sliced per circuit (2^k networks).
+constexpr int kMaxSlicedVars = 16;
 
 struct Network {
     qtb_network_info info{};
@@ -152,6 +157,8 @@ struct DeviceBuffers {
 struct qtb_plan {
     int32_t n_params = 0;
     int32_t order_trials = 0;   // extra randomized greedy orders per network
+    int32_t max_width = 0;      // slice circuits whose width reaches this (0 = never)
+    int32_t n_groups = 0;       // circuits added (networks of a circuit share a group)
     std::vector<qtb::Network> nets;
     // global gate table, built from the networks' local entries
     std::map<qtb::EntryKey, int32_t> entry_index;
@@ -180,11 +187,12 @@ void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int compile_circuit(int32_t n_qubits, const qtb_gate* gates, int32_t n_gates,
                     int32_t simplify_passes, const double* params, int32_t n_params,
-                    int32_t order_trials, Network* out, std::string* err);
+                    int32_t order_trials, int32_t max_width, std::vector<Network>* outs,
+                    std::string* err);
 int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indices,
                     int32_t u, int32_t v, int32_t p, int32_t composer,
                     std::vector<qtb_gate>* gates, int32_t* n_qubits, std::string* err);
-void merge_network(qtb_plan* plan, Network&& net);
+void merge_network(qtb_plan* plan, Network&& net, int32_t group);
 void flatten_plan(qtb_plan* plan);
 uint64_t encode_runs(uint32_t mask, uint32_t w);
 void build_blobs(qtb_plan* plan);

@@ -145,7 +145,7 @@ __device__ void table_entry(const DevEntry& en, const DevTerm* terms, const doub
         alpha += terms[en.expr_begin + t].coef * params[terms[en.expr_begin + t].param];
     const int n = 1 << en.rank_out;
     for (int o = 0; o < n; ++o) {
-        uint32_t ixb = 0;   // sliced axes stay 0
+        uint32_t ixb = en.sliced_value;   // sliced axes at their values
         for (int a = 0; a < en.rank_out; ++a)
             ixb |= (uint32_t)((o >> (en.rank_out - 1 - a)) & 1) << en.perm[a];
         const double2 v = gate_value(en.kind, alpha, ixb);
@@ -185,6 +185,7 @@ struct RunArgs {
     uint32_t total_jobs;          // networks of the run over all its launches
     const float2* terms;          // the run's edge terms, [total_jobs]
     double* energy;               // MaxCut energy of the run, or null
+    double energy_groups;         // circuits (edge terms) of the run's networks
 };
 
 constexpr int kStatusArena = 1;        // network arena larger than the launch's capacity
@@ -245,8 +246,8 @@ __device__ __forceinline__ void neumaier_add(double& sum, double& comp, double x
 }
 
 // Compensated fp64 sum of Re(terms) by one CTA in a fixed order, then
-// energy = (n - sum) / 2.
-__device__ void reduce_energy(const float2* terms, uint32_t n, double* energy) {
+// energy = (n_groups - sum) / 2.
+__device__ void reduce_energy(const float2* terms, uint32_t n, double n_groups, double* energy) {
     __shared__ double ws[32], wc[32];
     double s = 0.0, c = 0.0;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) neumaier_add(s, c, (double)__ldcg(terms + i).x);
@@ -268,7 +269,7 @@ __device__ void reduce_energy(const float2* terms, uint32_t n, double* energy) {
             neumaier_add(ts, tc, ws[i]);
             neumaier_add(ts, tc, wc[i]);
         }
-        *energy = ((double)n - (ts + tc)) * 0.5;
+        *energy = (n_groups - (ts + tc)) * 0.5;
     }
 }
 
@@ -335,7 +336,7 @@ __device__ void build_table(const unsigned char* common, const RunArgs& a, float
         for (int t = 0; t < en.expr_count; ++t)
             alpha += terms[en.expr_begin + t].coef * __ldg(a.params + terms[en.expr_begin + t].param);
         const int o = (int)(i - en.off);
-        uint32_t ixb = 0;
+        uint32_t ixb = en.sliced_value;   // sliced axes at their values
         for (int ax = 0; ax < en.rank_out; ++ax)
             ixb |= (uint32_t)((o >> (en.rank_out - 1 - ax)) & 1) << en.perm[ax];
         const double2 v = gate_value(en.kind, alpha, ixb);
@@ -435,14 +436,16 @@ __global__ void __launch_bounds__(kPersistent ? 512 : 1024) qtb_network_kernel(
         }
         const Job job = jobs[kPersistent ? s_job : blockIdx.x];
         const DevNetRun net = *job.net;
-        if (net.arena_elems > a.arena_capacity || net.blob_bytes > a.blob_capacity) {
+        // blob_capacity 0: the launch reads plan blobs from global memory
+        const bool staged = a.blob_capacity != 0;
+        if (net.arena_elems > a.arena_capacity || (staged && net.blob_bytes > a.blob_capacity)) {
             if (threadIdx.x == 0)
                 atomicOr(a.status, net.arena_elems > a.arena_capacity ? kStatusArena : kStatusBlob);
             return;
         }
         // the first staging of a CTA also brings the plan-wide gate entries
         const bool with_common = kSmemTable && !table_ready;
-        if (!stage(blob, a.blobs + net.blob_off16, net.blob_bytes, common, a.common,
+        if (!stage(blob, a.blobs + net.blob_off16, staged ? net.blob_bytes : 0u, common, a.common,
                    with_common ? a.common_bytes : 0u, bar, parity, a.status))
             return;
         parity ^= 1u;
@@ -450,7 +453,9 @@ __global__ void __launch_bounds__(kPersistent ? 512 : 1024) qtb_network_kernel(
             build_table(common, a, stable);
             table_ready = true;
         }
-        const float2 term = contract_network<kSmemTable>(net, blob, table, arena);
+        const unsigned char* nblob =
+            staged ? blob : reinterpret_cast<const unsigned char*>(a.blobs + net.blob_off16);
+        const float2 term = contract_network<kSmemTable>(net, nblob, table, arena);
         if (threadIdx.x == 0) {
             *job.term = term;
             if (a.energy) {
@@ -461,7 +466,7 @@ __global__ void __launch_bounds__(kPersistent ? 512 : 1024) qtb_network_kernel(
         __syncthreads();   // blob and arena are reused by the next network
         if (a.energy && is_last) {
             __threadfence();
-            reduce_energy(a.terms, a.total_jobs, a.energy);
+            reduce_energy(a.terms, a.total_jobs, a.energy_groups, a.energy);
             if (threadIdx.x == 0) *a.done = 0u;   // ready for the next run
             __syncthreads();
         }
@@ -531,6 +536,7 @@ struct RunCache {
     std::vector<LaunchClass> pclasses;  // persistent schedule (+ global-arena class)
     size_t scratch_elems = 0;
     bool smem_table = true;
+    double n_groups = 0.0;              // distinct circuits among the range's networks
 };
 
 }  // namespace qtb
@@ -696,6 +702,9 @@ static size_t net_need(const DevNetRun& r, size_t fixed) {
 // first so its long critical path starts early.
 static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms, RunCache* rc) {
     rc->smem_table = plan->table_elems <= kSmemTableLimitElems;
+    rc->n_groups = 0.0;
+    for (int32_t i = first; i < first + count; ++i)
+        if (i == first || plan->nets[i].info.group != plan->nets[i - 1].info.group) rc->n_groups += 1.0;
     const size_t fixed = fixed_smem(plan, rc->smem_table);
     std::vector<std::vector<int32_t>> members(kMaxClasses);
     for (int32_t i = first; i < first + count; ++i) {
@@ -707,8 +716,6 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
                 c = b;
                 break;
             }
-        if (c == kSmemClasses && fixed + (size_t)r.blob_bytes > kSmemLimitBytes)
-            return fail(QTB_ERR_UNSUPPORTED, "network plan blob exceeds shared memory");
         members[c].push_back(i);
     }
     // a class holds the largest blob and the largest arena of its members;
@@ -749,7 +756,10 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
             jobs.push_back(j);
         }
         lc.capacity = (cap + 3u) & ~3u;
-        lc.blob_capacity = blob;
+        // a global-arena class whose largest blob does not fit shared memory
+        // reads every member's blob from global memory (capacity 0)
+        lc.blob_capacity = (!smem && fixed + (size_t)blob > kSmemLimitBytes) ? 0u : blob;
+        blob = lc.blob_capacity;
         lc.threads = persistent ? 256 : class_threads(maxe, lc.n_jobs);
         lc.smem_bytes = fixed + (size_t)blob + (smem ? 8 * (size_t)lc.capacity : 0);
         return lc;
@@ -1077,6 +1087,7 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
     a.total_jobs = (uint32_t)count;
     a.terms = static_cast<const float2*>(terms_dev);
     a.energy = energy_dev;
+    a.energy_groups = rc->n_groups;
     const int n_entries = (int)plan->entries.size();
     if (!rc->smem_table && n_entries > 0) {
         qtb_table_kernel<<<(n_entries + 127) / 128, 128, 0, st>>>(
@@ -1230,6 +1241,9 @@ int qtb_plan_run_noalloc(qtb_plan* plan, int32_t first, int32_t count, const dou
     a.total_jobs = (uint32_t)count;
     a.terms = static_cast<const float2*>(terms_dev);
     a.energy = energy_dev;
+    a.energy_groups = 0.0;
+    for (int32_t i = first; i < first + count; ++i)
+        if (i == first || plan->nets[i].info.group != plan->nets[i - 1].info.group) a.energy_groups += 1.0;
     const int threads = threads_for(maxe);
     if (smem_table)
         qtb_network_kernel<false, true, false><<<count, threads, smem_bytes, st>>>(jobs, a);
@@ -1265,6 +1279,22 @@ int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32
         out[4 * c + 2] = (int32_t)lc.smem_bytes;
         out[4 * c + 3] = (lc.smem ? 1 : 0) | (lc.persistent ? 2 : 0);
     }
+    return QTB_OK;
+}
+
+int qtb_plan_device_bytes(const qtb_plan* plan, size_t* bytes) {
+    if (!plan || !bytes) return fail(QTB_ERR_ARG, "plan_device_bytes: bad arguments");
+    // images qtb_plan_upload sends, gate table, jobs of both schedules
+    size_t b = 0, blob = 0;
+    for (const Network& n : plan->nets) {
+        blob += n.phases.size() * sizeof(DevPhase) + n.ops.size() * sizeof(DevOp) +
+                n.ins.size() * sizeof(DevIn) + 16;
+        for (const DevPhase& ph : n.phases) blob += 2 * ((ph.total_elems + kChunkElems - 1) / kChunkElems);
+    }
+    b += blob + plan->nets.size() * (sizeof(DevNetRun) + 2 * sizeof(Job));
+    b += plan->entries.size() * sizeof(DevEntry) + plan->terms.size() * sizeof(DevTerm) + 64;
+    b += (size_t)plan->table_elems * sizeof(float2);
+    *bytes = b;
     return QTB_OK;
 }
 

@@ -28,9 +28,9 @@ def _require_cuda():
         raise RuntimeError('qtensor_b200 needs a CUDA device; there is no CPU fallback')
 
 
-def graph_key(G, p, composer, ordering, trials=0):
+def graph_key(G, p, composer, ordering, trials=0, max_width=0):
     h = hashlib.sha1()
-    h.update(repr((p, composer, ordering, trials, G.number_of_nodes())).encode())
+    h.update(repr((p, composer, ordering, trials, max_width, G.number_of_nodes())).encode())
     h.update(repr(list(G.nodes())).encode())
     h.update(repr(list(G.edges())).encode())
     return h.hexdigest()
@@ -45,11 +45,14 @@ class CompiledGraph:
         self.p = p
         self.composer = composer
         self.n_edges = len(edges)
+        self.n_networks = len(plan)
         self.device = device
-        self.terms = torch.empty(self.n_edges, dtype=torch.complex64, device=device)
+        # networks of one edge (its slices) are contiguous and share a group
+        self.groups = plan.groups()
+        self.terms = torch.empty(self.n_networks, dtype=torch.complex64, device=device)
         self.energy = torch.empty(1, dtype=torch.float64, device=device)
         self.params = torch.empty(2 * p, dtype=torch.float64, device=device)
-        nbytes = plan.scratch_bytes(0, self.n_edges)
+        nbytes = plan.scratch_bytes(0, self.n_networks)
         self.scratch = (torch.empty(max(nbytes, 8), dtype=torch.uint8, device=device)
                         if nbytes else None)
         self._infos = None
@@ -69,6 +72,7 @@ class CompiledGraph:
         widths = [i['treewidth'] for i in infos]
         return {
             'edges': self.n_edges,
+            'networks': self.n_networks,
             'width_max': max(widths), 'width_mean': float(np.mean(widths)),
             'ops': int(sum(i['n_ops'] for i in infos)),
             'phases_max': max(i['n_phases'] for i in infos),
@@ -82,8 +86,15 @@ class CompiledGraph:
     def launch(self, params_dev=None, stream=None):
         """Contract all edge networks asynchronously; energy lands in ``self.energy``."""
         stream = torch.cuda.current_stream(self.device) if stream is None else stream
-        self.plan.run(0, self.n_edges, self.params if params_dev is None else params_dev,
+        self.plan.run(0, self.n_networks, self.params if params_dev is None else params_dev,
                       self.terms, self.energy, self.scratch, stream.cuda_stream)
+
+    def edge_terms(self):
+        """Per-edge amplitudes of the last run (slices summed), complex128."""
+        vals = self.terms.cpu().numpy().astype(np.complex128)
+        out = np.zeros(self.n_edges, dtype=np.complex128)
+        np.add.at(out, self.groups - self.groups[0], vals)
+        return out
 
     def _capture(self):
         """CUDA graph of one call: pinned angles -> device, gate table,
@@ -134,7 +145,7 @@ class QAOAEnergyEngine:
     """
 
     def __init__(self, composer='default', ordering='native', device=None, threads=0,
-                 cache_size=16, order_trials=16, autotune=True):
+                 cache_size=16, order_trials=16, autotune=True, max_width=24):
         _require_cuda()
         if ordering not in ('native', 'reference'):
             raise ValueError('ordering must be "native" or "reference"')
@@ -146,6 +157,7 @@ class QAOAEnergyEngine:
         self.cache_size = cache_size
         self.order_trials = order_trials if ordering == 'native' else 0
         self.autotune = autotune
+        self.max_width = max_width
         self._cache = {}
         self._by_id = {}        # id(G) -> (weakref, nodes, edges, p, key)
         self._lock = threading.Lock()
@@ -166,6 +178,7 @@ class QAOAEnergyEngine:
         edges = list(G.edges())
         plan = NetworkPlan(2 * p)
         plan.set_order_trials(self.order_trials)
+        plan.set_max_width(self.max_width)
         if self.ordering == 'native':
             csr = graph_csr(G)
             index = {v: i for i, v in enumerate(csr[0])}
@@ -194,7 +207,7 @@ class QAOAEnergyEngine:
             ref, n, m, hp, key = hit
             if ref() is G and hp == p and n == G.number_of_nodes() and m == G.number_of_edges():
                 return key
-        key = graph_key(G, p, self.composer, self.ordering, self.order_trials)
+        key = graph_key(G, p, self.composer, self.ordering, self.order_trials, self.max_width)
         try:
             self._by_id[id(G)] = (weakref.ref(G), G.number_of_nodes(), G.number_of_edges(), p, key)
         except TypeError:
@@ -227,13 +240,14 @@ class QAOAEnergyEngine:
         return cg.energy_of(self._params(p, gamma, beta))
 
     def edge_terms(self, G, gamma, beta):
-        """``<Z_u Z_v>`` of every edge (complex64 numpy array, edge order of ``G.edges()``)."""
+        """``<Z_u Z_v>`` of every edge (numpy complex, edge order of ``G.edges()``;
+        sliced edges are summed over their slices)."""
         gamma = np.asarray(gamma, dtype=np.float64).ravel()
         p = len(gamma)
         cg = self.compile(G, p, gamma, beta)
         cg.params.copy_(torch.from_numpy(self._params(p, gamma, beta)))
         cg.launch()
-        return cg.terms.cpu().numpy()
+        return cg.edge_terms()
 
     def check_device(self, cg):
         """Raise if a kernel of ``cg`` reported an error status (synchronises)."""

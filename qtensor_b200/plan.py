@@ -37,6 +37,15 @@ class NetworkPlan:
         self.uploaded = False
 
     # ------------------------------------------------------------ compile
+    def set_max_width(self, max_width):
+        """Slice circuits added afterwards whose greedy width reaches
+        ``max_width`` into 2^k networks (0 = never)."""
+        check(self._lib.qtb_plan_set_max_width(self._h, int(max_width)))
+
+    def groups(self):
+        """Circuit (group) of every network."""
+        return np.array([self.info(i)['group'] for i in range(len(self))], dtype=np.int64)
+
     def set_order_trials(self, trials):
         """Randomized greedy orders tried per network added afterwards (0 =
         the reference's greedy order only)."""
@@ -139,6 +148,12 @@ class NetworkPlan:
         out = np.zeros(4 * 16, dtype=np.int32)
         check(self._lib.qtb_plan_last_launch_config(self._h, ptr(out), len(out), ctypes.byref(n)))
         return [tuple(int(x) for x in out[4 * c:4 * c + 4]) for c in range(min(n.value, 16))]
+
+    def device_bytes(self):
+        """Device memory the uploaded plan holds (excluding run buffers)."""
+        n = ctypes.c_size_t()
+        check(self._lib.qtb_plan_device_bytes(self._h, ctypes.byref(n)))
+        return n.value
 
     def device_status(self):
         s = ctypes.c_int32()

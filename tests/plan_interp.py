@@ -51,7 +51,8 @@ def gate_table(exported, params):
                     for i in range(e['expr_begin'], e['expr_begin'] + e['expr_count']))
         t = np.asarray(_gate_tensor(int(e['kind']), alpha), dtype=np.complex128)
         assert t.ndim == e['rank_in']
-        idx = tuple(0 if (e['sliced_mask'] >> a) & 1 else slice(None) for a in range(t.ndim))
+        idx = tuple(((int(e['sliced_value']) >> a) & 1) if (e['sliced_mask'] >> a) & 1 else slice(None)
+                    for a in range(t.ndim))
         kept = [a for a in range(t.ndim) if not (e['sliced_mask'] >> a) & 1]
         t = t[idx]
         perm = [int(x) for x in e['perm'][:e['rank_out']]]
@@ -170,7 +171,14 @@ def run_network(exported, table, net_index):
     return table[res & ~_lib.SRC_TABLE] if res & _lib.SRC_TABLE else arena[res]
 
 
-def run_plan(plan, params):
+def run_plan(plan, params, per_circuit=True):
+    """Amplitude of every circuit (slices summed), or of every network."""
     ex = plan.export()
     table = gate_table(ex, np.asarray(params, dtype=np.float64))
-    return np.array([run_network(ex, table, i) for i in range(len(ex['runs']))])
+    vals = np.array([run_network(ex, table, i) for i in range(len(ex['runs']))])
+    if not per_circuit:
+        return vals
+    groups = plan.groups()
+    out = np.zeros(groups.max() + 1 if len(groups) else 0, dtype=np.complex128)
+    np.add.at(out, groups, vals)
+    return out

@@ -99,8 +99,13 @@ def test_engine_rejects_bad_angles(cuda_device):
         _engine().energy_expectation(graphs.regular(10), [0.1, 0.2], [0.3])
 
 
-def test_engine_needs_cuda_loudly(monkeypatch):
-    from qtensor_b200 import engine
-    monkeypatch.setattr(torch.cuda, 'is_available', lambda: False)
-    with pytest.raises(RuntimeError, match='no CPU fallback'):
-        engine.QAOAEnergyEngine()
+@pytest.mark.parametrize('name,max_width', [('cfg2', 9), ('cfg4', 17)])
+def test_engine_sliced(cuda_device, name, max_width):
+    """Sliced networks (2^k per edge, FeynmanSimulator semantics) give the
+    reference's edge terms and energy."""
+    eng = _engine(max_width=max_width)
+    G, w = golden_graph(name)
+    cg = eng.compile(G, len(w['gamma']), w['gamma'], w['beta'])
+    assert cg.n_networks > cg.n_edges
+    assert max(i['treewidth'] for i in cg.infos) < max_width
+    _check(eng, name)

@@ -1,0 +1,79 @@
+"""Continuous-batching server: every result equals the reference energy, is
+the same alone and in a mix of concurrent requests, and a failing request
+fails alone."""
+import networkx as nx
+import numpy as np
+import pytest
+
+import graphs
+import qtensor_port as port
+from conftest import golden_graph
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(n, seed=0):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        N = int(rng.integers(16, 60))
+        p = int(rng.integers(1, 4))
+        if i % 2:
+            G = nx.erdos_renyi_graph(N, 3 / (N - 1), seed=int(rng.integers(1 << 30)))
+        else:
+            G = nx.random_regular_graph(3, N + (N % 2), seed=int(rng.integers(1 << 30)))
+        gamma, beta = graphs.angles(p, seed=int(rng.integers(1 << 30)))
+        if G.number_of_edges():
+            out.append((G, gamma, beta))
+    return out
+
+
+def test_server_matches_reference(cuda_device):
+    from qtensor_b200.serve import QAOAServer
+    G, w = golden_graph('cfg2')
+    with QAOAServer() as srv:
+        res = srv.submit(G, w['gamma'], w['beta']).result(timeout=120)
+    assert abs(res.energy - w['energy']) <= 1e-5 * abs(w['energy'])
+    assert res.edges == G.number_of_edges() and res.latency > 0
+
+
+def test_alone_and_in_the_mix_agree(cuda_device):
+    """Each request's energy is identical whether it runs alone (one stream,
+    one request at a time) or together with the others (four streams, all
+    submitted at once), and equals the oracle's."""
+    from qtensor_b200.serve import QAOAServer
+    reqs = _requests(14)
+    with QAOAServer(n_streams=1) as srv:
+        alone = [srv.submit(*r).result(timeout=120).energy for r in reqs]
+    with QAOAServer(n_streams=4) as srv:
+        futs = [srv.submit(*r) for r in reqs]
+        mixed = [f.result(timeout=120).energy for f in futs]
+    assert alone == mixed
+    for (G, gamma, beta), e in list(zip(reqs, mixed))[:4]:
+        ref = float(port.energy_expectation(G, gamma, beta)[0])
+        assert abs(e - ref) <= 1e-5 * max(1.0, abs(ref))
+
+
+def test_failing_request_fails_alone(cuda_device):
+    from qtensor_b200.serve import QAOAServer
+    reqs = _requests(4, seed=3)
+    with QAOAServer(memory_budget=1 << 30) as srv:
+        bad_angles = srv.submit(reqs[0][0], [0.1, 0.2], [0.3])          # p mismatch
+        empty = srv.submit(nx.empty_graph(5), [0.1], [0.2])             # no edges
+        good = [srv.submit(*r) for r in reqs]
+        with pytest.raises(ValueError):
+            bad_angles.result(timeout=60)
+        with pytest.raises(ValueError):
+            empty.result(timeout=60)
+        energies = [f.result(timeout=120).energy for f in good]
+    for (G, gamma, beta), e in zip(reqs, energies):
+        ref = float(port.energy_expectation(G, gamma, beta)[0])
+        assert abs(e - ref) <= 1e-5 * max(1.0, abs(ref))
+
+
+def test_over_budget_request_is_rejected(cuda_device):
+    from qtensor_b200.serve import QAOAServer
+    G = graphs.regular(200)
+    with QAOAServer(memory_budget=1024) as srv:
+        with pytest.raises(MemoryError):
+            srv.submit(G, [0.1], [0.2]).result(timeout=60)

@@ -1,0 +1,43 @@
+"""Host-side logic that needs no GPU: serving admission control and the
+loud failure of the product paths without a CUDA device."""
+import pytest
+import torch
+
+from qtensor_b200.serve import AdmissionControl
+
+
+def test_admission_respects_budget_and_slots():
+    adm = AdmissionControl(budget_bytes=100, slots=2)
+    assert adm.fits_ever(100) and not adm.fits_ever(101)
+    a = adm.try_admit(60)
+    assert a == 0
+    assert adm.try_admit(50) is None          # memory: 60 + 50 > 100
+    b = adm.try_admit(40)
+    assert b == 1
+    assert adm.try_admit(1) is None           # no slot left
+    adm.release(a, 60)
+    assert adm.used == 40 and adm.try_admit(60) == 0
+    adm.release(0, 60)
+    adm.release(1, 40)
+    assert adm.used == 0 and adm.free_slots == [0, 1]
+
+
+def test_engine_needs_cuda_loudly(monkeypatch):
+    from qtensor_b200 import engine
+    monkeypatch.setattr(torch.cuda, 'is_available', lambda: False)
+    with pytest.raises(RuntimeError, match='no CPU fallback'):
+        engine.QAOAEnergyEngine()
+
+
+def test_server_needs_cuda_loudly(monkeypatch):
+    from qtensor_b200 import serve
+    monkeypatch.setattr(torch.cuda, 'is_available', lambda: False)
+    with pytest.raises(RuntimeError, match='no CPU fallback'):
+        serve.QAOAServer()
+
+
+def test_backend_needs_cuda_loudly(monkeypatch):
+    from qtensor_b200.backend import B200Backend
+    monkeypatch.setattr(torch.cuda, 'is_available', lambda: False)
+    with pytest.raises(RuntimeError, match='no CPU fallback'):
+        B200Backend().get_sliced_buckets([[]], {}, {})

@@ -151,3 +151,23 @@ def test_bucket_desc_validation_without_device():
     ptrs[0] = 16
     assert lib.qtb_bucket_c64(ctypes.byref(desc), ptrs, ctypes.c_void_p(8), None) == 1
     assert 'outside the union' in _lib.last_error()
+
+
+@pytest.mark.parametrize('name,max_width', [('cfg1_default', 3), ('cfg2', 11), ('test_grid2d_n3_p3_d0', 8)])
+def test_sliced_networks_sum_to_reference(name, max_width):
+    """Slicing (FeynmanSimulator's parallel variables, greedy max-degree
+    choice): every circuit becomes 2^k networks whose amplitudes sum to the
+    reference's edge term; sliced widths stay below max_width."""
+    G, w = golden_graph(name)
+    p = len(w['gamma'])
+    plan = NetworkPlan(2 * p)
+    plan.set_max_width(max_width)
+    plan.add_lightcones(graph_csr(G), np.array(list(G.edges())), p, 0, _params(w))
+    infos = plan.infos()
+    assert max(i['n_slices'] for i in infos) > 1            # slicing happened
+    assert all(i['treewidth'] < max_width for i in infos)
+    groups = plan.groups()
+    assert np.all(np.diff(groups) >= 0) and groups[-1] == len(w['terms']) - 1
+    vals = plan_interp.run_plan(plan, _params(w))
+    ref = np.array([complex(*t) for t in w['terms']])
+    assert np.max(np.abs(vals - ref)) < 1e-12
