@@ -57,6 +57,10 @@ def parse():
     ap.add_argument('--nodes', type=int, default=1000)
     ap.add_argument('--p', type=int, default=3)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--serving-requests', type=int, default=64,
+                    help='requests of the serving run (0 skips it)')
+    ap.add_argument('--serving-rate', type=float, default=20.0,
+                    help='Poisson arrival rate of the serving run, requests/s')
     return ap.parse_args()
 
 
@@ -169,6 +173,100 @@ class ClockSampler:
         return {'sm_mhz': statistics.median(sms) if sms else None,
                 'sm_max_mhz': max(maxes) if maxes else None,
                 'reasons': sorted(reasons), 'samples': len(sms)}
+
+
+# ------------------------------------------------------------------ serving
+def serving_requests(n, seed=0):
+    """The serving workload: 3-regular or Erdos-Renyi (mean degree 3)
+    graphs, N uniform in 16..500, p uniform in 1..4, angles U[0, pi)."""
+    import networkx as nx
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < n:
+        N = int(rng.integers(16, 501))
+        p = int(rng.integers(1, 5))
+        if rng.random() < 0.5:
+            G = nx.random_regular_graph(3, N + (N % 2), seed=int(rng.integers(1 << 30)))
+        else:
+            G = nx.erdos_renyi_graph(N, 3 / (N - 1), seed=int(rng.integers(1 << 30)))
+        if G.number_of_edges():
+            gamma, beta = graphs.angles(p, seed=int(rng.integers(1 << 30)))
+            out.append((G, gamma, beta))
+    return out
+
+
+def run_serving(n_requests, rate, device_index):
+    """Poisson stream through the continuous-batching server, then the same
+    requests one at a time on a single-stream server."""
+    from qtensor_b200.serve import QAOAServer
+    reqs = serving_requests(n_requests)
+    rng = np.random.default_rng(1)
+    gaps = rng.exponential(1.0 / rate, size=len(reqs))
+
+    def summarize(results, wall):
+        ok = [r for r in results if not isinstance(r, Exception)]
+        lat = np.array([r.latency for r in ok]) * 1e3
+        edges = sum(r.edges for r in ok)
+        pct = (lambda q: float(np.percentile(lat, q)) if len(lat) else None)
+        return {'completed': len(ok), 'rejected': len(results) - len(ok),
+                'p50_ms': pct(50), 'p95_ms': pct(95), 'p99_ms': pct(99),
+                'edge_terms_per_s': edges / wall if wall > 0 else None, 'wall_s': wall}
+
+    def collect(futs):
+        out = []
+        for f in futs:
+            try:
+                out.append(f.result(timeout=600))
+            except Exception as exc:     # noqa: BLE001 - rejected (too wide, over budget)
+                out.append(exc)
+        return out
+
+    with QAOAServer(device=device_index, n_streams=4) as srv:
+        t0 = time.perf_counter()
+        futs = []
+        for (G, gamma, beta), gap in zip(reqs, gaps):
+            time.sleep(gap)
+            futs.append(srv.submit(G, gamma, beta))
+        stream = collect(futs)
+        wall_stream = time.perf_counter() - t0
+    with QAOAServer(device=device_index, n_streams=1, compile_workers=1) as srv:
+        t0 = time.perf_counter()
+        alone = []
+        for r in reqs:
+            alone.extend(collect([srv.submit(*r)]))
+        wall_alone = time.perf_counter() - t0
+
+    def same(a, b):
+        if isinstance(a, Exception) or isinstance(b, Exception):
+            return isinstance(a, Exception) and isinstance(b, Exception)
+        return a.energy == b.energy
+    return {'workload': '{} requests: 3-regular or Erdos-Renyi (mean degree 3), N U[16,500], '
+                        'p U[1,4], angles U[0,pi) (seed 0); Poisson arrivals at {} req/s '
+                        '(seed 1); slicing from width 22, at most 256 slices per edge'.format(
+                            len(reqs), rate),
+            'continuous_batching': summarize(stream, wall_stream),
+            'one_at_a_time': summarize(alone, wall_alone),
+            'same_energy_alone_and_in_mix': all(same(a, b) for a, b in zip(stream, alone))}
+
+
+def oracle_error(eng, G, p):
+    """Edge terms at the reference fixture's angles against its complex128
+    values (the fixture holds every edge of the seed-0 workload graph)."""
+    path = os.path.join(ROOT, 'tests', 'golden', 'qaoa_reference.json')
+    try:
+        with open(path) as f:
+            w = json.load(f)['workloads']['cfg3']
+    except (OSError, KeyError, ValueError):
+        return None
+    if [list(e) for e in G.edges()] != [list(e) for e in w['edges']] or len(w['gamma']) != p:
+        return None
+    terms = eng.edge_terms(G, w['gamma'], w['beta'])
+    ref = np.array([complex(*t) for t in w['terms']])
+    E = eng.energy_expectation(G, w['gamma'], w['beta'])
+    return {'edge_terms': len(ref), 'max_abs_error': float(np.max(np.abs(terms - ref))),
+            'mean_abs_error': float(np.mean(np.abs(terms - ref))),
+            'energy_rel_error': abs(E - w['energy']) / abs(w['energy']),
+            'oracle': 'complex128 reference values, tests/golden/qaoa_reference.json'}
 
 
 # ------------------------------------------------------------------ GPU arm
@@ -295,6 +393,11 @@ def run_b200(args):
     barrier()
     clk = clocks.stop()
 
+    errors = oracle_error(eng, G, p) if rank == 0 else None
+    serving = None
+    if rank == 0 and world == 1 and args.serving_requests > 0:
+        serving = run_serving(args.serving_requests, args.serving_rate, local)
+
     total_ms = sum(step_ms)
     e2e_total = sum(e2e_ms)
     if pg:
@@ -336,6 +439,8 @@ def run_b200(args):
             'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': 8 * 2 * p,
                     'd2h_bytes_per_step': 8, 'ms_per_step': e2e_total / args.steps},
             'clocks': clk,
+            'error_vs_oracle': errors,
+            'serving': serving,
             # every kernel of a step is a qtb_network_kernel class launch (gate
             # table and energy reduction are fused into it)
             'gpu_launches': int(kernel_launches),

@@ -150,8 +150,11 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
  * below; the circuit then becomes 2^k networks, one per assignment of the
  * k sliced variables, whose amplitudes sum to the circuit's.  Networks of a
  * circuit are contiguous and share qtb_network_info.group; qtb_plan_run's
- * energy counts groups, not networks.  0 (default) never slices.         */
-int qtb_plan_set_max_width(qtb_plan* plan, int32_t max_width);
+ * energy counts groups, not networks.  max_width 0 (default) never slices.
+ * A circuit that would need more than max_slices networks (default 256,
+ * at most 2^16) fails to compile with QTB_ERR_UNSUPPORTED before any slice
+ * is built, which bounds host memory and compile time per circuit.      */
+int qtb_plan_set_max_width(qtb_plan* plan, int32_t max_width, int32_t max_slices);
 
 /* Elimination-order search for networks added afterwards: 0 (default) keeps
  * the reference's greedy rule (first node of least degree); trials > 0 also

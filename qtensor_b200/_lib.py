@@ -110,7 +110,7 @@ def _declare(lib):
                                              c.c_int32, c.c_int32, P, c.POINTER(c.c_int32)]),
         'qtb_plan_add_lightcones': (c.c_int, [P, c.c_int32, P, P, P, c.c_int32, c.c_int32,
                                               c.c_int32, P, c.c_int32, c.POINTER(c.c_int32)]),
-        'qtb_plan_set_max_width': (c.c_int, [P, c.c_int32]),
+        'qtb_plan_set_max_width': (c.c_int, [P, c.c_int32, c.c_int32]),
         'qtb_plan_set_order_trials': (c.c_int, [P, c.c_int32]),
         'qtb_plan_n_networks': (c.c_int, [P, c.POINTER(c.c_int32)]),
         'qtb_plan_network_info': (c.c_int, [P, c.c_int32, c.POINTER(NetworkInfo)]),

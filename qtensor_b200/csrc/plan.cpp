@@ -400,8 +400,8 @@ static double greedy_order(int V, const std::vector<std::vector<int32_t>>& cliqu
 
 int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
                     int32_t simplify_passes, const double* params, int32_t n_params,
-                    int32_t order_trials, int32_t max_width, std::vector<Network>* outs,
-                    std::string* err) {
+                    int32_t order_trials, int32_t max_width, int32_t max_slices,
+                    std::vector<Network>* outs, std::string* err) {
     outs->clear();
     std::vector<AngleCheck> checks;
     if (n_qubits <= 0 || n_gates < 0 || (n_gates > 0 && in_gates == nullptr)) {
@@ -537,9 +537,11 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
     best_order();
     auto width = [&]() { return gdeg.empty() ? 0 : *std::max_element(gdeg.begin(), gdeg.end()); };
     while (max_width > 0 && width() >= max_width) {
-        if ((int)par.size() >= kMaxSlicedVars) {
+        if ((int)par.size() >= kMaxSlicedVars || (1ll << (par.size() + 1)) > (long long)max_slices) {
             *err = "compile: width " + std::to_string(width()) + " still >= " + std::to_string(max_width) +
-                   " after slicing " + std::to_string(kMaxSlicedVars) + " variables";
+                   " after slicing " + std::to_string(par.size()) + " variables (at most " +
+                   std::to_string(std::min<long long>(max_slices, 1ll << kMaxSlicedVars)) +
+                   " slices per circuit)";
             return QTB_ERR_UNSUPPORTED;
         }
         // distinct-neighbour degree in the graph with the sliced nodes removed
@@ -1014,7 +1016,7 @@ int qtb_plan_add_circuit(qtb_plan* plan, int32_t n_qubits, const qtb_gate* gates
     std::vector<Network> nets;
     std::string err;
     int rc = compile_circuit(n_qubits, gates, n_gates, simplify_passes, params, plan->n_params,
-                             plan->order_trials, plan->max_width, &nets, &err);
+                             plan->order_trials, plan->max_width, plan->max_slices, &nets, &err);
     if (rc) return fail(rc, err);
     std::lock_guard<std::mutex> lock(plan->mu);
     if (net_index) *net_index = (int32_t)plan->nets.size();
@@ -1058,7 +1060,7 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
             if (!rc)
                 rc = compile_circuit(nq, gates.data(), (int32_t)gates.size(), composer == 0 ? 2 : 0,
                                      params, plan->n_params, plan->order_trials, plan->max_width,
-                                     &nets[i], &errs[i]);
+                                     plan->max_slices, &nets[i], &errs[i]);
             codes[i] = rc;
         }
     };
@@ -1079,9 +1081,11 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
     return QTB_OK;
 }
 
-int qtb_plan_set_max_width(qtb_plan* plan, int32_t max_width) {
-    if (!plan || max_width < 0) return fail(QTB_ERR_ARG, "plan_set_max_width: bad arguments");
+int qtb_plan_set_max_width(qtb_plan* plan, int32_t max_width, int32_t max_slices) {
+    if (!plan || max_width < 0 || max_slices < 1)
+        return fail(QTB_ERR_ARG, "plan_set_max_width: bad arguments");
     plan->max_width = max_width;
+    plan->max_slices = max_slices;
     return QTB_OK;
 }
 

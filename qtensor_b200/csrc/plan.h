@@ -158,6 +158,7 @@ struct qtb_plan {
     int32_t n_params = 0;
     int32_t order_trials = 0;   // extra randomized greedy orders per network
     int32_t max_width = 0;      // slice circuits whose width reaches this (0 = never)
+    int32_t max_slices = 256;   // networks one sliced circuit may become
     int32_t n_groups = 0;       // circuits added (networks of a circuit share a group)
     std::vector<qtb::Network> nets;
     // global gate table, built from the networks' local entries
@@ -187,8 +188,8 @@ void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int compile_circuit(int32_t n_qubits, const qtb_gate* gates, int32_t n_gates,
                     int32_t simplify_passes, const double* params, int32_t n_params,
-                    int32_t order_trials, int32_t max_width, std::vector<Network>* outs,
-                    std::string* err);
+                    int32_t order_trials, int32_t max_width, int32_t max_slices,
+                    std::vector<Network>* outs, std::string* err);
 int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indices,
                     int32_t u, int32_t v, int32_t p, int32_t composer,
                     std::vector<qtb_gate>* gates, int32_t* n_qubits, std::string* err);

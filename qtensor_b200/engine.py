@@ -28,9 +28,9 @@ def _require_cuda():
         raise RuntimeError('qtensor_b200 needs a CUDA device; there is no CPU fallback')
 
 
-def graph_key(G, p, composer, ordering, trials=0, max_width=0):
+def graph_key(G, p, composer, ordering, trials=0, slicing=(0, 0)):
     h = hashlib.sha1()
-    h.update(repr((p, composer, ordering, trials, max_width, G.number_of_nodes())).encode())
+    h.update(repr((p, composer, ordering, trials, slicing, G.number_of_nodes())).encode())
     h.update(repr(list(G.nodes())).encode())
     h.update(repr(list(G.edges())).encode())
     return h.hexdigest()
@@ -145,7 +145,8 @@ class QAOAEnergyEngine:
     """
 
     def __init__(self, composer='default', ordering='native', device=None, threads=0,
-                 cache_size=16, order_trials=16, autotune=True, max_width=24):
+                 cache_size=16, order_trials=16, autotune=True, max_width=24,
+                 max_slices=256):
         _require_cuda()
         if ordering not in ('native', 'reference'):
             raise ValueError('ordering must be "native" or "reference"')
@@ -158,6 +159,7 @@ class QAOAEnergyEngine:
         self.order_trials = order_trials if ordering == 'native' else 0
         self.autotune = autotune
         self.max_width = max_width
+        self.max_slices = max_slices
         self._cache = {}
         self._by_id = {}        # id(G) -> (weakref, nodes, edges, p, key)
         self._lock = threading.Lock()
@@ -178,7 +180,7 @@ class QAOAEnergyEngine:
         edges = list(G.edges())
         plan = NetworkPlan(2 * p)
         plan.set_order_trials(self.order_trials)
-        plan.set_max_width(self.max_width)
+        plan.set_max_width(self.max_width, self.max_slices)
         if self.ordering == 'native':
             csr = graph_csr(G)
             index = {v: i for i, v in enumerate(csr[0])}
@@ -207,7 +209,8 @@ class QAOAEnergyEngine:
             ref, n, m, hp, key = hit
             if ref() is G and hp == p and n == G.number_of_nodes() and m == G.number_of_edges():
                 return key
-        key = graph_key(G, p, self.composer, self.ordering, self.order_trials, self.max_width)
+        key = graph_key(G, p, self.composer, self.ordering, self.order_trials,
+                        (self.max_width, self.max_slices))
         try:
             self._by_id[id(G)] = (weakref.ref(G), G.number_of_nodes(), G.number_of_edges(), p, key)
         except TypeError:

@@ -37,10 +37,11 @@ class NetworkPlan:
         self.uploaded = False
 
     # ------------------------------------------------------------ compile
-    def set_max_width(self, max_width):
+    def set_max_width(self, max_width, max_slices=256):
         """Slice circuits added afterwards whose greedy width reaches
-        ``max_width`` into 2^k networks (0 = never)."""
-        check(self._lib.qtb_plan_set_max_width(self._h, int(max_width)))
+        ``max_width`` into 2^k networks (0 = never); a circuit that would
+        need more than ``max_slices`` networks fails to compile."""
+        check(self._lib.qtb_plan_set_max_width(self._h, int(max_width), int(max_slices)))
 
     def groups(self):
         """Circuit (group) of every network."""

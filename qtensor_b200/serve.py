@@ -82,17 +82,20 @@ class QAOAServer:
 
     n_streams: requests in flight on the GPU at once; memory_budget: bytes of
     device memory the in-flight requests may hold; max_width: networks whose
-    greedy width reaches it are sliced; compile_workers: host threads
+    greedy width reaches it are sliced, into at most max_slices networks
+    per edge (a request needing more fails alone); compile_workers: host threads
     compiling requests concurrently (each also uses the C++ compiler's own
     threads)."""
 
-    def __init__(self, device=None, n_streams=4, memory_budget=16 << 30, max_width=20,
-                 composer='default', order_trials=8, compile_workers=2, compile_threads=0):
+    def __init__(self, device=None, n_streams=4, memory_budget=16 << 30, max_width=22,
+                 max_slices=256, composer='default', order_trials=8, compile_workers=2,
+                 compile_threads=0):
         if not torch.cuda.is_available():
             raise RuntimeError('QAOAServer needs a CUDA device; there is no CPU fallback')
         self.device = torch.device('cuda', torch.cuda.current_device() if device is None else device)
         self.cid = composer_id(composer)
         self.max_width = max_width
+        self.max_slices = max_slices
         self.order_trials = order_trials
         self.compile_threads = compile_threads
         _lib.check(_lib.lib().qtb_init(self.device.index))
@@ -143,7 +146,7 @@ class QAOAServer:
             torch.cuda.set_device(self.device)
             plan = NetworkPlan(2 * p)
             plan.set_order_trials(self.order_trials)
-            plan.set_max_width(self.max_width)
+            plan.set_max_width(self.max_width, self.max_slices)
             plan.add_lightcones(csr, edges, p, self.cid, params, self.compile_threads)
             job = _Compiled()
             job.future, job.plan, job.params = fut, plan, params
