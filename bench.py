@@ -393,6 +393,23 @@ def run_b200(args):
     barrier()
     clk = clocks.stop()
 
+    # ---- the plain path: one bucket-kernel launch per bucket over the same
+    # plans (the drop-in backend's kernel), a few steps
+    plain_steps = 3
+    cg.params.copy_(params_dev[0])
+    cg.launch_plain()
+    plain_ms = []
+    for i in range(plain_steps):
+        flush.fill_(float(i))
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        cg.params.copy_(params_dev[args.warmup + i])
+        cg.launch_plain()
+        e.record(stream)
+        e.synchronize()
+        plain_ms.append(s.elapsed_time(e))
+    plain_ms_step = sum(plain_ms) / plain_steps
+
     errors = oracle_error(eng, G, p) if rank == 0 else None
     serving = None
     if rank == 0 and world == 1 and args.serving_requests > 0:
@@ -440,6 +457,13 @@ def run_b200(args):
                     'd2h_bytes_per_step': 8, 'ms_per_step': e2e_total / args.steps},
             'clocks': clk,
             'error_vs_oracle': errors,
+            'plain': {'value': stats['edges'] / (plain_ms_step / 1e3), 'unit': UNIT,
+                      'ms_per_step': plain_ms_step, 'steps': plain_steps,
+                      'bucket_launches_per_step': stats['ops'],
+                      'what': 'same plans, one qtb_bucket_kernel launch per bucket (the '
+                              'drop-in process_bucket kernel), networks in sequence, '
+                              'intermediates in global memory, complex64',
+                      'batched_over_plain': value / (world * stats['edges'] / (plain_ms_step / 1e3))},
             'serving': serving,
             # every kernel of a step is a qtb_network_kernel class launch (gate
             # table and energy reduction are fused into it)

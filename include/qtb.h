@@ -203,6 +203,20 @@ int qtb_plan_scratch_bytes(const qtb_plan* plan, int32_t first, int32_t count,
 int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* params_dev,
                  void* terms_dev, double* energy_dev, void* scratch_dev, void* stream);
 
+/* The plain path over the same compiled plan: every bucket of every network
+ * is one launch of the qtb_bucket_c64 kernel (the drop-in backend's
+ * process_bucket, qtensor/ProcessingFrameworks.py:29-31, as called by
+ * bucket_elimination in QtreeSimulator.simulate_batch, Simulate.py:90-94),
+ * networks one after another, intermediates in scratch_dev (global memory,
+ * qtb_plan_plain_scratch_bytes(), reused by every network), the gate table
+ * in global memory, then the same fp64 compensated energy as qtb_plan_run.
+ * Results equal qtb_plan_run's within complex64 rounding.                 */
+int qtb_plan_plain_scratch_bytes(const qtb_plan* plan, int32_t first, int32_t count,
+                                 size_t* bytes);
+int qtb_plan_run_plain(qtb_plan* plan, int32_t first, int32_t count, const double* params_dev,
+                       void* terms_dev, double* energy_dev, void* scratch_dev,
+                       size_t scratch_bytes, void* stream);
+
 /* Schedule and block-size autotuning: when enabled, the first qtb_plan_run
  * of a network range (outside stream capture) times every launch class of
  * the class schedule (one CTA per network, networks grouped by shared

@@ -30,7 +30,8 @@ EXPORTS = (
     'qtb_plan_n_networks',
     'qtb_plan_network_info', 'qtb_plan_network_peo', 'qtb_plan_check_params',
     'qtb_plan_export', 'qtb_plan_table_elems', 'qtb_plan_upload',
-    'qtb_plan_scratch_bytes', 'qtb_plan_run', 'qtb_plan_set_autotune',
+    'qtb_plan_scratch_bytes', 'qtb_plan_run', 'qtb_plan_plain_scratch_bytes',
+    'qtb_plan_run_plain', 'qtb_plan_set_autotune',
     'qtb_plan_last_launch_config', 'qtb_plan_device_bytes', 'qtb_plan_device_status',
     'qtb_plan_set_timing', 'qtb_plan_collect_timing', 'qtb_plan_run_noalloc',
 )
@@ -128,6 +129,8 @@ def _declare(lib):
         'qtb_plan_set_timing': (c.c_int, [P, c.c_int32]),
         'qtb_plan_collect_timing': (c.c_int, [P, c.POINTER(c.c_double), c.POINTER(c.c_int64)]),
         'qtb_plan_run_noalloc': (c.c_int, [P, c.c_int32, c.c_int32, P, P, P, P]),
+        'qtb_plan_plain_scratch_bytes': (c.c_int, [P, c.c_int32, c.c_int32, c.POINTER(c.c_size_t)]),
+        'qtb_plan_run_plain': (c.c_int, [P, c.c_int32, c.c_int32, P, P, P, P, c.c_size_t, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -1150,6 +1150,103 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
     return QTB_OK;
 }
 
+// ------------------------------------------------- plain per-bucket run
+}  // extern "C"
+
+namespace qtb {
+
+// Energy of a plain run: one CTA, the same compensated sum as the executor.
+__global__ void __launch_bounds__(256) qtb_energy_kernel(const float2* terms, uint32_t n,
+                                                         double n_groups, double* energy) {
+    reduce_energy(terms, n, n_groups, energy);
+}
+
+// Circuits (groups) of networks [first, first+count): networks of a circuit
+// are contiguous, so this counts group changes.
+static int32_t count_groups(const qtb_plan* plan, int32_t first, int32_t count) {
+    int32_t groups = 0, last = -1;
+    for (int32_t i = first; i < first + count; ++i)
+        if (plan->nets[i].info.group != last) {
+            last = plan->nets[i].info.group;
+            ++groups;
+        }
+    return groups;
+}
+
+}  // namespace qtb
+
+extern "C" {
+
+int qtb_plan_plain_scratch_bytes(const qtb_plan* plan, int32_t first, int32_t count, size_t* bytes) {
+    if (!plan || !bytes) return fail(QTB_ERR_ARG, "plan_plain_scratch_bytes: null argument");
+    if (first < 0 || count < 1 || first + count > (int32_t)plan->nets.size())
+        return fail(QTB_ERR_ARG, "plan_plain_scratch_bytes: network range out of bounds");
+    size_t elems = 0;
+    for (int32_t i = first; i < first + count; ++i)
+        elems = std::max<size_t>(elems, (size_t)plan->nets[i].info.arena_elems);
+    *bytes = 8 * elems;
+    return QTB_OK;
+}
+
+int qtb_plan_run_plain(qtb_plan* plan, int32_t first, int32_t count, const double* params_dev,
+                       void* terms_dev, double* energy_dev, void* scratch_dev, size_t scratch_bytes,
+                       void* stream) {
+    if (!plan || !terms_dev || (plan->n_params > 0 && !params_dev))
+        return fail(QTB_ERR_ARG, "plan_run_plain: null argument");
+    if (!plan->uploaded) return fail(QTB_ERR_ARG, "plan_run_plain: plan not uploaded");
+    if (first < 0 || count < 1 || first + count > (int32_t)plan->dnets.size())
+        return fail(QTB_ERR_ARG, "plan_run_plain: network range out of bounds");
+    size_t need = 0;
+    int r = qtb_plan_plain_scratch_bytes(plan, first, count, &need);
+    if (r) return r;
+    if (need > 0 && (!scratch_dev || scratch_bytes < need))
+        return fail(QTB_ERR_ARG, "plan_run_plain: scratch smaller than qtb_plan_plain_scratch_bytes");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int n_entries = (int)plan->entries.size();
+    if (n_entries > 0) {
+        qtb_table_kernel<<<(n_entries + 127) / 128, 128, 0, st>>>(
+            static_cast<const DevEntry*>(plan->dev.entries), n_entries,
+            static_cast<const DevTerm*>(plan->dev.terms), params_dev,
+            static_cast<float2*>(plan->dev.table));
+        QTB_CUDA(cudaGetLastError());
+    }
+    const float2* table = static_cast<const float2*>(plan->dev.table);
+    float2* arena = static_cast<float2*>(scratch_dev);
+    float2* terms = static_cast<float2*>(terms_dev);
+    // networks run one after another on st, so they share one arena
+    for (int32_t i = first; i < first + count; ++i) {
+        const DevNet& net = plan->dnets[i];
+        for (uint32_t o = 0; o < net.n_ops; ++o) {
+            const DevOp& op = plan->dops[net.op_begin + o];
+            if (op.k < 1 || op.k > QTB_MAX_BUCKET_INPUTS)
+                return fail(QTB_ERR_UNSUPPORTED, "plan_run_plain: bucket of more than 16 tensors");
+            BucketArgs a{};
+            for (int t = 0; t < op.k; ++t) {
+                const DevIn& in = plan->dins[op.in_begin + t];
+                a.in[t] = (in.src & kSrcTable) ? table + (in.src & ~kSrcTable) : arena + in.src;
+                a.mask[t] = in.mask;
+            }
+            a.out = arena + op.dst;
+            a.k = op.k;
+            a.sum = op.sum;
+            a.w = op.u - op.sum;
+            const uint64_t n_out = 1ull << a.w;
+            const uint64_t blocks = std::min<uint64_t>((n_out + 255) / 256, 148ull * 16);
+            qtb_bucket_kernel<<<(unsigned)blocks, 256, 0, st>>>(a);
+            QTB_CUDA(cudaGetLastError());
+        }
+        const float2* res = (net.result_src & kSrcTable) ? table + (net.result_src & ~kSrcTable)
+                                                         : arena + net.result_src;
+        QTB_CUDA(cudaMemcpyAsync(terms + (i - first), res, sizeof(float2), cudaMemcpyDeviceToDevice, st));
+    }
+    if (energy_dev) {
+        qtb_energy_kernel<<<1, 256, 0, st>>>(terms, (uint32_t)count,
+                                             (double)count_groups(plan, first, count), energy_dev);
+        QTB_CUDA(cudaGetLastError());
+    }
+    return QTB_OK;
+}
+
 // ------------------------------------------------- allocation-free run
 }  // extern "C"
 

@@ -56,6 +56,7 @@ class CompiledGraph:
         self.scratch = (torch.empty(max(nbytes, 8), dtype=torch.uint8, device=device)
                         if nbytes else None)
         self._infos = None
+        self._plain_scratch = None
         # host side of the captured call: pinned angles in, pinned energy out
         self.host_params = torch.zeros(2 * p, dtype=torch.float64, pin_memory=True)
         self.host_energy = torch.zeros(1, dtype=torch.float64, pin_memory=True)
@@ -88,6 +89,18 @@ class CompiledGraph:
         stream = torch.cuda.current_stream(self.device) if stream is None else stream
         self.plan.run(0, self.n_networks, self.params if params_dev is None else params_dev,
                       self.terms, self.energy, self.scratch, stream.cuda_stream)
+
+    def launch_plain(self, params_dev=None, stream=None):
+        """The plain path, asynchronously: one bucket-kernel launch per bucket
+        (the drop-in backend's process_bucket), networks in sequence,
+        intermediates in global memory; results in ``self.terms`` and
+        ``self.energy`` as with ``launch``."""
+        stream = torch.cuda.current_stream(self.device) if stream is None else stream
+        if self._plain_scratch is None:
+            nbytes = self.plan.plain_scratch_bytes(0, self.n_networks)
+            self._plain_scratch = torch.empty(max(nbytes, 8), dtype=torch.uint8, device=self.device)
+        self.plan.run_plain(0, self.n_networks, self.params if params_dev is None else params_dev,
+                            self.terms, self.energy, self._plain_scratch, stream.cuda_stream)
 
     def edge_terms(self):
         """Per-edge amplitudes of the last run (slices summed), complex128."""
@@ -235,22 +248,36 @@ class QAOAEnergyEngine:
         return np.concatenate([gamma, beta])
 
     # ------------------------------------------------------------ run
-    def energy_expectation(self, G, gamma, beta):
-        """Expected MaxCut value of the depth-p QAOA state (p = len(gamma))."""
+    def energy_expectation(self, G, gamma, beta, path='batched'):
+        """Expected MaxCut value of the depth-p QAOA state (p = len(gamma)).
+
+        path: ``'batched'`` (whole-network executor, one graph replay) or
+        ``'plain'`` (one bucket-kernel launch per bucket)."""
         gamma = np.asarray(gamma, dtype=np.float64).ravel()
         p = len(gamma)
         cg = self.compile(G, p, gamma, beta)
-        return cg.energy_of(self._params(p, gamma, beta))
+        if path == 'batched':
+            return cg.energy_of(self._params(p, gamma, beta))
+        self._launch(cg, p, gamma, beta, path)
+        return float(cg.energy.cpu()[0])
 
-    def edge_terms(self, G, gamma, beta):
+    def edge_terms(self, G, gamma, beta, path='batched'):
         """``<Z_u Z_v>`` of every edge (numpy complex, edge order of ``G.edges()``;
         sliced edges are summed over their slices)."""
         gamma = np.asarray(gamma, dtype=np.float64).ravel()
         p = len(gamma)
         cg = self.compile(G, p, gamma, beta)
-        cg.params.copy_(torch.from_numpy(self._params(p, gamma, beta)))
-        cg.launch()
+        self._launch(cg, p, gamma, beta, path)
         return cg.edge_terms()
+
+    def _launch(self, cg, p, gamma, beta, path):
+        if path not in ('batched', 'plain'):
+            raise ValueError('path must be "batched" or "plain"')
+        cg.params.copy_(torch.from_numpy(self._params(p, gamma, beta)))
+        if path == 'batched':
+            cg.launch()
+        else:
+            cg.launch_plain()
 
     def check_device(self, cg):
         """Raise if a kernel of ``cg`` reported an error status (synchronises)."""

@@ -137,6 +137,23 @@ class NetworkPlan:
                                      ptr(terms_dev), ptr(energy_dev), ptr(scratch_dev),
                                      ctypes.c_void_p(int(stream))))
 
+    def plain_scratch_bytes(self, first=0, count=None):
+        count = len(self) - first if count is None else count
+        n = ctypes.c_size_t()
+        check(self._lib.qtb_plan_plain_scratch_bytes(self._h, int(first), int(count),
+                                                     ctypes.byref(n)))
+        return n.value
+
+    def run_plain(self, first, count, params_dev, terms_dev, energy_dev=None, scratch_dev=None,
+                  stream=0):
+        """The plain path: one bucket kernel launch per bucket of networks
+        [first, first+count), intermediates in ``scratch_dev`` (global
+        memory of ``plain_scratch_bytes``), asynchronous on ``stream``."""
+        nbytes = 0 if scratch_dev is None else scratch_dev.numel() * scratch_dev.element_size()
+        check(self._lib.qtb_plan_run_plain(self._h, int(first), int(count), ptr(params_dev),
+                                           ptr(terms_dev), ptr(energy_dev), ptr(scratch_dev),
+                                           nbytes, ctypes.c_void_p(int(stream))))
+
     def set_autotune(self, enable):
         """Time every launch class with 64..1024 threads per CTA on the first
         run of a range and keep the fastest."""

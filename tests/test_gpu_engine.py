@@ -109,3 +109,21 @@ def test_engine_sliced(cuda_device, name, max_width):
     assert cg.n_networks > cg.n_edges
     assert max(i['treewidth'] for i in cg.infos) < max_width
     _check(eng, name)
+
+
+@pytest.mark.parametrize('name,max_width', [('cfg1_default', 24), ('cfg2', 24), ('cfg4', 24),
+                                            ('cfg2', 9)])
+def test_plain_path_matches_batched_and_reference(cuda_device, name, max_width):
+    """The plain path (one bucket-kernel launch per bucket over the same
+    compiled plans) gives the reference's edge terms and energy, and the
+    batched executor's within complex64 rounding."""
+    eng = _engine(max_width=max_width)
+    G, w = golden_graph(name)
+    plain = eng.edge_terms(G, w['gamma'], w['beta'], path='plain')
+    batched = eng.edge_terms(G, w['gamma'], w['beta'])
+    ref = np.array([complex(*t) for t in w['terms']])
+    assert np.max(np.abs(plain - ref)) < TOL
+    assert np.max(np.abs(plain - batched)) < TOL
+    E = eng.energy_expectation(G, w['gamma'], w['beta'], path='plain')
+    assert abs(E - w['energy']) <= TOL * abs(w['energy'])
+    assert eng.compile(G, len(w['gamma'])).plan.device_status() == 0
