@@ -57,7 +57,7 @@ def parse():
     ap.add_argument('--nodes', type=int, default=1000)
     ap.add_argument('--p', type=int, default=3)
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--serving-requests', type=int, default=64,
+    ap.add_argument('--serving-requests', type=int, default=128,
                     help='requests of the serving run (0 skips it)')
     ap.add_argument('--serving-rate', type=float, default=20.0,
                     help='Poisson arrival rate of the serving run, requests/s')

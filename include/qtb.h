@@ -228,7 +228,9 @@ int qtb_plan_run_plain(qtb_plan* plan, int32_t first, int32_t count, const doubl
 int qtb_plan_set_autotune(qtb_plan* plan, int32_t enable);
 /* Launch classes of the plan's most recent run: 4 ints per class (networks,
  * threads per CTA, dynamic shared memory bytes, flags: 1 = shared-memory
- * arena, 2 = persistent launch taking networks from a queue).             */
+ * arena, 2 = persistent launch taking networks from a queue, 4 = a wave of
+ * wide networks contracted by the whole GPU step by step, arenas in
+ * scratch).                                                               */
 int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32_t* n_classes);
 
 /* Device memory the plan holds once uploaded (images, gate table, job

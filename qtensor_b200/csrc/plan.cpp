@@ -105,7 +105,7 @@ uint64_t encode_runs(uint32_t mask, uint32_t w) {
             first_start = bit;
             first_len = len;
         }
-        runs |= (uint64_t)(bit | (len << 5) | (dst << 10)) << (15 * n);
+        runs |= (uint64_t)(bit | (len << 5)) << (10 * n);
         ++n;
         dst += len;
         bit += len;
@@ -536,12 +536,18 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
     };
     best_order();
     auto width = [&]() { return gdeg.empty() ? 0 : *std::max_element(gdeg.begin(), gdeg.end()); };
+    // variables that may still be sliced within max_slices
+    int slice_budget = 0;
+    while (slice_budget < kMaxSlicedVars && (2ll << slice_budget) <= (long long)max_slices) ++slice_budget;
     while (max_width > 0 && width() >= max_width) {
-        if ((int)par.size() >= kMaxSlicedVars || (1ll << (par.size() + 1)) > (long long)max_slices) {
+        // removing one variable lowers the treewidth by at most one, so a
+        // width more than twice the remaining budget above the target is
+        // out of reach: fail now instead of after the whole budget
+        const int remaining = slice_budget - (int)par.size();
+        if (remaining <= 0 || width() - max_width + 1 > 2 * remaining) {
             *err = "compile: width " + std::to_string(width()) + " still >= " + std::to_string(max_width) +
                    " after slicing " + std::to_string(par.size()) + " variables (at most " +
-                   std::to_string(std::min<long long>(max_slices, 1ll << kMaxSlicedVars)) +
-                   " slices per circuit)";
+                   std::to_string(1ll << slice_budget) + " slices per circuit)";
             return QTB_ERR_UNSUPPORTED;
         }
         // distinct-neighbour degree in the graph with the sliced nodes removed
@@ -720,8 +726,11 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
         if (!result.table) ops[result.id].consumer_level = max_level + 1;
         std::vector<int32_t> by_level(ops.size());
         std::iota(by_level.begin(), by_level.end(), 0);
-        std::stable_sort(by_level.begin(), by_level.end(),
-                         [&](int32_t x, int32_t y) { return ops[x].level < ops[y].level; });
+        // within a level the widest op first: every op of a phase then starts
+        // at a multiple of its own (power-of-two) size
+        std::stable_sort(by_level.begin(), by_level.end(), [&](int32_t x, int32_t y) {
+            return ops[x].level != ops[y].level ? ops[x].level < ops[y].level : ops[x].w > ops[y].w;
+        });
         struct Live { uint32_t off, size; int32_t end; };
         std::vector<Live> active;
         uint32_t arena = 0, max_elems = 1;
@@ -1049,11 +1058,12 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
     std::vector<int> codes(n_edges, 0);
     std::vector<std::string> errs(n_edges);
     std::atomic<int32_t> next{0};
+    std::atomic<bool> failed{false};   // one failing edge fails the call: stop early
     auto worker = [&]() {
         std::vector<qtb_gate> gates;
         for (;;) {
             const int32_t i = next.fetch_add(1);
-            if (i >= n_edges) break;
+            if (i >= n_edges || failed.load(std::memory_order_relaxed)) break;
             int32_t nq = 0;
             int rc = build_lightcone(n_nodes, indptr, indices, edges[2 * i], edges[2 * i + 1], p,
                                      composer, &gates, &nq, &errs[i]);
@@ -1062,6 +1072,7 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
                                      params, plan->n_params, plan->order_trials, plan->max_width,
                                      plan->max_slices, &nets[i], &errs[i]);
             codes[i] = rc;
+            if (rc) failed.store(true, std::memory_order_relaxed);
         }
     };
     int nt = n_threads > 0 ? n_threads : (int)std::thread::hardware_concurrency();

@@ -31,15 +31,16 @@ struct DevOp {
 // contiguous runs; bits 60..62 of `runs` hold the run count n.
 //   n <= 1: bits 0..31 = length mask of the run, bits 32..36 = its start
 //           (the gather is (j >> start) & lenmask; 0 when n == 0);
-//   2 <= n <= kMaxRuns: run r (15 bits at 15*r) = start | len << 5 |
-//           dst << 10 moves bits [start, start+len) of j to [dst, ...);
+//   2 <= n <= kMaxRuns: run r (10 bits at 10*r) = start | len << 5 moves
+//           bits [start, start+len) of j to the next free operand bits
+//           (runs in increasing start order, packed from bit 0 up);
 //   n == kRunsFallback: more runs than kMaxRuns, gather bit by bit.
 struct DevIn {
     uint32_t mask;      // bit (u-1-v) set <=> union variable v is an axis
     uint32_t src;       // arena offset, or kSrcTable | gate-table offset
     uint64_t runs;
 };
-constexpr int kMaxRuns = 4;
+constexpr int kMaxRuns = 6;
 constexpr uint64_t kRunsFallback = 7;
 
 // Ops of one dependency level; a barrier follows every phase.  In a network

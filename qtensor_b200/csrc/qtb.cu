@@ -53,13 +53,14 @@ __device__ __forceinline__ uint32_t gather_bits(uint32_t j, const DevIn& d, uint
     const uint32_t n = (uint32_t)(d.runs >> 60);
     if (n <= 1u) return (j >> ((uint32_t)(d.runs >> 32) & 31u)) & (uint32_t)d.runs;
     if (n == (uint32_t)kRunsFallback) return pext32(j, d.mask & low_mask);
-    uint32_t off = 0;
+    uint32_t off = 0, dst = 0;
 #pragma unroll
     for (uint32_t r = 0; r < (uint32_t)kMaxRuns; ++r) {
         if (r < n) {
-            const uint32_t rr = (uint32_t)(d.runs >> (15 * r)) & 0x7fffu;
-            const uint32_t start = rr & 31u, len = (rr >> 5) & 31u, dst = rr >> 10;
+            const uint32_t rr = (uint32_t)(d.runs >> (10 * r)) & 0x3ffu;
+            const uint32_t start = rr & 31u, len = rr >> 5;
             off |= ((j >> start) & ((1u << len) - 1u)) << dst;
+            dst += len;
         }
     }
     return off;
@@ -192,6 +193,7 @@ constexpr int kStatusArena = 1;        // network arena larger than the launch's
 constexpr int kStatusStageTimeout = 2; // a staging copy did not complete in time
 constexpr int kStatusBlob = 4;         // network blob larger than the launch's capacity
 constexpr int kStatusQueue = 8;        // persistent launch without a job queue
+constexpr int kStatusWideTimeout = 16; // a wide-network step waited too long for its predecessor
 constexpr uint32_t kStageSpinLimit = 1u << 26;
 constexpr uint32_t kSmemTableLimitElems = 2048;   // 16 KB of gate table per CTA
 
@@ -473,6 +475,316 @@ __global__ void __launch_bounds__(kPersistent ? 512 : 1024) qtb_network_kernel(
     }
 }
 
+// ----------------------------------------------------------------- K4
+// Wide networks (arenas too large for shared memory) are contracted by the
+// whole GPU at once.  The networks of a wave advance together, one step per
+// elimination phase: step s holds phase s of every wave network that has
+// one, its elements concatenated (segments) and cut into tiles.  CTAs claim
+// tiles in order from a queue; a tile of step s starts once every tile of
+// step s-1 has finished.  A CTA only ever waits for tiles that were claimed
+// before its own, i.e. by CTAs that are running, so the scheme needs no
+// co-residency guarantee (no cooperative launch), and every wait is bounded.
+struct WideNet {
+    const DevNetRun* run;
+    float2* term;
+    uint64_t arena_off;     // complex64 elements into the wave's arenas
+    uint64_t pad;
+};
+
+struct WideStep {
+    uint32_t seg_begin;     // into the wave's segments
+    uint32_t n_segs;
+    uint32_t tile_begin;    // first tile of the step
+    uint32_t n_tiles;
+    uint32_t total_elems;
+    uint32_t tile_elems;    // elements per tile of this step (a multiple of 4 x block size)
+    uint32_t pad[2];
+};
+
+struct WideSeg {
+    uint32_t net;           // wave-local network
+    uint32_t elem_begin;    // first element of the network's phase within the step
+};
+
+struct WideArgs {
+    const WideNet* nets;
+    const WideStep* steps;
+    const WideSeg* segs;
+    unsigned int* counters;   // [0] next tile, [1 + s] finished tiles of step s (zeroed per launch)
+    float2* arenas;
+    uint32_t n_nets;
+    uint32_t n_steps;
+    uint32_t n_tiles;         // tile n_tiles (the last one) writes the wave's terms
+};
+
+static_assert(sizeof(WideNet) == 32, "WideNet layout");
+static_assert(sizeof(WideStep) == 32, "WideStep layout");
+constexpr uint32_t kWideSpinLimit = 1u << 24;
+constexpr int kWideThreads = 256;
+constexpr uint32_t kWideBatch = 4;                                  // elements per thread in flight
+constexpr uint32_t kWideMinTile = kWideBatch * kWideThreads;         // 1024
+constexpr uint32_t kWideMaxTile = 8 * kWideMinTile;
+
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ DevIn ldg_in(const DevIn* p) {
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(p));
+    DevIn d;
+    d.mask = v.x;
+    d.src = v.y;
+    d.runs = (uint64_t)v.z | ((uint64_t)v.w << 32);
+    return d;
+}
+
+__device__ __forceinline__ DevOp ldg_op(const DevOp* p) {
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(p));
+    DevOp o;
+    o.u = (uint8_t)(v.x & 0xffu);
+    o.sum = (uint8_t)((v.x >> 8) & 0xffu);
+    o.k = (uint8_t)((v.x >> 16) & 0xffu);
+    o.pad = 0;
+    o.dst = v.y;
+    o.elem_begin = v.z;
+    o.in_begin = v.w;
+    return o;
+}
+
+// compute_element for a network whose arena and plan live in global memory
+// and are written by other CTAs: arena reads bypass L1 (ld.cg), plan and
+// gate-table reads go through the read-only path.
+__device__ __forceinline__ void compute_element_wide(const DevOp& op, uint32_t j, const DevIn* ins,
+                                                     const float2* __restrict__ table,
+                                                     float2* __restrict__ arena) {
+    const uint32_t w = op.u - op.sum;
+    const uint32_t low = (1u << w) - 1u;
+    const DevIn* in = ins + op.in_begin;
+    float2 p0 = make_float2(1.f, 0.f), p1 = make_float2(1.f, 0.f);
+    for (uint32_t t0 = 0; t0 < op.k; t0 += 4) {
+        DevIn d[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+            if (t0 + t < op.k) d[t] = ldg_in(in + t0 + t);
+        float2 x0[4], x1[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            if (t0 + t < op.k) {
+                const uint32_t off = gather_bits(j, d[t], low);
+                const bool tab = d[t].src & kSrcTable;
+                const float2* base = tab ? table + (d[t].src & ~kSrcTable) : arena + d[t].src;
+                x0[t] = tab ? __ldg(base + off) : __ldcg(base + off);
+                x1[t] = x0[t];
+                if (op.sum && ((d[t].mask >> w) & 1u)) {
+                    const uint32_t stride = 1u << (__popc(d[t].mask) - 1);
+                    x1[t] = tab ? __ldg(base + off + stride) : __ldcg(base + off + stride);
+                }
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            if (t0 + t < op.k) {
+                p0 = (t0 + t == 0) ? x0[t] : cmul(p0, x0[t]);
+                p1 = (t0 + t == 0) ? x1[t] : cmul(p1, x1[t]);
+            }
+        }
+    }
+    arena[op.dst + j] = op.sum ? make_float2(p0.x + p1.x, p0.y + p1.y) : p0;
+}
+
+// Four elements j, j + 256, j + 512, j + 768 of one op at once, bits 8 and
+// 9 of j zero: the four differ from j only in those bits, so each operand
+// offset is the gathered offset of j plus the gathered bits 8 and 9 (one
+// full gather per operand, not four), and the loads of two operands for all
+// four elements are issued together (eight L2 requests in flight per thread).
+__device__ __forceinline__ void compute_elements_wide4(const DevOp& op, uint32_t j, const DevIn* ins,
+                                                       const float2* __restrict__ table,
+                                                       float2* __restrict__ arena) {
+    const uint32_t w = op.u - op.sum;
+    const uint32_t low = (1u << w) - 1u;
+    const DevIn* in = ins + op.in_begin;
+    float2 p0[kWideBatch], p1[kWideBatch];
+#pragma unroll
+    for (uint32_t e = 0; e < kWideBatch; ++e) p0[e] = p1[e] = make_float2(1.f, 0.f);
+    for (uint32_t t0 = 0; t0 < op.k; t0 += 2) {
+        DevIn d[2];
+#pragma unroll
+        for (int t = 0; t < 2; ++t)
+            if (t0 + t < op.k) d[t] = ldg_in(in + t0 + t);
+        float2 x0[2][kWideBatch], x1[2][kWideBatch];
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+            if (t0 + t < op.k) {
+                const bool tab = d[t].src & kSrcTable;
+                const float2* base = tab ? table + (d[t].src & ~kSrcTable) : arena + d[t].src;
+                const bool has_sum = op.sum && ((d[t].mask >> w) & 1u);
+                const uint32_t stride_s = has_sum ? 1u << (__popc(d[t].mask) - 1) : 0u;
+                const uint32_t m = d[t].mask & low;
+                const uint32_t b8 = ((m >> 8) & 1u) << __popc(m & 0xffu);
+                const uint32_t b9 = ((m >> 9) & 1u) << __popc(m & 0x1ffu);
+                uint32_t off[kWideBatch];
+                off[0] = gather_bits(j, d[t], low);
+                off[1] = off[0] + b8;
+                off[2] = off[0] + b9;
+                off[3] = off[0] + b8 + b9;
+#pragma unroll
+                for (uint32_t e = 0; e < kWideBatch; ++e) {
+                    x0[t][e] = tab ? __ldg(base + off[e]) : __ldcg(base + off[e]);
+                    x1[t][e] = has_sum ? (tab ? __ldg(base + off[e] + stride_s) : __ldcg(base + off[e] + stride_s))
+                                       : x0[t][e];
+                }
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+            if (t0 + t < op.k) {
+#pragma unroll
+                for (uint32_t e = 0; e < kWideBatch; ++e) {
+                    p0[e] = cmul(p0[e], x0[t][e]);
+                    p1[e] = cmul(p1[e], x1[t][e]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (uint32_t e = 0; e < kWideBatch; ++e)
+        arena[op.dst + j + e * 256u] = op.sum ? make_float2(p0[e].x + p1[e].x, p0[e].y + p1[e].y) : p0[e];
+}
+
+__global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArgs w, const RunArgs a) {
+    __shared__ uint32_t s_tile;
+    __shared__ int s_ok, s_last;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(w.counters, 1u);
+        __syncthreads();
+        const uint32_t t = s_tile;
+        if (t > w.n_tiles) break;
+        uint32_t s = w.n_steps;   // the result tile follows the last step
+        if (t < w.n_tiles) {
+            uint32_t lo = 0, hi = w.n_steps - 1u;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1u) >> 1;
+                if (__ldg(&w.steps[mid].tile_begin) <= t) lo = mid;
+                else hi = mid - 1u;
+            }
+            s = lo;
+        }
+        if (threadIdx.x == 0) {
+            s_ok = 1;
+            if (s > 0) {
+                const uint32_t need = __ldg(&w.steps[s - 1].n_tiles);
+                uint32_t it = 0;
+                while (ld_acquire(w.counters + s) < need) {
+                    if (++it > kWideSpinLimit) {
+                        atomicOr(a.status, kStatusWideTimeout);
+                        s_ok = 0;
+                        break;
+                    }
+                    if (it > 16) __nanosleep(128);
+                }
+            }
+            __threadfence();
+        }
+        __syncthreads();
+        if (!s_ok) return;
+        if (t == w.n_tiles) {
+            // every step is done: the wave's terms, then the run's energy if
+            // this wave finished the run's last networks
+            for (uint32_t n = threadIdx.x; n < w.n_nets; n += blockDim.x) {
+                const WideNet wn = w.nets[n];
+                const DevNetRun net = *wn.run;
+                const float2* arena = w.arenas + wn.arena_off;
+                *wn.term = (net.result_src & kSrcTable) ? __ldg(a.gtable + (net.result_src & ~kSrcTable))
+                                                        : __ldcg(arena + net.result_src);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                s_last = 0;
+                if (a.energy) {
+                    __threadfence();
+                    s_last = atomicAdd(a.done, w.n_nets) == a.total_jobs - w.n_nets;
+                }
+            }
+            __syncthreads();
+            if (s_last) {
+                __threadfence();
+                reduce_energy(a.terms, a.total_jobs, a.energy_groups, a.energy);
+                if (threadIdx.x == 0) *a.done = 0u;
+            }
+            break;
+        }
+        const WideStep st = w.steps[s];
+        const uint32_t e0 = (t - st.tile_begin) * st.tile_elems;
+        const uint32_t e1 = min(e0 + st.tile_elems, st.total_elems);
+        // per-thread cache of the current segment and op
+        uint32_t seg_lo = 1u, seg_hi = 0u, op_lo = 1u, op_hi = 0u, ph_total = 0u;
+        const unsigned char* blob = nullptr;
+        const DevIn* ins = nullptr;
+        const DevOp* ops = nullptr;
+        const uint16_t* chunk = nullptr;
+        float2* arena = nullptr;
+        DevOp op{};
+        uint32_t op_last = 0;
+        const uint32_t bd = blockDim.x;
+        for (uint32_t g = e0 + threadIdx.x; g < e1;) {
+            if (g < seg_lo || g >= seg_hi) {
+                uint32_t lo = st.seg_begin, hi = st.seg_begin + st.n_segs - 1u;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi + 1u) >> 1;
+                    if (__ldg(&w.segs[mid].elem_begin) <= g) lo = mid;
+                    else hi = mid - 1u;
+                }
+                const WideSeg sg = w.segs[lo];
+                seg_lo = sg.elem_begin;
+                seg_hi = lo + 1u < st.seg_begin + st.n_segs ? __ldg(&w.segs[lo + 1u].elem_begin) : st.total_elems;
+                const WideNet wn = w.nets[sg.net];
+                const DevNetRun net = *wn.run;
+                blob = reinterpret_cast<const unsigned char*>(a.blobs + net.blob_off16);
+                const DevPhase ph = reinterpret_cast<const DevPhase*>(blob)[s];
+                ph_total = ph.total_elems;
+                ops = reinterpret_cast<const DevOp*>(blob + net.n_phases * sizeof(DevPhase));
+                ins = reinterpret_cast<const DevIn*>(blob + net.ins_off);
+                chunk = reinterpret_cast<const uint16_t*>(blob + ph.chunk_off);
+                arena = w.arenas + wn.arena_off;
+                op_last = ph.op_first + ph.op_count - 1u;
+                op_lo = 1u;
+                op_hi = 0u;
+            }
+            const uint32_t l = g - seg_lo;
+            if (l >= ph_total) {   // padding between segments
+                g += bd;
+                continue;
+            }
+            if (l < op_lo || l >= op_hi) {
+                uint32_t oi = __ldg(chunk + l / kChunkElems);
+                op = ldg_op(ops + oi);
+                while (l >= op.elem_begin + (1u << (op.u - op.sum)) && oi < op_last) op = ldg_op(ops + ++oi);
+                op_lo = op.elem_begin;
+                op_hi = op.elem_begin + (1u << (op.u - op.sum));
+            }
+            // four elements of the same op that differ only in bits 8 and 9
+            // of the op index (the common case in wide phases: tiles,
+            // segments and ops start at multiples of 1024)
+            const uint32_t j = l - op.elem_begin;
+            if (bd == 256u && (j & 0x300u) == 0u && g + (kWideBatch - 1) * bd < min(e1, seg_hi) &&
+                l + (kWideBatch - 1) * bd < op_hi) {
+                compute_elements_wide4(op, j, ins, a.gtable, arena);
+                g += kWideBatch * bd;
+            } else {
+                compute_element_wide(op, j, ins, a.gtable, arena);
+                g += bd;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(w.counters + 1 + s, 1u);
+        }
+    }
+}
+
 // ----------------------------------------------------------------- host
 static int cuda_fail(cudaError_t e, const char* what) {
     return fail(QTB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -526,6 +838,13 @@ static CommonImage common_image(const qtb_plan* plan) {
     return c;
 }
 
+// One wave of wide networks: its tables live in RunCache::wide_buf.
+struct WideWave {
+    size_t nets_off, steps_off, segs_off, counters_off;   // bytes into wide_buf
+    uint32_t n_nets, n_steps, n_tiles;
+    int grid;
+};
+
 struct RunCache {
     Job* jobs = nullptr;                // class-mode jobs, persistent-mode jobs, counters
     unsigned int* done = nullptr;
@@ -533,8 +852,11 @@ struct RunCache {
     bool tuned = false;                 // schedule and block sizes chosen by the autotuner
     bool persistent = false;            // the schedule in use
     std::vector<LaunchClass> classes;   // class schedule, widest first
-    std::vector<LaunchClass> pclasses;  // persistent schedule (+ global-arena class)
-    size_t scratch_elems = 0;
+    std::vector<LaunchClass> pclasses;  // persistent schedule
+    std::vector<WideWave> waves;        // wide networks (both schedules), run one after another
+    void* wide_buf = nullptr;
+    size_t counters_bytes = 0;          // counters of all waves, zeroed before a run
+    size_t scratch_elems = 0;           // arenas of the largest wave
     bool smem_table = true;
     double n_groups = 0.0;              // distinct circuits among the range's networks
 };
@@ -565,6 +887,13 @@ static qtb_plan_device* dev_state(const qtb_plan* p) {
     return it->second;
 }
 
+static void free_run(RunCache* rc) {
+    if (rc->jobs) cudaFree(rc->jobs);
+    if (rc->wide_buf) cudaFree(rc->wide_buf);
+    rc->jobs = nullptr;
+    rc->wide_buf = nullptr;
+}
+
 static void free_device(qtb_plan* plan) {
     DeviceBuffers& d = plan->dev;
     void* ptrs[] = {d.runs, d.blobs, d.entries, d.table, d.status};   // terms lives in entries
@@ -572,8 +901,7 @@ static void free_device(qtb_plan* plan) {
         if (p) cudaFree(p);
     d = DeviceBuffers();
     qtb_plan_device* s = dev_state(plan);
-    for (auto& kv : s->runs)
-        if (kv.second.jobs) cudaFree(kv.second.jobs);
+    for (auto& kv : s->runs) free_run(&kv.second);
     s->runs.clear();
     plan->uploaded = false;
 }
@@ -696,11 +1024,127 @@ static size_t net_need(const DevNetRun& r, size_t fixed) {
     return fixed + (size_t)r.blob_bytes + 8 * (size_t)((r.arena_elems + 3u) & ~3u);
 }
 
+// Wide waves of a run: the networks too large for shared memory, largest
+// arena first, packed into waves whose arenas fit kWideWaveBytes (a larger
+// network forms a wave of its own).  Per wave: networks, steps (one per
+// phase index, its segments the wave networks that have that phase) and
+// tiles of kWideTileElems elements; one device buffer holds all tables.
+constexpr size_t kWideWaveBytes = size_t(1) << 30;
+
+static int build_waves(qtb_plan* plan, std::vector<int32_t> wide, int32_t first, float2* terms,
+                       RunCache* rc, bool device) {
+    rc->waves.clear();
+    rc->counters_bytes = 0;
+    if (wide.empty()) return QTB_OK;
+    auto arena_of = [&](int32_t i) { return ((size_t)plan->druns[i].arena_elems + 63) & ~size_t(63); };
+    std::stable_sort(wide.begin(), wide.end(), [&](int32_t x, int32_t y) { return arena_of(x) > arena_of(y); });
+    const auto* runs = static_cast<const DevNetRun*>(plan->dev.runs);
+    int per_sm = 0, sms = 0, dev = 0;
+    QTB_CUDA(cudaGetDevice(&dev));
+    QTB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qtb_wide_kernel, kWideThreads, 0));
+    std::vector<WideNet> nets;
+    std::vector<WideStep> steps;
+    std::vector<WideSeg> segs;
+    struct Range { size_t net0, step0, seg0; };
+    std::vector<Range> ranges;
+    size_t pos = 0;
+    while (pos < wide.size()) {
+        // members of this wave
+        size_t end = pos, elems = 0;
+        while (end < wide.size() && (end == pos || elems + arena_of(wide[end]) <= kWideWaveBytes / 8)) {
+            elems += arena_of(wide[end]);
+            ++end;
+        }
+        if (elems >= (size_t(1) << 31))
+            return fail(QTB_ERR_UNSUPPORTED, "plan_run: network arena of 2^31 elements or more");
+        Range rg{nets.size(), steps.size(), segs.size()};
+        WideWave wv{};
+        wv.n_nets = (uint32_t)(end - pos);
+        uint32_t max_phases = 0;
+        size_t off = 0;
+        for (size_t k = pos; k < end; ++k) {
+            const int32_t i = wide[k];
+            WideNet wn{};
+            wn.run = runs + i;
+            wn.term = terms + (i - first);
+            wn.arena_off = off;
+            off += arena_of(i);
+            nets.push_back(wn);
+            max_phases = std::max(max_phases, plan->druns[i].n_phases);
+        }
+        rc->scratch_elems = std::max(rc->scratch_elems, off);
+        uint32_t tiles = 0;
+        for (uint32_t ph = 0; ph < max_phases; ++ph) {
+            WideStep st{};
+            st.seg_begin = (uint32_t)(segs.size() - rg.seg0);
+            uint32_t total = 0;
+            for (size_t k = pos; k < end; ++k) {
+                const Network& n = plan->nets[wide[k]];
+                if (ph >= n.phases.size()) continue;
+                // segments start at multiples of kWideMinTile, so that with the
+                // ops of a phase sorted widest first the elements a thread
+                // batches differ only in bits 8 and 9 of their op index
+                total = (total + kWideMinTile - 1) & ~(kWideMinTile - 1);
+                segs.push_back(WideSeg{(uint32_t)(k - pos), total});
+                total += n.phases[ph].total_elems;
+            }
+            st.n_segs = (uint32_t)(segs.size() - rg.seg0) - st.seg_begin;
+            st.total_elems = total;
+            st.tile_begin = tiles;
+            // about two tiles per resident CTA, within [kWideMinTile, kWideMaxTile]
+            const uint32_t target = total / (uint32_t)(2 * std::max(1, per_sm) * sms) + 1;
+            st.tile_elems = std::min(kWideMaxTile, ((target + kWideMinTile - 1) / kWideMinTile) * kWideMinTile);
+            st.n_tiles = std::max(1u, (total + st.tile_elems - 1) / st.tile_elems);
+            tiles += st.n_tiles;
+            steps.push_back(st);
+        }
+        wv.n_steps = max_phases;
+        wv.n_tiles = tiles;
+        wv.grid = std::max(1, std::min<int>((int)tiles + 1, std::max(1, per_sm) * sms));
+        rc->waves.push_back(wv);
+        ranges.push_back(rg);
+        pos = end;
+    }
+    // device image: per wave [nets][steps][segs][counters], 256-byte aligned
+    auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
+    size_t bytes = 0;
+    for (size_t v = 0; v < rc->waves.size(); ++v) {
+        WideWave& wv = rc->waves[v];
+        const size_t n_segs = (v + 1 < ranges.size() ? ranges[v + 1].seg0 : segs.size()) - ranges[v].seg0;
+        wv.nets_off = bytes;
+        bytes = align(bytes + wv.n_nets * sizeof(WideNet));
+        wv.steps_off = bytes;
+        bytes = align(bytes + wv.n_steps * sizeof(WideStep));
+        wv.segs_off = bytes;
+        bytes = align(bytes + n_segs * sizeof(WideSeg));
+    }
+    const size_t counters0 = bytes;
+    for (WideWave& wv : rc->waves) {
+        wv.counters_off = bytes;
+        bytes += (1 + (size_t)wv.n_steps) * sizeof(unsigned int);
+    }
+    rc->counters_bytes = bytes - counters0;
+    if (!device) return QTB_OK;   // sizes only (qtb_plan_scratch_bytes)
+    std::vector<uint8_t> image(align(bytes), 0);
+    for (size_t v = 0; v < rc->waves.size(); ++v) {
+        const WideWave& wv = rc->waves[v];
+        const size_t n_segs = (v + 1 < ranges.size() ? ranges[v + 1].seg0 : segs.size()) - ranges[v].seg0;
+        std::memcpy(image.data() + wv.nets_off, nets.data() + ranges[v].net0, wv.n_nets * sizeof(WideNet));
+        std::memcpy(image.data() + wv.steps_off, steps.data() + ranges[v].step0, wv.n_steps * sizeof(WideStep));
+        std::memcpy(image.data() + wv.segs_off, segs.data() + ranges[v].seg0, n_segs * sizeof(WideSeg));
+    }
+    QTB_CUDA(cudaMalloc(&rc->wide_buf, image.size()));
+    QTB_CUDA(cudaMemcpy(rc->wide_buf, image.data(), image.size(), cudaMemcpyHostToDevice));
+    return QTB_OK;
+}
+
 // Launch classes of a run: each network goes to the shared-memory class of
 // the most resident CTAs per SM its staging + arena allows (networks too
 // large for shared memory use a global arena), the largest class launched
 // first so its long critical path starts early.
-static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms, RunCache* rc) {
+static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms, RunCache* rc,
+                     bool device = true) {
     rc->smem_table = plan->table_elems <= kSmemTableLimitElems;
     rc->n_groups = 0.0;
     for (int32_t i = first; i < first + count; ++i)
@@ -767,15 +1211,10 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
     rc->classes.clear();
     rc->pclasses.clear();
     rc->scratch_elems = 0;
-    // class schedule
-    for (int c = kMaxClasses - 1; c >= 0; --c) {
+    // class schedule; networks too large for shared memory run as wide waves
+    for (int c = kSmemClasses - 1; c >= 0; --c) {
         if (members[c].empty()) continue;
-        LaunchClass lc = make_class(members[c], c < kSmemClasses, false);
-        if (!lc.smem) {
-            lc.scratch_offset = rc->scratch_elems;
-            rc->scratch_elems += (size_t)lc.capacity * lc.n_jobs;
-        }
-        rc->classes.push_back(lc);
+        rc->classes.push_back(make_class(members[c], true, false));
     }
     // persistent schedule: every shared-memory network in one queue, widest
     // (largest arena, then most phases) first; the global-arena class as is
@@ -788,10 +1227,6 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
             return rx.arena_elems != ry.arena_elems ? rx.arena_elems > ry.arena_elems
                                                     : rx.n_phases > ry.n_phases;
         });
-        if (!members[kSmemClasses].empty()) {
-            for (const LaunchClass& lc : rc->classes)
-                if (!lc.smem) rc->pclasses.push_back(lc);   // same jobs, same scratch
-        }
         if (!all.empty()) {
             LaunchClass lc = make_class(all, true, true);
             if (fixed + lc.blob_capacity + 8 * (size_t)lc.capacity <= kSmemLimitBytes)
@@ -800,6 +1235,7 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
                 rc->pclasses.clear();   // no single shared-memory size fits all: class schedule only
         }
     }
+    if (!device) return build_waves(plan, members[kSmemClasses], first, terms, rc, false);
     // jobs of both schedules, then 16 bytes of counters (done, queue), zeroed
     const size_t job_bytes = jobs.size() * sizeof(Job);
     void* buf = nullptr;
@@ -814,7 +1250,7 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
             int r = persistent_grid(lc, rc->smem_table, &lc.grid);
             if (r) return r;
         }
-    return QTB_OK;
+    return build_waves(plan, members[kSmemClasses], first, terms, rc, true);
 }
 
 }  // namespace qtb
@@ -866,6 +1302,10 @@ int qtb_bucket_c64(const qtb_bucket_desc* d, const void* const* inputs, void* ou
 int qtb_plan_upload(qtb_plan* plan) {
     if (!plan) return fail(QTB_ERR_ARG, "plan_upload: null plan");
     std::lock_guard<std::mutex> lock(plan->mu);
+    // the executor's shared-memory limits on the current device (qtb_init
+    // does the same; a caller that skipped it still gets working launches)
+    int r0 = allow_all_smem();
+    if (r0) return r0;
     free_device(plan);
     flatten_plan(plan);
     build_blobs(plan);
@@ -894,8 +1334,7 @@ static int get_run(qtb_plan* plan, int32_t first, int32_t count, void* terms, Ru
     if (it == s->runs.end()) {
         if (s->runs.size() >= 64) {   // callers cycling through many output buffers
             QTB_CUDA(cudaDeviceSynchronize());
-            for (auto& kv : s->runs)
-                if (kv.second.jobs) cudaFree(kv.second.jobs);
+            for (auto& kv : s->runs) free_run(&kv.second);
             s->runs.clear();
         }
         RunCache rc;
@@ -917,27 +1356,59 @@ int qtb_plan_scratch_bytes(const qtb_plan* plan_c, int32_t first, int32_t count,
     if (count == 0) return QTB_OK;
     // the exact class split of this range (the same one qtb_plan_run uses)
     RunCache rc;
-    int r = build_run(plan, first, count, nullptr, &rc);
+    int r = build_run(plan, first, count, nullptr, &rc, false);   // sizes only, no device memory
+    free_run(&rc);
     if (r) return r;
-    if (rc.jobs) cudaFree(rc.jobs);
     *bytes = rc.scratch_elems * sizeof(float2);
     return QTB_OK;
 }
 
 static int ensure_streams(qtb_plan_device* s);
 
+// The wide waves of a run, one after another on st: counters zeroed, then
+// one K4 launch per wave over the shared arena scratch.
+static int launch_waves(const RunCache* rc, const RunArgs& base, void* scratch_dev, cudaStream_t st) {
+    if (rc->waves.empty()) return QTB_OK;
+    char* buf = static_cast<char*>(rc->wide_buf);
+    QTB_CUDA(cudaMemsetAsync(buf + rc->waves[0].counters_off, 0, rc->counters_bytes, st));
+    for (const WideWave& wv : rc->waves) {
+        WideArgs w{};
+        w.nets = reinterpret_cast<const WideNet*>(buf + wv.nets_off);
+        w.steps = reinterpret_cast<const WideStep*>(buf + wv.steps_off);
+        w.segs = reinterpret_cast<const WideSeg*>(buf + wv.segs_off);
+        w.counters = reinterpret_cast<unsigned int*>(buf + wv.counters_off);
+        w.arenas = static_cast<float2*>(scratch_dev);
+        w.n_nets = wv.n_nets;
+        w.n_steps = wv.n_steps;
+        w.n_tiles = wv.n_tiles;
+        qtb_wide_kernel<<<wv.grid, kWideThreads, 0, st>>>(w, base);
+        QTB_CUDA(cudaGetLastError());
+    }
+    return QTB_OK;
+}
+
 // Launch a schedule on st: a persistent class needs its queue zeroed first
-// (a memset node when captured); several classes run concurrently on
-// forked streams joined back into st.
+// (a memset node when captured); several classes, and the wide waves, run
+// concurrently on forked streams joined back into st.
 static int launch_schedule(qtb_plan_device* s, const RunCache* rc,
                            const std::vector<LaunchClass>& sched, const RunArgs& base,
-                           void* scratch_dev, cudaStream_t st) {
+                           void* scratch_dev, cudaStream_t st, bool with_waves = true) {
     int r = ensure_streams(s);
     if (r) return r;
     for (const LaunchClass& lc : sched)
         if (lc.persistent) QTB_CUDA(cudaMemsetAsync(rc->queue, 0, sizeof(unsigned int), st));
-    const bool forked = sched.size() > 1;
+    const bool waves = with_waves && !rc->waves.empty();
+    const bool forked = sched.size() + (waves ? 1 : 0) > 1;
     if (forked) QTB_CUDA(cudaEventRecord(s->fork, st));
+    if (waves) {
+        cudaStream_t ws = forked ? s->aux[kMaxClasses - 1] : st;
+        if (forked) QTB_CUDA(cudaStreamWaitEvent(ws, s->fork, 0));
+        if ((r = launch_waves(rc, base, scratch_dev, ws))) return r;
+        if (forked) {
+            QTB_CUDA(cudaEventRecord(s->join[kMaxClasses - 1], ws));
+            QTB_CUDA(cudaStreamWaitEvent(st, s->join[kMaxClasses - 1], 0));
+        }
+    }
     for (size_t c = 0; c < sched.size(); ++c) {
         const LaunchClass& lc = sched[c];
         cudaStream_t cs = forked ? s->aux[c] : st;
@@ -994,7 +1465,8 @@ static int autotune_run(qtb_plan_device* s, RunCache* rc, const RunArgs& base, v
             std::vector<LaunchClass> one(1, lc);
             one[0].threads = t;
             float ms = 1e30f;
-            if ((r = time_it([&] { return launch_schedule(s, rc, one, a, scratch_dev, st); }, &ms))) return r;
+            if ((r = time_it([&] { return launch_schedule(s, rc, one, a, scratch_dev, st, false); }, &ms)))
+                return r;
             if (log)
                 std::fprintf(stderr, "qtb autotune: class of %d networks (smem %zu B) %4d threads %.1f us\n",
                              lc.n_jobs, lc.smem_bytes, t, 1e3 * ms);
@@ -1114,7 +1586,7 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
     a.energy = energy_dev;
     a.energy_groups = rc->n_groups;
     const int n_entries = (int)plan->entries.size();
-    if (!rc->smem_table && n_entries > 0) {
+    if ((!rc->smem_table || !rc->waves.empty()) && n_entries > 0) {
         qtb_table_kernel<<<(n_entries + 127) / 128, 128, 0, st>>>(
             static_cast<const DevEntry*>(plan->dev.entries), n_entries,
             static_cast<const DevTerm*>(plan->dev.terms), params_dev,
@@ -1145,7 +1617,7 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
     if (s->timing) {
         QTB_CUDA(cudaEventRecord(ev.second, st));
         s->pending.push_back(ev);
-        s->kernel_launches += (int64_t)sched.size();
+        s->kernel_launches += (int64_t)(sched.size() + rc->waves.size());
     }
     return QTB_OK;
 }
@@ -1393,14 +1865,22 @@ int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32
         return QTB_OK;
     }
     const std::vector<LaunchClass>& sched = rc->persistent ? rc->pclasses : rc->classes;
-    *n_classes = (int32_t)sched.size();
+    *n_classes = (int32_t)(sched.size() + rc->waves.size());
     if (!out) return QTB_OK;
     for (int32_t c = 0; c < *n_classes && 4 * c + 3 < cap; ++c) {
-        const LaunchClass& lc = sched[c];
-        out[4 * c] = lc.n_jobs;
-        out[4 * c + 1] = lc.threads;
-        out[4 * c + 2] = (int32_t)lc.smem_bytes;
-        out[4 * c + 3] = (lc.smem ? 1 : 0) | (lc.persistent ? 2 : 0);
+        if (c < (int32_t)sched.size()) {
+            const LaunchClass& lc = sched[c];
+            out[4 * c] = lc.n_jobs;
+            out[4 * c + 1] = lc.threads;
+            out[4 * c + 2] = (int32_t)lc.smem_bytes;
+            out[4 * c + 3] = (lc.smem ? 1 : 0) | (lc.persistent ? 2 : 0);
+        } else {
+            const WideWave& wv = rc->waves[c - sched.size()];
+            out[4 * c] = (int32_t)wv.n_nets;
+            out[4 * c + 1] = kWideThreads;
+            out[4 * c + 2] = 0;
+            out[4 * c + 3] = 4;
+        }
     }
     return QTB_OK;
 }

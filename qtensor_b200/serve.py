@@ -104,6 +104,7 @@ class QAOAServer:
         self._compile_pool = ThreadPoolExecutor(max_workers=compile_workers)
         self._ready = queue.Queue()          # compiled requests, arrival order
         self._stop = threading.Event()
+        self._retired = []                   # finished plans awaiting release (dispatcher only)
         self._dispatcher = threading.Thread(target=self._dispatch_loop, daemon=True)
         self._dispatcher.start()
         self.stats = collections.Counter()
@@ -198,7 +199,10 @@ class QAOAServer:
             self.stats['failed'] += 1
             job.future.set_exception(exc)
         finally:
-            job.plan.close()
+            # freeing device memory synchronises the whole device, so finished
+            # plans are released while the GPU has no request in flight (or
+            # in batches), not while other requests' kernels run
+            self._retired.append(job.plan)
 
     def _dispatch_loop(self):
         torch.cuda.set_device(self.device)
@@ -248,6 +252,10 @@ class QAOAServer:
                 else:
                     still.append(fl)
             inflight = still
+            if self._retired and (not inflight or len(self._retired) >= 32):
+                for plan in self._retired:
+                    plan.close()
+                self._retired = []
             if done_input and not inflight and not waiting:
                 return
             if inflight:

@@ -83,10 +83,12 @@ def _gather_runs(j, runs):
     if n <= 1:                       # pre-decoded single run
         return (j >> ((runs >> 32) & 31)) & (runs & 0xffffffff)
     off = np.zeros_like(j)
+    dst = 0
     for r in range(n):
-        rr = (runs >> (15 * r)) & 0x7fff
-        start, length, dst = rr & 31, (rr >> 5) & 31, rr >> 10
+        rr = (runs >> (10 * r)) & 0x3ff
+        start, length = rr & 31, rr >> 5
         off |= ((j >> start) & ((1 << length) - 1)) << dst
+        dst += length
     return off
 
 
