@@ -179,18 +179,25 @@ class QAOAEnergyEngine:
         _lib.check(_lib.lib().qtb_init(self.device.index))
 
     # ------------------------------------------------------------ compile
-    def compile(self, G, p, gamma=None, beta=None):
-        """Compile (or fetch) the device plan of every edge of ``G`` at depth p.
+    def compile(self, G, p, gamma=None, beta=None, edges=None):
+        """Compile (or fetch) the device plan of every edge of ``G`` at depth p
+        (or of the edges whose indices in ``G.edges()`` order are ``edges``).
 
         The angles only steer the simplifier's near-zero cancellation test;
         a plan whose decisions depend on them is recompiled when they change."""
         params = self._params(p, gamma, beta)
         key = self._key(G, p)
+        if edges is not None:
+            edges = tuple(int(i) for i in edges)
+            key += ':' + hashlib.sha1(repr(edges).encode()).hexdigest()
         with self._lock:
             cg = self._cache.get(key)
             if cg is not None and cg.plan.params_valid(params):
                 return cg
-        edges = list(G.edges())
+        all_edges = list(G.edges())
+        edges = all_edges if edges is None else [all_edges[i] for i in edges]
+        if not edges:
+            raise ValueError('no edges to compile')
         plan = NetworkPlan(2 * p)
         plan.set_order_trials(self.order_trials)
         plan.set_max_width(self.max_width, self.max_slices)
@@ -248,25 +255,28 @@ class QAOAEnergyEngine:
         return np.concatenate([gamma, beta])
 
     # ------------------------------------------------------------ run
-    def energy_expectation(self, G, gamma, beta, path='batched'):
+    def energy_expectation(self, G, gamma, beta, path='batched', edges=None):
         """Expected MaxCut value of the depth-p QAOA state (p = len(gamma)).
 
         path: ``'batched'`` (whole-network executor, one graph replay) or
-        ``'plain'`` (one bucket-kernel launch per bucket)."""
+        ``'plain'`` (one bucket-kernel launch per bucket).  With ``edges``
+        (indices into ``G.edges()``) the value is the share of those edges,
+        ``(len(edges) - Re sum of their terms) / 2``: shares of disjoint edge
+        sets add up to the energy."""
         gamma = np.asarray(gamma, dtype=np.float64).ravel()
         p = len(gamma)
-        cg = self.compile(G, p, gamma, beta)
+        cg = self.compile(G, p, gamma, beta, edges)
         if path == 'batched':
             return cg.energy_of(self._params(p, gamma, beta))
         self._launch(cg, p, gamma, beta, path)
         return float(cg.energy.cpu()[0])
 
-    def edge_terms(self, G, gamma, beta, path='batched'):
-        """``<Z_u Z_v>`` of every edge (numpy complex, edge order of ``G.edges()``;
-        sliced edges are summed over their slices)."""
+    def edge_terms(self, G, gamma, beta, path='batched', edges=None):
+        """``<Z_u Z_v>`` of every edge (numpy complex, edge order of ``G.edges()``,
+        or of ``edges``; sliced edges are summed over their slices)."""
         gamma = np.asarray(gamma, dtype=np.float64).ravel()
         p = len(gamma)
-        cg = self.compile(G, p, gamma, beta)
+        cg = self.compile(G, p, gamma, beta, edges)
         self._launch(cg, p, gamma, beta, path)
         return cg.edge_terms()
 

@@ -126,4 +126,26 @@ def test_plain_path_matches_batched_and_reference(cuda_device, name, max_width):
     assert np.max(np.abs(plain - batched)) < TOL
     E = eng.energy_expectation(G, w['gamma'], w['beta'], path='plain')
     assert abs(E - w['energy']) <= TOL * abs(w['energy'])
-    assert eng.compile(G, len(w['gamma'])).plan.device_status() == 0
+    assert eng.compile(G, len(w['gamma']), w['gamma'], w['beta']).plan.device_status() == 0
+
+
+def test_wide_waves_match_plain_path(cuda_device):
+    """Erdos-Renyi N=400 p=3 (seed 24323709): 147 networks too large for
+    shared memory (2 GB of arenas) run as two whole-GPU waves next to the
+    shared-memory classes; every edge term equals the plain per-bucket
+    path's (an independent execution of the same plans) and the energies
+    agree."""
+    import networkx as nx
+    G = nx.erdos_renyi_graph(400, 3 / 399, seed=24323709)
+    gamma, beta = graphs.angles(3, seed=1)
+    eng = _engine(max_width=22)
+    batched = eng.edge_terms(G, gamma, beta)
+    cg = eng.compile(G, 3, gamma, beta)
+    waves = [c for c in cg.plan.last_launch_config() if c[3] & 4]
+    assert len(waves) >= 2
+    plain = eng.edge_terms(G, gamma, beta, path='plain')
+    assert np.max(np.abs(batched - plain)) < TOL
+    E = eng.energy_expectation(G, gamma, beta)
+    Ep = eng.energy_expectation(G, gamma, beta, path='plain')
+    assert abs(E - Ep) <= TOL * abs(Ep)
+    assert cg.plan.device_status() == 0
