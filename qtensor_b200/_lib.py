@@ -77,7 +77,7 @@ class NetworkInfo(ctypes.Structure):
 # numpy views of the exported plan arrays (plan.h)
 NET_DTYPE = np.dtype([('op_begin', '<u4'), ('n_ops', '<u4'), ('phase_begin', '<u4'),
                       ('n_phases', '<u4'), ('arena_elems', '<u4'), ('result_src', '<u4'),
-                      ('max_elems', '<u4'), ('tail_start', '<u4')])
+                      ('max_elems', '<u4'), ('pad', '<u4')])
 OP_DTYPE = np.dtype([('u', 'u1'), ('sum', 'u1'), ('k', 'u1'), ('pad', 'u1'), ('dst', '<u4'),
                      ('elem_begin', '<u4'), ('in_begin', '<u4')])
 IN_DTYPE = np.dtype([('mask', '<u4'), ('src', '<u4'), ('runs', '<u8')])
@@ -89,7 +89,7 @@ ENTRY_DTYPE = np.dtype([('kind', '<i4'), ('expr_begin', '<i4'), ('expr_count', '
 TERM_DTYPE = np.dtype([('param', '<i4'), ('pad', '<i4'), ('coef', '<f8')])
 RUN_DTYPE = np.dtype([('blob_off16', '<u4'), ('blob_bytes', '<u4'), ('n_phases', '<u4'),
                       ('ins_off', '<u4'), ('arena_elems', '<u4'), ('result_src', '<u4'),
-                      ('max_elems', '<u4'), ('pad', '<u4')])
+                      ('max_elems', '<u4'), ('tail_start', '<u4')])
 SRC_TABLE = 0x80000000
 
 _lib = None

@@ -279,7 +279,10 @@ __device__ void reduce_energy(const float2* terms, uint32_t n, double n_groups, 
 // (and at j with the summed bit set), summed over the bucket variable.
 // Operands are handled in groups of four so their descriptor and value
 // loads issue together instead of as one dependent chain per operand.
-template <bool kSmemTable>
+//   kUnified: table and arena both in shared memory, the arena at
+//   table + round-up-to-16-bytes(table): single-run operands carrying their
+//   unified address (DevIn fast fields) are read without decoding.
+template <bool kSmemTable, bool kUnified>
 __device__ __forceinline__ void compute_element(const DevOp& op, uint32_t j, const DevIn* ins,
                                                 const float2* __restrict__ table,
                                                 float2* __restrict__ arena) {
@@ -287,6 +290,28 @@ __device__ __forceinline__ void compute_element(const DevOp& op, uint32_t j, con
     const uint32_t low = (1u << w) - 1u;
     const DevIn* in = ins + op.in_begin;
     float2 p0 = make_float2(1.f, 0.f), p1 = make_float2(1.f, 0.f);
+    if (kUnified) {
+        // every operand fast: one 8-byte descriptor load, a shift, a mask
+        bool all_fast = true;
+        for (uint32_t t = 0; t < op.k; ++t) {
+            const uint64_t r = in[t].runs;
+            const uint32_t hi = (uint32_t)(r >> 32);
+            if (!(hi & kFastValid)) {
+                all_fast = false;
+                break;
+            }
+            const uint32_t off = ((hi >> 5) & 0xffffu) + ((j >> (hi & 31u)) & (uint32_t)r);
+            const float2 x0 = table[off];
+            const float2 x1 = (hi & kFastSum) ? table[off + (1u << ((hi >> 22) & 31u))] : x0;
+            p0 = t == 0 ? x0 : cmul(p0, x0);
+            p1 = t == 0 ? x1 : cmul(p1, x1);
+        }
+        if (all_fast) {
+            arena[op.dst + j] = op.sum ? make_float2(p0.x + p1.x, p0.y + p1.y) : p0;
+            return;
+        }
+        p0 = p1 = make_float2(1.f, 0.f);
+    }
     for (uint32_t t0 = 0; t0 < op.k; t0 += 4) {
         DevIn d[4];
 #pragma unroll
@@ -348,7 +373,7 @@ __device__ void build_table(const unsigned char* common, const RunArgs& a, float
 }
 
 // The phases of one staged network; its scalar result is returned to thread 0.
-template <bool kSmemTable>
+template <bool kSmemTable, bool kUnified>
 __device__ float2 contract_network(const DevNetRun& net, const unsigned char* blob,
                                    const float2* __restrict__ table, float2* __restrict__ arena) {
     const DevPhase* phases = reinterpret_cast<const DevPhase*>(blob);
@@ -373,7 +398,7 @@ __device__ float2 contract_network(const DevNetRun& net, const unsigned char* bl
                     op_end = op.elem_begin + (1u << (op.u - op.sum));
                 }
             }
-            compute_element<kSmemTable>(op, g - op.elem_begin, ins, table, arena);
+            compute_element<kSmemTable, kUnified>(op, g - op.elem_begin, ins, table, arena);
         }
         __syncthreads();
     }
@@ -386,7 +411,7 @@ __device__ float2 contract_network(const DevNetRun& net, const unsigned char* bl
                 uint32_t oi = ph.op_first;
                 DevOp op = ops[oi];
                 while (g >= op.elem_begin + (1u << (op.u - op.sum))) op = ops[++oi];
-                compute_element<kSmemTable>(op, g - op.elem_begin, ins, table, arena);
+                compute_element<kSmemTable, kUnified>(op, g - op.elem_begin, ins, table, arena);
             }
             __syncwarp();
         }
@@ -457,7 +482,7 @@ __global__ void __launch_bounds__(kPersistent ? 512 : 1024) qtb_network_kernel(
         }
         const unsigned char* nblob =
             staged ? blob : reinterpret_cast<const unsigned char*>(a.blobs + net.blob_off16);
-        const float2 term = contract_network<kSmemTable>(net, nblob, table, arena);
+        const float2 term = contract_network<kSmemTable, kSmemTable && kSmemArena>(net, nblob, table, arena);
         if (threadIdx.x == 0) {
             *job.term = term;
             if (a.energy) {

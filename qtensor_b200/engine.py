@@ -57,6 +57,8 @@ class CompiledGraph:
                         if nbytes else None)
         self._infos = None
         self._plain_scratch = None
+        # simplifier decisions that hold only for some angles (rechecked per call)
+        self.angle_checks = any(i['angle_specific'] for i in self.infos)
         # host side of the captured call: pinned angles in, pinned energy out
         self.host_params = torch.zeros(2 * p, dtype=torch.float64, pin_memory=True)
         self.host_energy = torch.zeros(1, dtype=torch.float64, pin_memory=True)
@@ -141,10 +143,14 @@ class CompiledGraph:
         doubles) by one graph replay and one synchronisation."""
         if self._graph is None:
             self._capture()
-        self.host_params.numpy()[:] = params
+            self._host_params_np = self.host_params.numpy()
+            self._host_energy_np = self.host_energy.numpy()
+            self._done = torch.cuda.Event()
+        self._host_params_np[:] = params
         self._graph.replay()
-        torch.cuda.current_stream(self.device).synchronize()
-        return float(self.host_energy.numpy()[0])
+        self._done.record(torch.cuda.current_stream(self.device))
+        self._done.synchronize()
+        return float(self._host_energy_np[0])
 
 
 class QAOAEnergyEngine:
@@ -192,8 +198,8 @@ class QAOAEnergyEngine:
             key += ':' + hashlib.sha1(repr(edges).encode()).hexdigest()
         with self._lock:
             cg = self._cache.get(key)
-            if cg is not None and cg.plan.params_valid(params):
-                return cg
+        if cg is not None and (not cg.angle_checks or cg.plan.params_valid(params)):
+            return cg
         all_edges = list(G.edges())
         edges = all_edges if edges is None else [all_edges[i] for i in edges]
         if not edges:
@@ -222,17 +228,19 @@ class QAOAEnergyEngine:
 
     def _key(self, G, p):
         """Plan-cache key of ``G``.  The full key hashes every edge; a graph
-        object seen before with the same node and edge counts reuses its key
-        (call ``invalidate(G)`` after mutating a graph in place)."""
+        object seen before with the same node count reuses its key without
+        rehashing (networkx counts edges in O(nodes), which would cost more
+        than a whole contraction), so call ``invalidate(G)`` after changing
+        a graph's edges in place."""
         hit = self._by_id.get(id(G))
         if hit is not None:
-            ref, n, m, hp, key = hit
-            if ref() is G and hp == p and n == G.number_of_nodes() and m == G.number_of_edges():
+            ref, n, hp, key = hit
+            if ref() is G and hp == p and n == len(G):
                 return key
         key = graph_key(G, p, self.composer, self.ordering, self.order_trials,
                         (self.max_width, self.max_slices))
         try:
-            self._by_id[id(G)] = (weakref.ref(G), G.number_of_nodes(), G.number_of_edges(), p, key)
+            self._by_id[id(G)] = (weakref.ref(G), len(G), p, key)
         except TypeError:
             pass
         return key
@@ -242,7 +250,8 @@ class QAOAEnergyEngine:
         hit = self._by_id.pop(id(G), None)
         if hit is not None:
             with self._lock:
-                self._cache.pop(hit[4], None)
+                for k in [k for k in self._cache if k.split(':')[0] == hit[3]]:
+                    self._cache.pop(k)
 
     @staticmethod
     def _params(p, gamma, beta):
