@@ -275,6 +275,22 @@ __device__ void reduce_energy(const float2* terms, uint32_t n, double n_groups, 
     }
 }
 
+// The op of a phase holding flattened element g, starting from op `oi` at
+// or before it (`op` holds ops[oi]).  The ops of a phase are sorted by
+// non-increasing size, so jumping (g - start) >> w ops ahead never passes
+// the op holding g (every op after oi has at most 2^w elements); a short
+// walk over ops of smaller size finishes.  Returns the op index.
+template <typename LoadOp>
+__device__ __forceinline__ uint32_t find_op(uint32_t g, uint32_t oi, DevOp& op, LoadOp load) {
+    const uint32_t jump = (g - op.elem_begin) >> (op.u - op.sum);
+    if (jump) {
+        oi += jump;
+        op = load(oi);
+    }
+    while (g >= op.elem_begin + (1u << (op.u - op.sum))) op = load(++oi);
+    return oi;
+}
+
 // One output element j of op: the product of its operands gathered at j
 // (and at j with the summed bit set), summed over the bucket variable.
 // Operands are handled in groups of four so their descriptor and value
@@ -282,7 +298,8 @@ __device__ void reduce_energy(const float2* terms, uint32_t n, double n_groups, 
 //   kUnified: table and arena both in shared memory, the arena at
 //   table + round-up-to-16-bytes(table): single-run operands carrying their
 //   unified address (DevIn fast fields) are read without decoding.
-template <bool kSmemTable, bool kUnified>
+//   kGroup: operands whose loads are issued together (fewer registers when 2).
+template <bool kSmemTable, bool kUnified, int kGroup = 4>
 __device__ __forceinline__ void compute_element(const DevOp& op, uint32_t j, const DevIn* ins,
                                                 const float2* __restrict__ table,
                                                 float2* __restrict__ arena) {
@@ -312,14 +329,14 @@ __device__ __forceinline__ void compute_element(const DevOp& op, uint32_t j, con
         }
         p0 = p1 = make_float2(1.f, 0.f);
     }
-    for (uint32_t t0 = 0; t0 < op.k; t0 += 4) {
-        DevIn d[4];
+    for (uint32_t t0 = 0; t0 < op.k; t0 += kGroup) {
+        DevIn d[kGroup];
 #pragma unroll
-        for (int t = 0; t < 4; ++t)
+        for (int t = 0; t < kGroup; ++t)
             if (t0 + t < op.k) d[t] = in[t0 + t];
-        float2 x0[4], x1[4];
+        float2 x0[kGroup], x1[kGroup];
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
+        for (int t = 0; t < kGroup; ++t) {
             if (t0 + t < op.k) {
                 const uint32_t off = gather_bits(j, d[t], low);
                 const bool tab = d[t].src & kSrcTable;
@@ -335,7 +352,7 @@ __device__ __forceinline__ void compute_element(const DevOp& op, uint32_t j, con
             }
         }
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
+        for (int t = 0; t < kGroup; ++t) {
             if (t0 + t < op.k) {
                 p0 = (t0 + t == 0) ? x0[t] : cmul(p0, x0[t]);
                 p1 = (t0 + t == 0) ? x1[t] : cmul(p1, x1[t]);
@@ -373,7 +390,7 @@ __device__ void build_table(const unsigned char* common, const RunArgs& a, float
 }
 
 // The phases of one staged network; its scalar result is returned to thread 0.
-template <bool kSmemTable, bool kUnified>
+template <bool kSmemTable, bool kUnified, int kGroup = 4>
 __device__ float2 contract_network(const DevNetRun& net, const unsigned char* blob,
                                    const float2* __restrict__ table, float2* __restrict__ arena) {
     const DevPhase* phases = reinterpret_cast<const DevPhase*>(blob);
@@ -392,13 +409,10 @@ __device__ float2 contract_network(const DevNetRun& net, const unsigned char* bl
                 // ops may share a chunk, so step forward to the one holding g
                 oi = chunk[g / kChunkElems];
                 op = ops[oi];
+                oi = find_op(g, oi, op, [&](uint32_t i) { return ops[i]; });
                 op_end = op.elem_begin + (1u << (op.u - op.sum));
-                while (g >= op_end) {
-                    op = ops[++oi];
-                    op_end = op.elem_begin + (1u << (op.u - op.sum));
-                }
             }
-            compute_element<kSmemTable, kUnified>(op, g - op.elem_begin, ins, table, arena);
+            compute_element<kSmemTable, kUnified, kGroup>(op, g - op.elem_begin, ins, table, arena);
         }
         __syncthreads();
     }
@@ -408,10 +422,9 @@ __device__ float2 contract_network(const DevNetRun& net, const unsigned char* bl
             const DevPhase ph = phases[p];
             const uint32_t g = threadIdx.x;
             if (g < ph.total_elems) {
-                uint32_t oi = ph.op_first;
-                DevOp op = ops[oi];
-                while (g >= op.elem_begin + (1u << (op.u - op.sum))) op = ops[++oi];
-                compute_element<kSmemTable, kUnified>(op, g - op.elem_begin, ins, table, arena);
+                DevOp op = ops[ph.op_first];
+                find_op(g, ph.op_first, op, [&](uint32_t i) { return ops[i]; });
+                compute_element<kSmemTable, kUnified, kGroup>(op, g - op.elem_begin, ins, table, arena);
             }
             __syncwarp();
         }
@@ -432,8 +445,10 @@ __device__ float2 contract_network(const DevNetRun& net, const unsigned char* bl
 // After each network thread 0 writes its term; with a.energy set, the CTA
 // that finishes the run's last network sums Re(terms) in fp64 and writes
 // the energy.
-template <bool kSmemArena, bool kSmemTable, bool kPersistent>
-__global__ void __launch_bounds__(kPersistent ? 512 : 1024) qtb_network_kernel(
+//   kLean (persistent, 128 threads): registers capped for 8 CTAs per SM, so
+//   small networks keep twice as many in flight per SM.
+template <bool kSmemArena, bool kSmemTable, bool kPersistent, bool kLean = false>
+__global__ void __launch_bounds__(kLean ? 128 : (kPersistent ? 512 : 1024), kLean ? 8 : 1) qtb_network_kernel(
     const Job* __restrict__ jobs, const RunArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
@@ -482,7 +497,8 @@ __global__ void __launch_bounds__(kPersistent ? 512 : 1024) qtb_network_kernel(
         }
         const unsigned char* nblob =
             staged ? blob : reinterpret_cast<const unsigned char*>(a.blobs + net.blob_off16);
-        const float2 term = contract_network<kSmemTable, kSmemTable && kSmemArena>(net, nblob, table, arena);
+        const float2 term = contract_network<kSmemTable, kSmemTable && kSmemArena && !kLean, kLean ? 2 : 4>(
+            net, nblob, table, arena);
         if (threadIdx.x == 0) {
             *job.term = term;
             if (a.energy) {
@@ -783,9 +799,9 @@ __global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArg
                 continue;
             }
             if (l < op_lo || l >= op_hi) {
-                uint32_t oi = __ldg(chunk + l / kChunkElems);
+                const uint32_t oi = __ldg(chunk + l / kChunkElems);
                 op = ldg_op(ops + oi);
-                while (l >= op.elem_begin + (1u << (op.u - op.sum)) && oi < op_last) op = ldg_op(ops + ++oi);
+                find_op(l, oi, op, [&](uint32_t i) { return ldg_op(ops + min(i, op_last)); });
                 op_lo = op.elem_begin;
                 op_hi = op.elem_begin + (1u << (op.u - op.sum));
             }
@@ -830,10 +846,13 @@ constexpr uint32_t kSmemReservePerCta = 1024;
 constexpr int kClassCtas[] = {16, 12, 10, 8, 6, 5, 4, 3, 2, 1};
 constexpr int kSmemClasses = (int)(sizeof(kClassCtas) / sizeof(kClassCtas[0]));
 constexpr int kMaxClasses = kSmemClasses + 1;   // + the global-arena class
+constexpr int kLeanThreads = 128;
+constexpr int kLeanCtasPerSm = 8;
 
 struct LaunchClass {
     bool smem;
     bool persistent;        // CTAs take networks from the run's queue
+    bool lean;              // persistent, 128 threads, registers capped (8 CTAs per SM)
     int grid;               // CTAs (= n_jobs unless persistent)
     uint32_t capacity;      // arena elements per CTA
     uint32_t blob_capacity; // plan-blob bytes per CTA
@@ -870,14 +889,17 @@ struct WideWave {
     int grid;
 };
 
+constexpr int kSchedClasses = 0, kSchedPersistent = 1, kSchedHybrid = 2;
+
 struct RunCache {
     Job* jobs = nullptr;                // class-mode jobs, persistent-mode jobs, counters
     unsigned int* done = nullptr;
     unsigned int* queue = nullptr;
     bool tuned = false;                 // schedule and block sizes chosen by the autotuner
-    bool persistent = false;            // the schedule in use
+    int schedule = 0;                   // the schedule in use (kSched*)
     std::vector<LaunchClass> classes;   // class schedule, widest first
     std::vector<LaunchClass> pclasses;  // persistent schedule
+    std::vector<LaunchClass> hclasses;  // hybrid schedule: large networks as classes + lean queue
     std::vector<WideWave> waves;        // wide networks (both schedules), run one after another
     void* wide_buf = nullptr;
     size_t counters_bytes = 0;          // counters of all waves, zeroed before a run
@@ -912,6 +934,17 @@ static qtb_plan_device* dev_state(const qtb_plan* p) {
     return it->second;
 }
 
+static const std::vector<LaunchClass>& schedule_of(const RunCache* rc) {
+    return rc->schedule == kSchedPersistent ? rc->pclasses
+           : rc->schedule == kSchedHybrid   ? rc->hclasses
+                                            : rc->classes;
+}
+
+// Grid of the hybrid schedule's lean queue: its resident CTAs on the GPU
+// less the slots the large-network CTAs (launched first) take, counted in
+// lean CTAs by threads (registers) and by shared memory.
+static int hybrid_lean_grid(std::vector<LaunchClass>& sched, bool smem_table);
+
 static void free_run(RunCache* rc) {
     if (rc->jobs) cudaFree(rc->jobs);
     if (rc->wide_buf) cudaFree(rc->wide_buf);
@@ -934,6 +967,12 @@ static void free_device(qtb_plan* plan) {
 // Kernel instantiation for a launch class.
 template <bool kA, bool kT>
 static void launch_one(const LaunchClass& lc, const Job* jobs, const RunArgs& a, cudaStream_t st) {
+    if constexpr (kA) {
+        if (lc.lean) {
+            qtb_network_kernel<true, kT, true, true><<<lc.grid, kLeanThreads, lc.smem_bytes, st>>>(jobs, a);
+            return;
+        }
+    }
     if (lc.persistent)
         qtb_network_kernel<kA, kT, true><<<lc.grid, lc.threads, lc.smem_bytes, st>>>(jobs, a);
     else
@@ -951,9 +990,9 @@ static void launch_class(const LaunchClass& lc, bool smem_table, const Job* jobs
     }
 }
 
-template <bool kA, bool kT, bool kP>
+template <bool kA, bool kT, bool kP, bool kL = false>
 static cudaError_t allow_smem() {
-    return cudaFuncSetAttribute(qtb_network_kernel<kA, kT, kP>,
+    return cudaFuncSetAttribute(qtb_network_kernel<kA, kT, kP, kL>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimitBytes);
 }
 
@@ -966,6 +1005,8 @@ static int allow_all_smem() {
     QTB_CUDA((allow_smem<true, false, true>()));
     QTB_CUDA((allow_smem<false, true, true>()));
     QTB_CUDA((allow_smem<false, false, true>()));
+    QTB_CUDA((allow_smem<true, true, true, true>()));
+    QTB_CUDA((allow_smem<true, false, true, true>()));
     return QTB_OK;
 }
 
@@ -974,7 +1015,14 @@ static int persistent_grid(const LaunchClass& lc, bool smem_table, int* grid) {
     int per_sm = 0, sms = 0, dev = 0;
     QTB_CUDA(cudaGetDevice(&dev));
     QTB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    if (lc.smem) {
+    if (lc.lean) {
+        if (smem_table)
+            QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, qtb_network_kernel<true, true, true, true>, kLeanThreads, lc.smem_bytes));
+        else
+            QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, qtb_network_kernel<true, false, true, true>, kLeanThreads, lc.smem_bytes));
+    } else if (lc.smem) {
         if (smem_table)
             QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
                 &per_sm, qtb_network_kernel<true, true, true>, lc.threads, lc.smem_bytes));
@@ -985,6 +1033,31 @@ static int persistent_grid(const LaunchClass& lc, bool smem_table, int* grid) {
         per_sm = 1;
     }
     *grid = std::max(1, std::min(lc.n_jobs, std::max(1, per_sm) * sms));
+    return QTB_OK;
+}
+
+static int hybrid_lean_grid(std::vector<LaunchClass>& sched, bool smem_table) {
+    LaunchClass* lean = nullptr;
+    for (LaunchClass& lc : sched)
+        if (lc.lean) lean = &lc;
+    if (!lean) return QTB_OK;
+    int full = 0;
+    LaunchClass probe = *lean;
+    probe.n_jobs = 1 << 30;
+    int r = persistent_grid(probe, smem_table, &full);
+    if (r) return r;
+    long long taken = 0;
+    for (const LaunchClass& lc : sched) {
+        if (lc.lean) continue;
+        const long long by_threads = (lc.threads + kLeanThreads - 1) / kLeanThreads;
+        const long long by_smem = lean->smem_bytes ? (long long)((lc.smem_bytes + lean->smem_bytes - 1) / lean->smem_bytes) : 1;
+        taken += (long long)lc.n_jobs * std::max(by_threads, by_smem);
+    }
+    int sms = 0, dev = 0;
+    QTB_CUDA(cudaGetDevice(&dev));
+    QTB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long long grid = std::max<long long>(sms, (long long)full - taken);
+    lean->grid = (int)std::max<long long>(1, std::min<long long>(lean->n_jobs, grid));
     return QTB_OK;
 }
 
@@ -1242,22 +1315,59 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
         rc->classes.push_back(make_class(members[c], true, false));
     }
     // persistent schedule: every shared-memory network in one queue, widest
-    // (largest arena, then most phases) first; the global-arena class as is
+    // (largest arena, then most phases) first
+    std::vector<int32_t> all;
+    for (int c = 0; c < kSmemClasses; ++c) all.insert(all.end(), members[c].begin(), members[c].end());
+    std::stable_sort(all.begin(), all.end(), [&](int32_t x, int32_t y) {
+        const DevNetRun& rx = plan->druns[x];
+        const DevNetRun& ry = plan->druns[y];
+        return rx.arena_elems != ry.arena_elems ? rx.arena_elems > ry.arena_elems
+                                                : rx.n_phases > ry.n_phases;
+    });
+    if (!all.empty()) {
+        LaunchClass lc = make_class(all, true, true);
+        if (fixed + lc.blob_capacity + 8 * (size_t)lc.capacity <= kSmemLimitBytes)
+            rc->pclasses.push_back(lc);   // else no single shared-memory size fits all
+    }
+    // hybrid schedule: networks whose staging + arena fit an eighth of an SM
+    // in one lean persistent queue (kLeanCtasPerSm CTAs per SM), the others
+    // as class launches (one CTA per network, more threads), launched first
+    // so that their longer critical paths start early
+    rc->hclasses.clear();
     {
-        std::vector<int32_t> all;
-        for (int c = 0; c < kSmemClasses; ++c) all.insert(all.end(), members[c].begin(), members[c].end());
-        std::stable_sort(all.begin(), all.end(), [&](int32_t x, int32_t y) {
-            const DevNetRun& rx = plan->druns[x];
-            const DevNetRun& ry = plan->druns[y];
-            return rx.arena_elems != ry.arena_elems ? rx.arena_elems > ry.arena_elems
-                                                    : rx.n_phases > ry.n_phases;
-        });
-        if (!all.empty()) {
-            LaunchClass lc = make_class(all, true, true);
-            if (fixed + lc.blob_capacity + 8 * (size_t)lc.capacity <= kSmemLimitBytes)
-                rc->pclasses.insert(rc->pclasses.begin(), lc);
-            else
-                rc->pclasses.clear();   // no single shared-memory size fits all: class schedule only
+        int lean_class = 0;
+        while (lean_class < kSmemClasses && kClassCtas[lean_class] != kLeanCtasPerSm) ++lean_class;
+        const uint32_t lean_bound = class_bound(lean_class);
+        std::vector<int32_t> lean, big;
+        for (int32_t i : all) (net_need(plan->druns[i], fixed) <= lean_bound ? lean : big).push_back(i);
+        // the lean queue holds its largest blob and its largest arena at once
+        for (;;) {
+            uint32_t blob = 0, arena = 0;
+            for (int32_t i : lean) {
+                blob = std::max(blob, plan->druns[i].blob_bytes);
+                arena = std::max(arena, (plan->druns[i].arena_elems + 3u) & ~3u);
+            }
+            if (lean.empty() || fixed + blob + 8 * (size_t)arena <= lean_bound) break;
+            auto worst = std::max_element(lean.begin(), lean.end(), [&](int32_t x, int32_t y) {
+                return net_need(plan->druns[x], fixed) < net_need(plan->druns[y], fixed);
+            });
+            big.push_back(*worst);
+            lean.erase(worst);
+        }
+        if (!lean.empty() && !big.empty()) {
+            std::vector<int> class_of(count, kSmemClasses);
+            for (int c = 0; c < kSmemClasses; ++c)
+                for (int32_t i : members[c]) class_of[i - first] = c;
+            for (int c = kSmemClasses - 1; c >= 0; --c) {
+                std::vector<int32_t> m;
+                for (int32_t i : big)
+                    if (class_of[i - first] == c) m.push_back(i);
+                if (!m.empty()) rc->hclasses.push_back(make_class(m, true, false));
+            }
+            LaunchClass lc = make_class(lean, true, true);
+            lc.lean = true;
+            lc.threads = kLeanThreads;
+            rc->hclasses.push_back(lc);
         }
     }
     if (!device) return build_waves(plan, members[kSmemClasses], first, terms, rc, false);
@@ -1275,6 +1385,10 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
             int r = persistent_grid(lc, rc->smem_table, &lc.grid);
             if (r) return r;
         }
+    if (!rc->hclasses.empty()) {
+        int r = hybrid_lean_grid(rc->hclasses, rc->smem_table);
+        if (r) return r;
+    }
     return build_waves(plan, members[kSmemClasses], first, terms, rc, true);
 }
 
@@ -1535,17 +1649,49 @@ static int autotune_run(qtb_plan_device* s, RunCache* rc, const RunArgs& base, v
             pers_ms = best;
         }
     }
-    rc->persistent = pers_ms < class_ms;
+    // hybrid schedule: the large-network classes with 256..1024 threads
+    float hyb_ms = 1e30f;
+    if (!rc->hclasses.empty()) {
+        int best_t = 512;
+        for (int t : {256, 512, 1024}) {
+            std::vector<LaunchClass> sched = rc->hclasses;
+            for (LaunchClass& q : sched)
+                if (!q.lean) q.threads = t;
+            if ((r = hybrid_lean_grid(sched, rc->smem_table))) return r;
+            float ms = 1e30f;
+            if ((r = time_it([&] { return launch_schedule(s, rc, sched, a, scratch_dev, st); }, &ms)))
+                return r;
+            if (log)
+                std::fprintf(stderr, "qtb autotune: hybrid schedule, large networks %4d threads %.1f us\n", t,
+                             1e3 * ms);
+            if (ms < hyb_ms) {
+                hyb_ms = ms;
+                best_t = t;
+            }
+        }
+        for (LaunchClass& q : rc->hclasses)
+            if (!q.lean) q.threads = best_t;
+        if ((r = hybrid_lean_grid(rc->hclasses, rc->smem_table))) return r;
+    }
+    rc->schedule = kSchedClasses;
+    float best_ms = class_ms;
+    if (pers_ms < best_ms) {
+        rc->schedule = kSchedPersistent;
+        best_ms = pers_ms;
+    }
+    if (hyb_ms < best_ms) rc->schedule = kSchedHybrid;
     if (log)
-        std::fprintf(stderr, "qtb autotune: class schedule %.1f us, persistent %.1f us -> %s\n",
-                     1e3 * class_ms, 1e3 * pers_ms, rc->persistent ? "persistent" : "classes");
+        std::fprintf(stderr, "qtb autotune: class schedule %.1f us, persistent %.1f us, hybrid %.1f us -> %s\n",
+                     1e3 * class_ms, 1e3 * pers_ms, 1e3 * hyb_ms,
+                     rc->schedule == kSchedHybrid ? "hybrid" : rc->schedule == kSchedPersistent ? "persistent" : "classes");
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     rc->tuned = true;
     return QTB_OK;
 }
 
-// QTB_SCHEDULE=persistent:<128|256|512> or QTB_SCHEDULE=classes in the
+// QTB_SCHEDULE=persistent:<128|256|512>, hybrid:<256|512|1024> (threads of
+// the large-network classes) or QTB_SCHEDULE=classes in the
 // environment fixes the schedule of every range without timing it, so that a
 // profiler sees one chosen configuration.  Returns 1 when it applied.
 static int forced_schedule(RunCache* rc, int* err) {
@@ -1560,9 +1706,16 @@ static int forced_schedule(RunCache* rc, int* err) {
                 q.threads = t;
                 if ((*err = persistent_grid(q, rc->smem_table, &q.grid))) return 0;
             }
-        rc->persistent = true;
+        rc->schedule = kSchedPersistent;
+    } else if (std::strncmp(env, "hybrid:", 7) == 0 && !rc->hclasses.empty()) {
+        const int t = std::atoi(env + 7);
+        if (t != 256 && t != 512 && t != 1024) return 0;
+        for (LaunchClass& q : rc->hclasses)
+            if (!q.lean) q.threads = t;
+        if ((*err = hybrid_lean_grid(rc->hclasses, rc->smem_table))) return 0;
+        rc->schedule = kSchedHybrid;
     } else if (std::strcmp(env, "classes") == 0) {
-        rc->persistent = false;
+        rc->schedule = kSchedClasses;
     } else {
         return 0;
     }
@@ -1626,7 +1779,7 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
         if (cap == cudaStreamCaptureStatusNone && (r = autotune_run(s, rc, a, scratch_dev, st))) return r;
     }
     s->last = rc;
-    const std::vector<LaunchClass>& sched = rc->persistent ? rc->pclasses : rc->classes;
+    const std::vector<LaunchClass>& sched = schedule_of(rc);
     std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
     if (s->timing) {
         if (!s->spare.empty()) {
@@ -1889,7 +2042,7 @@ int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32
         *n_classes = 0;
         return QTB_OK;
     }
-    const std::vector<LaunchClass>& sched = rc->persistent ? rc->pclasses : rc->classes;
+    const std::vector<LaunchClass>& sched = schedule_of(rc);
     *n_classes = (int32_t)(sched.size() + rc->waves.size());
     if (!out) return QTB_OK;
     for (int32_t c = 0; c < *n_classes && 4 * c + 3 < cap; ++c) {
@@ -1898,7 +2051,7 @@ int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32
             out[4 * c] = lc.n_jobs;
             out[4 * c + 1] = lc.threads;
             out[4 * c + 2] = (int32_t)lc.smem_bytes;
-            out[4 * c + 3] = (lc.smem ? 1 : 0) | (lc.persistent ? 2 : 0);
+            out[4 * c + 3] = (lc.smem ? 1 : 0) | (lc.persistent ? 2 : 0) | (lc.lean ? 8 : 0);
         } else {
             const WideWave& wv = rc->waves[c - sched.size()];
             out[4 * c] = (int32_t)wv.n_nets;

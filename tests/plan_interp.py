@@ -161,6 +161,10 @@ def run_network(exported, table, net_index):
             assert int(ph['op_first']) <= oi < int(ph['op_first'] + ph['op_count'])
             e = 32 * c
             assert starts[oi] <= e < starts[oi] + (1 << int(ops[oi]['u'] - ops[oi]['sum']))
+        # the executor's op lookup relies on ops of non-increasing size
+        widths = [int(ops[o]['u'] - ops[o]['sum'])
+                  for o in range(int(ph['op_first']), int(ph['op_first'] + ph['op_count']))]
+        assert all(a >= b for a, b in zip(widths, widths[1:]))
         writes = []
         elem = 0
         for o in range(int(ph['op_first']), int(ph['op_first'] + ph['op_count'])):

@@ -149,3 +149,24 @@ def test_wide_waves_match_plain_path(cuda_device):
     Ep = eng.energy_expectation(G, gamma, beta, path='plain')
     assert abs(E - Ep) <= TOL * abs(Ep)
     assert cg.plan.device_status() == 0
+
+
+@pytest.mark.parametrize('schedule', ['classes', 'persistent:256', 'hybrid:512', 'hybrid:1024'])
+def test_every_schedule_matches_reference(cuda_device, monkeypatch, schedule):
+    """Each executor schedule the autotuner may pick (size classes, one
+    persistent queue, large-network classes + lean queue), forced through
+    QTB_SCHEDULE, gives the reference's edge terms for all 1500 edges of the
+    N=1000 p=3 workload."""
+    monkeypatch.setenv('QTB_SCHEDULE', schedule)
+    eng = _engine()
+    G, w = golden_graph('cfg3')
+    terms = eng.edge_terms(G, w['gamma'], w['beta'])
+    ref = np.array([complex(*t) for t in w['terms']])
+    assert np.max(np.abs(terms - ref)) < TOL
+    cfg = eng.compile(G, 3, w['gamma'], w['beta']).plan.last_launch_config()
+    if schedule.startswith('hybrid'):
+        assert any(c[3] & 8 for c in cfg) and any(not c[3] & 2 for c in cfg)
+    elif schedule == 'classes':
+        assert not any(c[3] & 2 for c in cfg)
+    else:
+        assert len(cfg) == 1 and cfg[0][3] & 2 and cfg[0][1] == 256
