@@ -143,6 +143,17 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
                             int32_t p, int32_t composer, const double* params,
                             int32_t n_threads, int32_t* first_net_index);
 
+/* Batch of amplitudes <b|U|0> of one circuit (QtreeSimulator.simulate_batch,
+ * qtensor/Simulate.py:66-94, batch_vars free output qubits): for every
+ * bitstring b of qubits 0..batch_vars-1 (qubit 0 the most significant bit,
+ * the order of the reference's flattened result) and the other qubits 0,
+ * the circuit's network with those bra values fixed; 2^batch_vars circuits
+ * (groups) *first_group.. in order, each with its slices.  batch_vars 0 is
+ * qtb_plan_add_circuit (simulate / simulate_state).                       */
+int qtb_plan_add_circuit_batch(qtb_plan* plan, int32_t n_qubits, const qtb_gate* gates, int32_t n_gates,
+                               int32_t simplify_passes, const double* params, int32_t batch_vars,
+                               int32_t* net_index, int32_t* first_group);
+
 /* Slicing of circuits added afterwards (qtensor/FeynmanSimulator.py:49-84,
  * SlicesOptimizer qtensor/optimisation/Optimizer.py:90-159): when the
  * greedy width reaches max_width, variables of highest degree are removed

@@ -68,3 +68,53 @@ def qaoa_p1_edge_term(G, edge, gamma, beta):
             - 0.25 * np.sin(2 * b) ** 2 * np.cos(g) ** (du + dv - 2 * lam)
             * (1 - np.cos(2 * g) ** lam))
     return 1 - 2 * c_uv
+
+
+def _gate_matrix(name, alpha):
+    """Standard matrix of a gate (qubit order of its arguments, first
+    argument most significant); '+' suffix: conjugate transpose."""
+    dagger = name.endswith('+')
+    base = name.rstrip('+')
+    r2 = 1 / np.sqrt(2)
+    if base == 'H':
+        m = np.array([[r2, r2], [r2, -r2]])
+    elif base == 'X':
+        m = np.array([[0, 1], [1, 0]], dtype=complex)
+    elif base == 'Y':
+        m = np.array([[0, -1j], [1j, 0]])
+    elif base == 'Z':
+        m = np.diag([1, -1]).astype(complex)
+    elif base == 'T':
+        m = np.diag([1, np.exp(1j * np.pi / 4)])
+    elif base == 'cX':
+        m = np.array([[1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 0, 1], [0, 0, 1, 0]], dtype=complex)
+    elif base == 'cZ':
+        m = np.diag([1, 1, 1, -1]).astype(complex)
+    elif base == 'ZPhase':
+        m = np.diag([1, np.exp(1j * np.pi * alpha)])
+    elif base in ('XPhase', 'YPhase'):
+        c, s = np.cos(np.pi * alpha / 2), np.sin(np.pi * alpha / 2)
+        rot = (np.array([[c, -1j * s], [-1j * s, c]]) if base == 'XPhase'
+               else np.array([[c, -s], [s, c]], dtype=complex))
+        m = np.exp(1j * np.pi * alpha / 2) * rot
+    elif base == 'ZZ':
+        p = np.exp(1j * np.pi * alpha / 2)
+        m = np.diag([1 / p, p, p, 1 / p])
+    else:
+        raise ValueError(name)
+    return m.conj().T if dagger else m
+
+
+def circuit_state(gates, n_qubits):
+    """Dense ``U |0...0>`` of ``gates`` = [(name, qubits, alpha), ...],
+    applied in list order; qubit 0 is the most significant bit."""
+    psi = np.zeros(2 ** n_qubits, dtype=complex)
+    psi[0] = 1
+    psi = psi.reshape([2] * n_qubits)
+    for name, qubits, alpha in gates:
+        m = _gate_matrix(name, alpha)
+        k = len(qubits)
+        m = m.reshape([2] * (2 * k))
+        psi = np.tensordot(m, psi, axes=(list(range(k, 2 * k)), list(qubits)))
+        psi = np.moveaxis(psi, list(range(k)), list(qubits))
+    return psi.reshape(-1)

@@ -25,7 +25,8 @@ COMPOSER_DEFAULT, COMPOSER_ZZ, COMPOSER_CX = 0, 1, 2
 EXPORTS = (
     'qtb_version', 'qtb_init', 'qtb_last_error', 'qtb_bucket_c64',
     'qtb_plan_create', 'qtb_plan_destroy', 'qtb_plan_add_circuit',
-    'qtb_plan_add_lightcone', 'qtb_plan_add_lightcones', 'qtb_plan_set_max_width',
+    'qtb_plan_add_lightcone', 'qtb_plan_add_lightcones', 'qtb_plan_add_circuit_batch',
+    'qtb_plan_set_max_width',
     'qtb_plan_set_order_trials',
     'qtb_plan_n_networks',
     'qtb_plan_network_info', 'qtb_plan_network_peo', 'qtb_plan_check_params',
@@ -107,6 +108,8 @@ def _declare(lib):
         'qtb_plan_destroy': (c.c_int, [P]),
         'qtb_plan_add_circuit': (c.c_int, [P, c.c_int32, P, c.c_int32, c.c_int32, P,
                                            c.POINTER(c.c_int32)]),
+        'qtb_plan_add_circuit_batch': (c.c_int, [P, c.c_int32, P, c.c_int32, c.c_int32, P, c.c_int32,
+                                                 c.POINTER(c.c_int32), c.POINTER(c.c_int32)]),
         'qtb_plan_add_lightcone': (c.c_int, [P, c.c_int32, P, P, c.c_int32, c.c_int32,
                                              c.c_int32, c.c_int32, P, c.POINTER(c.c_int32)]),
         'qtb_plan_add_lightcones': (c.c_int, [P, c.c_int32, P, P, P, c.c_int32, c.c_int32,

@@ -412,8 +412,12 @@ static double greedy_order(int V, const std::vector<std::vector<int32_t>>& cliqu
 int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
                     int32_t simplify_passes, const double* params, int32_t n_params,
                     int32_t order_trials, int32_t max_width, int32_t max_slices,
-                    std::vector<Network>* outs, std::string* err) {
+                    int32_t batch_vars, std::vector<Network>* outs, std::string* err) {
     outs->clear();
+    if (batch_vars < 0 || batch_vars > n_qubits || batch_vars > kMaxBatchVars) {
+        *err = "compile: batch_vars must be in 0.." + std::to_string(std::min(n_qubits, kMaxBatchVars));
+        return QTB_ERR_ARG;
+    }
     std::vector<AngleCheck> checks;
     if (n_qubits <= 0 || n_gates < 0 || (n_gates > 0 && in_gates == nullptr)) {
         *err = "compile: invalid circuit arguments";
@@ -598,9 +602,13 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
     for (int32_t i = 0; i < 2 * nq; ++i) sliced[i] = 1;
     for (size_t i = 0; i < par.size(); ++i) sliced[perm[var_of[par[i]]]] = 1;
 
-    // one network per assignment of the sliced (parallel) variables
+    // one network per assignment of the sliced (parallel) variables, per
+    // output bitstring of the first batch_vars qubits (their bra variables,
+    // new ids nq + q, take the bits of `amp`, qubit 0 most significant)
+    uint64_t amp = 0;
     auto build = [&](uint64_t slice_bits, Network* out) -> int {
         std::vector<char> value(n_vars, 0);
+        for (int32_t q = 0; q < batch_vars; ++q) value[nq + q] = (char)((amp >> (batch_vars - 1 - q)) & 1u);
         for (size_t i = 0; i < par.size(); ++i)
             value[perm[var_of[par[i]]]] = (char)((slice_bits >> (par.size() - 1 - i)) & 1u);
         // ---- reorder + slice: tensors become references to gate-table entries
@@ -820,11 +828,13 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
         return QTB_OK;
     };
     const uint64_t n_slices = 1ull << par.size();
-    outs->resize(n_slices);
-    for (uint64_t sl = 0; sl < n_slices; ++sl) {
-        int rc = build(sl, &(*outs)[sl]);
-        if (rc) return rc;
-    }
+    const uint64_t n_amps = 1ull << batch_vars;
+    outs->resize(n_amps * n_slices);
+    for (amp = 0; amp < n_amps; ++amp)
+        for (uint64_t sl = 0; sl < n_slices; ++sl) {
+            int rc = build(sl, &(*outs)[amp * n_slices + sl]);
+            if (rc) return rc;
+        }
     return QTB_OK;
 }
 // ------------------------------------------------------ native lightcone
@@ -1043,12 +1053,32 @@ int qtb_plan_add_circuit(qtb_plan* plan, int32_t n_qubits, const qtb_gate* gates
     std::vector<Network> nets;
     std::string err;
     int rc = compile_circuit(n_qubits, gates, n_gates, simplify_passes, params, plan->n_params,
-                             plan->order_trials, plan->max_width, plan->max_slices, &nets, &err);
+                             plan->order_trials, plan->max_width, plan->max_slices, 0, &nets, &err);
     if (rc) return fail(rc, err);
     std::lock_guard<std::mutex> lock(plan->mu);
     if (net_index) *net_index = (int32_t)plan->nets.size();
     const int32_t group = plan->n_groups++;
     for (auto& n : nets) merge_network(plan, std::move(n), group);
+    return QTB_OK;
+}
+
+int qtb_plan_add_circuit_batch(qtb_plan* plan, int32_t n_qubits, const qtb_gate* gates, int32_t n_gates,
+                               int32_t simplify_passes, const double* params, int32_t batch_vars,
+                               int32_t* net_index, int32_t* first_group) {
+    if (!plan) return fail(QTB_ERR_ARG, "plan_add_circuit_batch: null plan");
+    std::vector<Network> nets;
+    std::string err;
+    int rc = compile_circuit(n_qubits, gates, n_gates, simplify_passes, params, plan->n_params,
+                             plan->order_trials, plan->max_width, plan->max_slices, batch_vars, &nets, &err);
+    if (rc) return fail(rc, err);
+    const size_t n_amps = size_t(1) << batch_vars;
+    const size_t per_amp = nets.size() / n_amps;
+    std::lock_guard<std::mutex> lock(plan->mu);
+    if (net_index) *net_index = (int32_t)plan->nets.size();
+    if (first_group) *first_group = plan->n_groups;
+    const int32_t group0 = plan->n_groups;
+    plan->n_groups += (int32_t)n_amps;
+    for (size_t i = 0; i < nets.size(); ++i) merge_network(plan, std::move(nets[i]), group0 + (int32_t)(i / per_amp));
     return QTB_OK;
 }
 
@@ -1088,7 +1118,7 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
             if (!rc)
                 rc = compile_circuit(nq, gates.data(), (int32_t)gates.size(), composer == 0 ? 2 : 0,
                                      params, plan->n_params, plan->order_trials, plan->max_width,
-                                     plan->max_slices, &nets[i], &errs[i]);
+                                     plan->max_slices, 0, &nets[i], &errs[i]);
             codes[i] = rc;
             if (rc) failed.store(true, std::memory_order_relaxed);
         }

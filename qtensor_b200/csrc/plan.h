@@ -143,6 +143,8 @@ struct AngleCheck {
 
 // Most variables sliced per circuit (2^k networks).
 constexpr int kMaxSlicedVars = 16;
+// Most output qubits of an amplitude batch (2^k amplitudes per circuit).
+constexpr int kMaxBatchVars = 16;
 
 struct Network {
     qtb_network_info info{};
@@ -202,7 +204,7 @@ int fail(int code, const std::string& msg);
 int compile_circuit(int32_t n_qubits, const qtb_gate* gates, int32_t n_gates,
                     int32_t simplify_passes, const double* params, int32_t n_params,
                     int32_t order_trials, int32_t max_width, int32_t max_slices,
-                    std::vector<Network>* outs, std::string* err);
+                    int32_t batch_vars, std::vector<Network>* outs, std::string* err);
 int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indices,
                     int32_t u, int32_t v, int32_t p, int32_t composer,
                     std::vector<qtb_gate>* gates, int32_t* n_qubits, std::string* err);

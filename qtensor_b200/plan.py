@@ -61,6 +61,19 @@ class NetworkPlan:
         self.uploaded = False
         return idx.value
 
+    def add_circuit_batch(self, n_qubits, gates, params, batch_vars, simplify_passes=0):
+        """Networks of the 2^batch_vars amplitudes <b|U|0> (b over qubits
+        0..batch_vars-1, qubit 0 most significant); returns (first network,
+        first group): amplitude i is group first_group + i."""
+        gates = np.ascontiguousarray(gates, dtype=_lib.GATE_DTYPE)
+        params = np.ascontiguousarray(params, dtype=np.float64)
+        idx, grp = ctypes.c_int32(), ctypes.c_int32()
+        check(self._lib.qtb_plan_add_circuit_batch(self._h, int(n_qubits), ptr(gates), len(gates),
+                                                   int(simplify_passes), ptr(params), int(batch_vars),
+                                                   ctypes.byref(idx), ctypes.byref(grp)))
+        self.uploaded = False
+        return idx.value, grp.value
+
     def add_lightcones(self, csr, edges, p, composer, params, threads=0):
         """Compile the lightcone network of every edge (pairs of node ids)."""
         _, indptr, indices = csr

@@ -1,0 +1,139 @@
+"""Amplitude simulation of arbitrary circuits on one B200.
+
+``QtreeSimulator`` mirrors the reference's ``QtreeSimulator``
+(qtensor/Simulate.py:22-94): ``simulate_batch(qc, batch_vars)`` returns the
+2^batch_vars amplitudes ``<b 0..0| U |0..0>`` over the first ``batch_vars``
+qubits, flattened with qubit 0 as the most significant bit, like the
+reference's output tensor over its free variables; ``simulate`` and
+``simulate_state`` are ``batch_vars=0``.  The contraction runs through the
+same plan compiler and device executor as the QAOA engine: every output
+bitstring is one network with its bra values fixed (plus its slices when
+the width reaches ``max_width``), all contracted in one launch.
+
+Circuits are lists of the reference's qtree gate objects -- anything with
+``name``, ``qubits`` and (for rotations) ``parameters['alpha']`` -- or a
+``qtensor_b200._lib.GATE_DTYPE`` array with its parameter vector.
+Supported gates: M, I, H, X, Y, Z, T, cX, cZ, ZPhase, XPhase, YPhase, ZZ and
+their daggers (name suffix '+': rotations with the angle negated, T+ as
+ZPhase(-1/4), the others self-adjoint).
+"""
+import numpy as np
+import torch
+
+from . import _lib
+from .plan import NetworkPlan
+
+_FIXED = {'M': _lib.GATE_M, 'H': _lib.GATE_H, 'X': _lib.GATE_X, 'Y': _lib.GATE_Y,
+          'Z': _lib.GATE_Z, 'T': _lib.GATE_T, 'cX': _lib.GATE_CX, 'cZ': _lib.GATE_CZ}
+_ROTATIONS = {'ZPhase': _lib.GATE_ZPHASE, 'XPhase': _lib.GATE_XPHASE,
+              'YPhase': _lib.GATE_YPHASE, 'ZZ': _lib.GATE_ZZ}
+
+
+def _attr(gate, name):
+    v = getattr(gate, name)
+    return v() if callable(v) else v
+
+
+def gates_from_circuit(qc):
+    """(n_qubits, gate array, params) of a list of qtree-style gate objects:
+    every rotation angle becomes its own parameter (coefficient 1)."""
+    rows, params, n_qubits = [], [], 0
+    for gate in qc:
+        name = str(_attr(gate, 'name'))
+        dagger = name.endswith('+')
+        base = name.rstrip('+')
+        qubits = [int(q) for q in _attr(gate, 'qubits')]
+        if qubits:
+            n_qubits = max(n_qubits, max(qubits) + 1)
+        if base == 'I':
+            continue
+        q0 = qubits[0]
+        q1 = qubits[1] if len(qubits) > 1 else -1
+        if base in _FIXED:
+            if base == 'T' and dagger:
+                params.append(-0.25)
+                rows.append((_lib.GATE_ZPHASE, q0, -1, len(params) - 1, 1.0))
+            else:
+                rows.append((_FIXED[base], q0, q1, -1, 0.0))
+        elif base in _ROTATIONS:
+            alpha = float(_attr(gate, 'parameters')['alpha'])
+            params.append(-alpha if dagger else alpha)
+            rows.append((_ROTATIONS[base], q0, q1, len(params) - 1, 1.0))
+        else:
+            raise NotImplementedError('gate {!r} is not supported'.format(name))
+    return n_qubits, np.array(rows, dtype=_lib.GATE_DTYPE), np.array(params, dtype=np.float64)
+
+
+class QtreeSimulator:
+    """``simulate_batch`` / ``simulate`` / ``simulate_state`` of the reference
+    simulator, contracted on the GPU (complex64 products, amplitudes summed
+    over slices in fp64 on the host).
+
+    max_tw: like the reference, a ``ValueError`` when the contraction width
+    exceeds it (before slicing); max_width / max_slices: circuits whose width
+    reaches max_width are sliced into at most max_slices networks per
+    amplitude; order_trials: extra randomized greedy orders per network."""
+
+    def __init__(self, device=None, max_tw=None, max_width=26, max_slices=256, order_trials=8):
+        if not torch.cuda.is_available():
+            raise RuntimeError('qtensor_b200 needs a CUDA device; there is no CPU fallback')
+        self.device = torch.device('cuda', torch.cuda.current_device() if device is None else device)
+        self.max_tw = max_tw
+        self.max_width = max_width
+        self.max_slices = max_slices
+        self.order_trials = order_trials
+        _lib.check(_lib.lib().qtb_init(self.device.index))
+        self.plan = None
+
+    def _compile(self, qc, batch_vars, params=None):
+        if isinstance(qc, np.ndarray):
+            gates = np.ascontiguousarray(qc, dtype=_lib.GATE_DTYPE)
+            params = np.zeros(0) if params is None else np.asarray(params, dtype=np.float64)
+            used = [int(g['q0']) for g in gates] + [int(g['q1']) for g in gates if g['q1'] >= 0]
+            n_qubits = max(used) + 1 if used else 0
+        else:
+            n_qubits, gates, params = gates_from_circuit(qc)
+        n_qubits = max(n_qubits, batch_vars, 1)
+        plan = NetworkPlan(len(params))
+        plan.set_order_trials(self.order_trials)
+        plan.set_max_width(self.max_width, self.max_slices)
+        first, group0 = plan.add_circuit_batch(n_qubits, gates, params, batch_vars)
+        if self.max_tw is not None:
+            width = max(i['treewidth'] for i in plan.infos())
+            if width > self.max_tw:
+                plan.close()
+                raise ValueError('Treewidth {} is larger than max_tw={}.'.format(width, self.max_tw))
+        return plan, params, group0
+
+    def simulate_batch(self, qc, batch_vars=0, peo=None, params=None):
+        """Amplitudes of the 2^batch_vars output bitstrings of qubits
+        0..batch_vars-1 (others 0), qubit 0 the most significant bit."""
+        if peo is not None:
+            raise NotImplementedError('a given elimination order is not supported; '
+                                      'the plan compiler chooses its own')
+        plan, params, group0 = self._compile(qc, int(batch_vars), params)
+        try:
+            with torch.cuda.device(self.device):
+                plan.upload()
+                n = len(plan)
+                params_dev = torch.from_numpy(params).to(self.device) if len(params) else None
+                terms = torch.empty(n, dtype=torch.complex64, device=self.device)
+                nbytes = plan.scratch_bytes(0, n)
+                scratch = torch.empty(nbytes, dtype=torch.uint8, device=self.device) if nbytes else None
+                stream = torch.cuda.current_stream(self.device)
+                plan.run(0, n, params_dev, terms, None, scratch, stream.cuda_stream)
+                vals = terms.cpu().numpy().astype(np.complex128)
+                status = plan.device_status()
+                if status:
+                    raise _lib.QtbError(_lib.QTB_ERR_DEVICE, 'device status word {:#x}'.format(status))
+            out = np.zeros(1 << int(batch_vars), dtype=np.complex128)
+            np.add.at(out, plan.groups() - group0, vals)
+            return out
+        finally:
+            plan.close()
+
+    def simulate(self, qc):
+        return self.simulate_state(qc)
+
+    def simulate_state(self, qc, peo=None):
+        return self.simulate_batch(qc, batch_vars=0, peo=peo)

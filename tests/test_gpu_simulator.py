@@ -1,0 +1,41 @@
+"""QtreeSimulator on the GPU against the reference's simulate_batch fixtures
+(seeded random circuits of H, X, Y, Z, T, cX, cZ, ZPhase, XPhase, YPhase,
+ZZ and their daggers; batch_vars up to 5), with and without slicing."""
+import numpy as np
+import pytest
+
+from test_batch_amplitudes import CASES, Gate, amplitudes, circuit
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+@pytest.mark.parametrize('ci', range(len(CASES)))
+def test_simulate_batch_matches_reference(cuda_device, ci):
+    from qtensor_b200.simulator import QtreeSimulator
+    case = CASES[ci]
+    sim = QtreeSimulator()
+    for k in case['amplitudes']:
+        got = sim.simulate_batch(circuit(case), batch_vars=int(k))
+        assert np.max(np.abs(got - amplitudes(case, int(k)))) < TOL
+    state = sim.simulate(circuit(case))
+    assert state.shape == (1,) and abs(state[0] - amplitudes(case, 0)[0]) < TOL
+
+
+def test_simulate_batch_sliced(cuda_device):
+    from qtensor_b200.simulator import QtreeSimulator
+    case = CASES[2]
+    got = QtreeSimulator(max_width=3).simulate_batch(circuit(case), batch_vars=2)
+    assert np.max(np.abs(got - amplitudes(case, 2))) < TOL
+
+
+def test_simulator_errors_like_reference(cuda_device):
+    from qtensor_b200.simulator import QtreeSimulator
+    case = CASES[1]
+    with pytest.raises(ValueError, match='max_tw'):
+        QtreeSimulator(max_tw=1).simulate_batch(circuit(case), batch_vars=1)
+    with pytest.raises(NotImplementedError):
+        QtreeSimulator().simulate_batch(circuit(case), peo=[0, 1])
+    with pytest.raises(NotImplementedError):
+        QtreeSimulator().simulate([Gate('SWAP', [0, 1])])
