@@ -67,9 +67,15 @@ __device__ __forceinline__ uint32_t gather_bits(uint32_t j, const DevIn& d, uint
 }
 
 // ----------------------------------------------------------------- K1
+// Operand t of output element j: the bits of j its mask selects, gathered by
+// the precompiled runs (mask, runs as in DevIn), and with the summed
+// variable set, `stride[t]` further (the summed variable is the operand's
+// most significant axis; stride 0 when the operand does not hold it).
 struct BucketArgs {
     const float2* in[QTB_MAX_BUCKET_INPUTS];
+    uint64_t runs[QTB_MAX_BUCKET_INPUTS];
     uint32_t mask[QTB_MAX_BUCKET_INPUTS];
+    uint32_t stride[QTB_MAX_BUCKET_INPUTS];
     float2* out;
     int32_t k;
     int32_t w;     // output variables
@@ -78,17 +84,33 @@ struct BucketArgs {
 
 __global__ void __launch_bounds__(256) qtb_bucket_kernel(const BucketArgs a) {
     const uint64_t n_out = 1ull << a.w;
-    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n_out;
-         j += (uint64_t)gridDim.x * blockDim.x) {
-        float2 acc = make_float2(0.f, 0.f);
-        for (int s = 0; s <= a.sum; ++s) {
-            const uint32_t idx = (uint32_t)j | ((uint32_t)s << a.w);
-            float2 prod = a.in[0][pext32(idx, a.mask[0])];
-            for (int t = 1; t < a.k; ++t) prod = cmul(prod, a.in[t][pext32(idx, a.mask[t])]);
-            acc = s == 0 ? prod : make_float2(acc.x + prod.x, acc.y + prod.y);
+    const uint32_t low = a.w >= 32 ? 0xffffffffu : (1u << a.w) - 1u;
+    for (uint64_t jj = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; jj < n_out;
+         jj += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t j = (uint32_t)jj;
+        float2 p0 = make_float2(1.f, 0.f), p1 = make_float2(1.f, 0.f);
+        for (int t = 0; t < a.k; ++t) {
+            DevIn d;
+            d.mask = a.mask[t];
+            d.src = 0;
+            d.runs = a.runs[t];
+            const uint32_t off = gather_bits(j, d, low);
+            const float2 x0 = a.in[t][off];
+            const float2 x1 = (a.sum && a.stride[t]) ? a.in[t][off + a.stride[t]] : x0;
+            p0 = t == 0 ? x0 : cmul(p0, x0);
+            p1 = t == 0 ? x1 : cmul(p1, x1);
         }
-        a.out[j] = acc;
+        a.out[j] = a.sum ? make_float2(p0.x + p1.x, p0.y + p1.y) : p0;
     }
+}
+
+// Gathers of operand t of a bucket over n_vars variables (variable 0 at
+// mask bit n_vars - 1, summed when sum_first).
+static void bucket_operand(BucketArgs* a, int t, uint32_t mask, int n_vars, int sum_first) {
+    const uint32_t w = (uint32_t)(n_vars - sum_first);
+    a->mask[t] = mask;
+    a->runs[t] = encode_runs(mask, w);
+    a->stride[t] = (sum_first && ((mask >> w) & 1u)) ? 1u << (__builtin_popcount(mask) - 1) : 0u;
 }
 
 // ----------------------------------------------------------------- K0
@@ -563,6 +585,7 @@ static_assert(sizeof(WideStep) == 32, "WideStep layout");
 constexpr uint32_t kWideSpinLimit = 1u << 24;
 constexpr int kWideThreads = 256;
 constexpr uint32_t kWideBatch = 4;                                  // elements per thread in flight
+constexpr uint32_t kWideGroup = 1;                                  // operands per batch of loads
 constexpr uint32_t kWideMinTile = kWideBatch * kWideThreads;         // 1024
 constexpr uint32_t kWideMaxTile = 8 * kWideMinTile;
 
@@ -638,8 +661,9 @@ __device__ __forceinline__ void compute_element_wide(const DevOp& op, uint32_t j
 // Four elements j, j + 256, j + 512, j + 768 of one op at once, bits 8 and
 // 9 of j zero: the four differ from j only in those bits, so each operand
 // offset is the gathered offset of j plus the gathered bits 8 and 9 (one
-// full gather per operand, not four), and the loads of two operands for all
-// four elements are issued together (eight L2 requests in flight per thread).
+// full gather per operand, not four), and the loads of kWideGroup operands
+// for all four elements are issued together (eight L2 requests in flight per
+// thread and operand).
 __device__ __forceinline__ void compute_elements_wide4(const DevOp& op, uint32_t j, const DevIn* ins,
                                                        const float2* __restrict__ table,
                                                        float2* __restrict__ arena) {
@@ -649,14 +673,14 @@ __device__ __forceinline__ void compute_elements_wide4(const DevOp& op, uint32_t
     float2 p0[kWideBatch], p1[kWideBatch];
 #pragma unroll
     for (uint32_t e = 0; e < kWideBatch; ++e) p0[e] = p1[e] = make_float2(1.f, 0.f);
-    for (uint32_t t0 = 0; t0 < op.k; t0 += 2) {
-        DevIn d[2];
+    for (uint32_t t0 = 0; t0 < op.k; t0 += kWideGroup) {
+        DevIn d[kWideGroup];
 #pragma unroll
-        for (int t = 0; t < 2; ++t)
+        for (int t = 0; t < kWideGroup; ++t)
             if (t0 + t < op.k) d[t] = ldg_in(in + t0 + t);
-        float2 x0[2][kWideBatch], x1[2][kWideBatch];
+        float2 x0[kWideGroup][kWideBatch], x1[kWideGroup][kWideBatch];
 #pragma unroll
-        for (int t = 0; t < 2; ++t) {
+        for (int t = 0; t < kWideGroup; ++t) {
             if (t0 + t < op.k) {
                 const bool tab = d[t].src & kSrcTable;
                 const float2* base = tab ? table + (d[t].src & ~kSrcTable) : arena + d[t].src;
@@ -679,7 +703,7 @@ __device__ __forceinline__ void compute_elements_wide4(const DevOp& op, uint32_t
             }
         }
 #pragma unroll
-        for (int t = 0; t < 2; ++t) {
+        for (int t = 0; t < kWideGroup; ++t) {
             if (t0 + t < op.k) {
 #pragma unroll
                 for (uint32_t e = 0; e < kWideBatch; ++e) {
@@ -694,7 +718,7 @@ __device__ __forceinline__ void compute_elements_wide4(const DevOp& op, uint32_t
         arena[op.dst + j + e * 256u] = op.sum ? make_float2(p0[e].x + p1[e].x, p0[e].y + p1[e].y) : p0[e];
 }
 
-__global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArgs w, const RunArgs a) {
+__global__ void __launch_bounds__(kWideThreads, 3) qtb_wide_kernel(const WideArgs w, const RunArgs a) {
     __shared__ uint32_t s_tile;
     __shared__ int s_ok, s_last;
     for (;;) {
@@ -1424,7 +1448,7 @@ int qtb_bucket_c64(const qtb_bucket_desc* d, const void* const* inputs, void* ou
         if (!inputs[t]) return fail(QTB_ERR_ARG, "bucket: null input pointer");
         if (d->masks[t] & ~all) return fail(QTB_ERR_ARG, "bucket: mask names a variable outside the union");
         a.in[t] = static_cast<const float2*>(inputs[t]);
-        a.mask[t] = d->masks[t];
+        bucket_operand(&a, t, d->masks[t], d->n_vars, d->sum_first);
     }
     a.out = static_cast<float2*>(output);
     a.k = d->n_inputs;
@@ -1874,7 +1898,7 @@ int qtb_plan_run_plain(qtb_plan* plan, int32_t first, int32_t count, const doubl
             for (int t = 0; t < op.k; ++t) {
                 const DevIn& in = plan->dins[op.in_begin + t];
                 a.in[t] = (in.src & kSrcTable) ? table + (in.src & ~kSrcTable) : arena + in.src;
-                a.mask[t] = in.mask;
+                bucket_operand(&a, t, in.mask, op.u, op.sum);
             }
             a.out = arena + op.dst;
             a.k = op.k;
