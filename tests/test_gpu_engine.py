@@ -170,3 +170,14 @@ def test_every_schedule_matches_reference(cuda_device, monkeypatch, schedule):
         assert not any(c[3] & 2 for c in cfg)
     else:
         assert len(cfg) == 1 and cfg[0][3] & 2 and cfg[0][1] == 256
+
+
+def test_reference_named_simulator(cuda_device):
+    """QAOAQtreeSimulator under the reference's method names."""
+    from qtensor_b200.qaoa import QAOAQtreeSimulator
+    G, w = golden_graph('cfg2')
+    sim = QAOAQtreeSimulator('default')
+    for E in (sim.energy_expectation(G, w['gamma'], w['beta']),
+              sim.energy_expectation_parallel(G, w['gamma'], w['beta'], n_processes=8),
+              sim.energy_expectation_mpi(G, w['gamma'], w['beta'])):
+        assert abs(E - w['energy']) <= TOL * abs(w['energy'])

@@ -41,3 +41,28 @@ def test_backend_needs_cuda_loudly(monkeypatch):
     monkeypatch.setattr(torch.cuda, 'is_available', lambda: False)
     with pytest.raises(RuntimeError, match='no CPU fallback'):
         B200Backend().get_sliced_buckets([[]], {}, {})
+
+
+def test_composer_names_follow_the_reference():
+    from qtensor_b200.qaoa import composer_name
+
+    class DefaultQAOAComposer:
+        pass
+
+    class ZZQtreeQAOAComposer:
+        pass
+
+    assert composer_name(DefaultQAOAComposer) == 'default'
+    assert composer_name(ZZQtreeQAOAComposer) == 'zz'
+    assert composer_name('cx') == 'cx'
+    with pytest.raises(ValueError):
+        composer_name('qiskit')
+
+
+def test_simulators_need_cuda_loudly(monkeypatch):
+    from qtensor_b200 import simulator, qaoa
+    monkeypatch.setattr(torch.cuda, 'is_available', lambda: False)
+    with pytest.raises(RuntimeError, match='no CPU fallback'):
+        simulator.QtreeSimulator()
+    with pytest.raises(RuntimeError, match='no CPU fallback'):
+        qaoa.QAOAQtreeSimulator()
