@@ -117,17 +117,6 @@ uint64_t encode_runs(uint32_t mask, uint32_t w) {
     return runs | (n << 60);
 }
 
-uint64_t fast_fields(const DevIn& in, uint32_t op_w, bool op_sum, uint32_t table_elems) {
-    if ((in.runs >> 60) > 1) return 0;   // multi-run gathers keep their encoding
-    const uint32_t table_pad = (table_elems + 1u) & ~1u;   // table bytes rounded up to 16
-    const uint32_t base = (in.src & kSrcTable) ? (in.src & ~kSrcTable) : table_pad + in.src;
-    if (base > 0xffffu) return 0;
-    const bool has_sum = op_sum && ((in.mask >> op_w) & 1u);
-    const uint32_t slog = has_sum ? (uint32_t)__builtin_popcount(in.mask) - 1u : 0u;
-    const uint64_t hi = ((uint64_t)base << 5) | (has_sum ? kFastSum : 0u) | ((uint64_t)slog << 22) | kFastValid;
-    return hi << 32;
-}
-
 // ------------------------------------------------------------- simplifier
 namespace {
 
@@ -1011,14 +1000,7 @@ void build_blobs(qtb_plan* plan) {
         uint8_t* dst = plan->dblobs.data() + base;
         std::memcpy(dst, phases.data(), ph_bytes);     // op_first already network-local
         std::memcpy(dst + ph_bytes, n.ops.data(), op_bytes);   // in_begin network-local
-        // single-run operands get their unified shared-memory address
-        std::vector<DevIn> ins = n.ins;
-        for (const DevOp& op : n.ops)
-            for (uint32_t t = 0; t < op.k; ++t) {
-                DevIn& in = ins[op.in_begin + t];
-                in.runs |= fast_fields(in, (uint32_t)(op.u - op.sum), op.sum != 0, plan->table_elems);
-            }
-        std::memcpy(dst + ph_bytes + op_bytes, ins.data(), in_bytes);
+        std::memcpy(dst + ph_bytes + op_bytes, n.ins.data(), in_bytes);
         if (!chunks.empty())
             std::memcpy(dst + chunk_base, chunks.data(), chunks.size() * sizeof(uint16_t));
         plan->druns.push_back(r);

@@ -35,14 +35,6 @@ struct DevOp {
 //           bits [start, start+len) of j to the next free operand bits
 //           (runs in increasing start order, packed from bit 0 up);
 //   n == kRunsFallback: more runs than kMaxRuns, gather bit by bit.
-// Single-run operands in a network blob also carry, in bits 37..59, their
-// address in the executor's unified shared-memory space (gate table, then
-// the arena at the table's size rounded up to 16 bytes), so a kernel whose
-// table and arena are both in shared memory reads them without decoding:
-//   bits 37..52  base: unified complex64 offset of the operand
-//   bit  53      the op sums and this operand holds the summed variable
-//   bits 54..58  log2 of that variable's stride in the operand
-//   bit  59      the fields above are valid (base fits in 16 bits)
 struct DevIn {
     uint32_t mask;      // bit (u-1-v) set <=> union variable v is an axis
     uint32_t src;       // arena offset, or kSrcTable | gate-table offset
@@ -50,10 +42,6 @@ struct DevIn {
 };
 constexpr int kMaxRuns = 6;
 constexpr uint64_t kRunsFallback = 7;
-constexpr uint32_t kFastValid = 1u << 27;   // bit 59 of runs, as bit 27 of its high word
-constexpr uint32_t kFastSum = 1u << 21;     // bit 53
-// Unified-address fields of a single-run operand (see DevIn).
-uint64_t fast_fields(const DevIn& in, uint32_t op_w, bool op_sum, uint32_t table_elems);
 
 // Ops of one dependency level; a barrier follows every phase.  In a network
 // blob, chunk_off is the byte offset of the phase's chunk table: for every

@@ -315,13 +315,10 @@ __device__ __forceinline__ uint32_t find_op(uint32_t g, uint32_t oi, DevOp& op, 
 
 // One output element j of op: the product of its operands gathered at j
 // (and at j with the summed bit set), summed over the bucket variable.
-// Operands are handled in groups of four so their descriptor and value
-// loads issue together instead of as one dependent chain per operand.
-//   kUnified: table and arena both in shared memory, the arena at
-//   table + round-up-to-16-bytes(table): single-run operands carrying their
-//   unified address (DevIn fast fields) are read without decoding.
-//   kGroup: operands whose loads are issued together (fewer registers when 2).
-template <bool kSmemTable, bool kUnified, int kGroup = 4>
+// Operands are taken one at a time: most ops have two or three, and a fixed
+// group of operand slots would issue predicated-off instructions for the
+// absent ones (measured: 84 -> 68 us per N=1000 p=3 step).
+template <bool kSmemTable>
 __device__ __forceinline__ void compute_element(const DevOp& op, uint32_t j, const DevIn* ins,
                                                 const float2* __restrict__ table,
                                                 float2* __restrict__ arena) {
@@ -329,57 +326,21 @@ __device__ __forceinline__ void compute_element(const DevOp& op, uint32_t j, con
     const uint32_t low = (1u << w) - 1u;
     const DevIn* in = ins + op.in_begin;
     float2 p0 = make_float2(1.f, 0.f), p1 = make_float2(1.f, 0.f);
-    if (kUnified) {
-        // every operand fast: one 8-byte descriptor load, a shift, a mask
-        bool all_fast = true;
-        for (uint32_t t = 0; t < op.k; ++t) {
-            const uint64_t r = in[t].runs;
-            const uint32_t hi = (uint32_t)(r >> 32);
-            if (!(hi & kFastValid)) {
-                all_fast = false;
-                break;
-            }
-            const uint32_t off = ((hi >> 5) & 0xffffu) + ((j >> (hi & 31u)) & (uint32_t)r);
-            const float2 x0 = table[off];
-            const float2 x1 = (hi & kFastSum) ? table[off + (1u << ((hi >> 22) & 31u))] : x0;
-            p0 = t == 0 ? x0 : cmul(p0, x0);
-            p1 = t == 0 ? x1 : cmul(p1, x1);
+    for (uint32_t t = 0; t < op.k; ++t) {
+        const DevIn d = in[t];
+        const uint32_t off = gather_bits(j, d, low);
+        const bool tab = d.src & kSrcTable;
+        const float2* base = tab ? table + (d.src & ~kSrcTable) : arena + d.src;
+        const float2 x0 = (tab && !kSmemTable) ? __ldg(base + off) : base[off];
+        float2 x1 = x0;
+        // the summed variable is union bit w and, in an operand that has it,
+        // that operand's most significant axis: a fixed stride
+        if (op.sum && ((d.mask >> w) & 1u)) {
+            const uint32_t stride = 1u << (__popc(d.mask) - 1);
+            x1 = (tab && !kSmemTable) ? __ldg(base + off + stride) : base[off + stride];
         }
-        if (all_fast) {
-            arena[op.dst + j] = op.sum ? make_float2(p0.x + p1.x, p0.y + p1.y) : p0;
-            return;
-        }
-        p0 = p1 = make_float2(1.f, 0.f);
-    }
-    for (uint32_t t0 = 0; t0 < op.k; t0 += kGroup) {
-        DevIn d[kGroup];
-#pragma unroll
-        for (int t = 0; t < kGroup; ++t)
-            if (t0 + t < op.k) d[t] = in[t0 + t];
-        float2 x0[kGroup], x1[kGroup];
-#pragma unroll
-        for (int t = 0; t < kGroup; ++t) {
-            if (t0 + t < op.k) {
-                const uint32_t off = gather_bits(j, d[t], low);
-                const bool tab = d[t].src & kSrcTable;
-                const float2* base = tab ? table + (d[t].src & ~kSrcTable) : arena + d[t].src;
-                x0[t] = (tab && !kSmemTable) ? __ldg(base + off) : base[off];
-                x1[t] = x0[t];
-                // the summed variable is union bit w and, in an operand that
-                // has it, that operand's most significant axis: a fixed stride
-                if (op.sum && ((d[t].mask >> w) & 1u)) {
-                    const uint32_t stride = 1u << (__popc(d[t].mask) - 1);
-                    x1[t] = (tab && !kSmemTable) ? __ldg(base + off + stride) : base[off + stride];
-                }
-            }
-        }
-#pragma unroll
-        for (int t = 0; t < kGroup; ++t) {
-            if (t0 + t < op.k) {
-                p0 = (t0 + t == 0) ? x0[t] : cmul(p0, x0[t]);
-                p1 = (t0 + t == 0) ? x1[t] : cmul(p1, x1[t]);
-            }
-        }
+        p0 = t == 0 ? x0 : cmul(p0, x0);
+        p1 = t == 0 ? x1 : cmul(p1, x1);
     }
     arena[op.dst + j] = op.sum ? make_float2(p0.x + p1.x, p0.y + p1.y) : p0;
 }
@@ -412,7 +373,7 @@ __device__ void build_table(const unsigned char* common, const RunArgs& a, float
 }
 
 // The phases of one staged network; its scalar result is returned to thread 0.
-template <bool kSmemTable, bool kUnified, int kGroup = 4>
+template <bool kSmemTable>
 __device__ float2 contract_network(const DevNetRun& net, const unsigned char* blob,
                                    const float2* __restrict__ table, float2* __restrict__ arena) {
     const DevPhase* phases = reinterpret_cast<const DevPhase*>(blob);
@@ -434,7 +395,7 @@ __device__ float2 contract_network(const DevNetRun& net, const unsigned char* bl
                 oi = find_op(g, oi, op, [&](uint32_t i) { return ops[i]; });
                 op_end = op.elem_begin + (1u << (op.u - op.sum));
             }
-            compute_element<kSmemTable, kUnified, kGroup>(op, g - op.elem_begin, ins, table, arena);
+            compute_element<kSmemTable>(op, g - op.elem_begin, ins, table, arena);
         }
         __syncthreads();
     }
@@ -446,7 +407,7 @@ __device__ float2 contract_network(const DevNetRun& net, const unsigned char* bl
             if (g < ph.total_elems) {
                 DevOp op = ops[ph.op_first];
                 find_op(g, ph.op_first, op, [&](uint32_t i) { return ops[i]; });
-                compute_element<kSmemTable, kUnified, kGroup>(op, g - op.elem_begin, ins, table, arena);
+                compute_element<kSmemTable>(op, g - op.elem_begin, ins, table, arena);
             }
             __syncwarp();
         }
@@ -519,8 +480,7 @@ __global__ void __launch_bounds__(kLean ? 128 : (kPersistent ? 512 : 1024), kLea
         }
         const unsigned char* nblob =
             staged ? blob : reinterpret_cast<const unsigned char*>(a.blobs + net.blob_off16);
-        const float2 term = contract_network<kSmemTable, kSmemTable && kSmemArena && !kLean, kLean ? 2 : 4>(
-            net, nblob, table, arena);
+        const float2 term = contract_network<kSmemTable>(net, nblob, table, arena);
         if (threadIdx.x == 0) {
             *job.term = term;
             if (a.energy) {

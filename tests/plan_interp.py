@@ -92,28 +92,6 @@ def _gather_runs(j, runs):
     return off
 
 
-def _check_fast_fields(d, off, sv, s, w, table_elems):
-    """The unified shared-memory address of a single-run operand (runs bits
-    37..59): base = gate-table offset, or the arena offset after the table
-    rounded up to 16 bytes; the summed variable's stride as its log2."""
-    runs = int(d['runs'])
-    hi = runs >> 32
-    if not (hi >> 27) & 1:      # multi-run gather, or base beyond 16 bits
-        return
-    assert (runs >> 60) <= 1
-    src = int(d['src'])
-    table_pad = (table_elems + 1) & ~1
-    base = src & ~_lib.SRC_TABLE if src & _lib.SRC_TABLE else table_pad + src
-    assert (hi >> 5) & 0xffff == base
-    mask = int(d['mask'])
-    has_sum = bool(s) and bool((mask >> w) & 1)
-    assert bool((hi >> 21) & 1) == has_sum
-    stride = (1 << ((hi >> 22) & 31)) if has_sum else 0
-    j = np.arange(1 << w, dtype=np.int64)
-    fast = ((j >> (hi & 31)) & (runs & 0xffffffff)) + sv * stride
-    assert np.array_equal(fast, off)
-
-
 def network_views(exported, net_index):
     """Phases, ops and operands of one network, decoded from its executor
     blob exactly as the device kernel addresses them (network-local)."""
@@ -188,7 +166,6 @@ def run_network(exported, table, net_index):
                         top = (mask >> w) & 1 if s else 0
                         stride = 1 << (bin(mask).count('1') - 1) if top else 0
                         assert np.array_equal(off, low + sv * stride)
-                    _check_fast_fields(d, off, sv, s, w, exported['table_elems'])
                     prod = prod * load(int(d['src']), off)
                 acc = acc + prod
             writes.append((int(op['dst']), acc))
