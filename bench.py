@@ -280,11 +280,12 @@ def measured_peak_hbm():
 
 
 def profiled_traffic():
-    """DRAM bytes per executor launch from the committed ncu summary, if any."""
+    """DRAM bytes of the executor's launches per step, from the committed
+    ncu summary, if any."""
     path = os.path.join(ROOT, 'profiles', 'network_kernel_cfg3.json')
     try:
         with open(path) as f:
-            return json.load(f).get('dram_bytes_per_launch')
+            return json.load(f).get('dram_bytes_per_step')
     except (OSError, ValueError):
         return None
 

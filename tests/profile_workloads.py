@@ -1,0 +1,115 @@
+"""Workloads for the ncu captures summarised under profiles/ (measurement
+infrastructure, not collected as tests).  Each mode runs a small, fixed
+amount of work and checks its result, so that the same command can run once
+without the profiler and then under it.
+
+    python tests/profile_workloads.py cfg3        # 3-regular N=1000 p=3, 20 executor steps
+    python tests/profile_workloads.py er400       # Erdos-Renyi N=400 p=3 (wide waves), 3 runs
+    python tests/profile_workloads.py bucket24    # one 24-variable bucket through qtb_bucket_c64, 5 runs
+    python tests/profile_workloads.py plain_cfg1  # 3-regular N=20 p=1 through the plain per-bucket path
+
+QTB_SCHEDULE (see qtb.cu) fixes the executor schedule, so that the
+profiler's serialised replays cannot steer the autotuner.
+"""
+import ctypes
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path[:0] = [ROOT, os.path.join(ROOT, 'tests')]
+
+import networkx as nx  # noqa: E402
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+import graphs  # noqa: E402
+from conftest import golden_graph  # noqa: E402
+from qtensor_b200 import _lib  # noqa: E402
+from qtensor_b200.engine import QAOAEnergyEngine  # noqa: E402
+
+
+def cfg3():
+    G, w = golden_graph('cfg3')
+    eng = QAOAEnergyEngine()
+    cg = eng.compile(G, 3, w['gamma'], w['beta'])
+    cg.params.copy_(torch.from_numpy(np.concatenate([w['gamma'], w['beta']])))
+    graph = cg.device_graph()
+    for _ in range(20):
+        graph.replay()
+    torch.cuda.synchronize()
+    E = float(cg.energy.cpu()[0])
+    assert abs(E - w['energy']) <= 1e-5 * abs(w['energy']), (E, w['energy'])
+    assert cg.plan.device_status() == 0
+    print('launch classes', cg.plan.last_launch_config())
+
+
+def er400():
+    G = nx.erdos_renyi_graph(400, 3 / 399, seed=24323709)
+    g, b = graphs.angles(3, seed=1)
+    eng = QAOAEnergyEngine(max_width=22, autotune=False)
+    cg = eng.compile(G, 3, g, b)
+    cg.params.copy_(torch.from_numpy(np.concatenate([g, b])))
+    for _ in range(3):
+        cg.launch()
+    torch.cuda.synchronize()
+    assert cg.plan.device_status() == 0
+    print('launch classes', cg.plan.last_launch_config())
+
+
+def bucket24():
+    """One bucket of 24 binary variables, variable 0 summed: A over every
+    variable but the lowest (2^23 elements), B over variable 0 and the 12
+    lowest (2^13), a gate over variable 0 and the lowest (2^2); output 2^23
+    (64 MB read, 64 MB written)."""
+    lib = _lib.lib()
+    _lib.check(lib.qtb_init(0))
+    u = 24
+    masks = [((1 << u) - 1) & ~1, (1 << (u - 1)) | 0xfff, (1 << (u - 1)) | 1]
+    gen = torch.Generator(device='cuda').manual_seed(0)
+    ins = [torch.randn(1 << bin(m).count('1'), dtype=torch.complex64, device='cuda', generator=gen)
+           for m in masks]
+    out = torch.empty(1 << (u - 1), dtype=torch.complex64, device='cuda')
+    desc = _lib.BucketDesc()
+    desc.n_inputs, desc.n_vars, desc.sum_first = 3, u, 1
+    for i, m in enumerate(masks):
+        desc.masks[i] = m
+    ptrs = (ctypes.c_void_p * 3)(*[x.data_ptr() for x in ins])
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(5):
+        s.record()
+        _lib.check(lib.qtb_bucket_c64(ctypes.byref(desc), ptrs, ctypes.c_void_p(out.data_ptr()),
+                                      ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        e.record()
+        e.synchronize()
+        print('bucket %.1f us' % (1e3 * s.elapsed_time(e)))
+    A, B, C = [x.cpu().numpy() for x in ins]
+    o = out.cpu().numpy()
+
+    def pext(x, m):
+        r, bit = 0, 0
+        for b in range(32):
+            if (m >> b) & 1:
+                r |= ((x >> b) & 1) << bit
+                bit += 1
+        return r
+    for j in [0, 1, 12345, (1 << 23) - 1]:
+        acc = 0
+        for sbit in range(2):
+            idx = j | (sbit << (u - 1))
+            acc += A[pext(idx, masks[0])] * B[pext(idx, masks[1])] * C[pext(idx, masks[2])]
+        assert abs(acc - o[j]) < 1e-3 * max(1, abs(acc)), (j, acc, o[j])
+
+
+def plain_cfg1():
+    G, w = golden_graph('cfg1_default')
+    eng = QAOAEnergyEngine()
+    for _ in range(2):
+        t = eng.edge_terms(G, w['gamma'], w['beta'], path='plain')
+        eng.energy_expectation(G, w['gamma'], w['beta'], path='plain')
+    ref = np.array([complex(*x) for x in w['terms']])
+    assert np.max(np.abs(t - ref)) < 1e-5
+
+
+if __name__ == '__main__':
+    {'cfg3': cfg3, 'er400': er400, 'bucket24': bucket24, 'plain_cfg1': plain_cfg1}[sys.argv[1]]()
+    print('ok', sys.argv[1])
