@@ -57,6 +57,8 @@ def parse():
     ap.add_argument('--nodes', type=int, default=1000)
     ap.add_argument('--p', type=int, default=3)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--plain-steps', type=int, default=3,
+                    help='steps of the plain per-bucket comparison (0 skips it)')
     ap.add_argument('--serving-requests', type=int, default=128,
                     help='requests of the serving run (0 skips it)')
     ap.add_argument('--serving-rate', type=float, default=20.0,
@@ -269,6 +271,77 @@ def oracle_error(eng, G, p):
             'oracle': 'complex128 reference values, tests/golden/qaoa_reference.json'}
 
 
+# ------------------------------------------------------------------ plain backend by width
+def plain_width_classes(device_index, reps=10, per_class=64):
+    """The drop-in bucket kernel (qtb_bucket_c64, BucketBackend.process_bucket)
+    per bucket output-width class, on the real bucket shapes of the 3-regular
+    N=100 p=3 workload's plans (up to `per_class` buckets per width, random
+    complex64 operands of their shapes, launched back to back), plus one
+    24-variable bucket (64 MB in, 64 MB out) for the bandwidth-bound end.
+    GB/s of algorithmic bytes 8 (sum of inputs + output)."""
+    import ctypes
+    import torch
+    from qtensor_b200 import _lib
+    from qtensor_b200.engine import QAOAEnergyEngine
+    lib = _lib.lib()
+    dev = torch.device('cuda', device_index)
+    G2 = graphs.regular(100, seed=0)
+    g, b = graphs.angles(3, seed=0)
+    ex = QAOAEnergyEngine(device=device_index).compile(G2, 3, g, b).plan.export()
+    ops, ins = ex['ops'], ex['ins']
+    classes = {}
+    for o in ops:
+        classes.setdefault(int(o['u']) - int(o['sum']), []).append(o)
+    gen = torch.Generator(device=dev).manual_seed(0)
+
+    def time_buckets(descs, nbytes):
+        stream = torch.cuda.current_stream(dev)
+        for d, ptrs, out in descs:    # warm-up
+            _lib.check(lib.qtb_bucket_c64(ctypes.byref(d), ptrs, out, ctypes.c_void_p(stream.cuda_stream)))
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(reps):
+            for d, ptrs, out in descs:
+                _lib.check(lib.qtb_bucket_c64(ctypes.byref(d), ptrs, out, ctypes.c_void_p(stream.cuda_stream)))
+        e.record(stream)
+        e.synchronize()
+        ms = s.elapsed_time(e) / reps
+        return {'buckets': len(descs), 'us_per_bucket': 1e3 * ms / len(descs),
+                'gbs': nbytes / (ms / 1e3) / 1e9}
+
+    def make(masks, n_vars, sum_first, keep):
+        d = _lib.BucketDesc()
+        d.n_inputs, d.n_vars, d.sum_first = len(masks), n_vars, sum_first
+        bufs, nbytes = [], 0
+        for i, m in enumerate(masks):
+            d.masks[i] = m
+            t = torch.randn(1 << bin(m).count('1'), dtype=torch.complex64, device=dev, generator=gen)
+            bufs.append(t)
+            nbytes += 8 * t.numel()
+        out = torch.empty(1 << (n_vars - sum_first), dtype=torch.complex64, device=dev)
+        nbytes += 8 * out.numel()
+        keep.extend(bufs + [out])
+        ptrs = (ctypes.c_void_p * len(masks))(*[t.data_ptr() for t in bufs])
+        return (d, ptrs, ctypes.c_void_p(out.data_ptr())), nbytes
+
+    result, keep = {}, []
+    for w in sorted(classes):
+        descs, nbytes = [], 0
+        for o in classes[w][:per_class]:
+            masks = [int(ins[int(o['in_begin']) + t]['mask']) for t in range(int(o['k']))]
+            dsc, nb = make(masks, int(o['u']), int(o['sum']), keep)
+            descs.append(dsc)
+            nbytes += nb
+        result['w%d' % w] = time_buckets(descs, nbytes)
+    u = 24
+    dsc, nb = make([((1 << u) - 1) & ~1, (1 << (u - 1)) | 0xfff, (1 << (u - 1)) | 1], u, 1, keep)
+    result['bucket24'] = time_buckets([dsc], nb)
+    return {'workload': 'bucket shapes of the 3-regular N=100 p=3 plans by output width (up to {} per '
+                        'class, back to back, {} repetitions) and one 24-variable bucket; GB/s of '
+                        'algorithmic bytes'.format(per_class, reps),
+            'classes': result}
+
+
 # ------------------------------------------------------------------ GPU arm
 def measured_peak_hbm():
     path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
@@ -396,9 +469,10 @@ def run_b200(args):
 
     # ---- the plain path: one bucket-kernel launch per bucket over the same
     # plans (the drop-in backend's kernel), a few steps
-    plain_steps = 3
-    cg.params.copy_(params_dev[0])
-    cg.launch_plain()
+    plain_steps = args.plain_steps
+    if plain_steps:
+        cg.params.copy_(params_dev[0])
+        cg.launch_plain()
     plain_ms = []
     for i in range(plain_steps):
         flush.fill_(float(i))
@@ -409,9 +483,10 @@ def run_b200(args):
         e.record(stream)
         e.synchronize()
         plain_ms.append(s.elapsed_time(e))
-    plain_ms_step = sum(plain_ms) / plain_steps
+    plain_ms_step = sum(plain_ms) / plain_steps if plain_steps else float('nan')
 
     errors = oracle_error(eng, G, p) if rank == 0 else None
+    plain_widths = plain_width_classes(local) if rank == 0 and args.plain_steps > 0 else None
     serving = None
     if rank == 0 and world == 1 and args.serving_requests > 0:
         serving = run_serving(args.serving_requests, args.serving_rate, local)
@@ -458,7 +533,8 @@ def run_b200(args):
                     'd2h_bytes_per_step': 8, 'ms_per_step': e2e_total / args.steps},
             'clocks': clk,
             'error_vs_oracle': errors,
-            'plain': {'value': stats['edges'] / (plain_ms_step / 1e3), 'unit': UNIT,
+            'plain_by_width': plain_widths,
+            'plain': None if not plain_steps else {'value': stats['edges'] / (plain_ms_step / 1e3), 'unit': UNIT,
                       'ms_per_step': plain_ms_step, 'steps': plain_steps,
                       'bucket_launches_per_step': stats['ops'],
                       'what': 'same plans, one qtb_bucket_kernel launch per bucket (the '
