@@ -248,8 +248,22 @@ int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32
  * lists), excluding the caller's terms/energy/scratch buffers.            */
 int qtb_plan_device_bytes(const qtb_plan* plan, size_t* bytes);
 
-/* Device error word of the last run on this plan (0 = ok); synchronises. */
+/* Device error word of the last run on this plan (0 = ok); synchronises.
+ * Bits: 1 arena larger than the launch's capacity, 2 a staging copy did not
+ * complete in time, 4 plan blob larger than the launch's capacity, 8
+ * persistent launch without its queue, 16 a wide-network step waited too
+ * long for its predecessor.  Every device wait is bounded: a kernel that
+ * gives up sets its bit and returns; no kernel traps.                      */
 int qtb_plan_device_status(qtb_plan* plan, int32_t* status);
+
+#define QTB_STATUS_WAIT_TIMEOUT 16
+
+/* Failure-detection self-test (no counterpart in the reference): one thread
+ * waits, with the executor's bounded counter wait (a wide-network step
+ * waiting for its predecessor), on a counter that nothing increments; after
+ * spin_limit polls it gives up and sets QTB_STATUS_WAIT_TIMEOUT in a status
+ * word returned in *status_out.  Synchronous; the device stays usable.    */
+int qtb_selftest_wait_timeout(int32_t spin_limit, int32_t* status_out);
 
 /* CUDA-event timing of the network-executor launches of qtb_plan_run, on
  * the run's stream.  set_timing resets the totals; collect_timing waits for

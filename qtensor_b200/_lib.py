@@ -34,6 +34,8 @@ EXPORTS = (
     'qtb_plan_scratch_bytes', 'qtb_plan_run', 'qtb_plan_plain_scratch_bytes',
     'qtb_plan_run_plain', 'qtb_plan_set_autotune',
     'qtb_plan_last_launch_config', 'qtb_plan_device_bytes', 'qtb_plan_device_status',
+    'qtb_selftest_wait_timeout',
+    'qtb_selftest_wait_timeout',
     'qtb_plan_set_timing', 'qtb_plan_collect_timing', 'qtb_plan_run_noalloc',
 )
 NOALLOC_SCRATCH_BYTES = 64 << 20
@@ -92,6 +94,7 @@ RUN_DTYPE = np.dtype([('blob_off16', '<u4'), ('blob_bytes', '<u4'), ('n_phases',
                       ('ins_off', '<u4'), ('arena_elems', '<u4'), ('result_src', '<u4'),
                       ('max_elems', '<u4'), ('tail_start', '<u4')])
 SRC_TABLE = 0x80000000
+STATUS_WAIT_TIMEOUT = 16
 
 _lib = None
 
@@ -129,6 +132,7 @@ def _declare(lib):
         'qtb_plan_last_launch_config': (c.c_int, [P, P, c.c_int32, c.POINTER(c.c_int32)]),
         'qtb_plan_device_bytes': (c.c_int, [P, c.POINTER(c.c_size_t)]),
         'qtb_plan_device_status': (c.c_int, [P, c.POINTER(c.c_int32)]),
+        'qtb_selftest_wait_timeout': (c.c_int, [c.c_int32, c.POINTER(c.c_int32)]),
         'qtb_plan_set_timing': (c.c_int, [P, c.c_int32]),
         'qtb_plan_collect_timing': (c.c_int, [P, c.POINTER(c.c_double), c.POINTER(c.c_int64)]),
         'qtb_plan_run_noalloc': (c.c_int, [P, c.c_int32, c.c_int32, P, P, P, P]),

@@ -216,7 +216,7 @@ constexpr int kStatusStageTimeout = 2; // a staging copy did not complete in tim
 constexpr int kStatusBlob = 4;         // network blob larger than the launch's capacity
 constexpr int kStatusQueue = 8;        // persistent launch without a job queue
 constexpr int kStatusWideTimeout = 16; // a wide-network step waited too long for its predecessor
-constexpr uint32_t kStageSpinLimit = 1u << 26;
+constexpr uint32_t kStageSpinLimit = 1u << 25;   // about 1.5 s of polling
 constexpr uint32_t kSmemTableLimitElems = 2048;   // 16 KB of gate table per CTA
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -542,7 +542,7 @@ struct WideArgs {
 
 static_assert(sizeof(WideNet) == 32, "WideNet layout");
 static_assert(sizeof(WideStep) == 32, "WideStep layout");
-constexpr uint32_t kWideSpinLimit = 1u << 24;
+constexpr uint32_t kWideSpinLimit = 1u << 23;   // about 1 s of polling
 constexpr int kWideThreads = 256;
 constexpr uint32_t kWideBatch = 4;                                  // elements per thread in flight
 constexpr uint32_t kWideGroup = 1;                                  // operands per batch of loads
@@ -553,6 +553,21 @@ __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
     unsigned int v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
+}
+
+// Bounded wait until *counter reaches need (acquire).  Returns false after
+// `limit` polls, having set `flag` in *status.
+__device__ bool wait_counter(const unsigned int* counter, unsigned int need, uint32_t limit, int* status,
+                             int flag) {
+    uint32_t it = 0;
+    while (ld_acquire(counter) < need) {
+        if (++it > limit) {
+            atomicOr(status, flag);
+            return false;
+        }
+        if (it > 16) __nanosleep(128);
+    }
+    return true;
 }
 
 __device__ __forceinline__ DevIn ldg_in(const DevIn* p) {
@@ -698,18 +713,9 @@ __global__ void __launch_bounds__(kWideThreads, 3) qtb_wide_kernel(const WideArg
         }
         if (threadIdx.x == 0) {
             s_ok = 1;
-            if (s > 0) {
-                const uint32_t need = __ldg(&w.steps[s - 1].n_tiles);
-                uint32_t it = 0;
-                while (ld_acquire(w.counters + s) < need) {
-                    if (++it > kWideSpinLimit) {
-                        atomicOr(a.status, kStatusWideTimeout);
-                        s_ok = 0;
-                        break;
-                    }
-                    if (it > 16) __nanosleep(128);
-                }
-            }
+            if (s > 0 && !wait_counter(w.counters + s, __ldg(&w.steps[s - 1].n_tiles), kWideSpinLimit,
+                                       a.status, kStatusWideTimeout))
+                s_ok = 0;
             __threadfence();
         }
         __syncthreads();
@@ -1879,6 +1885,42 @@ int qtb_plan_run_plain(qtb_plan* plan, int32_t first, int32_t count, const doubl
         QTB_CUDA(cudaGetLastError());
     }
     return QTB_OK;
+}
+
+// ------------------------------------------------- failure detection self-test
+}  // extern "C"
+
+namespace qtb {
+
+// One thread waits, with the executor's bounded wait, on a counter that
+// nothing increments; it gives up after `limit` polls and reports through
+// the status word, as a wide-network step whose predecessor never finishes
+// would.  Only the counter word and the status word are touched.
+__global__ void qtb_selftest_wait_kernel(const unsigned int* counter, uint32_t limit, int* status) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) wait_counter(counter, 1u, limit, status, kStatusWideTimeout);
+}
+
+}  // namespace qtb
+
+extern "C" {
+
+int qtb_selftest_wait_timeout(int32_t spin_limit, int32_t* status_out) {
+    if (!status_out || spin_limit < 1) return fail(QTB_ERR_ARG, "selftest_wait_timeout: bad arguments");
+    void* buf = nullptr;
+    QTB_CUDA(cudaMalloc(&buf, 16));
+    int r = QTB_OK;
+    unsigned int* counter = static_cast<unsigned int*>(buf);
+    int* status = reinterpret_cast<int*>(static_cast<char*>(buf) + 8);
+    cudaError_t e = cudaMemset(buf, 0, 16);
+    if (e == cudaSuccess) {
+        qtb_selftest_wait_kernel<<<1, 32>>>(counter, (uint32_t)spin_limit, status);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(status_out, status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) r = cuda_fail(e, "selftest_wait_timeout");
+    cudaFree(buf);
+    return r;
 }
 
 // ------------------------------------------------- allocation-free run
