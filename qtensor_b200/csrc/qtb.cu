@@ -9,12 +9,19 @@
 //                            generated from the request's angles (qtree gate
 //                            tensors, OpFactory.py:44-58), the buckets in
 //                            dependency phases with intermediates in shared
-//                            memory (or a per-CTA global arena), and in the
-//                            last CTA to finish the fp64 Neumaier sum of the
-//                            edge terms with the MaxCut post-processing
-//                            (QAOASimulator.py:27-41)
+//                            memory (a per-CTA global arena in the
+//                            allocation-free run), and in the last CTA to
+//                            finish the fp64 Neumaier sum of the edge terms
+//                            with the MaxCut post-processing
+//                            (QAOASimulator.py:27-41); class, persistent,
+//                            lean-persistent and hybrid schedules
+//   K4  qtb_wide_kernel      networks too large for shared memory, in waves
+//                            contracted by the whole GPU one elimination
+//                            phase at a time (tile queue, bounded waits)
 //   K0  qtb_table_kernel     the gate table in global memory, for plans whose
-//                            table does not fit in shared memory
+//                            table does not fit in shared memory and for
+//                            wide waves
+//   qtb_energy_kernel        the energy of a plain (per-bucket) run
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -835,7 +842,7 @@ constexpr uint32_t kSmemReservePerCta = 1024;
 // goes to the class of the most CTAs per SM its staging + arena allows).
 constexpr int kClassCtas[] = {16, 12, 10, 8, 6, 5, 4, 3, 2, 1};
 constexpr int kSmemClasses = (int)(sizeof(kClassCtas) / sizeof(kClassCtas[0]));
-constexpr int kMaxClasses = kSmemClasses + 1;   // + the global-arena class
+constexpr int kMaxClasses = kSmemClasses + 1;   // + the stream of the wide waves
 constexpr int kLeanThreads = 128;
 constexpr int kLeanCtasPerSm = 8;
 
@@ -849,7 +856,7 @@ struct LaunchClass {
     int threads;
     int n_jobs;
     size_t job_offset;      // into the job buffer
-    size_t scratch_offset;  // elements into scratch (global-arena class)
+    size_t scratch_offset;  // elements into scratch (classes without a shared arena)
     size_t smem_bytes;
 };
 
@@ -1094,9 +1101,9 @@ static int class_threads(uint32_t max_elems, int n_jobs) {
     return t;
 }
 
-// Launch classes of a run: networks bucketed by the shared memory they need
-// (16 KB, 48 KB, 112 KB, 224 KB; larger arenas go to global scratch), the
-// widest class first so its long critical path starts early.
+// Shared memory every CTA of a run needs besides its network's blob and
+// arena: the mbarrier, and with a shared gate table the plan-wide entries,
+// angle terms and the table itself.
 static size_t fixed_smem(const qtb_plan* plan, bool smem_table) {
     if (!smem_table) return 16;
     const size_t table = ((size_t)plan->table_elems * 8 + 15) & ~size_t(15);
@@ -1229,7 +1236,7 @@ static int build_waves(qtb_plan* plan, std::vector<int32_t> wide, int32_t first,
 
 // Launch classes of a run: each network goes to the shared-memory class of
 // the most resident CTAs per SM its staging + arena allows (networks too
-// large for shared memory use a global arena), the largest class launched
+// large for shared memory run as wide waves), the largest class launched
 // first so its long critical path starts early.
 static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms, RunCache* rc,
                      bool device = true) {
@@ -1242,7 +1249,7 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
     for (int32_t i = first; i < first + count; ++i) {
         const DevNetRun& r = plan->druns[i];
         const size_t need = net_need(r, fixed);
-        int c = kSmemClasses;   // global arena
+        int c = kSmemClasses;   // too large for shared memory: a wide wave
         for (int b = 0; b < kSmemClasses; ++b)
             if (need <= class_bound(b)) {
                 c = b;
