@@ -242,18 +242,26 @@ int simplify(std::vector<Gate>* gates, std::vector<AngleCheck>* checks, bool* an
         }
         cir[i] = make_sgate(sk, g.q, g.angle, g.expr);
     }
+    // same-site pairs (i < j) visited by distance j - i, ties in order of i:
+    // the reference's visiting order, with pairs formed within groups of
+    // gates of the same kind on the same qubits instead of over all pairs
+    std::map<std::tuple<int, int, int, int>, std::vector<int>> sites;
+    for (int i = 0; i < n; ++i)
+        sites[std::make_tuple(cir[i].kind, cir[i].nq, cir[i].q[0], cir[i].nq > 1 ? cir[i].q[1] : -1)].push_back(i);
     std::vector<std::pair<int, int>> pairs;
-    for (int i = 0; i + 1 < n; ++i)
-        for (int j = i + 1; j < n; ++j)
-            if (same_site(cir[i], cir[j])) pairs.emplace_back(i, j);
+    for (const auto& kv : sites) {
+        const std::vector<int>& g = kv.second;
+        for (size_t x = 0; x + 1 < g.size(); ++x)
+            for (size_t y = x + 1; y < g.size(); ++y)
+                if (same_site(cir[g[x]], cir[g[y]])) pairs.emplace_back(g[x], g[y]);
+    }
     if (pairs.empty()) return QTB_OK;
-    std::vector<int> order(pairs.size());
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-        return pairs[x].second - pairs[x].first < pairs[y].second - pairs[y].first;
+    std::sort(pairs.begin(), pairs.end(), [](const std::pair<int, int>& x, const std::pair<int, int>& y) {
+        const int dx = x.second - x.first, dy = y.second - y.first;
+        return dx != dy ? dx < dy : x.first < y.first;
     });
-    for (int idx : order) {
-        const int a = pairs[idx].first, b = pairs[idx].second;
+    for (const auto& pr : pairs) {
+        const int a = pr.first, b = pr.second;
         if (cir[a].kind == SK_ID || cir[b].kind == SK_ID) continue;
         bool ok = true;
         for (int m = a + 1; m < b && ok; ++m) ok = commute(cir[a], cir[m]);
@@ -315,12 +323,16 @@ struct OpRec {
 
 }  // namespace
 
-// Greedy min-degree order over the line graph (nodes in first-appearance
-// order); returns the order and the degree of every eliminated node.  With
-// seed == 0 ties go to the first node in order (the reference's rule,
-// qtensor/utils.py:30-32); otherwise a deterministic xorshift stream picks
-// uniformly among the tied nodes (the zero-temperature limit of
-// RGreedyOptimizer, qtensor/optimisation/RGreedy.py:36-62).
+// Greedy minimum-degree elimination on the line graph (cliques = tensors,
+// nodes in first-appearance order); returns the order and the degree of
+// every eliminated node.  seed 0: the reference's rule, the first node
+// (lowest index) of least distinct-neighbour count (qtensor/utils.py:30-32);
+// other seeds: a uniformly random node among those of least count
+// (xorshift64 on the seed; the zero-temperature limit of RGreedyOptimizer,
+// qtensor/optimisation/RGreedy.py:36-62).  Nodes of each degree are
+// kept in a bitset, so the lowest-index node of least degree is the lowest
+// set bit of the least non-empty bucket and the k-th tie its k-th set bit.
+// Returns sum over eliminations of 2^degree.
 static double greedy_order(int V, const std::vector<std::vector<int32_t>>& cliques, uint64_t seed,
                            std::vector<int32_t>* order, std::vector<int32_t>* degrees,
                            const std::vector<char>* removed = nullptr) {
@@ -342,32 +354,61 @@ static double greedy_order(int V, const std::vector<std::vector<int32_t>>& cliqu
                     ++deg[b];
                 }
             }
-    std::vector<int32_t> alive;
+    // degree buckets over the alive nodes
+    std::vector<std::vector<uint64_t>> bucket;
+    std::vector<int32_t> bucket_count;
+    auto bucket_of = [&](int d) -> std::vector<uint64_t>& {
+        if ((int)bucket.size() <= d) {
+            bucket.resize(d + 1);
+            bucket_count.resize(d + 1, 0);
+        }
+        if (bucket[d].empty()) bucket[d].assign(W, 0);
+        return bucket[d];
+    };
+    auto add = [&](int x, int d) {
+        bucket_of(d)[x >> 6] |= 1ull << (x & 63);
+        ++bucket_count[d];
+    };
+    auto del = [&](int x, int d) {
+        bucket[d][x >> 6] &= ~(1ull << (x & 63));
+        --bucket_count[d];
+    };
+    int n_alive = 0;
     for (int x = 0; x < V; ++x)
-        if (!gone(x)) alive.push_back(x);
-    std::vector<int32_t> nbrs, ties;
+        if (!gone(x)) {
+            add(x, deg[x]);
+            ++n_alive;
+        }
+    std::vector<int32_t> nbrs;
     uint64_t rng = seed;
     double cost = 0.0;
     order->clear();
     degrees->clear();
-    while (!alive.empty()) {
-        size_t best = 0;
+    for (; n_alive > 0; --n_alive) {
+        int dmin = 0;
+        while (bucket_count[dmin] == 0) ++dmin;
+        const std::vector<uint64_t>& bk = bucket[dmin];
+        int x = -1;
         if (seed == 0) {
-            for (size_t i = 1; i < alive.size(); ++i)
-                if (deg[alive[i]] < deg[alive[best]]) best = i;
+            for (int w = 0; w < W && x < 0; ++w)
+                if (bk[w]) x = w * 64 + __builtin_ctzll(bk[w]);
         } else {
-            int32_t dmin = deg[alive[0]];
-            for (size_t i = 1; i < alive.size(); ++i) dmin = std::min(dmin, deg[alive[i]]);
-            ties.clear();
-            for (size_t i = 0; i < alive.size(); ++i)
-                if (deg[alive[i]] == dmin) ties.push_back((int32_t)i);
             rng ^= rng << 13;
             rng ^= rng >> 7;
             rng ^= rng << 17;
-            best = (size_t)ties[rng % ties.size()];
+            int k = (int)(rng % (uint64_t)bucket_count[dmin]);
+            for (int w = 0; w < W && x < 0; ++w) {
+                const int c = __builtin_popcountll(bk[w]);
+                if (k >= c) {
+                    k -= c;
+                    continue;
+                }
+                uint64_t bits = bk[w];
+                for (; k > 0; --k) bits &= bits - 1;
+                x = w * 64 + __builtin_ctzll(bits);
+            }
         }
-        const int x = alive[best];
-        alive.erase(alive.begin() + best);
+        del(x, dmin);
         nbrs.clear();
         for (int w = 0; w < W; ++w) {
             uint64_t bits = adj[(size_t)x * W + w];
@@ -382,6 +423,7 @@ static double greedy_order(int V, const std::vector<std::vector<int32_t>>& cliqu
         cost += std::ldexp(1.0, (int)nbrs.size());
         for (int a : nbrs) {
             clr(a, x);
+            del(a, deg[a]);
             --deg[a];
         }
         for (size_t i = 0; i < nbrs.size(); ++i)
@@ -394,6 +436,7 @@ static double greedy_order(int V, const std::vector<std::vector<int32_t>>& cliqu
                     ++deg[b];
                 }
             }
+        for (int a : nbrs) add(a, deg[a]);
     }
     return cost;
 }
@@ -401,7 +444,8 @@ static double greedy_order(int V, const std::vector<std::vector<int32_t>>& cliqu
 int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
                     int32_t simplify_passes, const double* params, int32_t n_params,
                     int32_t order_trials, int32_t max_width, int32_t max_slices,
-                    int32_t batch_vars, std::vector<Network>* outs, std::string* err) {
+                    int32_t batch_vars, std::vector<Network>* outs, std::string* err,
+                    const std::atomic<bool>* abort) {
     outs->clear();
     if (batch_vars < 0 || batch_vars > n_qubits || batch_vars > kMaxBatchVars) {
         *err = "compile: batch_vars must be in 0.." + std::to_string(std::min(n_qubits, kMaxBatchVars));
@@ -544,6 +588,7 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
     int slice_budget = 0;
     while (slice_budget < kMaxSlicedVars && (2ll << slice_budget) <= (long long)max_slices) ++slice_budget;
     while (max_width > 0 && width() >= max_width) {
+        if (abort && abort->load(std::memory_order_relaxed)) return kCompileAborted;
         // removing one variable lowers the treewidth by at most one, so a
         // width more than twice the remaining budget above the target is
         // out of reach: fail now instead of after the whole budget
@@ -742,6 +787,7 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
         struct Live { uint32_t off, size; int32_t end; };
         std::vector<Live> active;
         uint32_t arena = 0, max_elems = 1;
+        // `active` stays sorted by offset: first fit over the live intervals
         for (int32_t oi : by_level) {
             OpRec& op = ops[oi];
             active.erase(std::remove_if(active.begin(), active.end(),
@@ -750,14 +796,16 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
             const uint32_t size = 1u << op.w;
             max_elems = std::max(max_elems, size);
             const uint32_t need = (size + 3u) & ~3u;
-            std::sort(active.begin(), active.end(), [](const Live& a, const Live& b) { return a.off < b.off; });
             uint32_t off = 0;
             for (const Live& l : active) {
                 if (off + need <= l.off) break;
                 off = std::max(off, l.off + l.size);
             }
             op.dst = off;
-            active.push_back({off, need, op.consumer_level});
+            const Live item{off, need, op.consumer_level};
+            active.insert(std::upper_bound(active.begin(), active.end(), item,
+                                           [](const Live& a, const Live& b) { return a.off < b.off; }),
+                          item);
             arena = std::max(arena, off + need);
         }
 
@@ -1100,9 +1148,9 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
             if (!rc)
                 rc = compile_circuit(nq, gates.data(), (int32_t)gates.size(), composer == 0 ? 2 : 0,
                                      params, plan->n_params, plan->order_trials, plan->max_width,
-                                     plan->max_slices, 0, &nets[i], &errs[i]);
+                                     plan->max_slices, 0, &nets[i], &errs[i], &failed);
             codes[i] = rc;
-            if (rc) failed.store(true, std::memory_order_relaxed);
+            if (rc && rc != kCompileAborted) failed.store(true, std::memory_order_relaxed);
         }
     };
     int nt = n_threads > 0 ? n_threads : (int)std::thread::hardware_concurrency();
@@ -1111,8 +1159,9 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
     for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
     worker();
     for (auto& t : pool) t.join();
-    for (int32_t i = 0; i < n_edges; ++i)
-        if (codes[i]) return fail(codes[i], "edge " + std::to_string(i) + ": " + errs[i]);
+    for (int32_t i = 0; i < n_edges; ++i)   // the first genuine failure (not an abort)
+        if (codes[i] && codes[i] != kCompileAborted)
+            return fail(codes[i], "edge " + std::to_string(i) + ": " + errs[i]);
     std::lock_guard<std::mutex> lock(plan->mu);
     if (first_net_index) *first_net_index = (int32_t)plan->nets.size();
     for (auto& circuit : nets) {

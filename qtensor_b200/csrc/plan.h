@@ -1,6 +1,7 @@
 // Internal plan structures shared by the host plan compiler (plan.cpp) and
 // the device executor (qtb.cu).  Not part of the public C ABI.
 #pragma once
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <mutex>
@@ -192,7 +193,10 @@ int fail(int code, const std::string& msg);
 int compile_circuit(int32_t n_qubits, const qtb_gate* gates, int32_t n_gates,
                     int32_t simplify_passes, const double* params, int32_t n_params,
                     int32_t order_trials, int32_t max_width, int32_t max_slices,
-                    int32_t batch_vars, std::vector<Network>* outs, std::string* err);
+                    int32_t batch_vars, std::vector<Network>* outs, std::string* err,
+                    const std::atomic<bool>* abort = nullptr);
+// compile_circuit's result when `abort` was raised while it ran.
+constexpr int kCompileAborted = -1;
 int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indices,
                     int32_t u, int32_t v, int32_t p, int32_t composer,
                     std::vector<qtb_gate>* gates, int32_t* n_qubits, std::string* err);
