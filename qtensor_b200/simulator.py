@@ -137,3 +137,36 @@ class QtreeSimulator:
 
     def simulate_state(self, qc, peo=None):
         return self.simulate_batch(qc, batch_vars=0, peo=peo)
+
+
+class FeynmanSimulator(QtreeSimulator):
+    """``FeynmanSimulator.simulate`` / ``simulate_batch_adaptive``
+    (qtensor/FeynmanSimulator.py:27-100): the circuit is sliced over parallel
+    variables, chosen greedily by degree until its width drops below
+    ``max_tw - tw_bias`` (``SlicesOptimizer``, qtensor/optimisation/
+    Optimizer.py:88-160), and the amplitudes of all 2^k paths are summed.
+    Here every path is one network of a single launch, so ``pool_type`` and
+    ``n_processes`` have nothing to do.  ``max_tw`` defaults, like the
+    reference's memory rule, to log2 of the device's free bytes over the
+    8-byte complex64 element.  At most ``max_slices`` paths per amplitude."""
+
+    def __init__(self, *args, pool_type='process', n_processes=None, max_tw=None, max_slices=4096,
+                 **kwargs):
+        super().__init__(*args, max_slices=max_slices, **kwargs)
+        self.slice_max_tw = max_tw
+        self.pool_type = pool_type
+        self.n_processes = 2 if n_processes is None else n_processes
+
+    def _target_width(self, tw_bias):
+        max_tw = self.slice_max_tw
+        if max_tw is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            max_tw = int(np.log2(free)) - 3
+        return max(1, int(max_tw) - int(tw_bias))
+
+    def simulate(self, qc, batch_vars=0, tw_bias=2):
+        return self.simulate_batch_adaptive(qc, batch_vars, tw_bias=tw_bias)
+
+    def simulate_batch_adaptive(self, qc, batch_vars=0, tw_bias=2):
+        self.max_width = self._target_width(tw_bias)
+        return self.simulate_batch(qc, batch_vars=batch_vars)

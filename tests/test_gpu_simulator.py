@@ -39,3 +39,14 @@ def test_simulator_errors_like_reference(cuda_device):
         QtreeSimulator().simulate_batch(circuit(case), peo=[0, 1])
     with pytest.raises(NotImplementedError):
         QtreeSimulator().simulate([Gate('SWAP', [0, 1])])
+
+
+def test_feynman_simulator_matches_reference(cuda_device):
+    """FeynmanSimulator semantics: sliced below max_tw - tw_bias, paths summed."""
+    from qtensor_b200.simulator import FeynmanSimulator
+    case = CASES[2]
+    sim = FeynmanSimulator(max_tw=5, n_processes=4)
+    got = sim.simulate(circuit(case), batch_vars=2, tw_bias=2)
+    assert np.max(np.abs(got - amplitudes(case, 2))) < TOL
+    got0 = FeynmanSimulator().simulate_batch_adaptive(circuit(case))
+    assert abs(got0[0] - amplitudes(case, 0)[0]) < TOL
