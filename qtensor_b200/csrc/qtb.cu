@@ -551,7 +551,9 @@ static_assert(sizeof(WideNet) == 32, "WideNet layout");
 static_assert(sizeof(WideStep) == 32, "WideStep layout");
 constexpr uint32_t kWideSpinLimit = 1u << 23;   // about 1 s of polling
 constexpr int kWideThreads = 256;
-constexpr uint32_t kWideBatch = 4;                                  // elements per thread in flight
+constexpr uint32_t kWideBatchLog = 2;                               // log2 of the elements per thread in flight
+constexpr uint32_t kWideBatch = 1u << kWideBatchLog;
+constexpr uint32_t kWideBatchBits = (kWideBatch - 1u) << 8;          // the bits of j above the thread index
 constexpr uint32_t kWideGroup = 1;                                  // operands per batch of loads
 constexpr uint32_t kWideMinTile = kWideBatch * kWideThreads;         // 1024
 constexpr uint32_t kWideMaxTile = 8 * kWideMinTile;
@@ -640,13 +642,13 @@ __device__ __forceinline__ void compute_element_wide(const DevOp& op, uint32_t j
     arena[op.dst + j] = op.sum ? make_float2(p0.x + p1.x, p0.y + p1.y) : p0;
 }
 
-// Four elements j, j + 256, j + 512, j + 768 of one op at once, bits 8 and
-// 9 of j zero: the four differ from j only in those bits, so each operand
-// offset is the gathered offset of j plus the gathered bits 8 and 9 (one
-// full gather per operand, not four), and the loads of kWideGroup operands
-// for all four elements are issued together (eight L2 requests in flight per
-// thread and operand).
-__device__ __forceinline__ void compute_elements_wide4(const DevOp& op, uint32_t j, const DevIn* ins,
+// kWideBatch elements j + 256 e of one op at once, with the kWideBatchLog
+// bits of j from bit 8 up zero: they differ from j only in those bits, so
+// each operand offset is the gathered offset of j plus the gathered offsets
+// of those bits (one full gather per operand, not kWideBatch), and the
+// loads of kWideGroup operands for all elements are issued together
+// (2 kWideBatch L2 requests in flight per thread and operand).
+__device__ __forceinline__ void compute_elements_wide(const DevOp& op, uint32_t j, const DevIn* ins,
                                                        const float2* __restrict__ table,
                                                        float2* __restrict__ arena) {
     const uint32_t w = op.u - op.sum;
@@ -669,13 +671,21 @@ __device__ __forceinline__ void compute_elements_wide4(const DevOp& op, uint32_t
                 const bool has_sum = op.sum && ((d[t].mask >> w) & 1u);
                 const uint32_t stride_s = has_sum ? 1u << (__popc(d[t].mask) - 1) : 0u;
                 const uint32_t m = d[t].mask & low;
-                const uint32_t b8 = ((m >> 8) & 1u) << __popc(m & 0xffu);
-                const uint32_t b9 = ((m >> 9) & 1u) << __popc(m & 0x1ffu);
+                // bit 8 + i of j lands at operand bit popc(m below it) when m has it
+                uint32_t bit_off[kWideBatchLog];
+#pragma unroll
+                for (uint32_t i = 0; i < kWideBatchLog; ++i)
+                    bit_off[i] = ((m >> (8 + i)) & 1u) << __popc(m & ((1u << (8 + i)) - 1u));
                 uint32_t off[kWideBatch];
                 off[0] = gather_bits(j, d[t], low);
-                off[1] = off[0] + b8;
-                off[2] = off[0] + b9;
-                off[3] = off[0] + b8 + b9;
+#pragma unroll
+                for (uint32_t e = 1; e < kWideBatch; ++e) {
+                    uint32_t o = off[0];
+#pragma unroll
+                    for (uint32_t i = 0; i < kWideBatchLog; ++i)
+                        if ((e >> i) & 1u) o += bit_off[i];
+                    off[e] = o;
+                }
 #pragma unroll
                 for (uint32_t e = 0; e < kWideBatch; ++e) {
                     x0[t][e] = tab ? __ldg(base + off[e]) : __ldcg(base + off[e]);
@@ -802,13 +812,13 @@ __global__ void __launch_bounds__(kWideThreads, 3) qtb_wide_kernel(const WideArg
                 op_lo = op.elem_begin;
                 op_hi = op.elem_begin + (1u << (op.u - op.sum));
             }
-            // four elements of the same op that differ only in bits 8 and 9
-            // of the op index (the common case in wide phases: tiles,
-            // segments and ops start at multiples of 1024)
+            // kWideBatch elements of the same op that differ only in the bits
+            // from bit 8 up of the op index (the common case in wide phases:
+            // tiles, segments and ops start at multiples of kWideMinTile)
             const uint32_t j = l - op.elem_begin;
-            if (bd == 256u && (j & 0x300u) == 0u && g + (kWideBatch - 1) * bd < min(e1, seg_hi) &&
+            if (bd == 256u && (j & kWideBatchBits) == 0u && g + (kWideBatch - 1) * bd < min(e1, seg_hi) &&
                 l + (kWideBatch - 1) * bd < op_hi) {
-                compute_elements_wide4(op, j, ins, a.gtable, arena);
+                compute_elements_wide(op, j, ins, a.gtable, arena);
                 g += kWideBatch * bd;
             } else {
                 compute_element_wide(op, j, ins, a.gtable, arena);

@@ -181,3 +181,17 @@ def test_reference_named_simulator(cuda_device):
               sim.energy_expectation_parallel(G, w['gamma'], w['beta'], n_processes=8),
               sim.energy_expectation_mpi(G, w['gamma'], w['beta'])):
         assert abs(E - w['energy']) <= TOL * abs(w['energy'])
+
+
+def test_composers_agree_and_terms_are_real(cuda_device):
+    """The reference's consistency checks: simplified (default), ZZ and CX
+    circuits give the same energy (qtensor/tests/test_simplify_circuit.py,
+    test_composers.py), and every edge term is real (test_simulators.py:68-85)."""
+    G, w = golden_graph('cfg2')
+    energies = []
+    for comp in ('default', 'zz', 'cx'):
+        eng = _engine(composer=comp)
+        terms = eng.edge_terms(G, w['gamma'], w['beta'])
+        assert np.max(np.abs(terms.imag)) < TOL
+        energies.append(eng.energy_expectation(G, w['gamma'], w['beta']))
+    assert max(energies) - min(energies) <= TOL * abs(w['energy'])
