@@ -551,7 +551,7 @@ static_assert(sizeof(WideNet) == 32, "WideNet layout");
 static_assert(sizeof(WideStep) == 32, "WideStep layout");
 constexpr uint32_t kWideSpinLimit = 1u << 23;   // about 1 s of polling
 constexpr int kWideThreads = 256;
-constexpr uint32_t kWideBatchLog = 2;                               // log2 of the elements per thread in flight
+constexpr uint32_t kWideBatchLog = 3;                               // log2 of the elements per thread in flight
 constexpr uint32_t kWideBatch = 1u << kWideBatchLog;
 constexpr uint32_t kWideBatchBits = (kWideBatch - 1u) << 8;          // the bits of j above the thread index
 constexpr uint32_t kWideGroup = 1;                                  // operands per batch of loads
@@ -710,7 +710,7 @@ __device__ __forceinline__ void compute_elements_wide(const DevOp& op, uint32_t 
         arena[op.dst + j + e * 256u] = op.sum ? make_float2(p0[e].x + p1[e].x, p0[e].y + p1[e].y) : p0[e];
 }
 
-__global__ void __launch_bounds__(kWideThreads, 3) qtb_wide_kernel(const WideArgs w, const RunArgs a) {
+__global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArgs w, const RunArgs a) {
     __shared__ uint32_t s_tile;
     __shared__ int s_ok, s_last;
     for (;;) {
