@@ -879,7 +879,7 @@ int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indic
                     int32_t v, int32_t p, int32_t composer, std::vector<qtb_gate>* gates,
                     int32_t* n_qubits, std::string* err) {
     if (n_nodes <= 0 || !indptr || !indices || u < 0 || v < 0 || u >= n_nodes || v >= n_nodes ||
-        u == v || p < 1 || composer < 0 || composer > 2) {
+        u == v || p < 0 || composer < 0 || composer > 2) {
         *err = "lightcone: invalid arguments";
         return QTB_ERR_ARG;
     }

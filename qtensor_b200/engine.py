@@ -274,6 +274,9 @@ class QAOAEnergyEngine:
         sets add up to the energy."""
         gamma = np.asarray(gamma, dtype=np.float64).ravel()
         p = len(gamma)
+        if G.number_of_edges() == 0 or (edges is not None and len(edges) == 0):
+            self._params(p, gamma, beta)       # same argument checks
+            return 0.0                         # an empty sum of edge terms (QAOASimulator.py:27-41)
         cg = self.compile(G, p, gamma, beta, edges)
         if path == 'batched':
             return cg.energy_of(self._params(p, gamma, beta))
@@ -285,6 +288,9 @@ class QAOAEnergyEngine:
         or of ``edges``; sliced edges are summed over their slices)."""
         gamma = np.asarray(gamma, dtype=np.float64).ravel()
         p = len(gamma)
+        if G.number_of_edges() == 0 or (edges is not None and len(edges) == 0):
+            self._params(p, gamma, beta)
+            return np.zeros(0, dtype=np.complex128)
         cg = self.compile(G, p, gamma, beta, edges)
         self._launch(cg, p, gamma, beta, path)
         return cg.edge_terms()

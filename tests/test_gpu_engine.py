@@ -195,3 +195,23 @@ def test_composers_agree_and_terms_are_real(cuda_device):
         assert np.max(np.abs(terms.imag)) < TOL
         energies.append(eng.energy_expectation(G, w['gamma'], w['beta']))
     assert max(energies) - min(energies) <= TOL * abs(w['energy'])
+
+
+def test_edge_cases_follow_the_reference(cuda_device):
+    """Edge cases with the reference's answers (oracle port): p = 0 (only the
+    Hadamard layer: every <ZZ> is 0, energy |E|/2), a graph without edges
+    (an empty sum: 0), isolated nodes and a single edge."""
+    import networkx as nx
+    import qtensor_port as port
+    eng = _engine()
+    G = graphs.regular(10, seed=1)
+    assert abs(eng.energy_expectation(G, [], []) - G.number_of_edges() / 2) < TOL
+    assert eng.energy_expectation(nx.empty_graph(5), [0.3], [0.2]) == 0.0
+    assert len(eng.edge_terms(nx.empty_graph(5), [0.3], [0.2])) == 0
+    H = nx.Graph([(0, 1)])
+    H.add_nodes_from([2, 3])
+    g, b = graphs.angles(2, seed=3)
+    ref = float(np.real(np.ravel(port.energy_expectation(H, g, b))[0]))
+    assert abs(eng.energy_expectation(H, g, b) - ref) <= TOL * max(1.0, abs(ref))
+    with pytest.raises(ValueError):
+        eng.energy_expectation(G, [0.1], [])

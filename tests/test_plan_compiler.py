@@ -171,3 +171,14 @@ def test_sliced_networks_sum_to_reference(name, max_width):
     vals = plan_interp.run_plan(plan, _params(w))
     ref = np.array([complex(*t) for t in w['terms']])
     assert np.max(np.abs(vals - ref)) < 1e-12
+
+
+def test_p0_lightcones_match_reference():
+    """p = 0: the cone is the edge alone under the Hadamard layer, every
+    <ZZ> is 0 and the energy is |E| / 2, as the reference computes it."""
+    G = graphs.regular(10, seed=1)
+    plan = NetworkPlan(0)
+    plan.add_lightcones(graph_csr(G), np.array(list(G.edges())), 0, 0, np.zeros(0))
+    vals = plan_interp.run_plan(plan, np.zeros(0))
+    ref = float(np.real(np.ravel(port.energy_expectation(G, [], []))[0]))
+    assert abs((G.number_of_edges() - vals.real.sum()) / 2 - ref) < 1e-12
