@@ -21,7 +21,14 @@
  *                          BucketBackend.process_bucket (Simulate.py:90-94), for
  *                          every edge of QAOASimulator.energy_expectation
  *                          qtensor/QAOASimulator.py:44-66 (+ _post_process_energy :27-41)
+ *   qtb_plan_run_plain  <- the same, one process_bucket launch per bucket
+ *   qtb_plan_add_circuit_batch <- QtreeSimulator.simulate_batch(qc, batch_vars)
+ *                          qtensor/Simulate.py:66-94 (free output qubits)
+ *   qtb_plan_set_max_width <- FeynmanSimulator slicing, qtensor/FeynmanSimulator.py:49-84
+ *                          with SlicesOptimizer / GreedyParvars
  *   qtb_last_error      <- Python exceptions raised by the reference backends
+ * Entry points without a counterpart in the reference are marked where they
+ * are declared (allocation-free run, failure-detection self-test).
  */
 #ifndef QTB_H
 #define QTB_H
