@@ -555,7 +555,7 @@ constexpr uint32_t kWideBatchLog = 3;                               // log2 of t
 constexpr uint32_t kWideBatch = 1u << kWideBatchLog;
 constexpr uint32_t kWideBatchBits = (kWideBatch - 1u) << 8;          // the bits of j above the thread index
 constexpr uint32_t kWideGroup = 1;                                  // operands per batch of loads
-constexpr uint32_t kWideMinTile = kWideBatch * kWideThreads;         // 1024
+constexpr uint32_t kWideMinTile = kWideBatch * kWideThreads;         // 2048
 constexpr uint32_t kWideMaxTile = 8 * kWideMinTile;
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
