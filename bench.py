@@ -41,7 +41,7 @@ import graphs  # noqa: E402
 
 METRIC = 'QAOA edge terms/s (3-regular N=1000 p=3)'
 UNIT = 'edge terms/s'
-PUBLISHED_TERMS_PER_S = 1500 / 4.89   # N=1000 p=3, 4.89 s, 56 processes
+PUBLISHED_TERMS_PER_S = 1500 / 4.89   # the reference's published N=1000 p=3 energy: 4.89 s on 56 processes
 WORKLOAD = {'workload': 'qaoa-maxcut energy, random 3-regular N=1000 (seed 0+rank), p=3, '
                         'default composer, greedy order; 1500 edge-term networks per step',
             'graph_nodes': 1000, 'p': 3, 'edges': 1500, 'composer': 'default',
