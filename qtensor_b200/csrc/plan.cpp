@@ -488,19 +488,6 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
         int rc = simplify(&gates, &checks, &angle_specific, err);
         if (rc) return rc;
     }
-    // every qubit must keep a gate (n_qubits counts qubits that appear)
-    {
-        std::vector<char> seen(n_qubits, 0);
-        for (const Gate& g : gates) {
-            seen[g.q[0]] = 1;
-            if (g.q[1] >= 0) seen[g.q[1]] = 1;
-        }
-        for (int q = 0; q < n_qubits; ++q)
-            if (!seen[q]) {
-                *err = "compile: qubit " + std::to_string(q) + " has no gate";
-                return QTB_ERR_ARG;
-            }
-    }
 
     // ---- qtree layout: bra vars 0..nq-1, gates from the bra side
     const int nq = n_qubits;

@@ -50,3 +50,17 @@ def test_feynman_simulator_matches_reference(cuda_device):
     assert np.max(np.abs(got - amplitudes(case, 2))) < TOL
     got0 = FeynmanSimulator().simulate_batch_adaptive(circuit(case))
     assert abs(got0[0] - amplitudes(case, 0)[0]) < TOL
+
+
+def test_idle_qubits_and_empty_circuits(cuda_device):
+    """Qubits without gates contribute <b|0> (the measurement tensor joins
+    their bra and ket variables), as in the reference's circ2buckets."""
+    import statevector as sv
+    from qtensor_b200 import _lib
+    from qtensor_b200.simulator import QtreeSimulator
+    sim = QtreeSimulator()
+    gates = [('H', [2], None), ('cX', [2, 0], None)]
+    got = sim.simulate_batch([Gate(*g) for g in gates], batch_vars=3)
+    assert np.max(np.abs(got - sv.circuit_state(gates, 3))) < TOL
+    empty = sim.simulate_batch(np.zeros(0, dtype=_lib.GATE_DTYPE), batch_vars=2)
+    assert np.max(np.abs(empty - np.array([1, 0, 0, 0]))) < TOL
