@@ -99,3 +99,28 @@ def test_random_circuits_match_dense_state(case):
     psi = sv.circuit_state([(name, q, 0.0 if a is None else a) for name, q, a in gates], n)
     want = psi[np.arange(2 ** k) << (n - k)]
     assert np.max(np.abs(vals - want)) < 1e-10
+
+
+@SETTINGS
+@given(qaoa_cases())
+def test_random_graphs_sliced_match_reference(case):
+    """Slicing forced one below each circuit's width: the slices of an edge
+    sum to the reference's term."""
+    G, p, gamma, beta, comp = case
+    if G.number_of_edges() == 0:
+        return
+    edges = list(G.edges())[:3]
+    params = np.concatenate([gamma, beta])
+    probe = NetworkPlan(2 * p)
+    probe.add_lightcones(graph_csr(G), np.array(edges), p, composer_id(comp), params)
+    width = max(i['treewidth'] for i in probe.infos())
+    if width < 3:
+        return
+    plan = NetworkPlan(2 * p)
+    plan.set_max_width(width, 1 << 12)
+    plan.add_lightcones(graph_csr(G), np.array(edges), p, composer_id(comp), params)
+    assert max(i['n_slices'] for i in plan.infos()) > 1
+    vals = plan_interp.run_plan(plan, params)
+    ref = np.array([complex(np.ravel(port.edge_energy(G, gamma, beta, e, composer=comp))[0])
+                    for e in edges])
+    assert np.max(np.abs(vals - ref)) < 1e-10
