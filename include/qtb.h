@@ -214,7 +214,8 @@ int qtb_plan_upload(qtb_plan* plan);
  *               circuits they belong to -- the MaxCut energy when the
  *               circuits are the edge terms of one graph; may be NULL;
  *   scratch_dev device memory of qtb_plan_scratch_bytes(); may be NULL when
- *               that size is 0.
+ *               that size is 0.  qtb_plan_scratch_bytes also works before
+ *               qtb_plan_upload (host work only), for budgeting.
  * The gate table is generated on the device from params_dev.             */
 int qtb_plan_scratch_bytes(const qtb_plan* plan, int32_t first, int32_t count,
                            size_t* bytes);

@@ -1144,10 +1144,14 @@ static int build_waves(qtb_plan* plan, std::vector<int32_t> wide, int32_t first,
     auto arena_of = [&](int32_t i) { return ((size_t)plan->druns[i].arena_elems + 63) & ~size_t(63); };
     std::stable_sort(wide.begin(), wide.end(), [&](int32_t x, int32_t y) { return arena_of(x) > arena_of(y); });
     const auto* runs = static_cast<const DevNetRun*>(plan->dev.runs);
-    int per_sm = 0, sms = 0, dev = 0;
-    QTB_CUDA(cudaGetDevice(&dev));
-    QTB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qtb_wide_kernel, kWideThreads, 0));
+    // resident CTAs size the tiles and the grid; a size-only build needs
+    // neither (and may run without a device)
+    int per_sm = 1, sms = 148, dev = 0;
+    if (device) {
+        QTB_CUDA(cudaGetDevice(&dev));
+        QTB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qtb_wide_kernel, kWideThreads, 0));
+    }
     std::vector<WideNet> nets;
     std::vector<WideStep> steps;
     std::vector<WideSeg> segs;
@@ -1171,7 +1175,7 @@ static int build_waves(qtb_plan* plan, std::vector<int32_t> wide, int32_t first,
         for (size_t k = pos; k < end; ++k) {
             const int32_t i = wide[k];
             WideNet wn{};
-            wn.run = runs + i;
+            wn.run = runs ? runs + i : nullptr;   // null in a size-only build
             wn.term = terms + (i - first);
             wn.arena_off = off;
             off += arena_of(i);
@@ -1300,7 +1304,7 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
             blob = std::max(blob, plan->druns[i].blob_bytes);
             maxe = std::max(maxe, plan->druns[i].max_elems);
             Job j;
-            j.net = runs + i;
+            j.net = runs ? runs + i : nullptr;    // null in a size-only build
             j.term = terms + (i - first);
             jobs.push_back(j);
         }
@@ -1495,7 +1499,14 @@ static int get_run(qtb_plan* plan, int32_t first, int32_t count, void* terms, Ru
 int qtb_plan_scratch_bytes(const qtb_plan* plan_c, int32_t first, int32_t count, size_t* bytes) {
     qtb_plan* plan = const_cast<qtb_plan*>(plan_c);
     if (!plan || !bytes) return fail(QTB_ERR_ARG, "plan_scratch_bytes: bad arguments");
-    if (!plan->uploaded) return fail(QTB_ERR_ARG, "plan_scratch_bytes: plan not uploaded");
+    if (!plan->uploaded) {
+        // before upload: the same host images qtb_plan_upload builds, so that a
+        // caller can budget device memory before it allocates any
+        std::lock_guard<std::mutex> lock(plan->mu);
+        flatten_plan(plan);
+        build_blobs(plan);
+        plan->common_bytes = (uint32_t)common_image(plan).bytes.size();
+    }
     if (first < 0 || count < 0 || first + count > (int32_t)plan->druns.size())
         return fail(QTB_ERR_ARG, "plan_scratch_bytes: range out of bounds");
     *bytes = 0;

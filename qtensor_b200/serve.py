@@ -46,7 +46,7 @@ class Result:
 
 
 class _Compiled:
-    __slots__ = ('future', 'plan', 'params', 'n_edges', 'n_networks', 'bytes', 'submitted')
+    __slots__ = ('future', 'plan', 'params', 'n_edges', 'n_networks', 'bytes', 'scratch', 'submitted')
 
 
 class _Inflight:
@@ -158,8 +158,10 @@ class QAOAServer:
             job.future, job.plan, job.params = fut, plan, params
             job.n_edges, job.n_networks = len(edges), len(plan)
             job.submitted = submitted
-            # plan images + run buffers (terms, energy, params, scratch)
-            job.bytes = plan.device_bytes() + 8 * job.n_networks + 64 + 8 * len(params)
+            # plan images + run buffers (terms, energy, params) + scratch (the
+            # arenas of wide networks), all known before anything is allocated
+            job.scratch = plan.scratch_bytes(0, job.n_networks)
+            job.bytes = plan.device_bytes() + job.scratch + 8 * job.n_networks + 64 + 8 * len(params)
             self._ready.put(job)
         except Exception as exc:     # noqa: BLE001 - the request fails alone
             self.stats['failed'] += 1
@@ -170,7 +172,7 @@ class QAOAServer:
         stream = self.streams[slot]
         with torch.cuda.stream(stream):
             job.plan.upload()
-            scratch_bytes = job.plan.scratch_bytes(0, job.n_networks)
+            scratch_bytes = job.scratch
             buffers = {
                 'params': torch.from_numpy(job.params).to(self.device, non_blocking=False),
                 'terms': torch.empty(job.n_networks, dtype=torch.complex64, device=self.device),

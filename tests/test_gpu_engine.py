@@ -215,3 +215,16 @@ def test_edge_cases_follow_the_reference(cuda_device):
     assert abs(eng.energy_expectation(H, g, b) - ref) <= TOL * max(1.0, abs(ref))
     with pytest.raises(ValueError):
         eng.energy_expectation(G, [0.1], [])
+
+
+def test_scratch_bytes_same_before_and_after_upload(cuda_device):
+    """The pre-upload size (used by the server's admission) is the size the
+    uploaded plan's run needs."""
+    from qtensor_b200.plan import NetworkPlan, graph_csr
+    G, w = golden_graph('cfg4')
+    params = np.concatenate([w['gamma'], w['beta']])
+    plan = NetworkPlan(8)
+    plan.add_lightcones(graph_csr(G), np.array(list(G.edges())), 4, 0, params)
+    before = plan.scratch_bytes(0, len(plan))
+    plan.upload()
+    assert plan.scratch_bytes(0, len(plan)) == before > 0

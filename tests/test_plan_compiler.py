@@ -182,3 +182,18 @@ def test_p0_lightcones_match_reference():
     vals = plan_interp.run_plan(plan, np.zeros(0))
     ref = float(np.real(np.ravel(port.energy_expectation(G, [], []))[0]))
     assert abs((G.number_of_edges() - vals.real.sum()) / 2 - ref) < 1e-12
+
+
+def test_scratch_bytes_before_upload():
+    """The scratch a run needs (arenas of networks too large for shared
+    memory) is known before upload, so a server can budget it; on the
+    N=256 p=4 workload it is the wide networks' arenas, at most 1 GiB
+    plus the largest one."""
+    G, w = golden_graph('cfg4')
+    plan = NetworkPlan(8)
+    plan.set_order_trials(4)
+    plan.add_lightcones(graph_csr(G), np.array(list(G.edges())), 4, 0, _params(w))
+    nbytes = plan.scratch_bytes(0, len(plan))
+    arenas = np.array([8 * i['arena_elems'] for i in plan.infos()])
+    assert 0 < nbytes <= arenas[arenas > 200 * 1024].sum() + 64 * 8 * len(arenas)
+    assert nbytes <= (1 << 30) + arenas.max() + 512
