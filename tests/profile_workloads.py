@@ -7,6 +7,7 @@ without the profiler and then under it.
     python tests/profile_workloads.py er400       # Erdos-Renyi N=400 p=3 (wide waves), 3 runs
     python tests/profile_workloads.py bucket24    # one 24-variable bucket through qtb_bucket_c64, 5 runs
     python tests/profile_workloads.py plain_cfg1  # 3-regular N=20 p=1 through the plain per-bucket path
+    python tests/profile_workloads.py aux         # allocation-free run (N=100 p=3) and the wait self-test
 
 QTB_SCHEDULE (see qtb.cu) fixes the executor schedule, so that the
 profiler's serialised replays cannot steer the autotuner.
@@ -110,6 +111,34 @@ def plain_cfg1():
     assert np.max(np.abs(t - ref)) < 1e-5
 
 
+def aux():
+    """qtb_plan_run_noalloc twice on the N=100 p=3 workload (its job kernel
+    and executor) and the bounded-wait self-test kernel."""
+    from qtensor_b200.plan import NetworkPlan, graph_csr
+    lib = _lib.lib()
+    _lib.check(lib.qtb_init(0))
+    G, w = golden_graph('cfg2')
+    params = np.concatenate([w['gamma'], w['beta']])
+    plan = NetworkPlan(6)
+    plan.add_lightcones(graph_csr(G), np.array(list(G.edges())), 3, 0, params)
+    plan.upload()
+    n = len(plan)
+    dev = torch.device('cuda', 0)
+    params_dev = torch.from_numpy(params).to(dev)
+    terms = torch.empty(n, dtype=torch.complex64, device=dev)
+    energy = torch.empty(1, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        _lib.check(lib.qtb_plan_run_noalloc(
+            plan._h, 0, n, ctypes.c_void_p(params_dev.data_ptr()), ctypes.c_void_p(terms.data_ptr()),
+            ctypes.c_void_p(energy.data_ptr()), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        torch.cuda.synchronize()
+        assert abs(float(energy.item()) - w['energy']) <= 1e-5 * abs(w['energy'])
+    status = ctypes.c_int32(0)
+    _lib.check(lib.qtb_selftest_wait_timeout(1 << 12, ctypes.byref(status)))
+    assert status.value == _lib.STATUS_WAIT_TIMEOUT
+
+
 if __name__ == '__main__':
-    {'cfg3': cfg3, 'er400': er400, 'bucket24': bucket24, 'plain_cfg1': plain_cfg1}[sys.argv[1]]()
+    {'cfg3': cfg3, 'er400': er400, 'bucket24': bucket24, 'plain_cfg1': plain_cfg1,
+     'aux': aux}[sys.argv[1]]()
     print('ok', sys.argv[1])
