@@ -244,27 +244,69 @@ int simplify(std::vector<Gate>* gates, std::vector<AngleCheck>* checks, bool* an
     }
     // same-site pairs (i < j) visited by distance j - i, ties in order of i:
     // the reference's visiting order, with pairs formed within groups of
-    // gates of the same kind on the same qubits instead of over all pairs
-    std::map<std::tuple<int, int, int, int>, std::vector<int>> sites;
-    for (int i = 0; i < n; ++i)
-        sites[std::make_tuple(cir[i].kind, cir[i].nq, cir[i].q[0], cir[i].nq > 1 ? cir[i].q[1] : -1)].push_back(i);
-    std::vector<std::pair<int, int>> pairs;
-    for (const auto& kv : sites) {
-        const std::vector<int>& g = kv.second;
-        for (size_t x = 0; x + 1 < g.size(); ++x)
-            for (size_t y = x + 1; y < g.size(); ++y)
-                if (same_site(cir[g[x]], cir[g[y]])) pairs.emplace_back(g[x], g[y]);
+    // gates of the same kind on the same qubits instead of over all pairs.
+    // Groups: gate indices sorted by (kind, qubits), ties by index.
+    auto site_less = [&](int x, int y) {
+        const SGate &gx = cir[x], &gy = cir[y];
+        if (gx.kind != gy.kind) return gx.kind < gy.kind;
+        if (gx.nq != gy.nq) return gx.nq < gy.nq;
+        if (gx.q[0] != gy.q[0]) return gx.q[0] < gy.q[0];
+        const int x1 = gx.nq > 1 ? gx.q[1] : -1, y1 = gy.nq > 1 ? gy.q[1] : -1;
+        return x1 != y1 ? x1 < y1 : x < y;
+    };
+    std::vector<int> by_site(n), group_end(n), rank(n);
+    std::iota(by_site.begin(), by_site.end(), 0);
+    std::sort(by_site.begin(), by_site.end(), site_less);
+    for (int s = n - 1; s >= 0; --s) {
+        const bool last = s == n - 1 || !same_site(cir[by_site[s]], cir[by_site[s + 1]]);
+        group_end[s] = last ? s + 1 : group_end[s + 1];
+        rank[by_site[s]] = s;
     }
-    if (pairs.empty()) return QTB_OK;
-    std::sort(pairs.begin(), pairs.end(), [](const std::pair<int, int>& x, const std::pair<int, int>& y) {
-        const int dx = x.second - x.first, dy = y.second - y.first;
-        return dx != dy ? dx < dy : x.first < y.first;
-    });
+    // pairs generated in order of their first gate, then a stable counting
+    // sort by distance: (distance, first) order without a comparison sort
+    std::vector<std::pair<int, int>> by_first;
+    std::vector<int> count_at(n + 1, 0);
+    for (int a = 0; a < n; ++a)
+        for (int s = rank[a] + 1; s < group_end[rank[a]]; ++s) {
+            by_first.emplace_back(a, by_site[s]);
+            ++count_at[by_site[s] - a];
+        }
+    if (by_first.empty()) return QTB_OK;
+    for (int d = 0, acc = 0; d <= n; ++d) {
+        const int c = count_at[d];
+        count_at[d] = acc;
+        acc += c;
+    }
+    std::vector<std::pair<int, int>> pairs(by_first.size());
+    for (const auto& pr : by_first) pairs[count_at[pr.second - pr.first]++] = pr;
+    // gates touching each qubit, in circuit order: a gate commutes with
+    // every gate that shares none of its qubits, so the commutation scan
+    // between a and b only visits the gates on a's qubits
+    int n_q = 0;
+    for (const SGate& g : cir)
+        for (int k = 0; k < g.nq; ++k) n_q = std::max(n_q, g.q[k] + 1);
+    std::vector<int> q_begin(n_q + 1, 0), on_qubit, slot(2 * (size_t)n, -1);
+    for (const SGate& g : cir)
+        for (int k = 0; k < g.nq; ++k) ++q_begin[g.q[k] + 1];
+    for (int q = 0; q < n_q; ++q) q_begin[q + 1] += q_begin[q];
+    on_qubit.resize(q_begin[n_q]);
+    {
+        std::vector<int> fill(q_begin.begin(), q_begin.end() - 1);
+        for (int i = 0; i < n; ++i)
+            for (int k = 0; k < cir[i].nq; ++k) {
+                slot[2 * (size_t)i + k] = fill[cir[i].q[k]];
+                on_qubit[fill[cir[i].q[k]]++] = i;
+            }
+    }
     for (const auto& pr : pairs) {
         const int a = pr.first, b = pr.second;
         if (cir[a].kind == SK_ID || cir[b].kind == SK_ID) continue;
         bool ok = true;
-        for (int m = a + 1; m < b && ok; ++m) ok = commute(cir[a], cir[m]);
+        for (int k = 0; k < cir[a].nq && ok; ++k) {
+            const int end = q_begin[cir[a].q[k] + 1];
+            for (int t = slot[2 * (size_t)a + k] + 1; t < end && on_qubit[t] < b && ok; ++t)
+                ok = commute(cir[a], cir[on_qubit[t]]);
+        }
         if (!ok) continue;
         const double total = cir[a].angle + cir[b].angle;
         const Expr sym = expr_add(cir[a].expr, cir[b].expr);
@@ -306,16 +348,21 @@ struct TRec {
     std::vector<int32_t> vars;   // native axis order
 };
 
+// A tensor of a bucket: a gate-table entry or an op's result, with its
+// variables (sorted new ids, sliced ones included) at [off, off + len) of
+// the circuit's variable pool; `next` links the tensors of one bucket.
 struct Ref {
     bool table = false;
     int32_t id = -1;                // local entry id or op id
-    std::vector<int32_t> vars;      // sorted new ids, sliced ones included
+    int32_t off = 0, len = 0;
+    int32_t next = -1;
 };
 
+// A bucket operation; its operands are [in_begin, in_begin + k) of the
+// build's operand arrays.
 struct OpRec {
     int32_t u = 0, sum = 0, w = 0;
-    std::vector<Ref> inputs;
-    std::vector<uint32_t> masks;
+    int32_t in_begin = 0, k = 0;
     int32_t level = 0;
     int32_t consumer_level = 0;
     uint32_t dst = 0;
@@ -333,27 +380,45 @@ struct OpRec {
 // kept in a bitset, so the lowest-index node of least degree is the lowest
 // set bit of the least non-empty bucket and the k-th tie its k-th set bit.
 // Returns sum over eliminations of 2^degree.
-static double greedy_order(int V, const std::vector<std::vector<int32_t>>& cliques, uint64_t seed,
-                           std::vector<int32_t>* order, std::vector<int32_t>* degrees,
-                           const std::vector<char>* removed = nullptr) {
-    const int W = (V + 63) / 64;
-    std::vector<uint64_t> adj((size_t)V * W, 0);
-    auto test = [&](int a, int b) { return (adj[(size_t)a * W + (b >> 6)] >> (b & 63)) & 1; };
-    auto set = [&](int a, int b) { adj[(size_t)a * W + (b >> 6)] |= 1ull << (b & 63); };
-    auto clr = [&](int a, int b) { adj[(size_t)a * W + (b >> 6)] &= ~(1ull << (b & 63)); };
-    std::vector<int32_t> deg(V, 0);
-    auto gone = [&](int x) { return removed && (*removed)[x]; };
+// The line graph as bit rows (one row of W words per node) with the
+// distinct-neighbour count of every node; removed nodes have no edges.
+struct LineGraph {
+    int V = 0, W = 0;
+    std::vector<uint64_t> adj;
+    std::vector<int32_t> deg;
+};
+
+static void line_graph(int V, const std::vector<std::vector<int32_t>>& cliques,
+                       const std::vector<char>& removed, LineGraph* g) {
+    g->V = V;
+    g->W = (V + 63) / 64;
+    const int W = g->W;
+    g->adj.assign((size_t)V * W, 0);
+    g->deg.assign(V, 0);
+    std::vector<uint64_t>& adj = g->adj;
     for (const auto& c : cliques)
         for (size_t i = 0; i < c.size(); ++i)
             for (size_t j = i + 1; j < c.size(); ++j) {
-                int a = c[i], b = c[j];
-                if (a != b && !gone(a) && !gone(b) && !test(a, b)) {
-                    set(a, b);
-                    set(b, a);
-                    ++deg[a];
-                    ++deg[b];
-                }
+                const int a = c[i], b = c[j];
+                if (a == b || removed[a] || removed[b] || ((adj[(size_t)a * W + (b >> 6)] >> (b & 63)) & 1))
+                    continue;
+                adj[(size_t)a * W + (b >> 6)] |= 1ull << (b & 63);
+                adj[(size_t)b * W + (a >> 6)] |= 1ull << (a & 63);
+                ++g->deg[a];
+                ++g->deg[b];
             }
+}
+
+static double greedy_order(const LineGraph& g, const std::vector<char>& removed, uint64_t seed,
+                           std::vector<int32_t>* order, std::vector<int32_t>* degrees) {
+    const int V = g.V, W = g.W;
+    static thread_local std::vector<uint64_t> adj;   // working copy, filled in per order
+    adj.assign(g.adj.begin(), g.adj.end());
+    auto test = [&](int a, int b) { return (adj[(size_t)a * W + (b >> 6)] >> (b & 63)) & 1; };
+    auto set = [&](int a, int b) { adj[(size_t)a * W + (b >> 6)] |= 1ull << (b & 63); };
+    auto clr = [&](int a, int b) { adj[(size_t)a * W + (b >> 6)] &= ~(1ull << (b & 63)); };
+    std::vector<int32_t> deg(g.deg);
+    auto gone = [&](int x) { return removed[x] != 0; };
     // degree buckets over the alive nodes
     std::vector<std::vector<uint64_t>> bucket;
     std::vector<int32_t> bucket_count;
@@ -557,11 +622,13 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
     std::vector<char> removed(V, 0);
     std::vector<int32_t> par;   // sliced line-graph nodes, in slicing order
     std::vector<int32_t> gorder, gdeg, torder, tdeg;
+    LineGraph lg;
     auto best_order = [&]() {
-        double best_cost = greedy_order(V, cliques, 0, &gorder, &gdeg, &removed);
+        line_graph(V, cliques, removed, &lg);
+        double best_cost = greedy_order(lg, removed, 0, &gorder, &gdeg);
         for (int32_t t = 1; t <= order_trials; ++t) {
             const uint64_t seed = 0x9E3779B97F4A7C15ull * (uint64_t)t + (uint64_t)V;
-            const double c = greedy_order(V, cliques, seed, &torder, &tdeg, &removed);
+            const double c = greedy_order(lg, removed, seed, &torder, &tdeg);
             if (c < best_cost) {
                 best_cost = c;
                 gorder.swap(torder);
@@ -586,17 +653,12 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
                    std::to_string(1ll << slice_budget) + " slices per circuit)";
             return QTB_ERR_UNSUPPORTED;
         }
-        // distinct-neighbour degree in the graph with the sliced nodes removed
-        std::vector<std::vector<char>> adj(V, std::vector<char>(V, 0));
-        for (const auto& c : cliques)
-            for (size_t i = 0; i < c.size(); ++i)
-                for (size_t j = i + 1; j < c.size(); ++j)
-                    if (!removed[c[i]] && !removed[c[j]] && c[i] != c[j]) adj[c[i]][c[j]] = adj[c[j]][c[i]] = 1;
+        // distinct-neighbour degree in the graph with the sliced nodes
+        // removed: the line graph of the last order search
         int best = -1, best_deg = -1;
         for (int x = 0; x < V; ++x) {
             if (removed[x]) continue;
-            int d = 0;
-            for (int y = 0; y < V; ++y) d += adj[x][y];
+            const int d = lg.deg[x];
             if (d > best_deg) {
                 best_deg = d;
                 best = x;
@@ -623,83 +685,147 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
     for (int32_t i = 0; i < 2 * nq; ++i) sliced[i] = 1;
     for (size_t i = 0; i < par.size(); ++i) sliced[perm[var_of[par[i]]]] = 1;
 
-    // one network per assignment of the sliced (parallel) variables, per
-    // output bitstring of the first batch_vars qubits (their bra variables,
-    // new ids nq + q, take the bits of `amp`, qubit 0 most significant)
-    uint64_t amp = 0;
-    auto build = [&](uint64_t slice_bits, Network* out) -> int {
-        std::vector<char> value(n_vars, 0);
-        for (int32_t q = 0; q < batch_vars; ++q) value[nq + q] = (char)((amp >> (batch_vars - 1 - q)) & 1u);
-        for (size_t i = 0; i < par.size(); ++i)
-            value[perm[var_of[par[i]]]] = (char)((slice_bits >> (par.size() - 1 - i)) & 1u);
-        // ---- reorder + slice: tensors become references to gate-table entries
-        std::vector<std::vector<Ref>> nb(n_vars);
-        std::map<EntryKey, int32_t> local;
-        out->checks = checks;
-        out->peo = peo;
+    // Per circuit, in bucket order: each tensor's variables in elimination
+    // order (new ids, ascending), the native axis each came from, and the
+    // slice-independent part of its gate-table key (kind, expression, rank,
+    // sliced axes, kept-axis permutation), interned as a base id.  Only the
+    // values of the sliced axes differ between the networks of the circuit.
+    struct TView {
+        int32_t off, rank, base;
+        uint8_t sliced_mask;
+    };
+    std::vector<TView> tview;
+    std::vector<int32_t> tvars;     // pool: tensor variables, then op results
+    std::vector<int8_t> taxes;
+    std::vector<EntryKey> bases;    // sliced_value 0
+    {
+        std::map<EntryKey, int32_t> base_index;
+        EntryKey key;
+        std::vector<int> axes;
         for (const auto& b : buckets)
             for (int32_t ti : b) {
                 const TRec& t = tensors[ti];
                 const int r = (int)t.vars.size();
-                std::vector<int> axes(r);
+                axes.resize(r);
                 std::iota(axes.begin(), axes.end(), 0);
                 std::sort(axes.begin(), axes.end(),
                           [&](int x, int y) { return perm[t.vars[x]] < perm[t.vars[y]]; });
-                EntryKey key;
+                TView v{(int32_t)tvars.size(), r, -1, 0};
                 key.kind = t.kind;
                 key.expr = t.expr;
                 key.rank_in = (int8_t)r;
                 key.sliced_mask = 0;
                 key.sliced_value = 0;
-                Ref ref;
-                ref.table = true;
+                key.perm.clear();
                 for (int a : axes) {
                     const int32_t nv = perm[t.vars[a]];
-                    ref.vars.push_back(nv);
-                    if (sliced[nv]) {
-                        key.sliced_mask |= (uint8_t)(1u << a);
-                        if (value[nv]) key.sliced_value |= (uint8_t)(1u << a);
-                    } else {
-                        key.perm.push_back((int8_t)a);
-                    }
+                    tvars.push_back(nv);
+                    taxes.push_back((int8_t)a);
+                    if (sliced[nv]) key.sliced_mask |= (uint8_t)(1u << a);
+                    else key.perm.push_back((int8_t)a);
                 }
-                auto it = local.find(key);
-                if (it == local.end()) {
-                    it = local.emplace(key, (int32_t)out->entries.size()).first;
-                    out->entries.push_back(key);
+                v.sliced_mask = key.sliced_mask;
+                auto it = base_index.find(key);
+                if (it == base_index.end()) {
+                    it = base_index.emplace(key, (int32_t)bases.size()).first;
+                    bases.push_back(key);
                 }
-                ref.id = it->second;
-                nb[ref.vars[0]].push_back(std::move(ref));
+                v.base = it->second;
+                tview.push_back(v);
             }
+    }
+    const size_t tensor_pool = tvars.size();
+
+    // one network per assignment of the sliced (parallel) variables, per
+    // output bitstring of the first batch_vars qubits (their bra variables,
+    // new ids nq + q, take the bits of `amp`, qubit 0 most significant)
+    uint64_t amp = 0;
+    // per-build working arrays, kept across the networks of the circuit
+    std::vector<char> value(n_vars);
+    std::vector<int32_t> head(n_vars), tail(n_vars), live_pos(n_vars, -1);
+    std::vector<std::vector<std::pair<uint8_t, int32_t>>> local_of(bases.size());
+    std::vector<Ref> refs;
+    std::vector<OpRec> ops;
+    std::vector<uint8_t> in_table;
+    std::vector<int32_t> in_id;
+    std::vector<uint32_t> in_mask;
+    std::vector<int32_t> U, liveU, scalars, by_level;
+    auto build = [&](uint64_t slice_bits, Network* out) -> int {
+        std::fill(value.begin(), value.end(), 0);
+        for (int32_t q = 0; q < batch_vars; ++q) value[nq + q] = (char)((amp >> (batch_vars - 1 - q)) & 1u);
+        for (size_t i = 0; i < par.size(); ++i)
+            value[perm[var_of[par[i]]]] = (char)((slice_bits >> (par.size() - 1 - i)) & 1u);
+        // ---- reorder + slice: tensors become references to gate-table
+        // entries, listed per bucket (head/tail/next) in arrival order
+        tvars.resize(tensor_pool);
+        std::fill(head.begin(), head.end(), -1);
+        std::fill(tail.begin(), tail.end(), -1);
+        for (auto& l : local_of) l.clear();
+        refs.clear();
+        auto append = [&](int32_t bucket, const Ref& r) {
+            const int32_t idx = (int32_t)refs.size();
+            refs.push_back(r);
+            refs.back().next = -1;
+            if (tail[bucket] < 0) head[bucket] = idx;
+            else refs[tail[bucket]].next = idx;
+            tail[bucket] = idx;
+        };
+        out->checks = checks;
+        out->peo = peo;
+        out->entries.clear();
+        for (const TView& v : tview) {
+            uint8_t sv = 0;
+            for (int32_t i = 0; i < v.rank; ++i) {
+                const int32_t nv = tvars[v.off + i];
+                if (sliced[nv] && value[nv]) sv |= (uint8_t)(1u << taxes[v.off + i]);
+            }
+            int32_t id = -1;
+            for (const auto& e : local_of[v.base])
+                if (e.first == sv) id = e.second;
+            if (id < 0) {
+                id = (int32_t)out->entries.size();
+                local_of[v.base].emplace_back(sv, id);
+                out->entries.push_back(bases[v.base]);
+                out->entries.back().sliced_value = sv;
+            }
+            append(tvars[v.off], Ref{true, id, v.off, v.rank, -1});
+        }
 
         // ---- symbolic bucket elimination
-        std::vector<OpRec> ops;
-        std::vector<Ref> scalars;
+        ops.clear();
+        in_table.clear();
+        in_id.clear();
+        in_mask.clear();
+        scalars.clear();
         double ref_flops = 0.0;
         int32_t max_rank = 0;
         for (int32_t n = 0; n < n_vars; ++n) {
-            std::vector<Ref>& b = nb[n];
-            if (b.empty()) continue;
-            std::vector<int32_t> U;
-            for (const Ref& r : b) U.insert(U.end(), r.vars.begin(), r.vars.end());
+            if (head[n] < 0) continue;
+            U.clear();
+            int32_t count = 0;
+            for (int32_t r = head[n]; r >= 0; r = refs[r].next, ++count)
+                U.insert(U.end(), tvars.begin() + refs[r].off, tvars.begin() + refs[r].off + refs[r].len);
             std::sort(U.begin(), U.end());
             U.erase(std::unique(U.begin(), U.end()), U.end());
             if (U.empty() || U[0] != n) {
                 *err = "compile: bucket " + std::to_string(n) + " holds a tensor without its variable";
                 return QTB_ERR_ARG;
             }
-            ref_flops += std::ldexp(1.0, (int)U.size() - 1) * (double)(1 + b.size());
-            std::vector<int32_t> outv(U.begin() + 1, U.end());
+            ref_flops += std::ldexp(1.0, (int)U.size() - 1) * (double)(1 + count);
+            const int32_t out_off = (int32_t)tvars.size(), out_len = (int32_t)U.size() - 1;
+            tvars.insert(tvars.end(), U.begin() + 1, U.end());
             Ref res;
             const bool live = !sliced[n];
-            if (b.size() == 1 && !live) {
-                res = b[0];      // product of one tensor over a size-1 variable: a copy
-                res.vars = outv;
+            if (count == 1 && !live) {
+                res = refs[head[n]];   // product of one tensor over a size-1 variable: a copy
             } else {
                 OpRec op;
-                std::vector<int32_t> liveU;
+                liveU.clear();
                 for (int32_t v : U)
-                    if (!sliced[v]) liveU.push_back(v);
+                    if (!sliced[v]) {
+                        live_pos[v] = (int32_t)liveU.size();
+                        liveU.push_back(v);
+                    }
                 op.u = (int32_t)liveU.size();
                 op.sum = live ? 1 : 0;
                 op.w = op.u - op.sum;
@@ -712,25 +838,27 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
                     *err = "compile: network has more than 65535 bucket operations";
                     return QTB_ERR_UNSUPPORTED;
                 }
-                for (const Ref& r : b) {
+                op.in_begin = (int32_t)in_id.size();
+                op.k = count;
+                for (int32_t r = head[n]; r >= 0; r = refs[r].next) {
                     uint32_t m = 0;
-                    for (int32_t v : r.vars) {
-                        if (sliced[v]) continue;
-                        const int pos = (int)(std::lower_bound(liveU.begin(), liveU.end(), v) - liveU.begin());
-                        m |= 1u << (op.u - 1 - pos);
+                    for (int32_t i = 0; i < refs[r].len; ++i) {
+                        const int32_t v = tvars[refs[r].off + i];
+                        if (!sliced[v]) m |= 1u << (op.u - 1 - live_pos[v]);
                     }
-                    op.masks.push_back(m);
-                    op.inputs.push_back(r);
+                    in_mask.push_back(m);
+                    in_table.push_back(refs[r].table ? 1 : 0);
+                    in_id.push_back(refs[r].id);
                 }
                 res.table = false;
                 res.id = (int32_t)ops.size();
-                res.vars = outv;
-                ops.push_back(std::move(op));
+                ops.push_back(op);
             }
-            if (outv.empty()) scalars.push_back(std::move(res));
-            else nb[outv[0]].push_back(std::move(res));
-            b.clear();
-            b.shrink_to_fit();
+            res.off = out_off;
+            res.len = out_len;
+            if (out_len == 0) scalars.push_back((int32_t)refs.size());
+            if (out_len == 0) refs.push_back(res);
+            else append(tvars[out_off], res);
         }
         if (scalars.empty()) {
             *err = "compile: network has no scalar result";
@@ -738,33 +866,36 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
         }
         Ref result;
         if (scalars.size() == 1) {
-            result = scalars[0];
+            result = refs[scalars[0]];
         } else {
             OpRec op;
             op.u = op.sum = op.w = 0;
-            for (const Ref& r : scalars) {
-                op.inputs.push_back(r);
-                op.masks.push_back(0);
+            op.in_begin = (int32_t)in_id.size();
+            op.k = (int32_t)scalars.size();
+            for (int32_t s : scalars) {
+                in_table.push_back(refs[s].table ? 1 : 0);
+                in_id.push_back(refs[s].id);
+                in_mask.push_back(0);
             }
             result.table = false;
             result.id = (int32_t)ops.size();
-            ops.push_back(std::move(op));
+            ops.push_back(op);
         }
 
         // ---- dependency levels, arena intervals
         int32_t max_level = 0;
         for (OpRec& op : ops) {
             int32_t lv = 0;
-            for (const Ref& r : op.inputs)
-                if (!r.table) lv = std::max(lv, ops[r.id].level);
+            for (int32_t t = op.in_begin; t < op.in_begin + op.k; ++t)
+                if (!in_table[t]) lv = std::max(lv, ops[in_id[t]].level);
             op.level = lv + 1;
             max_level = std::max(max_level, op.level);
         }
         for (OpRec& op : ops)
-            for (const Ref& r : op.inputs)
-                if (!r.table) ops[r.id].consumer_level = op.level;
+            for (int32_t t = op.in_begin; t < op.in_begin + op.k; ++t)
+                if (!in_table[t]) ops[in_id[t]].consumer_level = op.level;
         if (!result.table) ops[result.id].consumer_level = max_level + 1;
-        std::vector<int32_t> by_level(ops.size());
+        by_level.resize(ops.size());
         std::iota(by_level.begin(), by_level.end(), 0);
         // within a level the widest op first: every op of a phase then starts
         // at a multiple of its own (power-of-two) size
@@ -811,21 +942,20 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
                 DevOp d{};
                 d.u = (uint8_t)op.u;
                 d.sum = (uint8_t)op.sum;
-                d.k = (uint8_t)op.inputs.size();
+                d.k = (uint8_t)op.k;
                 d.dst = op.dst;
                 d.elem_begin = elems;
                 d.in_begin = (uint32_t)out->ins.size();
-                for (size_t t = 0; t < op.inputs.size(); ++t) {
-                    const Ref& r = op.inputs[t];
+                for (int32_t t = op.in_begin; t < op.in_begin + op.k; ++t) {
                     DevIn in{};
-                    in.mask = op.masks[t];
-                    in.src = r.table ? (kSrcTable | (uint32_t)r.id) : ops[r.id].dst;
+                    in.mask = in_mask[t];
+                    in.src = in_table[t] ? (kSrcTable | (uint32_t)in_id[t]) : ops[in_id[t]].dst;
                     in.runs = encode_runs(in.mask, (uint32_t)op.w);
                     out->ins.push_back(in);
                     alg_bytes += 8.0 * std::ldexp(1.0, __builtin_popcount(in.mask));
                 }
                 alg_bytes += 8.0 * std::ldexp(1.0, op.w);
-                alg_flops += 6.0 * (double)(op.inputs.size() - 1) * std::ldexp(1.0, op.u) +
+                alg_flops += 6.0 * (double)(op.k - 1) * std::ldexp(1.0, op.u) +
                              (op.sum ? 2.0 * std::ldexp(1.0, op.w) : 0.0);
                 elems += 1u << op.w;
                 out->ops.push_back(d);
@@ -870,9 +1000,22 @@ int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indic
         *err = "lightcone: invalid arguments";
         return QTB_ERR_ARG;
     }
-    // BFS from the edge, radius p
+    // BFS from the edge, radius p.  Distances and qubit numbers live in
+    // per-thread node arrays (-1 = outside the cone), reset after each edge,
+    // so an edge costs its cone's size, not the graph's.
+    static thread_local std::vector<int32_t> dist, qubit;
+    if ((int32_t)dist.size() < n_nodes) {
+        dist.resize(n_nodes, -1);
+        qubit.resize(n_nodes, -1);
+    }
     std::vector<int32_t> frontier = {u, v}, cone = {u, v};
-    std::map<int32_t, int32_t> dist = {{u, 0}, {v, 0}};
+    struct Reset {
+        std::vector<int32_t>& cone;
+        ~Reset() {
+            for (int32_t x : cone) dist[x] = qubit[x] = -1;
+        }
+    } reset{cone};
+    dist[u] = dist[v] = 0;
     for (int d = 1; d <= p; ++d) {
         std::vector<int32_t> next;
         for (int32_t x : frontier)
@@ -882,7 +1025,8 @@ int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indic
                     *err = "lightcone: neighbour id out of range";
                     return QTB_ERR_ARG;
                 }
-                if (dist.emplace(y, d).second) {
+                if (dist[y] < 0) {
+                    dist[y] = d;
                     next.push_back(y);
                     cone.push_back(y);
                 }
@@ -890,7 +1034,6 @@ int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indic
         frontier.swap(next);
     }
     std::sort(cone.begin(), cone.end());
-    std::map<int32_t, int32_t> qubit;
     for (size_t i = 0; i < cone.size(); ++i) qubit[cone[i]] = (int32_t)i;
     const int32_t nq = (int32_t)cone.size();
     std::vector<qtb_gate> ansatz;
@@ -905,7 +1048,7 @@ int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indic
             std::vector<int32_t> nb;
             for (int64_t e = indptr[x]; e < indptr[x + 1]; ++e) {
                 const int32_t y = indices[e];
-                if (y > x && dist.count(y) && dist[y] <= radius) nb.push_back(y);
+                if (y > x && y < n_nodes && dist[y] >= 0 && dist[y] <= radius) nb.push_back(y);
             }
             std::sort(nb.begin(), nb.end());
             nb.erase(std::unique(nb.begin(), nb.end()), nb.end());
