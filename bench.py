@@ -225,22 +225,32 @@ def serving_requests(n, seed=0):
     return out
 
 
-def run_serving(n_requests, rate, device_index):
-    """Poisson stream through the continuous-batching server, then the same
-    requests one at a time on a single-stream server."""
+def run_serving(n_requests, rate, device_index, plain_budget_s=20.0):
+    """Poisson stream through the continuous-batching server; the same
+    requests one at a time on a single-stream server; and, as the drop-in
+    comparison, requests one at a time through the plain backend (one
+    bucket-kernel launch per bucket, compile included) until about
+    ``plain_budget_s`` seconds have passed."""
+    from qtensor_b200.engine import QAOAEnergyEngine
     from qtensor_b200.serve import QAOAServer
     reqs = serving_requests(n_requests)
     rng = np.random.default_rng(1)
     gaps = rng.exponential(1.0 / rate, size=len(reqs))
 
+    def pct(values, q):
+        return float(np.percentile(values, q)) if len(values) else None
+
     def summarize(results, wall):
         ok = [r for r in results if not isinstance(r, Exception)]
         lat = np.array([r.latency for r in ok]) * 1e3
         edges = sum(r.edges for r in ok)
-        pct = (lambda q: float(np.percentile(lat, q)) if len(lat) else None)
-        return {'completed': len(ok), 'rejected': len(results) - len(ok),
-                'p50_ms': pct(50), 'p95_ms': pct(95), 'p99_ms': pct(99),
-                'edge_terms_per_s': edges / wall if wall > 0 else None, 'wall_s': wall}
+        out = {'completed': len(ok), 'rejected': len(results) - len(ok),
+               'p50_ms': pct(lat, 50), 'p95_ms': pct(lat, 95), 'p99_ms': pct(lat, 99),
+               'edge_terms_per_s': edges / wall if wall > 0 else None, 'wall_s': wall}
+        # where the median request's time went
+        for name in ('compile_s', 'wait_s', 'gpu_s'):
+            out['p50_' + name[:-2] + '_ms'] = pct(np.array([getattr(r, name) for r in ok]) * 1e3, 50)
+        return out
 
     def collect(futs):
         out = []
@@ -266,6 +276,30 @@ def run_serving(n_requests, rate, device_index):
             alone.extend(collect([srv.submit(*r)]))
         wall_alone = time.perf_counter() - t0
 
+    # the plain backend, same compile settings as the server, one request at a time
+    eng = QAOAEnergyEngine(device=device_index, max_width=22, max_slices=256, order_trials=8,
+                           cache_size=1)
+    plain_lat, plain_edges, plain_err, n_plain = [], 0, 0.0, 0
+    t0 = time.perf_counter()
+    for (G, gamma, beta), batched in zip(reqs, stream):
+        if time.perf_counter() - t0 > plain_budget_s:
+            break
+        if isinstance(batched, Exception):
+            continue
+        t = time.perf_counter()
+        E = eng.energy_expectation(G, gamma, beta, path='plain')
+        plain_lat.append((time.perf_counter() - t) * 1e3)
+        plain_edges += G.number_of_edges()
+        plain_err = max(plain_err, abs(E - batched.energy) / max(abs(batched.energy), 1e-30))
+        n_plain += 1
+    wall_plain = time.perf_counter() - t0
+    plain = {'completed': n_plain, 'p50_ms': pct(plain_lat, 50), 'p95_ms': pct(plain_lat, 95),
+             'p99_ms': pct(plain_lat, 99),
+             'edge_terms_per_s': plain_edges / wall_plain if wall_plain > 0 else None,
+             'wall_s': wall_plain, 'max_rel_diff_vs_batched': plain_err,
+             'sample': 'the first admissible requests of the stream, in order, for about {:.0f} s'.format(
+                 plain_budget_s)}
+
     def same(a, b):
         if isinstance(a, Exception) or isinstance(b, Exception):
             return isinstance(a, Exception) and isinstance(b, Exception)
@@ -275,7 +309,8 @@ def run_serving(n_requests, rate, device_index):
                         '(seed 1); slicing from width 22, at most 256 slices per edge'.format(
                             len(reqs), rate),
             'continuous_batching': summarize(stream, wall_stream),
-            'one_at_a_time': summarize(alone, wall_alone),
+            'batched_one_at_a_time': summarize(alone, wall_alone),
+            'plain_one_at_a_time': plain,
             'same_energy_alone_and_in_mix': all(same(a, b) for a, b in zip(stream, alone))}
 
 

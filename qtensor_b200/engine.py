@@ -180,7 +180,7 @@ class QAOAEnergyEngine:
         self.max_width = max_width
         self.max_slices = max_slices
         self._cache = {}
-        self._by_id = {}        # id(G) -> (weakref, nodes, edges, p, key)
+        self._by_id = {}        # id(G) -> (weakref, nodes, p, key, edge count)
         self._lock = threading.Lock()
         _lib.check(_lib.lib().qtb_init(self.device.index))
 
@@ -234,16 +234,24 @@ class QAOAEnergyEngine:
         a graph's edges in place."""
         hit = self._by_id.get(id(G))
         if hit is not None:
-            ref, n, hp, key = hit
+            ref, n, hp, key, _ = hit
             if ref() is G and hp == p and n == len(G):
                 return key
         key = graph_key(G, p, self.composer, self.ordering, self.order_trials,
                         (self.max_width, self.max_slices))
         try:
-            self._by_id[id(G)] = (weakref.ref(G), len(G), p, key)
+            self._by_id[id(G)] = (weakref.ref(G), len(G), p, key, G.number_of_edges())
         except TypeError:
             pass
         return key
+
+    def _n_edges(self, G):
+        """Edge count of ``G``, from the plan-cache entry of a graph object
+        seen before (same rule as ``_key``), else counted."""
+        hit = self._by_id.get(id(G))
+        if hit is not None and hit[0]() is G and hit[1] == len(G):
+            return hit[4]
+        return G.number_of_edges()
 
     def invalidate(self, G):
         """Forget cached plans of ``G`` (after changing it in place)."""
@@ -274,7 +282,7 @@ class QAOAEnergyEngine:
         sets add up to the energy."""
         gamma = np.asarray(gamma, dtype=np.float64).ravel()
         p = len(gamma)
-        if G.number_of_edges() == 0 or (edges is not None and len(edges) == 0):
+        if (edges is not None and len(edges) == 0) or self._n_edges(G) == 0:
             self._params(p, gamma, beta)       # same argument checks
             return 0.0                         # an empty sum of edge terms (QAOASimulator.py:27-41)
         cg = self.compile(G, p, gamma, beta, edges)
@@ -288,7 +296,7 @@ class QAOAEnergyEngine:
         or of ``edges``; sliced edges are summed over their slices)."""
         gamma = np.asarray(gamma, dtype=np.float64).ravel()
         p = len(gamma)
-        if G.number_of_edges() == 0 or (edges is not None and len(edges) == 0):
+        if (edges is not None and len(edges) == 0) or self._n_edges(G) == 0:
             self._params(p, gamma, beta)
             return np.zeros(0, dtype=np.complex128)
         cg = self.compile(G, p, gamma, beta, edges)

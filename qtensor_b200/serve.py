@@ -29,24 +29,43 @@ from .plan import NetworkPlan, graph_csr
 
 
 class Result:
-    """Energy of one request with its timeline (host clock, seconds)."""
-    __slots__ = ('energy', 'edges', 'networks', 'submitted', 'admitted', 'finished')
+    """Energy of one request with its timeline (host clock, seconds):
+    submitted -> compiled (plan built on a host worker) -> admitted (launched
+    on a stream) -> finished (energy on the host)."""
+    __slots__ = ('energy', 'edges', 'networks', 'submitted', 'admitted', 'finished', 'compiled')
 
-    def __init__(self, energy, edges, networks, submitted, admitted, finished):
+    def __init__(self, energy, edges, networks, submitted, admitted, finished, compiled=None):
         self.energy = energy
         self.edges = edges
         self.networks = networks
         self.submitted = submitted
         self.admitted = admitted
         self.finished = finished
+        self.compiled = admitted if compiled is None else compiled
 
     @property
     def latency(self):
         return self.finished - self.submitted
 
+    @property
+    def compile_s(self):
+        """Waiting for a compile worker plus compiling."""
+        return self.compiled - self.submitted
+
+    @property
+    def wait_s(self):
+        """Compiled, waiting for memory or a stream slot."""
+        return self.admitted - self.compiled
+
+    @property
+    def gpu_s(self):
+        """Admitted until the energy reached the host."""
+        return self.finished - self.admitted
+
 
 class _Compiled:
-    __slots__ = ('future', 'plan', 'params', 'n_edges', 'n_networks', 'bytes', 'scratch', 'submitted')
+    __slots__ = ('future', 'plan', 'params', 'n_edges', 'n_networks', 'bytes', 'scratch', 'submitted',
+                 'compiled')
 
 
 class _Inflight:
@@ -162,6 +181,7 @@ class QAOAServer:
             # arenas of wide networks), all known before anything is allocated
             job.scratch = plan.scratch_bytes(0, job.n_networks)
             job.bytes = plan.device_bytes() + job.scratch + 8 * job.n_networks + 64 + 8 * len(params)
+            job.compiled = time.perf_counter()
             self._ready.put(job)
         except Exception as exc:     # noqa: BLE001 - the request fails alone
             self.stats['failed'] += 1
@@ -199,7 +219,7 @@ class QAOAServer:
             if status:
                 raise _lib.QtbError(_lib.QTB_ERR_DEVICE, 'device status word {:#x}'.format(status))
             res = Result(float(fl.energy_host.numpy()[0]), job.n_edges, job.n_networks,
-                         job.submitted, fl.admitted, time.perf_counter())
+                         job.submitted, fl.admitted, time.perf_counter(), job.compiled)
             self.stats['done'] += 1
             job.future.set_result(res)
         except Exception as exc:     # noqa: BLE001

@@ -35,6 +35,7 @@ def test_server_matches_reference(cuda_device):
         res = srv.submit(G, w['gamma'], w['beta']).result(timeout=120)
     assert abs(res.energy - w['energy']) <= 1e-5 * abs(w['energy'])
     assert res.edges == G.number_of_edges() and res.latency > 0
+    assert res.submitted <= res.compiled <= res.admitted <= res.finished
 
 
 def test_alone_and_in_the_mix_agree(cuda_device):

@@ -3,7 +3,7 @@ loud failure of the product paths without a CUDA device."""
 import pytest
 import torch
 
-from qtensor_b200.serve import AdmissionControl
+from qtensor_b200.serve import AdmissionControl, Result
 
 
 def test_admission_respects_budget_and_slots():
@@ -20,6 +20,17 @@ def test_admission_respects_budget_and_slots():
     adm.release(0, 60)
     adm.release(1, 40)
     assert adm.used == 0 and adm.free_slots == [0, 1]
+
+
+def test_result_timeline_splits_latency():
+    r = Result(-1.5, 3, 4, submitted=10.0, admitted=10.25, finished=10.75, compiled=10.125)
+    assert r.compile_s == pytest.approx(0.125)
+    assert r.wait_s == pytest.approx(0.125)
+    assert r.gpu_s == pytest.approx(0.5)
+    assert r.compile_s + r.wait_s + r.gpu_s == pytest.approx(r.latency)
+    # without a compile stamp the wait is counted as compile time
+    r = Result(0.0, 0, 0, 1.0, 2.0, 2.0)
+    assert r.wait_s == 0.0 and r.compile_s == pytest.approx(1.0)
 
 
 def test_engine_needs_cuda_loudly(monkeypatch):
