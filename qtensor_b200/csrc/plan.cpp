@@ -1112,6 +1112,7 @@ void merge_network(qtb_plan* plan, Network&& net, int32_t group) {
     net.entries.shrink_to_fit();
     plan->nets.push_back(std::move(net));
     plan->uploaded = false;
+    plan->images_valid = false;
 }
 
 void flatten_plan(qtb_plan* plan) {
@@ -1183,6 +1184,13 @@ void build_blobs(qtb_plan* plan) {
             std::memcpy(dst + chunk_base, chunks.data(), chunks.size() * sizeof(uint16_t));
         plan->druns.push_back(r);
     }
+}
+
+void ensure_images(qtb_plan* plan) {
+    if (plan->images_valid) return;
+    flatten_plan(plan);
+    build_blobs(plan);
+    plan->images_valid = true;
 }
 
 }  // namespace qtb
@@ -1356,8 +1364,7 @@ int qtb_plan_check_params(const qtb_plan* plan, const double* params, int32_t* v
 int qtb_plan_export(qtb_plan* plan, int32_t which, void* buf, size_t cap, size_t* size) {
     if (!plan || !size) return fail(QTB_ERR_ARG, "plan_export: bad arguments");
     std::lock_guard<std::mutex> lock(plan->mu);
-    flatten_plan(plan);
-    build_blobs(plan);
+    ensure_images(plan);
     const void* src = nullptr;
     size_t n = 0;
     switch (which) {

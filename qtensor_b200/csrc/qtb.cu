@@ -1457,8 +1457,7 @@ int qtb_plan_upload(qtb_plan* plan) {
     int r0 = allow_all_smem();
     if (r0) return r0;
     free_device(plan);
-    flatten_plan(plan);
-    build_blobs(plan);
+    ensure_images(plan);
     int r;
     if ((r = upload_vec(plan->druns, &plan->dev.runs))) return r;
     if ((r = upload_vec(plan->dblobs, &plan->dev.blobs))) return r;
@@ -1503,8 +1502,7 @@ int qtb_plan_scratch_bytes(const qtb_plan* plan_c, int32_t first, int32_t count,
         // before upload: the same host images qtb_plan_upload builds, so that a
         // caller can budget device memory before it allocates any
         std::lock_guard<std::mutex> lock(plan->mu);
-        flatten_plan(plan);
-        build_blobs(plan);
+        ensure_images(plan);
         plan->common_bytes = (uint32_t)common_image(plan).bytes.size();
     }
     if (first < 0 || count < 0 || first + count > (int32_t)plan->druns.size())
