@@ -197,3 +197,24 @@ def test_scratch_bytes_before_upload():
     arenas = np.array([8 * i['arena_elems'] for i in plan.infos()])
     assert 0 < nbytes <= arenas[arenas > 200 * 1024].sum() + 64 * 8 * len(arenas)
     assert nbytes <= (1 << 30) + arenas.max() + 512
+
+
+def test_images_follow_networks_added_after_an_export():
+    """The flattened images are built once and reused; networks added after
+    an export (or a scratch sizing) appear in the next one, and the result
+    equals a plan that compiled every edge at once."""
+    G = graphs.regular(30, seed=3)
+    edges = np.array(list(G.edges()))
+    params = np.concatenate(graphs.angles(2, seed=5))
+    split = NetworkPlan(4)
+    split.add_lightcones(graph_csr(G), edges[:20], 2, 0, params)
+    first = split.export()
+    split.scratch_bytes(0, len(split))
+    split.add_lightcones(graph_csr(G), edges[20:], 2, 0, params)
+    whole = NetworkPlan(4)
+    whole.add_lightcones(graph_csr(G), edges, 2, 0, params)
+    a, b = split.export(), whole.export()
+    assert len(a['nets']) == len(edges) > len(first['nets'])
+    for key in ('nets', 'ops', 'ins', 'phases', 'runs', 'blobs'):
+        assert np.array_equal(a[key], b[key]), key
+    assert np.max(np.abs(plan_interp.run_plan(split, params) - plan_interp.run_plan(whole, params))) == 0
