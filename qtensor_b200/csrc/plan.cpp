@@ -414,9 +414,6 @@ static double greedy_order(const LineGraph& g, const std::vector<char>& removed,
     const int V = g.V, W = g.W;
     static thread_local std::vector<uint64_t> adj;   // working copy, filled in per order
     adj.assign(g.adj.begin(), g.adj.end());
-    auto test = [&](int a, int b) { return (adj[(size_t)a * W + (b >> 6)] >> (b & 63)) & 1; };
-    auto set = [&](int a, int b) { adj[(size_t)a * W + (b >> 6)] |= 1ull << (b & 63); };
-    auto clr = [&](int a, int b) { adj[(size_t)a * W + (b >> 6)] &= ~(1ull << (b & 63)); };
     std::vector<int32_t> deg(g.deg);
     auto gone = [&](int x) { return removed[x] != 0; };
     // degree buckets over the alive nodes
@@ -486,22 +483,23 @@ static double greedy_order(const LineGraph& g, const std::vector<char>& removed,
         order->push_back(x);
         degrees->push_back((int32_t)nbrs.size());
         cost += std::ldexp(1.0, (int)nbrs.size());
+        // eliminate x: its neighbours become a clique.  Row by row, a
+        // neighbour's row takes x's row, loses a and x, and its degree is
+        // the row's population (the same graph as joining every pair).
+        const uint64_t* rx = &adj[(size_t)x * W];
         for (int a : nbrs) {
-            clr(a, x);
             del(a, deg[a]);
-            --deg[a];
-        }
-        for (size_t i = 0; i < nbrs.size(); ++i)
-            for (size_t j = i + 1; j < nbrs.size(); ++j) {
-                int a = nbrs[i], b = nbrs[j];
-                if (!test(a, b)) {
-                    set(a, b);
-                    set(b, a);
-                    ++deg[a];
-                    ++deg[b];
-                }
+            uint64_t* ra = &adj[(size_t)a * W];
+            int d = 0;
+            for (int w = 0; w < W; ++w) {
+                ra[w] |= rx[w];
+                if (w == (a >> 6)) ra[w] &= ~(1ull << (a & 63));
+                if (w == (x >> 6)) ra[w] &= ~(1ull << (x & 63));
+                d += __builtin_popcountll(ra[w]);
             }
-        for (int a : nbrs) add(a, deg[a]);
+            deg[a] = d;
+            add(a, d);
+        }
     }
     return cost;
 }
