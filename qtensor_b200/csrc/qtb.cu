@@ -89,26 +89,74 @@ struct BucketArgs {
     int32_t sum;
 };
 
-__global__ void __launch_bounds__(256) qtb_bucket_kernel(const BucketArgs a) {
-    const uint64_t n_out = 1ull << a.w;
-    const uint32_t low = a.w >= 32 ? 0xffffffffu : (1u << a.w) - 1u;
-    for (uint64_t jj = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; jj < n_out;
-         jj += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t j = (uint32_t)jj;
-        float2 p0 = make_float2(1.f, 0.f), p1 = make_float2(1.f, 0.f);
+// Each thread contracts up to kBucketBatch output elements, one grid width
+// apart (so every load stays coalesced across the warp; a bucket smaller
+// than the grid gives each thread one element), operand by operand: all their
+// gathers are in flight together, which a bandwidth-bound bucket needs to
+// keep enough bytes moving per SM.  The operand descriptors are copied to
+// shared memory once per block, so the operand loop reads them with a
+// runtime index without holding all sixteen slots in registers.  Each
+// element's product folds its operands left to right, as one element at a
+// time would.
+constexpr int kBucketBatch = 4;
+constexpr int kBucketThreads = 256;
+
+__global__ void __launch_bounds__(kBucketThreads) qtb_bucket_kernel(const BucketArgs a) {
+    __shared__ const float2* s_in[QTB_MAX_BUCKET_INPUTS];
+    __shared__ uint64_t s_runs[QTB_MAX_BUCKET_INPUTS];
+    __shared__ uint32_t s_mask[QTB_MAX_BUCKET_INPUTS], s_stride[QTB_MAX_BUCKET_INPUTS];
+    if (threadIdx.x < (uint32_t)a.k) {
+        s_in[threadIdx.x] = a.in[threadIdx.x];
+        s_runs[threadIdx.x] = a.runs[threadIdx.x];
+        s_mask[threadIdx.x] = a.mask[threadIdx.x];
+        s_stride[threadIdx.x] = a.sum ? a.stride[threadIdx.x] : 0u;
+    }
+    __syncthreads();
+    // 32-bit indices: at most 2^31 outputs (QTB_MAX_BUCKET_VARS), and
+    // base + kBucketBatch grid widths stays below 2^32
+    const uint32_t n_out = 1u << a.w;
+    const uint32_t low = n_out - 1u;
+    const uint32_t grid = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + threadIdx.x; base < n_out; base += grid * kBucketBatch) {
+        float2 p0[kBucketBatch], p1[kBucketBatch];
+#pragma unroll 1
         for (int t = 0; t < a.k; ++t) {
             DevIn d;
-            d.mask = a.mask[t];
+            d.mask = s_mask[t];
             d.src = 0;
-            d.runs = a.runs[t];
-            const uint32_t off = gather_bits(j, d, low);
-            const float2 x0 = a.in[t][off];
-            const float2 x1 = (a.sum && a.stride[t]) ? a.in[t][off + a.stride[t]] : x0;
-            p0 = t == 0 ? x0 : cmul(p0, x0);
-            p1 = t == 0 ? x1 : cmul(p1, x1);
+            d.runs = s_runs[t];
+            const float2* __restrict__ in = s_in[t];
+            const uint32_t stride = s_stride[t];
+            float2 x0[kBucketBatch], x1[kBucketBatch];
+#pragma unroll
+            for (int i = 0; i < kBucketBatch; ++i) {
+                const uint32_t jj = base + i * grid;
+                x0[i] = x1[i] = make_float2(0.f, 0.f);
+                if (jj < n_out) {
+                    const uint32_t off = gather_bits(jj, d, low);
+                    x0[i] = in[off];
+                    x1[i] = stride ? in[off + stride] : x0[i];
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < kBucketBatch; ++i) {
+                p0[i] = t == 0 ? x0[i] : cmul(p0[i], x0[i]);
+                p1[i] = t == 0 ? x1[i] : cmul(p1[i], x1[i]);
+            }
         }
-        a.out[j] = a.sum ? make_float2(p0.x + p1.x, p0.y + p1.y) : p0;
+#pragma unroll
+        for (int i = 0; i < kBucketBatch; ++i) {
+            const uint32_t jj = base + i * grid;
+            if (jj < n_out) a.out[jj] = a.sum ? make_float2(p0[i].x + p1[i].x, p0[i].y + p1[i].y) : p0[i];
+        }
     }
+}
+
+// Grid of a bucket launch over 2^w outputs: one thread per element up to
+// eight blocks for each of the 148 SMs; larger buckets give every thread up
+// to kBucketBatch elements per pass of the grid-stride loop.
+static unsigned bucket_blocks(int32_t w) {
+    return (unsigned)std::min<uint64_t>(((1ull << w) + kBucketThreads - 1) / kBucketThreads, 148ull * 8);
 }
 
 // Gathers of operand t of a bucket over n_vars variables (variable 0 at
@@ -1441,10 +1489,7 @@ int qtb_bucket_c64(const qtb_bucket_desc* d, const void* const* inputs, void* ou
     a.k = d->n_inputs;
     a.sum = d->sum_first;
     a.w = d->n_vars - d->sum_first;
-    const uint64_t n_out = 1ull << a.w;
-    const int threads = 256;
-    const uint64_t blocks = std::min<uint64_t>((n_out + threads - 1) / threads, 148ull * 16);
-    qtb_bucket_kernel<<<(unsigned)blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(a);
+    qtb_bucket_kernel<<<bucket_blocks(a.w), kBucketThreads, 0, static_cast<cudaStream_t>(stream)>>>(a);
     QTB_CUDA(cudaGetLastError());
     return QTB_OK;
 }
@@ -1896,9 +1941,7 @@ int qtb_plan_run_plain(qtb_plan* plan, int32_t first, int32_t count, const doubl
             a.k = op.k;
             a.sum = op.sum;
             a.w = op.u - op.sum;
-            const uint64_t n_out = 1ull << a.w;
-            const uint64_t blocks = std::min<uint64_t>((n_out + 255) / 256, 148ull * 16);
-            qtb_bucket_kernel<<<(unsigned)blocks, 256, 0, st>>>(a);
+            qtb_bucket_kernel<<<bucket_blocks(a.w), kBucketThreads, 0, st>>>(a);
             QTB_CUDA(cudaGetLastError());
         }
         const float2* res = (net.result_src & kSrcTable) ? table + (net.result_src & ~kSrcTable)
