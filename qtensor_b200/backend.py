@@ -150,3 +150,107 @@ class B200Backend:
         if isinstance(data, torch.Tensor):
             return data.cpu().numpy()
         return np.asarray(data)
+
+
+class PerfBackend:
+    """Per-bucket timing around another backend, the counterpart of
+    QTensor's ``PerfBackend`` (qtensor/ProcessingFrameworks.py:152-234).
+
+    ``Backend`` is the wrapped class (``B200Backend`` by default;
+    ``from_backend`` builds a subclass for another one).  Every
+    ``process_bucket`` is bracketed by CUDA events on the current stream, so
+    the recorded time is the bucket's device time, not its launch time;
+    events are resolved when a report is asked for.  Records are keyed by
+    ``str`` of the bucket's index tuples, as the reference keys them.
+    ``gen_report`` returns the reference's text report (the slowest
+    buckets, then totals) and prints a markdown table of per-bucket figures
+    with their max / mean / sum."""
+    Backend = B200Backend
+
+    def __init__(self, *args, print=False, num_lines=20, **kwargs):
+        self.backend = self.Backend(*args, **kwargs)
+        self._print = print
+        self.max_lines = num_lines
+        self._pending = {}           # key -> (indices, start event, end event)
+        self._profile_results = {}   # key -> (indices, seconds)
+
+    @classmethod
+    def from_backend(cls, backend, *args, **kwargs):
+        """A ``PerfBackend`` around ``backend`` (a backend class)."""
+        class CustomGeneratedBackend(cls):
+            Backend = backend
+        return CustomGeneratedBackend(*args, **kwargs)
+
+    def process_bucket(self, bucket, no_sum=False):
+        if not torch.cuda.is_available():
+            raise RuntimeError('PerfBackend times buckets with CUDA events and needs a CUDA device')
+        indices = [tensor.indices for tensor in bucket]
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record()
+        result = self.backend.process_bucket(bucket, no_sum=no_sum)
+        end.record()
+        self._pending[str(indices)] = (indices, start, end)
+        return result
+
+    def get_sliced_buckets(self, buckets, data_dict, slice_dict):
+        return self.backend.get_sliced_buckets(buckets, data_dict, slice_dict)
+
+    def get_result_data(self, result):
+        return self.backend.get_result_data(result)
+
+    @property
+    def profile_results(self):
+        """``{key: (indices, seconds)}`` of every bucket timed so far."""
+        for key, (indices, start, end) in self._pending.items():
+            end.synchronize()
+            seconds = start.elapsed_time(end) / 1e3
+            if self._print:
+                print('PROF:: perf data process bucket time: {}'.format(seconds))
+            self._profile_results[key] = (indices, seconds)
+        self._pending.clear()
+        return self._profile_results
+
+    @staticmethod
+    def _perfect_bucket_flop(bucket_indices):
+        """Ideal operation count of a bucket, the reference's estimate
+        (ProcessingFrameworks.py:186-196): result size (the union less the
+        contracted index) times (one summation + one multiplication per
+        tensor)."""
+        union = set().union(*[set(ixs) for ixs in bucket_indices])
+        size_of_result = 2 ** (len(union) - 1) if union else 1
+        return size_of_result * (1 + len(bucket_indices))
+
+    def gen_report(self):
+        data = sorted(self.profile_results.values(), key=lambda pair: pair[1], reverse=True)
+        max_lines = self.max_lines
+        lines = [str([i, ixs, t]) for i, (ixs, t) in enumerate(data[:max_lines])]
+        rep = '\n'.join(lines)
+        if len(data) > max_lines:
+            rep += '\n ... and {} lines more...'.format(len(data) - max_lines)
+        fields = ('bucket_len', 'time', 'flop', 'FLOPS', 'max_size', 'min_size', 'result_size')
+        records = []
+        for ixs, t in data[:max_lines]:
+            flop = self._perfect_bucket_flop(ixs)
+            records.append((len(ixs), t, flop, flop / t if t > 0 else float('inf'),
+                            max(len(i) for i in ixs), min(len(i) for i in ixs),
+                            len(set().union(*[set(i) for i in ixs])) - 1))
+        if records:
+            table = ['| measure | ' + ' | '.join(fields) + ' |', '|---' * (len(fields) + 1) + '|']
+            cols = list(zip(*records))
+            for name, fn in (('max', max), ('mean', lambda c: sum(c) / len(c)), ('sum', sum)):
+                table.append('| {} | '.format(name) + ' | '.join('{:.4g}'.format(fn(c)) for c in cols) + ' |')
+            print('\n'.join(table))
+        total_time = sum(t for _, t in data)
+        rep += '\n======\n'
+        rep += 'Total time: ' + str(total_time)
+        rep += '\nTotal bucket contractions: ' + str(len(data))
+        rep += '\nMean time for contraction: ' + str(total_time / len(data) if data else 0.0)
+        rep += '\n'
+        return rep
+
+
+class PerfB200Backend(PerfBackend):
+    """``PerfBackend`` around ``B200Backend`` (the reference's
+    ``PerfNumpyBackend`` pattern)."""
+    Backend = B200Backend

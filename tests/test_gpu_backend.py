@@ -114,3 +114,26 @@ def test_backend_pickles_without_device_state():
     from qtensor_b200.backend import B200Backend
     b = pickle.loads(pickle.dumps(B200Backend(device=0)))
     assert b._device is None and b._device_index == 0
+
+
+def test_perf_backend_times_every_bucket(cuda_device, capsys):
+    """PerfB200Backend (the reference's PerfBackend around the drop-in
+    backend): same amplitudes, one device time per distinct bucket, the
+    reference's ideal flop count, and the text report with its totals."""
+    from qtensor_b200.backend import B200Backend, PerfB200Backend, PerfBackend
+    G, w = golden_graph('cfg1_default')
+    edge = list(G.edges())[0]
+    circ = port.lightcone_circuit(G, edge, w['gamma'], w['beta'], 'default')
+    perf = PerfB200Backend()
+    amp = port.simulate_amplitude(circ, backend=perf)
+    assert abs(amp[0] - complex(*w['terms'][0])) < TOL
+    results = perf.profile_results
+    assert results and all(t > 0 for _, t in results.values())
+    rep = perf.gen_report()
+    assert 'Total bucket contractions: {}'.format(len(results)) in rep
+    assert '| max |' in capsys.readouterr().out
+    wrapped = PerfBackend.from_backend(B200Backend)
+    assert isinstance(wrapped.backend, B200Backend)
+    # union of 3 indices -> result 2^2, two tensors -> 4 * (1 + 2)
+    a, b, c = Var(1), Var(2), Var(3)
+    assert PerfBackend._perfect_bucket_flop([(a, b), (a, c)]) == 12

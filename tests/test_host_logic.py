@@ -77,3 +77,10 @@ def test_simulators_need_cuda_loudly(monkeypatch):
         simulator.QtreeSimulator()
     with pytest.raises(RuntimeError, match='no CPU fallback'):
         qaoa.QAOAQtreeSimulator()
+
+
+def test_perf_backend_needs_cuda_loudly(monkeypatch):
+    from qtensor_b200.backend import PerfB200Backend
+    monkeypatch.setattr(torch.cuda, 'is_available', lambda: False)
+    with pytest.raises(RuntimeError, match='CUDA'):
+        PerfB200Backend().process_bucket([object()])
