@@ -181,6 +181,18 @@ int qtb_plan_set_max_width(qtb_plan* plan, int32_t max_width, int32_t max_slices
  * RGreedyOptimizer, qtensor/optimisation/RGreedy.py:15-77).               */
 int qtb_plan_set_order_trials(qtb_plan* plan, int32_t trials);
 
+/* Structural sharing for qtb_plan_add_lightcones calls made afterwards
+ * (enable 1, the default): edges whose lightcones are isomorphic, by a map
+ * that keeps every node's distance from the edge and sends the edge's ends
+ * to the edge's ends, contract to the same <Z_u Z_v>, so the first such
+ * edge (in edge order) is compiled and the others copy its networks.  Each
+ * edge still has networks of its own in the plan and on the device; only
+ * the host compile is shared.  The canonical key is compared in full, so a
+ * share is never made on a hash alone.  No counterpart in the reference,
+ * which compiles every edge (qtensor/QAOASimulator.py:44-66).  0 compiles
+ * every edge from its own lightcone.                                     */
+int qtb_plan_set_share_lightcones(qtb_plan* plan, int32_t enable);
+
 int qtb_plan_n_networks(const qtb_plan* plan, int32_t* n);
 int qtb_plan_network_info(const qtb_plan* plan, int32_t net, qtb_network_info* info);
 /* Elimination order of a network as variable ids of the qtree layout

@@ -27,14 +27,13 @@ EXPORTS = (
     'qtb_plan_create', 'qtb_plan_destroy', 'qtb_plan_add_circuit',
     'qtb_plan_add_lightcone', 'qtb_plan_add_lightcones', 'qtb_plan_add_circuit_batch',
     'qtb_plan_set_max_width',
-    'qtb_plan_set_order_trials',
+    'qtb_plan_set_order_trials', 'qtb_plan_set_share_lightcones',
     'qtb_plan_n_networks',
     'qtb_plan_network_info', 'qtb_plan_network_peo', 'qtb_plan_check_params',
     'qtb_plan_export', 'qtb_plan_table_elems', 'qtb_plan_upload',
     'qtb_plan_scratch_bytes', 'qtb_plan_run', 'qtb_plan_plain_scratch_bytes',
     'qtb_plan_run_plain', 'qtb_plan_set_autotune',
     'qtb_plan_last_launch_config', 'qtb_plan_device_bytes', 'qtb_plan_device_status',
-    'qtb_selftest_wait_timeout',
     'qtb_selftest_wait_timeout',
     'qtb_plan_set_timing', 'qtb_plan_collect_timing', 'qtb_plan_run_noalloc',
 )
@@ -119,6 +118,7 @@ def _declare(lib):
                                               c.c_int32, P, c.c_int32, c.POINTER(c.c_int32)]),
         'qtb_plan_set_max_width': (c.c_int, [P, c.c_int32, c.c_int32]),
         'qtb_plan_set_order_trials': (c.c_int, [P, c.c_int32]),
+        'qtb_plan_set_share_lightcones': (c.c_int, [P, c.c_int32]),
         'qtb_plan_n_networks': (c.c_int, [P, c.POINTER(c.c_int32)]),
         'qtb_plan_network_info': (c.c_int, [P, c.c_int32, c.POINTER(NetworkInfo)]),
         'qtb_plan_network_peo': (c.c_int, [P, c.c_int32, P, c.c_int32, c.POINTER(c.c_int32)]),

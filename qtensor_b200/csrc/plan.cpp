@@ -18,11 +18,13 @@
 //                    the bucket arithmetic of ProcessingFrameworks.py:45-147
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <numeric>
 #include <thread>
 #include <tuple>
+#include <unordered_map>
 
 #include "plan.h"
 
@@ -1077,6 +1079,125 @@ int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indic
     return QTB_OK;
 }
 
+// ------------------------------------------------------ lightcone classes
+// Structural key of an edge's lightcone: the cone (nodes within distance p
+// of u or v) with every node's distance, every edge among cone nodes, and
+// u and v in their roles, written in a canonical numbering.  Two edges with
+// equal keys have isomorphic lightcones through a map that keeps distances
+// and sends u to u and v to v, so their circuits are relabelings of each
+// other and contract to the same <Z_u Z_v>: one compiled network serves
+// both.  Equality of the full keys is what proves it; the numbering only
+// decides how often isomorphic cones get equal keys.  It comes from colour
+// refinement (distance, role, then the multiset of neighbour colours until
+// the classes stop splitting) and a level-by-level order: distance, colour,
+// the lowest rank among the node's neighbours one level closer, then the
+// node id.  On trees this numbers isomorphic cones alike; on cones with
+// cycles, ties broken by node id may give distinct keys (a missed share,
+// never a wrong one).
+void cone_key(int32_t n_nodes, const int64_t* indptr, const int32_t* indices, int32_t u, int32_t v,
+              int32_t p, std::vector<int32_t>* key) {
+    static thread_local std::vector<int32_t> dist, loc;
+    if ((int32_t)dist.size() < n_nodes) {
+        dist.resize(n_nodes, -1);
+        loc.resize(n_nodes, -1);
+    }
+    std::vector<int32_t> cone = {u, v};
+    struct Reset {
+        std::vector<int32_t>& cone;
+        ~Reset() {
+            for (int32_t x : cone) dist[x] = loc[x] = -1;
+        }
+    } reset{cone};
+    dist[u] = dist[v] = 0;
+    for (size_t head = 0; head < cone.size(); ++head) {
+        const int32_t x = cone[head];
+        if (dist[x] == p) continue;
+        for (int64_t e = indptr[x]; e < indptr[x + 1]; ++e) {
+            const int32_t y = indices[e];
+            if (y >= 0 && y < n_nodes && dist[y] < 0) {
+                dist[y] = dist[x] + 1;
+                cone.push_back(y);
+            }
+        }
+    }
+    const int n = (int)cone.size();
+    for (int i = 0; i < n; ++i) loc[cone[i]] = i;
+    // induced subgraph, local indices
+    std::vector<std::vector<int32_t>> nbr(n);
+    for (int i = 0; i < n; ++i) {
+        const int32_t x = cone[i];
+        for (int64_t e = indptr[x]; e < indptr[x + 1]; ++e) {
+            const int32_t y = indices[e];
+            if (y >= 0 && y < n_nodes && y != x && loc[y] >= 0) nbr[i].push_back(loc[y]);
+        }
+        std::sort(nbr[i].begin(), nbr[i].end());
+        nbr[i].erase(std::unique(nbr[i].begin(), nbr[i].end()), nbr[i].end());
+    }
+    // colour refinement to a stable partition
+    std::vector<int32_t> color(n);
+    std::vector<std::vector<int32_t>> sig(n);
+    std::vector<int32_t> idx(n);
+    auto relabel = [&]() {
+        std::iota(idx.begin(), idx.end(), 0);
+        std::sort(idx.begin(), idx.end(), [&](int a, int b) { return sig[a] < sig[b]; });
+        int classes = 0;
+        for (int k = 0; k < n; ++k) {
+            if (k > 0 && sig[idx[k]] != sig[idx[k - 1]]) ++classes;
+            color[idx[k]] = classes;
+        }
+        return classes + 1;
+    };
+    for (int i = 0; i < n; ++i) sig[i] = {dist[cone[i]], i == 0 ? 1 : (i == 1 ? 2 : 0)};
+    int classes = relabel();
+    for (int round = 0; round < n; ++round) {
+        for (int i = 0; i < n; ++i) {
+            sig[i].assign(1, color[i]);
+            for (int32_t j : nbr[i]) sig[i].push_back(color[j]);
+            std::sort(sig[i].begin() + 1, sig[i].end());
+        }
+        const int next = relabel();
+        if (next == classes) break;
+        classes = next;
+    }
+    // level-by-level canonical ranks
+    std::vector<int32_t> rank(n, -1), order;
+    rank[0] = 0;
+    rank[1] = 1;
+    order = {0, 1};
+    for (int d = 1; d <= p; ++d) {
+        std::vector<int32_t> level;
+        std::vector<int32_t> up(n, INT32_MAX);
+        for (int i = 0; i < n; ++i)
+            if (dist[cone[i]] == d) {
+                level.push_back(i);
+                for (int32_t j : nbr[i])
+                    if (dist[cone[j]] == d - 1) up[i] = std::min(up[i], rank[j]);
+            }
+        std::sort(level.begin(), level.end(), [&](int a, int b) {
+            if (color[a] != color[b]) return color[a] < color[b];
+            if (up[a] != up[b]) return up[a] < up[b];
+            return cone[a] < cone[b];
+        });
+        for (int32_t i : level) {
+            rank[i] = (int32_t)order.size();
+            order.push_back(i);
+        }
+    }
+    key->clear();
+    key->push_back(n);
+    key->push_back(p);
+    for (int32_t i : order) key->push_back(dist[cone[i]]);
+    std::vector<std::pair<int32_t, int32_t>> edges;
+    for (int i = 0; i < n; ++i)
+        for (int32_t j : nbr[i])
+            if (rank[i] < rank[j]) edges.emplace_back(rank[i], rank[j]);
+    std::sort(edges.begin(), edges.end());
+    for (const auto& e : edges) {
+        key->push_back(e.first);
+        key->push_back(e.second);
+    }
+}
+
 // ------------------------------------------------------ plan assembly
 void merge_network(qtb_plan* plan, Network&& net, int32_t group) {
     net.info.group = group;
@@ -1196,6 +1317,23 @@ void ensure_images(qtb_plan* plan) {
 // =================================================================== C ABI
 using namespace qtb;
 
+// Runs fn(i) for i in [0, n) on up to n_threads threads (0 = all cores).
+namespace qtb {
+template <typename Fn>
+static void parallel_for(int32_t n, int32_t n_threads, Fn fn) {
+    std::atomic<int32_t> next{0};
+    auto worker = [&]() {
+        for (int32_t i; (i = next.fetch_add(1)) < n;) fn(i);
+    };
+    int nt = n_threads > 0 ? n_threads : (int)std::thread::hardware_concurrency();
+    nt = std::max(1, std::min(nt, std::max(1, n)));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& t : pool) t.join();
+}
+}  // namespace qtb
+
 extern "C" {
 
 int qtb_last_error(char* buf, size_t len) {
@@ -1268,36 +1406,63 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
                             int32_t* first_net_index) {
     if (!plan || !edges || n_edges < 0) return fail(QTB_ERR_ARG, "plan_add_lightcones: bad arguments");
     if (plan->n_params != 2 * p) return fail(QTB_ERR_ARG, "plan_add_lightcones: plan needs 2*p params");
+    if (n_edges > 0 && (n_nodes <= 0 || !indptr || !indices))
+        return fail(QTB_ERR_ARG, "plan_add_lightcones: bad graph");
     std::vector<std::vector<Network>> nets(n_edges);
     std::vector<int> codes(n_edges, 0);
     std::vector<std::string> errs(n_edges);
-    std::atomic<int32_t> next{0};
-    std::atomic<bool> failed{false};   // one failing edge fails the call: stop early
-    auto worker = [&]() {
-        std::vector<qtb_gate> gates;
-        for (;;) {
-            const int32_t i = next.fetch_add(1);
-            if (i >= n_edges || failed.load(std::memory_order_relaxed)) break;
-            int32_t nq = 0;
-            int rc = build_lightcone(n_nodes, indptr, indices, edges[2 * i], edges[2 * i + 1], p,
-                                     composer, &gates, &nq, &errs[i]);
-            if (!rc)
-                rc = compile_circuit(nq, gates.data(), (int32_t)gates.size(), composer == 0 ? 2 : 0,
-                                     params, plan->n_params, plan->order_trials, plan->max_width,
-                                     plan->max_slices, 0, &nets[i], &errs[i], &failed);
-            codes[i] = rc;
-            if (rc && rc != kCompileAborted) failed.store(true, std::memory_order_relaxed);
+    // edges whose lightcones are isomorphic share one compile: the first
+    // edge of each class (in edge order, so plans do not depend on thread
+    // timing) is compiled, the others copy its networks
+    std::vector<int32_t> rep(n_edges);
+    std::iota(rep.begin(), rep.end(), 0);
+    if (plan->share_lightcones && n_edges > 1) {
+        std::vector<std::vector<int32_t>> keys(n_edges);
+        parallel_for(n_edges, n_threads, [&](int32_t i) {
+            const int32_t a = edges[2 * i], b = edges[2 * i + 1];
+            if (a >= 0 && b >= 0 && a < n_nodes && b < n_nodes && a != b && p >= 0)
+                cone_key(n_nodes, indptr, indices, a, b, p, &keys[i]);
+        });
+        std::unordered_map<uint64_t, std::vector<int32_t>> classes;
+        for (int32_t i = 0; i < n_edges; ++i) {
+            if (keys[i].empty()) continue;   // invalid edge: compiled alone, reports its error
+            uint64_t h = 1469598103934665603ull;
+            for (int32_t x : keys[i]) h = (h ^ (uint32_t)x) * 1099511628211ull;
+            auto& members = classes[h];
+            for (int32_t r : members)
+                if (keys[r] == keys[i]) {
+                    rep[i] = r;
+                    break;
+                }
+            if (rep[i] == i) members.push_back(i);
         }
-    };
-    int nt = n_threads > 0 ? n_threads : (int)std::thread::hardware_concurrency();
-    nt = std::max(1, std::min(nt, std::max(1, n_edges)));
-    std::vector<std::thread> pool;
-    for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
-    worker();
-    for (auto& t : pool) t.join();
+    }
+    std::vector<int32_t> todo;
+    for (int32_t i = 0; i < n_edges; ++i)
+        if (rep[i] == i) todo.push_back(i);
+    std::atomic<bool> failed{false};   // one failing edge fails the call: stop early
+    parallel_for((int32_t)todo.size(), n_threads, [&](int32_t t) {
+        const int32_t i = todo[t];
+        if (failed.load(std::memory_order_relaxed)) {
+            codes[i] = kCompileAborted;
+            return;
+        }
+        static thread_local std::vector<qtb_gate> gates;
+        int32_t nq = 0;
+        int rc = build_lightcone(n_nodes, indptr, indices, edges[2 * i], edges[2 * i + 1], p,
+                                 composer, &gates, &nq, &errs[i]);
+        if (!rc)
+            rc = compile_circuit(nq, gates.data(), (int32_t)gates.size(), composer == 0 ? 2 : 0,
+                                 params, plan->n_params, plan->order_trials, plan->max_width,
+                                 plan->max_slices, 0, &nets[i], &errs[i], &failed);
+        codes[i] = rc;
+        if (rc && rc != kCompileAborted) failed.store(true, std::memory_order_relaxed);
+    });
     for (int32_t i = 0; i < n_edges; ++i)   // the first genuine failure (not an abort)
-        if (codes[i] && codes[i] != kCompileAborted)
-            return fail(codes[i], "edge " + std::to_string(i) + ": " + errs[i]);
+        if (codes[rep[i]] && codes[rep[i]] != kCompileAborted)
+            return fail(codes[rep[i]], "edge " + std::to_string(i) + ": " + errs[rep[i]]);
+    for (int32_t i = 0; i < n_edges; ++i)
+        if (rep[i] != i) nets[i] = nets[rep[i]];
     std::lock_guard<std::mutex> lock(plan->mu);
     if (first_net_index) *first_net_index = (int32_t)plan->nets.size();
     for (auto& circuit : nets) {
@@ -1312,6 +1477,12 @@ int qtb_plan_set_max_width(qtb_plan* plan, int32_t max_width, int32_t max_slices
         return fail(QTB_ERR_ARG, "plan_set_max_width: bad arguments");
     plan->max_width = max_width;
     plan->max_slices = max_slices;
+    return QTB_OK;
+}
+
+int qtb_plan_set_share_lightcones(qtb_plan* plan, int32_t enable) {
+    if (!plan) return fail(QTB_ERR_ARG, "plan_set_share_lightcones: null plan");
+    plan->share_lightcones = enable != 0;
     return QTB_OK;
 }
 

@@ -161,6 +161,7 @@ struct DeviceBuffers {
 struct qtb_plan {
     int32_t n_params = 0;
     int32_t order_trials = 0;   // extra randomized greedy orders per network
+    bool share_lightcones = true;   // isomorphic lightcones share one compile
     int32_t max_width = 0;      // slice circuits whose width reaches this (0 = never)
     int32_t max_slices = 256;   // networks one sliced circuit may become
     int32_t n_groups = 0;       // circuits added (networks of a circuit share a group)
@@ -198,6 +199,9 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* gates, int32_t n_gates,
                     const std::atomic<bool>* abort = nullptr);
 // compile_circuit's result when `abort` was raised while it ran.
 constexpr int kCompileAborted = -1;
+// Canonical structural key of an edge's lightcone (see plan.cpp).
+void cone_key(int32_t n_nodes, const int64_t* indptr, const int32_t* indices, int32_t u, int32_t v,
+              int32_t p, std::vector<int32_t>* key);
 int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indices,
                     int32_t u, int32_t v, int32_t p, int32_t composer,
                     std::vector<qtb_gate>* gates, int32_t* n_qubits, std::string* err);

@@ -52,6 +52,11 @@ class NetworkPlan:
         the reference's greedy order only)."""
         check(self._lib.qtb_plan_set_order_trials(self._h, int(trials)))
 
+    def set_share_lightcones(self, enable):
+        """Compile edges with isomorphic lightcones once and copy the networks
+        (default on; only ``add_lightcones`` made afterwards)."""
+        check(self._lib.qtb_plan_set_share_lightcones(self._h, 1 if enable else 0))
+
     def add_circuit(self, n_qubits, gates, params, simplify_passes=0):
         gates = np.ascontiguousarray(gates, dtype=_lib.GATE_DTYPE)
         params = np.ascontiguousarray(params, dtype=np.float64)

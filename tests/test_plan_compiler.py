@@ -207,14 +207,67 @@ def test_images_follow_networks_added_after_an_export():
     edges = np.array(list(G.edges()))
     params = np.concatenate(graphs.angles(2, seed=5))
     split = NetworkPlan(4)
+    split.set_share_lightcones(False)     # classes would differ between the two calls
     split.add_lightcones(graph_csr(G), edges[:20], 2, 0, params)
     first = split.export()
     split.scratch_bytes(0, len(split))
     split.add_lightcones(graph_csr(G), edges[20:], 2, 0, params)
     whole = NetworkPlan(4)
+    whole.set_share_lightcones(False)
     whole.add_lightcones(graph_csr(G), edges, 2, 0, params)
     a, b = split.export(), whole.export()
     assert len(a['nets']) == len(edges) > len(first['nets'])
     for key in ('nets', 'ops', 'ins', 'phases', 'runs', 'blobs'):
         assert np.array_equal(a[key], b[key]), key
     assert np.max(np.abs(plan_interp.run_plan(split, params) - plan_interp.run_plan(whole, params))) == 0
+
+
+def _network_blobs(plan):
+    ex = plan.export()
+    runs, blobs = ex['runs'], ex['blobs']
+    return [bytes(blobs[16 * int(r['blob_off16']):16 * int(r['blob_off16']) + int(r['blob_bytes'])])
+            for r in runs]
+
+
+def test_isomorphic_lightcones_share_one_compile():
+    """On a ring every edge's lightcone is the same path, so with sharing
+    every edge gets the first edge's networks (byte-identical blobs), and
+    the edge terms equal the reference's with and without sharing."""
+    import networkx as nx
+    G = nx.cycle_graph(12)
+    edges = np.array(list(G.edges()))
+    gamma, beta = graphs.angles(2, seed=9)
+    params = np.concatenate([gamma, beta])
+    ref = np.array([complex(np.ravel(port.edge_energy(G, gamma, beta, tuple(e)))[0]) for e in edges])
+    shared, own = NetworkPlan(4), NetworkPlan(4)
+    own.set_share_lightcones(False)
+    for plan in (shared, own):
+        plan.add_lightcones(graph_csr(G), edges, 2, 0, params)
+        assert np.max(np.abs(plan_interp.run_plan(plan, params) - ref)) < 1e-10
+    assert len(set(_network_blobs(shared))) == 1
+    assert len(set(_network_blobs(own))) > 1      # the wrap-around edge numbers its cone apart
+
+
+@pytest.mark.parametrize('seed', [0, 1, 2])
+def test_lightcone_sharing_keeps_every_edge_term(seed):
+    """Random 3-regular and Erdos-Renyi graphs (cones with and without
+    cycles): sharing changes no edge term, and on the 3-regular graph it
+    finds isomorphic cones to share."""
+    import networkx as nx
+    for G in (graphs.regular(60, seed=seed), nx.erdos_renyi_graph(40, 3 / 39, seed=seed)):
+        if G.number_of_edges() == 0:
+            continue
+        edges = np.array(list(G.edges()))
+        params = np.concatenate(graphs.angles(2, seed=seed))
+        vals = []
+        for share in (True, False):
+            plan = NetworkPlan(4)
+            plan.set_share_lightcones(share)
+            plan.add_lightcones(graph_csr(G), edges, 2, 0, params)
+            vals.append(plan_interp.run_plan(plan, params))
+        assert np.max(np.abs(vals[0] - vals[1])) < 1e-10
+    plan = NetworkPlan(4)
+    plan.add_lightcones(graph_csr(graphs.regular(60, seed=seed)),
+                        np.array(list(graphs.regular(60, seed=seed).edges())), 2, 0, params)
+    blobs = _network_blobs(plan)
+    assert len(set(blobs)) < len(blobs)
