@@ -241,6 +241,7 @@ def serving_requests(n, seed=0):
 
 def run_serving(n_requests, rate, device_index, plain_budget_s=20.0):
     """Poisson stream through the continuous-batching server; the same
+    stream through a FIFO queue (one compile worker, one stream); the same
     requests one at a time on a single-stream server; and, as the drop-in
     comparison, requests one at a time through the plain backend (one
     bucket-kernel launch per bucket, compile included) until about
@@ -275,14 +276,21 @@ def run_serving(n_requests, rate, device_index, plain_budget_s=20.0):
                 out.append(exc)
         return out
 
-    with QAOAServer(device=device_index, n_streams=4) as srv:
+    def poisson(srv):
         t0 = time.perf_counter()
         futs = []
         for (G, gamma, beta), gap in zip(reqs, gaps):
             time.sleep(gap)
             futs.append(srv.submit(G, gamma, beta))
-        stream = collect(futs)
-        wall_stream = time.perf_counter() - t0
+        out = collect(futs)
+        return out, time.perf_counter() - t0
+
+    with QAOAServer(device=device_index, n_streams=4) as srv:
+        stream, wall_stream = poisson(srv)
+    # the same arrivals through a plain FIFO queue: one compile worker, one
+    # request on the GPU at a time
+    with QAOAServer(device=device_index, n_streams=1, compile_workers=1) as srv:
+        fifo, wall_fifo = poisson(srv)
     with QAOAServer(device=device_index, n_streams=1, compile_workers=1) as srv:
         t0 = time.perf_counter()
         alone = []
@@ -323,6 +331,7 @@ def run_serving(n_requests, rate, device_index, plain_budget_s=20.0):
                         '(seed 1); slicing from width 22, at most 256 slices per edge'.format(
                             len(reqs), rate),
             'continuous_batching': summarize(stream, wall_stream),
+            'fifo_queue': summarize(fifo, wall_fifo),
             'batched_one_at_a_time': summarize(alone, wall_alone),
             'plain_one_at_a_time': plain,
             'same_energy_alone_and_in_mix': all(same(a, b) for a, b in zip(stream, alone))}
