@@ -1263,9 +1263,13 @@ void flatten_plan(qtb_plan* plan) {
 }
 
 // Per-network blobs with network-local indices (see DevNetRun).
+// Networks whose blobs are byte-identical (edges that shared a compile, or
+// equal slices) point at one copy: each is still contracted on its own, but
+// the plan image holds one blob, which the executors then stage from L2.
 void build_blobs(qtb_plan* plan) {
     plan->druns.clear();
     plan->dblobs.clear();
+    std::unordered_map<uint64_t, std::vector<uint32_t>> seen;   // hash -> blob offsets (16 B units)
     for (const Network& n : plan->nets) {
         DevNetRun r{};
         r.blob_off16 = (uint32_t)(plan->dblobs.size() / 16);
@@ -1301,6 +1305,19 @@ void build_blobs(qtb_plan* plan) {
         std::memcpy(dst + ph_bytes + op_bytes, n.ins.data(), in_bytes);
         if (!chunks.empty())
             std::memcpy(dst + chunk_base, chunks.data(), chunks.size() * sizeof(uint16_t));
+        uint64_t h = 1469598103934665603ull ^ total;
+        for (size_t b = 0; b < total; ++b) h = (h ^ dst[b]) * 1099511628211ull;
+        auto& offs = seen[h];
+        for (uint32_t o : offs) {
+            const DevNetRun& prev = plan->druns[o];
+            if (prev.blob_bytes == total &&
+                std::memcmp(plan->dblobs.data() + 16 * (size_t)prev.blob_off16, dst, total) == 0) {
+                r.blob_off16 = prev.blob_off16;
+                plan->dblobs.resize(base);
+                break;
+            }
+        }
+        if (r.blob_off16 == (uint32_t)(base / 16)) offs.push_back((uint32_t)plan->druns.size());
         plan->druns.push_back(r);
     }
 }
