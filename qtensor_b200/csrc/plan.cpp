@@ -1232,6 +1232,7 @@ void merge_network(qtb_plan* plan, Network&& net, int32_t group) {
     plan->nets.push_back(std::move(net));
     plan->uploaded = false;
     plan->images_valid = false;
+    plan->flat_valid = false;
 }
 
 void flatten_plan(qtb_plan* plan) {
@@ -1305,8 +1306,13 @@ void build_blobs(qtb_plan* plan) {
         std::memcpy(dst + ph_bytes + op_bytes, n.ins.data(), in_bytes);
         if (!chunks.empty())
             std::memcpy(dst + chunk_base, chunks.data(), chunks.size() * sizeof(uint16_t));
-        uint64_t h = 1469598103934665603ull ^ total;
-        for (size_t b = 0; b < total; ++b) h = (h ^ dst[b]) * 1099511628211ull;
+        uint64_t h = 0x9E3779B97F4A7C15ull ^ total;   // blobs are whole 16-byte units
+        for (size_t b = 0; b < total; b += 8) {
+            uint64_t word;
+            std::memcpy(&word, dst + b, 8);
+            h = (h ^ word) * 0xff51afd7ed558ccdull;
+            h ^= h >> 32;
+        }
         auto& offs = seen[h];
         for (uint32_t o : offs) {
             const DevNetRun& prev = plan->druns[o];
@@ -1324,9 +1330,14 @@ void build_blobs(qtb_plan* plan) {
 
 void ensure_images(qtb_plan* plan) {
     if (plan->images_valid) return;
-    flatten_plan(plan);
     build_blobs(plan);
     plan->images_valid = true;
+}
+
+void ensure_flat(qtb_plan* plan) {
+    if (plan->flat_valid) return;
+    flatten_plan(plan);
+    plan->flat_valid = true;
 }
 
 }  // namespace qtb
@@ -1551,6 +1562,7 @@ int qtb_plan_export(qtb_plan* plan, int32_t which, void* buf, size_t cap, size_t
     if (!plan || !size) return fail(QTB_ERR_ARG, "plan_export: bad arguments");
     std::lock_guard<std::mutex> lock(plan->mu);
     ensure_images(plan);
+    ensure_flat(plan);
     const void* src = nullptr;
     size_t n = 0;
     switch (which) {

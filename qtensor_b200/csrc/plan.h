@@ -179,7 +179,8 @@ struct qtb_plan {
     std::vector<qtb::DevPhase> dphases;
     std::vector<qtb::DevNetRun> druns;
     std::vector<uint8_t> dblobs;
-    bool images_valid = false;       // the flattened images above match `nets`
+    bool images_valid = false;       // druns and dblobs match `nets`
+    bool flat_valid = false;         // dnets, dops, dins and dphases match `nets`
     uint32_t common_bytes = 0;       // staged gate entries + angle terms
     uint32_t common_terms_off = 0;
     bool uploaded = false;
@@ -207,8 +208,11 @@ int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indic
                     std::vector<qtb_gate>* gates, int32_t* n_qubits, std::string* err);
 void merge_network(qtb_plan* plan, Network&& net, int32_t group);
 void flatten_plan(qtb_plan* plan);
-// flatten_plan + build_blobs unless the images already match the networks.
+// build_blobs (the executors' per-network images) unless they already
+// match the networks.
 void ensure_images(qtb_plan* plan);
+// flatten_plan (the plain path's and the export's arrays) likewise.
+void ensure_flat(qtb_plan* plan);
 uint64_t encode_runs(uint32_t mask, uint32_t w);
 void build_blobs(qtb_plan* plan);
 int rank_of_kind(int32_t kind);

@@ -1905,6 +1905,10 @@ int qtb_plan_run_plain(qtb_plan* plan, int32_t first, int32_t count, const doubl
     if (!plan || !terms_dev || (plan->n_params > 0 && !params_dev))
         return fail(QTB_ERR_ARG, "plan_run_plain: null argument");
     if (!plan->uploaded) return fail(QTB_ERR_ARG, "plan_run_plain: plan not uploaded");
+    {
+        std::lock_guard<std::mutex> lock(plan->mu);
+        ensure_flat(plan);   // the flattened arrays are built on first use
+    }
     if (first < 0 || count < 1 || first + count > (int32_t)plan->dnets.size())
         return fail(QTB_ERR_ARG, "plan_run_plain: network range out of bounds");
     size_t need = 0;
