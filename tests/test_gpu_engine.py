@@ -228,3 +228,35 @@ def test_scratch_bytes_same_before_and_after_upload(cuda_device):
     before = plan.scratch_bytes(0, len(plan))
     plan.upload()
     assert plan.scratch_bytes(0, len(plan)) == before > 0
+
+
+def test_shared_lightcones_match_own_compiles_on_device(cuda_device):
+    """On the device, a plan whose isomorphic lightcones share one compile
+    (and one blob) gives every edge the term of a plan that compiles every
+    edge from its own lightcone, and both match the reference fixture."""
+    from qtensor_b200.plan import NetworkPlan, graph_csr
+    G, w = golden_graph('cfg2')
+    params = np.concatenate([w['gamma'], w['beta']])
+    ref = np.array([complex(*t) for t in w['terms']])
+    params_dev = torch.from_numpy(params).to(cuda_device)
+    out = []
+    for share in (True, False):
+        plan = NetworkPlan(6)
+        plan.set_order_trials(4)
+        plan.set_share_lightcones(share)
+        plan.add_lightcones(graph_csr(G), np.array(list(G.edges())), 3, 0, params)
+        plan.upload()
+        n = len(plan)
+        terms = torch.empty(n, dtype=torch.complex64, device=cuda_device)
+        nbytes = plan.scratch_bytes(0, n)
+        scratch = torch.empty(max(nbytes, 8), dtype=torch.uint8, device=cuda_device) if nbytes else None
+        plan.run(0, n, params_dev, terms, None, scratch, torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        assert plan.device_status() == 0
+        out.append(terms.cpu().numpy())
+        if share:
+            ex = plan.export()
+            assert len(set(ex['runs']['blob_off16'].tolist())) < n     # blobs are shared
+    assert np.max(np.abs(out[0] - ref)) < 1e-5
+    assert np.max(np.abs(out[1] - ref)) < 1e-5
+    assert np.max(np.abs(out[0] - out[1])) < 2e-6
