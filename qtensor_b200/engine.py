@@ -191,7 +191,10 @@ class QAOAEnergyEngine:
 
         The angles only steer the simplifier's near-zero cancellation test;
         a plan whose decisions depend on them is recompiled when they change."""
-        params = self._params(p, gamma, beta)
+        return self._compile(G, p, self._params(p, gamma, beta), edges)
+
+    def _compile(self, G, p, params, edges=None):
+        """``compile`` with the angles already checked and packed."""
         key = self._key(G, p)
         if edges is not None:
             edges = tuple(int(i) for i in edges)
@@ -285,9 +288,10 @@ class QAOAEnergyEngine:
         if (edges is not None and len(edges) == 0) or self._n_edges(G) == 0:
             self._params(p, gamma, beta)       # same argument checks
             return 0.0                         # an empty sum of edge terms (QAOASimulator.py:27-41)
-        cg = self.compile(G, p, gamma, beta, edges)
+        params = self._params(p, gamma, beta)
+        cg = self._compile(G, p, params, edges)
         if path == 'batched':
-            return cg.energy_of(self._params(p, gamma, beta))
+            return cg.energy_of(params)
         self._launch(cg, p, gamma, beta, path)
         return float(cg.energy.cpu()[0])
 
