@@ -271,3 +271,38 @@ def test_lightcone_sharing_keeps_every_edge_term(seed):
                         np.array(list(graphs.regular(60, seed=seed).edges())), 2, 0, params)
     blobs = _network_blobs(plan)
     assert len(set(blobs)) < len(blobs)
+
+
+def _share_partition(plan):
+    """Edges grouped by the blob their networks point at (one network per edge)."""
+    offs = plan.export()['runs']['blob_off16'].tolist()
+    first = {}
+    return [first.setdefault(o, i) for i, o in enumerate(offs)]
+
+
+@pytest.mark.parametrize('seed', [3, 4])
+def test_lightcone_classes_do_not_depend_on_node_labels(seed):
+    """On trees the canonical key is label-free: relabelling the graph's
+    nodes at random (edges kept in the same order) gives the same classes
+    of shared edges, and the same edge terms."""
+    import networkx as nx
+    rng = np.random.default_rng(seed)
+    T = nx.random_labeled_tree(60, seed=seed) if hasattr(nx, 'random_labeled_tree') \
+        else nx.random_tree(60, seed=seed)
+    perm = rng.permutation(60)
+    T2 = nx.Graph()
+    T2.add_nodes_from(sorted(int(perm[v]) for v in T.nodes()))
+    edges = list(T.edges())
+    T2.add_edges_from((int(perm[a]), int(perm[b])) for a, b in edges)
+    params = np.concatenate(graphs.angles(2, seed=seed))
+    plans = []
+    for G, E in ((T, edges), (T2, [(int(perm[a]), int(perm[b])) for a, b in edges])):
+        csr = graph_csr(G)
+        index = {v: i for i, v in enumerate(csr[0])}
+        plan = NetworkPlan(4)
+        plan.add_lightcones(csr, np.array([(index[a], index[b]) for a, b in E], dtype=np.int32), 2, 0, params)
+        plans.append(plan)
+    assert _share_partition(plans[0]) == _share_partition(plans[1])
+    assert len(set(_share_partition(plans[0]))) < len(edges)
+    vals = [plan_interp.run_plan(pl, params) for pl in plans]
+    assert np.max(np.abs(vals[0] - vals[1])) < 1e-10
