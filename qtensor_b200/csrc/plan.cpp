@@ -1090,7 +1090,7 @@ int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indic
 // decides how often isomorphic cones get equal keys.  It comes from colour
 // refinement (distance, role, then the multiset of neighbour colours until
 // the classes stop splitting) and a level-by-level order: distance, colour,
-// the lowest rank among the node's neighbours one level closer, then the
+// the sorted ranks of the node's neighbours one level closer, then the
 // node id.  On trees this numbers isomorphic cones alike; on cones with
 // cycles, ties broken by node id may give distinct keys (a missed share,
 // never a wrong one).
@@ -1166,12 +1166,13 @@ void cone_key(int32_t n_nodes, const int64_t* indptr, const int32_t* indices, in
     order = {0, 1};
     for (int d = 1; d <= p; ++d) {
         std::vector<int32_t> level;
-        std::vector<int32_t> up(n, INT32_MAX);
+        std::vector<std::vector<int32_t>> up(n);   // ranks of the neighbours one level closer
         for (int i = 0; i < n; ++i)
             if (dist[cone[i]] == d) {
                 level.push_back(i);
                 for (int32_t j : nbr[i])
-                    if (dist[cone[j]] == d - 1) up[i] = std::min(up[i], rank[j]);
+                    if (dist[cone[j]] == d - 1) up[i].push_back(rank[j]);
+                std::sort(up[i].begin(), up[i].end());
             }
         std::sort(level.begin(), level.end(), [&](int a, int b) {
             if (color[a] != color[b]) return color[a] < color[b];
