@@ -306,3 +306,15 @@ def test_lightcone_classes_do_not_depend_on_node_labels(seed):
     assert len(set(_share_partition(plans[0]))) < len(edges)
     vals = [plan_interp.run_plan(pl, params) for pl in plans]
     assert np.max(np.abs(vals[0] - vals[1])) < 1e-10
+
+
+@pytest.mark.parametrize('bad', [(3, 3), (3, 99), (-1, 2)])
+def test_invalid_edge_fails_the_call_with_sharing(bad):
+    """An invalid edge among valid ones fails the whole call, names the edge,
+    and adds no network, with lightcone sharing on (the default)."""
+    G = graphs.regular(10, seed=1)
+    edges = np.array(list(G.edges()) + [bad], dtype=np.int32)
+    plan = NetworkPlan(2)
+    with pytest.raises(_lib.QtbError, match='edge {}: lightcone'.format(len(edges) - 1)):
+        plan.add_lightcones(graph_csr(G), edges, 1, 0, np.zeros(2))
+    assert len(plan) == 0
