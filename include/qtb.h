@@ -187,7 +187,9 @@ int qtb_plan_set_order_trials(qtb_plan* plan, int32_t trials);
  * to the edge's ends, contract to the same <Z_u Z_v>, so the first such
  * edge (in edge order) is compiled and the others copy its networks.  Each
  * edge still has networks of its own in the plan and on the device; only
- * the host compile is shared.  The canonical key is compared in full, so a
+ * the host compile is shared, so a shared edge's qtb_plan_network_info and
+ * qtb_plan_network_peo are those of its class's first edge (the same cone,
+ * numbered as that edge's).  The canonical key is compared in full, so a
  * share is never made on a hash alone.  No counterpart in the reference,
  * which compiles every edge (qtensor/QAOASimulator.py:44-66).  0 compiles
  * every edge from its own lightcone.                                     */
