@@ -37,20 +37,23 @@ def lpt_shards(costs, world):
     return [sorted(s) for s in shards]
 
 
-def sharded_energy(G, gamma, beta, partial_energy, group=None, shards=None, device=None):
+def sharded_energy(G, gamma, beta, partial_energy, group=None, shards=None, device=None,
+                   n_edges=None):
     """Energy of ``G`` from the ranks' shares.
 
     partial_energy(G, gamma, beta, edges) -> float: this rank's share,
     ``(len(edges) - Re sum of their edge terms) / 2``; it is called with an
     empty list on a rank that has no edges.  shards: one edge-index list per
     rank (default ``shard_edges``).  device: where the all-reduce tensor
-    lives (a CUDA device for NCCL; CPU for gloo).  Every rank takes part in
-    the same single all-reduce, also when its share is empty."""
+    lives (a CUDA device for NCCL; CPU for gloo).  n_edges: G's edge count
+    when the caller knows it (networkx counts edges in O(nodes)).  Every
+    rank takes part in the same single all-reduce, also when its share is
+    empty."""
     import torch.distributed as dist
     rank = dist.get_rank(group)
     world = dist.get_world_size(group)
-    n = G.number_of_edges()
-    mine = shard_edges(n, rank, world) if shards is None else list(shards[rank])
+    n = G.number_of_edges() if n_edges is None else n_edges
+    mine = shard_edges(n, rank, world) if shards is None else shards[rank]
     share = float(partial_energy(G, gamma, beta, mine)) if mine else 0.0
     t = torch.tensor([share], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
@@ -70,18 +73,26 @@ class DistributedQAOAEnergy:
         self._shards = {}
 
     def _shards_for(self, G, p, gamma, beta):
-        """LPT shards from the plans' algorithmic flops (every rank compiles
-        the whole graph once to cost it), or None for strided shards."""
-        if not self.lpt:
-            return None
+        """One tuple of edge indices per rank, kept per graph (the same
+        tuple every call, so the engine hashes a share once): LPT from the
+        plans' algorithmic flops (every rank compiles the whole graph once
+        to cost it), or strided."""
         key = self.engine._key(G, p)
         if key not in self._shards:
-            cg = self.engine.compile(G, p, gamma, beta)
-            costs = np.zeros(cg.n_edges)
-            for g, info in zip(cg.groups - cg.groups[0], cg.infos):
-                costs[g] += info['alg_flops']
             import torch.distributed as dist
-            self._shards[key] = lpt_shards(costs, dist.get_world_size(self.group))
+            world = dist.get_world_size(self.group)
+            if self.lpt:
+                cg = self.engine.compile(G, p, gamma, beta)
+                costs = np.zeros(cg.n_edges)
+                for g, info in zip(cg.groups - cg.groups[0], cg.infos):
+                    costs[g] += info['alg_flops']
+                shards = lpt_shards(costs, world)
+            else:
+                n = self.engine._n_edges(G)
+                shards = [shard_edges(n, r, world) for r in range(world)]
+            if len(self._shards) >= 64:
+                self._shards.pop(next(iter(self._shards)))
+            self._shards[key] = [tuple(s) for s in shards]
         return self._shards[key]
 
     def energy_expectation(self, G, gamma, beta):
@@ -91,4 +102,5 @@ class DistributedQAOAEnergy:
         def share(G_, gamma_, beta_, edges):
             return self.engine.energy_expectation(G_, gamma_, beta_, edges=edges)
 
-        return sharded_energy(G, gamma, beta, share, self.group, shards, device=self.engine.device)
+        return sharded_energy(G, gamma, beta, share, self.group, shards, device=self.engine.device,
+                              n_edges=self.engine._n_edges(G))

@@ -181,6 +181,7 @@ class QAOAEnergyEngine:
         self.max_slices = max_slices
         self._cache = {}
         self._by_id = {}        # id(G) -> (weakref, nodes, p, key, edge count)
+        self._edge_digests = {}  # id(edge subset) -> (subset, tuple, digest, length)
         self._lock = threading.Lock()
         _lib.check(_lib.lib().qtb_init(self.device.index))
 
@@ -197,8 +198,8 @@ class QAOAEnergyEngine:
         """``compile`` with the angles already checked and packed."""
         key = self._key(G, p)
         if edges is not None:
-            edges = tuple(int(i) for i in edges)
-            key += ':' + hashlib.sha1(repr(edges).encode()).hexdigest()
+            edges, digest = self._edges_digest(edges)
+            key += ':' + digest
         with self._lock:
             cg = self._cache.get(key)
         if cg is not None and (not cg.angle_checks or cg.plan.params_valid(params)):
@@ -255,6 +256,23 @@ class QAOAEnergyEngine:
         if hit is not None and hit[0]() is G and hit[1] == len(G):
             return hit[4]
         return G.number_of_edges()
+
+    def _edges_digest(self, edges):
+        """``(tuple of edge indices, digest)`` of an edge subset.  The digest
+        of the last few subset tuples is kept (with a reference, so an id
+        is not reused while it is cached): a caller that passes the same
+        tuple every call, such as a rank's shard, pays for hashing once."""
+        hit = self._edge_digests.get(id(edges))
+        if hit is not None and hit[0] is edges and hit[3] == len(edges):
+            return hit[1], hit[2]
+        t = tuple(int(i) for i in edges)
+        digest = hashlib.sha1(repr(t).encode()).hexdigest()
+        if not isinstance(edges, tuple):      # a list may change in place: hash it every call
+            return t, digest
+        if len(self._edge_digests) >= 64:
+            self._edge_digests.pop(next(iter(self._edge_digests)))
+        self._edge_digests[id(edges)] = (edges, t, digest, len(edges))
+        return t, digest
 
     def invalidate(self, G):
         """Forget cached plans of ``G`` (after changing it in place)."""

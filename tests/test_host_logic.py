@@ -84,3 +84,24 @@ def test_perf_backend_needs_cuda_loudly(monkeypatch):
     monkeypatch.setattr(torch.cuda, 'is_available', lambda: False)
     with pytest.raises(RuntimeError, match='CUDA'):
         PerfB200Backend().process_bucket([object()])
+
+
+def test_edge_subset_digest_is_memoised_for_tuples_only():
+    """The plan-cache key of an edge subset: a tuple passed again is not
+    rehashed (a rank's shard), a list is hashed every call (it may change in
+    place), and equal subsets give equal keys."""
+    import hashlib
+    import types
+    from qtensor_b200.engine import QAOAEnergyEngine
+    fake = types.SimpleNamespace(_edge_digests={})
+    shard = (0, 2, 4, 6)
+    t1, d1 = QAOAEnergyEngine._edges_digest(fake, shard)
+    assert t1 == shard and d1 == hashlib.sha1(repr(shard).encode()).hexdigest()
+    assert id(shard) in fake._edge_digests
+    t2, d2 = QAOAEnergyEngine._edges_digest(fake, shard)
+    assert (t2, d2) == (t1, d1)
+    as_list = [0, 2, 4, 6]
+    t3, d3 = QAOAEnergyEngine._edges_digest(fake, as_list)
+    assert (t3, d3) == (t1, d1) and id(as_list) not in fake._edge_digests
+    as_list.append(8)
+    assert QAOAEnergyEngine._edges_digest(fake, as_list)[1] != d1
