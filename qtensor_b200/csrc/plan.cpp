@@ -1094,6 +1094,63 @@ int build_lightcone(int32_t n_nodes, const int64_t* indptr, const int32_t* indic
 // node id.  On trees this numbers isomorphic cones alike; on cones with
 // cycles, ties broken by node id may give distinct keys (a missed share,
 // never a wrong one).
+// Coarse invariant of an edge's lightcone, cheap to compute: cone size,
+// number of edges among cone nodes, and the (distance, degree in the cone)
+// histogram.  Isomorphic cones (as cone_key defines them) have equal
+// invariants, so an edge whose invariant no other edge has cannot share and
+// skips cone_key.
+void cone_invariant(int32_t n_nodes, const int64_t* indptr, const int32_t* indices, int32_t u, int32_t v,
+                    int32_t p, std::vector<int32_t>* inv) {
+    static thread_local std::vector<int32_t> dist;
+    if ((int32_t)dist.size() < n_nodes) dist.resize(n_nodes, -1);
+    std::vector<int32_t> cone = {u, v};
+    struct Reset {
+        std::vector<int32_t>& cone;
+        ~Reset() {
+            for (int32_t x : cone) dist[x] = -1;
+        }
+    } reset{cone};
+    dist[u] = dist[v] = 0;
+    for (size_t head = 0; head < cone.size(); ++head) {
+        const int32_t x = cone[head];
+        if (dist[x] == p) continue;
+        for (int64_t e = indptr[x]; e < indptr[x + 1]; ++e) {
+            const int32_t y = indices[e];
+            if (y >= 0 && y < n_nodes && dist[y] < 0) {
+                dist[y] = dist[x] + 1;
+                cone.push_back(y);
+            }
+        }
+    }
+    std::vector<int64_t> cells;   // distance * 2^32 + degree, one per node
+    int64_t twice_edges = 0;
+    for (int32_t x : cone) {
+        int32_t deg = 0;
+        int32_t prev = -1;
+        std::vector<int32_t> nb;
+        for (int64_t e = indptr[x]; e < indptr[x + 1]; ++e) {
+            const int32_t y = indices[e];
+            if (y >= 0 && y < n_nodes && y != x && dist[y] >= 0) nb.push_back(y);
+        }
+        std::sort(nb.begin(), nb.end());
+        for (int32_t y : nb)
+            if (y != prev) {
+                ++deg;
+                prev = y;
+            }
+        twice_edges += deg;
+        cells.push_back(((int64_t)dist[x] << 32) | (int64_t)deg);
+    }
+    std::sort(cells.begin(), cells.end());
+    inv->clear();
+    inv->push_back((int32_t)cone.size());
+    inv->push_back((int32_t)(twice_edges / 2));
+    for (int64_t c : cells) {
+        inv->push_back((int32_t)(c >> 32));
+        inv->push_back((int32_t)(c & 0xffffffff));
+    }
+}
+
 void cone_key(int32_t n_nodes, const int64_t* indptr, const int32_t* indices, int32_t u, int32_t v,
               int32_t p, std::vector<int32_t>* key) {
     static thread_local std::vector<int32_t> dist, loc;
@@ -1122,38 +1179,52 @@ void cone_key(int32_t n_nodes, const int64_t* indptr, const int32_t* indices, in
     }
     const int n = (int)cone.size();
     for (int i = 0; i < n; ++i) loc[cone[i]] = i;
-    // induced subgraph, local indices
-    std::vector<std::vector<int32_t>> nbr(n);
+    // induced subgraph in CSR form, local indices
+    std::vector<int32_t> off(n + 1, 0), adj;
     for (int i = 0; i < n; ++i) {
         const int32_t x = cone[i];
+        const auto begin = (std::ptrdiff_t)adj.size();
         for (int64_t e = indptr[x]; e < indptr[x + 1]; ++e) {
             const int32_t y = indices[e];
-            if (y >= 0 && y < n_nodes && y != x && loc[y] >= 0) nbr[i].push_back(loc[y]);
+            if (y >= 0 && y < n_nodes && y != x && loc[y] >= 0) adj.push_back(loc[y]);
         }
-        std::sort(nbr[i].begin(), nbr[i].end());
-        nbr[i].erase(std::unique(nbr[i].begin(), nbr[i].end()), nbr[i].end());
+        std::sort(adj.begin() + begin, adj.end());
+        adj.erase(std::unique(adj.begin() + begin, adj.end()), adj.end());
+        off[i + 1] = (int32_t)adj.size();
     }
-    // colour refinement to a stable partition
+    // colour refinement to a stable partition.  A round's colour is a hash
+    // of the node's colour and its neighbours' sorted colours; a collision
+    // could only merge classes and cost a share, because keys are compared
+    // in full.
     std::vector<int32_t> color(n);
-    std::vector<std::vector<int32_t>> sig(n);
-    std::vector<int32_t> idx(n);
+    std::vector<uint64_t> h(n);
+    std::vector<int32_t> idx(n), nc;
     auto relabel = [&]() {
         std::iota(idx.begin(), idx.end(), 0);
-        std::sort(idx.begin(), idx.end(), [&](int a, int b) { return sig[a] < sig[b]; });
+        std::sort(idx.begin(), idx.end(), [&](int a, int b) { return h[a] < h[b]; });
         int classes = 0;
         for (int k = 0; k < n; ++k) {
-            if (k > 0 && sig[idx[k]] != sig[idx[k - 1]]) ++classes;
+            if (k > 0 && h[idx[k]] != h[idx[k - 1]]) ++classes;
             color[idx[k]] = classes;
         }
         return classes + 1;
     };
-    for (int i = 0; i < n; ++i) sig[i] = {dist[cone[i]], i == 0 ? 1 : (i == 1 ? 2 : 0)};
+    auto mix = [](uint64_t x, uint64_t y) {
+        x ^= y + 0x9E3779B97F4A7C15ull + (x << 6) + (x >> 2);
+        x *= 0xff51afd7ed558ccdull;
+        return x ^ (x >> 33);
+    };
+    for (int i = 0; i < n; ++i)
+        h[i] = mix((uint64_t)dist[cone[i]], (uint64_t)(i == 0 ? 1 : (i == 1 ? 2 : 0)));
     int classes = relabel();
     for (int round = 0; round < n; ++round) {
         for (int i = 0; i < n; ++i) {
-            sig[i].assign(1, color[i]);
-            for (int32_t j : nbr[i]) sig[i].push_back(color[j]);
-            std::sort(sig[i].begin() + 1, sig[i].end());
+            nc.clear();
+            for (int32_t k = off[i]; k < off[i + 1]; ++k) nc.push_back(color[adj[k]]);
+            std::sort(nc.begin(), nc.end());
+            uint64_t x = mix(0x51ED270Bull, (uint64_t)color[i]);
+            for (int32_t c : nc) x = mix(x, (uint64_t)c);
+            h[i] = mix(x, nc.size());
         }
         const int next = relabel();
         if (next == classes) break;
@@ -1164,19 +1235,26 @@ void cone_key(int32_t n_nodes, const int64_t* indptr, const int32_t* indices, in
     rank[0] = 0;
     rank[1] = 1;
     order = {0, 1};
+    std::vector<int32_t> level, up, up_begin(n), up_end(n);   // ranks of the neighbours one level closer
     for (int d = 1; d <= p; ++d) {
-        std::vector<int32_t> level;
-        std::vector<std::vector<int32_t>> up(n);   // ranks of the neighbours one level closer
+        level.clear();
+        up.clear();
         for (int i = 0; i < n; ++i)
             if (dist[cone[i]] == d) {
                 level.push_back(i);
-                for (int32_t j : nbr[i])
-                    if (dist[cone[j]] == d - 1) up[i].push_back(rank[j]);
-                std::sort(up[i].begin(), up[i].end());
+                up_begin[i] = (int32_t)up.size();
+                for (int32_t k = off[i]; k < off[i + 1]; ++k)
+                    if (dist[cone[adj[k]]] == d - 1) up.push_back(rank[adj[k]]);
+                up_end[i] = (int32_t)up.size();
+                std::sort(up.begin() + up_begin[i], up.end());
             }
         std::sort(level.begin(), level.end(), [&](int a, int b) {
             if (color[a] != color[b]) return color[a] < color[b];
-            if (up[a] != up[b]) return up[a] < up[b];
+            const bool ab = std::lexicographical_compare(up.begin() + up_begin[a], up.begin() + up_end[a],
+                                                         up.begin() + up_begin[b], up.begin() + up_end[b]);
+            const bool ba = std::lexicographical_compare(up.begin() + up_begin[b], up.begin() + up_end[b],
+                                                         up.begin() + up_begin[a], up.begin() + up_end[a]);
+            if (ab != ba) return ab;
             return cone[a] < cone[b];
         });
         for (int32_t i : level) {
@@ -1190,8 +1268,8 @@ void cone_key(int32_t n_nodes, const int64_t* indptr, const int32_t* indices, in
     for (int32_t i : order) key->push_back(dist[cone[i]]);
     std::vector<std::pair<int32_t, int32_t>> edges;
     for (int i = 0; i < n; ++i)
-        for (int32_t j : nbr[i])
-            if (rank[i] < rank[j]) edges.emplace_back(rank[i], rank[j]);
+        for (int32_t k = off[i]; k < off[i + 1]; ++k)
+            if (rank[i] < rank[adj[k]]) edges.emplace_back(rank[i], rank[adj[k]]);
     std::sort(edges.begin(), edges.end());
     for (const auto& e : edges) {
         key->push_back(e.first);
@@ -1446,12 +1524,38 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
     std::vector<int32_t> rep(n_edges);
     std::iota(rep.begin(), rep.end(), 0);
     if (plan->share_lightcones && n_edges > 1) {
+        auto valid = [&](int32_t i) {
+            const int32_t a = edges[2 * i], b = edges[2 * i + 1];
+            return a >= 0 && b >= 0 && a < n_nodes && b < n_nodes && a != b && p >= 0;
+        };
+        // coarse invariants first: only edges whose invariant recurs can share
         std::vector<std::vector<int32_t>> keys(n_edges);
         parallel_for(n_edges, n_threads, [&](int32_t i) {
-            const int32_t a = edges[2 * i], b = edges[2 * i + 1];
-            if (a >= 0 && b >= 0 && a < n_nodes && b < n_nodes && a != b && p >= 0)
-                cone_key(n_nodes, indptr, indices, a, b, p, &keys[i]);
+            if (valid(i)) cone_invariant(n_nodes, indptr, indices, edges[2 * i], edges[2 * i + 1], p, &keys[i]);
         });
+        {
+            std::unordered_map<uint64_t, std::vector<int32_t>> seen;
+            std::vector<char> recurs(n_edges, 0);
+            for (int32_t i = 0; i < n_edges; ++i) {
+                if (keys[i].empty()) continue;
+                uint64_t h = 1469598103934665603ull;
+                for (int32_t x : keys[i]) h = (h ^ (uint32_t)x) * 1099511628211ull;
+                auto& firsts = seen[h];   // first edge of every distinct invariant
+                bool found = false;
+                for (int32_t r : firsts)
+                    if (keys[r] == keys[i]) {
+                        recurs[r] = recurs[i] = 1;
+                        found = true;
+                        break;
+                    }
+                if (!found) firsts.push_back(i);
+            }
+            for (int32_t i = 0; i < n_edges; ++i)
+                if (!recurs[i]) keys[i].clear();
+            parallel_for(n_edges, n_threads, [&](int32_t i) {
+                if (recurs[i]) cone_key(n_nodes, indptr, indices, edges[2 * i], edges[2 * i + 1], p, &keys[i]);
+            });
+        }
         std::unordered_map<uint64_t, std::vector<int32_t>> classes;
         for (int32_t i = 0; i < n_edges; ++i) {
             if (keys[i].empty()) continue;   // invalid edge: compiled alone, reports its error
