@@ -125,16 +125,18 @@ namespace {
 enum SKind { SK_ZZ, SK_X, SK_Y, SK_ZP, SK_H, SK_CX, SK_Z, SK_ID };
 enum SBasis { SB_Z = 1, SB_X, SB_Y, SB_XY, SB_CA, SB_CB };
 
+// A gate as the simplifier sees it; its symbolic angle is expression
+// `expr` of the pass's pool (-1: none), so gates move without copying it.
 struct SGate {
     int kind = SK_ID;
     int nq = 0;
     int q[2] = {-1, -1};
     int basis[2] = {0, 0};
     double angle = 0.0;
-    Expr expr;
+    int32_t expr = -1;
 };
 
-SGate make_sgate(int kind, const int* qs, double angle, const Expr& expr) {
+SGate make_sgate(int kind, const int* qs, double angle, int32_t expr) {
     SGate g;
     g.kind = kind;
     g.angle = angle;
@@ -153,21 +155,21 @@ SGate make_sgate(int kind, const int* qs, double angle, const Expr& expr) {
             g.basis[0] = SB_CA;
             g.basis[1] = SB_CB;
             g.angle = 0.0;
-            g.expr.clear();
+            g.expr = -1;
             break;
         case SK_H:
             g.nq = 1;
             g.q[0] = qs[0];
             g.basis[0] = SB_XY;
             g.angle = M_PI / 2.0 / std::sqrt(2.0);   // fixed, gates.py hadamard
-            g.expr.clear();
+            g.expr = -1;
             break;
         case SK_Z:
             g.nq = 1;
             g.q[0] = qs[0];
             g.basis[0] = SB_Z;
             g.angle = 0.0;
-            g.expr.clear();
+            g.expr = -1;
             break;
         case SK_X: case SK_Y: case SK_ZP:
             g.nq = 1;
@@ -178,7 +180,7 @@ SGate make_sgate(int kind, const int* qs, double angle, const Expr& expr) {
             g.kind = SK_ID;
             g.nq = 0;
             g.angle = 0.0;
-            g.expr.clear();
+            g.expr = -1;
     }
     return g;
 }
@@ -235,6 +237,7 @@ int simplify(std::vector<Gate>* gates, std::vector<AngleCheck>* checks, bool* an
     const int n = (int)gates->size();
     if (n == 0) return QTB_OK;
     std::vector<SGate> cir(n);
+    std::vector<Expr> pool(n);   // gate i's expression, then merged ones
     for (int i = 0; i < n; ++i) {
         const Gate& g = (*gates)[i];
         int sk = skind_of(g.kind);
@@ -242,8 +245,12 @@ int simplify(std::vector<Gate>* gates, std::vector<AngleCheck>* checks, bool* an
             *err = "simplifier: gate kind " + std::to_string(g.kind) + " has no commutation record";
             return QTB_ERR_UNSUPPORTED;
         }
-        cir[i] = make_sgate(sk, g.q, g.angle, g.expr);
+        cir[i] = make_sgate(sk, g.q, g.angle, i);
     }
+    for (int i = 0; i < n; ++i)
+        if (cir[i].expr >= 0) pool[i] = std::move((*gates)[i].expr);
+    static const Expr kNoExpr;
+    auto expr_of = [&](const SGate& g) -> const Expr& { return g.expr >= 0 ? pool[g.expr] : kNoExpr; };
     // same-site pairs (i < j) visited by distance j - i, ties in order of i:
     // the reference's visiting order, with pairs formed within groups of
     // gates of the same kind on the same qubits instead of over all pairs.
@@ -311,7 +318,7 @@ int simplify(std::vector<Gate>* gates, std::vector<AngleCheck>* checks, bool* an
         }
         if (!ok) continue;
         const double total = cir[a].angle + cir[b].angle;
-        const Expr sym = expr_add(cir[a].expr, cir[b].expr);
+        Expr sym = expr_add(expr_of(cir[a]), expr_of(cir[b]));
         const bool param = cir[a].kind == SK_ZZ || cir[a].kind == SK_X || cir[a].kind == SK_Y ||
                            cir[a].kind == SK_ZP;
         if (std::fabs(total) < 1e-5) {
@@ -323,7 +330,8 @@ int simplify(std::vector<Gate>* gates, std::vector<AngleCheck>* checks, bool* an
             cir[b] = SGate();
         } else {
             if (param) checks->push_back({sym, false});
-            SGate merged = make_sgate(cir[a].kind, cir[a].q, total, sym);
+            pool.push_back(std::move(sym));
+            SGate merged = make_sgate(cir[a].kind, cir[a].q, total, (int32_t)pool.size() - 1);
             cir[a] = SGate();
             cir[b] = merged;
         }
@@ -336,7 +344,7 @@ int simplify(std::vector<Gate>* gates, std::vector<AngleCheck>* checks, bool* an
         g.q[0] = s.q[0];
         g.q[1] = s.nq > 1 ? s.q[1] : -1;
         g.angle = s.angle;
-        g.expr = s.expr;
+        if (s.expr >= 0) g.expr = std::move(pool[s.expr]);
         out.push_back(std::move(g));
     }
     gates->swap(out);
