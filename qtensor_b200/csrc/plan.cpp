@@ -1432,6 +1432,10 @@ void ensure_flat(qtb_plan* plan) {
 // =================================================================== C ABI
 using namespace qtb;
 
+// Most int32 words of cone invariants and keys one lightcone call may hold
+// (256 MiB); past it, edges are compiled without sharing.
+constexpr size_t kShareKeyLimit = size_t(1) << 26;
+
 // Runs fn(i) for i in [0, n) on up to n_threads threads (0 = all cores).
 namespace qtb {
 template <typename Fn>
@@ -1541,7 +1545,13 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
         parallel_for(n_edges, n_threads, [&](int32_t i) {
             if (valid(i)) cone_invariant(n_nodes, indptr, indices, edges[2 * i], edges[2 * i + 1], p, &keys[i]);
         });
-        {
+        size_t held = 0;
+        for (const auto& k : keys) held += k.size();
+        if (held > kShareKeyLimit) {   // very large cones: compile every edge, hold no keys
+            keys.clear();
+            keys.shrink_to_fit();
+            keys.resize(n_edges);
+        } else {
             std::unordered_map<uint64_t, std::vector<int32_t>> seen;
             std::vector<char> recurs(n_edges, 0);
             for (int32_t i = 0; i < n_edges; ++i) {
@@ -1566,7 +1576,7 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
         }
         std::unordered_map<uint64_t, std::vector<int32_t>> classes;
         for (int32_t i = 0; i < n_edges; ++i) {
-            if (keys[i].empty()) continue;   // invalid edge: compiled alone, reports its error
+            if (keys[i].empty()) continue;   // no key (invalid edge, or a cone no other matches): alone
             uint64_t h = 1469598103934665603ull;
             for (int32_t x : keys[i]) h = (h ^ (uint32_t)x) * 1099511628211ull;
             auto& members = classes[h];
