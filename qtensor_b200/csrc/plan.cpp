@@ -426,23 +426,18 @@ static double greedy_order(const LineGraph& g, const std::vector<char>& removed,
     adj.assign(g.adj.begin(), g.adj.end());
     std::vector<int32_t> deg(g.deg);
     auto gone = [&](int x) { return removed[x] != 0; };
-    // degree buckets over the alive nodes
-    std::vector<std::vector<uint64_t>> bucket;
-    std::vector<int32_t> bucket_count;
-    auto bucket_of = [&](int d) -> std::vector<uint64_t>& {
-        if ((int)bucket.size() <= d) {
-            bucket.resize(d + 1);
-            bucket_count.resize(d + 1, 0);
-        }
-        if (bucket[d].empty()) bucket[d].assign(W, 0);
-        return bucket[d];
-    };
+    // degree buckets over the alive nodes: bucket d is W words at d * W
+    // (a degree is below V)
+    static thread_local std::vector<uint64_t> bucket;
+    static thread_local std::vector<int32_t> bucket_count;
+    bucket.assign((size_t)std::max(V, 1) * W, 0);
+    bucket_count.assign(std::max(V, 1), 0);
     auto add = [&](int x, int d) {
-        bucket_of(d)[x >> 6] |= 1ull << (x & 63);
+        bucket[(size_t)d * W + (x >> 6)] |= 1ull << (x & 63);
         ++bucket_count[d];
     };
     auto del = [&](int x, int d) {
-        bucket[d][x >> 6] &= ~(1ull << (x & 63));
+        bucket[(size_t)d * W + (x >> 6)] &= ~(1ull << (x & 63));
         --bucket_count[d];
     };
     int n_alive = 0;
@@ -456,10 +451,13 @@ static double greedy_order(const LineGraph& g, const std::vector<char>& removed,
     double cost = 0.0;
     order->clear();
     degrees->clear();
+    // eliminating a node of least degree d leaves every degree at least
+    // d - 1, so the search for the next least degree starts there
+    int dmin = 0;
     for (; n_alive > 0; --n_alive) {
-        int dmin = 0;
+        dmin = std::max(0, dmin - 1);
         while (bucket_count[dmin] == 0) ++dmin;
-        const std::vector<uint64_t>& bk = bucket[dmin];
+        const uint64_t* bk = &bucket[(size_t)dmin * W];
         int x = -1;
         if (seed == 0) {
             for (int w = 0; w < W && x < 0; ++w)
