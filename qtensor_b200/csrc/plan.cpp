@@ -94,14 +94,12 @@ uint64_t encode_runs(uint32_t mask, uint32_t w) {
     const uint32_t low = w >= 32 ? mask : (mask & ((1u << w) - 1u));
     uint64_t runs = 0;
     uint64_t n = 0;
-    uint32_t dst = 0, first_start = 0, first_len = 0;
-    for (uint32_t bit = 0; bit < 32;) {
-        if (!((low >> bit) & 1u)) {
-            ++bit;
-            continue;
-        }
-        uint32_t len = 0;
-        while (bit + len < 32 && ((low >> (bit + len)) & 1u)) ++len;
+    uint32_t first_start = 0, first_len = 0;
+    // runs in ascending bit order: the lowest set bit starts one, and its
+    // length is the number of ones from there
+    for (uint64_t rest = low; rest;) {
+        const uint32_t bit = (uint32_t)__builtin_ctzll(rest);
+        const uint32_t len = (uint32_t)__builtin_ctzll(~(rest >> bit));
         if (n == (uint64_t)kMaxRuns) return kRunsFallback << 60;
         if (n == 0) {
             first_start = bit;
@@ -109,8 +107,7 @@ uint64_t encode_runs(uint32_t mask, uint32_t w) {
         }
         runs |= (uint64_t)(bit | (len << 5)) << (10 * n);
         ++n;
-        dst += len;
-        bit += len;
+        rest &= ~(((1ull << len) - 1ull) << bit);
     }
     if (n <= 1) {   // pre-decoded single run
         const uint64_t lenmask = first_len >= 32 ? 0xffffffffull : ((1ull << first_len) - 1ull);
