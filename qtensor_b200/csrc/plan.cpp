@@ -908,12 +908,18 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
         struct Live { uint32_t off, size; int32_t end; };
         std::vector<Live> active;
         uint32_t arena = 0, max_elems = 1;
-        // `active` stays sorted by offset: first fit over the live intervals
+        // `active` stays sorted by offset: first fit over the live intervals.
+        // Ops come in level order and an interval placed at a level ends
+        // after it, so expired intervals are swept once per level.
+        int32_t swept = -1;
         for (int32_t oi : by_level) {
             OpRec& op = ops[oi];
-            active.erase(std::remove_if(active.begin(), active.end(),
-                                        [&](const Live& l) { return l.end < op.level; }),
-                         active.end());
+            if (op.level != swept) {
+                active.erase(std::remove_if(active.begin(), active.end(),
+                                            [&](const Live& l) { return l.end < op.level; }),
+                             active.end());
+                swept = op.level;
+            }
             const uint32_t size = 1u << op.w;
             max_elems = std::max(max_elems, size);
             const uint32_t need = (size + 3u) & ~3u;
