@@ -1314,7 +1314,8 @@ void merge_network(qtb_plan* plan, Network&& net, int32_t group) {
     for (DevIn& in : net.ins)
         if (in.src & kSrcTable) in.src = kSrcTable | table_off[in.src & ~kSrcTable];
     if (net.result_src & kSrcTable) net.result_src = kSrcTable | table_off[net.result_src & ~kSrcTable];
-    for (AngleCheck& c : net.checks) plan->checks.push_back(c);
+    for (AngleCheck& c : net.checks)   // networks of a circuit, and shared edges, repeat decisions
+        if (plan->check_index.emplace(c.must_be_small, c.expr).second) plan->checks.push_back(c);
     net.entries.clear();
     net.entries.shrink_to_fit();
     plan->nets.push_back(std::move(net));

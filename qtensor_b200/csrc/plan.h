@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <map>
 #include <mutex>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -171,7 +172,8 @@ struct qtb_plan {
     std::vector<qtb::DevEntry> entries;
     std::vector<qtb::DevTerm> terms;
     uint32_t table_elems = 0;
-    std::vector<qtb::AngleCheck> checks;
+    std::vector<qtb::AngleCheck> checks;   // distinct decisions over all networks
+    std::set<std::pair<bool, qtb::Expr>> check_index;
     // flattened device images
     std::vector<qtb::DevNet> dnets;
     std::vector<qtb::DevOp> dops;
