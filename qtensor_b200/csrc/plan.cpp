@@ -509,6 +509,107 @@ static double greedy_order(const LineGraph& g, const std::vector<char>& removed,
     return cost;
 }
 
+// Minimum-fill elimination on the same line graph: the next node is the one
+// whose elimination adds the fewest new edges among its neighbours (ties:
+// least degree, then the lowest index for seed 0 or a random one).  It is
+// the classic fill-in heuristic for treewidth (e.g. Bodlaender and Koster,
+// "Treewidth computations I. Upper bounds", 2010), used here as extra
+// candidates of the native order search; the reference's rule stays
+// greedy_order with seed 0.  fill(x) = sum over neighbours a of x of the
+// neighbours of x not adjacent to a, halved.  Eliminating x only changes the
+// rows of its neighbours, so only they and their neighbours are rescored.
+// Returns sum over eliminations of 2^degree.
+static double minfill_order(const LineGraph& g, const std::vector<char>& removed, uint64_t seed,
+                            std::vector<int32_t>* order, std::vector<int32_t>* degrees) {
+    const int V = g.V, W = g.W;
+    static thread_local std::vector<uint64_t> adj, touched;
+    static thread_local std::vector<int64_t> fill;
+    adj.assign(g.adj.begin(), g.adj.end());
+    std::vector<int32_t> deg(g.deg);
+    fill.assign(V, 0);
+    touched.assign(W, 0);
+    std::vector<char> alive(V, 0);
+    auto row = [&](int x) { return &adj[(size_t)x * W]; };
+    auto score = [&](int x) {
+        const uint64_t* rx = row(x);
+        int64_t f = 0;
+        for (int w = 0; w < W; ++w)
+            for (uint64_t bits = rx[w]; bits; bits &= bits - 1) {
+                const int a = w * 64 + __builtin_ctzll(bits);
+                const uint64_t* ra = row(a);
+                int64_t miss = 0;
+                for (int k = 0; k < W; ++k) miss += __builtin_popcountll(rx[k] & ~ra[k]);
+                f += miss - 1;   // a itself is in rx and not in ra
+            }
+        return f / 2;
+    };
+    int n_alive = 0;
+    for (int x = 0; x < V; ++x)
+        if (!removed[x]) {
+            alive[x] = 1;
+            ++n_alive;
+        }
+    for (int x = 0; x < V; ++x)
+        if (alive[x]) fill[x] = score(x);
+    uint64_t rng = seed;
+    double cost = 0.0;
+    order->clear();
+    degrees->clear();
+    std::vector<int32_t> nbrs, ties;
+    for (; n_alive > 0; --n_alive) {
+        int64_t best_f = INT64_MAX;
+        int best_d = INT_MAX;
+        ties.clear();
+        for (int x = 0; x < V; ++x) {
+            if (!alive[x]) continue;
+            if (fill[x] < best_f || (fill[x] == best_f && deg[x] < best_d)) {
+                best_f = fill[x];
+                best_d = deg[x];
+                ties.clear();
+            }
+            if (fill[x] == best_f && deg[x] == best_d) ties.push_back(x);
+        }
+        int x = ties[0];
+        if (seed != 0) {
+            rng ^= rng << 13;
+            rng ^= rng >> 7;
+            rng ^= rng << 17;
+            x = ties[rng % ties.size()];
+        }
+        alive[x] = 0;
+        nbrs.clear();
+        uint64_t* rx = row(x);
+        for (int w = 0; w < W; ++w)
+            for (uint64_t bits = rx[w]; bits; bits &= bits - 1) nbrs.push_back(w * 64 + __builtin_ctzll(bits));
+        order->push_back(x);
+        degrees->push_back((int32_t)nbrs.size());
+        cost += std::ldexp(1.0, (int)nbrs.size());
+        // neighbours become a clique; x leaves the graph
+        std::fill(touched.begin(), touched.end(), 0);
+        for (int a : nbrs) {
+            uint64_t* ra = row(a);
+            int d = 0;
+            for (int w = 0; w < W; ++w) {
+                ra[w] |= rx[w];
+                if (w == (a >> 6)) ra[w] &= ~(1ull << (a & 63));
+                if (w == (x >> 6)) ra[w] &= ~(1ull << (x & 63));
+                d += __builtin_popcountll(ra[w]);
+                touched[w] |= ra[w];
+            }
+            deg[a] = d;
+            touched[a >> 6] |= 1ull << (a & 63);
+        }
+        for (int w = 0; w < W; ++w) rx[w] = 0;
+        touched[x >> 6] &= ~(1ull << (x & 63));
+        for (int w = 0; w < W; ++w)
+            for (uint64_t bits = touched[w]; bits; bits &= bits - 1) {
+                const int y = w * 64 + __builtin_ctzll(bits);
+                if (alive[y]) fill[y] = score(y);
+            }
+    }
+    return cost;
+}
+
 int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
                     int32_t simplify_passes, const double* params, int32_t n_params,
                     int32_t order_trials, int32_t max_width, int32_t max_slices,
@@ -626,18 +727,27 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
     std::vector<int32_t> par;   // sliced line-graph nodes, in slicing order
     std::vector<int32_t> gorder, gdeg, torder, tdeg;
     LineGraph lg;
+    // With trials, the minimum-fill heuristic competes too: its
+    // deterministic order plus one randomized order per four greedy trials.
     auto best_order = [&]() {
         line_graph(V, cliques, removed, &lg);
         double best_cost = greedy_order(lg, removed, 0, &gorder, &gdeg);
-        for (int32_t t = 1; t <= order_trials; ++t) {
-            const uint64_t seed = 0x9E3779B97F4A7C15ull * (uint64_t)t + (uint64_t)V;
-            const double c = greedy_order(lg, removed, seed, &torder, &tdeg);
+        auto keep = [&](double c) {
             if (c < best_cost) {
                 best_cost = c;
                 gorder.swap(torder);
                 gdeg.swap(tdeg);
             }
+        };
+        for (int32_t t = 1; t <= order_trials; ++t) {
+            const uint64_t seed = 0x9E3779B97F4A7C15ull * (uint64_t)t + (uint64_t)V;
+            keep(greedy_order(lg, removed, seed, &torder, &tdeg));
         }
+        if (order_trials > 0)
+            for (int32_t t = 0; t <= order_trials / 4; ++t) {
+                const uint64_t seed = t == 0 ? 0 : 0xD1B54A32D192ED03ull * (uint64_t)t + (uint64_t)V;
+                keep(minfill_order(lg, removed, seed, &torder, &tdeg));
+            }
     };
     best_order();
     auto width = [&]() { return gdeg.empty() ? 0 : *std::max_element(gdeg.begin(), gdeg.end()); };
@@ -905,9 +1015,13 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
         std::stable_sort(by_level.begin(), by_level.end(), [&](int32_t x, int32_t y) {
             return ops[x].level != ops[y].level ? ops[x].level < ops[y].level : ops[x].w > ops[y].w;
         });
-        struct Live { uint32_t off, size; int32_t end; };
+        // Offsets are computed in 64 bits: an arena (and a phase) must stay
+        // below kMaxArenaElems, since arena offsets share their word with
+        // the kSrcTable flag and the executors index elements in 32 bits.
+        struct Live { uint64_t off, size; int32_t end; };
         std::vector<Live> active;
-        uint32_t arena = 0, max_elems = 1;
+        uint64_t arena = 0;
+        uint32_t max_elems = 1;
         // `active` stays sorted by offset: first fit over the live intervals.
         // Ops come in level order and an interval placed at a level ends
         // after it, so expired intervals are swept once per level.
@@ -920,20 +1034,26 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
                              active.end());
                 swept = op.level;
             }
-            const uint32_t size = 1u << op.w;
-            max_elems = std::max(max_elems, size);
-            const uint32_t need = (size + 3u) & ~3u;
-            uint32_t off = 0;
+            const uint64_t size = uint64_t(1) << op.w;
+            max_elems = (uint32_t)std::max<uint64_t>(max_elems, size);
+            const uint64_t need = (size + 3u) & ~uint64_t(3);
+            uint64_t off = 0;
             for (const Live& l : active) {
                 if (off + need <= l.off) break;
                 off = std::max(off, l.off + l.size);
             }
-            op.dst = off;
+            op.dst = (uint32_t)off;
             const Live item{off, need, op.consumer_level};
             active.insert(std::upper_bound(active.begin(), active.end(), item,
                                            [](const Live& a, const Live& b) { return a.off < b.off; }),
                           item);
             arena = std::max(arena, off + need);
+            if (arena > kMaxArenaElems) {
+                *err = "compile: network needs an arena of more than " + std::to_string(kMaxArenaElems) +
+                       " complex64 elements (width " + std::to_string(op.w) +
+                       "); slice it (qtb_plan_set_max_width)";
+                return QTB_ERR_UNSUPPORTED;
+            }
         }
 
         // ---- device images: ops in phase order

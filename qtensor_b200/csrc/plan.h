@@ -131,6 +131,11 @@ struct AngleCheck {
     bool must_be_small;   // true: |expr| < 1e-5 (cancelled); false: >= 1e-5 (merged)
 };
 
+// Largest network arena (complex64 elements, 16 GiB): arena offsets must
+// stay below the kSrcTable flag bit, and a wide wave rounds each arena up
+// to 64 elements inside 31-bit element counts.
+constexpr uint64_t kMaxArenaElems = (uint64_t(1) << 31) - 64;
+
 // Most variables sliced per circuit (2^k networks).
 constexpr int kMaxSlicedVars = 16;
 // Most output qubits of an amplitude batch (2^k amplitudes per circuit).

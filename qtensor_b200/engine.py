@@ -159,13 +159,18 @@ class QAOAEnergyEngine:
     composer: ``'default'`` (ZZ gates + commutation simplifier, QTensor's
     ``DefaultQAOAComposer``), ``'zz'`` or ``'cx'``.
     ordering: ``'native'`` (C++ lightcones, multithreaded, and the cheapest of
-    ``order_trials`` randomized greedy orders per network) or ``'reference'``
-    (QTensor's exact qubit numbering and greedy elimination order).
+    the reference greedy order, ``order_trials`` randomized greedy orders and
+    minimum-fill orders per network) or ``'reference'`` (QTensor's exact
+    qubit numbering and greedy elimination order).
+    max_width / max_slices: a circuit whose width reaches ``max_width`` is
+    sliced into at most ``max_slices`` networks (FeynmanSimulator's scheme,
+    qtensor/FeynmanSimulator.py:49-84); the default 29 slices only what one
+    B200's memory cannot hold unsliced.
     """
 
     def __init__(self, composer='default', ordering='native', device=None, threads=0,
-                 cache_size=16, order_trials=16, autotune=True, max_width=24,
-                 max_slices=256):
+                 cache_size=16, order_trials=16, autotune=True, max_width=29,
+                 max_slices=1024):
         _require_cuda()
         if ordering not in ('native', 'reference'):
             raise ValueError('ordering must be "native" or "reference"')

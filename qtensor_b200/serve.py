@@ -100,14 +100,20 @@ class QAOAServer:
     """Continuous-batching energy server.
 
     n_streams: requests in flight on the GPU at once; memory_budget: bytes of
-    device memory the in-flight requests may hold; max_width: networks whose
-    greedy width reaches it are sliced, into at most max_slices networks
-    per edge (a request needing more fails alone); compile_workers: host threads
-    compiling requests concurrently (each also uses the C++ compiler's own
-    threads)."""
+    device memory the in-flight requests may hold (default: three quarters
+    of the device's memory); max_width: networks whose width (best of the
+    greedy and minimum-fill orders) reaches it are sliced, into at most
+    max_slices networks per edge.  The default 29 keeps every unsliced
+    network's largest tensor at 2^28 complex64 elements (2 GiB) and its
+    arena below 16 GiB, so only circuits that do not fit HBM are sliced.  A
+    request that would need more slices fails alone and fast: its lightcones
+    are wider than any exact contraction on one GPU can hold (the reference
+    would have to allocate tensors of that width too).  compile_workers:
+    host threads compiling requests concurrently (each also uses the C++
+    compiler's own threads)."""
 
-    def __init__(self, device=None, n_streams=4, memory_budget=16 << 30, max_width=22,
-                 max_slices=256, composer='default', order_trials=8, compile_workers=2,
+    def __init__(self, device=None, n_streams=4, memory_budget=None, max_width=29,
+                 max_slices=1024, composer='default', order_trials=8, compile_workers=2,
                  compile_threads=0):
         if not torch.cuda.is_available():
             raise RuntimeError('QAOAServer needs a CUDA device; there is no CPU fallback')
@@ -118,6 +124,8 @@ class QAOAServer:
         self.order_trials = order_trials
         self.compile_threads = compile_threads
         _lib.check(_lib.lib().qtb_init(self.device.index))
+        if memory_budget is None:
+            memory_budget = torch.cuda.get_device_properties(self.device).total_memory * 3 // 4
         self.admission = AdmissionControl(memory_budget, n_streams)
         self.streams = [torch.cuda.Stream(self.device) for _ in range(n_streams)]
         self._compile_pool = ThreadPoolExecutor(max_workers=compile_workers)

@@ -54,3 +54,15 @@ def by_name(name):
         _, kind, n, p, d = name.split('_')
         return family(kind, int(n[1:]), int(d[1:]))
     raise KeyError(name)
+
+
+def erdos_renyi(n, seed, mean_degree=3):
+    """Erdos-Renyi graph of the serving workload (edge probability mean_degree / (n - 1))."""
+    return nx.erdos_renyi_graph(n, mean_degree / (n - 1), seed=seed)
+
+
+# Graphs of the serving workload whose widest edges are the corner cases of
+# the compiler (seeds as the serving stream draws them).
+ER_P4_N109 = dict(n=109, seed=716218221, p=4)   # edges of width 40+: intractable
+ER_P3_N335 = dict(n=335, seed=949594894, p=3)   # one edge of width 28-31
+ER_P3_N213 = dict(n=213, seed=796350419, p=3)   # edges of width 28-31

@@ -318,3 +318,68 @@ def test_invalid_edge_fails_the_call_with_sharing(bad):
     with pytest.raises(_lib.QtbError, match='edge {}: lightcone'.format(len(edges) - 1)):
         plan.add_lightcones(graph_csr(G), edges, 1, 0, np.zeros(2))
     assert len(plan) == 0
+
+
+def _edge_plan(G, edge, p, max_width, max_slices, trials=8):
+    csr = graph_csr(G)
+    idx = {v: i for i, v in enumerate(csr[0])}
+    plan = NetworkPlan(2 * p)
+    plan.set_order_trials(trials)
+    plan.set_max_width(max_width, max_slices)
+    g, b = graphs.angles(p, seed=1)
+    plan.add_lightcones(csr, np.array([[idx[edge[0]], idx[edge[1]]]], dtype=np.int32), p,
+                        composer_id('default'), np.concatenate([g, b]), 1)
+    return plan
+
+
+def _widest_edge(G, p):
+    """An edge of G whose lightcone the reference's greedy order makes
+    widest (port of OrderingOptimizer, qtensor/optimisation/Optimizer.py:65-87)."""
+    g, b = graphs.angles(p, seed=1)
+    best = None
+    for e in list(G.edges())[:12]:
+        circ = port.lightcone_circuit(G, e, g, b)
+        buckets, _, bra, ket = port.circuit_to_network(circ)
+        _, width = port.order_network(buckets, bra, ket)
+        if best is None or width > best[1]:
+            best = (e, width)
+    return best
+
+
+def test_network_beyond_arena_limit_is_rejected_not_crashed():
+    """A lightcone whose contraction needs an arena beyond 2^31 complex64
+    elements fails to compile with QTB_ERR_UNSUPPORTED (it used to write
+    arena offsets into the gate-table flag bit and crash the compiler).  The
+    reference's own greedy order gives that edge a width of 40 or more: its
+    NumpyBackend would have to allocate a 2^40-element tensor, so no exact
+    bucket elimination answers it."""
+    G = graphs.erdos_renyi(graphs.ER_P4_N109['n'], graphs.ER_P4_N109['seed'])
+    edge, ref_width = _widest_edge(G, 4)
+    assert ref_width >= 40
+    with pytest.raises(_lib.QtbError) as exc:
+        _edge_plan(G, edge, 4, max_width=0, max_slices=256)
+    assert exc.value.code == _lib.QTB_ERR_UNSUPPORTED
+    assert 'arena' in str(exc.value) or 'exceeds the limit' in str(exc.value)
+    # with slicing the request fails fast, naming the width it would need
+    with pytest.raises(_lib.QtbError) as exc:
+        _edge_plan(G, edge, 4, max_width=29, max_slices=1024)
+    assert exc.value.code == _lib.QTB_ERR_UNSUPPORTED and 'width' in str(exc.value)
+
+
+def test_minfill_candidates_never_worse_than_greedy():
+    """The native order search keeps the cheapest (sum of 2^width over
+    eliminations) of the reference greedy order, randomized greedy orders
+    and minimum-fill orders: edge by edge its width is at most the
+    reference order's, and over the edges it moves fewer bytes."""
+    G = graphs.erdos_renyi(graphs.ER_P3_N213['n'], graphs.ER_P3_N213['seed'])
+    ref_bytes = nat_bytes = 0.0
+    for e in list(G.edges())[:20]:
+        try:
+            ref = _edge_plan(G, e, 3, 0, 1, trials=0).info(0)
+        except _lib.QtbError:
+            continue     # the reference order is too wide to compile at all
+        nat = _edge_plan(G, e, 3, 0, 1, trials=8).info(0)
+        assert nat['treewidth'] <= ref['treewidth']
+        ref_bytes += ref['alg_bytes']
+        nat_bytes += nat['alg_bytes']
+    assert nat_bytes < ref_bytes
