@@ -9,7 +9,15 @@ same batched GPU contraction (process counts do not apply);
 ``energy_expectation_mpi`` shards the edges over an initialised
 ``torch.distributed`` group when there is one (every rank receives the
 energy), and otherwise runs on this GPU.
+
+The energies come back in the reference's shape: its per-edge amplitudes are
+the flattened one-element arrays of ``QtreeSimulator.simulate`` and their sum
+goes through ``_post_process_energy`` (qtensor/QAOASimulator.py:27-41), so a
+graph with edges gives a float64 array of shape (1,) (callers index
+``E[0]``), and a graph without edges the plain float 0.0.
 """
+import numpy as np
+
 from .engine import QAOAEnergyEngine
 
 _COMPOSERS = {'DefaultQAOAComposer': 'default', 'ZZQtreeQAOAComposer': 'zz',
@@ -23,6 +31,13 @@ def composer_name(composer):
     return _COMPOSERS[key]
 
 
+def _reference_shape(G, E):
+    """``_post_process_energy``'s result type for an energy ``E``."""
+    if G.number_of_edges() == 0:
+        return 0.0
+    return np.array([E], dtype=np.float64)
+
+
 class QAOAQtreeSimulator:
     """The reference simulator's energy API over ``QAOAEnergyEngine``."""
 
@@ -31,21 +46,21 @@ class QAOAQtreeSimulator:
         self._distributed = None
 
     def energy_expectation(self, G, gamma, beta):
-        return self.engine.energy_expectation(G, gamma, beta)
+        return _reference_shape(G, self.engine.energy_expectation(G, gamma, beta))
 
     def energy_expectation_parallel(self, G, gamma, beta, n_processes=None):
-        return self.engine.energy_expectation(G, gamma, beta)
+        return _reference_shape(G, self.engine.energy_expectation(G, gamma, beta))
 
     def energy_expectation_mpi(self, G, gamma, beta, n_processes=None, print_perf=False):
         import torch.distributed as dist
         if not (dist.is_available() and dist.is_initialized()):
-            return self.engine.energy_expectation(G, gamma, beta)
+            return _reference_shape(G, self.engine.energy_expectation(G, gamma, beta))
         from .distributed import sharded_energy
 
         def share(G_, gamma_, beta_, edges):
             return self.engine.energy_expectation(G_, gamma_, beta_, edges=edges)
 
-        return sharded_energy(G, gamma, beta, share, device=self.engine.device)
+        return _reference_shape(G, sharded_energy(G, gamma, beta, share, device=self.engine.device))
 
 
 QAOASimulator = QAOAQtreeSimulator
