@@ -295,24 +295,31 @@ int qtb_plan_set_timing(qtb_plan* plan, int32_t enable);
 int qtb_plan_collect_timing(qtb_plan* plan, double* total_ms, int64_t* launches);
 
 /* ------------------------------------------------- allocation-free run
- * No counterpart in the reference.  For callers that cannot allocate device
- * memory while they run -- code inside a CUDA stream capture, or a host
- * framework that owns every device allocation through its own pool:
+ * No counterpart in the reference.  For callers that must not allocate
+ * device memory while they run: a host framework that owns every device
+ * allocation through its own pool (a cudaMalloc behind its back escapes its
+ * accounting), or a process held to a fixed device-memory budget.
  * qtb_plan_run may allocate on first use of a range (job arrays, streams,
- * events) and needs caller-allocated scratch for wide networks, this entry
+ * events) and needs caller-allocated scratch for wide networks; this entry
  * point allocates nothing.  It contracts networks [first, first+count) of an
  * already uploaded plan (qtb_plan_upload, which allocates, is a set-up step)
  * with every network's arena, the job list and the completion counter in one
  * library-owned static device array of QTB_NOALLOC_SCRATCH_BYTES, held by
- * every GPU that loads the library until the process exits.  Results equal
- * qtb_plan_run's.  Requests needing more than the array (16 B per network
- * plus count x the largest arena of the range x 8 B, plus 512 B) fail with
- * QTB_ERR_UNSUPPORTED and a message; split the range.  The first call on a
- * device looks up the array's device address (once per device, that device
- * current) and should come before any stream capture.  Every call shares
- * the array and it keeps the last call's contents (the counter is cleared
- * on the stream by each call): calls that overlap on the GPU race, so issue
- * them on one stream or serialise them.                                   */
+ * every GPU that loads the library until the process exits.  Every network
+ * runs on one CTA with its arena in that array (plan blobs too large for
+ * shared memory are read from global memory), so a network too wide for
+ * shared memory, which qtb_plan_run would contract with the whole GPU, runs
+ * far slower here.  Results equal qtb_plan_run's.  Requests needing more than
+ * the array (16 B per network plus count x the largest arena of the range x
+ * 8 B, plus 512 B) fail with QTB_ERR_UNSUPPORTED and a message; split the
+ * range.  The first call on a device looks up the array's device address
+ * (once per device, that device current) and should come before any stream
+ * capture.  Every call shares the array and it keeps the last call's
+ * contents (the counter is cleared on the stream by each call): calls that
+ * overlap on the GPU race, so issue them on one stream or serialise them.
+ * A call also races with a qtb_plan_run of the same plan that overlaps it
+ * on the GPU: both write the plan's gate table in global memory (when it
+ * does not fit shared memory) and its status word.                        */
 #define QTB_NOALLOC_SCRATCH_BYTES (64u << 20)
 int qtb_plan_run_noalloc(qtb_plan* plan, int32_t first, int32_t count, const double* params_dev,
                          void* terms_dev, double* energy_dev, void* stream);

@@ -1,7 +1,8 @@
 """Import the reference ``qtensor`` package on top of the oracle ``qtree``.
 
 TEST INFRASTRUCTURE ONLY, and only where a read-only checkout of the
-reference exists (``QTENSOR_REFERENCE`` or the default location below); the
+reference exists (``QTENSOR_REFERENCE``, else a directory ``reference`` beside
+this repository's root); the
 fixture generator ``tests/golden/make_golden.py`` and the CPU test that pins
 ``oracle/qtensor_port.py`` against the reference use it.
 
@@ -17,7 +18,8 @@ import time
 import types
 
 ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_REFERENCE = '/root/reference'
+# a checkout named ``reference`` next to the repository root
+DEFAULT_REFERENCE = os.path.join(os.path.dirname(os.path.dirname(ORACLE_DIR)), 'reference')
 
 
 def reference_root():

@@ -324,32 +324,27 @@ __device__ __forceinline__ void neumaier_add(double& sum, double& comp, double x
     sum = t;
 }
 
-// Compensated fp64 sum of Re(terms) by one CTA in a fixed order, then
-// energy = (n_groups - sum) / 2.
-__device__ void reduce_energy(const float2* terms, uint32_t n, double n_groups, double* energy) {
-    __shared__ double ws[32], wc[32];
+// Compensated fp64 sum of Re(terms) by one warp (all 32 lanes call it) in
+// a fixed order -- lane l sums terms l, l + 32, ..., then a butterfly --
+// then energy = (n_groups - sum) / 2.  The order does not depend on the
+// launch shape, so every schedule gives the same energy for the same terms.
+__device__ void reduce_energy_warp(const float2* terms, uint32_t n, double n_groups, double* energy) {
+    const uint32_t lane = threadIdx.x & 31u;
     double s = 0.0, c = 0.0;
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) neumaier_add(s, c, (double)__ldcg(terms + i).x);
+    for (uint32_t i = lane; i < n; i += 32u) neumaier_add(s, c, (double)__ldcg(terms + i).x);
     for (int off = 16; off > 0; off >>= 1) {
         const double os = __shfl_xor_sync(0xffffffffu, s, off);
         const double oc = __shfl_xor_sync(0xffffffffu, c, off);
         neumaier_add(s, c, os);
         neumaier_add(s, c, oc);
     }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0) {
-        ws[warp] = s;
-        wc[warp] = c;
-    }
+    if (lane == 0) *energy = (n_groups - (s + c)) * 0.5;
+}
+
+// The same by a whole CTA: its first warp sums, the others wait.
+__device__ void reduce_energy(const float2* terms, uint32_t n, double n_groups, double* energy) {
+    if (threadIdx.x < 32) reduce_energy_warp(terms, n, n_groups, energy);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double ts = 0.0, tc = 0.0;
-        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
-            neumaier_add(ts, tc, ws[i]);
-            neumaier_add(ts, tc, wc[i]);
-        }
-        *energy = (n_groups - (ts + tc)) * 0.5;
-    }
 }
 
 // The op of a phase holding flattened element g, starting from op `oi` at
@@ -550,6 +545,126 @@ __global__ void __launch_bounds__(kLean ? 128 : (kPersistent ? 512 : 1024), kLea
             if (threadIdx.x == 0) *a.done = 0u;   // ready for the next run
             __syncthreads();
         }
+    }
+}
+
+// ----------------------------------------------------------------- K3w
+// Warp-per-network executor for small networks: every warp of a persistent
+// CTA takes networks from the run's queue and contracts each one alone,
+// staging its blob into the warp's own shared-memory slot by one bulk copy
+// (the warp's mbarrier, bounded wait) and keeping its arena in the slot
+// after it.  A phase is ceil(elements / 32) rounds of the warp, lane l
+// taking element 32 r + l, so the op of a round's first element is the
+// phase's chunk-table entry r; phases are separated by warp barriers only.
+// With no CTA barrier between dependent phases and about twelve networks
+// in flight per SM, a run of small networks is bound by the warps' issue
+// rate rather than by the per-phase latency of a whole CTA.  Shared memory:
+// [plan-wide gate entries + angle terms][gate table] once per CTA (when
+// kSmemTable), then per warp [mbarrier, 16 B][blob, blob_capacity]
+// [arena, arena_capacity complex64].
+constexpr int kWarpMaxThreads = 256;
+
+__device__ __forceinline__ void warp_bar_wait(uint64_t* bar, uint32_t parity, int* status, bool* ok) {
+    const uint32_t bar_a = smem_addr(bar);
+    uint32_t done = 0;
+    for (uint32_t it = 0; it < kStageSpinLimit; ++it) {
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}" : "=r"(done) : "r"(bar_a), "r"(parity) : "memory");
+        if (done) break;
+        if (it > 64) __nanosleep(32);
+    }
+    if (!done && (threadIdx.x & 31u) == 0) atomicOr(status, kStatusStageTimeout);
+    *ok = __all_sync(0xffffffffu, done != 0);
+}
+
+template <bool kSmemTable>
+__global__ void __launch_bounds__(kWarpMaxThreads) qtb_warp_network_kernel(const Job* __restrict__ jobs,
+                                                                          const RunArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (a.queue == nullptr) {
+        if (threadIdx.x == 0) atomicOr(a.status, kStatusQueue);
+        return;
+    }
+    unsigned char* common = smem;
+    float2* stable = reinterpret_cast<float2*>(smem + (kSmemTable ? a.common_bytes : 0u));
+    const uint32_t table_bytes = kSmemTable ? ((a.table_elems * 8u + 15u) & ~15u) : 0u;
+    const uint32_t slot_bytes = 16u + a.blob_capacity + 8u * a.arena_capacity;
+    unsigned char* slot = smem + (kSmemTable ? a.common_bytes : 0u) + table_bytes + warp * slot_bytes;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(slot);
+    unsigned char* blob = slot + 16;
+    float2* arena = reinterpret_cast<float2*>(blob + a.blob_capacity);
+    if (kSmemTable) {
+        // plan-wide gate entries and angle terms (tiny), then the table
+        const uint4* src = a.common;
+        uint4* dst = reinterpret_cast<uint4*>(common);
+        for (uint32_t i = threadIdx.x; i < a.common_bytes / 16u; i += blockDim.x) dst[i] = __ldg(src + i);
+        __syncthreads();
+        build_table(common, a, stable);
+    }
+    const float2* __restrict__ table = kSmemTable ? stable : a.gtable;
+    if (lane == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    uint32_t parity = 0;
+    for (;;) {
+        uint32_t job = 0;
+        if (lane == 0) job = atomicAdd(a.queue, 1u);
+        job = __shfl_sync(0xffffffffu, job, 0);
+        if (job >= a.n_jobs) break;
+        const Job jb = jobs[job];
+        const DevNetRun net = *jb.net;
+        if (net.arena_elems > a.arena_capacity || net.blob_bytes > a.blob_capacity) {
+            if (lane == 0) atomicOr(a.status, net.arena_elems > a.arena_capacity ? kStatusArena : kStatusBlob);
+            return;
+        }
+        if (lane == 0) {
+            // the slot was last read by this warp's generic loads
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            const uint32_t bar_a = smem_addr(bar);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(net.blob_bytes)
+                         : "memory");
+            bulk_copy(blob, a.blobs + net.blob_off16, net.blob_bytes, bar_a);
+        }
+        bool ok = false;
+        warp_bar_wait(bar, parity, a.status, &ok);
+        if (!ok) return;
+        parity ^= 1u;
+        const DevPhase* phases = reinterpret_cast<const DevPhase*>(blob);
+        const DevOp* ops = reinterpret_cast<const DevOp*>(blob + net.n_phases * sizeof(DevPhase));
+        const DevIn* ins = reinterpret_cast<const DevIn*>(blob + net.ins_off);
+        for (uint32_t p = 0; p < net.n_phases; ++p) {
+            const DevPhase ph = phases[p];
+            const uint16_t* chunk = reinterpret_cast<const uint16_t*>(blob + ph.chunk_off);
+            for (uint32_t r = 0; r * 32u < ph.total_elems; ++r) {
+                const uint32_t g = r * 32u + lane;
+                if (g < ph.total_elems) {
+                    uint32_t oi = chunk[r];
+                    DevOp op = ops[oi];
+                    find_op(g, oi, op, [&](uint32_t i) { return ops[i]; });
+                    compute_element<kSmemTable>(op, g - op.elem_begin, ins, table, arena);
+                }
+            }
+            __syncwarp();
+        }
+        uint32_t last = 0;
+        if (lane == 0) {
+            *jb.term = (net.result_src & kSrcTable) ? table[net.result_src & ~kSrcTable] : arena[net.result_src];
+            if (a.energy) {
+                __threadfence();
+                last = atomicAdd(a.done, 1u) == a.total_jobs - 1u;
+            }
+        }
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (a.energy && last) {
+            __threadfence();
+            reduce_energy_warp(a.terms, a.total_jobs, a.energy_groups, a.energy);
+            if (lane == 0) *a.done = 0u;   // ready for the next run
+        }
+        __syncwarp();   // the slot is reused by the next network
     }
 }
 
@@ -903,11 +1018,13 @@ constexpr int kSmemClasses = (int)(sizeof(kClassCtas) / sizeof(kClassCtas[0]));
 constexpr int kMaxClasses = kSmemClasses + 1;   // + the stream of the wide waves
 constexpr int kLeanThreads = 128;
 constexpr int kLeanCtasPerSm = 8;
+constexpr int kWarpDefaultThreads = 128;   // warps per CTA of the warp queue x 32
 
 struct LaunchClass {
     bool smem;
     bool persistent;        // CTAs take networks from the run's queue
     bool lean;              // persistent, 128 threads, registers capped (8 CTAs per SM)
+    bool warp;              // persistent, every warp takes networks (qtb_warp_network_kernel)
     int grid;               // CTAs (= n_jobs unless persistent)
     uint32_t capacity;      // arena elements per CTA
     uint32_t blob_capacity; // plan-blob bytes per CTA
@@ -944,7 +1061,7 @@ struct WideWave {
     int grid;
 };
 
-constexpr int kSchedClasses = 0, kSchedPersistent = 1, kSchedHybrid = 2;
+constexpr int kSchedClasses = 0, kSchedPersistent = 1, kSchedHybrid = 2, kSchedWarp = 3;
 
 struct RunCache {
     Job* jobs = nullptr;                // class-mode jobs, persistent-mode jobs, counters
@@ -955,6 +1072,7 @@ struct RunCache {
     std::vector<LaunchClass> classes;   // class schedule, widest first
     std::vector<LaunchClass> pclasses;  // persistent schedule
     std::vector<LaunchClass> hclasses;  // hybrid schedule: large networks as classes + lean queue
+    std::vector<LaunchClass> wclasses;  // warp schedule: large networks as classes + warp queue
     std::vector<WideWave> waves;        // wide networks (both schedules), run one after another
     void* wide_buf = nullptr;
     size_t counters_bytes = 0;          // counters of all waves, zeroed before a run
@@ -992,6 +1110,7 @@ static qtb_plan_device* dev_state(const qtb_plan* p) {
 static const std::vector<LaunchClass>& schedule_of(const RunCache* rc) {
     return rc->schedule == kSchedPersistent ? rc->pclasses
            : rc->schedule == kSchedHybrid   ? rc->hclasses
+           : rc->schedule == kSchedWarp     ? rc->wclasses
                                             : rc->classes;
 }
 
@@ -1022,6 +1141,10 @@ static void free_device(qtb_plan* plan) {
 // Kernel instantiation for a launch class.
 template <bool kA, bool kT>
 static void launch_one(const LaunchClass& lc, const Job* jobs, const RunArgs& a, cudaStream_t st) {
+    if (lc.warp) {
+        qtb_warp_network_kernel<kT><<<lc.grid, lc.threads, lc.smem_bytes, st>>>(jobs, a);
+        return;
+    }
     if constexpr (kA) {
         if (lc.lean) {
             qtb_network_kernel<true, kT, true, true><<<lc.grid, kLeanThreads, lc.smem_bytes, st>>>(jobs, a);
@@ -1062,6 +1185,10 @@ static int allow_all_smem() {
     QTB_CUDA((allow_smem<false, false, true>()));
     QTB_CUDA((allow_smem<true, true, true, true>()));
     QTB_CUDA((allow_smem<true, false, true, true>()));
+    QTB_CUDA(cudaFuncSetAttribute(qtb_warp_network_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kSmemLimitBytes));
+    QTB_CUDA(cudaFuncSetAttribute(qtb_warp_network_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kSmemLimitBytes));
     return QTB_OK;
 }
 
@@ -1070,7 +1197,18 @@ static int persistent_grid(const LaunchClass& lc, bool smem_table, int* grid) {
     int per_sm = 0, sms = 0, dev = 0;
     QTB_CUDA(cudaGetDevice(&dev));
     QTB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    if (lc.lean) {
+    if (lc.warp) {
+        if (smem_table)
+            QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qtb_warp_network_kernel<true>,
+                                                                   lc.threads, lc.smem_bytes));
+        else
+            QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qtb_warp_network_kernel<false>,
+                                                                   lc.threads, lc.smem_bytes));
+        // enough CTAs for one warp per network
+        const int warps = std::max(1, lc.threads / 32);
+        *grid = std::max(1, std::min((lc.n_jobs + warps - 1) / warps, std::max(1, per_sm) * sms));
+        return QTB_OK;
+    } else if (lc.lean) {
         if (smem_table)
             QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
                 &per_sm, qtb_network_kernel<true, true, true, true>, kLeanThreads, lc.smem_bytes));
@@ -1094,7 +1232,7 @@ static int persistent_grid(const LaunchClass& lc, bool smem_table, int* grid) {
 static int hybrid_lean_grid(std::vector<LaunchClass>& sched, bool smem_table) {
     LaunchClass* lean = nullptr;
     for (LaunchClass& lc : sched)
-        if (lc.lean) lean = &lc;
+        if (lc.lean || lc.warp) lean = &lc;
     if (!lean) return QTB_OK;
     int full = 0;
     LaunchClass probe = *lean;
@@ -1103,8 +1241,8 @@ static int hybrid_lean_grid(std::vector<LaunchClass>& sched, bool smem_table) {
     if (r) return r;
     long long taken = 0;
     for (const LaunchClass& lc : sched) {
-        if (lc.lean) continue;
-        const long long by_threads = (lc.threads + kLeanThreads - 1) / kLeanThreads;
+        if (&lc == lean) continue;
+        const long long by_threads = (lc.threads + lean->threads - 1) / lean->threads;
         const long long by_smem = lean->smem_bytes ? (long long)((lc.smem_bytes + lean->smem_bytes - 1) / lean->smem_bytes) : 1;
         taken += (long long)lc.n_jobs * std::max(by_threads, by_smem);
     }
@@ -1112,8 +1250,36 @@ static int hybrid_lean_grid(std::vector<LaunchClass>& sched, bool smem_table) {
     QTB_CUDA(cudaGetDevice(&dev));
     QTB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const long long grid = std::max<long long>(sms, (long long)full - taken);
-    lean->grid = (int)std::max<long long>(1, std::min<long long>(lean->n_jobs, grid));
+    // a warp queue needs one warp per network at most
+    const int per_cta = lean->warp ? std::max(1, lean->threads / 32) : 1;
+    const long long need = (lean->n_jobs + per_cta - 1) / per_cta;
+    lean->grid = (int)std::max<long long>(1, std::min<long long>(need, grid));
     return QTB_OK;
+}
+
+// Shared memory of a warp-queue launch class of `threads` threads: the
+// fixed part, then one slot (mbarrier, blob, arena) per warp.
+static size_t warp_slot(const LaunchClass& lc) {
+    return 16 + (size_t)lc.blob_capacity + 8 * (size_t)lc.capacity;
+}
+static size_t warp_smem(const LaunchClass& lc, size_t fixed, int threads) {
+    return fixed + (size_t)(threads / 32) * warp_slot(lc);
+}
+
+// Re-shape the warp queue of a schedule to `threads` threads per CTA (its
+// shared memory and grid follow); false if that does not fit a CTA.
+static bool set_warp_threads(std::vector<LaunchClass>& sched, bool smem_table, int threads, int* err) {
+    *err = QTB_OK;
+    for (LaunchClass& q : sched)
+        if (q.warp) {
+            const size_t fixed = q.smem_bytes - (size_t)(q.threads / 32) * warp_slot(q);
+            const size_t smem = warp_smem(q, fixed, threads);
+            if (smem > kSmemLimitBytes) return false;
+            q.threads = threads;
+            q.smem_bytes = smem;
+        }
+    *err = hybrid_lean_grid(sched, smem_table);
+    return *err == QTB_OK;
 }
 
 static void destroy_streams(qtb_plan_device* s) {
@@ -1429,6 +1595,40 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
             rc->hclasses.push_back(lc);
         }
     }
+    // warp schedule: the networks whose warp slot (blob + arena) is at most
+    // the 95th percentile of the run's slots go to one warp queue (every
+    // warp contracts its own network), the others run as class launches,
+    // started first
+    rc->wclasses.clear();
+    if (!all.empty()) {
+        auto slot_of = [&](int32_t i) {
+            return 16 + (size_t)plan->druns[i].blob_bytes + 8 * (size_t)((plan->druns[i].arena_elems + 3u) & ~3u);
+        };
+        std::vector<size_t> slots;
+        for (int32_t i : all) slots.push_back(slot_of(i));
+        std::sort(slots.begin(), slots.end());
+        const size_t cap = std::min(slots[std::min(slots.size() - 1, slots.size() * 95 / 100)],
+                                    (kSmemLimitBytes - fixed) / 2);
+        std::vector<int32_t> small, large;
+        for (int32_t i : all) (slot_of(i) <= cap ? small : large).push_back(i);
+        if (!small.empty()) {
+            std::vector<int> class_of(count, kSmemClasses);
+            for (int c = 0; c < kSmemClasses; ++c)
+                for (int32_t i : members[c]) class_of[i - first] = c;
+            for (int c = kSmemClasses - 1; c >= 0; --c) {
+                std::vector<int32_t> m;
+                for (int32_t i : large)
+                    if (class_of[i - first] == c) m.push_back(i);
+                if (!m.empty()) rc->wclasses.push_back(make_class(m, true, false));
+            }
+            LaunchClass lc = make_class(small, true, true);
+            lc.warp = true;
+            lc.threads = kWarpDefaultThreads;
+            while (lc.threads > 32 && warp_smem(lc, fixed, lc.threads) > kSmemLimitBytes) lc.threads /= 2;
+            lc.smem_bytes = warp_smem(lc, fixed, lc.threads);
+            rc->wclasses.push_back(lc);
+        }
+    }
     if (!device) return build_waves(plan, members[kSmemClasses], first, terms, rc, false);
     // jobs of both schedules, then 16 bytes of counters (done, queue), zeroed
     const size_t job_bytes = jobs.size() * sizeof(Job);
@@ -1446,6 +1646,10 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
         }
     if (!rc->hclasses.empty()) {
         int r = hybrid_lean_grid(rc->hclasses, rc->smem_table);
+        if (r) return r;
+    }
+    if (!rc->wclasses.empty()) {
+        int r = hybrid_lean_grid(rc->wclasses, rc->smem_table);
         if (r) return r;
     }
     return build_waves(plan, members[kSmemClasses], first, terms, rc, true);
@@ -1712,6 +1916,7 @@ static int autotune_run(qtb_plan_device* s, RunCache* rc, const RunArgs& base, v
     }
     // hybrid schedule: the large-network classes with 256..1024 threads
     float hyb_ms = 1e30f;
+    int big_threads = 512;   // block size of large-network classes, as the hybrid tuning finds
     if (!rc->hclasses.empty()) {
         int best_t = 512;
         for (int t : {256, 512, 1024}) {
@@ -1732,7 +1937,33 @@ static int autotune_run(qtb_plan_device* s, RunCache* rc, const RunArgs& base, v
         }
         for (LaunchClass& q : rc->hclasses)
             if (!q.lean) q.threads = best_t;
+        big_threads = best_t;
         if ((r = hybrid_lean_grid(rc->hclasses, rc->smem_table))) return r;
+    }
+    // warp schedule: the warp queue with 2, 4 or 8 warps per CTA (the
+    // large-network classes keep their tuned block size)
+    float warp_ms = 1e30f;
+    if (!rc->wclasses.empty()) {
+        for (LaunchClass& q : rc->wclasses)
+            if (!q.warp) q.threads = big_threads;
+        int best_t = 0;
+        for (int t : {64, 128, 256}) {
+            std::vector<LaunchClass> sched = rc->wclasses;
+            if (!set_warp_threads(sched, rc->smem_table, t, &r)) {
+                if (r) return r;
+                continue;
+            }
+            float ms = 1e30f;
+            if ((r = time_it([&] { return launch_schedule(s, rc, sched, a, scratch_dev, st); }, &ms)))
+                return r;
+            if (log)
+                std::fprintf(stderr, "qtb autotune: warp schedule %4d threads per CTA %.1f us\n", t, 1e3 * ms);
+            if (ms < warp_ms) {
+                warp_ms = ms;
+                best_t = t;
+            }
+        }
+        if (best_t && !set_warp_threads(rc->wclasses, rc->smem_table, best_t, &r) && r) return r;
     }
     rc->schedule = kSchedClasses;
     float best_ms = class_ms;
@@ -1740,11 +1971,19 @@ static int autotune_run(qtb_plan_device* s, RunCache* rc, const RunArgs& base, v
         rc->schedule = kSchedPersistent;
         best_ms = pers_ms;
     }
-    if (hyb_ms < best_ms) rc->schedule = kSchedHybrid;
+    if (hyb_ms < best_ms) {
+        rc->schedule = kSchedHybrid;
+        best_ms = hyb_ms;
+    }
+    if (warp_ms < best_ms) rc->schedule = kSchedWarp;
     if (log)
-        std::fprintf(stderr, "qtb autotune: class schedule %.1f us, persistent %.1f us, hybrid %.1f us -> %s\n",
-                     1e3 * class_ms, 1e3 * pers_ms, 1e3 * hyb_ms,
-                     rc->schedule == kSchedHybrid ? "hybrid" : rc->schedule == kSchedPersistent ? "persistent" : "classes");
+        std::fprintf(stderr,
+                     "qtb autotune: class schedule %.1f us, persistent %.1f us, hybrid %.1f us, warp %.1f us -> %s\n",
+                     1e3 * class_ms, 1e3 * pers_ms, 1e3 * hyb_ms, 1e3 * warp_ms,
+                     rc->schedule == kSchedWarp       ? "warp"
+                     : rc->schedule == kSchedHybrid   ? "hybrid"
+                     : rc->schedule == kSchedPersistent ? "persistent"
+                                                      : "classes");
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     rc->tuned = true;
@@ -1752,7 +1991,8 @@ static int autotune_run(qtb_plan_device* s, RunCache* rc, const RunArgs& base, v
 }
 
 // QTB_SCHEDULE=persistent:<128|256|512>, hybrid:<256|512|1024> (threads of
-// the large-network classes) or QTB_SCHEDULE=classes in the
+// the large-network classes), warp:<64|128|256> (threads per CTA of the
+// warp queue) or QTB_SCHEDULE=classes in the
 // environment fixes the schedule of every range without timing it, so that a
 // profiler sees one chosen configuration.  Returns 1 when it applied.
 static int forced_schedule(RunCache* rc, int* err) {
@@ -1775,6 +2015,11 @@ static int forced_schedule(RunCache* rc, int* err) {
             if (!q.lean) q.threads = t;
         if ((*err = hybrid_lean_grid(rc->hclasses, rc->smem_table))) return 0;
         rc->schedule = kSchedHybrid;
+    } else if (std::strncmp(env, "warp:", 5) == 0 && !rc->wclasses.empty()) {
+        const int t = std::atoi(env + 5);
+        if (t != 64 && t != 128 && t != 256) return 0;
+        if (!set_warp_threads(rc->wclasses, rc->smem_table, t, err)) return 0;
+        rc->schedule = kSchedWarp;
     } else if (std::strcmp(env, "classes") == 0) {
         rc->schedule = kSchedClasses;
     } else {
@@ -2065,9 +2310,11 @@ int qtb_plan_run_noalloc(qtb_plan* plan, int32_t first, int32_t count, const dou
         maxe = std::max(maxe, plan->druns[i].max_elems);
     }
     cap = (cap + 3u) & ~3u;
+    // a range whose largest blob does not fit shared memory reads every
+    // blob from global memory (blob capacity 0), as qtb_plan_run's global
+    // classes do
+    if (fixed + blob > kSmemLimitBytes) blob = 0;
     const size_t smem_bytes = fixed + blob;
-    if (smem_bytes > kSmemLimitBytes)
-        return fail(QTB_ERR_UNSUPPORTED, "run_noalloc: network plan blob exceeds shared memory");
     const size_t jobs_off = 512;
     const size_t arenas_off = jobs_off + (((size_t)count * sizeof(Job) + 255) & ~size_t(255));
     const size_t need = arenas_off + (size_t)count * cap * sizeof(float2);
@@ -2150,7 +2397,7 @@ int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32
             out[4 * c] = lc.n_jobs;
             out[4 * c + 1] = lc.threads;
             out[4 * c + 2] = (int32_t)lc.smem_bytes;
-            out[4 * c + 3] = (lc.smem ? 1 : 0) | (lc.persistent ? 2 : 0) | (lc.lean ? 8 : 0);
+            out[4 * c + 3] = (lc.smem ? 1 : 0) | (lc.persistent ? 2 : 0) | (lc.lean ? 8 : 0) | (lc.warp ? 16 : 0);
         } else {
             const WideWave& wv = rc->waves[c - sched.size()];
             out[4 * c] = (int32_t)wv.n_nets;

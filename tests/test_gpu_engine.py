@@ -151,12 +151,14 @@ def test_wide_waves_match_plain_path(cuda_device):
     assert cg.plan.device_status() == 0
 
 
-@pytest.mark.parametrize('schedule', ['classes', 'persistent:256', 'hybrid:512', 'hybrid:1024'])
+@pytest.mark.parametrize('schedule', ['classes', 'persistent:256', 'hybrid:512', 'hybrid:1024',
+                                      'warp:64', 'warp:128', 'warp:256'])
 def test_every_schedule_matches_reference(cuda_device, monkeypatch, schedule):
     """Each executor schedule the autotuner may pick (size classes, one
-    persistent queue, large-network classes + lean queue), forced through
-    QTB_SCHEDULE, gives the reference's edge terms for all 1500 edges of the
-    N=1000 p=3 workload."""
+    persistent queue, large-network classes + lean queue, large-network
+    classes + warp-per-network queue), forced through QTB_SCHEDULE, gives
+    the reference's edge terms for all 1500 edges of the N=1000 p=3
+    workload."""
     monkeypatch.setenv('QTB_SCHEDULE', schedule)
     eng = _engine()
     G, w = golden_graph('cfg3')
@@ -166,6 +168,8 @@ def test_every_schedule_matches_reference(cuda_device, monkeypatch, schedule):
     cfg = eng.compile(G, 3, w['gamma'], w['beta']).plan.last_launch_config()
     if schedule.startswith('hybrid'):
         assert any(c[3] & 8 for c in cfg) and any(not c[3] & 2 for c in cfg)
+    elif schedule.startswith('warp'):
+        assert any(c[3] & 16 and c[1] == int(schedule[5:]) for c in cfg)
     elif schedule == 'classes':
         assert not any(c[3] & 2 for c in cfg)
     else:
@@ -173,14 +177,20 @@ def test_every_schedule_matches_reference(cuda_device, monkeypatch, schedule):
 
 
 def test_reference_named_simulator(cuda_device):
-    """QAOAQtreeSimulator under the reference's method names."""
+    """QAOAQtreeSimulator under the reference's method names, returning the
+    reference's result shape: a one-element float64 array for a graph with
+    edges (qtensor/QAOASimulator.py:27-41,65), 0.0 without edges."""
+    import networkx as nx
     from qtensor_b200.qaoa import QAOAQtreeSimulator
     G, w = golden_graph('cfg2')
     sim = QAOAQtreeSimulator('default')
     for E in (sim.energy_expectation(G, w['gamma'], w['beta']),
               sim.energy_expectation_parallel(G, w['gamma'], w['beta'], n_processes=8),
               sim.energy_expectation_mpi(G, w['gamma'], w['beta'])):
-        assert abs(E - w['energy']) <= TOL * abs(w['energy'])
+        assert isinstance(E, np.ndarray) and E.shape == (1,) and E.dtype == np.float64
+        assert abs(E[0] - w['energy']) <= TOL * abs(w['energy'])
+    empty = nx.empty_graph(5)
+    assert sim.energy_expectation(empty, [0.1], [0.2]) == 0.0
 
 
 def test_composers_agree_and_terms_are_real(cuda_device):
