@@ -174,6 +174,26 @@ int qtb_plan_add_circuit_batch(qtb_plan* plan, int32_t n_qubits, const qtb_gate*
  * is built, which bounds host memory and compile time per circuit.      */
 int qtb_plan_set_max_width(qtb_plan* plan, int32_t max_width, int32_t max_slices);
 
+/* How circuits added afterwards choose their sliced variables when they
+ * reach max_width (results are the same; widths and slice counts differ):
+ *   QTB_SLICE_GREEDY     variables of highest degree, one at a time, until
+ *                        the width drops below max_width (GreedyParvars +
+ *                        SlicesOptimizer, qtensor/optimisation/Greedy.py:78-91,
+ *                        Optimizer.py:109-159); the default;
+ *   QTB_SLICE_TREE_TRIM  TreeTrimSplitter (Optimizer.py:178-224): rounds of
+ *                        int(0.2 x excess width) + 1 variables lying in the
+ *                        most largest elimination cliques;
+ *   QTB_SLICE_LATE       LateParOptimizer (late_parallelisation.py:30-202):
+ *                        each variable sliced at the step of the elimination
+ *                        order that leaves the least width; the order is the
+ *                        contracted prefixes, then the rest.
+ * The order search with trials still runs on the sliced graph for the
+ * greedy and tree-trimming choices.                                       */
+#define QTB_SLICE_GREEDY 0
+#define QTB_SLICE_TREE_TRIM 1
+#define QTB_SLICE_LATE 2
+int qtb_plan_set_slicing(qtb_plan* plan, int32_t method);
+
 /* Elimination-order search for networks added afterwards: 0 (default) keeps
  * the reference's greedy rule (first node of least degree); trials > 0 also
  * runs that many seeded greedy orders with random tie-breaking and keeps

@@ -20,13 +20,14 @@ GATE_M, GATE_H, GATE_Z, GATE_X, GATE_Y, GATE_CX, GATE_CZ = range(7)
 GATE_ZPHASE, GATE_XPHASE, GATE_YPHASE, GATE_ZZ, GATE_T = range(7, 12)
 
 COMPOSER_DEFAULT, COMPOSER_ZZ, COMPOSER_CX = 0, 1, 2
+SLICE_GREEDY, SLICE_TREE_TRIM, SLICE_LATE = 0, 1, 2
 
 # Exported entry points, in the order of include/qtb.h.
 EXPORTS = (
     'qtb_version', 'qtb_init', 'qtb_last_error', 'qtb_bucket_c64',
     'qtb_plan_create', 'qtb_plan_destroy', 'qtb_plan_add_circuit',
     'qtb_plan_add_lightcone', 'qtb_plan_add_lightcones', 'qtb_plan_add_circuit_batch',
-    'qtb_plan_set_max_width',
+    'qtb_plan_set_max_width', 'qtb_plan_set_slicing',
     'qtb_plan_set_order_trials', 'qtb_plan_set_share_lightcones',
     'qtb_plan_n_networks',
     'qtb_plan_network_info', 'qtb_plan_network_peo', 'qtb_plan_check_params',
@@ -117,6 +118,7 @@ def _declare(lib):
         'qtb_plan_add_lightcones': (c.c_int, [P, c.c_int32, P, P, P, c.c_int32, c.c_int32,
                                               c.c_int32, P, c.c_int32, c.POINTER(c.c_int32)]),
         'qtb_plan_set_max_width': (c.c_int, [P, c.c_int32, c.c_int32]),
+        'qtb_plan_set_slicing': (c.c_int, [P, c.c_int32]),
         'qtb_plan_set_order_trials': (c.c_int, [P, c.c_int32]),
         'qtb_plan_set_share_lightcones': (c.c_int, [P, c.c_int32]),
         'qtb_plan_n_networks': (c.c_int, [P, c.POINTER(c.c_int32)]),

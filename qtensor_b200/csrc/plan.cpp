@@ -610,9 +610,275 @@ static double minfill_order(const LineGraph& g, const std::vector<char>& removed
     return cost;
 }
 
+// ------------------------------------------------------ slicing choices
+// The reference's line graph as a multigraph (QtreeTensorNet.get_line_graph,
+// qtensor/optimisation/TensorNet.py:53-58, through qtree buckets2graph): one
+// edge per pair of variables of every tensor and a self-loop for a tensor
+// of one variable, multiplicities kept; eliminating a node adds one more
+// edge between every pair of its neighbours (qtensor/utils.py:77-87).
+// GreedyParvars ranks nodes by the multigraph degree (parallel edges
+// counted, a self-loop twice: Greedy.py:78-91); the greedy order only sees
+// distinct neighbours, kept as bit rows beside the multiplicities.
+struct MultiGraph {
+    int V = 0, W = 0;
+    std::vector<uint32_t> cnt;    // V x V multiplicities, self-loops on the diagonal
+    std::vector<uint64_t> bits;   // V x W distinct neighbours (no self)
+    std::vector<int64_t> mdeg;    // multigraph degree
+    std::vector<char> alive;
+
+    void init(int v, const std::vector<std::vector<int32_t>>& tensors) {
+        V = v;
+        W = (V + 63) / 64;
+        cnt.assign((size_t)V * V, 0);
+        bits.assign((size_t)V * W, 0);
+        mdeg.assign(V, 0);
+        alive.assign(V, 1);
+        for (const auto& t : tensors) {
+            if (t.size() == 1) {
+                ++cnt[(size_t)t[0] * V + t[0]];
+                mdeg[t[0]] += 2;
+            }
+            for (size_t i = 0; i < t.size(); ++i)
+                for (size_t j = i + 1; j < t.size(); ++j) add_edge(t[i], t[j]);
+        }
+    }
+    void add_edge(int a, int b) {
+        ++cnt[(size_t)a * V + b];
+        ++cnt[(size_t)b * V + a];
+        ++mdeg[a];
+        ++mdeg[b];
+        bits[(size_t)a * W + (b >> 6)] |= 1ull << (b & 63);
+        bits[(size_t)b * W + (a >> 6)] |= 1ull << (a & 63);
+    }
+    void neighbours(int x, std::vector<int32_t>* out) const {
+        out->clear();
+        for (int w = 0; w < W; ++w)
+            for (uint64_t m = bits[(size_t)x * W + w]; m; m &= m - 1) out->push_back(w * 64 + __builtin_ctzll(m));
+    }
+    // len(graph[x]): distinct neighbours, x itself included when it has a self-loop
+    int n_neighbors(int x) const {
+        int n = cnt[(size_t)x * V + x] ? 1 : 0;
+        for (int w = 0; w < W; ++w) n += __builtin_popcountll(bits[(size_t)x * W + w]);
+        return n;
+    }
+    void drop(int x, std::vector<int32_t>* nb) {
+        neighbours(x, nb);
+        for (int a : *nb) {
+            mdeg[a] -= cnt[(size_t)a * V + x];
+            cnt[(size_t)a * V + x] = cnt[(size_t)x * V + a] = 0;
+            bits[(size_t)a * W + (x >> 6)] &= ~(1ull << (x & 63));
+        }
+        for (int w = 0; w < W; ++w) bits[(size_t)x * W + w] = 0;
+        cnt[(size_t)x * V + x] = 0;
+        mdeg[x] = 0;
+        alive[x] = 0;
+    }
+    // graph.remove_node (slicing a variable)
+    void remove(int x) {
+        std::vector<int32_t> nb;
+        drop(x, &nb);
+    }
+    // eliminate_node_no_structure
+    void eliminate(int x) {
+        std::vector<int32_t> nb;
+        drop(x, &nb);
+        for (size_t i = 0; i < nb.size(); ++i)
+            for (size_t j = i + 1; j < nb.size(); ++j) add_edge(nb[i], nb[j]);
+    }
+    // GreedyParvars.step: the first node (node order) of largest degree
+    int max_degree_node() const {
+        int best = -1;
+        for (int x = 0; x < V; ++x)
+            if (alive[x] && (best < 0 || mdeg[x] > mdeg[best])) best = x;
+        return best;
+    }
+    // the simple graph of the live nodes, optionally without node `skip`
+    void simple(LineGraph* g, std::vector<char>* removed, int skip = -1) const {
+        g->V = V;
+        g->W = W;
+        g->adj = bits;
+        g->deg.assign(V, 0);
+        removed->assign(V, 0);
+        for (int x = 0; x < V; ++x) (*removed)[x] = alive[x] ? 0 : 1;
+        if (skip >= 0) {
+            (*removed)[skip] = 1;
+            for (int w = 0; w < W; ++w) g->adj[(size_t)skip * W + w] = 0;
+            for (int x = 0; x < V; ++x) g->adj[(size_t)x * W + (skip >> 6)] &= ~(1ull << (skip & 63));
+        }
+        for (int x = 0; x < V; ++x)
+            for (int w = 0; w < W; ++w) g->deg[x] += __builtin_popcountll(g->adj[(size_t)x * W + w]);
+    }
+};
+
+// Widths (neighbour counts at elimination) of `order` on the simple graph g.
+static int order_width(const LineGraph& g, const std::vector<char>& removed, const std::vector<int32_t>& order,
+                       std::vector<int32_t>* degrees) {
+    const int W = g.W;
+    std::vector<uint64_t> adj(g.adj);
+    std::vector<char> gone(removed);
+    degrees->clear();
+    int width = 0;
+    for (int x : order) {
+        if (gone[x]) continue;
+        uint64_t* rx = &adj[(size_t)x * W];
+        std::vector<int32_t> nb;
+        for (int w = 0; w < W; ++w)
+            for (uint64_t m = rx[w]; m; m &= m - 1) nb.push_back(w * 64 + __builtin_ctzll(m));
+        degrees->push_back((int32_t)nb.size());
+        width = std::max(width, (int)nb.size());
+        for (int a : nb) {
+            uint64_t* ra = &adj[(size_t)a * W];
+            for (int w = 0; w < W; ++w) ra[w] |= rx[w];
+            ra[a >> 6] &= ~(1ull << (a & 63));
+            ra[x >> 6] &= ~(1ull << (x & 63));
+        }
+        gone[x] = 1;
+    }
+    return width;
+}
+
+// LateParOptimizer (qtensor/optimisation/late_parallelisation.py:30-202)
+// with one variable per bunch, until the width is at most `target`: from
+// the reference's greedy order, for every step s of the order the graph is
+// contracted up to s, its node of largest multigraph degree sliced
+// (slice_greedy, GreedyParvars) and the rest ordered greedily; the step of
+// least width max(widths of the contracted prefix, widths of the new order)
+// wins (the first one on ties, numpy argmin), its prefix is kept and the
+// search repeats on the sliced graph.  The neighbour count of a prefix step
+// is taken with the +1 of find_slice_at_step (:101).  Steps whose prefix
+// width alone already reaches the best width found are not evaluated (they
+// cannot be chosen).  Returns false when the order runs out first.
+static bool late_slicing(const MultiGraph& g0, int target, int max_vars, std::vector<int32_t>* peo,
+                         std::vector<int32_t>* par, int* final_width) {
+    MultiGraph g = g0;
+    LineGraph lg;
+    std::vector<char> removed;
+    std::vector<int32_t> ordering, path, cand_order, cand_path;
+    g.simple(&lg, &removed);
+    greedy_order(lg, removed, 0, &ordering, &path);
+    peo->clear();
+    par->clear();
+    *final_width = path.empty() ? 0 : *std::max_element(path.begin(), path.end());
+    if (*final_width <= target) {
+        *peo = ordering;
+        return true;
+    }
+    while ((int)par->size() < max_vars) {
+        // find_slice_at_step(ordering, g, 1)
+        MultiGraph work = g;
+        int best_tw = INT_MAX, best_step = -1, best_var = -1, largest = 0;
+        std::vector<int32_t> best_order;
+        for (size_t s = 0; s + 1 < ordering.size(); ++s) {
+            const int node = ordering[s];
+            const int step_tw = work.n_neighbors(node) + 1;
+            if (std::max(largest, step_tw) >= best_tw) break;   // no later step can win
+            const int x = work.max_degree_node();
+            work.simple(&lg, &removed, x);
+            greedy_order(lg, removed, 0, &cand_order, &cand_path);
+            largest = std::max(largest, step_tw);
+            const int tw = std::max(largest, cand_path.empty() ? 0 : *std::max_element(cand_path.begin(), cand_path.end()));
+            if (tw < best_tw) {
+                best_tw = tw;
+                best_step = (int)s;
+                best_var = x;
+                best_order = cand_order;
+            }
+            work.eliminate(node);
+        }
+        if (best_step < 0) return false;
+        for (int s = 0; s < best_step; ++s) {
+            peo->push_back(ordering[s]);
+            g.eliminate(ordering[s]);
+        }
+        g.remove(best_var);
+        par->push_back(best_var);
+        ordering = best_order;
+        *final_width = best_tw;
+        if (best_tw <= target) {
+            peo->insert(peo->end(), ordering.begin(), ordering.end());
+            return true;
+        }
+    }
+    return false;
+}
+
+// Tree trimming (TreeTrimSplitter, qtensor/optimisation/Optimizer.py:178-224):
+// while the greedy width exceeds `target`, remove int(0.2 * excess) + 1
+// variables at once, then reorder.  The variables come from
+// split_graph_by_tree_trimming of the qtree package (github.com/DaniloZZZ/
+// qtree, PyPI qtensor-qtree, version unpinned), which is absent from the
+// reference; this restates the published heuristic (Schutski, Khakhulin,
+// Oseledets, Kolmakov, "Simple heuristics for efficient parallel tensor
+// contraction and quantum circuit simulation", Phys. Rev. A 102, 062614,
+// 2020): one variable at a time, the one lying in the most cliques of the
+// largest size among the elimination cliques (a node with its neighbours
+// when it is eliminated) of the current greedy order, ties to the earliest
+// in that order (the reference relabels nodes by order position first),
+// reordering after each removal.
+static bool tree_trim_slicing(const LineGraph& g0, std::vector<char> removed, int target, int max_vars,
+                              std::vector<int32_t>* order, std::vector<int32_t>* degrees,
+                              std::vector<int32_t>* par) {
+    const int V = g0.V, W = g0.W;
+    LineGraph g = g0;
+    par->clear();
+    greedy_order(g, removed, 0, order, degrees);
+    auto width = [&]() { return degrees->empty() ? 0 : *std::max_element(degrees->begin(), degrees->end()); };
+    std::vector<int64_t> hits(V);
+    std::vector<int32_t> nb;
+    while (width() > target) {
+        const int n_target = (int)((width() - target) * 0.2) + 1;
+        for (int k = 0; k < n_target; ++k) {
+            if ((int)par->size() >= max_vars) return false;
+            // elimination cliques of the current order
+            std::vector<uint64_t> adj(g.adj);
+            std::fill(hits.begin(), hits.end(), 0);
+            std::vector<int32_t> pos(V, INT_MAX);
+            for (size_t i = 0; i < order->size(); ++i) pos[(*order)[i]] = (int32_t)i;
+            const int w = width();
+            std::vector<char> gone(removed);
+            for (int x : *order) {
+                uint64_t* rx = &adj[(size_t)x * W];
+                nb.clear();
+                for (int q = 0; q < W; ++q)
+                    for (uint64_t m = rx[q]; m; m &= m - 1) nb.push_back(q * 64 + __builtin_ctzll(m));
+                if ((int)nb.size() == w) {
+                    ++hits[x];
+                    for (int a : nb) ++hits[a];
+                }
+                for (int a : nb) {
+                    uint64_t* ra = &adj[(size_t)a * W];
+                    for (int q = 0; q < W; ++q) ra[q] |= rx[q];
+                    ra[a >> 6] &= ~(1ull << (a & 63));
+                    ra[x >> 6] &= ~(1ull << (x & 63));
+                }
+                gone[x] = 1;
+            }
+            int best = -1;
+            for (int x = 0; x < V; ++x)
+                if (!removed[x] && hits[x] > 0 &&
+                    (best < 0 || hits[x] > hits[best] || (hits[x] == hits[best] && pos[x] < pos[best])))
+                    best = x;
+            if (best < 0) return false;
+            // remove it from the graph (no fill-in)
+            for (int q = 0; q < W; ++q)
+                for (uint64_t m = g.adj[(size_t)best * W + q]; m; m &= m - 1) {
+                    const int a = q * 64 + __builtin_ctzll(m);
+                    g.adj[(size_t)a * W + (best >> 6)] &= ~(1ull << (best & 63));
+                    --g.deg[a];
+                }
+            for (int q = 0; q < W; ++q) g.adj[(size_t)best * W + q] = 0;
+            g.deg[best] = 0;
+            removed[best] = 1;
+            par->push_back(best);
+            greedy_order(g, removed, 0, order, degrees);
+        }
+    }
+    return true;
+}
+
 int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
                     int32_t simplify_passes, const double* params, int32_t n_params,
-                    int32_t order_trials, int32_t max_width, int32_t max_slices,
+                    int32_t order_trials, int32_t max_width, int32_t max_slices, int32_t slicing,
                     int32_t batch_vars, std::vector<Network>* outs, std::string* err,
                     const std::atomic<bool>* abort) {
     outs->clear();
@@ -702,7 +968,7 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
 
     // ---- line graph (first-appearance node order) and greedy order
     std::vector<int32_t> node_of(n_vars, -1), var_of;
-    std::vector<std::vector<int32_t>> cliques;
+    std::vector<std::vector<int32_t>> cliques, tnodes;   // tnodes: every tensor's nodes (late slicing)
     for (const auto& b : buckets)
         for (int32_t ti : b) {
             std::vector<int32_t> c;
@@ -714,6 +980,7 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
                 }
                 c.push_back(node_of[v]);
             }
+            if (slicing == QTB_SLICE_LATE && !c.empty()) tnodes.push_back(c);
             if (c.size() > 1) cliques.push_back(std::move(c));
         }
     // trial 0: the reference's greedy rule; trials 1..order_trials: seeded
@@ -754,7 +1021,42 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
     // variables that may still be sliced within max_slices
     int slice_budget = 0;
     while (slice_budget < kMaxSlicedVars && (2ll << slice_budget) <= (long long)max_slices) ++slice_budget;
-    while (max_width > 0 && width() >= max_width) {
+    auto out_of_budget = [&](const char* how) {
+        *err = "compile: width " + std::to_string(width()) + " still >= " + std::to_string(max_width) +
+               " after " + how + " slicing of at most " + std::to_string(slice_budget) + " variables (" +
+               std::to_string(1ll << slice_budget) + " slices per circuit)";
+        return QTB_ERR_UNSUPPORTED;
+    };
+    // a width far above the target is out of reach of any slicing within
+    // the budget (the greedy loop below applies the same bound per step)
+    if (max_width > 0 && slicing != QTB_SLICE_GREEDY && width() - max_width + 1 > 2 * slice_budget)
+        return out_of_budget(slicing == QTB_SLICE_LATE ? "late" : "tree-trimming");
+    if (max_width > 0 && width() >= max_width && slicing == QTB_SLICE_TREE_TRIM) {
+        // TreeTrimSplitter's choice of variables, then the order search on
+        // the sliced graph (the reference reorders greedily; with trials the
+        // cheaper candidates compete as for an unsliced circuit)
+        std::vector<char> none(V, 0);
+        line_graph(V, cliques, none, &lg);
+        const bool ok = tree_trim_slicing(lg, none, max_width - 1, slice_budget, &gorder, &gdeg, &par);
+        for (int32_t x : par) removed[x] = 1;
+        if (!ok) return out_of_budget("tree-trimming");
+        if (order_trials > 0) best_order();
+    } else if (max_width > 0 && width() >= max_width && slicing == QTB_SLICE_LATE) {
+        // LateParOptimizer's sliced variables and order (prefix contracted
+        // before each slice, then the greedy order of the sliced rest)
+        MultiGraph mg;
+        mg.init(V, tnodes);
+        int late_width = 0;
+        const bool ok = late_slicing(mg, max_width - 1, slice_budget, &gorder, &par, &late_width);
+        for (int32_t x : par) removed[x] = 1;
+        line_graph(V, cliques, removed, &lg);
+        if (!ok) {
+            greedy_order(lg, removed, 0, &gorder, &gdeg);
+            return out_of_budget("late");
+        }
+        order_width(lg, removed, gorder, &gdeg);
+    }
+    while (max_width > 0 && width() >= max_width && slicing == QTB_SLICE_GREEDY) {
         if (abort && abort->load(std::memory_order_relaxed)) return kCompileAborted;
         // removing one variable lowers the treewidth by at most one, so a
         // width more than twice the remaining budget above the target is
@@ -1598,7 +1900,7 @@ int qtb_plan_add_circuit(qtb_plan* plan, int32_t n_qubits, const qtb_gate* gates
     std::vector<Network> nets;
     std::string err;
     int rc = compile_circuit(n_qubits, gates, n_gates, simplify_passes, params, plan->n_params,
-                             plan->order_trials, plan->max_width, plan->max_slices, 0, &nets, &err);
+                             plan->order_trials, plan->max_width, plan->max_slices, plan->slicing, 0, &nets, &err);
     if (rc) return fail(rc, err);
     std::lock_guard<std::mutex> lock(plan->mu);
     if (net_index) *net_index = (int32_t)plan->nets.size();
@@ -1614,7 +1916,8 @@ int qtb_plan_add_circuit_batch(qtb_plan* plan, int32_t n_qubits, const qtb_gate*
     std::vector<Network> nets;
     std::string err;
     int rc = compile_circuit(n_qubits, gates, n_gates, simplify_passes, params, plan->n_params,
-                             plan->order_trials, plan->max_width, plan->max_slices, batch_vars, &nets, &err);
+                             plan->order_trials, plan->max_width, plan->max_slices, plan->slicing, batch_vars,
+                             &nets, &err);
     if (rc) return fail(rc, err);
     const size_t n_amps = size_t(1) << batch_vars;
     const size_t per_amp = nets.size() / n_amps;
@@ -1727,7 +2030,7 @@ int qtb_plan_add_lightcones(qtb_plan* plan, int32_t n_nodes, const int64_t* indp
         if (!rc)
             rc = compile_circuit(nq, gates.data(), (int32_t)gates.size(), composer == 0 ? 2 : 0,
                                  params, plan->n_params, plan->order_trials, plan->max_width,
-                                 plan->max_slices, 0, &nets[i], &errs[i], &failed);
+                                 plan->max_slices, plan->slicing, 0, &nets[i], &errs[i], &failed);
         codes[i] = rc;
         if (rc && rc != kCompileAborted) failed.store(true, std::memory_order_relaxed);
     });
@@ -1750,6 +2053,13 @@ int qtb_plan_set_max_width(qtb_plan* plan, int32_t max_width, int32_t max_slices
         return fail(QTB_ERR_ARG, "plan_set_max_width: bad arguments");
     plan->max_width = max_width;
     plan->max_slices = max_slices;
+    return QTB_OK;
+}
+
+int qtb_plan_set_slicing(qtb_plan* plan, int32_t method) {
+    if (!plan || method < QTB_SLICE_GREEDY || method > QTB_SLICE_LATE)
+        return fail(QTB_ERR_ARG, "plan_set_slicing: unknown method");
+    plan->slicing = method;
     return QTB_OK;
 }
 

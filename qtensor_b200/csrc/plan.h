@@ -170,6 +170,7 @@ struct qtb_plan {
     bool share_lightcones = true;   // isomorphic lightcones share one compile
     int32_t max_width = 0;      // slice circuits whose width reaches this (0 = never)
     int32_t max_slices = 256;   // networks one sliced circuit may become
+    int32_t slicing = QTB_SLICE_GREEDY;   // how sliced variables are chosen
     int32_t n_groups = 0;       // circuits added (networks of a circuit share a group)
     std::vector<qtb::Network> nets;
     // global gate table, built from the networks' local entries
@@ -202,7 +203,7 @@ void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int compile_circuit(int32_t n_qubits, const qtb_gate* gates, int32_t n_gates,
                     int32_t simplify_passes, const double* params, int32_t n_params,
-                    int32_t order_trials, int32_t max_width, int32_t max_slices,
+                    int32_t order_trials, int32_t max_width, int32_t max_slices, int32_t slicing,
                     int32_t batch_vars, std::vector<Network>* outs, std::string* err,
                     const std::atomic<bool>* abort = nullptr);
 // compile_circuit's result when `abort` was raised while it ran.

@@ -165,12 +165,14 @@ class QAOAEnergyEngine:
     max_width / max_slices: a circuit whose width reaches ``max_width`` is
     sliced into at most ``max_slices`` networks (FeynmanSimulator's scheme,
     qtensor/FeynmanSimulator.py:49-84); the default 29 slices only what one
-    B200's memory cannot hold unsliced.
+    B200's memory cannot hold unsliced.  slicing: ``'greedy'``
+    (GreedyParvars), ``'tree_trim'`` (TreeTrimSplitter) or ``'late'``
+    (LateParOptimizer) choice of the sliced variables.
     """
 
     def __init__(self, composer='default', ordering='native', device=None, threads=0,
                  cache_size=16, order_trials=16, autotune=True, max_width=29,
-                 max_slices=1024):
+                 max_slices=1024, slicing='greedy'):
         _require_cuda()
         if ordering not in ('native', 'reference'):
             raise ValueError('ordering must be "native" or "reference"')
@@ -184,6 +186,7 @@ class QAOAEnergyEngine:
         self.autotune = autotune
         self.max_width = max_width
         self.max_slices = max_slices
+        self.slicing = slicing
         self._cache = {}
         self._by_id = {}        # id(G) -> (weakref, nodes, p, key, edge count)
         self._edge_digests = {}  # id(edge subset) -> (subset, tuple, digest, length)
@@ -216,6 +219,7 @@ class QAOAEnergyEngine:
         plan = NetworkPlan(2 * p)
         plan.set_order_trials(self.order_trials)
         plan.set_max_width(self.max_width, self.max_slices)
+        plan.set_slicing(self.slicing)
         if self.ordering == 'native':
             csr = graph_csr(G)
             index = {v: i for i, v in enumerate(csr[0])}
@@ -247,7 +251,7 @@ class QAOAEnergyEngine:
             if ref() is G and hp == p and n == len(G):
                 return key
         key = graph_key(G, p, self.composer, self.ordering, self.order_trials,
-                        (self.max_width, self.max_slices))
+                        (self.max_width, self.max_slices, self.slicing))
         try:
             self._by_id[id(G)] = (weakref.ref(G), len(G), p, key, G.number_of_edges())
         except TypeError:

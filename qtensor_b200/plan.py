@@ -43,6 +43,14 @@ class NetworkPlan:
         need more than ``max_slices`` networks fails to compile."""
         check(self._lib.qtb_plan_set_max_width(self._h, int(max_width), int(max_slices)))
 
+    def set_slicing(self, method):
+        """How circuits added afterwards choose sliced variables: ``'greedy'``
+        (GreedyParvars, the default), ``'tree_trim'`` (TreeTrimSplitter) or
+        ``'late'`` (LateParOptimizer)."""
+        code = {'greedy': _lib.SLICE_GREEDY, 'tree_trim': _lib.SLICE_TREE_TRIM,
+                'late': _lib.SLICE_LATE}[method]
+        check(self._lib.qtb_plan_set_slicing(self._h, code))
+
     def groups(self):
         """Circuit (group) of every network."""
         return np.array([self.info(i)['group'] for i in range(len(self))], dtype=np.int64)

@@ -72,9 +72,12 @@ class QtreeSimulator:
     max_tw: like the reference, a ``ValueError`` when the contraction width
     exceeds it (before slicing); max_width / max_slices: circuits whose width
     reaches max_width are sliced into at most max_slices networks per
-    amplitude; order_trials: extra randomized greedy orders per network."""
+    amplitude; slicing: how the sliced variables are chosen (``'greedy'``,
+    ``'tree_trim'`` or ``'late'``, see ``NetworkPlan.set_slicing``);
+    order_trials: extra randomized greedy orders per network."""
 
-    def __init__(self, device=None, max_tw=None, max_width=26, max_slices=256, order_trials=8):
+    def __init__(self, device=None, max_tw=None, max_width=26, max_slices=256, order_trials=8,
+                 slicing='greedy'):
         if not torch.cuda.is_available():
             raise RuntimeError('qtensor_b200 needs a CUDA device; there is no CPU fallback')
         self.device = torch.device('cuda', torch.cuda.current_device() if device is None else device)
@@ -82,6 +85,7 @@ class QtreeSimulator:
         self.max_width = max_width
         self.max_slices = max_slices
         self.order_trials = order_trials
+        self.slicing = slicing
         _lib.check(_lib.lib().qtb_init(self.device.index))
         self.plan = None
 
@@ -97,6 +101,7 @@ class QtreeSimulator:
         plan = NetworkPlan(len(params))
         plan.set_order_trials(self.order_trials)
         plan.set_max_width(self.max_width, self.max_slices)
+        plan.set_slicing(self.slicing)
         first, group0 = plan.add_circuit_batch(n_qubits, gates, params, batch_vars)
         if self.max_tw is not None:
             width = max(i['treewidth'] for i in plan.infos())
@@ -139,12 +144,62 @@ class QtreeSimulator:
         return self.simulate_batch(qc, batch_vars=0, peo=peo)
 
 
+class SlicesOptimizer:
+    """Choice of parallel (sliced) variables of ``FeynmanSimulator``
+    (qtensor/optimisation/Optimizer.py:90-159): variables of highest degree
+    (GreedyParvars) until the width drops below ``max_tw - tw_bias``.  Only
+    the slicing parameters are kept: the plan compiler does the work."""
+    method = 'greedy'
+
+    def __init__(self, tw_bias=2, max_tw=None, **kwargs):
+        self.tw_bias = tw_bias
+        self.max_tw = kwargs.get('target_tw') or max_tw
+
+    def max_width(self, default_max_tw):
+        """The plan compiler's ``max_width``: slice while width >= it."""
+        max_tw = default_max_tw if self.max_tw is None else self.max_tw
+        return max(1, int(max_tw) - int(self.tw_bias))
+
+
+class TreeTrimSplitter(SlicesOptimizer):
+    """TreeTrimSplitter (qtensor/optimisation/Optimizer.py:178-224): rounds of
+    int(0.2 x excess) + 1 variables from the largest elimination cliques,
+    until the width is at most ``max_tw - tw_bias``."""
+    method = 'tree_trim'
+
+    def max_width(self, default_max_tw):
+        return super().max_width(default_max_tw) + 1
+
+
+class LateParOptimizer:
+    """LateParOptimizer (qtensor/optimisation/late_parallelisation.py:30-202)
+    with one variable per bunch: each variable is sliced at the step of the
+    elimination order that leaves the least width, until the width is at
+    most ``target_tw``."""
+    method = 'late'
+
+    def __init__(self, target_tw=None, par_vars=None, p_bunch=None, n_bunches=None,
+                 ordering_algo='greedy', slicing_algo='greedy'):
+        if ordering_algo != 'greedy' or slicing_algo != 'greedy':
+            raise ValueError('only the greedy ordering and slicing algorithms are supported')
+        if par_vars is not None or n_bunches is not None:
+            raise NotImplementedError('a fixed number of sliced variables is not supported; give target_tw')
+        self.target_tw = target_tw
+
+    def max_width(self, default_max_tw):
+        target = default_max_tw if self.target_tw is None else self.target_tw
+        return max(1, int(target) + 1)
+
+
 class FeynmanSimulator(QtreeSimulator):
     """``FeynmanSimulator.simulate`` / ``simulate_batch_adaptive``
     (qtensor/FeynmanSimulator.py:27-100): the circuit is sliced over parallel
     variables, chosen greedily by degree until its width drops below
     ``max_tw - tw_bias`` (``SlicesOptimizer``, qtensor/optimisation/
     Optimizer.py:88-160), and the amplitudes of all 2^k paths are summed.
+    Assigning ``sim.optimizer = TreeTrimSplitter(...)`` or
+    ``LateParOptimizer(target_tw=...)`` selects those choices instead, as
+    the reference's tests do (qtensor/tests/test_qaoa_energy.py:116-117).
     Here every path is one network of a single launch, so ``pool_type`` and
     ``n_processes`` have nothing to do.  ``max_tw`` defaults, like the
     reference's memory rule, to log2 of the device's free bytes over the
@@ -154,6 +209,7 @@ class FeynmanSimulator(QtreeSimulator):
                  **kwargs):
         super().__init__(*args, max_slices=max_slices, **kwargs)
         self.slice_max_tw = max_tw
+        self.optimizer = None
         self.pool_type = pool_type
         self.n_processes = 2 if n_processes is None else n_processes
 
@@ -168,5 +224,10 @@ class FeynmanSimulator(QtreeSimulator):
         return self.simulate_batch_adaptive(qc, batch_vars, tw_bias=tw_bias)
 
     def simulate_batch_adaptive(self, qc, batch_vars=0, tw_bias=2):
-        self.max_width = self._target_width(tw_bias)
+        if self.optimizer is None:
+            self.max_width = self._target_width(tw_bias)
+            self.slicing = 'greedy'
+        else:
+            self.max_width = self.optimizer.max_width(self._target_width(0))
+            self.slicing = self.optimizer.method
         return self.simulate_batch(qc, batch_vars=batch_vars)

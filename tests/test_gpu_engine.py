@@ -111,6 +111,36 @@ def test_engine_sliced(cuda_device, name, max_width):
     _check(eng, name)
 
 
+@pytest.mark.parametrize('slicing', ['tree_trim', 'late'])
+@pytest.mark.parametrize('name,max_width', [('cfg2', 9), ('cfg4', 15)])
+def test_engine_sliced_by_tree_trimming_and_late_slicing(cuda_device, name, max_width, slicing):
+    """The TreeTrimSplitter and LateParOptimizer choices of sliced variables
+    give the reference's edge terms and energy on the device."""
+    eng = _engine(max_width=max_width, slicing=slicing)
+    G, w = golden_graph(name)
+    cg = eng.compile(G, len(w['gamma']), w['gamma'], w['beta'])
+    assert cg.n_networks > cg.n_edges
+    _check(eng, name)
+
+
+def test_feynman_qaoa_with_tree_trim_splitter(cuda_device):
+    """The reference's test_qaoa_energy_feynman (qtensor/tests/
+    test_qaoa_energy.py:109-121): QtreeQAOAComposer on a 3-regular N=10
+    graph at p=3, sliced by TreeTrimSplitter(max_tw=13, tw_bias=0) and by a
+    tighter target, gives the plain energy; the oracle port agrees."""
+    import qtensor_port as port
+    G = graphs.regular(10, seed=1)
+    gamma, beta = [np.pi / 3] * 3, [np.pi / 2] * 3
+    plain = _engine(composer='cx', max_width=0).energy_expectation(G, gamma, beta)
+    ref = float(port.energy_expectation(G, gamma, beta, 'cx')[0])
+    assert abs(plain - ref) <= TOL * abs(ref)
+    for target in (13, 8):
+        eng = _engine(composer='cx', max_width=target + 1, slicing='tree_trim')
+        assert abs(eng.energy_expectation(G, gamma, beta) - plain) <= TOL * abs(plain)
+        eng = _engine(composer='cx', max_width=target + 1, slicing='late')
+        assert abs(eng.energy_expectation(G, gamma, beta) - plain) <= TOL * abs(plain)
+
+
 @pytest.mark.parametrize('name,max_width', [('cfg1_default', 24), ('cfg2', 24), ('cfg4', 24),
                                             ('cfg2', 9)])
 def test_plain_path_matches_batched_and_reference(cuda_device, name, max_width):
