@@ -20,7 +20,15 @@ fp64 compensated reduction to the energy.
   ``energy_expectation_parallel`` with its NumpyBackend, complex128 einsum)
   on all host cores, rank 0 only.
 Multi-GPU (torchrun): every rank contracts its own graph (weak scaling); no
-collective on the data path.
+collective on the data path.  ``--shard`` instead shards one Erdos-Renyi
+graph's edges over the ranks with one NCCL all-reduce per energy (strong
+scaling, its own JSON line).
+
+Extra legs on one GPU (rank 0): the reference greedy order, 3-regular N=256
+p=4 with its error against the complex128 fixture, the recorded reference
+driver's backend calls replayed into the drop-in backend, the plain
+per-bucket path, the serving stream, and (``--serving-saturate N``) the
+serving workload offered above the server's capacity.
 """
 import argparse
 import json
@@ -63,6 +71,22 @@ def parse():
                     help='requests of the serving run (0 skips it)')
     ap.add_argument('--serving-rate', type=float, default=20.0,
                     help='Poisson arrival rate of the serving run, requests/s')
+    ap.add_argument('--serving-saturate', type=int, default=0,
+                    help='requests of an extra serving run offered faster than the server '
+                         'completes them (0 skips it; the stated stream is 10000)')
+    ap.add_argument('--serving-saturate-rate', type=float, default=2000.0,
+                    help='arrival rate of the saturation run, requests/s')
+    ap.add_argument('--cfg4-steps', type=int, default=10,
+                    help='steps of the 3-regular N=256 p=4 leg (0 skips it)')
+    ap.add_argument('--reference-order-steps', type=int, default=10,
+                    help='steps of the leg with the reference greedy order (0 skips it)')
+    ap.add_argument('--no-dropin', action='store_true',
+                    help="skip the replay of the reference driver's recorded backend calls")
+    ap.add_argument('--shard', action='store_true',
+                    help='under torchrun: shard one graph\'s edges over the ranks (one NCCL '
+                         'all-reduce per energy) instead of one graph per rank')
+    ap.add_argument('--shard-nodes', type=int, default=400,
+                    help='Erdos-Renyi graph size of the sharded mode (p=3)')
     return ap.parse_args()
 
 
@@ -239,6 +263,73 @@ def serving_requests(n, seed=0):
     return out
 
 
+# Contraction work a serving request may bring (algorithmic bytes): about
+# two seconds of the wide-network executor; the one request of the 128-request
+# stream above it (Erdos-Renyi N=73 p=4, 72 TB) would hold the GPU for a minute.
+SERVING_MAX_REQUEST_BYTES = 4e12
+
+
+def _pct(values, q):
+    return float(np.percentile(values, q)) if len(values) else None
+
+
+def _rejections(results):
+    """Failed requests by cause: lightcones too wide for any exact
+    contraction within the slice budget, over the work budget, other."""
+    from qtensor_b200._lib import QtbError
+    from qtensor_b200.serve import RequestTooLarge
+    out = {'too_wide': 0, 'over_work_budget': 0, 'other': 0}
+    for r in results:
+        if isinstance(r, RequestTooLarge):
+            out['over_work_budget'] += 1
+        elif isinstance(r, QtbError) and 'width' in str(r):
+            out['too_wide'] += 1
+        elif isinstance(r, Exception):
+            out['other'] += 1
+    return out
+
+
+def summarize_serving(results, wall):
+    ok = [r for r in results if not isinstance(r, Exception)]
+    lat = np.array([r.latency for r in ok]) * 1e3
+    edges = sum(r.edges for r in ok)
+    out = {'completed': len(ok), 'rejected': len(results) - len(ok),
+           'rejected_by_cause': _rejections(results),
+           'p50_ms': _pct(lat, 50), 'p95_ms': _pct(lat, 95), 'p99_ms': _pct(lat, 99),
+           'edge_terms_per_s': edges / wall if wall > 0 else None, 'wall_s': wall}
+    # where the median request's time went
+    for name in ('compile_s', 'wait_s', 'gpu_s'):
+        out['p50_' + name[:-2] + '_ms'] = _pct(np.array([getattr(r, name) for r in ok]) * 1e3, 50)
+    return out
+
+
+def run_serving_saturated(n_requests, rate, device_index):
+    """The serving workload offered faster than the server completes it
+    (Poisson arrivals at ``rate``, far above its capacity): the edge terms/s
+    are then the server's sustained throughput, not the arrival rate."""
+    from qtensor_b200.serve import QAOAServer
+    reqs = serving_requests(n_requests, seed=2)
+    gaps = np.random.default_rng(3).exponential(1.0 / rate, size=len(reqs))
+    with QAOAServer(device=device_index, n_streams=8, compile_workers=4,
+                    max_request_bytes=SERVING_MAX_REQUEST_BYTES) as srv:
+        t0 = time.perf_counter()
+        futs = []
+        for r, gap in zip(reqs, gaps):
+            time.sleep(gap)
+            futs.append(srv.submit(*r))
+        out = []
+        for f in futs:
+            try:
+                out.append(f.result(timeout=3600))
+            except Exception as exc:     # noqa: BLE001 - rejected (too wide, over budget)
+                out.append(exc)
+        wall = time.perf_counter() - t0
+    res = summarize_serving(out, wall)
+    res['workload'] = ('{} requests of the serving distribution (seed 2), Poisson arrivals at {} req/s '
+                       '(seed 3); 8 streams, 4 compile workers').format(len(reqs), rate)
+    return res
+
+
 def run_serving(n_requests, rate, device_index, plain_budget_s=20.0):
     """Poisson stream through the continuous-batching server; the same
     stream through a FIFO queue (one compile worker, one stream); the same
@@ -251,21 +342,9 @@ def run_serving(n_requests, rate, device_index, plain_budget_s=20.0):
     reqs = serving_requests(n_requests)
     rng = np.random.default_rng(1)
     gaps = rng.exponential(1.0 / rate, size=len(reqs))
-
-    def pct(values, q):
-        return float(np.percentile(values, q)) if len(values) else None
-
-    def summarize(results, wall):
-        ok = [r for r in results if not isinstance(r, Exception)]
-        lat = np.array([r.latency for r in ok]) * 1e3
-        edges = sum(r.edges for r in ok)
-        out = {'completed': len(ok), 'rejected': len(results) - len(ok),
-               'p50_ms': pct(lat, 50), 'p95_ms': pct(lat, 95), 'p99_ms': pct(lat, 99),
-               'edge_terms_per_s': edges / wall if wall > 0 else None, 'wall_s': wall}
-        # where the median request's time went
-        for name in ('compile_s', 'wait_s', 'gpu_s'):
-            out['p50_' + name[:-2] + '_ms'] = pct(np.array([getattr(r, name) for r in ok]) * 1e3, 50)
-        return out
+    pct = _pct
+    summarize = summarize_serving
+    budget = SERVING_MAX_REQUEST_BYTES
 
     def collect(futs):
         out = []
@@ -285,13 +364,13 @@ def run_serving(n_requests, rate, device_index, plain_budget_s=20.0):
         out = collect(futs)
         return out, time.perf_counter() - t0
 
-    with QAOAServer(device=device_index, n_streams=4) as srv:
+    with QAOAServer(device=device_index, n_streams=4, max_request_bytes=budget) as srv:
         stream, wall_stream = poisson(srv)
     # the same arrivals through a plain FIFO queue: one compile worker, one
     # request on the GPU at a time
-    with QAOAServer(device=device_index, n_streams=1, compile_workers=1) as srv:
+    with QAOAServer(device=device_index, n_streams=1, compile_workers=1, max_request_bytes=budget) as srv:
         fifo, wall_fifo = poisson(srv)
-    with QAOAServer(device=device_index, n_streams=1, compile_workers=1) as srv:
+    with QAOAServer(device=device_index, n_streams=1, compile_workers=1, max_request_bytes=budget) as srv:
         t0 = time.perf_counter()
         alone = []
         for r in reqs:
@@ -299,7 +378,7 @@ def run_serving(n_requests, rate, device_index, plain_budget_s=20.0):
         wall_alone = time.perf_counter() - t0
 
     # the plain backend, same compile settings as the server, one request at a time
-    eng = QAOAEnergyEngine(device=device_index, max_width=22, max_slices=256, order_trials=8,
+    eng = QAOAEnergyEngine(device=device_index, max_width=29, max_slices=1024, order_trials=8,
                            cache_size=1)
     plain_lat, plain_edges, plain_err, n_plain = [], 0, 0.0, 0
     t0 = time.perf_counter()
@@ -328,8 +407,8 @@ def run_serving(n_requests, rate, device_index, plain_budget_s=20.0):
         return a.energy == b.energy
     return {'workload': '{} requests: 3-regular or Erdos-Renyi (mean degree 3), N U[16,500], '
                         'p U[1,4], angles U[0,pi) (seed 0); Poisson arrivals at {} req/s '
-                        '(seed 1); slicing from width 22, at most 256 slices per edge'.format(
-                            len(reqs), rate),
+                        '(seed 1); slicing from width 29, at most 1024 slices per edge, at most '
+                        '{:.0e} algorithmic bytes per request'.format(len(reqs), rate, budget),
             'continuous_batching': summarize(stream, wall_stream),
             'fifo_queue': summarize(fifo, wall_fifo),
             'batched_one_at_a_time': summarize(alone, wall_alone),
@@ -449,6 +528,181 @@ def profiled_traffic():
         return None
 
 
+def device_steps(eng, cg, G, p, angle_sets, flush, stream, warmup, steps):
+    """Device-resident steps of a compiled graph: per step, the step's
+    angles are checked on the host against the plan's angle-dependent
+    simplifier decisions (qtb_plan_check_params; a plan that no longer holds
+    is recompiled before the step, outside the events), copied device to
+    device into the plan's angle buffer, and one captured contraction graph
+    is replayed; CUDA events around each step, L2 flushed between steps.
+    Returns (per-step ms, the compiled graph in use, angle-check record)."""
+    import torch
+    dev = cg.params.device
+    params_dev = [torch.from_numpy(a).to(dev) for a in angle_sets]
+    checks = {'steps_checked': 0, 'recompiled': 0}
+
+    def ready(i):
+        nonlocal cg
+        checks['steps_checked'] += 1
+        if cg.angle_checks and not cg.plan.params_valid(angle_sets[i]):
+            cg = eng.compile(G, p, angle_sets[i][:p], angle_sets[i][p:])
+            checks['recompiled'] += 1
+        return cg.device_graph()
+
+    for i in range(warmup):
+        graph = ready(i)
+        cg.params.copy_(params_dev[i])
+        graph.replay()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for i in range(steps):
+        graph = ready(warmup + i)
+        flush.fill_(float(i))
+        starts[i].record(stream)
+        cg.params.copy_(params_dev[warmup + i])
+        graph.replay()
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in zip(starts, ends)], cg, checks
+
+
+def run_cfg4(device_index, flush, steps, warmup=3):
+    """3-regular N=256 p=4 (seed 0, 384 edge terms): compile, error of every
+    edge term against the complex128 reference fixture, device-resident
+    edge terms/s, and how the networks split between the shared-memory
+    executor (K3) and the wide waves (K4)."""
+    import torch
+    from qtensor_b200.engine import QAOAEnergyEngine
+    with open(os.path.join(ROOT, 'tests', 'golden', 'qaoa_reference.json')) as f:
+        w = json.load(f)['workloads']['cfg4']
+    G = graphs.regular(256)
+    assert [list(e) for e in G.edges()] == w['edges']
+    eng = QAOAEnergyEngine(device=device_index)
+    t0 = time.perf_counter()
+    cg = eng.compile(G, 4, w['gamma'], w['beta'])
+    compile_s = time.perf_counter() - t0
+    terms = eng.edge_terms(G, w['gamma'], w['beta'])
+    ref = np.array([complex(*t) for t in w['terms']])
+    E = eng.energy_expectation(G, w['gamma'], w['beta'])
+    angle_sets = [np.concatenate(graphs.angles(4, seed=400 + i)) for i in range(warmup + steps)]
+    stream = torch.cuda.current_stream()
+    step_ms, cg, checks = device_steps(eng, cg, G, 4, angle_sets, flush, stream, warmup, steps)
+    ms = sum(step_ms) / steps
+    stats = cg.stats()
+    cfg = cg.plan.last_launch_config()
+    wave_nets = sum(c[0] for c in cfg if c[3] & 4)
+    return {'workload': '3-regular N=256 (seed 0), p=4, default composer, native order; '
+                        '384 edge-term networks per step; no slicing needed (widths below 29)',
+            'edge_terms_per_s': stats['edges'] / (ms / 1e3), 'ms_per_step': ms, 'steps': steps,
+            'compile_s': compile_s, 'width_max': stats['width_max'], 'networks': stats['networks'],
+            'alg_bytes_per_step': stats['alg_bytes'],
+            'alg_gbs_per_step_time': stats['alg_bytes'] / (ms / 1e3) / 1e9,
+            'networks_shared_memory_executor': stats['networks'] - wave_nets,
+            'networks_wide_waves': wave_nets,
+            'launch_classes': [{'networks': c[0], 'threads': c[1], 'smem_bytes': c[2], 'flags': c[3]}
+                               for c in cfg],
+            'max_abs_error_vs_oracle': float(np.max(np.abs(terms - ref))),
+            'energy_rel_error': abs(E - w['energy']) / abs(w['energy']),
+            'angle_checks': checks}
+
+
+def run_reference_order(G, p, device_index, flush, steps, warmup=3):
+    """The headline workload with QTensor's own lightcone numbering and greedy
+    elimination order (ordering='reference'), so that the order search's
+    share of the speed-up is visible."""
+    import torch
+    from qtensor_b200.engine import QAOAEnergyEngine
+    eng = QAOAEnergyEngine(ordering='reference', device=device_index)
+    g0, b0 = graphs.angles(p, seed=0)
+    t0 = time.perf_counter()
+    cg = eng.compile(G, p, g0, b0)
+    compile_s = time.perf_counter() - t0
+    angle_sets = [np.concatenate(graphs.angles(p, seed=100 + i)) for i in range(warmup + steps)]
+    step_ms, cg, checks = device_steps(eng, cg, G, p, angle_sets, flush, torch.cuda.current_stream(),
+                                       warmup, steps)
+    ms = sum(step_ms) / steps
+    stats = cg.stats()
+    return {'edge_terms_per_s': stats['edges'] / (ms / 1e3), 'ms_per_step': ms, 'steps': steps,
+            'compile_s': compile_s, 'width_max': stats['width_max'],
+            'alg_bytes_per_step': stats['alg_bytes'], 'angle_checks': checks}
+
+
+def run_dropin(device_index):
+    """The drop-in path as the reference drives it: every backend call the
+    reference's QAOAQtreeSimulator made with its NumpyBackend (recorded in
+    tests/golden/dropin_trace.json) replayed into B200Backend -- one
+    qtb_bucket_c64 launch per process_bucket -- timed per edge term."""
+    import torch
+    import dropin_replay
+    from qtensor_b200.backend import B200Backend
+    be = B200Backend(device=device_index)
+    out = {}
+    for name, w in dropin_replay.load().items():
+        inputs = [dropin_replay.edge_inputs(rec) for rec in w['edges']]
+        dropin_replay.replay_edge(be, w['edges'][0], inputs[0])     # warm-up
+        torch.cuda.synchronize()
+        err = 0.0
+        t0 = time.perf_counter()
+        for rec, inp in zip(w['edges'], inputs):
+            amp, _ = dropin_replay.replay_edge(be, rec, inp)
+            err = max(err, float(np.max(np.abs(amp - [complex(*z) for z in rec['amplitude']]))))
+        dt = time.perf_counter() - t0
+        calls = sum(len(r['calls']) for r in w['edges'])
+        out[name] = {'edges': len(w['edges']), 'process_bucket_calls': calls,
+                     'edge_terms_per_s': len(w['edges']) / dt, 'us_per_process_bucket': 1e6 * dt / calls,
+                     'max_abs_error_vs_recorded': err}
+    out['what'] = ("the reference QAOAQtreeSimulator's recorded get_sliced_buckets / process_bucket / "
+                   'get_result_data calls replayed into B200Backend (host Python per call, one bucket '
+                   'kernel launch per process_bucket, result read back per edge)')
+    return out
+
+
+def run_sharded(args, dev, local, rank, world):
+    """One Erdos-Renyi graph (mean degree 3, p=3) sharded over the ranks by
+    longest processing time on the plans' flops: each rank contracts its
+    share and one NCCL all-reduce of fp64 shares gives every rank the
+    energy (DistributedQAOAEnergy).  Timed per energy with CUDA events on
+    every rank, max over ranks."""
+    import torch
+    import torch.distributed as dist
+    from qtensor_b200.distributed import DistributedQAOAEnergy
+    G = graphs.erdos_renyi(args.shard_nodes, seed=24323709)
+    p = 3
+    denergy = DistributedQAOAEnergy(lpt=True, device=local)
+    for i in range(args.warmup):
+        denergy.energy_expectation(G, *graphs.angles(p, seed=500 + i))
+    torch.cuda.synchronize()
+    dist.barrier()
+    stream = torch.cuda.current_stream(dev)
+    total_ms, energies = 0.0, []
+    for i in range(args.steps):
+        g, b = graphs.angles(p, seed=600 + i)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        energies.append(denergy.energy_expectation(G, g, b))
+        e.record(stream)
+        e.synchronize()
+        total_ms += s.elapsed_time(e)
+    dist.barrier()
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = t.item() / args.steps
+    n_edges = G.number_of_edges()
+    if rank == 0:
+        print(json.dumps({
+            'metric': 'QAOA edge terms/s (Erdos-Renyi N={} p=3, edges sharded over ranks)'.format(args.shard_nodes),
+            'value': n_edges / (ms / 1e3), 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'strong',
+            'vs_baseline': None, 'dtype': 'c64', 'data': 'synthetic', 'impl': 'b200', 'mode': 'shard',
+            'config': {'workload': 'one Erdos-Renyi graph N={} (seed 24323709), p=3, {} edges; LPT '
+                                   'shards by plan flops; one NCCL all-reduce per energy'.format(
+                                       args.shard_nodes, n_edges)},
+            'energy_first_step': energies[0] if energies else None}), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def run_b200(args):
     rank, world, local = dist_env()
     G = graphs.regular(args.nodes, seed=rank)
@@ -469,16 +723,18 @@ def run_b200(args):
     import torch
     torch.cuda.set_device(local)
     dev = torch.device('cuda', local)
-    # nvidia-smi takes a moment to start; launch it before the compile so
-    # its samples cover warm-up and the timed steps
-    clocks = ClockSampler(local)
-    clocks.start()
     pg = None
     if world > 1:
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group('nccl', timeout=timedelta(seconds=120), device_id=dev)
         pg = dist
+        if args.shard:
+            return run_sharded(args, dev, local, rank, world)
+    # nvidia-smi takes a moment to start; launch it before the compile so
+    # its samples cover warm-up and the timed steps
+    clocks = ClockSampler(local)
+    clocks.start()
 
     from qtensor_b200.engine import QAOAEnergyEngine
     eng = QAOAEnergyEngine(composer='default', ordering='native', device=local)
@@ -496,32 +752,17 @@ def run_b200(args):
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     angle_sets = [np.concatenate(graphs.angles(p, seed=100 + i)) for i in range(args.warmup + args.steps)]
-    params_dev = [torch.from_numpy(a).to(dev) for a in angle_sets]
 
     def barrier():
         torch.cuda.synchronize()
         if pg:
             pg.barrier()
 
-    # ---- device-resident steps (clock samples cover warm-up and timed steps):
-    # a step = the step's angles copied (device to device) into the plan's
-    # angle buffer + one replay of the captured contraction graph
-    graph = cg.device_graph()
-    for i in range(args.warmup):
-        cg.params.copy_(params_dev[i])
-        graph.replay()
+    # ---- device-resident steps (clock samples cover warm-up and timed steps)
     barrier()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    step_ms, cg, angle_checks = device_steps(eng, cg, G, p, angle_sets, flush, stream, args.warmup,
+                                             args.steps)
     barrier()
-    for i in range(args.steps):
-        flush.fill_(float(i))
-        starts[i].record(stream)
-        cg.params.copy_(params_dev[args.warmup + i])
-        graph.replay()
-        ends[i].record(stream)
-    barrier()
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     # the executor alone: external timing events captured around the class
     # launches (fork to join) inside a graph, replayed once per step
     ev_a = torch.cuda.Event(enable_timing=True, external=True)
@@ -533,6 +774,7 @@ def run_b200(args):
         ev_b.record()
     n_classes = len(cg.plan.last_launch_config())
     kernel_ms = 0.0
+    params_dev = [torch.from_numpy(a).to(dev) for a in angle_sets]
     for i in range(args.steps):
         flush.fill_(float(i))
         cg.params.copy_(params_dev[args.warmup + i])
@@ -581,10 +823,18 @@ def run_b200(args):
     plain_ms_step = sum(plain_ms) / plain_steps if plain_steps else float('nan')
 
     errors = oracle_error(eng, G, p) if rank == 0 else None
-    plain_widths = plain_width_classes(local) if rank == 0 and args.plain_steps > 0 else None
+    extra = rank == 0 and world == 1
+    plain_widths = plain_width_classes(local) if extra and args.plain_steps > 0 else None
+    cfg4 = run_cfg4(local, flush, args.cfg4_steps) if extra and args.cfg4_steps > 0 else None
+    ref_order = (run_reference_order(G, p, local, flush, args.reference_order_steps)
+                 if extra and args.reference_order_steps > 0 else None)
+    dropin = run_dropin(local) if extra and not args.no_dropin else None
     serving = None
-    if rank == 0 and world == 1 and args.serving_requests > 0:
+    if extra and args.serving_requests > 0:
         serving = run_serving(args.serving_requests, args.serving_rate, local)
+    if extra and args.serving_saturate > 0:
+        serving = dict(serving or {})
+        serving['saturated'] = run_serving_saturated(args.serving_saturate, args.serving_saturate_rate, local)
 
     total_ms = sum(step_ms)
     e2e_total = sum(e2e_ms)
@@ -601,6 +851,8 @@ def run_b200(args):
     launches_per_step = kernel_launches / args.steps
     peak, peak_kind = measured_peak_hbm()
     achieved = stats['alg_bytes'] / (kernel_step_ms / 1e3) / 1e9
+    cold_e2e_s = compile_s + first_call_s
+    cold_rate = stats['edges'] / cold_e2e_s
     if rank == 0:
         line = {
             'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world,
@@ -612,15 +864,18 @@ def run_b200(args):
                            parallelism='one graph per rank' if world > 1 else 'single GPU',
                            width_max=stats['width_max'], ops_per_step=stats['ops'],
                            compile_s=compile_s, first_call_s=first_call_s,
-                           cold_e2e_s=compile_s + first_call_s, alg_bytes_per_step=stats['alg_bytes'],
+                           cold_e2e_s=cold_e2e_s, cold_e2e_terms_per_s=cold_rate,
+                           cold_ratio_vs_cpu_baseline=(cold_rate / cpu['value']) if cpu else None,
+                           alg_bytes_per_step=stats['alg_bytes'],
+                           angle_checks=angle_checks,
                            launch_classes=[{'networks': c[0], 'threads': c[1], 'smem_bytes': c[2],
-                                            'smem_arena': bool(c[3] & 1),
-                                            'persistent': bool(c[3] & 2)}
+                                            'smem_arena': bool(c[3] & 1), 'persistent': bool(c[3] & 2),
+                                            'warp_queue': bool(c[3] & 16)}
                                            for c in cg.plan.last_launch_config()],
                            alg_flops_per_step=stats['alg_flops']),
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                          'frac': achieved / peak, 'traffic': profiled_traffic(),
-                         'kernel': 'qtb_network_kernel', 'peak_source': peak_kind,
+                         'kernel': 'qtb_network_kernel / qtb_warp_network_kernel', 'peak_source': peak_kind,
                          'kernel_ms_per_step': kernel_step_ms,
                          'class_launches_per_step': launches_per_step,
                          'alg_bytes_per_step': stats['alg_bytes']},
@@ -629,6 +884,9 @@ def run_b200(args):
                     'd2h_bytes_per_step': 8, 'ms_per_step': e2e_total / args.steps},
             'clocks': clk,
             'error_vs_oracle': errors,
+            'reference_order': ref_order,
+            'cfg4': cfg4,
+            'dropin': dropin,
             'plain_by_width': plain_widths,
             'plain': None if not plain_steps else {'value': stats['edges'] / (plain_ms_step / 1e3), 'unit': UNIT,
                       'ms_per_step': plain_ms_step, 'steps': plain_steps,
@@ -638,8 +896,8 @@ def run_b200(args):
                               'intermediates in global memory, complex64',
                       'batched_over_plain': value / (world * stats['edges'] / (plain_ms_step / 1e3))},
             'serving': serving,
-            # every kernel of a step is a qtb_network_kernel class launch (gate
-            # table and energy reduction are fused into it)
+            # every kernel of a step is an executor launch (gate table and
+            # energy reduction are fused into it)
             'gpu_launches': int(kernel_launches),
         }
         print(json.dumps(line), flush=True)

@@ -63,6 +63,10 @@ class Result:
         return self.finished - self.admitted
 
 
+class RequestTooLarge(RuntimeError):
+    """A request whose contraction work exceeds the server's budget."""
+
+
 class _Compiled:
     __slots__ = ('future', 'plan', 'params', 'n_edges', 'n_networks', 'bytes', 'scratch', 'submitted',
                  'compiled')
@@ -108,13 +112,16 @@ class QAOAServer:
     arena below 16 GiB, so only circuits that do not fit HBM are sliced.  A
     request that would need more slices fails alone and fast: its lightcones
     are wider than any exact contraction on one GPU can hold (the reference
-    would have to allocate tensors of that width too).  compile_workers:
-    host threads compiling requests concurrently (each also uses the C++
-    compiler's own threads)."""
+    would have to allocate tensors of that width too).  max_request_bytes:
+    a request whose plans move more algorithmic bytes than this (the sum
+    over its buckets of inputs read plus output written) fails at compile
+    time instead of holding the GPU for minutes; None admits any.
+    compile_workers: host threads compiling requests concurrently (each also
+    uses the C++ compiler's own threads)."""
 
     def __init__(self, device=None, n_streams=4, memory_budget=None, max_width=29,
                  max_slices=1024, composer='default', order_trials=8, compile_workers=2,
-                 compile_threads=0):
+                 compile_threads=0, max_request_bytes=None):
         if not torch.cuda.is_available():
             raise RuntimeError('QAOAServer needs a CUDA device; there is no CPU fallback')
         self.device = torch.device('cuda', torch.cuda.current_device() if device is None else device)
@@ -123,6 +130,7 @@ class QAOAServer:
         self.max_slices = max_slices
         self.order_trials = order_trials
         self.compile_threads = compile_threads
+        self.max_request_bytes = max_request_bytes
         _lib.check(_lib.lib().qtb_init(self.device.index))
         if memory_budget is None:
             memory_budget = torch.cuda.get_device_properties(self.device).total_memory * 3 // 4
@@ -181,6 +189,12 @@ class QAOAServer:
             plan.set_order_trials(self.order_trials)
             plan.set_max_width(self.max_width, self.max_slices)
             plan.add_lightcones(csr, edges, p, self.cid, params, self.compile_threads)
+            if self.max_request_bytes is not None:
+                work = sum(plan.info(i)['alg_bytes'] for i in range(len(plan)))
+                if work > self.max_request_bytes:
+                    plan.close()
+                    raise RequestTooLarge('request moves {:.3g} bytes in its contractions, over the '
+                                          'server\'s budget of {:.3g}'.format(work, self.max_request_bytes))
             job = _Compiled()
             job.future, job.plan, job.params = fut, plan, params
             job.n_edges, job.n_networks = len(edges), len(plan)
