@@ -26,6 +26,8 @@
  *                          qtensor/Simulate.py:66-94 (free output qubits)
  *   qtb_plan_set_max_width <- FeynmanSimulator slicing, qtensor/FeynmanSimulator.py:49-84
  *                          with SlicesOptimizer / GreedyParvars
+ *   qtb_contract_*      <- tcontract.mkl_contract_complex / mkl_contract_sum of
+ *                          CMKLExtendedBackend (ProcessingFrameworks.py:41-147)
  *   qtb_last_error      <- Python exceptions raised by the reference backends
  * Entry points without a counterpart in the reference are marked where they
  * are declared (allocation-free run, failure-detection self-test).
@@ -77,6 +79,29 @@ typedef struct {
  * complex64 array of 2^(n_vars - sum_first) elements. Asynchronous on stream. */
 int qtb_bucket_c64(const qtb_bucket_desc* desc, const void* const* inputs,
                    void* output, void* stream);
+
+/* ------------------------------------------------- merged-index contractions
+ * The two products of the reference's extended bucket backend
+ * CMKLExtendedBackend (qtensor/ProcessingFrameworks.py:41-147), whose native
+ * module tcontract (an MKL extension) the reference does not ship; complex64,
+ * row-major, device pointers, asynchronous on stream.
+ *   qtb_contract_outer_c64  <- tcontract.mkl_contract_complex (:65-66):
+ *                              c[n,m,k] = a[n,m] * b[n,k]
+ *   qtb_contract_sum_c64    <- tcontract.mkl_contract_sum (:129-130):
+ *                              C[f,m,n] = sum_k A[k,f,m] * B[k,f,n]
+ * The contract-sum runs on the tcgen05 tensor cores (mode 2, or mode 0 when
+ * K >= 32 and M, N >= 64): complex products in 3xTF32 (each operand split
+ * into TF32 high and low parts), FP32 accumulation in tensor memory, 128 x
+ * 128 output tiles; else (mode 1, or mode 0 for smaller shapes) on the CUDA
+ * cores in FP32.  scratch (qtb_contract_sum_scratch_bytes for the same
+ * shape and mode) holds the split operands; its first 4 bytes are a status
+ * word, 0 after a good run, 2 when a staging copy or the MMAs did not
+ * complete within the kernel's bounded wait.                              */
+int qtb_contract_outer_c64(const void* a, const void* b, void* c, int64_t n, int64_t m, int64_t k,
+                           void* stream);
+int qtb_contract_sum_scratch_bytes(int64_t K, int64_t F, int64_t M, int64_t N, int32_t mode, size_t* bytes);
+int qtb_contract_sum_c64(const void* A, const void* B, void* C, int64_t K, int64_t F, int64_t M, int64_t N,
+                         int32_t mode, void* scratch, size_t scratch_bytes, void* stream);
 
 /* ------------------------------------------------- plan compiler (host C++) */
 /* Gate kinds of a circuit given to the plan compiler. */

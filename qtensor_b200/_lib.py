@@ -25,6 +25,7 @@ SLICE_GREEDY, SLICE_TREE_TRIM, SLICE_LATE = 0, 1, 2
 # Exported entry points, in the order of include/qtb.h.
 EXPORTS = (
     'qtb_version', 'qtb_init', 'qtb_last_error', 'qtb_bucket_c64',
+    'qtb_contract_outer_c64', 'qtb_contract_sum_scratch_bytes', 'qtb_contract_sum_c64',
     'qtb_plan_create', 'qtb_plan_destroy', 'qtb_plan_add_circuit',
     'qtb_plan_add_lightcone', 'qtb_plan_add_lightcones', 'qtb_plan_add_circuit_batch',
     'qtb_plan_set_max_width', 'qtb_plan_set_slicing',
@@ -107,6 +108,11 @@ def _declare(lib):
         'qtb_init': (c.c_int, [c.c_int]),
         'qtb_last_error': (c.c_int, [c.c_char_p, c.c_size_t]),
         'qtb_bucket_c64': (c.c_int, [c.POINTER(BucketDesc), c.POINTER(P), P, P]),
+        'qtb_contract_outer_c64': (c.c_int, [P, P, P, c.c_int64, c.c_int64, c.c_int64, P]),
+        'qtb_contract_sum_scratch_bytes': (c.c_int, [c.c_int64, c.c_int64, c.c_int64, c.c_int64, c.c_int32,
+                                                     c.POINTER(c.c_size_t)]),
+        'qtb_contract_sum_c64': (c.c_int, [P, P, P, c.c_int64, c.c_int64, c.c_int64, c.c_int64, c.c_int32,
+                                           P, c.c_size_t, P]),
         'qtb_plan_create': (c.c_int, [c.c_int32, c.POINTER(P)]),
         'qtb_plan_destroy': (c.c_int, [P]),
         'qtb_plan_add_circuit': (c.c_int, [P, c.c_int32, P, c.c_int32, c.c_int32, P,

@@ -152,6 +152,104 @@ class B200Backend:
         return np.asarray(data)
 
 
+class B200ExtendedBackend(B200Backend):
+    """QTensor's ``CMKLExtendedBackend`` (qtensor/ProcessingFrameworks.py:41-147)
+    on the GPU, its absent native ``tcontract`` module replaced by
+    ``qtensor_b200.tcontract``: the bucket's first tensors are merged by
+    outer products over their common indices (``mkl_contract_complex``), the
+    last one is contracted with a sum over the bucket index
+    (``mkl_contract_sum``, on the tensor cores when its shape is large;
+    ``mode`` forces 'simt' or 'tensor').  Inputs are sliced and uploaded as
+    by ``B200Backend``; index bookkeeping, transposes and result names follow
+    the reference's, so results equal ``NumpyBackend``'s within complex64
+    rounding (3xTF32 on the tensor cores).  A single-tensor sum goes through
+    ``qtb_bucket_c64`` as in ``B200Backend``."""
+
+    def __init__(self, device=None, mode='auto'):
+        super().__init__(device)
+        self.mode = mode
+
+    def __getstate__(self):
+        state = super().__getstate__()
+        state['mode'] = self.mode
+        return state
+
+    def __setstate__(self, state):
+        super().__setstate__(state)
+        self.mode = state.get('mode', 'auto')
+
+    def _data(self, tensor):
+        data = tensor.data
+        if not isinstance(data, torch.Tensor):
+            data = torch.from_numpy(np.ascontiguousarray(np.asarray(data), dtype=np.complex64))
+        return data.to(self._device, dtype=torch.complex64)
+
+    @staticmethod
+    def _size(indices, data, ix):
+        return data.shape[list(indices).index(ix)]
+
+    def _merge(self, result_data, result_indices, tensor):
+        """``merge_with_result`` (:50-78): c[n,m,k] = a[n,m] b[n,k] over the
+        common (n), result-only (m) and tensor-only (k) indices."""
+        from . import tcontract
+        ixa, ixb = tuple(result_indices), tuple(tensor.indices)
+        b_data = self._data(tensor)
+        common = sorted(set(ixa) & set(ixb), key=int)
+        dist_a = [x for x in ixa if x not in common]
+        dist_b = [x for x in ixb if x not in common]
+        a = result_data.permute([ixa.index(x) for x in common + dist_a]).contiguous()
+        b = b_data.permute([ixb.index(x) for x in common + dist_b]).contiguous()
+        n = int(np.prod([self._size(ixa, result_data, x) for x in common], dtype=np.int64))
+        m = int(np.prod([self._size(ixa, result_data, x) for x in dist_a], dtype=np.int64))
+        k = int(np.prod([self._size(ixb, b_data, x) for x in dist_b], dtype=np.int64))
+        c = torch.empty((n, m, k), dtype=torch.complex64, device=self._device)
+        tcontract.mkl_contract_complex(a.reshape(n, m), b.reshape(n, k), c)
+        out_indices = tuple(sorted(set(ixa + ixb), key=int))
+        ixc = common + dist_a + dist_b
+        sizes = [self._size(ixa, result_data, x) if x in ixa else self._size(ixb, b_data, x) for x in ixc]
+        out = c.reshape(sizes).permute([ixc.index(x) for x in out_indices])
+        return out.contiguous(), out_indices
+
+    def process_bucket(self, bucket, no_sum=False):
+        from . import tcontract
+        self._ensure()
+        if len(bucket) == 0:
+            raise ValueError('process_bucket: empty bucket')
+        if len(bucket) < 2 and not no_sum:
+            return super().process_bucket(bucket, no_sum=no_sum)
+        result_indices = tuple(bucket[0].indices)
+        result_data = self._data(bucket[0])
+        for tensor in bucket[1:-1]:
+            result_data, result_indices = self._merge(result_data, result_indices, tensor)
+        tag = result_indices[0].identity if result_indices else 'f'
+        make = type(bucket[0])
+        if no_sum:
+            if len(bucket) > 1:
+                result_data, result_indices = self._merge(result_data, result_indices, bucket[-1])
+            return make('E{}'.format(tag), result_indices, data=result_data)
+        # contraction with the sum over the bucket index (:112-147)
+        last = bucket[-1]
+        last_data = self._data(last)
+        ixa, ixb = result_indices, tuple(last.indices)
+        k, fm, fn = ixa[:1], ixa[1:], ixb[1:]
+        if ixb[:1] != k:
+            raise ValueError('process_bucket: the last tensor does not start with the bucket index')
+        f = tuple(sorted(set(fm) & set(fn), key=int))
+        m = tuple(x for x in fm if x not in f)
+        n = tuple(x for x in fn if x not in f)
+        a = result_data.permute([ixa.index(x) for x in k + f + m]).contiguous()
+        b = last_data.permute([ixb.index(x) for x in k + f + n]).contiguous()
+        shapes = {x: self._size(ixb, last_data, x) for x in ixb}
+        shapes.update({x: self._size(ixa, result_data, x) for x in ixa})
+        K, F, M, N = [int(np.prod([shapes[x] for x in grp], dtype=np.int64)) for grp in (k, f, m, n)]
+        c = torch.empty((F, M, N), dtype=torch.complex64, device=self._device)
+        tcontract.mkl_contract_sum(a.reshape(K, F, M), b.reshape(K, F, N), c, mode=self.mode)
+        out_indices = tuple(sorted(set(ixa + ixb), key=int))[1:]
+        ixc = f + m + n
+        out = c.reshape([shapes[x] for x in ixc]).permute([ixc.index(x) for x in out_indices])
+        return make('E{}'.format(tag), out_indices, data=out.contiguous())
+
+
 class PerfBackend:
     """Per-bucket timing around another backend, the counterpart of
     QTensor's ``PerfBackend`` (qtensor/ProcessingFrameworks.py:152-234).

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, 'csrc')
 LIB = os.path.join(HERE, 'libqtb.so')
-SOURCES = ['plan.cpp', 'qtb.cu']
+SOURCES = ['plan.cpp', 'qtb.cu', 'contract.cu']
 ARCH_FLAGS = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
 

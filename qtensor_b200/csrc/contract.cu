@@ -1,0 +1,372 @@
+// Merged-index contractions of the reference's extended bucket backend
+// (CMKLExtendedBackend, qtensor/ProcessingFrameworks.py:41-147), whose
+// native dependency ``tcontract`` (an MKL C extension) is absent from the
+// reference:
+//
+//   qtb_contract_outer_c64  c[n,m,k] = a[n,m] * b[n,k]          (mkl_contract_complex, :60-66)
+//   qtb_contract_sum_c64    C[f,m,n] = sum_k A[k,f,m] * B[k,f,n] (mkl_contract_sum, :123-130)
+//
+// complex64 in and out.  The contract-sum is a batch of F complex GEMMs; with
+// a large summed dimension it runs on the tcgen05 tensor cores:
+//   * a pre-pass splits every operand into TF32 "hi" (rounded to nearest,
+//     cvt.rna.tf32.f32) and "lo" (the rounded remainder) planes of the real
+//     and imaginary parts, transposed to K-major and tiled 128 rows x 32 k in
+//     the canonical no-swizzle core-matrix layout (8 rows x 16 bytes), zero
+//     padded to whole tiles;
+//   * one CTA per (f, 128 x 128 output tile) stages the eight 16 KB planes of
+//     a k block with bulk copies (cp.async.bulk, mbarrier transaction count,
+//     bounded wait) and one thread issues tcgen05.mma kind::tf32 (M=128,
+//     N=128, K=8) into two TMEM accumulators, Re and Im, in FP32:
+//       Re += Ar_hi Br_hi + Ar_hi Br_lo + Ar_lo Br_hi - (Ai_hi Bi_hi + Ai_hi Bi_lo + Ai_lo Bi_hi)
+//       Im += Ar_hi Bi_hi + Ar_hi Bi_lo + Ar_lo Bi_hi + Ai_hi Br_hi + Ai_hi Br_lo + Ai_lo Br_hi
+//     (3xTF32: Ootomo and Yokota, "Recovering single precision accuracy from
+//     Tensor Cores while surpassing the FP32 theoretical peak performance",
+//     IJHPCA 2022; the lo x lo term is dropped), the negative terms through
+//     the instruction descriptor's negate-A bit;
+//   * the accumulators are read back with tcgen05.ld and written as complex64.
+// With a small summed dimension (the reference's own buckets sum one binary
+// index, K = 2) a tile would be mostly padding, and a CUDA-core kernel
+// computes the same sums in FP32.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <string>
+
+#include "plan.h"
+
+namespace qtb {
+
+// ----------------------------------------------------------------- CUDA cores
+// c[n,m,k] = a[n,m] * b[n,k], one element per thread (grid-stride).
+__global__ void qtb_outer_kernel(const float2* __restrict__ a, const float2* __restrict__ b,
+                                 float2* __restrict__ c, uint64_t n, uint64_t m, uint64_t k) {
+    const uint64_t total = n * m * k;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t kk = i % k, mm = (i / k) % m, nn = i / (k * m);
+        const float2 x = a[nn * m + mm], y = b[nn * k + kk];
+        c[i] = make_float2(x.x * y.x - x.y * y.y, x.x * y.y + x.y * y.x);
+    }
+}
+
+// C[f,m,n] = sum_k A[k,f,m] B[k,f,n], one output per thread, FP32 sums
+// over k in order.
+__global__ void qtb_contract_simt_kernel(const float2* __restrict__ A, const float2* __restrict__ B,
+                                         float2* __restrict__ C, uint64_t K, uint64_t F, uint64_t M,
+                                         uint64_t N) {
+    const uint64_t total = F * M * N;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t nn = i % N, mm = (i / N) % M, ff = i / (N * M);
+        float re = 0.f, im = 0.f;
+        for (uint64_t kk = 0; kk < K; ++kk) {
+            const float2 x = A[(kk * F + ff) * M + mm], y = B[(kk * F + ff) * N + nn];
+            re = fmaf(x.x, y.x, re);
+            re = fmaf(-x.y, y.y, re);
+            im = fmaf(x.x, y.y, im);
+            im = fmaf(x.y, y.x, im);
+        }
+        C[i] = make_float2(re, im);
+    }
+}
+
+// ----------------------------------------------------------------- tensor cores
+constexpr uint32_t kTcRows = 128;                     // tile rows (M of A tiles, N of B tiles)
+constexpr uint32_t kTcK = 32;                         // k per staged block
+constexpr uint32_t kTcTileWords = kTcRows * kTcK;     // 4096 x 32-bit = 16 KB
+constexpr uint32_t kTcPlanes = 4;                     // re_hi, re_lo, im_hi, im_lo
+constexpr uint32_t kTcThreads = 128;
+constexpr uint32_t kTcTmemCols = 256;                 // Re in columns 0..127, Im in 128..255
+constexpr uint32_t kTcSpinLimit = 1u << 24;           // bounded mbarrier waits (~1 s)
+constexpr int kTcStatusTimeout = 2;
+
+// Word of element (r, k) inside a 128 x 32 tile: core matrix (row group
+// r / 8, k chunk k / 4) at (g * 8 + c) * 32 words, 8 rows of 16 bytes each.
+__device__ __forceinline__ uint32_t tc_tile_word(uint32_t r, uint32_t k) {
+    return (((r >> 3) * 8u + (k >> 2)) << 5) + ((r & 7u) << 2) + (k & 3u);
+}
+
+__device__ __forceinline__ uint32_t tf32_round(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+// src[k][f][r] (complex64, R rows) -> for every f, planes q = 0..3 of
+// Rp x Kp TF32 words, tiles (row tile, k tile) in row-tile-major order.
+__global__ void qtb_tc_split_kernel(const float2* __restrict__ src, uint32_t* __restrict__ dst, uint32_t K,
+                                    uint32_t F, uint32_t R, uint32_t Rp, uint32_t Kp) {
+    const uint64_t plane = (uint64_t)Rp * Kp;
+    const uint64_t total = (uint64_t)F * plane;
+    const uint32_t k_tiles = Kp / kTcK;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        // rows fastest, so the source reads are coalesced
+        const uint32_t r = (uint32_t)(i % Rp);
+        const uint32_t k = (uint32_t)((i / Rp) % Kp);
+        const uint32_t f = (uint32_t)(i / plane);
+        float2 v = make_float2(0.f, 0.f);
+        if (r < R && k < K) v = src[((uint64_t)k * F + f) * R + r];
+        const uint32_t re_hi = tf32_round(v.x), im_hi = tf32_round(v.y);
+        const uint32_t re_lo = tf32_round(v.x - __uint_as_float(re_hi));
+        const uint32_t im_lo = tf32_round(v.y - __uint_as_float(im_hi));
+        const uint64_t base = (uint64_t)f * kTcPlanes * plane +
+                              ((uint64_t)(r / kTcRows) * k_tiles + k / kTcK) * kTcTileWords +
+                              tc_tile_word(r % kTcRows, k % kTcK);
+        dst[base] = re_hi;
+        dst[base + plane] = re_lo;
+        dst[base + 2 * plane] = im_hi;
+        dst[base + 3 * plane] = im_lo;
+    }
+}
+
+__device__ __forceinline__ uint32_t tc_smem(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor of a K-major, no-swizzle operand tile:
+// start address, leading byte offset (next 16-byte k chunk: 128 B), stride
+// byte offset (next 8-row group: 8 chunks x 128 B), descriptor version 1.
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) |
+           ((uint64_t)(1024u >> 4) << 32) | (uint64_t(1) << 46);
+}
+
+// Instruction descriptor: FP32 accumulator, TF32 A and B, both K-major,
+// N = 128 (>> 3 at bit 17), M = 128 (>> 4 at bit 24); bit 13 negates A.
+constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr uint32_t kTcIdescNegA = kTcIdesc | (1u << 13);
+
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+// Bounded wait for the mbarrier phase `parity`; false after the limit.
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
+    uint32_t done = 0;
+    for (uint32_t it = 0; it < kTcSpinLimit; ++it) {
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}" : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+        if (done) return true;
+        if (it > 64) __nanosleep(64);
+    }
+    return false;
+}
+
+// One CTA per (f, 128 x 128 tile of C).  Ap / Bp: the pre-pass planes.
+__global__ void __launch_bounds__(kTcThreads, 1)
+qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restrict__ Bp, float2* __restrict__ C,
+                       uint32_t F, uint32_t M, uint32_t N, uint32_t Mp, uint32_t Np, uint32_t Kp, int* status) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    // [A planes x4][B planes x4] (16 KB each), then two mbarriers and the TMEM slot
+    uint32_t* tiles = reinterpret_cast<uint32_t*>(smem);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 8 * kTcTileWords * 4);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
+    __shared__ int s_ok;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t nt = blockIdx.x, mt = blockIdx.y, f = blockIdx.z;
+    const uint32_t load_bar = tc_smem(&bars[0]), mma_bar = tc_smem(&bars[1]);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(load_bar));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mma_bar));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_ok = 1;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem(tmem_slot)),
+                     "r"(kTcTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = *tmem_slot;
+    const uint64_t a_plane = (uint64_t)Mp * Kp, b_plane = (uint64_t)Np * Kp;
+    const uint32_t k_tiles = Kp / kTcK;
+    const uint32_t* a_f = Ap + (uint64_t)f * kTcPlanes * a_plane + (uint64_t)mt * k_tiles * kTcTileWords;
+    const uint32_t* b_f = Bp + (uint64_t)f * kTcPlanes * b_plane + (uint64_t)nt * k_tiles * kTcTileWords;
+    for (uint32_t kt = 0; kt < k_tiles; ++kt) {
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(load_bar),
+                         "r"(8u * kTcTileWords * 4u)
+                         : "memory");
+            for (uint32_t q = 0; q < 8; ++q) {
+                const uint32_t* src = q < 4 ? a_f + q * a_plane + (uint64_t)kt * kTcTileWords
+                                            : b_f + (q - 4) * b_plane + (uint64_t)kt * kTcTileWords;
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                        tc_smem(tiles + q * kTcTileWords)),
+                    "l"(src), "r"(kTcTileWords * 4u), "r"(load_bar)
+                    : "memory");
+            }
+        }
+        if (!tc_wait(load_bar, kt & 1u)) {
+            if (threadIdx.x == 0) {
+                atomicOr(status, kTcStatusTimeout);
+                s_ok = 0;
+            }
+        }
+        __syncthreads();
+        if (!s_ok) break;
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            // planes: 0 Ar_hi 1 Ar_lo 2 Ai_hi 3 Ai_lo | 4 Br_hi 5 Br_lo 6 Bi_hi 7 Bi_lo
+            const uint32_t base = tc_smem(tiles);
+            const uint32_t re = tmem, im = tmem + 128u;
+            for (uint32_t s = 0; s < kTcK / 8; ++s) {
+                auto d = [&](uint32_t q) { return tc_desc(base + q * kTcTileWords * 4u + s * 256u); };
+                const uint32_t first = (kt == 0 && s == 0) ? 0u : 1u;
+                tc_mma(re, d(0), d(4), kTcIdesc, first);
+                tc_mma(re, d(0), d(5), kTcIdesc, 1u);
+                tc_mma(re, d(1), d(4), kTcIdesc, 1u);
+                tc_mma(re, d(2), d(6), kTcIdescNegA, 1u);
+                tc_mma(re, d(2), d(7), kTcIdescNegA, 1u);
+                tc_mma(re, d(3), d(6), kTcIdescNegA, 1u);
+                tc_mma(im, d(0), d(6), kTcIdesc, first);
+                tc_mma(im, d(0), d(7), kTcIdesc, 1u);
+                tc_mma(im, d(1), d(6), kTcIdesc, 1u);
+                tc_mma(im, d(2), d(4), kTcIdesc, 1u);
+                tc_mma(im, d(2), d(5), kTcIdesc, 1u);
+                tc_mma(im, d(3), d(4), kTcIdesc, 1u);
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mma_bar)
+                         : "memory");
+        }
+        // the tiles are overwritten by the next block only after the MMAs read them
+        if (!tc_wait(mma_bar, kt & 1u)) {
+            if (threadIdx.x == 0) {
+                atomicOr(status, kTcStatusTimeout);
+                s_ok = 0;
+            }
+        }
+        __syncthreads();
+        if (!s_ok) break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (s_ok) {
+        // warp w reads TMEM lanes 32w..32w+31: output rows of the tile
+        const uint32_t m = mt * kTcRows + warp * 32u + lane;
+        float2* crow = C + ((uint64_t)f * M + m) * N;
+        for (uint32_t c0 = 0; c0 < 128u; c0 += 8u) {
+            uint32_t r[8], i[8];
+            const uint32_t taddr = tmem + ((warp * 32u) << 16) + c0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7])
+                         : "r"(taddr));
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                         : "=r"(i[0]), "=r"(i[1]), "=r"(i[2]), "=r"(i[3]), "=r"(i[4]), "=r"(i[5]), "=r"(i[6]),
+                           "=r"(i[7])
+                         : "r"(taddr + 128u));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (m < M) {
+#pragma unroll
+                for (uint32_t j = 0; j < 8; ++j) {
+                    const uint32_t n = nt * kTcRows + c0 + j;
+                    if (n < N) crow[n] = make_float2(__uint_as_float(r[j]), __uint_as_float(i[j]));
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols));
+}
+
+constexpr size_t kTcSmemBytes = 8 * kTcTileWords * 4 + 64;
+
+static uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
+
+// Whether the contract-sum runs on the tensor cores: mode 1 never, 2
+// always, 0 when the summed dimension and both tile dimensions are large
+// enough for the tiles to be mostly data.
+static bool use_tensor_cores(int32_t mode, int64_t K, int64_t M, int64_t N) {
+    if (mode == 1) return false;
+    if (mode == 2) return true;
+    return K >= 32 && M >= 64 && N >= 64;
+}
+
+static int cuda_fail_c(cudaError_t e, const char* what) {
+    return fail(QTB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+}  // namespace qtb
+
+using namespace qtb;
+
+extern "C" {
+
+int qtb_contract_outer_c64(const void* a, const void* b, void* c, int64_t n, int64_t m, int64_t k,
+                           void* stream) {
+    if (!a || !b || !c || n < 1 || m < 1 || k < 1) return fail(QTB_ERR_ARG, "contract_outer: bad arguments");
+    const uint64_t total = (uint64_t)n * m * k;
+    const unsigned blocks = (unsigned)std::min<uint64_t>((total + 255) / 256, 148ull * 16);
+    qtb_outer_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const float2*>(a), static_cast<const float2*>(b), static_cast<float2*>(c), n, m, k);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? QTB_OK : cuda_fail_c(e, "contract_outer launch");
+}
+
+int qtb_contract_sum_scratch_bytes(int64_t K, int64_t F, int64_t M, int64_t N, int32_t mode, size_t* bytes) {
+    if (!bytes || K < 1 || F < 1 || M < 1 || N < 1 || mode < 0 || mode > 2)
+        return fail(QTB_ERR_ARG, "contract_sum_scratch_bytes: bad arguments");
+    if (!use_tensor_cores(mode, K, M, N)) {
+        *bytes = 16;
+        return QTB_OK;
+    }
+    const uint64_t Kp = round_up(K, kTcK), Mp = round_up(M, kTcRows), Np = round_up(N, kTcRows);
+    *bytes = 256 + (uint64_t)F * kTcPlanes * (Mp + Np) * Kp * 4;
+    return QTB_OK;
+}
+
+int qtb_contract_sum_c64(const void* A, const void* B, void* C, int64_t K, int64_t F, int64_t M, int64_t N,
+                         int32_t mode, void* scratch, size_t scratch_bytes, void* stream) {
+    if (!A || !B || !C || K < 1 || F < 1 || M < 1 || N < 1 || mode < 0 || mode > 2)
+        return fail(QTB_ERR_ARG, "contract_sum: bad arguments");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    size_t need = 0;
+    int r = qtb_contract_sum_scratch_bytes(K, F, M, N, mode, &need);
+    if (r) return r;
+    if (!scratch || scratch_bytes < need)
+        return fail(QTB_ERR_ARG, "contract_sum: scratch smaller than qtb_contract_sum_scratch_bytes");
+    cudaError_t e = cudaMemsetAsync(scratch, 0, 16, st);   // status word
+    if (e != cudaSuccess) return cuda_fail_c(e, "contract_sum status reset");
+    if (!use_tensor_cores(mode, K, M, N)) {
+        const uint64_t total = (uint64_t)F * M * N;
+        const unsigned blocks = (unsigned)std::min<uint64_t>((total + 255) / 256, 148ull * 16);
+        qtb_contract_simt_kernel<<<blocks, 256, 0, st>>>(static_cast<const float2*>(A),
+                                                         static_cast<const float2*>(B), static_cast<float2*>(C),
+                                                         K, F, M, N);
+        e = cudaGetLastError();
+        return e == cudaSuccess ? QTB_OK : cuda_fail_c(e, "contract_sum launch");
+    }
+    const uint64_t Kp = round_up(K, kTcK), Mp = round_up(M, kTcRows), Np = round_up(N, kTcRows);
+    if (Mp / kTcRows > 65535 || F > 65535 || Np / kTcRows > (1u << 31) || Kp > (1u << 30))
+        return fail(QTB_ERR_UNSUPPORTED, "contract_sum: shape beyond the tensor-core grid");
+    int* status = static_cast<int*>(scratch);
+    uint32_t* Ap = reinterpret_cast<uint32_t*>(static_cast<char*>(scratch) + 256);
+    uint32_t* Bp = Ap + (uint64_t)F * kTcPlanes * Mp * Kp;
+    auto split_blocks = [](uint64_t n) { return (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 32); };
+    qtb_tc_split_kernel<<<split_blocks((uint64_t)F * Mp * Kp), 256, 0, st>>>(
+        static_cast<const float2*>(A), Ap, (uint32_t)K, (uint32_t)F, (uint32_t)M, (uint32_t)Mp, (uint32_t)Kp);
+    qtb_tc_split_kernel<<<split_blocks((uint64_t)F * Np * Kp), 256, 0, st>>>(
+        static_cast<const float2*>(B), Bp, (uint32_t)K, (uint32_t)F, (uint32_t)N, (uint32_t)Np, (uint32_t)Kp);
+    // per device and cheap: set on every call
+    e = cudaFuncSetAttribute(qtb_tc_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kTcSmemBytes);
+    if (e != cudaSuccess) return cuda_fail_c(e, "contract_sum smem attribute");
+    dim3 grid((unsigned)(Np / kTcRows), (unsigned)(Mp / kTcRows), (unsigned)F);
+    qtb_tc_contract_kernel<<<grid, kTcThreads, kTcSmemBytes, st>>>(Ap, Bp, static_cast<float2*>(C), (uint32_t)F,
+                                                                  (uint32_t)M, (uint32_t)N, (uint32_t)Mp,
+                                                                  (uint32_t)Np, (uint32_t)Kp, status);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? QTB_OK : cuda_fail_c(e, "contract_sum launch");
+}
+
+}  // extern "C"
