@@ -378,7 +378,7 @@ def run_serving(n_requests, rate, device_index, plain_budget_s=20.0):
         wall_alone = time.perf_counter() - t0
 
     # the plain backend, same compile settings as the server, one request at a time
-    eng = QAOAEnergyEngine(device=device_index, max_width=29, max_slices=1024, order_trials=8,
+    eng = QAOAEnergyEngine(device=device_index, max_width=29, max_slices=1024, order_trials=4,
                            cache_size=1)
     plain_lat, plain_edges, plain_err, n_plain = [], 0, 0.0, 0
     t0 = time.perf_counter()

@@ -994,8 +994,15 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
     std::vector<int32_t> par;   // sliced line-graph nodes, in slicing order
     std::vector<int32_t> gorder, gdeg, torder, tdeg;
     LineGraph lg;
+    // variables that may be sliced within max_slices
+    int slice_budget = 0;
+    while (slice_budget < kMaxSlicedVars && (2ll << slice_budget) <= (long long)max_slices) ++slice_budget;
     // With trials, the minimum-fill heuristic competes too: its
     // deterministic order plus one randomized order per four greedy trials.
+    // It runs only while the greedy width is below max_width + 3, where it
+    // can decide whether (and how much) the circuit is sliced; further
+    // above, min-fill (which lowers widths by a few units) cannot change
+    // the outcome of the slicing step at hand.
     auto best_order = [&]() {
         line_graph(V, cliques, removed, &lg);
         double best_cost = greedy_order(lg, removed, 0, &gorder, &gdeg);
@@ -1010,7 +1017,9 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
             const uint64_t seed = 0x9E3779B97F4A7C15ull * (uint64_t)t + (uint64_t)V;
             keep(greedy_order(lg, removed, seed, &torder, &tdeg));
         }
-        if (order_trials > 0)
+        const int greedy_width = gdeg.empty() ? 0 : *std::max_element(gdeg.begin(), gdeg.end());
+        const bool far_above = max_width > 0 && greedy_width >= max_width + 3;
+        if (order_trials > 0 && !far_above)
             for (int32_t t = 0; t <= order_trials / 4; ++t) {
                 const uint64_t seed = t == 0 ? 0 : 0xD1B54A32D192ED03ull * (uint64_t)t + (uint64_t)V;
                 keep(minfill_order(lg, removed, seed, &torder, &tdeg));
@@ -1018,9 +1027,6 @@ int compile_circuit(int32_t n_qubits, const qtb_gate* in_gates, int32_t n_gates,
     };
     best_order();
     auto width = [&]() { return gdeg.empty() ? 0 : *std::max_element(gdeg.begin(), gdeg.end()); };
-    // variables that may still be sliced within max_slices
-    int slice_budget = 0;
-    while (slice_budget < kMaxSlicedVars && (2ll << slice_budget) <= (long long)max_slices) ++slice_budget;
     auto out_of_budget = [&](const char* how) {
         *err = "compile: width " + std::to_string(width()) + " still >= " + std::to_string(max_width) +
                " after " + how + " slicing of at most " + std::to_string(slice_budget) + " variables (" +

@@ -116,11 +116,13 @@ class QAOAServer:
     a request whose plans move more algorithmic bytes than this (the sum
     over its buckets of inputs read plus output written) fails at compile
     time instead of holding the GPU for minutes; None admits any.
-    compile_workers: host threads compiling requests concurrently (each also
-    uses the C++ compiler's own threads)."""
+    order_trials: randomized greedy orders per network (plus the minimum-fill
+    candidates they bring), fewer than the engine's 16 because a request's
+    compile is on its latency path.  compile_workers: host threads compiling
+    requests concurrently (each also uses the C++ compiler's own threads)."""
 
     def __init__(self, device=None, n_streams=4, memory_budget=None, max_width=29,
-                 max_slices=1024, composer='default', order_trials=8, compile_workers=2,
+                 max_slices=1024, composer='default', order_trials=4, compile_workers=2,
                  compile_threads=0, max_request_bytes=None):
         if not torch.cuda.is_available():
             raise RuntimeError('QAOAServer needs a CUDA device; there is no CPU fallback')

@@ -8,6 +8,7 @@ without the profiler and then under it.
     python tests/profile_workloads.py bucket24    # one 24-variable bucket through qtb_bucket_c64, 5 runs
     python tests/profile_workloads.py plain_cfg1  # 3-regular N=20 p=1 through the plain per-bucket path
     python tests/profile_workloads.py aux         # allocation-free run (N=100 p=3) and the wait self-test
+    python tests/profile_workloads.py contract    # tcontract contract-sum on the tensor cores, K=1024 F=2 M=N=1024
 
 QTB_SCHEDULE (see qtb.cu) fixes the executor schedule, so that the
 profiler's serialised replays cannot steer the autotuner.
@@ -138,7 +139,33 @@ def aux():
     assert status.value == _lib.STATUS_WAIT_TIMEOUT
 
 
+def contract():
+    """C[f,m,n] = sum_k A[k,f,m] B[k,f,n] with K=1024, F=2, M=N=1024 (3xTF32
+    on the tensor cores), 3 runs; checked against the CUDA-core path."""
+    from qtensor_b200 import tcontract
+    dev = torch.device('cuda', 0)
+    K, F, M, N = 1024, 2, 1024, 1024
+    gen = torch.Generator(device=dev).manual_seed(0)
+    a = torch.randn((K, F, M), dtype=torch.complex64, device=dev, generator=gen)
+    b = torch.randn((K, F, N), dtype=torch.complex64, device=dev, generator=gen)
+    c = torch.empty((F, M, N), dtype=torch.complex64, device=dev)
+    scratch = torch.empty(tcontract.contract_sum_scratch_bytes(K, F, M, N, 'tensor'), dtype=torch.uint8, device=dev)
+    s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        s_.record()
+        tcontract.mkl_contract_sum(a, b, c, mode='tensor', scratch=scratch)
+        e_.record()
+        e_.synchronize()
+        ms = s_.elapsed_time(e_)
+        print('contract-sum %.3f ms, %.1f TFLOP/s (8 M N K F useful flops)' % (ms, 8.0 * M * N * K * F / ms / 1e9))
+    assert int(scratch[:4].view(torch.int32).item()) == 0
+    ref = torch.empty_like(c)
+    tcontract.mkl_contract_sum(a, b, ref, mode='simt')
+    torch.cuda.synchronize()
+    assert ((c - ref).abs().max() <= 1e-5 * ref.abs().max()).item()
+
+
 if __name__ == '__main__':
     {'cfg3': cfg3, 'er400': er400, 'bucket24': bucket24, 'plain_cfg1': plain_cfg1,
-     'aux': aux}[sys.argv[1]]()
+     'aux': aux, 'contract': contract}[sys.argv[1]]()
     print('ok', sys.argv[1])
