@@ -478,10 +478,13 @@ __device__ float2 contract_network(const DevNetRun& net, const unsigned char* bl
 // After each network thread 0 writes its term; with a.energy set, the CTA
 // that finishes the run's last network sums Re(terms) in fp64 and writes
 // the energy.
-//   kLean (persistent, 128 threads): registers capped for 8 CTAs per SM, so
-//   small networks keep twice as many in flight per SM.
-template <bool kSmemArena, bool kSmemTable, bool kPersistent, bool kLean = false>
-__global__ void __launch_bounds__(kLean ? 128 : (kPersistent ? 512 : 1024), kLean ? 8 : 1) qtb_network_kernel(
+//   kLean 1 (persistent, 128 threads): registers capped for 8 CTAs per SM,
+//   so small networks keep twice as many in flight per SM; kLean 2 (96
+//   threads, 12 CTAs per SM) for networks whose staging and arena fit a
+//   twelfth of an SM, so that a run of N=1000 p=3 size is resident at once.
+template <bool kSmemArena, bool kSmemTable, bool kPersistent, int kLean = 0>
+__global__ void __launch_bounds__(kLean == 2 ? 96 : kLean ? 128 : (kPersistent ? 512 : 1024),
+                                  kLean == 2 ? 12 : kLean ? 8 : 1) qtb_network_kernel(
     const Job* __restrict__ jobs, const RunArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
@@ -1018,12 +1021,14 @@ constexpr int kSmemClasses = (int)(sizeof(kClassCtas) / sizeof(kClassCtas[0]));
 constexpr int kMaxClasses = kSmemClasses + 1;   // + the stream of the wide waves
 constexpr int kLeanThreads = 128;
 constexpr int kLeanCtasPerSm = 8;
+constexpr int kLean12Threads = 96;
+constexpr int kLean12CtasPerSm = 12;
 constexpr int kWarpDefaultThreads = 128;   // warps per CTA of the warp queue x 32
 
 struct LaunchClass {
     bool smem;
     bool persistent;        // CTAs take networks from the run's queue
-    bool lean;              // persistent, 128 threads, registers capped (8 CTAs per SM)
+    int lean;               // persistent, registers capped: 1 = 128 threads (8 CTAs per SM), 2 = 96 (12)
     bool warp;              // persistent, every warp takes networks (qtb_warp_network_kernel)
     int grid;               // CTAs (= n_jobs unless persistent)
     uint32_t capacity;      // arena elements per CTA
@@ -1061,7 +1066,7 @@ struct WideWave {
     int grid;
 };
 
-constexpr int kSchedClasses = 0, kSchedPersistent = 1, kSchedHybrid = 2, kSchedWarp = 3;
+constexpr int kSchedClasses = 0, kSchedPersistent = 1, kSchedHybrid = 2, kSchedWarp = 3, kSchedHybrid12 = 4;
 
 struct RunCache {
     Job* jobs = nullptr;                // class-mode jobs, persistent-mode jobs, counters
@@ -1072,6 +1077,7 @@ struct RunCache {
     std::vector<LaunchClass> classes;   // class schedule, widest first
     std::vector<LaunchClass> pclasses;  // persistent schedule
     std::vector<LaunchClass> hclasses;  // hybrid schedule: large networks as classes + lean queue
+    std::vector<LaunchClass> h12classes;  // the same with the 96-thread lean queue (12 CTAs per SM)
     std::vector<LaunchClass> wclasses;  // warp schedule: large networks as classes + warp queue
     std::vector<WideWave> waves;        // wide networks (both schedules), run one after another
     void* wide_buf = nullptr;
@@ -1111,6 +1117,7 @@ static const std::vector<LaunchClass>& schedule_of(const RunCache* rc) {
     return rc->schedule == kSchedPersistent ? rc->pclasses
            : rc->schedule == kSchedHybrid   ? rc->hclasses
            : rc->schedule == kSchedWarp     ? rc->wclasses
+           : rc->schedule == kSchedHybrid12 ? rc->h12classes
                                             : rc->classes;
 }
 
@@ -1146,8 +1153,12 @@ static void launch_one(const LaunchClass& lc, const Job* jobs, const RunArgs& a,
         return;
     }
     if constexpr (kA) {
+        if (lc.lean == 2) {
+            qtb_network_kernel<true, kT, true, 2><<<lc.grid, kLean12Threads, lc.smem_bytes, st>>>(jobs, a);
+            return;
+        }
         if (lc.lean) {
-            qtb_network_kernel<true, kT, true, true><<<lc.grid, kLeanThreads, lc.smem_bytes, st>>>(jobs, a);
+            qtb_network_kernel<true, kT, true, 1><<<lc.grid, kLeanThreads, lc.smem_bytes, st>>>(jobs, a);
             return;
         }
     }
@@ -1168,7 +1179,7 @@ static void launch_class(const LaunchClass& lc, bool smem_table, const Job* jobs
     }
 }
 
-template <bool kA, bool kT, bool kP, bool kL = false>
+template <bool kA, bool kT, bool kP, int kL = 0>
 static cudaError_t allow_smem() {
     return cudaFuncSetAttribute(qtb_network_kernel<kA, kT, kP, kL>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimitBytes);
@@ -1183,8 +1194,10 @@ static int allow_all_smem() {
     QTB_CUDA((allow_smem<true, false, true>()));
     QTB_CUDA((allow_smem<false, true, true>()));
     QTB_CUDA((allow_smem<false, false, true>()));
-    QTB_CUDA((allow_smem<true, true, true, true>()));
-    QTB_CUDA((allow_smem<true, false, true, true>()));
+    QTB_CUDA((allow_smem<true, true, true, 1>()));
+    QTB_CUDA((allow_smem<true, false, true, 1>()));
+    QTB_CUDA((allow_smem<true, true, true, 2>()));
+    QTB_CUDA((allow_smem<true, false, true, 2>()));
     QTB_CUDA(cudaFuncSetAttribute(qtb_warp_network_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kSmemLimitBytes));
     QTB_CUDA(cudaFuncSetAttribute(qtb_warp_network_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1208,13 +1221,20 @@ static int persistent_grid(const LaunchClass& lc, bool smem_table, int* grid) {
         const int warps = std::max(1, lc.threads / 32);
         *grid = std::max(1, std::min((lc.n_jobs + warps - 1) / warps, std::max(1, per_sm) * sms));
         return QTB_OK;
+    } else if (lc.lean == 2) {
+        if (smem_table)
+            QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, qtb_network_kernel<true, true, true, 2>, kLean12Threads, lc.smem_bytes));
+        else
+            QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, qtb_network_kernel<true, false, true, 2>, kLean12Threads, lc.smem_bytes));
     } else if (lc.lean) {
         if (smem_table)
             QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &per_sm, qtb_network_kernel<true, true, true, true>, kLeanThreads, lc.smem_bytes));
+                &per_sm, qtb_network_kernel<true, true, true, 1>, kLeanThreads, lc.smem_bytes));
         else
             QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &per_sm, qtb_network_kernel<true, false, true, true>, kLeanThreads, lc.smem_bytes));
+                &per_sm, qtb_network_kernel<true, false, true, 1>, kLeanThreads, lc.smem_bytes));
     } else if (lc.smem) {
         if (smem_table)
             QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
@@ -1559,9 +1579,12 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
     // as class launches (one CTA per network, more threads), launched first
     // so that their longer critical paths start early
     rc->hclasses.clear();
-    {
+    rc->h12classes.clear();
+    for (int variant = 1; variant <= 2; ++variant) {
+        std::vector<LaunchClass>& out = variant == 1 ? rc->hclasses : rc->h12classes;
+        const int lean_ctas = variant == 1 ? kLeanCtasPerSm : kLean12CtasPerSm;
         int lean_class = 0;
-        while (lean_class < kSmemClasses && kClassCtas[lean_class] != kLeanCtasPerSm) ++lean_class;
+        while (lean_class < kSmemClasses && kClassCtas[lean_class] != lean_ctas) ++lean_class;
         const uint32_t lean_bound = class_bound(lean_class);
         std::vector<int32_t> lean, big;
         for (int32_t i : all) (net_need(plan->druns[i], fixed) <= lean_bound ? lean : big).push_back(i);
@@ -1587,12 +1610,12 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
                 std::vector<int32_t> m;
                 for (int32_t i : big)
                     if (class_of[i - first] == c) m.push_back(i);
-                if (!m.empty()) rc->hclasses.push_back(make_class(m, true, false));
+                if (!m.empty()) out.push_back(make_class(m, true, false));
             }
             LaunchClass lc = make_class(lean, true, true);
-            lc.lean = true;
-            lc.threads = kLeanThreads;
-            rc->hclasses.push_back(lc);
+            lc.lean = variant;
+            lc.threads = variant == 1 ? kLeanThreads : kLean12Threads;
+            out.push_back(lc);
         }
     }
     // warp schedule: the networks whose warp slot (blob + arena) is at most
@@ -1646,6 +1669,10 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
         }
     if (!rc->hclasses.empty()) {
         int r = hybrid_lean_grid(rc->hclasses, rc->smem_table);
+        if (r) return r;
+    }
+    if (!rc->h12classes.empty()) {
+        int r = hybrid_lean_grid(rc->h12classes, rc->smem_table);
         if (r) return r;
     }
     if (!rc->wclasses.empty()) {
@@ -1940,6 +1967,31 @@ static int autotune_run(qtb_plan_device* s, RunCache* rc, const RunArgs& base, v
         big_threads = best_t;
         if ((r = hybrid_lean_grid(rc->hclasses, rc->smem_table))) return r;
     }
+    // hybrid schedule with the 96-thread lean queue (12 CTAs per SM), its
+    // large-network classes at 512 or 1024 threads
+    float hyb12_ms = 1e30f;
+    if (!rc->h12classes.empty()) {
+        int best_t = 512;
+        for (int t : {512, 1024}) {
+            std::vector<LaunchClass> sched = rc->h12classes;
+            for (LaunchClass& q : sched)
+                if (!q.lean) q.threads = t;
+            if ((r = hybrid_lean_grid(sched, rc->smem_table))) return r;
+            float ms = 1e30f;
+            if ((r = time_it([&] { return launch_schedule(s, rc, sched, a, scratch_dev, st); }, &ms)))
+                return r;
+            if (log)
+                std::fprintf(stderr, "qtb autotune: hybrid schedule (96-thread lean queue), large networks %4d threads %.1f us\n",
+                             t, 1e3 * ms);
+            if (ms < hyb12_ms) {
+                hyb12_ms = ms;
+                best_t = t;
+            }
+        }
+        for (LaunchClass& q : rc->h12classes)
+            if (!q.lean) q.threads = best_t;
+        if ((r = hybrid_lean_grid(rc->h12classes, rc->smem_table))) return r;
+    }
     // warp schedule: the warp queue with 2, 4 or 8 warps per CTA (the
     // large-network classes keep their tuned block size)
     float warp_ms = 1e30f;
@@ -1975,12 +2027,18 @@ static int autotune_run(qtb_plan_device* s, RunCache* rc, const RunArgs& base, v
         rc->schedule = kSchedHybrid;
         best_ms = hyb_ms;
     }
-    if (warp_ms < best_ms) rc->schedule = kSchedWarp;
+    if (warp_ms < best_ms) {
+        rc->schedule = kSchedWarp;
+        best_ms = warp_ms;
+    }
+    if (hyb12_ms < best_ms) rc->schedule = kSchedHybrid12;
     if (log)
         std::fprintf(stderr,
-                     "qtb autotune: class schedule %.1f us, persistent %.1f us, hybrid %.1f us, warp %.1f us -> %s\n",
-                     1e3 * class_ms, 1e3 * pers_ms, 1e3 * hyb_ms, 1e3 * warp_ms,
+                     "qtb autotune: class schedule %.1f us, persistent %.1f us, hybrid %.1f us, hybrid "
+                     "(96-thread lean) %.1f us, warp %.1f us -> %s\n",
+                     1e3 * class_ms, 1e3 * pers_ms, 1e3 * hyb_ms, 1e3 * hyb12_ms, 1e3 * warp_ms,
                      rc->schedule == kSchedWarp       ? "warp"
+                     : rc->schedule == kSchedHybrid12 ? "hybrid12"
                      : rc->schedule == kSchedHybrid   ? "hybrid"
                      : rc->schedule == kSchedPersistent ? "persistent"
                                                       : "classes");
@@ -1991,8 +2049,9 @@ static int autotune_run(qtb_plan_device* s, RunCache* rc, const RunArgs& base, v
 }
 
 // QTB_SCHEDULE=persistent:<128|256|512>, hybrid:<256|512|1024> (threads of
-// the large-network classes), warp:<64|128|256> (threads per CTA of the
-// warp queue) or QTB_SCHEDULE=classes in the
+// the large-network classes), hybrid12:<512|1024> (the same with the
+// 96-thread lean queue), warp:<64|128|256> (threads per CTA of the warp
+// queue) or QTB_SCHEDULE=classes in the
 // environment fixes the schedule of every range without timing it, so that a
 // profiler sees one chosen configuration.  Returns 1 when it applied.
 static int forced_schedule(RunCache* rc, int* err) {
@@ -2015,6 +2074,13 @@ static int forced_schedule(RunCache* rc, int* err) {
             if (!q.lean) q.threads = t;
         if ((*err = hybrid_lean_grid(rc->hclasses, rc->smem_table))) return 0;
         rc->schedule = kSchedHybrid;
+    } else if (std::strncmp(env, "hybrid12:", 9) == 0 && !rc->h12classes.empty()) {
+        const int t = std::atoi(env + 9);
+        if (t != 512 && t != 1024) return 0;
+        for (LaunchClass& q : rc->h12classes)
+            if (!q.lean) q.threads = t;
+        if ((*err = hybrid_lean_grid(rc->h12classes, rc->smem_table))) return 0;
+        rc->schedule = kSchedHybrid12;
     } else if (std::strncmp(env, "warp:", 5) == 0 && !rc->wclasses.empty()) {
         const int t = std::atoi(env + 5);
         if (t != 64 && t != 128 && t != 256) return 0;
@@ -2397,7 +2463,8 @@ int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32
             out[4 * c] = lc.n_jobs;
             out[4 * c + 1] = lc.threads;
             out[4 * c + 2] = (int32_t)lc.smem_bytes;
-            out[4 * c + 3] = (lc.smem ? 1 : 0) | (lc.persistent ? 2 : 0) | (lc.lean ? 8 : 0) | (lc.warp ? 16 : 0);
+            out[4 * c + 3] = (lc.smem ? 1 : 0) | (lc.persistent ? 2 : 0) | (lc.lean ? 8 : 0) | (lc.warp ? 16 : 0) |
+                             (lc.lean == 2 ? 32 : 0);
         } else {
             const WideWave& wv = rc->waves[c - sched.size()];
             out[4 * c] = (int32_t)wv.n_nets;

@@ -160,15 +160,16 @@ def test_plain_path_matches_batched_and_reference(cuda_device, name, max_width):
 
 
 def test_wide_waves_match_plain_path(cuda_device):
-    """Erdos-Renyi N=400 p=3 (seed 24323709): 147 networks too large for
-    shared memory (2 GB of arenas) run as two whole-GPU waves next to the
-    shared-memory classes; every edge term equals the plain per-bucket
-    path's (an independent execution of the same plans) and the energies
-    agree."""
+    """Erdos-Renyi N=400 p=3 (seed 24323709) with the reference's greedy rule
+    alone (order_trials=0, slicing from width 22): 247 networks too large
+    for shared memory (3.5 GB of arenas) run as several whole-GPU waves next
+    to the shared-memory classes; every edge term equals the plain
+    per-bucket path's (an independent execution of the same plans) and the
+    energies agree."""
     import networkx as nx
     G = nx.erdos_renyi_graph(400, 3 / 399, seed=24323709)
     gamma, beta = graphs.angles(3, seed=1)
-    eng = _engine(max_width=22)
+    eng = _engine(max_width=22, order_trials=0)
     batched = eng.edge_terms(G, gamma, beta)
     cg = eng.compile(G, 3, gamma, beta)
     waves = [c for c in cg.plan.last_launch_config() if c[3] & 4]
@@ -182,11 +183,12 @@ def test_wide_waves_match_plain_path(cuda_device):
 
 
 @pytest.mark.parametrize('schedule', ['classes', 'persistent:256', 'hybrid:512', 'hybrid:1024',
-                                      'warp:64', 'warp:128', 'warp:256'])
+                                      'hybrid12:512', 'hybrid12:1024', 'warp:64', 'warp:128', 'warp:256'])
 def test_every_schedule_matches_reference(cuda_device, monkeypatch, schedule):
     """Each executor schedule the autotuner may pick (size classes, one
     persistent queue, large-network classes + lean queue, large-network
-    classes + warp-per-network queue), forced through QTB_SCHEDULE, gives
+    classes + warp-per-network queue, large-network classes + 96-thread lean
+    queue at 12 CTAs per SM), forced through QTB_SCHEDULE, gives
     the reference's edge terms for all 1500 edges of the N=1000 p=3
     workload."""
     monkeypatch.setenv('QTB_SCHEDULE', schedule)
@@ -196,7 +198,9 @@ def test_every_schedule_matches_reference(cuda_device, monkeypatch, schedule):
     ref = np.array([complex(*t) for t in w['terms']])
     assert np.max(np.abs(terms - ref)) < TOL
     cfg = eng.compile(G, 3, w['gamma'], w['beta']).plan.last_launch_config()
-    if schedule.startswith('hybrid'):
+    if schedule.startswith('hybrid12'):
+        assert any(c[3] & 32 and c[1] == 96 for c in cfg)
+    elif schedule.startswith('hybrid'):
         assert any(c[3] & 8 for c in cfg) and any(not c[3] & 2 for c in cfg)
     elif schedule.startswith('warp'):
         assert any(c[3] & 16 and c[1] == int(schedule[5:]) for c in cfg)
