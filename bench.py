@@ -80,6 +80,8 @@ def parse():
                     help='steps of the 3-regular N=256 p=4 leg (0 skips it)')
     ap.add_argument('--reference-order-steps', type=int, default=10,
                     help='steps of the leg with the reference greedy order (0 skips it)')
+    ap.add_argument('--no-tensor-core', action='store_true',
+                    help='skip the tensor-core contract-sum leg')
     ap.add_argument('--no-dropin', action='store_true',
                     help="skip the replay of the reference driver's recorded backend calls")
     ap.add_argument('--shard', action='store_true',
@@ -658,6 +660,63 @@ def run_dropin(device_index):
     return out
 
 
+def measured_peak_tflops():
+    path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d['bf16_tflops']), 'measured (dense bf16 cuBLAS burst)'
+    except (OSError, KeyError, ValueError):
+        return 1590.0, 'fallback'
+
+
+def run_tensor_core_contract(device_index, reps=5):
+    """The reference's merged-index contraction C[f,m,n] = sum_k A[k,f,m]
+    B[k,f,n] (CMKLExtendedBackend's mkl_contract_sum) on a GEMM-shaped
+    workload, K = 1024, F = 2, M = N = 1024: the tcgen05 path (3xTF32
+    products, FP32 accumulation) against the CUDA-core path, with the
+    useful complex flops 8 F M N K per call and the error of 16 sampled
+    output rows against complex128 (numpy, on the host)."""
+    import torch
+    from qtensor_b200 import tcontract
+    dev = torch.device('cuda', device_index)
+    K, F, M, N = 1024, 2, 1024, 1024
+    rng = np.random.default_rng(7)
+    A = (rng.standard_normal((K, F, M)) + 1j * rng.standard_normal((K, F, M))).astype(np.complex64)
+    B = (rng.standard_normal((K, F, N)) + 1j * rng.standard_normal((K, F, N))).astype(np.complex64)
+    a, b = torch.from_numpy(A).to(dev), torch.from_numpy(B).to(dev)
+    out = {}
+    flops = 8.0 * F * M * N * K
+    for mode in ('tensor', 'simt'):
+        c = torch.empty((F, M, N), dtype=torch.complex64, device=dev)
+        scratch = torch.empty(tcontract.contract_sum_scratch_bytes(K, F, M, N, mode), dtype=torch.uint8, device=dev)
+        tcontract.mkl_contract_sum(a, b, c, mode=mode, scratch=scratch)     # warm-up
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(reps):
+            tcontract.mkl_contract_sum(a, b, c, mode=mode, scratch=scratch)
+        e.record()
+        e.synchronize()
+        ms = s.elapsed_time(e) / reps
+        status = int(scratch[:4].view(torch.int32).item())
+        rows = rng.choice(M, 16, replace=False)
+        got = c.cpu().numpy()
+        ref = np.einsum('kfm,kfn->fmn', A[:, :, rows].astype(np.complex128), B.astype(np.complex128))
+        err = float(np.max(np.abs(got[:, rows, :] - ref)) / np.max(np.abs(ref)))
+        out[mode] = {'ms': ms, 'useful_tflops': flops / (ms / 1e3) / 1e12, 'status': status,
+                     'max_rel_error_vs_complex128': err}
+    peak, source = measured_peak_tflops()
+    out['tensor']['frac_of_peak'] = out['tensor']['useful_tflops'] / peak
+    out['peak_tflops'] = peak
+    out['peak_source'] = source
+    out['tensor_over_simt'] = out['simt']['ms'] / out['tensor']['ms']
+    out['workload'] = ('C[f,m,n] = sum_k A[k,f,m] B[k,f,n], K=1024 F=2 M=N=1024 complex64 (includes the '
+                       'TF32 hi/lo split pre-pass); useful flops 8 F M N K; the 3xTF32 emulation runs 12 real '
+                       'MMA passes per complex product, so the useful rate is at most 1/3 of the TF32 rate')
+    return out
+
+
 def run_sharded(args, dev, local, rank, world):
     """One Erdos-Renyi graph (mean degree 3, p=3) sharded over the ranks by
     longest processing time on the plans' flops: each rank contracts its
@@ -829,6 +888,7 @@ def run_b200(args):
     ref_order = (run_reference_order(G, p, local, flush, args.reference_order_steps)
                  if extra and args.reference_order_steps > 0 else None)
     dropin = run_dropin(local) if extra and not args.no_dropin else None
+    tc_contract = run_tensor_core_contract(local) if extra and not args.no_tensor_core else None
     serving = None
     if extra and args.serving_requests > 0:
         serving = run_serving(args.serving_requests, args.serving_rate, local)
@@ -887,6 +947,7 @@ def run_b200(args):
             'reference_order': ref_order,
             'cfg4': cfg4,
             'dropin': dropin,
+            'tensor_core_contract': tc_contract,
             'plain_by_width': plain_widths,
             'plain': None if not plain_steps else {'value': stats['edges'] / (plain_ms_step / 1e3), 'unit': UNIT,
                       'ms_per_step': plain_ms_step, 'steps': plain_steps,

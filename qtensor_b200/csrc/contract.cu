@@ -13,17 +13,22 @@
 //     and imaginary parts, transposed to K-major and tiled 128 rows x 32 k in
 //     the canonical no-swizzle core-matrix layout (8 rows x 16 bytes), zero
 //     padded to whole tiles;
-//   * one CTA per (f, 128 x 128 output tile) stages the eight 16 KB planes of
-//     a k block with bulk copies (cp.async.bulk, mbarrier transaction count,
-//     bounded wait) and one thread issues tcgen05.mma kind::tf32 (M=128,
-//     N=128, K=8) into two TMEM accumulators, Re and Im, in FP32:
+//   * one CTA per (f, 128 x 64 output tile) stages the eight planes of a k
+//     block (16 KB of A, 8 KB of B each) with bulk copies (cp.async.bulk,
+//     mbarrier transaction count, bounded wait) and one thread issues
+//     tcgen05.mma kind::tf32 (M=128, N=64, K=8) into two TMEM accumulators,
+//     Re and Im, in FP32:
 //       Re += Ar_hi Br_hi + Ar_hi Br_lo + Ar_lo Br_hi - (Ai_hi Bi_hi + Ai_hi Bi_lo + Ai_lo Bi_hi)
 //       Im += Ar_hi Bi_hi + Ar_hi Bi_lo + Ar_lo Bi_hi + Ai_hi Br_hi + Ai_hi Br_lo + Ai_lo Br_hi
 //     (3xTF32: Ootomo and Yokota, "Recovering single precision accuracy from
 //     Tensor Cores while surpassing the FP32 theoretical peak performance",
 //     IJHPCA 2022; the lo x lo term is dropped), the negative terms through
 //     the instruction descriptor's negate-A bit;
-//   * the accumulators are read back with tcgen05.ld and written as complex64.
+//   * after every 32-k block the accumulators are read back (tcgen05.ld) and
+//     added into FP32 registers with round-to-nearest, since the tensor
+//     cores' own accumulation rounds toward zero (Ootomo and Yokota keep the
+//     long sum outside the tensor cores for the same reason); the registers
+//     are written as complex64.
 // With a small summed dimension (the reference's own buckets sum one binary
 // index, K = 2) a tile would be mostly padding, and a CUDA-core kernel
 // computes the same sums in FP32.
@@ -72,16 +77,18 @@ __global__ void qtb_contract_simt_kernel(const float2* __restrict__ A, const flo
 }
 
 // ----------------------------------------------------------------- tensor cores
-constexpr uint32_t kTcRows = 128;                     // tile rows (M of A tiles, N of B tiles)
+constexpr uint32_t kTcM = 128;                        // output tile rows (A tile rows)
+constexpr uint32_t kTcN = 64;                         // output tile columns (B tile rows)
 constexpr uint32_t kTcK = 32;                         // k per staged block
-constexpr uint32_t kTcTileWords = kTcRows * kTcK;     // 4096 x 32-bit = 16 KB
+constexpr uint32_t kTcAWords = kTcM * kTcK;           // 4096 x 32-bit = 16 KB per A plane
+constexpr uint32_t kTcBWords = kTcN * kTcK;           // 2048 x 32-bit =  8 KB per B plane
 constexpr uint32_t kTcPlanes = 4;                     // re_hi, re_lo, im_hi, im_lo
 constexpr uint32_t kTcThreads = 128;
-constexpr uint32_t kTcTmemCols = 256;                 // Re in columns 0..127, Im in 128..255
+constexpr uint32_t kTcTmemCols = 128;                 // Re in columns 0..63, Im in 64..127
 constexpr uint32_t kTcSpinLimit = 1u << 24;           // bounded mbarrier waits (~1 s)
 constexpr int kTcStatusTimeout = 2;
 
-// Word of element (r, k) inside a 128 x 32 tile: core matrix (row group
+// Word of element (r, k) inside a tile of 32 k: core matrix (row group
 // r / 8, k chunk k / 4) at (g * 8 + c) * 32 words, 8 rows of 16 bytes each.
 __device__ __forceinline__ uint32_t tc_tile_word(uint32_t r, uint32_t k) {
     return (((r >> 3) * 8u + (k >> 2)) << 5) + ((r & 7u) << 2) + (k & 3u);
@@ -94,12 +101,13 @@ __device__ __forceinline__ uint32_t tf32_round(float x) {
 }
 
 // src[k][f][r] (complex64, R rows) -> for every f, planes q = 0..3 of
-// Rp x Kp TF32 words, tiles (row tile, k tile) in row-tile-major order.
+// Rp x Kp TF32 words in tiles of `tile_rows` x 32 k, row-tile-major.
 __global__ void qtb_tc_split_kernel(const float2* __restrict__ src, uint32_t* __restrict__ dst, uint32_t K,
-                                    uint32_t F, uint32_t R, uint32_t Rp, uint32_t Kp) {
+                                    uint32_t F, uint32_t R, uint32_t Rp, uint32_t Kp, uint32_t tile_rows) {
     const uint64_t plane = (uint64_t)Rp * Kp;
     const uint64_t total = (uint64_t)F * plane;
     const uint32_t k_tiles = Kp / kTcK;
+    const uint32_t tile_words = tile_rows * kTcK;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
          i += (uint64_t)gridDim.x * blockDim.x) {
         // rows fastest, so the source reads are coalesced
@@ -112,8 +120,8 @@ __global__ void qtb_tc_split_kernel(const float2* __restrict__ src, uint32_t* __
         const uint32_t re_lo = tf32_round(v.x - __uint_as_float(re_hi));
         const uint32_t im_lo = tf32_round(v.y - __uint_as_float(im_hi));
         const uint64_t base = (uint64_t)f * kTcPlanes * plane +
-                              ((uint64_t)(r / kTcRows) * k_tiles + k / kTcK) * kTcTileWords +
-                              tc_tile_word(r % kTcRows, k % kTcK);
+                              ((uint64_t)(r / tile_rows) * k_tiles + k / kTcK) * tile_words +
+                              tc_tile_word(r % tile_rows, k % kTcK);
         dst[base] = re_hi;
         dst[base + plane] = re_lo;
         dst[base + 2 * plane] = im_hi;
@@ -134,8 +142,8 @@ __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
 }
 
 // Instruction descriptor: FP32 accumulator, TF32 A and B, both K-major,
-// N = 128 (>> 3 at bit 17), M = 128 (>> 4 at bit 24); bit 13 negates A.
-constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+// N = 64 (>> 3 at bit 17), M = 128 (>> 4 at bit 24); bit 13 negates A.
+constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((kTcN >> 3) << 17) | ((kTcM >> 4) << 24);
 constexpr uint32_t kTcIdescNegA = kTcIdesc | (1u << 13);
 
 __device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
@@ -159,14 +167,30 @@ __device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
     return false;
 }
 
-// One CTA per (f, 128 x 128 tile of C).  Ap / Bp: the pre-pass planes.
+// Eight 32-bit TMEM columns of this thread's lane.
+__device__ __forceinline__ void tc_ld8(uint32_t taddr, float* out) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 8; ++j) out[j] = __uint_as_float(r[j]);
+}
+
+// One CTA per (f, 128 x 64 tile of C).  Ap / Bp: the pre-pass planes.
+// Every 32-k block is accumulated in TMEM from zero and then added, with
+// round-to-nearest, into FP32 registers (one row of the tile per thread):
+// the tensor cores' accumulation rounds toward zero, and summing a long k
+// range in TMEM alone biases the result (about 3e-5 relative at K = 1000).
 __global__ void __launch_bounds__(kTcThreads, 1)
 qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restrict__ Bp, float2* __restrict__ C,
                        uint32_t F, uint32_t M, uint32_t N, uint32_t Mp, uint32_t Np, uint32_t Kp, int* status) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    // [A planes x4][B planes x4] (16 KB each), then two mbarriers and the TMEM slot
-    uint32_t* tiles = reinterpret_cast<uint32_t*>(smem);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 8 * kTcTileWords * 4);
+    // [A planes x4 (16 KB each)][B planes x4 (8 KB each)], two mbarriers, the TMEM slot
+    uint32_t* a_tiles = reinterpret_cast<uint32_t*>(smem);
+    uint32_t* b_tiles = a_tiles + kTcPlanes * kTcAWords;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(b_tiles + kTcPlanes * kTcBWords);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
     __shared__ int s_ok;
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -187,90 +211,93 @@ qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restri
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = *tmem_slot;
+    const uint32_t lane_addr = tmem + ((warp * 32u) << 16);   // this warp's 32 TMEM lanes
+    float acc_re[kTcN], acc_im[kTcN];
+#pragma unroll
+    for (uint32_t j = 0; j < kTcN; ++j) acc_re[j] = acc_im[j] = 0.f;
     const uint64_t a_plane = (uint64_t)Mp * Kp, b_plane = (uint64_t)Np * Kp;
     const uint32_t k_tiles = Kp / kTcK;
-    const uint32_t* a_f = Ap + (uint64_t)f * kTcPlanes * a_plane + (uint64_t)mt * k_tiles * kTcTileWords;
-    const uint32_t* b_f = Bp + (uint64_t)f * kTcPlanes * b_plane + (uint64_t)nt * k_tiles * kTcTileWords;
+    const uint32_t* a_f = Ap + (uint64_t)f * kTcPlanes * a_plane + (uint64_t)mt * k_tiles * kTcAWords;
+    const uint32_t* b_f = Bp + (uint64_t)f * kTcPlanes * b_plane + (uint64_t)nt * k_tiles * kTcBWords;
     for (uint32_t kt = 0; kt < k_tiles; ++kt) {
         if (threadIdx.x == 0) {
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(load_bar),
-                         "r"(8u * kTcTileWords * 4u)
+                         "r"(kTcPlanes * (kTcAWords + kTcBWords) * 4u)
                          : "memory");
-            for (uint32_t q = 0; q < 8; ++q) {
-                const uint32_t* src = q < 4 ? a_f + q * a_plane + (uint64_t)kt * kTcTileWords
-                                            : b_f + (q - 4) * b_plane + (uint64_t)kt * kTcTileWords;
+            for (uint32_t q = 0; q < kTcPlanes; ++q) {
                 asm volatile(
                     "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                        tc_smem(tiles + q * kTcTileWords)),
-                    "l"(src), "r"(kTcTileWords * 4u), "r"(load_bar)
+                        tc_smem(a_tiles + q * kTcAWords)),
+                    "l"(a_f + q * a_plane + (uint64_t)kt * kTcAWords), "r"(kTcAWords * 4u), "r"(load_bar)
+                    : "memory");
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                        tc_smem(b_tiles + q * kTcBWords)),
+                    "l"(b_f + q * b_plane + (uint64_t)kt * kTcBWords), "r"(kTcBWords * 4u), "r"(load_bar)
                     : "memory");
             }
         }
-        if (!tc_wait(load_bar, kt & 1u)) {
-            if (threadIdx.x == 0) {
-                atomicOr(status, kTcStatusTimeout);
-                s_ok = 0;
-            }
+        if (!tc_wait(load_bar, kt & 1u) && threadIdx.x == 0) {
+            atomicOr(status, kTcStatusTimeout);
+            s_ok = 0;
         }
         __syncthreads();
         if (!s_ok) break;
         if (threadIdx.x == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;");
-            // planes: 0 Ar_hi 1 Ar_lo 2 Ai_hi 3 Ai_lo | 4 Br_hi 5 Br_lo 6 Bi_hi 7 Bi_lo
-            const uint32_t base = tc_smem(tiles);
-            const uint32_t re = tmem, im = tmem + 128u;
+            // planes: A 0 Ar_hi 1 Ar_lo 2 Ai_hi 3 Ai_lo | B 0 Br_hi 1 Br_lo 2 Bi_hi 3 Bi_lo
+            const uint32_t abase = tc_smem(a_tiles), bbase = tc_smem(b_tiles);
+            const uint32_t re = tmem, im = tmem + kTcN;
             for (uint32_t s = 0; s < kTcK / 8; ++s) {
-                auto d = [&](uint32_t q) { return tc_desc(base + q * kTcTileWords * 4u + s * 256u); };
-                const uint32_t first = (kt == 0 && s == 0) ? 0u : 1u;
-                tc_mma(re, d(0), d(4), kTcIdesc, first);
-                tc_mma(re, d(0), d(5), kTcIdesc, 1u);
-                tc_mma(re, d(1), d(4), kTcIdesc, 1u);
-                tc_mma(re, d(2), d(6), kTcIdescNegA, 1u);
-                tc_mma(re, d(2), d(7), kTcIdescNegA, 1u);
-                tc_mma(re, d(3), d(6), kTcIdescNegA, 1u);
-                tc_mma(im, d(0), d(6), kTcIdesc, first);
-                tc_mma(im, d(0), d(7), kTcIdesc, 1u);
-                tc_mma(im, d(1), d(6), kTcIdesc, 1u);
-                tc_mma(im, d(2), d(4), kTcIdesc, 1u);
-                tc_mma(im, d(2), d(5), kTcIdesc, 1u);
-                tc_mma(im, d(3), d(4), kTcIdesc, 1u);
+                auto da = [&](uint32_t q) { return tc_desc(abase + q * kTcAWords * 4u + s * 256u); };
+                auto db = [&](uint32_t q) { return tc_desc(bbase + q * kTcBWords * 4u + s * 256u); };
+                const uint32_t first = s == 0 ? 0u : 1u;   // every block starts from zero
+                tc_mma(re, da(0), db(0), kTcIdesc, first);
+                tc_mma(re, da(0), db(1), kTcIdesc, 1u);
+                tc_mma(re, da(1), db(0), kTcIdesc, 1u);
+                tc_mma(re, da(2), db(2), kTcIdescNegA, 1u);
+                tc_mma(re, da(2), db(3), kTcIdescNegA, 1u);
+                tc_mma(re, da(3), db(2), kTcIdescNegA, 1u);
+                tc_mma(im, da(0), db(2), kTcIdesc, first);
+                tc_mma(im, da(0), db(3), kTcIdesc, 1u);
+                tc_mma(im, da(1), db(2), kTcIdesc, 1u);
+                tc_mma(im, da(2), db(0), kTcIdesc, 1u);
+                tc_mma(im, da(2), db(1), kTcIdesc, 1u);
+                tc_mma(im, da(3), db(0), kTcIdesc, 1u);
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mma_bar)
                          : "memory");
         }
-        // the tiles are overwritten by the next block only after the MMAs read them
-        if (!tc_wait(mma_bar, kt & 1u)) {
-            if (threadIdx.x == 0) {
-                atomicOr(status, kTcStatusTimeout);
-                s_ok = 0;
-            }
+        // the block's MMAs are done (tiles free, TMEM written)
+        if (!tc_wait(mma_bar, kt & 1u) && threadIdx.x == 0) {
+            atomicOr(status, kTcStatusTimeout);
+            s_ok = 0;
         }
         __syncthreads();
         if (!s_ok) break;
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    if (s_ok) {
-        // warp w reads TMEM lanes 32w..32w+31: output rows of the tile
-        const uint32_t m = mt * kTcRows + warp * 32u + lane;
-        float2* crow = C + ((uint64_t)f * M + m) * N;
-        for (uint32_t c0 = 0; c0 < 128u; c0 += 8u) {
-            uint32_t r[8], i[8];
-            const uint32_t taddr = tmem + ((warp * 32u) << 16) + c0;
-            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-                           "=r"(r[7])
-                         : "r"(taddr));
-            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                         : "=r"(i[0]), "=r"(i[1]), "=r"(i[2]), "=r"(i[3]), "=r"(i[4]), "=r"(i[5]), "=r"(i[6]),
-                           "=r"(i[7])
-                         : "r"(taddr + 128u));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (m < M) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
 #pragma unroll
-                for (uint32_t j = 0; j < 8; ++j) {
-                    const uint32_t n = nt * kTcRows + c0 + j;
-                    if (n < N) crow[n] = make_float2(__uint_as_float(r[j]), __uint_as_float(i[j]));
-                }
+        for (uint32_t c0 = 0; c0 < kTcN; c0 += 8u) {
+            float v[8];
+            tc_ld8(lane_addr + c0, v);
+#pragma unroll
+            for (uint32_t j = 0; j < 8; ++j) acc_re[c0 + j] += v[j];
+            tc_ld8(lane_addr + kTcN + c0, v);
+#pragma unroll
+            for (uint32_t j = 0; j < 8; ++j) acc_im[c0 + j] += v[j];
+        }
+        // every lane has read the block before the next block's MMAs overwrite it
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+    }
+    if (s_ok) {
+        const uint32_t m = mt * kTcM + warp * 32u + lane;
+        if (m < M) {
+            float2* crow = C + ((uint64_t)f * M + m) * N;
+#pragma unroll
+            for (uint32_t j = 0; j < kTcN; ++j) {
+                const uint32_t n = nt * kTcN + j;
+                if (n < N) crow[n] = make_float2(acc_re[j], acc_im[j]);
             }
         }
     }
@@ -279,7 +306,7 @@ qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restri
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols));
 }
 
-constexpr size_t kTcSmemBytes = 8 * kTcTileWords * 4 + 64;
+constexpr size_t kTcSmemBytes = kTcPlanes * (kTcAWords + kTcBWords) * 4 + 64;
 
 static uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
 
@@ -320,7 +347,7 @@ int qtb_contract_sum_scratch_bytes(int64_t K, int64_t F, int64_t M, int64_t N, i
         *bytes = 16;
         return QTB_OK;
     }
-    const uint64_t Kp = round_up(K, kTcK), Mp = round_up(M, kTcRows), Np = round_up(N, kTcRows);
+    const uint64_t Kp = round_up(K, kTcK), Mp = round_up(M, kTcM), Np = round_up(N, kTcN);
     *bytes = 256 + (uint64_t)F * kTcPlanes * (Mp + Np) * Kp * 4;
     return QTB_OK;
 }
@@ -346,22 +373,22 @@ int qtb_contract_sum_c64(const void* A, const void* B, void* C, int64_t K, int64
         e = cudaGetLastError();
         return e == cudaSuccess ? QTB_OK : cuda_fail_c(e, "contract_sum launch");
     }
-    const uint64_t Kp = round_up(K, kTcK), Mp = round_up(M, kTcRows), Np = round_up(N, kTcRows);
-    if (Mp / kTcRows > 65535 || F > 65535 || Np / kTcRows > (1u << 31) || Kp > (1u << 30))
+    const uint64_t Kp = round_up(K, kTcK), Mp = round_up(M, kTcM), Np = round_up(N, kTcN);
+    if (Mp / kTcM > 65535 || F > 65535 || Np / kTcN > (1u << 31) || Kp > (1u << 30))
         return fail(QTB_ERR_UNSUPPORTED, "contract_sum: shape beyond the tensor-core grid");
     int* status = static_cast<int*>(scratch);
     uint32_t* Ap = reinterpret_cast<uint32_t*>(static_cast<char*>(scratch) + 256);
     uint32_t* Bp = Ap + (uint64_t)F * kTcPlanes * Mp * Kp;
     auto split_blocks = [](uint64_t n) { return (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 32); };
     qtb_tc_split_kernel<<<split_blocks((uint64_t)F * Mp * Kp), 256, 0, st>>>(
-        static_cast<const float2*>(A), Ap, (uint32_t)K, (uint32_t)F, (uint32_t)M, (uint32_t)Mp, (uint32_t)Kp);
+        static_cast<const float2*>(A), Ap, (uint32_t)K, (uint32_t)F, (uint32_t)M, (uint32_t)Mp, (uint32_t)Kp, kTcM);
     qtb_tc_split_kernel<<<split_blocks((uint64_t)F * Np * Kp), 256, 0, st>>>(
-        static_cast<const float2*>(B), Bp, (uint32_t)K, (uint32_t)F, (uint32_t)N, (uint32_t)Np, (uint32_t)Kp);
+        static_cast<const float2*>(B), Bp, (uint32_t)K, (uint32_t)F, (uint32_t)N, (uint32_t)Np, (uint32_t)Kp, kTcN);
     // per device and cheap: set on every call
     e = cudaFuncSetAttribute(qtb_tc_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kTcSmemBytes);
     if (e != cudaSuccess) return cuda_fail_c(e, "contract_sum smem attribute");
-    dim3 grid((unsigned)(Np / kTcRows), (unsigned)(Mp / kTcRows), (unsigned)F);
+    dim3 grid((unsigned)(Np / kTcN), (unsigned)(Mp / kTcM), (unsigned)F);
     qtb_tc_contract_kernel<<<grid, kTcThreads, kTcSmemBytes, st>>>(Ap, Bp, static_cast<float2*>(C), (uint32_t)F,
                                                                   (uint32_t)M, (uint32_t)N, (uint32_t)Mp,
                                                                   (uint32_t)Np, (uint32_t)Kp, status);
