@@ -308,7 +308,9 @@ int qtb_plan_set_autotune(qtb_plan* plan, int32_t enable);
  * threads per CTA, dynamic shared memory bytes, flags: 1 = shared-memory
  * arena, 2 = persistent launch taking networks from a queue, 4 = a wave of
  * wide networks contracted by the whole GPU step by step, arenas in
- * scratch).                                                               */
+ * scratch, 8 = lean persistent queue (registers capped), 16 = warp-per-
+ * network queue, 32 = the 96-thread lean queue, 64 = networks of moderate
+ * size, one thread-block cluster each, arenas in scratch).                */
 int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32_t* n_classes);
 
 /* Device memory the plan holds once uploaded (images, gate table, job

@@ -999,6 +999,97 @@ __global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArg
     }
 }
 
+// ----------------------------------------------------------------- K5
+// Networks too large for shared memory but of moderate size (arenas up to
+// kClusterArenaElems) run one thread-block cluster of kClusterCtas CTAs
+// each: the cluster walks the network's phases, a phase's elements cut into
+// chunks of 2048 that the cluster's CTAs take in turn, and phases are
+// separated by the cluster barrier (release/acquire at cluster scope, after
+// a fence for the arena in global memory).  A cluster's CTAs are scheduled
+// together by the hardware, so the barrier needs no flag and no co-residency
+// assumption, unlike the grid-wide steps of K4; a network's critical path
+// is its phase chain at cluster-barrier latency, and the networks of a run
+// proceed independently.  The arena lives in global memory (read with
+// ld.cg: another CTA wrote it), the plan blob is read through the read-only
+// path.  A chunk that lies within one op of at least 2048 elements is
+// computed with the batched loads of K4 (eight elements per thread).
+struct ClusterJob {
+    const DevNetRun* run;
+    float2* term;
+    uint64_t arena_off;     // complex64 elements into the cluster arenas
+    uint64_t pad;
+};
+static_assert(sizeof(ClusterJob) == 32, "ClusterJob layout");
+constexpr int kClusterCtas = 8;
+constexpr int kClusterThreads = 256;
+constexpr uint32_t kClusterChunk = 2048;                     // elements per CTA turn (8 per thread)
+constexpr uint32_t kClusterArenaElems = 1u << 22;            // 32 MB arenas and below
+
+__global__ void __launch_bounds__(kClusterThreads) qtb_cluster_kernel(const ClusterJob* __restrict__ jobs,
+                                                                      float2* __restrict__ arenas, const RunArgs a) {
+    uint32_t rank, nctas;
+    asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    asm("mov.u32 %0, %%cluster_nctarank;" : "=r"(nctas));
+    __shared__ int s_last;
+    const ClusterJob job = jobs[blockIdx.x / nctas];
+    const DevNetRun net = *job.run;
+    const unsigned char* blob = reinterpret_cast<const unsigned char*>(a.blobs + net.blob_off16);
+    const DevOp* ops = reinterpret_cast<const DevOp*>(blob + net.n_phases * sizeof(DevPhase));
+    const DevIn* ins = reinterpret_cast<const DevIn*>(blob + net.ins_off);
+    float2* arena = arenas + job.arena_off;
+    const uint32_t t = threadIdx.x;
+    for (uint32_t p = 0; p < net.n_phases; ++p) {
+        const uint4 pv = __ldg(reinterpret_cast<const uint4*>(blob) + p);
+        const uint32_t op_first = pv.x, op_count = pv.y, total = pv.z;
+        const uint16_t* chunk = reinterpret_cast<const uint16_t*>(blob + pv.w);
+        const uint32_t op_last = op_first + op_count - 1u;
+        auto load = [&](uint32_t i) { return ldg_op(ops + min(i, op_last)); };
+        for (uint32_t base = rank * kClusterChunk; base < total; base += nctas * kClusterChunk) {
+            uint32_t oi = __ldg(chunk + base / kChunkElems);
+            DevOp op = ldg_op(ops + oi);
+            oi = find_op(base, oi, op, load);
+            const uint32_t size = 1u << (op.u - op.sum);
+            if (size >= kClusterChunk && base + kClusterChunk <= total) {
+                // the whole chunk lies in this op (ops start at multiples of their size)
+                compute_elements_wide(op, base + t - op.elem_begin, ins, a.gtable, arena);
+            } else {
+                uint32_t op_hi = op.elem_begin + size;
+#pragma unroll 1
+                for (uint32_t e = 0; e < kClusterChunk / kClusterThreads; ++e) {
+                    const uint32_t g = base + t + e * kClusterThreads;
+                    if (g >= total) break;
+                    if (g >= op_hi) {
+                        oi = __ldg(chunk + g / kChunkElems);
+                        op = ldg_op(ops + oi);
+                        oi = find_op(g, oi, op, load);
+                        op_hi = op.elem_begin + (1u << (op.u - op.sum));
+                    }
+                    compute_element_wide(op, g - op.elem_begin, ins, a.gtable, arena);
+                }
+            }
+        }
+        // every write of the phase is visible to the whole cluster before the next phase reads it
+        __threadfence();
+        asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+    }
+    if (rank != 0) return;
+    if (t == 0) {
+        *job.term = (net.result_src & kSrcTable) ? __ldg(a.gtable + (net.result_src & ~kSrcTable))
+                                                 : __ldcg(arena + net.result_src);
+        s_last = 0;
+        if (a.energy) {
+            __threadfence();
+            s_last = atomicAdd(a.done, 1u) == a.total_jobs - 1u;
+        }
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        reduce_energy(a.terms, a.total_jobs, a.energy_groups, a.energy);
+        if (t == 0) *a.done = 0u;
+    }
+}
+
 // ----------------------------------------------------------------- host
 static int cuda_fail(cudaError_t e, const char* what) {
     return fail(QTB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -1082,7 +1173,10 @@ struct RunCache {
     std::vector<WideWave> waves;        // wide networks (both schedules), run one after another
     void* wide_buf = nullptr;
     size_t counters_bytes = 0;          // counters of all waves, zeroed before a run
-    size_t scratch_elems = 0;           // arenas of the largest wave
+    size_t scratch_elems = 0;           // arenas of the largest wave, then the cluster arenas
+    void* cl_jobs = nullptr;            // ClusterJob per network of moderate size (K5)
+    int n_cl = 0;
+    size_t cl_arena_off = 0;            // elements into scratch where the cluster arenas start
     bool smem_table = true;
     double n_groups = 0.0;              // distinct circuits among the range's networks
 };
@@ -1129,8 +1223,10 @@ static int hybrid_lean_grid(std::vector<LaunchClass>& sched, bool smem_table);
 static void free_run(RunCache* rc) {
     if (rc->jobs) cudaFree(rc->jobs);
     if (rc->wide_buf) cudaFree(rc->wide_buf);
+    if (rc->cl_jobs) cudaFree(rc->cl_jobs);
     rc->jobs = nullptr;
     rc->wide_buf = nullptr;
+    rc->cl_jobs = nullptr;
 }
 
 static void free_device(qtb_plan* plan) {
@@ -1652,7 +1748,34 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
             rc->wclasses.push_back(lc);
         }
     }
-    if (!device) return build_waves(plan, members[kSmemClasses], first, terms, rc, false);
+    // networks too large for shared memory: moderate arenas run as clusters
+    // (K5), the rest as whole-GPU waves (K4)
+    std::vector<int32_t> wave_nets, cl_nets;
+    for (int32_t i : members[kSmemClasses])
+        (plan->druns[i].arena_elems <= kClusterArenaElems ? cl_nets : wave_nets).push_back(i);
+    auto place_clusters = [&](bool on_device) -> int {
+        rc->n_cl = (int)cl_nets.size();
+        rc->cl_arena_off = (rc->scratch_elems + 63) & ~size_t(63);
+        std::vector<ClusterJob> cj;
+        size_t off = 0;
+        for (int32_t i : cl_nets) {
+            ClusterJob j{};
+            j.run = runs ? runs + i : nullptr;
+            j.term = terms + (i - first);
+            j.arena_off = rc->cl_arena_off + off;
+            off += ((size_t)plan->druns[i].arena_elems + 63) & ~size_t(63);
+            cj.push_back(j);
+        }
+        if (!cj.empty()) rc->scratch_elems = rc->cl_arena_off + off;
+        if (!on_device || cj.empty()) return QTB_OK;
+        QTB_CUDA(cudaMalloc(&rc->cl_jobs, cj.size() * sizeof(ClusterJob)));
+        QTB_CUDA(cudaMemcpy(rc->cl_jobs, cj.data(), cj.size() * sizeof(ClusterJob), cudaMemcpyHostToDevice));
+        return QTB_OK;
+    };
+    if (!device) {
+        int r = build_waves(plan, wave_nets, first, terms, rc, false);
+        return r ? r : place_clusters(false);
+    }
     // jobs of both schedules, then 16 bytes of counters (done, queue), zeroed
     const size_t job_bytes = jobs.size() * sizeof(Job);
     void* buf = nullptr;
@@ -1679,7 +1802,8 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
         int r = hybrid_lean_grid(rc->wclasses, rc->smem_table);
         if (r) return r;
     }
-    return build_waves(plan, members[kSmemClasses], first, terms, rc, true);
+    int rw = build_waves(plan, wave_nets, first, terms, rc, true);
+    return rw ? rw : place_clusters(true);
 }
 
 }  // namespace qtb
@@ -1799,6 +1923,22 @@ static int ensure_streams(qtb_plan_device* s);
 // The wide waves of a run, one after another on st: counters zeroed, then
 // one K4 launch per wave over the shared arena scratch.
 static int launch_waves(const RunCache* rc, const RunArgs& base, void* scratch_dev, cudaStream_t st) {
+    if (rc->n_cl > 0) {
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3((unsigned)(rc->n_cl * kClusterCtas));
+        cfg.blockDim = dim3(kClusterThreads);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = kClusterCtas;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        QTB_CUDA(cudaLaunchKernelEx(&cfg, qtb_cluster_kernel, static_cast<const ClusterJob*>(rc->cl_jobs),
+                                    static_cast<float2*>(scratch_dev), base));
+    }
     if (rc->waves.empty()) return QTB_OK;
     char* buf = static_cast<char*>(rc->wide_buf);
     QTB_CUDA(cudaMemsetAsync(buf + rc->waves[0].counters_off, 0, rc->counters_bytes, st));
@@ -1828,7 +1968,7 @@ static int launch_schedule(qtb_plan_device* s, const RunCache* rc,
     if (r) return r;
     for (const LaunchClass& lc : sched)
         if (lc.persistent) QTB_CUDA(cudaMemsetAsync(rc->queue, 0, sizeof(unsigned int), st));
-    const bool waves = with_waves && !rc->waves.empty();
+    const bool waves = with_waves && (!rc->waves.empty() || rc->n_cl > 0);
     const bool forked = sched.size() + (waves ? 1 : 0) > 1;
     if (forked) QTB_CUDA(cudaEventRecord(s->fork, st));
     if (waves) {
@@ -2136,7 +2276,7 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
     a.energy = energy_dev;
     a.energy_groups = rc->n_groups;
     const int n_entries = (int)plan->entries.size();
-    if ((!rc->smem_table || !rc->waves.empty()) && n_entries > 0) {
+    if ((!rc->smem_table || !rc->waves.empty() || rc->n_cl > 0) && n_entries > 0) {
         qtb_table_kernel<<<(n_entries + 127) / 128, 128, 0, st>>>(
             static_cast<const DevEntry*>(plan->dev.entries), n_entries,
             static_cast<const DevTerm*>(plan->dev.terms), params_dev,
@@ -2167,7 +2307,7 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
     if (s->timing) {
         QTB_CUDA(cudaEventRecord(ev.second, st));
         s->pending.push_back(ev);
-        s->kernel_launches += (int64_t)(sched.size() + rc->waves.size());
+        s->kernel_launches += (int64_t)(sched.size() + rc->waves.size() + (rc->n_cl > 0 ? 1 : 0));
     }
     return QTB_OK;
 }
@@ -2455,7 +2595,7 @@ int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32
         return QTB_OK;
     }
     const std::vector<LaunchClass>& sched = schedule_of(rc);
-    *n_classes = (int32_t)(sched.size() + rc->waves.size());
+    *n_classes = (int32_t)(sched.size() + rc->waves.size() + (rc->n_cl > 0 ? 1 : 0));
     if (!out) return QTB_OK;
     for (int32_t c = 0; c < *n_classes && 4 * c + 3 < cap; ++c) {
         if (c < (int32_t)sched.size()) {
@@ -2465,12 +2605,17 @@ int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32
             out[4 * c + 2] = (int32_t)lc.smem_bytes;
             out[4 * c + 3] = (lc.smem ? 1 : 0) | (lc.persistent ? 2 : 0) | (lc.lean ? 8 : 0) | (lc.warp ? 16 : 0) |
                              (lc.lean == 2 ? 32 : 0);
-        } else {
+        } else if (c < (int32_t)(sched.size() + rc->waves.size())) {
             const WideWave& wv = rc->waves[c - sched.size()];
             out[4 * c] = (int32_t)wv.n_nets;
             out[4 * c + 1] = kWideThreads;
             out[4 * c + 2] = 0;
             out[4 * c + 3] = 4;
+        } else {   // the cluster launch (one cluster of kClusterCtas CTAs per network)
+            out[4 * c] = rc->n_cl;
+            out[4 * c + 1] = kClusterThreads;
+            out[4 * c + 2] = 0;
+            out[4 * c + 3] = 64;
         }
     }
     return QTB_OK;

@@ -95,11 +95,17 @@ def test_contract_rejects_bad_shapes_and_host_tensors(cuda_device):
 def test_extended_backend_replays_reference_driver(cuda_device, name, mode):
     """The reference driver's recorded backend calls through
     B200ExtendedBackend (mode 'tensor' sends every contract-sum of the
-    buckets to the tcgen05 path): every result and amplitude matches the
-    recorded NumpyBackend values."""
+    buckets to the tcgen05 path): every amplitude matches the recorded
+    NumpyBackend value within 1e-5, and so does every intermediate result
+    on the CUDA-core path.  On the tensor-core path an intermediate may sit
+    up to 5e-5 (relative squared norm) from the recorded one: each 3xTF32
+    contraction is within about 2^-22 of complex64 (the dropped lo x lo
+    term, round-toward-zero inside a k block), and a network chains about
+    130 of them before its scalar result."""
     from qtensor_b200.backend import B200ExtendedBackend
     w = dropin_replay.load()[name]
     be = B200ExtendedBackend(mode=mode)
+    mid_tol = TOL if mode != 'tensor' else 5 * TOL
     for rec in w['edges']:
         def check(k, res, rec=rec):
             call = rec['calls'][k]
@@ -107,8 +113,8 @@ def test_extended_backend_replays_reference_driver(cuda_device, name, mode):
             assert [dropin_replay.var_rec(v) for v in res.indices] == call['indices']
             got = res.data.detach().cpu().numpy().astype(np.complex128).reshape(-1)
             if 'data' in call:
-                assert np.max(np.abs(got - [complex(*z) for z in call['data']])) < TOL
+                assert np.max(np.abs(got - [complex(*z) for z in call['data']])) < mid_tol
             else:
-                assert abs(np.sum(np.abs(got) ** 2) - call['norm2']) < TOL * max(1.0, call['norm2'])
+                assert abs(np.sum(np.abs(got) ** 2) - call['norm2']) < mid_tol * max(1.0, call['norm2'])
         amp, _ = dropin_replay.replay_edge(be, rec, check=check)
         assert np.max(np.abs(amp - [complex(*z) for z in rec['amplitude']])) < TOL
