@@ -1750,9 +1750,13 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
     }
     // networks too large for shared memory: moderate arenas run as clusters
     // (K5), the rest as whole-GPU waves (K4)
+    // QTB_CLUSTER_MAX_ELEMS in the environment moves the limit (0: every
+    // such network in waves), so that both executors can be exercised
     std::vector<int32_t> wave_nets, cl_nets;
+    uint64_t cl_max = kClusterArenaElems;
+    if (const char* env = std::getenv("QTB_CLUSTER_MAX_ELEMS")) cl_max = std::strtoull(env, nullptr, 10);
     for (int32_t i : members[kSmemClasses])
-        (plan->druns[i].arena_elems <= kClusterArenaElems ? cl_nets : wave_nets).push_back(i);
+        (plan->druns[i].arena_elems <= cl_max ? cl_nets : wave_nets).push_back(i);
     auto place_clusters = [&](bool on_device) -> int {
         rc->n_cl = (int)cl_nets.size();
         rc->cl_arena_off = (rc->scratch_elems + 63) & ~size_t(63);

@@ -4,7 +4,8 @@ amount of work and checks its result, so that the same command can run once
 without the profiler and then under it.
 
     python tests/profile_workloads.py cfg3        # 3-regular N=1000 p=3, 20 executor steps
-    python tests/profile_workloads.py er400       # Erdos-Renyi N=400 p=3 (wide waves), 3 runs
+    python tests/profile_workloads.py er400       # Erdos-Renyi N=400 p=3 (wide networks), 3 runs
+    python tests/profile_workloads.py cfg4        # 3-regular N=256 p=4, 5 executor steps
     python tests/profile_workloads.py bucket24    # one 24-variable bucket through qtb_bucket_c64, 5 runs
     python tests/profile_workloads.py plain_cfg1  # 3-regular N=20 p=1 through the plain per-bucket path
     python tests/profile_workloads.py aux         # allocation-free run (N=100 p=3) and the wait self-test
@@ -37,6 +38,21 @@ def cfg3():
     cg.params.copy_(torch.from_numpy(np.concatenate([w['gamma'], w['beta']])))
     graph = cg.device_graph()
     for _ in range(20):
+        graph.replay()
+    torch.cuda.synchronize()
+    E = float(cg.energy.cpu()[0])
+    assert abs(E - w['energy']) <= 1e-5 * abs(w['energy']), (E, w['energy'])
+    assert cg.plan.device_status() == 0
+    print('launch classes', cg.plan.last_launch_config())
+
+
+def cfg4():
+    G, w = golden_graph('cfg4')
+    eng = QAOAEnergyEngine()
+    cg = eng.compile(G, 4, w['gamma'], w['beta'])
+    cg.params.copy_(torch.from_numpy(np.concatenate([w['gamma'], w['beta']])))
+    graph = cg.device_graph()
+    for _ in range(5):
         graph.replay()
     torch.cuda.synchronize()
     E = float(cg.energy.cpu()[0])
@@ -166,6 +182,6 @@ def contract():
 
 
 if __name__ == '__main__':
-    {'cfg3': cfg3, 'er400': er400, 'bucket24': bucket24, 'plain_cfg1': plain_cfg1,
+    {'cfg3': cfg3, 'cfg4': cfg4, 'er400': er400, 'bucket24': bucket24, 'plain_cfg1': plain_cfg1,
      'aux': aux, 'contract': contract}[sys.argv[1]]()
     print('ok', sys.argv[1])

@@ -159,21 +159,31 @@ def test_plain_path_matches_batched_and_reference(cuda_device, name, max_width):
     assert eng.compile(G, len(w['gamma']), w['gamma'], w['beta']).plan.device_status() == 0
 
 
-def test_wide_waves_match_plain_path(cuda_device):
+@pytest.mark.parametrize('cluster_max', [None, '0'])
+def test_wide_networks_match_plain_path(cuda_device, monkeypatch, cluster_max):
     """Erdos-Renyi N=400 p=3 (seed 24323709) with the reference's greedy rule
     alone (order_trials=0, slicing from width 22): 247 networks too large
-    for shared memory (3.5 GB of arenas) run as several whole-GPU waves next
-    to the shared-memory classes; every edge term equals the plain
-    per-bucket path's (an independent execution of the same plans) and the
-    energies agree."""
+    for shared memory (3.5 GB of arenas) run beside the shared-memory
+    classes, by default as one thread-block cluster each when their arena
+    is at most 32 MB (K5) and in whole-GPU waves above (K4), and with
+    QTB_CLUSTER_MAX_ELEMS=0 all in waves; either way every edge term equals
+    the plain per-bucket path's (an independent execution of the same
+    plans) and the energies agree."""
     import networkx as nx
+    if cluster_max is not None:
+        monkeypatch.setenv('QTB_CLUSTER_MAX_ELEMS', cluster_max)
     G = nx.erdos_renyi_graph(400, 3 / 399, seed=24323709)
     gamma, beta = graphs.angles(3, seed=1)
     eng = _engine(max_width=22, order_trials=0)
     batched = eng.edge_terms(G, gamma, beta)
     cg = eng.compile(G, 3, gamma, beta)
-    waves = [c for c in cg.plan.last_launch_config() if c[3] & 4]
-    assert len(waves) >= 2
+    cfg = cg.plan.last_launch_config()
+    waves = [c for c in cfg if c[3] & 4]
+    clusters = [c for c in cfg if c[3] & 64]
+    if cluster_max == '0':
+        assert len(waves) >= 2 and not clusters
+    else:
+        assert clusters and clusters[0][0] >= 100
     plain = eng.edge_terms(G, gamma, beta, path='plain')
     assert np.max(np.abs(batched - plain)) < TOL
     E = eng.energy_expectation(G, gamma, beta)

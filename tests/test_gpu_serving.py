@@ -38,21 +38,49 @@ def test_server_matches_reference(cuda_device):
     assert res.submitted <= res.compiled <= res.admitted <= res.finished
 
 
+def _wide_requests():
+    """Two wide requests of the serving stream: Erdos-Renyi N=400 p=3, whose
+    networks too large for shared memory run on the cluster executor, and
+    Erdos-Renyi N=335 p=3 (seed 949594894), whose widest edge (width 28,
+    arenas of about 5 GB) runs in whole-GPU waves."""
+    er400 = nx.erdos_renyi_graph(400, 3 / 399, seed=24323709)
+    er335 = graphs.erdos_renyi(graphs.ER_P3_N335['n'], graphs.ER_P3_N335['seed'])
+    return [(er400,) + tuple(graphs.angles(3, seed=1)), (er335,) + tuple(graphs.angles(3, seed=2))]
+
+
 def test_alone_and_in_the_mix_agree(cuda_device):
     """Each request's energy is identical whether it runs alone (one stream,
     one request at a time) or together with the others (four streams, all
-    submitted at once), and equals the oracle's."""
+    submitted at once), and equals the oracle's.  The mix holds small
+    requests and two wide ones (cluster executor and wide waves), whose
+    kernels overlap the others'."""
     from qtensor_b200.serve import QAOAServer
     reqs = _requests(14)
+    reqs = reqs[:7] + _wide_requests() + reqs[7:]
     with QAOAServer(n_streams=1) as srv:
-        alone = [srv.submit(*r).result(timeout=120).energy for r in reqs]
+        alone = [srv.submit(*r).result(timeout=300) for r in reqs]
     with QAOAServer(n_streams=4) as srv:
         futs = [srv.submit(*r) for r in reqs]
-        mixed = [f.result(timeout=120).energy for f in futs]
-    assert alone == mixed
-    for (G, gamma, beta), e in list(zip(reqs, mixed))[:4]:
+        mixed = [f.result(timeout=300) for f in futs]
+    assert [r.energy for r in alone] == [r.energy for r in mixed]
+    assert max(r.networks for r in mixed) > 0
+    for (G, gamma, beta), r in list(zip(reqs, mixed))[:4]:
         ref = float(port.energy_expectation(G, gamma, beta)[0])
-        assert abs(e - ref) <= 1e-5 * max(1.0, abs(ref))
+        assert abs(r.energy - ref) <= 1e-5 * max(1.0, abs(ref))
+
+
+def test_wide_requests_run_on_the_wide_executors(cuda_device):
+    """The wide requests of the mix really use the cluster executor (K5) and
+    the wide waves (K4): their plans' launch classes say so."""
+    from qtensor_b200.engine import QAOAEnergyEngine
+    eng = QAOAEnergyEngine(order_trials=4)
+    flags = []
+    for G, gamma, beta in _wide_requests():
+        eng.energy_expectation(G, gamma, beta)
+        cg = eng.compile(G, 3, gamma, beta)
+        flags.append([c[3] for c in cg.plan.last_launch_config()])
+    assert any(f & 64 for f in flags[0])
+    assert any(f & 4 for f in flags[1])
 
 
 def test_failing_request_fails_alone(cuda_device):
