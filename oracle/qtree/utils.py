@@ -30,10 +30,20 @@ def get_einsum_expr(idx1, idx2):
 
 
 def unravel_index(value, dimensions):
-    """Mixed-radix digits of ``value``, most significant first (numpy order)."""
-    if len(dimensions) == 0:
-        return ()
-    return tuple(int(x) for x in np.unravel_index(int(value), tuple(dimensions)))
+    """Mixed-radix digits of ``value``, most significant first (the order of
+    ``numpy.unravel_index``, computed here for any number of dimensions:
+    lightcones of more than 64 qubits exceed numpy's array rank)."""
+    value = int(value)
+    total = 1
+    for d in dimensions:
+        total *= int(d)
+    if not 0 <= value < max(total, 1):
+        raise ValueError('index {} out of range for dimensions {}'.format(value, tuple(dimensions)))
+    digits = []
+    for d in reversed(dimensions):
+        value, r = divmod(value, int(d))
+        digits.append(r)
+    return tuple(reversed(digits))
 
 
 def slice_from_bits(value, variables):

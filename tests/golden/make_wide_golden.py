@@ -6,10 +6,10 @@ reference greedy width of 31 and more, and the engine compiles them only by
 slicing.  The port of the reference's path (``oracle/qtensor_port.py``: the
 reference's circuits, bucket layout, greedy order and NumpyBackend einsum
 in complex128) contracts every edge whose reference greedy width is at most
-``PORT_MAX_WIDTH`` (2^24 complex128 = 256 MB tensors); their terms go to
-``wide_request_reference.json``, with each edge's reference width.  Edges
-above that width are listed without terms (the port would need tensors of
-2^31 elements and more).
+``PORT_MAX_WIDTH`` (2^26 complex128 = 1 GB tensors; the widest ones two at a
+time to bound host memory); their terms go to ``wide_request_reference.json``,
+with each edge's reference width.  Edges above that width (28 to 35) are
+listed without terms: the port would need tensors of 2^28 to 2^35 elements.
 
     python tests/golden/make_wide_golden.py
 """
@@ -30,7 +30,8 @@ import graphs  # noqa: E402
 import qtensor_port as port  # noqa: E402
 
 GRAPH = dict(n=213, seed=796350419, p=3, angle_seed=656419913)
-PORT_MAX_WIDTH = 24
+PORT_MAX_WIDTH = 26
+SMALL_WIDTH = 24
 
 
 def request():
@@ -58,8 +59,12 @@ def main():
     t0 = time.time()
     with get_context('spawn').Pool(os.cpu_count()) as pool:
         widths = pool.map(edge_width, [(G, gamma, beta, e) for e in edges])
-        todo = [i for i, w in enumerate(widths) if w <= PORT_MAX_WIDTH]
-        terms = pool.map(edge_term, [(G, gamma, beta, edges[i]) for i in todo], chunksize=1)
+        small = [i for i, w in enumerate(widths) if w <= SMALL_WIDTH]
+        terms = pool.map(edge_term, [(G, gamma, beta, edges[i]) for i in small], chunksize=1)
+    large = [i for i, w in enumerate(widths) if SMALL_WIDTH < w <= PORT_MAX_WIDTH]
+    with get_context('spawn').Pool(2) as pool:
+        terms += pool.map(edge_term, [(G, gamma, beta, edges[i]) for i in large], chunksize=1)
+    todo = small + large
     out = {'generator': 'tests/golden/make_wide_golden.py', 'graph': GRAPH, 'gamma': gamma, 'beta': beta,
            'edges': [list(e) for e in edges], 'widths': widths, 'port_max_width': PORT_MAX_WIDTH,
            'terms': {str(i): [t.real, t.imag] for i, t in zip(todo, terms)}}

@@ -109,3 +109,31 @@ def test_golden_fixture_is_complete():
     names = set(golden())
     for want in ('cfg1_default', 'cfg1_cx', 'cfg1_zz', 'cfg2', 'cfg3', 'cfg4', 'petersen_p9'):
         assert want in names
+
+
+def test_slice_digits_beyond_numpy_rank():
+    """The oracle's slice_from_bits serves lightcones of more than 64 qubits
+    (numpy's unravel_index stops at 64 dimensions) with the same digits."""
+    from qtree.utils import unravel_index
+    for v, dims in ((0, (2, 2, 2)), (5, (2, 2, 2)), (7, (2, 3, 2)), (23, (3, 4, 2))):
+        assert unravel_index(v, dims) == tuple(int(x) for x in np.unravel_index(v, dims))
+    assert unravel_index(0, (2,) * 89) == (0,) * 89
+    assert unravel_index(2 ** 88 + 1, (2,) * 89) == (1,) + (0,) * 87 + (1,)
+
+
+def test_wide_request_fixture_rebuilds():
+    """The wide serving request of tests/golden/wide_request_reference.json
+    is rebuilt from its seeds, and its recorded widths are the reference
+    greedy widths of the port."""
+    import json
+    import os
+    from conftest import ROOT
+    with open(os.path.join(ROOT, 'tests', 'golden', 'wide_request_reference.json')) as f:
+        w = json.load(f)
+    G = graphs.erdos_renyi(w['graph']['n'], w['graph']['seed'])
+    assert [list(e) for e in G.edges()] == w['edges']
+    assert list(graphs.angles(3, w['graph']['angle_seed'])[0]) == w['gamma']
+    for i in (0, 1, 2):
+        circ = port.lightcone_circuit(G, tuple(w['edges'][i]), w['gamma'], w['beta'])
+        buckets, _, bra, ket = port.circuit_to_network(circ)
+        assert port.order_network(buckets, bra, ket)[1] == w['widths'][i]
