@@ -291,6 +291,11 @@ def _rejections(results):
     return out
 
 
+def _available_cpus():
+    from qtensor_b200._lib import available_cpus
+    return available_cpus()
+
+
 def summarize_serving(results, wall):
     ok = [r for r in results if not isinstance(r, Exception)]
     lat = np.array([r.latency for r in ok]) * 1e3
@@ -301,7 +306,9 @@ def summarize_serving(results, wall):
            'edge_terms_per_s': edges / wall if wall > 0 else None, 'wall_s': wall}
     # where the median request's time went
     for name in ('compile_s', 'wait_s', 'gpu_s'):
-        out['p50_' + name[:-2] + '_ms'] = _pct(np.array([getattr(r, name) for r in ok]) * 1e3, 50)
+        vals = np.array([getattr(r, name) for r in ok]) * 1e3
+        out['p50_' + name[:-2] + '_ms'] = _pct(vals, 50)
+        out['max_' + name[:-2] + '_ms'] = float(vals.max()) if len(vals) else None
     return out
 
 
@@ -407,7 +414,9 @@ def run_serving(n_requests, rate, device_index, plain_budget_s=20.0):
         if isinstance(a, Exception) or isinstance(b, Exception):
             return isinstance(a, Exception) and isinstance(b, Exception)
         return a.energy == b.energy
-    return {'workload': '{} requests: 3-regular or Erdos-Renyi (mean degree 3), N U[16,500], '
+    host = {'os_cpu_count': os.cpu_count(), 'available_cpus': _available_cpus()}
+    return {'host_cpus': host,
+            'workload': '{} requests: 3-regular or Erdos-Renyi (mean degree 3), N U[16,500], '
                         'p U[1,4], angles U[0,pi) (seed 0); Poisson arrivals at {} req/s '
                         '(seed 1); slicing from width 29, at most 1024 slices per edge, at most '
                         '{:.0e} algorithmic bytes per request'.format(len(reqs), rate, budget),

@@ -165,6 +165,35 @@ def lib():
     return _lib
 
 
+def available_cpus():
+    """CPUs this process may run on: its affinity mask, bounded by a cgroup
+    CPU quota (cgroup v2 ``cpu.max`` or v1 ``cpu.cfs_quota_us``); in a
+    container ``os.cpu_count()`` reports the host's."""
+    try:
+        n = len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        n = os.cpu_count() or 1
+    quota = None
+    try:
+        with open('/sys/fs/cgroup/cpu.max') as f:
+            q, period = f.read().split()[:2]
+            if q != 'max':
+                quota = float(q) / float(period)
+    except (OSError, ValueError):
+        try:
+            with open('/sys/fs/cgroup/cpu/cpu.cfs_quota_us') as f:
+                q = float(f.read())
+            with open('/sys/fs/cgroup/cpu/cpu.cfs_period_us') as f:
+                period = float(f.read())
+            if q > 0 and period > 0:
+                quota = q / period
+        except (OSError, ValueError):
+            pass
+    if quota:
+        n = min(n, max(1, int(-(-quota // 1))))
+    return max(1, n)
+
+
 def last_error():
     buf = ctypes.create_string_buffer(1024)
     lib().qtb_last_error(buf, len(buf))

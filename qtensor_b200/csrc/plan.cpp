@@ -26,6 +26,8 @@
 #include <tuple>
 #include <unordered_map>
 
+#include <sched.h>
+
 #include "plan.h"
 
 namespace qtb {
@@ -1866,7 +1868,46 @@ using namespace qtb;
 // (256 MiB); past it, edges are compiled without sharing.
 constexpr size_t kShareKeyLimit = size_t(1) << 26;
 
-// Runs fn(i) for i in [0, n) on up to n_threads threads (0 = all cores).
+// CPUs this process may run on: the hardware threads, bounded by its
+// affinity mask and by a cgroup CPU quota (cgroup v2 cpu.max, v1
+// cfs_quota_us / cfs_period_us).  In a container the hardware count is the
+// host's; threads beyond the quota are throttled in bursts, which showed as
+// compile latencies of seconds.
+static int available_cpus() {
+    static const int n = [] {
+        int c = (int)std::max(1u, std::thread::hardware_concurrency());
+        cpu_set_t set;
+        CPU_ZERO(&set);
+        if (sched_getaffinity(0, sizeof(set), &set) == 0) c = std::min(c, std::max(1, CPU_COUNT(&set)));
+        auto quota_cpus = [](double quota, double period) {
+            return (quota > 0 && period > 0) ? std::max(1, (int)std::ceil(quota / period)) : 0;
+        };
+        if (FILE* f = std::fopen("/sys/fs/cgroup/cpu.max", "r")) {
+            char q[32] = {0};
+            double period = 0;
+            if (std::fscanf(f, "%31s %lf", q, &period) == 2 && std::strcmp(q, "max") != 0) {
+                const int qc = quota_cpus(std::atof(q), period);
+                if (qc) c = std::min(c, qc);
+            }
+            std::fclose(f);
+        } else if (FILE* fq = std::fopen("/sys/fs/cgroup/cpu/cpu.cfs_quota_us", "r")) {
+            double quota = -1, period = 0;
+            if (std::fscanf(fq, "%lf", &quota) != 1) quota = -1;
+            std::fclose(fq);
+            if (FILE* fp = std::fopen("/sys/fs/cgroup/cpu/cpu.cfs_period_us", "r")) {
+                if (std::fscanf(fp, "%lf", &period) != 1) period = 0;
+                std::fclose(fp);
+            }
+            const int qc = quota_cpus(quota, period);
+            if (qc) c = std::min(c, qc);
+        }
+        return c;
+    }();
+    return n;
+}
+
+// Runs fn(i) for i in [0, n) on up to n_threads threads (0 = every CPU the
+// process may use).
 namespace qtb {
 template <typename Fn>
 static void parallel_for(int32_t n, int32_t n_threads, Fn fn) {
@@ -1874,7 +1915,7 @@ static void parallel_for(int32_t n, int32_t n_threads, Fn fn) {
     auto worker = [&]() {
         for (int32_t i; (i = next.fetch_add(1)) < n;) fn(i);
     };
-    int nt = n_threads > 0 ? n_threads : (int)std::thread::hardware_concurrency();
+    int nt = n_threads > 0 ? n_threads : available_cpus();
     nt = std::max(1, std::min(nt, std::max(1, n)));
     std::vector<std::thread> pool;
     for (int t = 1; t < nt; ++t) pool.emplace_back(worker);

@@ -1176,6 +1176,7 @@ struct RunCache {
     size_t scratch_elems = 0;           // arenas of the largest wave, then the cluster arenas
     void* cl_jobs = nullptr;            // ClusterJob per network of moderate size (K5)
     int n_cl = 0;
+    int cl_ctas = 8;                    // CTAs per cluster
     size_t cl_arena_off = 0;            // elements into scratch where the cluster arenas start
     bool smem_table = true;
     double n_groups = 0.0;              // distinct circuits among the range's networks
@@ -1298,6 +1299,7 @@ static int allow_all_smem() {
                                   (int)kSmemLimitBytes));
     QTB_CUDA(cudaFuncSetAttribute(qtb_warp_network_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kSmemLimitBytes));
+    QTB_CUDA(cudaFuncSetAttribute(qtb_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     return QTB_OK;
 }
 
@@ -1757,6 +1759,12 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
     if (const char* env = std::getenv("QTB_CLUSTER_MAX_ELEMS")) cl_max = std::strtoull(env, nullptr, 10);
     for (int32_t i : members[kSmemClasses])
         (plan->druns[i].arena_elems <= cl_max ? cl_nets : wave_nets).push_back(i);
+    // QTB_CLUSTER_CTAS (2, 4, 8 or 16) sets the CTAs per cluster
+    rc->cl_ctas = kClusterCtas;
+    if (const char* env = std::getenv("QTB_CLUSTER_CTAS")) {
+        const int c = std::atoi(env);
+        if (c == 2 || c == 4 || c == 8 || c == 16) rc->cl_ctas = c;
+    }
     auto place_clusters = [&](bool on_device) -> int {
         rc->n_cl = (int)cl_nets.size();
         rc->cl_arena_off = (rc->scratch_elems + 63) & ~size_t(63);
@@ -1929,13 +1937,13 @@ static int ensure_streams(qtb_plan_device* s);
 static int launch_waves(const RunCache* rc, const RunArgs& base, void* scratch_dev, cudaStream_t st) {
     if (rc->n_cl > 0) {
         cudaLaunchConfig_t cfg{};
-        cfg.gridDim = dim3((unsigned)(rc->n_cl * kClusterCtas));
+        cfg.gridDim = dim3((unsigned)(rc->n_cl * rc->cl_ctas));
         cfg.blockDim = dim3(kClusterThreads);
         cfg.dynamicSmemBytes = 0;
         cfg.stream = st;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = kClusterCtas;
+        attr[0].val.clusterDim.x = (unsigned)rc->cl_ctas;
         attr[0].val.clusterDim.y = 1;
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;

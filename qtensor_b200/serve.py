@@ -119,7 +119,8 @@ class QAOAServer:
     order_trials: randomized greedy orders per network (plus the minimum-fill
     candidates they bring), fewer than the engine's 16 because a request's
     compile is on its latency path.  compile_workers: host threads compiling
-    requests concurrently (each also uses the C++ compiler's own threads)."""
+    requests concurrently, each with compile_threads C++ threads (default:
+    its share of the CPUs the process may use)."""
 
     def __init__(self, device=None, n_streams=4, memory_budget=None, max_width=29,
                  max_slices=1024, composer='default', order_trials=4, compile_workers=2,
@@ -131,7 +132,8 @@ class QAOAServer:
         self.max_width = max_width
         self.max_slices = max_slices
         self.order_trials = order_trials
-        self.compile_threads = compile_threads
+        # the compile workers share the CPUs the process may use
+        self.compile_threads = compile_threads or max(1, _lib.available_cpus() // max(1, compile_workers))
         self.max_request_bytes = max_request_bytes
         _lib.check(_lib.lib().qtb_init(self.device.index))
         if memory_budget is None:
