@@ -240,6 +240,16 @@ int qtb_plan_set_order_trials(qtb_plan* plan, int32_t trials);
  * every edge from its own lightcone.                                     */
 int qtb_plan_set_share_lightcones(qtb_plan* plan, int32_t enable);
 
+/* Element records (enable 1, the default; set before qtb_plan_upload): for
+ * every distinct network blob whose gate table fits shared memory, the
+ * host resolves each output element's operand offsets (the bit gathers of
+ * its bucket's index sets, qtensor/ProcessingFrameworks.py:23-37 einsum)
+ * into per-element words, so that the shared-memory executors only load and
+ * multiply.  Same products in the same order as without records, so the
+ * terms are identical.  Costs (1 + operands) x 4 bytes per element of
+ * device memory, at most 256 MiB per plan; 0 keeps the plain plan blobs. */
+int qtb_plan_set_records(qtb_plan* plan, int32_t enable);
+
 int qtb_plan_n_networks(const qtb_plan* plan, int32_t* n);
 int qtb_plan_network_info(const qtb_plan* plan, int32_t net, qtb_network_info* info);
 /* Elimination order of a network as variable ids of the qtree layout
@@ -254,8 +264,9 @@ int qtb_plan_check_params(const qtb_plan* plan, const double* params, int32_t* v
  * device), for inspection and CPU-side verification of the compiler.
  * which: 0 networks (8 x u32 each), 1 ops (16 B each), 2 operands (8 B),
  * 3 phases (16 B), 4 gate-table entries (24 B), 5 angle terms (16 B),
- * 6 per-network executor records (8 x u32), 7 the per-network plan blobs
- * (phases, ops, operands with network-local indices) the executor stages.
+ * 6 per-network executor records (12 x u32), 7 the per-network plan blobs
+ * (phases, ops, operands with network-local indices) the executor stages,
+ * 8 the element records (u32 words; see qtb_plan_set_records).
  * Writes min(cap, size) bytes to buf (may be NULL) and the full size.     */
 int qtb_plan_export(qtb_plan* plan, int32_t which, void* buf, size_t cap, size_t* size);
 /* Complex64 elements of the gate table. */
@@ -310,7 +321,8 @@ int qtb_plan_set_autotune(qtb_plan* plan, int32_t enable);
  * wide networks contracted by the whole GPU step by step, arenas in
  * scratch, 8 = lean persistent queue (registers capped), 16 = warp-per-
  * network queue, 32 = the 96-thread lean queue, 64 = networks of moderate
- * size, one thread-block cluster each, arenas in scratch).                */
+ * size, one thread-block cluster each, arenas in scratch, 128 = networks
+ * with element records contract from them, qtb_plan_set_records).        */
 int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32_t* n_classes);
 
 /* Device memory the plan holds once uploaded (images, gate table, job

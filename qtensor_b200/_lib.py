@@ -29,7 +29,7 @@ EXPORTS = (
     'qtb_plan_create', 'qtb_plan_destroy', 'qtb_plan_add_circuit',
     'qtb_plan_add_lightcone', 'qtb_plan_add_lightcones', 'qtb_plan_add_circuit_batch',
     'qtb_plan_set_max_width', 'qtb_plan_set_slicing',
-    'qtb_plan_set_order_trials', 'qtb_plan_set_share_lightcones',
+    'qtb_plan_set_order_trials', 'qtb_plan_set_share_lightcones', 'qtb_plan_set_records',
     'qtb_plan_n_networks',
     'qtb_plan_network_info', 'qtb_plan_network_peo', 'qtb_plan_check_params',
     'qtb_plan_export', 'qtb_plan_table_elems', 'qtb_plan_upload',
@@ -93,7 +93,8 @@ ENTRY_DTYPE = np.dtype([('kind', '<i4'), ('expr_begin', '<i4'), ('expr_count', '
 TERM_DTYPE = np.dtype([('param', '<i4'), ('pad', '<i4'), ('coef', '<f8')])
 RUN_DTYPE = np.dtype([('blob_off16', '<u4'), ('blob_bytes', '<u4'), ('n_phases', '<u4'),
                       ('ins_off', '<u4'), ('arena_elems', '<u4'), ('result_src', '<u4'),
-                      ('max_elems', '<u4'), ('tail_start', '<u4')])
+                      ('max_elems', '<u4'), ('tail_start', '<u4'), ('rec_off', '<u4'),
+                      ('rec_words', '<u4'), ('pad0', '<u4'), ('pad1', '<u4')])
 SRC_TABLE = 0x80000000
 STATUS_WAIT_TIMEOUT = 16
 
@@ -127,6 +128,7 @@ def _declare(lib):
         'qtb_plan_set_slicing': (c.c_int, [P, c.c_int32]),
         'qtb_plan_set_order_trials': (c.c_int, [P, c.c_int32]),
         'qtb_plan_set_share_lightcones': (c.c_int, [P, c.c_int32]),
+        'qtb_plan_set_records': (c.c_int, [P, c.c_int32]),
         'qtb_plan_n_networks': (c.c_int, [P, c.POINTER(c.c_int32)]),
         'qtb_plan_network_info': (c.c_int, [P, c.c_int32, c.POINTER(NetworkInfo)]),
         'qtb_plan_network_peo': (c.c_int, [P, c.c_int32, P, c.c_int32, c.POINTER(c.c_int32)]),

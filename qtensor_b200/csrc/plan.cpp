@@ -1782,92 +1782,6 @@ void flatten_plan(qtb_plan* plan) {
     }
 }
 
-// Per-network blobs with network-local indices (see DevNetRun).
-// Networks whose blobs are byte-identical (edges that shared a compile, or
-// equal slices) point at one copy: each is still contracted on its own, but
-// the plan image holds one blob, which the executors then stage from L2.
-void build_blobs(qtb_plan* plan) {
-    plan->druns.clear();
-    plan->dblobs.clear();
-    std::unordered_map<uint64_t, std::vector<uint32_t>> seen;   // hash -> blob offsets (16 B units)
-    for (const Network& n : plan->nets) {
-        DevNetRun r{};
-        r.blob_off16 = (uint32_t)(plan->dblobs.size() / 16);
-        r.n_phases = (uint32_t)n.phases.size();
-        r.arena_elems = (uint32_t)n.info.arena_elems;
-        r.result_src = n.result_src;
-        r.max_elems = n.max_elems;
-        r.tail_start = (uint32_t)n.phases.size();
-        while (r.tail_start > 0 && n.phases[r.tail_start - 1].total_elems <= 32) --r.tail_start;
-        const size_t ph_bytes = n.phases.size() * sizeof(DevPhase);
-        const size_t op_bytes = n.ops.size() * sizeof(DevOp);
-        const size_t in_bytes = n.ins.size() * sizeof(DevIn);
-        r.ins_off = (uint32_t)(ph_bytes + op_bytes);
-        // chunk tables: op of every kChunkElems-th flattened element
-        std::vector<DevPhase> phases = n.phases;
-        std::vector<uint16_t> chunks;
-        size_t chunk_base = ph_bytes + op_bytes + in_bytes;
-        for (DevPhase& ph : phases) {
-            ph.chunk_off = (uint32_t)(chunk_base + chunks.size() * sizeof(uint16_t));
-            uint32_t oi = ph.op_first;
-            for (uint32_t e = 0; e < ph.total_elems; e += kChunkElems) {
-                while (oi + 1 < ph.op_first + ph.op_count && n.ops[oi + 1].elem_begin <= e) ++oi;
-                chunks.push_back((uint16_t)oi);
-            }
-        }
-        const size_t total = (chunk_base + chunks.size() * sizeof(uint16_t) + 15) & ~size_t(15);
-        r.blob_bytes = (uint32_t)total;
-        const size_t base = plan->dblobs.size();
-        plan->dblobs.resize(base + total, 0);
-        uint8_t* dst = plan->dblobs.data() + base;
-        std::memcpy(dst, phases.data(), ph_bytes);     // op_first already network-local
-        std::memcpy(dst + ph_bytes, n.ops.data(), op_bytes);   // in_begin network-local
-        std::memcpy(dst + ph_bytes + op_bytes, n.ins.data(), in_bytes);
-        if (!chunks.empty())
-            std::memcpy(dst + chunk_base, chunks.data(), chunks.size() * sizeof(uint16_t));
-        uint64_t h = 0x9E3779B97F4A7C15ull ^ total;   // blobs are whole 16-byte units
-        for (size_t b = 0; b < total; b += 8) {
-            uint64_t word;
-            std::memcpy(&word, dst + b, 8);
-            h = (h ^ word) * 0xff51afd7ed558ccdull;
-            h ^= h >> 32;
-        }
-        auto& offs = seen[h];
-        for (uint32_t o : offs) {
-            const DevNetRun& prev = plan->druns[o];
-            if (prev.blob_bytes == total &&
-                std::memcmp(plan->dblobs.data() + 16 * (size_t)prev.blob_off16, dst, total) == 0) {
-                r.blob_off16 = prev.blob_off16;
-                plan->dblobs.resize(base);
-                break;
-            }
-        }
-        if (r.blob_off16 == (uint32_t)(base / 16)) offs.push_back((uint32_t)plan->druns.size());
-        plan->druns.push_back(r);
-    }
-}
-
-void ensure_images(qtb_plan* plan) {
-    if (plan->images_valid) return;
-    build_blobs(plan);
-    plan->images_valid = true;
-}
-
-void ensure_flat(qtb_plan* plan) {
-    if (plan->flat_valid) return;
-    flatten_plan(plan);
-    plan->flat_valid = true;
-}
-
-}  // namespace qtb
-
-// =================================================================== C ABI
-using namespace qtb;
-
-// Most int32 words of cone invariants and keys one lightcone call may hold
-// (256 MiB); past it, edges are compiled without sharing.
-constexpr size_t kShareKeyLimit = size_t(1) << 26;
-
 // CPUs this process may run on: the hardware threads, bounded by its
 // affinity mask and by a cgroup CPU quota (cgroup v2 cpu.max, v1
 // cfs_quota_us / cfs_period_us).  In a container the hardware count is the
@@ -1908,7 +1822,6 @@ static int available_cpus() {
 
 // Runs fn(i) for i in [0, n) on up to n_threads threads (0 = every CPU the
 // process may use).
-namespace qtb {
 template <typename Fn>
 static void parallel_for(int32_t n, int32_t n_threads, Fn fn) {
     std::atomic<int32_t> next{0};
@@ -1922,7 +1835,207 @@ static void parallel_for(int32_t n, int32_t n_threads, Fn fn) {
     worker();
     for (auto& t : pool) t.join();
 }
+
+// Bits of x selected by m, packed from bit 0 up.
+static uint32_t pext_bits(uint32_t x, uint32_t m) {
+    uint32_t r = 0, bit = 1;
+    while (m) {
+        const uint32_t lo = m & (0u - m);
+        if (x & lo) r |= bit;
+        bit <<= 1;
+        m ^= lo;
+    }
+    return r;
+}
+
+// Largest operand count of a phase's ops.
+static uint32_t phase_kmax(const Network& n, const DevPhase& ph) {
+    uint32_t kmax = 1;
+    for (uint32_t o = ph.op_first; o < ph.op_first + ph.op_count; ++o) kmax = std::max<uint32_t>(kmax, n.ops[o].k);
+    return kmax;
+}
+
+// Words of a network's element records (layout at DevNetRun), or 0 when it
+// cannot have them: an op without operands or with more than kRecMaxK, an
+// arena past the shared-memory window (`smem_elems` complex64 elements
+// beside the gate table), or window offsets past 16 bits.
+static uint32_t record_words(const Network& n, uint32_t table_pad, uint64_t smem_elems) {
+    const uint64_t arena = n.info.arena_elems;
+    if (arena > smem_elems || table_pad + arena > 0xffffu) return 0;
+    for (const DevOp& op : n.ops)
+        if (op.k < 1 || op.k > kRecMaxK) return 0;
+    uint64_t words = 2 * n.phases.size();
+    for (const DevPhase& ph : n.phases) words += (uint64_t)(phase_kmax(n, ph) + 1) * ph.total_elems;
+    return words > 0xffffffffu ? 0 : (uint32_t)words;
+}
+
+// Writes a network's element records into rec (record_words words, zeroed),
+// with the gate table's padded size `table_pad` as the arena's offset in
+// the shared window.  The offsets are the bit gathers compute_element
+// would do, resolved once: the bits of element j that the operand's mask
+// selects, packed, plus its source; the summed variable is the operand's
+// top axis.
+static void fill_records(const Network& n, uint32_t table_pad, uint32_t* rec) {
+    const size_t n_ph = n.phases.size();
+    uint32_t payload = (uint32_t)(2 * n_ph);
+    uint32_t lo_tab[256];
+    for (size_t p = 0; p < n_ph; ++p) {
+        const DevPhase& ph = n.phases[p];
+        const uint32_t kmax = phase_kmax(n, ph);
+        const uint32_t total = ph.total_elems;
+        rec[2 * p] = payload;
+        rec[2 * p + 1] = total | kmax << 24;
+        uint32_t* row = rec + payload;
+        for (uint32_t o = ph.op_first; o < ph.op_first + ph.op_count; ++o) {
+            const DevOp& op = n.ops[o];
+            const uint32_t w = (uint32_t)op.u - op.sum;
+            const uint32_t low = (1u << w) - 1u;
+            for (uint32_t t = 0; t < op.k; ++t) {
+                const DevIn& d = n.ins[op.in_begin + t];
+                const uint32_t m = d.mask & low;
+                const uint32_t src = (d.src & kSrcTable) ? (d.src & ~kSrcTable) : table_pad + d.src;
+                const uint32_t stride = (op.sum && ((d.mask >> w) & 1u)) ? 1u << (__builtin_popcount(d.mask) - 1) : 0u;
+                uint32_t* r = row + (size_t)(t + 1) * total + op.elem_begin;
+                // j = hi << 8 | lo: the gather of the low byte from a table
+                const uint32_t m_lo = m & 0xffu, shift = (uint32_t)__builtin_popcount(m_lo);
+                const uint32_t n_lo = std::min(low, 255u) + 1u;
+                for (uint32_t x = 0; x < n_lo; ++x) lo_tab[x] = pext_bits(x, m_lo);
+                for (uint32_t hi = 0; hi <= (low >> 8); ++hi) {
+                    const uint32_t hoff = src + (pext_bits(hi, m >> 8) << shift);
+                    uint32_t* rh = r + (hi << 8);
+                    for (uint32_t x = 0; x < n_lo; ++x) {
+                        const uint32_t o0 = hoff + lo_tab[x];
+                        rh[x] = o0 | (o0 + stride) << 16;
+                    }
+                }
+            }
+            uint32_t* r0 = row + op.elem_begin;
+            const uint32_t head = (uint32_t)op.k << 16 | (uint32_t)op.sum << 24;
+            for (uint32_t j = 0; j <= low; ++j) r0[j] = (table_pad + op.dst + j) | head;
+        }
+        payload += (kmax + 1) * total;
+    }
+}
+
+// Per-network blobs with network-local indices (see DevNetRun).
+// Networks whose blobs are byte-identical (edges that shared a compile, or
+// equal slices) point at one copy: each is still contracted on its own, but
+// the plan image holds one blob, which the executors then stage from L2.
+// Element records follow the blobs: one copy per distinct blob, for plans
+// whose gate table fits shared memory, up to kRecMaxWords words per plan.
+void build_blobs(qtb_plan* plan) {
+    plan->druns.clear();
+    plan->dblobs.clear();
+    plan->drecs.clear();
+    const bool records = plan->records && plan->table_elems <= kSmemTableLimitElems;
+    const uint32_t table_pad = (plan->table_elems + 1u) & ~1u;
+    // shared memory left for an arena beside the staged gate entries,
+    // angle terms and gate table (an upper bound on what any launch has)
+    const uint64_t fixed = 16 + ((plan->entries.size() * sizeof(DevEntry) + 15) & ~size_t(15)) +
+                           plan->terms.size() * sizeof(DevTerm) + 8 * (uint64_t)table_pad;
+    const uint64_t smem_elems = fixed < kSmemLimitBytes ? (kSmemLimitBytes - fixed) / 8 : 0;
+    uint64_t rec_total = 0;
+    std::vector<std::pair<int32_t, uint32_t>> rec_todo;   // (network, first word)
+    std::unordered_map<uint64_t, std::vector<uint32_t>> seen;   // hash -> blob offsets (16 B units)
+    for (const Network& n : plan->nets) {
+        DevNetRun r{};
+        r.blob_off16 = (uint32_t)(plan->dblobs.size() / 16);
+        r.n_phases = (uint32_t)n.phases.size();
+        r.arena_elems = (uint32_t)n.info.arena_elems;
+        r.result_src = n.result_src;
+        r.max_elems = n.max_elems;
+        r.tail_start = (uint32_t)n.phases.size();
+        while (r.tail_start > 0 && n.phases[r.tail_start - 1].total_elems <= 32) --r.tail_start;
+        const size_t ph_bytes = n.phases.size() * sizeof(DevPhase);
+        const size_t op_bytes = n.ops.size() * sizeof(DevOp);
+        const size_t in_bytes = n.ins.size() * sizeof(DevIn);
+        r.ins_off = (uint32_t)(ph_bytes + op_bytes);
+        // chunk tables: op of every kChunkElems-th flattened element, for
+        // the executors that keep the arena in shared memory (a network
+        // whose arena cannot be there runs in waves or clusters, which find
+        // ops by search; its tables would grow with its elements)
+        std::vector<DevPhase> phases = n.phases;
+        std::vector<uint16_t> chunks;
+        size_t chunk_base = ph_bytes + op_bytes + in_bytes;
+        const bool chunked = 8 * (uint64_t)n.info.arena_elems <= kSmemLimitBytes;
+        for (DevPhase& ph : phases) {
+            ph.chunk_off = chunked ? (uint32_t)(chunk_base + chunks.size() * sizeof(uint16_t)) : 0u;
+            if (!chunked) continue;
+            uint32_t oi = ph.op_first;
+            for (uint32_t e = 0; e < ph.total_elems; e += kChunkElems) {
+                while (oi + 1 < ph.op_first + ph.op_count && n.ops[oi + 1].elem_begin <= e) ++oi;
+                chunks.push_back((uint16_t)oi);
+            }
+        }
+        const size_t total = (chunk_base + chunks.size() * sizeof(uint16_t) + 15) & ~size_t(15);
+        r.blob_bytes = (uint32_t)total;
+        const size_t base = plan->dblobs.size();
+        plan->dblobs.resize(base + total, 0);
+        uint8_t* dst = plan->dblobs.data() + base;
+        std::memcpy(dst, phases.data(), ph_bytes);     // op_first already network-local
+        std::memcpy(dst + ph_bytes, n.ops.data(), op_bytes);   // in_begin network-local
+        std::memcpy(dst + ph_bytes + op_bytes, n.ins.data(), in_bytes);
+        if (!chunks.empty())
+            std::memcpy(dst + chunk_base, chunks.data(), chunks.size() * sizeof(uint16_t));
+        uint64_t h = 0x9E3779B97F4A7C15ull ^ total;   // blobs are whole 16-byte units
+        for (size_t b = 0; b < total; b += 8) {
+            uint64_t word;
+            std::memcpy(&word, dst + b, 8);
+            h = (h ^ word) * 0xff51afd7ed558ccdull;
+            h ^= h >> 32;
+        }
+        auto& offs = seen[h];
+        for (uint32_t o : offs) {
+            const DevNetRun& prev = plan->druns[o];
+            if (prev.blob_bytes == total &&
+                std::memcmp(plan->dblobs.data() + 16 * (size_t)prev.blob_off16, dst, total) == 0) {
+                r.blob_off16 = prev.blob_off16;
+                r.rec_off = prev.rec_off;
+                r.rec_words = prev.rec_words;
+                plan->dblobs.resize(base);
+                break;
+            }
+        }
+        if (r.blob_off16 == (uint32_t)(base / 16)) {
+            offs.push_back((uint32_t)plan->druns.size());
+            const uint32_t words = records ? record_words(n, table_pad, smem_elems) : 0u;
+            if (words && rec_total + words <= kRecMaxWords) {
+                r.rec_off = (uint32_t)rec_total;
+                r.rec_words = words;
+                rec_total += words;
+                rec_todo.emplace_back((int32_t)plan->druns.size(), r.rec_off);
+            }
+        }
+        plan->druns.push_back(r);
+    }
+    plan->drecs.assign(rec_total, 0u);
+    parallel_for((int32_t)rec_todo.size(), 0, [&](int32_t t) {
+        const auto& job = rec_todo[t];
+        fill_records(plan->nets[job.first], table_pad, plan->drecs.data() + job.second);
+    });
+}
+
+void ensure_images(qtb_plan* plan) {
+    if (plan->images_valid) return;
+    build_blobs(plan);
+    plan->images_valid = true;
+}
+
+void ensure_flat(qtb_plan* plan) {
+    if (plan->flat_valid) return;
+    flatten_plan(plan);
+    plan->flat_valid = true;
+}
+
 }  // namespace qtb
+
+// =================================================================== C ABI
+using namespace qtb;
+
+// Most int32 words of cone invariants and keys one lightcone call may hold
+// (256 MiB); past it, edges are compiled without sharing.
+constexpr size_t kShareKeyLimit = size_t(1) << 26;
+
 
 extern "C" {
 
@@ -2116,6 +2229,15 @@ int qtb_plan_set_share_lightcones(qtb_plan* plan, int32_t enable) {
     return QTB_OK;
 }
 
+int qtb_plan_set_records(qtb_plan* plan, int32_t enable) {
+    if (!plan) return fail(QTB_ERR_ARG, "plan_set_records: null plan");
+    std::lock_guard<std::mutex> lock(plan->mu);
+    if (plan->uploaded) return fail(QTB_ERR_ARG, "plan_set_records: set before qtb_plan_upload");
+    if (plan->records != (enable != 0)) plan->images_valid = false;
+    plan->records = enable != 0;
+    return QTB_OK;
+}
+
 int qtb_plan_set_order_trials(qtb_plan* plan, int32_t trials) {
     if (!plan || trials < 0) return fail(QTB_ERR_ARG, "plan_set_order_trials: bad arguments");
     plan->order_trials = trials;
@@ -2176,6 +2298,7 @@ int qtb_plan_export(qtb_plan* plan, int32_t which, void* buf, size_t cap, size_t
         case 5: src = plan->terms.data(); n = plan->terms.size() * sizeof(DevTerm); break;
         case 6: src = plan->druns.data(); n = plan->druns.size() * sizeof(DevNetRun); break;
         case 7: src = plan->dblobs.data(); n = plan->dblobs.size(); break;
+        case 8: src = plan->drecs.data(); n = plan->drecs.size() * sizeof(uint32_t); break;
         default: return fail(QTB_ERR_ARG, "plan_export: unknown array");
     }
     *size = n;

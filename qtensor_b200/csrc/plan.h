@@ -48,7 +48,8 @@ constexpr uint64_t kRunsFallback = 7;
 // Ops of one dependency level; a barrier follows every phase.  In a network
 // blob, chunk_off is the byte offset of the phase's chunk table: for every
 // 32 flattened elements, the (network-local) index of the op holding the
-// chunk's first element.
+// chunk's first element.  Only networks whose arena can be in shared
+// memory have chunk tables (chunk_off 0 otherwise).
 struct DevPhase {
     uint32_t op_first;
     uint32_t op_count;
@@ -81,7 +82,30 @@ struct DevNetRun {
     uint32_t result_src;
     uint32_t max_elems;
     uint32_t tail_start;   // phases from here on have <= 32 elements each
+    uint32_t rec_off;      // first word of the network's element records
+    uint32_t rec_words;    // 0: the network has no element records
+    uint32_t pad0;
+    uint32_t pad1;
 };
+
+// Element records of a network (u32 words at DevNetRun::rec_off in the
+// plan's record array), for executors whose gate table and arena share one
+// shared-memory window S = [gate table, padded to an even element count]
+// [arena]:
+//   [phase header x n_phases][phase payloads]
+//   header p: word 0 = payload offset (words from rec_off),
+//             word 1 = elements of the phase | (largest operand count) << 24
+//   payload p, element g (kmax + 1 rows of `elements` words, row-major):
+//     row 0     = S offset of the output | k << 16 | sum << 24
+//     row 1 + t = operand t: S offset at the summed variable 0 (low 16 bits)
+//                 and at 1 (high 16 bits; equal when the operand lacks it)
+// Every offset the bit gathers of the op would compute is resolved on the
+// host, so the executor only loads and multiplies.
+constexpr uint32_t kRecMaxK = 8;                    // operands per op with records
+constexpr uint64_t kRecMaxWords = uint64_t(1) << 26;   // record words per plan (256 MiB)
+constexpr uint32_t kSmemTableLimitElems = 2048;   // 16 KB of gate table per CTA
+// Dynamic shared memory a CTA may use (B200: 227 KB per block).
+constexpr uint32_t kSmemLimitBytes = 224 * 1024;
 
 // Gate-table entry: the tensor of a gate, sliced and transposed into the
 // sorted-variable layout the network reads (device layout).
@@ -107,7 +131,7 @@ static_assert(sizeof(DevOp) == 16, "DevOp layout");
 static_assert(sizeof(DevIn) == 16, "DevIn layout");
 static_assert(sizeof(DevPhase) == 16, "DevPhase layout");
 static_assert(sizeof(DevNet) == 32, "DevNet layout");
-static_assert(sizeof(DevNetRun) == 32, "DevNetRun layout");
+static_assert(sizeof(DevNetRun) == 48, "DevNetRun layout");
 constexpr uint32_t kChunkElems = 32;
 static_assert(sizeof(DevEntry) == 24, "DevEntry layout");
 static_assert(sizeof(DevTerm) == 16, "DevTerm layout");
@@ -158,6 +182,7 @@ struct DeviceBuffers {
     void* blobs = nullptr;        // concatenated network blobs
     void* entries = nullptr;      // common image: gate entries then angle terms
     void* terms = nullptr;        // inside the entries allocation
+    void* recs = nullptr;         // element records (u32 words)
     void* table = nullptr;        // complex64 gate table
     void* status = nullptr;       // int error word
 };
@@ -187,7 +212,9 @@ struct qtb_plan {
     std::vector<qtb::DevPhase> dphases;
     std::vector<qtb::DevNetRun> druns;
     std::vector<uint8_t> dblobs;
-    bool images_valid = false;       // druns and dblobs match `nets`
+    std::vector<uint32_t> drecs;     // element records (DevNetRun::rec_off)
+    bool records = true;             // build element records for shared-memory executors
+    bool images_valid = false;       // druns, dblobs and drecs match `nets`
     bool flat_valid = false;         // dnets, dops, dins and dphases match `nets`
     uint32_t common_bytes = 0;       // staged gate entries + angle terms
     uint32_t common_terms_off = 0;

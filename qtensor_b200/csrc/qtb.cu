@@ -252,6 +252,7 @@ struct RunArgs {
     uint32_t terms_off;           // byte offset of the DevTerm array in common
     uint32_t table_elems;
     const double* params;
+    const uint32_t* recs;         // element records, or null: this launch reads plan blobs only
     const float2* gtable;         // global gate table (kernels without a shared table)
     float2* gscratch;             // global arenas (kernels without a shared arena)
     uint32_t arena_capacity;      // elements per CTA
@@ -272,7 +273,6 @@ constexpr int kStatusBlob = 4;         // network blob larger than the launch's 
 constexpr int kStatusQueue = 8;        // persistent launch without a job queue
 constexpr int kStatusWideTimeout = 16; // a wide-network step waited too long for its predecessor
 constexpr uint32_t kStageSpinLimit = 1u << 25;   // about 1.5 s of polling
-constexpr uint32_t kSmemTableLimitElems = 2048;   // 16 KB of gate table per CTA
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -468,6 +468,80 @@ __device__ float2 contract_network(const DevNetRun& net, const unsigned char* bl
     return result;
 }
 
+// ------------------------------------------- element records (see plan.h)
+// Header of phase p of a network's records (zero elements past the last).
+struct RecHead {
+    const uint32_t* rows;   // payload: row r of element g at rows[r * total + g]
+    uint32_t total;
+    uint32_t kmax;
+};
+
+__device__ __forceinline__ RecHead rec_head(const uint32_t* rec, uint32_t p, uint32_t n_phases) {
+    if (p >= n_phases) return RecHead{rec, 0u, 0u};
+    const uint2 h = __ldg(reinterpret_cast<const uint2*>(rec) + p);
+    return RecHead{rec + h.x, h.y & 0xffffffu, h.y >> 24};
+}
+
+// The record words of element g (zeros past the phase or the phase's rows).
+__device__ __forceinline__ void rec_load(const RecHead& h, uint32_t g, uint32_t (&w)[kRecMaxK + 1]) {
+#pragma unroll
+    for (uint32_t t = 0; t <= kRecMaxK; ++t)
+        w[t] = (g < h.total && t <= h.kmax) ? __ldg(h.rows + (size_t)t * h.total + g) : 0u;
+}
+
+// One output element from its record: the same products, in the same
+// operand order, as compute_element.
+__device__ __forceinline__ void rec_element(const uint32_t (&w)[kRecMaxK + 1], float2* __restrict__ S) {
+    const uint32_t d = w[0], k = (d >> 16) & 0xffu;
+    float2 p0 = S[w[1] & 0xffffu], p1 = S[w[1] >> 16];
+#pragma unroll
+    for (uint32_t t = 2; t <= kRecMaxK; ++t)
+        if (t <= k) {
+            p0 = cmul(p0, S[w[t] & 0xffffu]);
+            p1 = cmul(p1, S[w[t] >> 16]);
+        }
+    S[d & 0xffffu] = (d >> 24) ? make_float2(p0.x + p1.x, p0.y + p1.y) : p0;
+}
+
+// The phases of one network from its element records, S the shared window
+// [gate table][arena].  Each thread's record of its first element of the
+// next phase, and the header of the phase after, are loaded while the
+// current phase computes, so the loads from L2 overlap the phase and its
+// barrier instead of starting every phase.  Same phase split as
+// contract_network: phases of more than 32 elements on every thread with
+// block barriers, the tail on warp 0 with warp barriers.
+__device__ float2 contract_records(const DevNetRun& net, const uint32_t* __restrict__ rec,
+                                   float2* __restrict__ S, const float2* __restrict__ arena) {
+    const uint32_t tid = threadIdx.x;
+    RecHead h = rec_head(rec, 0, net.n_phases);
+    RecHead h1 = rec_head(rec, 1, net.n_phases);
+    uint32_t cur[kRecMaxK + 1];
+    rec_load(h, tid, cur);
+    for (uint32_t p = 0; p < net.n_phases; ++p) {
+        const bool tail = p >= net.tail_start;
+        if (tail && tid >= 32) break;
+        uint32_t nxt[kRecMaxK + 1];
+        rec_load(h1, tid, nxt);
+        const RecHead h2 = rec_head(rec, p + 2, net.n_phases);
+        if (tid < h.total) rec_element(cur, S);
+        for (uint32_t g = tid + blockDim.x; g < h.total; g += blockDim.x) {
+            uint32_t w[kRecMaxK + 1];
+            rec_load(h, g, w);
+            rec_element(w, S);
+        }
+        if (tail) __syncwarp();
+        else __syncthreads();
+        h = h1;
+        h1 = h2;
+#pragma unroll
+        for (uint32_t t = 0; t <= kRecMaxK; ++t) cur[t] = nxt[t];
+    }
+    float2 result = make_float2(0.f, 0.f);
+    if (tid == 0)
+        result = (net.result_src & kSrcTable) ? S[net.result_src & ~kSrcTable] : arena[net.result_src];
+    return result;
+}
+
 // Network executor.  Shared memory, in order: mbarrier (16 B), [plan-wide
 // gate entries + angle terms], the network's plan blob, [gate table],
 // [arena]; the bracketed parts exist when kSmemTable / kSmemArena.
@@ -514,8 +588,11 @@ __global__ void __launch_bounds__(kLean == 2 ? 96 : kLean ? 128 : (kPersistent ?
         }
         const Job job = jobs[kPersistent ? s_job : blockIdx.x];
         const DevNetRun net = *job.net;
-        // blob_capacity 0: the launch reads plan blobs from global memory
-        const bool staged = a.blob_capacity != 0;
+        // a network with element records needs no blob (shared table and
+        // arena only); otherwise blob_capacity 0: the launch reads plan
+        // blobs from global memory
+        const bool records = kSmemArena && kSmemTable && a.recs != nullptr && net.rec_words != 0;
+        const bool staged = !records && a.blob_capacity != 0;
         if (net.arena_elems > a.arena_capacity || (staged && net.blob_bytes > a.blob_capacity)) {
             if (threadIdx.x == 0)
                 atomicOr(a.status, net.arena_elems > a.arena_capacity ? kStatusArena : kStatusBlob);
@@ -523,17 +600,22 @@ __global__ void __launch_bounds__(kLean == 2 ? 96 : kLean ? 128 : (kPersistent ?
         }
         // the first staging of a CTA also brings the plan-wide gate entries
         const bool with_common = kSmemTable && !table_ready;
-        if (!stage(blob, a.blobs + net.blob_off16, staged ? net.blob_bytes : 0u, common, a.common,
-                   with_common ? a.common_bytes : 0u, bar, parity, a.status))
-            return;
-        parity ^= 1u;
+        const uint32_t blob_bytes = staged ? net.blob_bytes : 0u;
+        const uint32_t common_bytes = with_common ? a.common_bytes : 0u;
+        if (blob_bytes + common_bytes) {
+            if (!stage(blob, a.blobs + net.blob_off16, blob_bytes, common, a.common, common_bytes, bar, parity,
+                       a.status))
+                return;
+            parity ^= 1u;
+        }
         if (!table_ready) {
             build_table(common, a, stable);
             table_ready = true;
         }
         const unsigned char* nblob =
             staged ? blob : reinterpret_cast<const unsigned char*>(a.blobs + net.blob_off16);
-        const float2 term = contract_network<kSmemTable>(net, nblob, table, arena);
+        const float2 term = records ? contract_records(net, a.recs + net.rec_off, stable, arena)
+                                    : contract_network<kSmemTable>(net, nblob, table, arena);
         if (threadIdx.x == 0) {
             *job.term = term;
             if (a.energy) {
@@ -1001,8 +1083,8 @@ __global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArg
 
 // ----------------------------------------------------------------- K5
 // Networks too large for shared memory but of moderate size (arenas up to
-// kClusterArenaElems) run one thread-block cluster of kClusterCtas CTAs
-// each: the cluster walks the network's phases, a phase's elements cut into
+// QTB_CLUSTER_MAX_ELEMS, opt-in) can run one thread-block cluster of
+// kClusterCtas CTAs each: the cluster walks the network's phases, a phase's elements cut into
 // chunks of 2048 that the cluster's CTAs take in turn, and phases are
 // separated by the cluster barrier (release/acquire at cluster scope, after
 // a fence for the arena in global memory).  A cluster's CTAs are scheduled
@@ -1023,7 +1105,18 @@ static_assert(sizeof(ClusterJob) == 32, "ClusterJob layout");
 constexpr int kClusterCtas = 8;
 constexpr int kClusterThreads = 256;
 constexpr uint32_t kClusterChunk = 2048;                     // elements per CTA turn (8 per thread)
-constexpr uint32_t kClusterArenaElems = 1u << 22;            // 32 MB arenas and below
+
+// The op of a phase holding element g: the last of ops lo..hi whose first
+// element is at most g (binary search through the read-only path; wide
+// networks carry no chunk tables).
+__device__ __forceinline__ uint32_t search_op(const DevOp* ops, uint32_t lo, uint32_t hi, uint32_t g) {
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1u) >> 1;
+        if (__ldg(&ops[mid].elem_begin) <= g) lo = mid;
+        else hi = mid - 1u;
+    }
+    return lo;
+}
 
 __global__ void __launch_bounds__(kClusterThreads) qtb_cluster_kernel(const ClusterJob* __restrict__ jobs,
                                                                       float2* __restrict__ arenas, const RunArgs a) {
@@ -1041,13 +1134,10 @@ __global__ void __launch_bounds__(kClusterThreads) qtb_cluster_kernel(const Clus
     for (uint32_t p = 0; p < net.n_phases; ++p) {
         const uint4 pv = __ldg(reinterpret_cast<const uint4*>(blob) + p);
         const uint32_t op_first = pv.x, op_count = pv.y, total = pv.z;
-        const uint16_t* chunk = reinterpret_cast<const uint16_t*>(blob + pv.w);
         const uint32_t op_last = op_first + op_count - 1u;
-        auto load = [&](uint32_t i) { return ldg_op(ops + min(i, op_last)); };
         for (uint32_t base = rank * kClusterChunk; base < total; base += nctas * kClusterChunk) {
-            uint32_t oi = __ldg(chunk + base / kChunkElems);
+            uint32_t oi = search_op(ops, op_first, op_last, base);
             DevOp op = ldg_op(ops + oi);
-            oi = find_op(base, oi, op, load);
             const uint32_t size = 1u << (op.u - op.sum);
             if (size >= kClusterChunk && base + kClusterChunk <= total) {
                 // the whole chunk lies in this op (ops start at multiples of their size)
@@ -1059,9 +1149,8 @@ __global__ void __launch_bounds__(kClusterThreads) qtb_cluster_kernel(const Clus
                     const uint32_t g = base + t + e * kClusterThreads;
                     if (g >= total) break;
                     if (g >= op_hi) {
-                        oi = __ldg(chunk + g / kChunkElems);
+                        oi = search_op(ops, oi, op_last, g);
                         op = ldg_op(ops + oi);
-                        oi = find_op(g, oi, op, load);
                         op_hi = op.elem_begin + (1u << (op.u - op.sum));
                     }
                     compute_element_wide(op, g - op.elem_begin, ins, a.gtable, arena);
@@ -1100,8 +1189,6 @@ static int cuda_fail(cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
     } while (0)
 
-// Dynamic shared memory a CTA may use (B200: 227 KB per block).
-constexpr uint32_t kSmemLimitBytes = 224 * 1024;
 // Shared memory of one SM available to CTAs, and the per-CTA reserve.
 constexpr uint32_t kSmemPerSm = 228 * 1024;
 constexpr uint32_t kSmemReservePerCta = 1024;
@@ -1121,6 +1208,7 @@ struct LaunchClass {
     bool persistent;        // CTAs take networks from the run's queue
     int lean;               // persistent, registers capped: 1 = 128 threads (8 CTAs per SM), 2 = 96 (12)
     bool warp;              // persistent, every warp takes networks (qtb_warp_network_kernel)
+    bool records;           // networks with element records contract from them
     int grid;               // CTAs (= n_jobs unless persistent)
     uint32_t capacity;      // arena elements per CTA
     uint32_t blob_capacity; // plan-blob bytes per CTA
@@ -1232,7 +1320,7 @@ static void free_run(RunCache* rc) {
 
 static void free_device(qtb_plan* plan) {
     DeviceBuffers& d = plan->dev;
-    void* ptrs[] = {d.runs, d.blobs, d.entries, d.table, d.status};   // terms lives in entries
+    void* ptrs[] = {d.runs, d.blobs, d.recs, d.entries, d.table, d.status};   // terms lives in entries
     for (void* p : ptrs)
         if (p) cudaFree(p);
     d = DeviceBuffers();
@@ -1457,8 +1545,13 @@ static uint32_t class_bound(int c) {
     return std::min(b, kSmemLimitBytes);
 }
 
-static size_t net_need(const DevNetRun& r, size_t fixed) {
-    return fixed + (size_t)r.blob_bytes + 8 * (size_t)((r.arena_elems + 3u) & ~3u);
+// Blob bytes a network stages: none when it contracts from element records.
+static uint32_t staged_blob(const DevNetRun& r, bool records) {
+    return (records && r.rec_words) ? 0u : r.blob_bytes;
+}
+
+static size_t net_need(const DevNetRun& r, size_t fixed, bool records) {
+    return fixed + (size_t)staged_blob(r, records) + 8 * (size_t)((r.arena_elems + 3u) & ~3u);
 }
 
 // Wide waves of a run: the networks too large for shared memory, largest
@@ -1591,10 +1684,13 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
     for (int32_t i = first; i < first + count; ++i)
         if (i == first || plan->nets[i].info.group != plan->nets[i - 1].info.group) rc->n_groups += 1.0;
     const size_t fixed = fixed_smem(plan, rc->smem_table);
+    // element records serve the shared-memory executors of a plan whose
+    // gate table is in shared memory (the warp queue stages blobs)
+    const bool recs = rc->smem_table && !plan->drecs.empty();
     std::vector<std::vector<int32_t>> members(kMaxClasses);
     for (int32_t i = first; i < first + count; ++i) {
         const DevNetRun& r = plan->druns[i];
-        const size_t need = net_need(r, fixed);
+        const size_t need = net_need(r, fixed, recs);
         int c = kSmemClasses;   // too large for shared memory: a wide wave
         for (int b = 0; b < kSmemClasses; ++b)
             if (need <= class_bound(b)) {
@@ -1610,12 +1706,12 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
         for (;;) {
             uint32_t blob = 0, arena = 0;
             for (int32_t i : m) {
-                blob = std::max(blob, plan->druns[i].blob_bytes);
+                blob = std::max(blob, staged_blob(plan->druns[i], recs));
                 arena = std::max(arena, (plan->druns[i].arena_elems + 3u) & ~3u);
             }
             if (m.empty() || fixed + blob + 8 * (size_t)arena <= kSmemLimitBytes) break;
             auto big = std::max_element(m.begin(), m.end(), [&](int32_t x, int32_t y) {
-                return net_need(plan->druns[x], fixed) < net_need(plan->druns[y], fixed);
+                return net_need(plan->druns[x], fixed, recs) < net_need(plan->druns[y], fixed, recs);
             });
             members[kSmemClasses].push_back(*big);
             m.erase(big);
@@ -1623,17 +1719,18 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
     }
     std::vector<Job> jobs;
     const auto* runs = static_cast<const DevNetRun*>(plan->dev.runs);
-    auto make_class = [&](const std::vector<int32_t>& m, bool smem, bool persistent) {
+    auto make_class = [&](const std::vector<int32_t>& m, bool smem, bool persistent, bool with_recs = true) {
         LaunchClass lc{};
         lc.smem = smem;
         lc.persistent = persistent;
+        lc.records = smem && with_recs && recs;
         lc.job_offset = jobs.size();
         lc.n_jobs = (int)m.size();
         lc.grid = lc.n_jobs;
         uint32_t cap = 4, blob = 16, maxe = 1;
         for (int32_t i : m) {
             cap = std::max(cap, plan->druns[i].arena_elems);
-            blob = std::max(blob, plan->druns[i].blob_bytes);
+            blob = std::max(blob, staged_blob(plan->druns[i], lc.records));
             maxe = std::max(maxe, plan->druns[i].max_elems);
             Job j;
             j.net = runs ? runs + i : nullptr;    // null in a size-only build
@@ -1685,17 +1782,17 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
         while (lean_class < kSmemClasses && kClassCtas[lean_class] != lean_ctas) ++lean_class;
         const uint32_t lean_bound = class_bound(lean_class);
         std::vector<int32_t> lean, big;
-        for (int32_t i : all) (net_need(plan->druns[i], fixed) <= lean_bound ? lean : big).push_back(i);
+        for (int32_t i : all) (net_need(plan->druns[i], fixed, recs) <= lean_bound ? lean : big).push_back(i);
         // the lean queue holds its largest blob and its largest arena at once
         for (;;) {
             uint32_t blob = 0, arena = 0;
             for (int32_t i : lean) {
-                blob = std::max(blob, plan->druns[i].blob_bytes);
+                blob = std::max(blob, staged_blob(plan->druns[i], recs));
                 arena = std::max(arena, (plan->druns[i].arena_elems + 3u) & ~3u);
             }
             if (lean.empty() || fixed + blob + 8 * (size_t)arena <= lean_bound) break;
             auto worst = std::max_element(lean.begin(), lean.end(), [&](int32_t x, int32_t y) {
-                return net_need(plan->druns[x], fixed) < net_need(plan->druns[y], fixed);
+                return net_need(plan->druns[x], fixed, recs) < net_need(plan->druns[y], fixed, recs);
             });
             big.push_back(*worst);
             lean.erase(worst);
@@ -1742,7 +1839,7 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
                     if (class_of[i - first] == c) m.push_back(i);
                 if (!m.empty()) rc->wclasses.push_back(make_class(m, true, false));
             }
-            LaunchClass lc = make_class(small, true, true);
+            LaunchClass lc = make_class(small, true, true, false);
             lc.warp = true;
             lc.threads = kWarpDefaultThreads;
             while (lc.threads > 32 && warp_smem(lc, fixed, lc.threads) > kSmemLimitBytes) lc.threads /= 2;
@@ -1750,12 +1847,13 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
             rc->wclasses.push_back(lc);
         }
     }
-    // networks too large for shared memory: moderate arenas run as clusters
-    // (K5), the rest as whole-GPU waves (K4)
-    // QTB_CLUSTER_MAX_ELEMS in the environment moves the limit (0: every
-    // such network in waves), so that both executors can be exercised
+    // networks too large for shared memory run as whole-GPU waves (K4);
+    // QTB_CLUSTER_MAX_ELEMS=<elements> in the environment runs those whose
+    // arena is at most that as one thread-block cluster each (K5) instead.
+    // Waves are the default: on N=256 p=4 and Erdos-Renyi N=400 p=3 they
+    // took 0.71 and 2.06 ms, clusters of 2-16 CTAs 0.74-1.30 and 3.4-9.8 ms.
     std::vector<int32_t> wave_nets, cl_nets;
-    uint64_t cl_max = kClusterArenaElems;
+    uint64_t cl_max = 0;
     if (const char* env = std::getenv("QTB_CLUSTER_MAX_ELEMS")) cl_max = std::strtoull(env, nullptr, 10);
     for (int32_t i : members[kSmemClasses])
         (plan->druns[i].arena_elems <= cl_max ? cl_nets : wave_nets).push_back(i);
@@ -1873,6 +1971,7 @@ int qtb_plan_upload(qtb_plan* plan) {
     int r;
     if ((r = upload_vec(plan->druns, &plan->dev.runs))) return r;
     if ((r = upload_vec(plan->dblobs, &plan->dev.blobs))) return r;
+    if (!plan->drecs.empty() && (r = upload_vec(plan->drecs, &plan->dev.recs))) return r;
     {
         const CommonImage c = common_image(plan);
         plan->common_bytes = (uint32_t)c.bytes.size();
@@ -2000,6 +2099,7 @@ static int launch_schedule(qtb_plan_device* s, const RunCache* rc,
         ac.queue = rc->queue;
         ac.arena_capacity = lc.capacity;
         ac.blob_capacity = lc.blob_capacity;
+        ac.recs = lc.records ? base.recs : nullptr;
         ac.n_jobs = (uint32_t)lc.n_jobs;
         ac.gscratch = lc.smem ? nullptr : static_cast<float2*>(scratch_dev) + lc.scratch_offset;
         launch_class(lc, rc->smem_table, rc->jobs + lc.job_offset, ac, cs);
@@ -2280,6 +2380,7 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
     a.terms_off = plan->common_terms_off;
     a.table_elems = plan->table_elems;
     a.params = params_dev;
+    a.recs = static_cast<const uint32_t*>(plan->dev.recs);
     a.gtable = static_cast<const float2*>(plan->dev.table);
     a.status = static_cast<int*>(plan->dev.status);
     a.done = rc->done;
@@ -2616,7 +2717,7 @@ int qtb_plan_last_launch_config(qtb_plan* plan, int32_t* out, int32_t cap, int32
             out[4 * c + 1] = lc.threads;
             out[4 * c + 2] = (int32_t)lc.smem_bytes;
             out[4 * c + 3] = (lc.smem ? 1 : 0) | (lc.persistent ? 2 : 0) | (lc.lean ? 8 : 0) | (lc.warp ? 16 : 0) |
-                             (lc.lean == 2 ? 32 : 0);
+                             (lc.lean == 2 ? 32 : 0) | (lc.records ? 128 : 0);
         } else if (c < (int32_t)(sched.size() + rc->waves.size())) {
             const WideWave& wv = rc->waves[c - sched.size()];
             out[4 * c] = (int32_t)wv.n_nets;
@@ -2640,9 +2741,25 @@ int qtb_plan_device_bytes(const qtb_plan* plan, size_t* bytes) {
     for (const Network& n : plan->nets) {
         blob += n.phases.size() * sizeof(DevPhase) + n.ops.size() * sizeof(DevOp) +
                 n.ins.size() * sizeof(DevIn) + 16;
-        for (const DevPhase& ph : n.phases) blob += 2 * ((ph.total_elems + kChunkElems - 1) / kChunkElems);
+        if (8 * (uint64_t)n.info.arena_elems <= kSmemLimitBytes)   // chunk tables
+            for (const DevPhase& ph : n.phases) blob += 2 * ((ph.total_elems + kChunkElems - 1) / kChunkElems);
     }
     b += blob + plan->nets.size() * (sizeof(DevNetRun) + 2 * sizeof(Job));
+    // element records (an upper bound: one copy per network, not per distinct blob)
+    if (plan->records && plan->table_elems <= kSmemTableLimitElems) {
+        uint64_t words = 0;
+        for (const Network& n : plan->nets) {
+            if (8 * (uint64_t)n.info.arena_elems > kSmemLimitBytes) continue;
+            words += 2 * n.phases.size();
+            for (const DevPhase& ph : n.phases) {
+                uint32_t kmax = 1;
+                for (uint32_t o = ph.op_first; o < ph.op_first + ph.op_count; ++o)
+                    kmax = std::max<uint32_t>(kmax, n.ops[o].k);
+                words += (uint64_t)(kmax + 1) * ph.total_elems;
+            }
+        }
+        b += 4 * (size_t)std::min<uint64_t>(words, kRecMaxWords);
+    }
     b += plan->entries.size() * sizeof(DevEntry) + plan->terms.size() * sizeof(DevTerm) + 64;
     b += (size_t)plan->table_elems * sizeof(float2);
     *bytes = b;

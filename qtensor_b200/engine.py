@@ -168,11 +168,14 @@ class QAOAEnergyEngine:
     B200's memory cannot hold unsliced.  slicing: ``'greedy'``
     (GreedyParvars), ``'tree_trim'`` (TreeTrimSplitter) or ``'late'``
     (LateParOptimizer) choice of the sliced variables.
+    records: resolve every output element's operand offsets on the host, so
+    that the shared-memory executor only loads and multiplies (same
+    products, same order; off: the executor decodes the plan blobs).
     """
 
     def __init__(self, composer='default', ordering='native', device=None, threads=0,
                  cache_size=16, order_trials=16, autotune=True, max_width=29,
-                 max_slices=1024, slicing='greedy'):
+                 max_slices=1024, slicing='greedy', records=True):
         _require_cuda()
         if ordering not in ('native', 'reference'):
             raise ValueError('ordering must be "native" or "reference"')
@@ -187,6 +190,7 @@ class QAOAEnergyEngine:
         self.max_width = max_width
         self.max_slices = max_slices
         self.slicing = slicing
+        self.records = records
         self._cache = {}
         self._by_id = {}        # id(G) -> (weakref, nodes, p, key, edge count)
         self._edge_digests = {}  # id(edge subset) -> (subset, tuple, digest, length)
@@ -220,6 +224,7 @@ class QAOAEnergyEngine:
         plan.set_order_trials(self.order_trials)
         plan.set_max_width(self.max_width, self.max_slices)
         plan.set_slicing(self.slicing)
+        plan.set_records(self.records)
         if self.ordering == 'native':
             csr = graph_csr(G)
             index = {v: i for i, v in enumerate(csr[0])}

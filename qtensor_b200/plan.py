@@ -65,6 +65,11 @@ class NetworkPlan:
         (default on; only ``add_lightcones`` made afterwards)."""
         check(self._lib.qtb_plan_set_share_lightcones(self._h, 1 if enable else 0))
 
+    def set_records(self, enable):
+        """Per-element operand records for the shared-memory executors
+        (default on; set before ``upload``)."""
+        check(self._lib.qtb_plan_set_records(self._h, 1 if enable else 0))
+
     def add_circuit(self, n_qubits, gates, params, simplify_passes=0):
         gates = np.ascontiguousarray(gates, dtype=_lib.GATE_DTYPE)
         params = np.ascontiguousarray(params, dtype=np.float64)
@@ -134,7 +139,8 @@ class NetworkPlan:
                                                ('entries', _lib.ENTRY_DTYPE),
                                                ('terms', _lib.TERM_DTYPE),
                                                ('runs', _lib.RUN_DTYPE),
-                                               ('blobs', np.dtype('u1'))]):
+                                               ('blobs', np.dtype('u1')),
+                                               ('recs', np.dtype('<u4'))]):
             size = ctypes.c_size_t()
             check(self._lib.qtb_plan_export(self._h, which, None, 0, ctypes.byref(size)))
             buf = np.zeros(size.value // dtype.itemsize, dtype=dtype)

@@ -62,6 +62,10 @@ def gate_table(exported, params):
     return table
 
 
+# Shared memory one CTA may use; larger arenas have no chunk tables.
+SMEM_LIMIT_BYTES = 224 * 1024
+
+
 def _pext(x, m):
     """Bit gather on an integer array: the bits of x selected by mask m."""
     x = np.asarray(x, dtype=np.int64)
@@ -132,6 +136,9 @@ def run_network(exported, table, net_index):
         # 32-element chunk of the phase
         n_chunks = (int(ph['total_elems']) + 31) // 32
         co = int(ph['chunk_off'])
+        if 8 * int(net['arena_elems']) > SMEM_LIMIT_BYTES:   # wide: no chunk tables
+            assert co == 0
+            n_chunks = 0
         assert co + 2 * n_chunks <= len(blob)
         chunks = blob[co:co + 2 * n_chunks].view('<u2')
         starts = ops['elem_begin']
@@ -177,11 +184,61 @@ def run_network(exported, table, net_index):
     return table[res & ~_lib.SRC_TABLE] if res & _lib.SRC_TABLE else arena[res]
 
 
-def run_plan(plan, params, per_circuit=True):
-    """Amplitude of every circuit (slices summed), or of every network."""
+def run_network_records(exported, table, net_index):
+    """A network from its element records, as the shared-memory executor
+    reads them: one window S = [gate table, padded to an even length]
+    [arena]; every element's output and operand offsets point into S.
+    Checks that records cover the phases exactly, that every read hits an
+    element written before (or the gate table) and every write the arena."""
+    run = exported['runs'][net_index]
+    words = int(run['rec_words'])
+    assert words > 0
+    rec = exported['recs'][int(run['rec_off']):int(run['rec_off']) + words].astype(np.int64)
+    n_tab = int(exported['table_elems'])
+    pad = (n_tab + 1) & ~1
+    arena_elems = int(run['arena_elems'])
+    S = np.full(pad + arena_elems, np.nan + 0j, dtype=np.complex128)
+    S[:n_tab] = table
+    n_ph = int(run['n_phases'])
+    used = 2 * n_ph
+
+    def load(off):
+        v = S[off]
+        assert not np.isnan(v.real).any(), 'read of an element nobody wrote'
+        return v
+
+    for p in range(n_ph):
+        payload, head = int(rec[2 * p]), int(rec[2 * p + 1])
+        total, kmax = head & 0xffffff, head >> 24
+        assert 1 <= kmax
+        rows = rec[payload:payload + (kmax + 1) * total].reshape(kmax + 1, total)
+        used += (kmax + 1) * total
+        d = rows[0]
+        dst, k, s = d & 0xffff, (d >> 16) & 0xff, d >> 24
+        assert np.all((k >= 1) & (k <= kmax)) and np.all((s == 0) | (s == 1))
+        assert np.all((dst >= pad) & (dst < pad + arena_elems))
+        assert len(np.unique(dst)) == total
+        p0 = load(rows[1] & 0xffff)
+        p1 = load(rows[1] >> 16)
+        for t in range(2, kmax + 1):
+            live = t <= k
+            lo, hi = rows[t][live] & 0xffff, rows[t][live] >> 16
+            p0[live] = p0[live] * load(lo)
+            p1[live] = p1[live] * load(hi)
+        S[dst] = np.where(s == 1, p0 + p1, p0)
+    assert used == words
+    res = int(run['result_src'])
+    return table[res & ~_lib.SRC_TABLE] if res & _lib.SRC_TABLE else S[pad + res]
+
+
+def run_plan(plan, params, per_circuit=True, records=False):
+    """Amplitude of every circuit (slices summed), or of every network;
+    with ``records`` every network that has element records is run from
+    them."""
     ex = plan.export()
     table = gate_table(ex, np.asarray(params, dtype=np.float64))
-    vals = np.array([run_network(ex, table, i) for i in range(len(ex['runs']))])
+    vals = np.array([run_network_records(ex, table, i) if records and ex['runs'][i]['rec_words']
+                     else run_network(ex, table, i) for i in range(len(ex['runs']))])
     if not per_circuit:
         return vals
     groups = plan.groups()

@@ -159,16 +159,16 @@ def test_plain_path_matches_batched_and_reference(cuda_device, name, max_width):
     assert eng.compile(G, len(w['gamma']), w['gamma'], w['beta']).plan.device_status() == 0
 
 
-@pytest.mark.parametrize('cluster_max', [None, '0'])
+@pytest.mark.parametrize('cluster_max', [None, str(1 << 22)])
 def test_wide_networks_match_plain_path(cuda_device, monkeypatch, cluster_max):
     """Erdos-Renyi N=400 p=3 (seed 24323709) with the reference's greedy rule
     alone (order_trials=0, slicing from width 22): 247 networks too large
     for shared memory (3.5 GB of arenas) run beside the shared-memory
-    classes, by default as one thread-block cluster each when their arena
-    is at most 32 MB (K5) and in whole-GPU waves above (K4), and with
-    QTB_CLUSTER_MAX_ELEMS=0 all in waves; either way every edge term equals
-    the plain per-bucket path's (an independent execution of the same
-    plans) and the energies agree."""
+    classes, by default in whole-GPU waves (K4), and with
+    QTB_CLUSTER_MAX_ELEMS=2^22 as one thread-block cluster each when their
+    arena is at most 32 MB (K5) and in waves above; either way every edge
+    term equals the plain per-bucket path's (an independent execution of
+    the same plans) and the energies agree."""
     import networkx as nx
     if cluster_max is not None:
         monkeypatch.setenv('QTB_CLUSTER_MAX_ELEMS', cluster_max)
@@ -180,7 +180,7 @@ def test_wide_networks_match_plain_path(cuda_device, monkeypatch, cluster_max):
     cfg = cg.plan.last_launch_config()
     waves = [c for c in cfg if c[3] & 4]
     clusters = [c for c in cfg if c[3] & 64]
-    if cluster_max == '0':
+    if cluster_max is None:
         assert len(waves) >= 2 and not clusters
     else:
         assert clusters and clusters[0][0] >= 100
@@ -218,6 +218,25 @@ def test_every_schedule_matches_reference(cuda_device, monkeypatch, schedule):
         assert not any(c[3] & 2 for c in cfg)
     else:
         assert len(cfg) == 1 and cfg[0][3] & 2 and cfg[0][1] == 256
+
+
+@pytest.mark.parametrize('name,p,max_width', [('cfg3', 3, 29), ('cfg4', 4, 29), ('cfg2', 3, 11)])
+def test_element_records_match_blob_path(cuda_device, name, p, max_width):
+    """The shared-memory executor contracting from element records gives the
+    reference's edge terms, and the terms of the same plans decoded from
+    their blobs (records off): N=1000 p=3, N=256 p=4, and N=100 p=3 sliced
+    below its width."""
+    G, w = golden_graph(name)
+    ref = np.array([complex(*t) for t in w['terms']])
+    out = []
+    for records in (True, False):
+        eng = _engine(max_width=max_width, records=records)
+        terms = eng.edge_terms(G, w['gamma'], w['beta'])
+        assert np.max(np.abs(terms - ref)) < TOL
+        cfg = eng.compile(G, p, w['gamma'], w['beta']).plan.last_launch_config()
+        assert any(c[3] & 128 for c in cfg) == records
+        out.append(terms)
+    assert np.max(np.abs(out[0] - out[1])) < 1e-6
 
 
 def test_reference_named_simulator(cuda_device):

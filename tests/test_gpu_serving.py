@@ -40,21 +40,23 @@ def test_server_matches_reference(cuda_device):
 
 def _wide_requests():
     """Two wide requests of the serving stream: Erdos-Renyi N=400 p=3, whose
-    networks too large for shared memory run on the cluster executor, and
-    Erdos-Renyi N=335 p=3 (seed 949594894), whose widest edge (width 28,
-    arenas of about 5 GB) runs in whole-GPU waves."""
+    networks too large for shared memory run on the cluster executor when
+    QTB_CLUSTER_MAX_ELEMS allows it, and Erdos-Renyi N=335 p=3 (seed
+    949594894), whose widest edge (width 28, arenas of about 5 GB) runs in
+    whole-GPU waves."""
     er400 = nx.erdos_renyi_graph(400, 3 / 399, seed=24323709)
     er335 = graphs.erdos_renyi(graphs.ER_P3_N335['n'], graphs.ER_P3_N335['seed'])
     return [(er400,) + tuple(graphs.angles(3, seed=1)), (er335,) + tuple(graphs.angles(3, seed=2))]
 
 
-def test_alone_and_in_the_mix_agree(cuda_device):
+def test_alone_and_in_the_mix_agree(cuda_device, monkeypatch):
     """Each request's energy is identical whether it runs alone (one stream,
     one request at a time) or together with the others (four streams, all
     submitted at once), and equals the oracle's.  The mix holds small
     requests and two wide ones (cluster executor and wide waves), whose
     kernels overlap the others'."""
     from qtensor_b200.serve import QAOAServer
+    monkeypatch.setenv('QTB_CLUSTER_MAX_ELEMS', str(1 << 22))
     reqs = _requests(14)
     reqs = reqs[:7] + _wide_requests() + reqs[7:]
     with QAOAServer(n_streams=1) as srv:
@@ -69,10 +71,11 @@ def test_alone_and_in_the_mix_agree(cuda_device):
         assert abs(r.energy - ref) <= 1e-5 * max(1.0, abs(ref))
 
 
-def test_wide_requests_run_on_the_wide_executors(cuda_device):
+def test_wide_requests_run_on_the_wide_executors(cuda_device, monkeypatch):
     """The wide requests of the mix really use the cluster executor (K5) and
     the wide waves (K4): their plans' launch classes say so."""
     from qtensor_b200.engine import QAOAEnergyEngine
+    monkeypatch.setenv('QTB_CLUSTER_MAX_ELEMS', str(1 << 22))
     eng = QAOAEnergyEngine(order_trials=4)
     flags = []
     for G, gamma, beta in _wide_requests():

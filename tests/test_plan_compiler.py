@@ -96,6 +96,60 @@ def test_native_plan_cfg3_shape():
     assert all(i['angle_specific'] == 0 for i in infos)
 
 
+@pytest.mark.parametrize('name', ['cfg1_default', 'cfg1_cx', 'test_random_n4_p4_d3', 'test_grid2d_n3_p3_d0',
+                                  'test_line_n8_p4_d0'])
+def test_element_records_match_reference(name):
+    """Every network's element records (resolved operand offsets in the
+    shared window) give the reference amplitude, reading only elements
+    written before them.  Networks whose arena cannot be in shared memory
+    have none."""
+    G, w = golden_graph(name)
+    plan = _ref_plan(G, w, w['composer'])
+    ex = plan.export()
+    has = ex['runs']['rec_words'] > 0
+    arena_bytes = 8 * ex['runs']['arena_elems'].astype(np.int64)
+    assert np.any(has)
+    assert np.all(has[arena_bytes <= 200 * 1024]) and not np.any(has[arena_bytes > 224 * 1024])
+    vals = plan_interp.run_plan(plan, _params(w), records=True)
+    ref = np.array([complex(*t) for t in w['terms']])
+    assert np.max(np.abs(vals - ref)) < 1e-12
+
+
+def test_element_records_sliced_and_native():
+    """Records of native-order and sliced networks (N=100 p=3 sample,
+    forced below its width) sum to the reference terms."""
+    G, w = golden_graph('cfg2')
+    edges = list(G.edges())[::10]
+    plan = NetworkPlan(6)
+    plan.set_max_width(11)
+    plan.add_lightcones(graph_csr(G), np.array(edges), 3, 0, _params(w), threads=4)
+    assert max(i['n_slices'] for i in plan.infos()) > 1
+    vals = plan_interp.run_plan(plan, _params(w), records=True)
+    ref = np.array([complex(*w['terms'][k]) for k in range(0, len(w['edges']), 10)])
+    assert np.max(np.abs(vals - ref)) < 1e-12
+
+
+def test_element_records_follow_shared_blobs():
+    """Networks with one blob share one copy of its records; with records
+    off the plan has none."""
+    G, w = golden_graph('cfg3')
+    edges = np.array(list(G.edges())[:300])
+    plan = NetworkPlan(6)
+    plan.add_lightcones(graph_csr(G), edges, 3, 0, _params(w))
+    runs = plan.export()['runs']
+    assert np.all(runs['rec_words'] > 0)
+    by_blob = {}
+    for r in runs:
+        by_blob.setdefault(int(r['blob_off16']), set()).add((int(r['rec_off']), int(r['rec_words'])))
+    assert all(len(v) == 1 for v in by_blob.values())
+    assert len({int(r['rec_off']) for r in runs}) == len(by_blob) < len(runs)
+    off = NetworkPlan(6)
+    off.set_records(False)
+    off.add_lightcones(graph_csr(G), edges, 3, 0, _params(w))
+    ex = off.export()
+    assert len(ex['recs']) == 0 and np.all(ex['runs']['rec_words'] == 0)
+
+
 def test_simplifier_keeps_reference_hadamard_merge():
     """The reference simplifier turns H.H on one qubit into a single H
     (simplify_circuit.py:69-70 with gates.py hadamard); the plan does too."""
@@ -217,7 +271,7 @@ def test_images_follow_networks_added_after_an_export():
     whole.add_lightcones(graph_csr(G), edges, 2, 0, params)
     a, b = split.export(), whole.export()
     assert len(a['nets']) == len(edges) > len(first['nets'])
-    for key in ('nets', 'ops', 'ins', 'phases', 'runs', 'blobs'):
+    for key in ('nets', 'ops', 'ins', 'phases', 'runs', 'blobs', 'recs'):
         assert np.array_equal(a[key], b[key]), key
     assert np.max(np.abs(plan_interp.run_plan(split, params) - plan_interp.run_plan(whole, params))) == 0
 
