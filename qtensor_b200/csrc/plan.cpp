@@ -1999,10 +1999,13 @@ void build_blobs(qtb_plan* plan) {
         if (r.blob_off16 == (uint32_t)(base / 16)) {
             offs.push_back((uint32_t)plan->druns.size());
             const uint32_t words = records ? record_words(n, table_pad, smem_elems) : 0u;
-            if (words && rec_total + words <= kRecMaxWords) {
-                r.rec_off = (uint32_t)rec_total;
+            // each network's records start on 16 bytes: the executor reads
+            // the phase headers as 8-byte pairs
+            const uint64_t start = (rec_total + 3) & ~uint64_t(3);
+            if (words && start + words <= kRecMaxWords) {
+                r.rec_off = (uint32_t)start;
                 r.rec_words = words;
-                rec_total += words;
+                rec_total = start + words;
                 rec_todo.emplace_back((int32_t)plan->druns.size(), r.rec_off);
             }
         }

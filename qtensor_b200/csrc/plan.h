@@ -88,8 +88,8 @@ struct DevNetRun {
     uint32_t pad1;
 };
 
-// Element records of a network (u32 words at DevNetRun::rec_off in the
-// plan's record array), for executors whose gate table and arena share one
+// Element records of a network (u32 words at DevNetRun::rec_off, a multiple
+// of 4, in the plan's record array), for executors whose gate table and arena share one
 // shared-memory window S = [gate table, padded to an even element count]
 // [arena]:
 //   [phase header x n_phases][phase payloads]

@@ -193,6 +193,7 @@ def run_network_records(exported, table, net_index):
     run = exported['runs'][net_index]
     words = int(run['rec_words'])
     assert words > 0
+    assert int(run['rec_off']) % 4 == 0       # 16-byte aligned: headers are read as 8-byte pairs
     rec = exported['recs'][int(run['rec_off']):int(run['rec_off']) + words].astype(np.int64)
     n_tab = int(exported['table_elems'])
     pad = (n_tab + 1) & ~1
