@@ -363,6 +363,22 @@ __device__ __forceinline__ uint32_t find_op(uint32_t g, uint32_t oi, DevOp& op, 
     return oi;
 }
 
+// The op of a phase holding element g: the last of ops lo..hi whose first
+// element is at most g, by binary search (kGlobal: the ops are in global
+// memory, read through the read-only path).  Networks whose arena cannot be
+// in shared memory carry no chunk tables (DevPhase::chunk_off 0); their ops
+// are found this way.
+template <bool kGlobal>
+__device__ __forceinline__ uint32_t search_op(const DevOp* ops, uint32_t lo, uint32_t hi, uint32_t g) {
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1u) >> 1;
+        const uint32_t first = kGlobal ? __ldg(&ops[mid].elem_begin) : ops[mid].elem_begin;
+        if (first <= g) lo = mid;
+        else hi = mid - 1u;
+    }
+    return lo;
+}
+
 // One output element j of op: the product of its operands gathered at j
 // (and at j with the summed bit set), summed over the bucket variable.
 // Operands are taken one at a time: most ops have two or three, and a fixed
@@ -440,7 +456,8 @@ __device__ float2 contract_network(const DevNetRun& net, const unsigned char* bl
             if (g >= op_end) {
                 // the chunk table names the op of g's 32-element chunk; small
                 // ops may share a chunk, so step forward to the one holding g
-                oi = chunk[g / kChunkElems];
+                oi = ph.chunk_off ? chunk[g / kChunkElems]
+                                  : search_op<false>(ops, ph.op_first, ph.op_first + ph.op_count - 1u, g);
                 op = ops[oi];
                 oi = find_op(g, oi, op, [&](uint32_t i) { return ops[i]; });
                 op_end = op.elem_begin + (1u << (op.u - op.sum));
@@ -727,7 +744,8 @@ __global__ void __launch_bounds__(kWarpMaxThreads) qtb_warp_network_kernel(const
             for (uint32_t r = 0; r * 32u < ph.total_elems; ++r) {
                 const uint32_t g = r * 32u + lane;
                 if (g < ph.total_elems) {
-                    uint32_t oi = chunk[r];
+                    uint32_t oi = ph.chunk_off ? chunk[r]
+                                               : search_op<false>(ops, ph.op_first, ph.op_first + ph.op_count - 1u, g);
                     DevOp op = ops[oi];
                     find_op(g, oi, op, [&](uint32_t i) { return ops[i]; });
                     compute_element<kSmemTable>(op, g - op.elem_begin, ins, table, arena);
@@ -1022,7 +1040,7 @@ __global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArg
         const uint16_t* chunk = nullptr;
         float2* arena = nullptr;
         DevOp op{};
-        uint32_t op_last = 0;
+        uint32_t op_first = 0, op_last = 0;
         const uint32_t bd = blockDim.x;
         for (uint32_t g = e0 + threadIdx.x; g < e1;) {
             if (g < seg_lo || g >= seg_hi) {
@@ -1042,8 +1060,9 @@ __global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArg
                 ph_total = ph.total_elems;
                 ops = reinterpret_cast<const DevOp*>(blob + net.n_phases * sizeof(DevPhase));
                 ins = reinterpret_cast<const DevIn*>(blob + net.ins_off);
-                chunk = reinterpret_cast<const uint16_t*>(blob + ph.chunk_off);
+                chunk = ph.chunk_off ? reinterpret_cast<const uint16_t*>(blob + ph.chunk_off) : nullptr;
                 arena = w.arenas + wn.arena_off;
+                op_first = ph.op_first;
                 op_last = ph.op_first + ph.op_count - 1u;
                 op_lo = 1u;
                 op_hi = 0u;
@@ -1054,7 +1073,7 @@ __global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArg
                 continue;
             }
             if (l < op_lo || l >= op_hi) {
-                const uint32_t oi = __ldg(chunk + l / kChunkElems);
+                const uint32_t oi = chunk ? __ldg(chunk + l / kChunkElems) : search_op<true>(ops, op_first, op_last, l);
                 op = ldg_op(ops + oi);
                 find_op(l, oi, op, [&](uint32_t i) { return ldg_op(ops + min(i, op_last)); });
                 op_lo = op.elem_begin;
@@ -1106,18 +1125,6 @@ constexpr int kClusterCtas = 8;
 constexpr int kClusterThreads = 256;
 constexpr uint32_t kClusterChunk = 2048;                     // elements per CTA turn (8 per thread)
 
-// The op of a phase holding element g: the last of ops lo..hi whose first
-// element is at most g (binary search through the read-only path; wide
-// networks carry no chunk tables).
-__device__ __forceinline__ uint32_t search_op(const DevOp* ops, uint32_t lo, uint32_t hi, uint32_t g) {
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi + 1u) >> 1;
-        if (__ldg(&ops[mid].elem_begin) <= g) lo = mid;
-        else hi = mid - 1u;
-    }
-    return lo;
-}
-
 __global__ void __launch_bounds__(kClusterThreads) qtb_cluster_kernel(const ClusterJob* __restrict__ jobs,
                                                                       float2* __restrict__ arenas, const RunArgs a) {
     uint32_t rank, nctas;
@@ -1136,7 +1143,7 @@ __global__ void __launch_bounds__(kClusterThreads) qtb_cluster_kernel(const Clus
         const uint32_t op_first = pv.x, op_count = pv.y, total = pv.z;
         const uint32_t op_last = op_first + op_count - 1u;
         for (uint32_t base = rank * kClusterChunk; base < total; base += nctas * kClusterChunk) {
-            uint32_t oi = search_op(ops, op_first, op_last, base);
+            uint32_t oi = search_op<true>(ops, op_first, op_last, base);
             DevOp op = ldg_op(ops + oi);
             const uint32_t size = 1u << (op.u - op.sum);
             if (size >= kClusterChunk && base + kClusterChunk <= total) {
@@ -1149,7 +1156,7 @@ __global__ void __launch_bounds__(kClusterThreads) qtb_cluster_kernel(const Clus
                     const uint32_t g = base + t + e * kClusterThreads;
                     if (g >= total) break;
                     if (g >= op_hi) {
-                        oi = search_op(ops, oi, op_last, g);
+                        oi = search_op<true>(ops, oi, op_last, g);
                         op = ldg_op(ops + oi);
                         op_hi = op.elem_begin + (1u << (op.u - op.sum));
                     }
