@@ -94,7 +94,9 @@ TERM_DTYPE = np.dtype([('param', '<i4'), ('pad', '<i4'), ('coef', '<f8')])
 RUN_DTYPE = np.dtype([('blob_off16', '<u4'), ('blob_bytes', '<u4'), ('n_phases', '<u4'),
                       ('ins_off', '<u4'), ('arena_elems', '<u4'), ('result_src', '<u4'),
                       ('max_elems', '<u4'), ('tail_start', '<u4'), ('rec_off', '<u4'),
-                      ('rec_words', '<u4'), ('pad0', '<u4'), ('pad1', '<u4')])
+                      ('rec_words', '<u4'), ('rec_format', '<u4'), ('pad1', '<u4')])
+REC_WIDE = 1
+REC_COMPACT = 2
 SRC_TABLE = 0x80000000
 STATUS_WAIT_TIMEOUT = 16
 

@@ -1859,14 +1859,64 @@ static uint32_t phase_kmax(const Network& n, const DevPhase& ph) {
 // cannot have them: an op without operands or with more than kRecMaxK, an
 // arena past the shared-memory window (`smem_elems` complex64 elements
 // beside the gate table), or window offsets past 16 bits.
-static uint32_t record_words(const Network& n, uint32_t table_pad, uint64_t smem_elems) {
+// Format of a network's element records (kRecCompact when its window and
+// operand counts allow, else kRecWide), or 0 when it cannot have them.
+static uint32_t record_format(const Network& n, uint32_t table_pad, uint64_t smem_elems) {
     const uint64_t arena = n.info.arena_elems;
     if (arena > smem_elems || table_pad + arena > 0xffffu) return 0;
-    for (const DevOp& op : n.ops)
+    uint32_t kmax = 0;
+    for (const DevOp& op : n.ops) {
         if (op.k < 1 || op.k > kRecMaxK) return 0;
+        kmax = std::max<uint32_t>(kmax, op.k);
+    }
+    return (table_pad + arena <= kRecCompactWindow && kmax <= kRecCompactMaxK) ? kRecCompact : kRecWide;
+}
+
+static uint32_t record_words(const Network& n, uint32_t format) {
     uint64_t words = 2 * n.phases.size();
-    for (const DevPhase& ph : n.phases) words += (uint64_t)(phase_kmax(n, ph) + 1) * ph.total_elems;
+    if (format == kRecCompact) {
+        words = (words + 3) & ~uint64_t(3);
+        for (const DevPhase& ph : n.phases) words += 4 * (uint64_t)ph.total_elems;
+    } else {
+        for (const DevPhase& ph : n.phases) words += (uint64_t)(phase_kmax(n, ph) + 1) * ph.total_elems;
+    }
     return words > 0xffffffffu ? 0 : (uint32_t)words;
+}
+
+// Offsets of operand d of an op (output bits `low`, summed bit w) for every
+// output element j, passed to emit(j, offset at summed variable 0, stride
+// to its offset at 1 or 0).  Gathers the low byte of j from a table.
+template <typename Emit>
+static void operand_offsets(const DevOp& op, const DevIn& d, uint32_t table_pad, uint32_t* lo_tab, Emit emit) {
+    const uint32_t w = (uint32_t)op.u - op.sum;
+    const uint32_t low = (1u << w) - 1u;
+    const uint32_t m = d.mask & low;
+    const uint32_t src = (d.src & kSrcTable) ? (d.src & ~kSrcTable) : table_pad + d.src;
+    const uint32_t stride = (op.sum && ((d.mask >> w) & 1u)) ? 1u << (__builtin_popcount(d.mask) - 1) : 0u;
+    const uint32_t m_lo = m & 0xffu, shift = (uint32_t)__builtin_popcount(m_lo);
+    const uint32_t n_lo = std::min(low, 255u) + 1u;
+    for (uint32_t x = 0; x < n_lo; ++x) lo_tab[x] = pext_bits(x, m_lo);
+    for (uint32_t hi = 0; hi <= (low >> 8); ++hi) {
+        const uint32_t hoff = src + (pext_bits(hi, m >> 8) << shift);
+        for (uint32_t x = 0; x < n_lo; ++x) emit((hi << 8) | x, hoff + lo_tab[x], stride);
+    }
+}
+
+// One phase of compact records (layout at kRecCompact), 8 fields per element.
+static void fill_compact_phase(const Network& n, const DevPhase& ph, uint32_t table_pad, uint16_t* f,
+                               uint32_t* lo_tab) {
+    for (uint32_t o = ph.op_first; o < ph.op_first + ph.op_count; ++o) {
+        const DevOp& op = n.ops[o];
+        const uint32_t low = (1u << ((uint32_t)op.u - op.sum)) - 1u;
+        uint16_t* r = f + 8 * (size_t)op.elem_begin;
+        for (uint32_t j = 0; j <= low; ++j)
+            r[8 * j] = (uint16_t)((table_pad + op.dst + j) | (uint32_t)(op.k - 1) << 12 | (uint32_t)op.sum << 15);
+        for (uint32_t t = 0; t < op.k; ++t)
+            operand_offsets(op, n.ins[op.in_begin + t], table_pad, lo_tab, [&](uint32_t j, uint32_t o0, uint32_t stride) {
+                const uint32_t code = stride ? (uint32_t)__builtin_ctz(stride) + 1u : 0u;
+                r[8 * j + 1 + t] = (uint16_t)(o0 | code << 12);
+            });
+    }
 }
 
 // Writes a network's element records into rec (record_words words, zeroed),
@@ -1875,9 +1925,10 @@ static uint32_t record_words(const Network& n, uint32_t table_pad, uint64_t smem
 // would do, resolved once: the bits of element j that the operand's mask
 // selects, packed, plus its source; the summed variable is the operand's
 // top axis.
-static void fill_records(const Network& n, uint32_t table_pad, uint32_t* rec) {
+static void fill_records(const Network& n, uint32_t table_pad, uint32_t format, uint32_t* rec) {
     const size_t n_ph = n.phases.size();
-    uint32_t payload = (uint32_t)(2 * n_ph);
+    const bool compact = format == kRecCompact;
+    uint32_t payload = (uint32_t)(compact ? (2 * n_ph + 3) & ~size_t(3) : 2 * n_ph);
     uint32_t lo_tab[256];
     for (size_t p = 0; p < n_ph; ++p) {
         const DevPhase& ph = n.phases[p];
@@ -1885,6 +1936,11 @@ static void fill_records(const Network& n, uint32_t table_pad, uint32_t* rec) {
         const uint32_t total = ph.total_elems;
         rec[2 * p] = payload;
         rec[2 * p + 1] = total | kmax << 24;
+        if (compact) {
+            fill_compact_phase(n, ph, table_pad, reinterpret_cast<uint16_t*>(rec + payload), lo_tab);
+            payload += 4 * total;
+            continue;
+        }
         uint32_t* row = rec + payload;
         for (uint32_t o = ph.op_first; o < ph.op_first + ph.op_count; ++o) {
             const DevOp& op = n.ops[o];
@@ -1992,19 +2048,22 @@ void build_blobs(qtb_plan* plan) {
                 r.blob_off16 = prev.blob_off16;
                 r.rec_off = prev.rec_off;
                 r.rec_words = prev.rec_words;
+                r.rec_format = prev.rec_format;
                 plan->dblobs.resize(base);
                 break;
             }
         }
         if (r.blob_off16 == (uint32_t)(base / 16)) {
             offs.push_back((uint32_t)plan->druns.size());
-            const uint32_t words = records ? record_words(n, table_pad, smem_elems) : 0u;
+            const uint32_t format = records ? record_format(n, table_pad, smem_elems) : 0u;
+            const uint32_t words = format ? record_words(n, format) : 0u;
             // each network's records start on 16 bytes: the executor reads
-            // the phase headers as 8-byte pairs
+            // phase headers as 8-byte pairs and compact records as 16 bytes
             const uint64_t start = (rec_total + 3) & ~uint64_t(3);
             if (words && start + words <= kRecMaxWords) {
                 r.rec_off = (uint32_t)start;
                 r.rec_words = words;
+                r.rec_format = format;
                 rec_total = start + words;
                 rec_todo.emplace_back((int32_t)plan->druns.size(), r.rec_off);
             }
@@ -2014,7 +2073,8 @@ void build_blobs(qtb_plan* plan) {
     plan->drecs.assign(rec_total, 0u);
     parallel_for((int32_t)rec_todo.size(), 0, [&](int32_t t) {
         const auto& job = rec_todo[t];
-        fill_records(plan->nets[job.first], table_pad, plan->drecs.data() + job.second);
+        fill_records(plan->nets[job.first], table_pad, plan->druns[job.first].rec_format,
+                     plan->drecs.data() + job.second);
     });
 }
 

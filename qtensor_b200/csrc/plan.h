@@ -84,7 +84,7 @@ struct DevNetRun {
     uint32_t tail_start;   // phases from here on have <= 32 elements each
     uint32_t rec_off;      // first word of the network's element records
     uint32_t rec_words;    // 0: the network has no element records
-    uint32_t pad0;
+    uint32_t rec_format;   // kRecWide or kRecCompact (when rec_words != 0)
     uint32_t pad1;
 };
 
@@ -100,7 +100,20 @@ struct DevNetRun {
 //     row 1 + t = operand t: S offset at the summed variable 0 (low 16 bits)
 //                 and at 1 (high 16 bits; equal when the operand lacks it)
 // Every offset the bit gathers of the op would compute is resolved on the
-// host, so the executor only loads and multiplies.
+// host, so the executor only loads and multiplies.  That is the wide
+// format (kRecWide).  A network whose window has at most kRecCompactWindow
+// elements and whose ops have at most kRecCompactMaxK operands uses the
+// compact format (kRecCompact) instead: the same headers, padded to 16
+// bytes, then per phase one 16-byte record per element (element-major),
+// eight 16-bit fields:
+//     field 0     = S offset of the output | (k - 1) << 12 | sum << 15
+//     field 1 + t = operand t: S offset at the summed variable 0 | c << 12,
+//                   its offset at 1 being that + ((1 << c) >> 1)
+// (c = 0 when the operand lacks the summed variable; 0 for t >= k).
+constexpr uint32_t kRecWide = 1;
+constexpr uint32_t kRecCompact = 2;
+constexpr uint32_t kRecCompactWindow = 4096;
+constexpr uint32_t kRecCompactMaxK = 7;
 constexpr uint32_t kRecMaxK = 8;                    // operands per op with records
 constexpr uint64_t kRecMaxWords = uint64_t(1) << 26;   // record words per plan (256 MiB)
 constexpr uint32_t kSmemTableLimitElems = 2048;   // 16 KB of gate table per CTA

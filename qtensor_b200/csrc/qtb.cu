@@ -559,6 +559,72 @@ __device__ float2 contract_records(const DevNetRun& net, const uint32_t* __restr
     return result;
 }
 
+// One output element from its compact record (kRecCompact): the same
+// products, in the same operand order, as compute_element.
+__device__ __forceinline__ void rec_element_compact(const uint4 r, float2* __restrict__ S) {
+    const uint32_t f[8] = {r.x & 0xffffu, r.x >> 16, r.y & 0xffffu, r.y >> 16,
+                           r.z & 0xffffu, r.z >> 16, r.w & 0xffffu, r.w >> 16};
+    const uint32_t k = ((f[0] >> 12) & 7u) + 1u;
+    const uint32_t o = f[1] & 0xfffu;
+    float2 p0 = S[o], p1 = S[o + ((1u << (f[1] >> 12)) >> 1)];
+#pragma unroll
+    for (uint32_t t = 2; t <= kRecCompactMaxK; ++t)
+        if (t <= k) {
+            const uint32_t ot = f[t] & 0xfffu;
+            p0 = cmul(p0, S[ot]);
+            p1 = cmul(p1, S[ot + ((1u << (f[t] >> 12)) >> 1)]);
+        }
+    S[f[0] & 0xfffu] = (f[0] >> 15) ? make_float2(p0.x + p1.x, p0.y + p1.y) : p0;
+}
+
+// Phase headers a CTA stages in shared memory for a compact-record network
+// (networks with more phases read the rest from global memory).
+constexpr uint32_t kRecHeadSmem = 64;
+
+// The phases of one network from its compact records.  The phase headers
+// are staged in shared memory; each thread's record of its first element
+// in the next three phases is in flight while the current phase computes,
+// so the loads from L2 overlap three phases and their barriers.  Same
+// phase split as contract_network.
+__device__ float2 contract_records_compact(const DevNetRun& net, const uint32_t* __restrict__ rec,
+                                           float2* __restrict__ S, const float2* __restrict__ arena,
+                                           uint2* __restrict__ s_head) {
+    const uint32_t tid = threadIdx.x, np = net.n_phases;
+    const uint2* ghead = reinterpret_cast<const uint2*>(rec);
+    const bool staged = np <= kRecHeadSmem;
+    if (staged)
+        for (uint32_t i = tid; i < np; i += blockDim.x) s_head[i] = __ldg(ghead + i);
+    __syncthreads();
+    auto head = [&](uint32_t p) {
+        return p >= np ? make_uint2(0u, 0u) : staged ? s_head[p] : __ldg(ghead + p);
+    };
+    auto first = [&](uint32_t p) {
+        const uint2 h = head(p);
+        return tid < (h.y & 0xffffffu) ? __ldg(reinterpret_cast<const uint4*>(rec + h.x) + tid)
+                                       : make_uint4(0u, 0u, 0u, 0u);
+    };
+    uint4 r0 = first(0), r1 = first(1), r2 = first(2);
+    for (uint32_t p = 0; p < np; ++p) {
+        const bool tail = p >= net.tail_start;
+        if (tail && tid >= 32) break;
+        const uint4 r3 = first(p + 3);
+        const uint2 h = head(p);
+        const uint32_t total = h.y & 0xffffffu;
+        if (tid < total) rec_element_compact(r0, S);
+        for (uint32_t g = tid + blockDim.x; g < total; g += blockDim.x)
+            rec_element_compact(__ldg(reinterpret_cast<const uint4*>(rec + h.x) + g), S);
+        if (tail) __syncwarp();
+        else __syncthreads();
+        r0 = r1;
+        r1 = r2;
+        r2 = r3;
+    }
+    float2 result = make_float2(0.f, 0.f);
+    if (tid == 0)
+        result = (net.result_src & kSrcTable) ? S[net.result_src & ~kSrcTable] : arena[net.result_src];
+    return result;
+}
+
 // Network executor.  Shared memory, in order: mbarrier (16 B), [plan-wide
 // gate entries + angle terms], the network's plan blob, [gate table],
 // [arena]; the bracketed parts exist when kSmemTable / kSmemArena.
@@ -587,6 +653,7 @@ __global__ void __launch_bounds__(kLean == 2 ? 96 : kLean ? 128 : (kPersistent ?
     float2* arena = kSmemArena ? reinterpret_cast<float2*>(after_table)
                                : a.gscratch + (size_t)blockIdx.x * a.arena_capacity;
     __shared__ unsigned int s_job, is_last;
+    __shared__ uint2 s_head[kSmemArena && kSmemTable ? kRecHeadSmem : 1];
     if (kPersistent && a.queue == nullptr) {   // a persistent launch needs its queue
         if (threadIdx.x == 0) atomicOr(a.status, kStatusQueue);
         return;
@@ -631,8 +698,11 @@ __global__ void __launch_bounds__(kLean == 2 ? 96 : kLean ? 128 : (kPersistent ?
         }
         const unsigned char* nblob =
             staged ? blob : reinterpret_cast<const unsigned char*>(a.blobs + net.blob_off16);
-        const float2 term = records ? contract_records(net, a.recs + net.rec_off, stable, arena)
-                                    : contract_network<kSmemTable>(net, nblob, table, arena);
+        float2 term;
+        if (!records) term = contract_network<kSmemTable>(net, nblob, table, arena);
+        else if (net.rec_format == kRecCompact)
+            term = contract_records_compact(net, a.recs + net.rec_off, stable, arena, s_head);
+        else term = contract_records(net, a.recs + net.rec_off, stable, arena);
         if (threadIdx.x == 0) {
             *job.term = term;
             if (a.energy) {

@@ -208,12 +208,35 @@ def run_network_records(exported, table, net_index):
         assert not np.isnan(v.real).any(), 'read of an element nobody wrote'
         return v
 
+    compact = int(run['rec_format']) == _lib.REC_COMPACT
+    if compact:
+        assert pad + arena_elems <= 4096
+        used = (used + 3) & ~3
     for p in range(n_ph):
         payload, head = int(rec[2 * p]), int(rec[2 * p + 1])
         total, kmax = head & 0xffffff, head >> 24
         assert 1 <= kmax
-        rows = rec[payload:payload + (kmax + 1) * total].reshape(kmax + 1, total)
-        used += (kmax + 1) * total
+        if compact:
+            # 8 little-endian 16-bit fields per element, decoded into the
+            # rows of the wide format
+            assert payload % 4 == 0 and kmax <= 7
+            f = exported['recs'][int(run['rec_off']) + payload:int(run['rec_off']) + payload + 4 * total]
+            f = f.view('<u2').astype(np.int64).reshape(total, 8)
+            used += 4 * total
+            d = f[:, 0]
+            k = ((d >> 12) & 7) + 1
+            assert np.all(k <= kmax)
+            rows = np.zeros((kmax + 1, total), dtype=np.int64)
+            rows[0] = (d & 0xfff) | k << 16 | (d >> 15) << 24
+            for t in range(kmax):
+                o0 = f[:, 1 + t] & 0xfff
+                code = f[:, 1 + t] >> 12
+                o1 = o0 + ((1 << code) >> 1)
+                assert np.all((f[:, 1 + t] == 0) | (t < k))
+                rows[1 + t] = np.where(t < k, o0 | o1 << 16, 0)
+        else:
+            rows = rec[payload:payload + (kmax + 1) * total].reshape(kmax + 1, total)
+            used += (kmax + 1) * total
         d = rows[0]
         dst, k, s = d & 0xffff, (d >> 16) & 0xff, d >> 24
         assert np.all((k >= 1) & (k <= kmax)) and np.all((s == 0) | (s == 1))

@@ -110,6 +110,9 @@ def test_element_records_match_reference(name):
     arena_bytes = 8 * ex['runs']['arena_elems'].astype(np.int64)
     assert np.any(has)
     assert np.all(has[arena_bytes <= 200 * 1024]) and not np.any(has[arena_bytes > 224 * 1024])
+    formats = set(ex['runs']['rec_format'][has].tolist())
+    if name == 'test_grid2d_n3_p3_d0':        # windows above and below 4096 elements
+        assert formats == {_lib.REC_WIDE, _lib.REC_COMPACT}
     vals = plan_interp.run_plan(plan, _params(w), records=True)
     ref = np.array([complex(*t) for t in w['terms']])
     assert np.max(np.abs(vals - ref)) < 1e-12
