@@ -253,6 +253,9 @@ struct RunArgs {
     uint32_t table_elems;
     const double* params;
     const uint32_t* recs;         // element records, or null: this launch reads plan blobs only
+    uint32_t recs_bytes;          // of the plan's whole record array
+    uint32_t runs_bytes;          // of the plan's DevNetRun array
+    const DevNetRun* runs;
     const float2* gtable;         // global gate table (kernels without a shared table)
     float2* gscratch;             // global arenas (kernels without a shared arena)
     uint32_t arena_capacity;      // elements per CTA
@@ -486,6 +489,24 @@ __device__ float2 contract_network(const DevNetRun& net, const unsigned char* bl
 }
 
 // ------------------------------------------- element records (see plan.h)
+// Part i of n of [p, p + bytes) into L2: a hint with nothing to wait for.
+// A launch whose CTAs each bring their part of the plan's small arrays
+// (records, runs, jobs) into L2 at once turns every CTA's later first
+// touches into L2 hits, instead of DRAM misses on the chain of dependent
+// loads that starts each network (after an L2 flush, or on a new plan).
+constexpr uint32_t kL2PrefetchMaxBytes = 32u << 20;
+__device__ __forceinline__ void l2_prefetch_part(const void* p, uint32_t bytes, uint32_t i, uint32_t n) {
+    bytes &= ~15u;
+    if (p == nullptr || bytes == 0 || bytes > kL2PrefetchMaxBytes) return;
+    const uint32_t part = ((bytes + n - 1u) / n + 15u) & ~15u;
+    const uint64_t begin = (uint64_t)i * part;
+    if (begin >= bytes) return;
+    const uint32_t size = (uint32_t)min((uint64_t)part, (uint64_t)bytes - begin);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(static_cast<const char*>(p) + begin),
+                 "r"(size)
+                 : "memory");
+}
+
 // Header of phase p of a network's records (zero elements past the last).
 struct RecHead {
     const uint32_t* rows;   // payload: row r of element g at rows[r * total + g]
@@ -657,6 +678,11 @@ __global__ void __launch_bounds__(kLean == 2 ? 96 : kLean ? 128 : (kPersistent ?
     if (kPersistent && a.queue == nullptr) {   // a persistent launch needs its queue
         if (threadIdx.x == 0) atomicOr(a.status, kStatusQueue);
         return;
+    }
+    if (threadIdx.x == 0) {
+        l2_prefetch_part(a.recs, a.recs_bytes, blockIdx.x, gridDim.x);
+        l2_prefetch_part(a.runs, a.runs_bytes, blockIdx.x, gridDim.x);
+        l2_prefetch_part(jobs, a.n_jobs * (uint32_t)sizeof(Job), blockIdx.x, gridDim.x);
     }
     mbar_init(bar);
     uint32_t parity = 0;
@@ -2458,6 +2484,9 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
     a.table_elems = plan->table_elems;
     a.params = params_dev;
     a.recs = static_cast<const uint32_t*>(plan->dev.recs);
+    a.recs_bytes = (uint32_t)(plan->drecs.size() * sizeof(uint32_t));
+    a.runs = static_cast<const DevNetRun*>(plan->dev.runs);
+    a.runs_bytes = (uint32_t)std::min<size_t>(plan->druns.size() * sizeof(DevNetRun), 0xffffffffu);
     a.gtable = static_cast<const float2*>(plan->dev.table);
     a.status = static_cast<int*>(plan->dev.status);
     a.done = rc->done;
