@@ -1902,13 +1902,34 @@ static void operand_offsets(const DevOp& op, const DevIn& d, uint32_t table_pad,
     }
 }
 
+// First record of every op of a phase (indexed from op_first): the ops in
+// order of decreasing operand count (stable), so that the 32 elements a
+// warp takes mostly share it and its loop over operands.  Each record
+// names its own output, so the order is free.
+static void record_positions(const Network& n, const DevPhase& ph, std::vector<uint32_t>& pos) {
+    std::vector<uint32_t> order(ph.op_count);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+        return n.ops[ph.op_first + x].k > n.ops[ph.op_first + y].k;
+    });
+    pos.assign(ph.op_count, 0u);
+    uint32_t next = 0;
+    for (uint32_t x : order) {
+        const DevOp& op = n.ops[ph.op_first + x];
+        pos[x] = next;
+        next += 1u << ((uint32_t)op.u - op.sum);
+    }
+}
+
 // One phase of compact records (layout at kRecCompact), 8 fields per element.
 static void fill_compact_phase(const Network& n, const DevPhase& ph, uint32_t table_pad, uint16_t* f,
                                uint32_t* lo_tab) {
+    std::vector<uint32_t> pos;
+    record_positions(n, ph, pos);
     for (uint32_t o = ph.op_first; o < ph.op_first + ph.op_count; ++o) {
         const DevOp& op = n.ops[o];
         const uint32_t low = (1u << ((uint32_t)op.u - op.sum)) - 1u;
-        uint16_t* r = f + 8 * (size_t)op.elem_begin;
+        uint16_t* r = f + 8 * (size_t)pos[o - ph.op_first];
         for (uint32_t j = 0; j <= low; ++j)
             r[8 * j] = (uint16_t)((table_pad + op.dst + j) | (uint32_t)(op.k - 1) << 12 | (uint32_t)op.sum << 15);
         for (uint32_t t = 0; t < op.k; ++t)
@@ -1942,8 +1963,11 @@ static void fill_records(const Network& n, uint32_t table_pad, uint32_t format, 
             continue;
         }
         uint32_t* row = rec + payload;
+        std::vector<uint32_t> pos;
+        record_positions(n, ph, pos);
         for (uint32_t o = ph.op_first; o < ph.op_first + ph.op_count; ++o) {
             const DevOp& op = n.ops[o];
+            const uint32_t first = pos[o - ph.op_first];
             const uint32_t w = (uint32_t)op.u - op.sum;
             const uint32_t low = (1u << w) - 1u;
             for (uint32_t t = 0; t < op.k; ++t) {
@@ -1951,7 +1975,7 @@ static void fill_records(const Network& n, uint32_t table_pad, uint32_t format, 
                 const uint32_t m = d.mask & low;
                 const uint32_t src = (d.src & kSrcTable) ? (d.src & ~kSrcTable) : table_pad + d.src;
                 const uint32_t stride = (op.sum && ((d.mask >> w) & 1u)) ? 1u << (__builtin_popcount(d.mask) - 1) : 0u;
-                uint32_t* r = row + (size_t)(t + 1) * total + op.elem_begin;
+                uint32_t* r = row + (size_t)(t + 1) * total + first;
                 // j = hi << 8 | lo: the gather of the low byte from a table
                 const uint32_t m_lo = m & 0xffu, shift = (uint32_t)__builtin_popcount(m_lo);
                 const uint32_t n_lo = std::min(low, 255u) + 1u;
@@ -1965,7 +1989,7 @@ static void fill_records(const Network& n, uint32_t table_pad, uint32_t format, 
                     }
                 }
             }
-            uint32_t* r0 = row + op.elem_begin;
+            uint32_t* r0 = row + first;
             const uint32_t head = (uint32_t)op.k << 16 | (uint32_t)op.sum << 24;
             for (uint32_t j = 0; j <= low; ++j) r0[j] = (table_pad + op.dst + j) | head;
         }
