@@ -64,7 +64,7 @@ def cfg4():
 def er400():
     G = nx.erdos_renyi_graph(400, 3 / 399, seed=24323709)
     g, b = graphs.angles(3, seed=1)
-    eng = QAOAEnergyEngine(max_width=22, autotune=False)
+    eng = QAOAEnergyEngine(autotune=False)
     cg = eng.compile(G, 3, g, b)
     cg.params.copy_(torch.from_numpy(np.concatenate([g, b])))
     for _ in range(3):
