@@ -10,25 +10,27 @@
 // a large summed dimension it runs on the tcgen05 tensor cores:
 //   * a pre-pass splits every operand into TF32 "hi" (rounded to nearest,
 //     cvt.rna.tf32.f32) and "lo" (the rounded remainder) planes of the real
-//     and imaginary parts, transposed to K-major and tiled 128 rows x 32 k in
-//     the canonical no-swizzle core-matrix layout (8 rows x 16 bytes), zero
-//     padded to whole tiles;
-//   * one CTA per (f, 128 x 64 output tile) stages the eight planes of a k
-//     block (16 KB of A, 8 KB of B each) with bulk copies (cp.async.bulk,
-//     mbarrier transaction count, bounded wait) and one thread issues
-//     tcgen05.mma kind::tf32 (M=128, N=64, K=8) into two TMEM accumulators,
-//     Re and Im, in FP32:
+//     and imaginary parts, transposed to K-major and tiled 128 (or 64) rows
+//     x 16 k in the canonical no-swizzle core-matrix layout (8 rows x 16
+//     bytes), zero padded to whole 32-k blocks;
+//   * one CTA per (f, 128 x 64 output tile): one lane stages the eight
+//     planes of each 16-k tile (8 KB of A, 4 KB of B each) into one of two
+//     shared-memory stages with bulk copies (cp.async.bulk, mbarrier
+//     transaction count, bounded wait), and issues tcgen05.mma kind::tf32
+//     (M=128, N=64, K=8) into Re and Im accumulators in TMEM, FP32, while
+//     the next tile's copy lands:
 //       Re += Ar_hi Br_hi + Ar_hi Br_lo + Ar_lo Br_hi - (Ai_hi Bi_hi + Ai_hi Bi_lo + Ai_lo Bi_hi)
 //       Im += Ar_hi Bi_hi + Ar_hi Bi_lo + Ar_lo Bi_hi + Ai_hi Br_hi + Ai_hi Br_lo + Ai_lo Br_hi
 //     (3xTF32: Ootomo and Yokota, "Recovering single precision accuracy from
 //     Tensor Cores while surpassing the FP32 theoretical peak performance",
 //     IJHPCA 2022; the lo x lo term is dropped), the negative terms through
 //     the instruction descriptor's negate-A bit;
-//   * after every 32-k block the accumulators are read back (tcgen05.ld) and
-//     added into FP32 registers with round-to-nearest, since the tensor
-//     cores' own accumulation rounds toward zero (Ootomo and Yokota keep the
-//     long sum outside the tensor cores for the same reason); the registers
-//     are written as complex64.
+//   * every 32-k block goes to one of two TMEM buffers from zero; four warps
+//     read a finished buffer back (tcgen05.ld) and add it into FP32
+//     registers with round-to-nearest while the next block fills the other
+//     buffer, since the tensor cores' own accumulation rounds toward zero
+//     (Ootomo and Yokota keep the long sum outside the tensor cores for the
+//     same reason); the registers are written as complex64.
 // With a small summed dimension (the reference's own buckets sum one binary
 // index, K = 2) a tile would be mostly padding, and a CUDA-core kernel
 // computes the same sums in FP32.
@@ -79,19 +81,24 @@ __global__ void qtb_contract_simt_kernel(const float2* __restrict__ A, const flo
 // ----------------------------------------------------------------- tensor cores
 constexpr uint32_t kTcM = 128;                        // output tile rows (A tile rows)
 constexpr uint32_t kTcN = 64;                         // output tile columns (B tile rows)
-constexpr uint32_t kTcK = 32;                         // k per staged block
-constexpr uint32_t kTcAWords = kTcM * kTcK;           // 4096 x 32-bit = 16 KB per A plane
-constexpr uint32_t kTcBWords = kTcN * kTcK;           // 2048 x 32-bit =  8 KB per B plane
+constexpr uint32_t kTcK = 32;                         // k per accumulation block (K padded to it)
+constexpr uint32_t kTcStageK = 16;                    // k per staged tile (two stages per block)
+constexpr uint32_t kTcStages = 2;                     // shared-memory stages in flight
+constexpr uint32_t kTcAWords = kTcM * kTcStageK;      // 2048 x 32-bit = 8 KB per A plane and stage
+constexpr uint32_t kTcBWords = kTcN * kTcStageK;      // 1024 x 32-bit = 4 KB per B plane and stage
 constexpr uint32_t kTcPlanes = 4;                     // re_hi, re_lo, im_hi, im_lo
-constexpr uint32_t kTcThreads = 128;
-constexpr uint32_t kTcTmemCols = 128;                 // Re in columns 0..63, Im in 64..127
+constexpr uint32_t kTcStageWords = kTcPlanes * (kTcAWords + kTcBWords);   // 48 KB per stage
+constexpr uint32_t kTcEpilogueWarps = 4;              // one per 32 TMEM lanes of the 128-row tile
+constexpr uint32_t kTcThreads = 32 * (kTcEpilogueWarps + 1);   // + the copy/MMA issuing warp
+constexpr uint32_t kTcBufCols = 2 * kTcN;             // one accumulator buffer: Re 0..63, Im 64..127
+constexpr uint32_t kTcTmemCols = 2 * kTcBufCols;      // two buffers
 constexpr uint32_t kTcSpinLimit = 1u << 24;           // bounded mbarrier waits (~1 s)
 constexpr int kTcStatusTimeout = 2;
 
-// Word of element (r, k) inside a tile of 32 k: core matrix (row group
-// r / 8, k chunk k / 4) at (g * 8 + c) * 32 words, 8 rows of 16 bytes each.
+// Word of element (r, k) inside a tile of 16 k: core matrix (row group
+// r / 8, k chunk k / 4) at (g * 4 + c) * 32 words, 8 rows of 16 bytes each.
 __device__ __forceinline__ uint32_t tc_tile_word(uint32_t r, uint32_t k) {
-    return (((r >> 3) * 8u + (k >> 2)) << 5) + ((r & 7u) << 2) + (k & 3u);
+    return (((r >> 3) * 4u + (k >> 2)) << 5) + ((r & 7u) << 2) + (k & 3u);
 }
 
 __device__ __forceinline__ uint32_t tf32_round(float x) {
@@ -101,13 +108,13 @@ __device__ __forceinline__ uint32_t tf32_round(float x) {
 }
 
 // src[k][f][r] (complex64, R rows) -> for every f, planes q = 0..3 of
-// Rp x Kp TF32 words in tiles of `tile_rows` x 32 k, row-tile-major.
+// Rp x Kp TF32 words in tiles of `tile_rows` x 16 k, row-tile-major.
 __global__ void qtb_tc_split_kernel(const float2* __restrict__ src, uint32_t* __restrict__ dst, uint32_t K,
                                     uint32_t F, uint32_t R, uint32_t Rp, uint32_t Kp, uint32_t tile_rows) {
     const uint64_t plane = (uint64_t)Rp * Kp;
     const uint64_t total = (uint64_t)F * plane;
-    const uint32_t k_tiles = Kp / kTcK;
-    const uint32_t tile_words = tile_rows * kTcK;
+    const uint32_t k_tiles = Kp / kTcStageK;
+    const uint32_t tile_words = tile_rows * kTcStageK;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
          i += (uint64_t)gridDim.x * blockDim.x) {
         // rows fastest, so the source reads are coalesced
@@ -120,8 +127,8 @@ __global__ void qtb_tc_split_kernel(const float2* __restrict__ src, uint32_t* __
         const uint32_t re_lo = tf32_round(v.x - __uint_as_float(re_hi));
         const uint32_t im_lo = tf32_round(v.y - __uint_as_float(im_hi));
         const uint64_t base = (uint64_t)f * kTcPlanes * plane +
-                              ((uint64_t)(r / tile_rows) * k_tiles + k / kTcK) * tile_words +
-                              tc_tile_word(r % tile_rows, k % kTcK);
+                              ((uint64_t)(r / tile_rows) * k_tiles + k / kTcStageK) * tile_words +
+                              tc_tile_word(r % tile_rows, k % kTcStageK);
         dst[base] = re_hi;
         dst[base + plane] = re_lo;
         dst[base + 2 * plane] = im_hi;
@@ -135,10 +142,10 @@ __device__ __forceinline__ uint32_t tc_smem(const void* p) {
 
 // Shared-memory matrix descriptor of a K-major, no-swizzle operand tile:
 // start address, leading byte offset (next 16-byte k chunk: 128 B), stride
-// byte offset (next 8-row group: 8 chunks x 128 B), descriptor version 1.
+// byte offset (next 8-row group: 4 chunks x 128 B), descriptor version 1.
 __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
     return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) |
-           ((uint64_t)(1024u >> 4) << 32) | (uint64_t(1) << 46);
+           ((uint64_t)(512u >> 4) << 32) | (uint64_t(1) << 46);
 }
 
 // Instruction descriptor: FP32 accumulator, TF32 A and B, both K-major,
@@ -178,27 +185,49 @@ __device__ __forceinline__ void tc_ld8(uint32_t taddr, float* out) {
     for (int j = 0; j < 8; ++j) out[j] = __uint_as_float(r[j]);
 }
 
-// One CTA per (f, 128 x 64 tile of C).  Ap / Bp: the pre-pass planes.
-// Every 32-k block is accumulated in TMEM from zero and then added, with
-// round-to-nearest, into FP32 registers (one row of the tile per thread):
-// the tensor cores' accumulation rounds toward zero, and summing a long k
-// range in TMEM alone biases the result (about 3e-5 relative at K = 1000).
-__global__ void __launch_bounds__(kTcThreads, 1)
+__device__ __forceinline__ void tc_bulk(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+// One CTA per (f, 128 x 64 tile of C), five warps.  Ap / Bp: the pre-pass
+// planes, in tiles of 16 k.
+//   * Warp 4 (one elected lane) stages tiles with bulk copies into two
+//     shared-memory stages and issues the MMAs: the copy of stage i + 1
+//     runs while stage i's MMAs execute.  Two stages make one 32-k block,
+//     accumulated in one of two TMEM buffers from zero.
+//   * Warps 0-3 (one per 32 TMEM lanes) read a finished block's buffer
+//     with tcgen05.ld and add it into FP32 registers with round-to-nearest
+//     (the tensor cores' own accumulation rounds toward zero, which over a
+//     long k range biases the sum: about 3e-5 relative at K = 1000), while
+//     the next block's MMAs fill the other buffer.
+// mbarriers: full[s] (stage s landed), empty[s] (stage s's MMAs done),
+// tfull[b] (buffer b's block done), tempty[b] (buffer b read, 128
+// arrivals).  Every wait is bounded; on a timeout the status word is set,
+// every role stops, and the CTA waits (bounded) for its copies and MMAs
+// in flight before freeing TMEM.
+__global__ void __launch_bounds__(kTcThreads, 2)
 qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restrict__ Bp, float2* __restrict__ C,
                        uint32_t F, uint32_t M, uint32_t N, uint32_t Mp, uint32_t Np, uint32_t Kp, int* status) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    // [A planes x4 (16 KB each)][B planes x4 (8 KB each)], two mbarriers, the TMEM slot
-    uint32_t* a_tiles = reinterpret_cast<uint32_t*>(smem);
-    uint32_t* b_tiles = a_tiles + kTcPlanes * kTcAWords;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(b_tiles + kTcPlanes * kTcBWords);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
-    __shared__ int s_ok;
+    // [stage 0: A planes x4 | B planes x4][stage 1: ...], eight mbarriers, the TMEM slot
+    uint32_t* stages = reinterpret_cast<uint32_t*>(smem);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(stages + kTcStages * kTcStageWords);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 8);
+    __shared__ volatile int s_ok;
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t nt = blockIdx.x, mt = blockIdx.y, f = blockIdx.z;
-    const uint32_t load_bar = tc_smem(&bars[0]), mma_bar = tc_smem(&bars[1]);
+    auto bar = [&](uint32_t i) { return tc_smem(&bars[i]); };   // 0-1 full, 2-3 empty, 4-5 tfull, 6-7 tempty
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(load_bar));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mma_bar));
+        for (uint32_t i = 0; i < 6; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar(i)));
+        for (uint32_t i = 6; i < 8; ++i)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar(i)), "r"(32 * kTcEpilogueWarps));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_ok = 1;
     }
@@ -211,93 +240,127 @@ qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restri
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = *tmem_slot;
-    const uint32_t lane_addr = tmem + ((warp * 32u) << 16);   // this warp's 32 TMEM lanes
-    float acc_re[kTcN], acc_im[kTcN];
-#pragma unroll
-    for (uint32_t j = 0; j < kTcN; ++j) acc_re[j] = acc_im[j] = 0.f;
     const uint64_t a_plane = (uint64_t)Mp * Kp, b_plane = (uint64_t)Np * Kp;
-    const uint32_t k_tiles = Kp / kTcK;
-    const uint32_t* a_f = Ap + (uint64_t)f * kTcPlanes * a_plane + (uint64_t)mt * k_tiles * kTcAWords;
-    const uint32_t* b_f = Bp + (uint64_t)f * kTcPlanes * b_plane + (uint64_t)nt * k_tiles * kTcBWords;
-    for (uint32_t kt = 0; kt < k_tiles; ++kt) {
-        if (threadIdx.x == 0) {
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(load_bar),
-                         "r"(kTcPlanes * (kTcAWords + kTcBWords) * 4u)
-                         : "memory");
-            for (uint32_t q = 0; q < kTcPlanes; ++q) {
-                asm volatile(
-                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                        tc_smem(a_tiles + q * kTcAWords)),
-                    "l"(a_f + q * a_plane + (uint64_t)kt * kTcAWords), "r"(kTcAWords * 4u), "r"(load_bar)
-                    : "memory");
-                asm volatile(
-                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                        tc_smem(b_tiles + q * kTcBWords)),
-                    "l"(b_f + q * b_plane + (uint64_t)kt * kTcBWords), "r"(kTcBWords * 4u), "r"(load_bar)
-                    : "memory");
+    const uint32_t n_stages = Kp / kTcStageK, n_blocks = Kp / kTcK;
+    auto fail_once = [&]() {
+        if (s_ok) atomicOr(status, kTcStatusTimeout);
+        s_ok = 0;
+    };
+    if (warp == kTcEpilogueWarps) {
+        if (lane == 0) {
+            const uint32_t* a_f = Ap + (uint64_t)f * kTcPlanes * a_plane + (uint64_t)mt * n_stages * kTcAWords;
+            const uint32_t* b_f = Bp + (uint64_t)f * kTcPlanes * b_plane + (uint64_t)nt * n_stages * kTcBWords;
+            auto stage_a = [&](uint32_t s) { return tc_smem(stages + s * kTcStageWords); };
+            auto stage_b = [&](uint32_t s) { return tc_smem(stages + s * kTcStageWords + kTcPlanes * kTcAWords); };
+            auto load = [&](uint32_t i) {   // stage tile i (16 k) into stage i % 2
+                const uint32_t s = i & 1u;
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar(s)),
+                             "r"(kTcStageWords * 4u)
+                             : "memory");
+                for (uint32_t q = 0; q < kTcPlanes; ++q) {
+                    tc_bulk(stage_a(s) + q * kTcAWords * 4u, a_f + q * a_plane + (uint64_t)i * kTcAWords,
+                            kTcAWords * 4u, bar(s));
+                    tc_bulk(stage_b(s) + q * kTcBWords * 4u, b_f + q * b_plane + (uint64_t)i * kTcBWords,
+                            kTcBWords * 4u, bar(s));
+                }
+            };
+            uint32_t loaded = 0, landed = 0;   // tiles whose copies were issued, waited for
+            uint32_t committed[2] = {0, 0}, retired[2] = {0, 0};   // empty[s] phases issued, waited for
+            load(0);
+            loaded = 1;
+            for (uint32_t i = 0; i < n_stages && s_ok; ++i) {
+                const uint32_t s = i & 1u, b = i >> 1, buf = b & 1u;
+                if ((i & 1u) == 0 && b >= 2 && !tc_wait(bar(6 + buf), ((b - 2) >> 1) & 1u)) {
+                    fail_once();   // the epilogue has not read this buffer's previous block
+                    break;
+                }
+                if (!tc_wait(bar(s), (i >> 1) & 1u)) {
+                    fail_once();
+                    break;
+                }
+                landed = i + 1;
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                // planes: A 0 Ar_hi 1 Ar_lo 2 Ai_hi 3 Ai_lo | B 0 Br_hi 1 Br_lo 2 Bi_hi 3 Bi_lo
+                const uint32_t abase = stage_a(s), bbase = stage_b(s);
+                const uint32_t re = tmem + buf * kTcBufCols, im = re + kTcN;
+                for (uint32_t ks = 0; ks < kTcStageK / 8; ++ks) {
+                    auto da = [&](uint32_t q) { return tc_desc(abase + q * kTcAWords * 4u + ks * 256u); };
+                    auto db = [&](uint32_t q) { return tc_desc(bbase + q * kTcBWords * 4u + ks * 256u); };
+                    const uint32_t first = ((i & 1u) == 0 && ks == 0) ? 0u : 1u;   // a block starts from zero
+                    tc_mma(re, da(0), db(0), kTcIdesc, first);
+                    tc_mma(re, da(0), db(1), kTcIdesc, 1u);
+                    tc_mma(re, da(1), db(0), kTcIdesc, 1u);
+                    tc_mma(re, da(2), db(2), kTcIdescNegA, 1u);
+                    tc_mma(re, da(2), db(3), kTcIdescNegA, 1u);
+                    tc_mma(re, da(3), db(2), kTcIdescNegA, 1u);
+                    tc_mma(im, da(0), db(2), kTcIdesc, first);
+                    tc_mma(im, da(0), db(3), kTcIdesc, 1u);
+                    tc_mma(im, da(1), db(2), kTcIdesc, 1u);
+                    tc_mma(im, da(2), db(0), kTcIdesc, 1u);
+                    tc_mma(im, da(2), db(1), kTcIdesc, 1u);
+                    tc_mma(im, da(3), db(0), kTcIdesc, 1u);
+                }
+                tc_commit(bar(2 + s));
+                ++committed[s];
+                if (i & 1u) tc_commit(bar(4 + buf));
+                // stage i + 1 goes into the other stage once its previous
+                // tile's MMAs (stage i - 1) are done; it lands while stage
+                // i's MMAs run
+                if (i + 1 < n_stages) {
+                    if (i >= 1) {
+                        if (!tc_wait(bar(2 + (s ^ 1u)), ((i - 1) >> 1) & 1u)) {
+                            fail_once();
+                            break;
+                        }
+                        ++retired[s ^ 1u];
+                    }
+                    load(i + 1);
+                    loaded = i + 2;
+                }
             }
+            // nothing of this CTA may still write shared memory or TMEM when
+            // it frees them: wait (bounded, in phase order) for the copies
+            // issued and not waited for, and for every MMA commit
+            for (uint32_t i = landed; i < loaded; ++i) tc_wait(bar(i & 1u), (i >> 1) & 1u);
+            for (uint32_t q = 0; q < 2; ++q)
+                for (uint32_t u = retired[q]; u < committed[q]; ++u) tc_wait(bar(2 + q), u & 1u);
         }
-        if (!tc_wait(load_bar, kt & 1u) && threadIdx.x == 0) {
-            atomicOr(status, kTcStatusTimeout);
-            s_ok = 0;
-        }
-        __syncthreads();
-        if (!s_ok) break;
-        if (threadIdx.x == 0) {
+        __syncwarp();
+    } else {
+        float acc_re[kTcN], acc_im[kTcN];
+#pragma unroll
+        for (uint32_t j = 0; j < kTcN; ++j) acc_re[j] = acc_im[j] = 0.f;
+        const uint32_t lane_addr = tmem + ((warp * 32u) << 16);   // this warp's 32 TMEM lanes
+        for (uint32_t b = 0; b < n_blocks; ++b) {
+            const uint32_t buf = b & 1u;
+            if (!s_ok) break;
+            if (!tc_wait(bar(4 + buf), (b >> 1) & 1u)) {
+                fail_once();
+                break;
+            }
             asm volatile("tcgen05.fence::after_thread_sync;");
-            // planes: A 0 Ar_hi 1 Ar_lo 2 Ai_hi 3 Ai_lo | B 0 Br_hi 1 Br_lo 2 Bi_hi 3 Bi_lo
-            const uint32_t abase = tc_smem(a_tiles), bbase = tc_smem(b_tiles);
-            const uint32_t re = tmem, im = tmem + kTcN;
-            for (uint32_t s = 0; s < kTcK / 8; ++s) {
-                auto da = [&](uint32_t q) { return tc_desc(abase + q * kTcAWords * 4u + s * 256u); };
-                auto db = [&](uint32_t q) { return tc_desc(bbase + q * kTcBWords * 4u + s * 256u); };
-                const uint32_t first = s == 0 ? 0u : 1u;   // every block starts from zero
-                tc_mma(re, da(0), db(0), kTcIdesc, first);
-                tc_mma(re, da(0), db(1), kTcIdesc, 1u);
-                tc_mma(re, da(1), db(0), kTcIdesc, 1u);
-                tc_mma(re, da(2), db(2), kTcIdescNegA, 1u);
-                tc_mma(re, da(2), db(3), kTcIdescNegA, 1u);
-                tc_mma(re, da(3), db(2), kTcIdescNegA, 1u);
-                tc_mma(im, da(0), db(2), kTcIdesc, first);
-                tc_mma(im, da(0), db(3), kTcIdesc, 1u);
-                tc_mma(im, da(1), db(2), kTcIdesc, 1u);
-                tc_mma(im, da(2), db(0), kTcIdesc, 1u);
-                tc_mma(im, da(2), db(1), kTcIdesc, 1u);
-                tc_mma(im, da(3), db(0), kTcIdesc, 1u);
+#pragma unroll
+            for (uint32_t c0 = 0; c0 < kTcN; c0 += 8u) {
+                float v[8];
+                tc_ld8(lane_addr + buf * kTcBufCols + c0, v);
+#pragma unroll
+                for (uint32_t j = 0; j < 8; ++j) acc_re[c0 + j] += v[j];
+                tc_ld8(lane_addr + buf * kTcBufCols + kTcN + c0, v);
+#pragma unroll
+                for (uint32_t j = 0; j < 8; ++j) acc_im[c0 + j] += v[j];
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mma_bar)
-                         : "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar(6 + buf)) : "memory");
         }
-        // the block's MMAs are done (tiles free, TMEM written)
-        if (!tc_wait(mma_bar, kt & 1u) && threadIdx.x == 0) {
-            atomicOr(status, kTcStatusTimeout);
-            s_ok = 0;
-        }
-        __syncthreads();
-        if (!s_ok) break;
-        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (s_ok) {
+            const uint32_t m = mt * kTcM + warp * 32u + lane;
+            if (m < M) {
+                float2* crow = C + ((uint64_t)f * M + m) * N;
 #pragma unroll
-        for (uint32_t c0 = 0; c0 < kTcN; c0 += 8u) {
-            float v[8];
-            tc_ld8(lane_addr + c0, v);
-#pragma unroll
-            for (uint32_t j = 0; j < 8; ++j) acc_re[c0 + j] += v[j];
-            tc_ld8(lane_addr + kTcN + c0, v);
-#pragma unroll
-            for (uint32_t j = 0; j < 8; ++j) acc_im[c0 + j] += v[j];
-        }
-        // every lane has read the block before the next block's MMAs overwrite it
-        asm volatile("tcgen05.fence::before_thread_sync;");
-        __syncthreads();
-    }
-    if (s_ok) {
-        const uint32_t m = mt * kTcM + warp * 32u + lane;
-        if (m < M) {
-            float2* crow = C + ((uint64_t)f * M + m) * N;
-#pragma unroll
-            for (uint32_t j = 0; j < kTcN; ++j) {
-                const uint32_t n = nt * kTcN + j;
-                if (n < N) crow[n] = make_float2(acc_re[j], acc_im[j]);
+                for (uint32_t j = 0; j < kTcN; ++j) {
+                    const uint32_t n = nt * kTcN + j;
+                    if (n < N) crow[n] = make_float2(acc_re[j], acc_im[j]);
+                }
             }
         }
     }
@@ -306,7 +369,7 @@ qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restri
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols));
 }
 
-constexpr size_t kTcSmemBytes = kTcPlanes * (kTcAWords + kTcBWords) * 4 + 64;
+constexpr size_t kTcSmemBytes = kTcStages * kTcStageWords * 4 + 8 * 8 + 16;
 
 static uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
 
