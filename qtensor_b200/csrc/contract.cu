@@ -82,12 +82,14 @@ __global__ void qtb_contract_simt_kernel(const float2* __restrict__ A, const flo
 constexpr uint32_t kTcM = 128;                        // output tile rows (A tile rows)
 constexpr uint32_t kTcN = 64;                         // output tile columns (B tile rows)
 constexpr uint32_t kTcK = 32;                         // k per accumulation block (K padded to it)
-constexpr uint32_t kTcStageK = 16;                    // k per staged tile (two stages per block)
-constexpr uint32_t kTcStages = 2;                     // shared-memory stages in flight
-constexpr uint32_t kTcAWords = kTcM * kTcStageK;      // 2048 x 32-bit = 8 KB per A plane and stage
-constexpr uint32_t kTcBWords = kTcN * kTcStageK;      // 1024 x 32-bit = 4 KB per B plane and stage
+constexpr uint32_t kTcStageK = 8;                     // k per staged tile (one MMA k step)
+constexpr uint32_t kTcStages = 4;                     // shared-memory stages (three copies in flight)
+constexpr uint32_t kTcStagesPerBlock = kTcK / kTcStageK;
+constexpr uint32_t kTcAWords = kTcM * kTcStageK;      // 1024 x 32-bit = 4 KB per A plane and stage
+constexpr uint32_t kTcBWords = kTcN * kTcStageK;      //  512 x 32-bit = 2 KB per B plane and stage
 constexpr uint32_t kTcPlanes = 4;                     // re_hi, re_lo, im_hi, im_lo
-constexpr uint32_t kTcStageWords = kTcPlanes * (kTcAWords + kTcBWords);   // 48 KB per stage
+constexpr uint32_t kTcStageWords = kTcPlanes * (kTcAWords + kTcBWords);   // 24 KB per stage
+constexpr uint32_t kTcChunks = kTcStageK / 4;         // 16-byte k chunks per row of a tile
 constexpr uint32_t kTcEpilogueWarps = 4;              // one per 32 TMEM lanes of the 128-row tile
 constexpr uint32_t kTcThreads = 32 * (kTcEpilogueWarps + 1);   // + the copy/MMA issuing warp
 constexpr uint32_t kTcBufCols = 2 * kTcN;             // one accumulator buffer: Re 0..63, Im 64..127
@@ -95,10 +97,11 @@ constexpr uint32_t kTcTmemCols = 2 * kTcBufCols;      // two buffers
 constexpr uint32_t kTcSpinLimit = 1u << 24;           // bounded mbarrier waits (~1 s)
 constexpr int kTcStatusTimeout = 2;
 
-// Word of element (r, k) inside a tile of 16 k: core matrix (row group
-// r / 8, k chunk k / 4) at (g * 4 + c) * 32 words, 8 rows of 16 bytes each.
+// Word of element (r, k) inside a tile of kTcStageK k: core matrix (row
+// group r / 8, k chunk k / 4) at (g * kTcChunks + c) * 32 words, 8 rows of
+// 16 bytes each.
 __device__ __forceinline__ uint32_t tc_tile_word(uint32_t r, uint32_t k) {
-    return (((r >> 3) * 4u + (k >> 2)) << 5) + ((r & 7u) << 2) + (k & 3u);
+    return (((r >> 3) * kTcChunks + (k >> 2)) << 5) + ((r & 7u) << 2) + (k & 3u);
 }
 
 __device__ __forceinline__ uint32_t tf32_round(float x) {
@@ -108,7 +111,7 @@ __device__ __forceinline__ uint32_t tf32_round(float x) {
 }
 
 // src[k][f][r] (complex64, R rows) -> for every f, planes q = 0..3 of
-// Rp x Kp TF32 words in tiles of `tile_rows` x 16 k, row-tile-major.
+// Rp x Kp TF32 words in tiles of `tile_rows` x kTcStageK k, row-tile-major.
 __global__ void qtb_tc_split_kernel(const float2* __restrict__ src, uint32_t* __restrict__ dst, uint32_t K,
                                     uint32_t F, uint32_t R, uint32_t Rp, uint32_t Kp, uint32_t tile_rows) {
     const uint64_t plane = (uint64_t)Rp * Kp;
@@ -142,10 +145,10 @@ __device__ __forceinline__ uint32_t tc_smem(const void* p) {
 
 // Shared-memory matrix descriptor of a K-major, no-swizzle operand tile:
 // start address, leading byte offset (next 16-byte k chunk: 128 B), stride
-// byte offset (next 8-row group: 4 chunks x 128 B), descriptor version 1.
+// byte offset (next 8-row group: kTcChunks chunks x 128 B), version 1.
 __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
     return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) |
-           ((uint64_t)(512u >> 4) << 32) | (uint64_t(1) << 46);
+           ((uint64_t)(kTcChunks * 128u >> 4) << 32) | (uint64_t(1) << 46);
 }
 
 // Instruction descriptor: FP32 accumulator, TF32 A and B, both K-major,
@@ -197,11 +200,12 @@ __device__ __forceinline__ void tc_commit(uint32_t bar) {
 }
 
 // One CTA per (f, 128 x 64 tile of C), five warps.  Ap / Bp: the pre-pass
-// planes, in tiles of 16 k.
-//   * Warp 4 (one elected lane) stages tiles with bulk copies into two
-//     shared-memory stages and issues the MMAs: the copy of stage i + 1
-//     runs while stage i's MMAs execute.  Two stages make one 32-k block,
-//     accumulated in one of two TMEM buffers from zero.
+// planes, in tiles of kTcStageK k.
+//   * Warp 4 (one elected lane) stages tiles with bulk copies into
+//     kTcStages shared-memory stages, kTcStages - 1 tiles ahead of the
+//     MMAs it issues, so that copies land while earlier tiles' MMAs run.
+//     kTcStagesPerBlock tiles make one 32-k block, accumulated in one of two
+//     TMEM buffers from zero.
 //   * Warps 0-3 (one per 32 TMEM lanes) read a finished block's buffer
 //     with tcgen05.ld and add it into FP32 registers with round-to-nearest
 //     (the tensor cores' own accumulation rounds toward zero, which over a
@@ -210,24 +214,29 @@ __device__ __forceinline__ void tc_commit(uint32_t bar) {
 // mbarriers: full[s] (stage s landed), empty[s] (stage s's MMAs done),
 // tfull[b] (buffer b's block done), tempty[b] (buffer b read, 128
 // arrivals).  Every wait is bounded; on a timeout the status word is set,
-// every role stops, and the CTA waits (bounded) for its copies and MMAs
-// in flight before freeing TMEM.
+// every role stops, and the CTA waits (bounded, in phase order) for its
+// copies and MMAs in flight before freeing TMEM.
 __global__ void __launch_bounds__(kTcThreads, 2)
 qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restrict__ Bp, float2* __restrict__ C,
                        uint32_t F, uint32_t M, uint32_t N, uint32_t Mp, uint32_t Np, uint32_t Kp, int* status) {
+    constexpr uint32_t NS = kTcStages;
     extern __shared__ __align__(1024) unsigned char smem[];
-    // [stage 0: A planes x4 | B planes x4][stage 1: ...], eight mbarriers, the TMEM slot
+    // [stage 0: A planes x4 | B planes x4][stage 1] ..., the mbarriers, the TMEM slot
     uint32_t* stages = reinterpret_cast<uint32_t*>(smem);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(stages + kTcStages * kTcStageWords);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 8);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(stages + NS * kTcStageWords);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * NS + 4);
     __shared__ volatile int s_ok;
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t nt = blockIdx.x, mt = blockIdx.y, f = blockIdx.z;
-    auto bar = [&](uint32_t i) { return tc_smem(&bars[i]); };   // 0-1 full, 2-3 empty, 4-5 tfull, 6-7 tempty
+    auto full = [&](uint32_t s) { return tc_smem(&bars[s]); };
+    auto empty = [&](uint32_t s) { return tc_smem(&bars[NS + s]); };
+    auto tfull = [&](uint32_t b) { return tc_smem(&bars[2 * NS + b]); };
+    auto tempty = [&](uint32_t b) { return tc_smem(&bars[2 * NS + 2 + b]); };
     if (threadIdx.x == 0) {
-        for (uint32_t i = 0; i < 6; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar(i)));
-        for (uint32_t i = 6; i < 8; ++i)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar(i)), "r"(32 * kTcEpilogueWarps));
+        for (uint32_t i = 0; i < 2 * NS + 2; ++i)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&bars[i])));
+        for (uint32_t b = 0; b < 2; ++b)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tempty(b)), "r"(32 * kTcEpilogueWarps));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_ok = 1;
     }
@@ -241,40 +250,40 @@ qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restri
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = *tmem_slot;
     const uint64_t a_plane = (uint64_t)Mp * Kp, b_plane = (uint64_t)Np * Kp;
-    const uint32_t n_stages = Kp / kTcStageK, n_blocks = Kp / kTcK;
+    const uint32_t n_tiles = Kp / kTcStageK, n_blocks = Kp / kTcK;
     auto fail_once = [&]() {
         if (s_ok) atomicOr(status, kTcStatusTimeout);
         s_ok = 0;
     };
     if (warp == kTcEpilogueWarps) {
         if (lane == 0) {
-            const uint32_t* a_f = Ap + (uint64_t)f * kTcPlanes * a_plane + (uint64_t)mt * n_stages * kTcAWords;
-            const uint32_t* b_f = Bp + (uint64_t)f * kTcPlanes * b_plane + (uint64_t)nt * n_stages * kTcBWords;
+            const uint32_t* a_f = Ap + (uint64_t)f * kTcPlanes * a_plane + (uint64_t)mt * n_tiles * kTcAWords;
+            const uint32_t* b_f = Bp + (uint64_t)f * kTcPlanes * b_plane + (uint64_t)nt * n_tiles * kTcBWords;
             auto stage_a = [&](uint32_t s) { return tc_smem(stages + s * kTcStageWords); };
             auto stage_b = [&](uint32_t s) { return tc_smem(stages + s * kTcStageWords + kTcPlanes * kTcAWords); };
-            auto load = [&](uint32_t i) {   // stage tile i (16 k) into stage i % 2
-                const uint32_t s = i & 1u;
-                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar(s)),
+            auto load = [&](uint32_t i) {   // tile i into stage i % NS
+                const uint32_t s = i % NS;
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full(s)),
                              "r"(kTcStageWords * 4u)
                              : "memory");
                 for (uint32_t q = 0; q < kTcPlanes; ++q) {
                     tc_bulk(stage_a(s) + q * kTcAWords * 4u, a_f + q * a_plane + (uint64_t)i * kTcAWords,
-                            kTcAWords * 4u, bar(s));
+                            kTcAWords * 4u, full(s));
                     tc_bulk(stage_b(s) + q * kTcBWords * 4u, b_f + q * b_plane + (uint64_t)i * kTcBWords,
-                            kTcBWords * 4u, bar(s));
+                            kTcBWords * 4u, full(s));
                 }
             };
             uint32_t loaded = 0, landed = 0;   // tiles whose copies were issued, waited for
-            uint32_t committed[2] = {0, 0}, retired[2] = {0, 0};   // empty[s] phases issued, waited for
-            load(0);
-            loaded = 1;
-            for (uint32_t i = 0; i < n_stages && s_ok; ++i) {
-                const uint32_t s = i & 1u, b = i >> 1, buf = b & 1u;
-                if ((i & 1u) == 0 && b >= 2 && !tc_wait(bar(6 + buf), ((b - 2) >> 1) & 1u)) {
+            uint32_t committed[NS] = {}, retired[NS] = {};   // empty[s] phases issued, waited for
+            for (; loaded < NS - 1 && loaded < n_tiles; ++loaded) load(loaded);
+            for (uint32_t i = 0; i < n_tiles && s_ok; ++i) {
+                const uint32_t s = i % NS, b = i / kTcStagesPerBlock, buf = b & 1u;
+                const bool block_first = i % kTcStagesPerBlock == 0;
+                if (block_first && b >= 2 && !tc_wait(tempty(buf), ((b - 2) >> 1) & 1u)) {
                     fail_once();   // the epilogue has not read this buffer's previous block
                     break;
                 }
-                if (!tc_wait(bar(s), (i >> 1) & 1u)) {
+                if (!tc_wait(full(s), (i / NS) & 1u)) {
                     fail_once();
                     break;
                 }
@@ -283,10 +292,11 @@ qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restri
                 // planes: A 0 Ar_hi 1 Ar_lo 2 Ai_hi 3 Ai_lo | B 0 Br_hi 1 Br_lo 2 Bi_hi 3 Bi_lo
                 const uint32_t abase = stage_a(s), bbase = stage_b(s);
                 const uint32_t re = tmem + buf * kTcBufCols, im = re + kTcN;
+#pragma unroll
                 for (uint32_t ks = 0; ks < kTcStageK / 8; ++ks) {
                     auto da = [&](uint32_t q) { return tc_desc(abase + q * kTcAWords * 4u + ks * 256u); };
                     auto db = [&](uint32_t q) { return tc_desc(bbase + q * kTcBWords * 4u + ks * 256u); };
-                    const uint32_t first = ((i & 1u) == 0 && ks == 0) ? 0u : 1u;   // a block starts from zero
+                    const uint32_t first = (block_first && ks == 0) ? 0u : 1u;   // a block starts from zero
                     tc_mma(re, da(0), db(0), kTcIdesc, first);
                     tc_mma(re, da(0), db(1), kTcIdesc, 1u);
                     tc_mma(re, da(1), db(0), kTcIdesc, 1u);
@@ -300,30 +310,29 @@ qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restri
                     tc_mma(im, da(2), db(1), kTcIdesc, 1u);
                     tc_mma(im, da(3), db(0), kTcIdesc, 1u);
                 }
-                tc_commit(bar(2 + s));
+                tc_commit(empty(s));
                 ++committed[s];
-                if (i & 1u) tc_commit(bar(4 + buf));
-                // stage i + 1 goes into the other stage once its previous
-                // tile's MMAs (stage i - 1) are done; it lands while stage
-                // i's MMAs run
-                if (i + 1 < n_stages) {
+                if (i % kTcStagesPerBlock == kTcStagesPerBlock - 1) tc_commit(tfull(buf));
+                // tile i + NS - 1 goes into the stage of tile i - 1 once that
+                // tile's MMAs are done; it lands while later tiles' MMAs run
+                if (loaded < n_tiles) {
                     if (i >= 1) {
-                        if (!tc_wait(bar(2 + (s ^ 1u)), ((i - 1) >> 1) & 1u)) {
+                        const uint32_t sp = (i - 1) % NS;
+                        if (!tc_wait(empty(sp), ((i - 1) / NS) & 1u)) {
                             fail_once();
                             break;
                         }
-                        ++retired[s ^ 1u];
+                        ++retired[sp];
                     }
-                    load(i + 1);
-                    loaded = i + 2;
+                    load(loaded++);
                 }
             }
             // nothing of this CTA may still write shared memory or TMEM when
             // it frees them: wait (bounded, in phase order) for the copies
             // issued and not waited for, and for every MMA commit
-            for (uint32_t i = landed; i < loaded; ++i) tc_wait(bar(i & 1u), (i >> 1) & 1u);
-            for (uint32_t q = 0; q < 2; ++q)
-                for (uint32_t u = retired[q]; u < committed[q]; ++u) tc_wait(bar(2 + q), u & 1u);
+            for (uint32_t i = landed; i < loaded; ++i) tc_wait(full(i % NS), (i / NS) & 1u);
+            for (uint32_t q = 0; q < NS; ++q)
+                for (uint32_t u = retired[q]; u < committed[q]; ++u) tc_wait(empty(q), u & 1u);
         }
         __syncwarp();
     } else {
@@ -334,7 +343,7 @@ qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restri
         for (uint32_t b = 0; b < n_blocks; ++b) {
             const uint32_t buf = b & 1u;
             if (!s_ok) break;
-            if (!tc_wait(bar(4 + buf), (b >> 1) & 1u)) {
+            if (!tc_wait(tfull(buf), (b >> 1) & 1u)) {
                 fail_once();
                 break;
             }
@@ -350,7 +359,7 @@ qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restri
                 for (uint32_t j = 0; j < 8; ++j) acc_im[c0 + j] += v[j];
             }
             asm volatile("tcgen05.fence::before_thread_sync;");
-            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar(6 + buf)) : "memory");
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tempty(buf)) : "memory");
         }
         if (s_ok) {
             const uint32_t m = mt * kTcM + warp * 32u + lane;
@@ -369,7 +378,7 @@ qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restri
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols));
 }
 
-constexpr size_t kTcSmemBytes = kTcStages * kTcStageWords * 4 + 8 * 8 + 16;
+constexpr size_t kTcSmemBytes = kTcStages * kTcStageWords * 4 + (2 * kTcStages + 4) * 8 + 16;
 
 static uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
 
