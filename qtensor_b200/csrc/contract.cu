@@ -80,15 +80,16 @@ __global__ void qtb_contract_simt_kernel(const float2* __restrict__ A, const flo
 
 // ----------------------------------------------------------------- tensor cores
 constexpr uint32_t kTcM = 128;                        // output tile rows (A tile rows)
-constexpr uint32_t kTcN = 64;                         // output tile columns (B tile rows)
+constexpr uint32_t kTcN = 64;                         // output tile columns (complex)
+constexpr uint32_t kTcBRows = 2 * kTcN;               // B tile rows: [Br | Bi] or [-Bi | Br]
 constexpr uint32_t kTcK = 32;                         // k per accumulation block (K padded to it)
 constexpr uint32_t kTcStageK = 8;                     // k per staged tile (one MMA k step)
-constexpr uint32_t kTcStages = 4;                     // shared-memory stages (three copies in flight)
+constexpr uint32_t kTcStages = 3;                     // shared-memory stages (two copies in flight)
 constexpr uint32_t kTcStagesPerBlock = kTcK / kTcStageK;
 constexpr uint32_t kTcAWords = kTcM * kTcStageK;      // 1024 x 32-bit = 4 KB per A plane and stage
-constexpr uint32_t kTcBWords = kTcN * kTcStageK;      //  512 x 32-bit = 2 KB per B plane and stage
-constexpr uint32_t kTcPlanes = 4;                     // re_hi, re_lo, im_hi, im_lo
-constexpr uint32_t kTcStageWords = kTcPlanes * (kTcAWords + kTcBWords);   // 24 KB per stage
+constexpr uint32_t kTcBWords = kTcBRows * kTcStageK;  // 1024 x 32-bit = 4 KB per B plane and stage
+constexpr uint32_t kTcPlanes = 4;                     // A: re_hi re_lo im_hi im_lo; B: B1_hi B1_lo B2_hi B2_lo
+constexpr uint32_t kTcStageWords = kTcPlanes * (kTcAWords + kTcBWords);   // 32 KB per stage
 constexpr uint32_t kTcChunks = kTcStageK / 4;         // 16-byte k chunks per row of a tile
 constexpr uint32_t kTcEpilogueWarps = 4;              // one per 32 TMEM lanes of the 128-row tile
 constexpr uint32_t kTcThreads = 32 * (kTcEpilogueWarps + 1);   // + the copy/MMA issuing warp
@@ -139,6 +140,43 @@ __global__ void qtb_tc_split_kernel(const float2* __restrict__ src, uint32_t* __
     }
 }
 
+// B[k][f][n] (complex64, N columns) -> for every f, the planes B1_hi,
+// B1_lo, B2_hi, B2_lo of (Np / 64) x 128 rows x Kp TF32 words in tiles of
+// 128 rows x kTcStageK k, row-tile-major: in the rows of output tile t,
+// B1 holds Br of columns 64 t .. 64 t + 63 then their Bi, and B2 holds -Bi
+// then Br.  The negation is exact in TF32.
+__global__ void qtb_tc_split_b_kernel(const float2* __restrict__ src, uint32_t* __restrict__ dst, uint32_t K,
+                                      uint32_t F, uint32_t N, uint32_t Np, uint32_t Kp) {
+    const uint64_t rows = (uint64_t)(Np / kTcN) * kTcBRows;
+    const uint64_t plane = rows * Kp;
+    const uint64_t total = (uint64_t)F * (Np / kTcN) * kTcN * Kp;   // one thread per (f, k, column)
+    const uint32_t k_tiles = Kp / kTcStageK;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t n = (uint32_t)(i % Np);   // columns fastest: coalesced source reads
+        const uint32_t k = (uint32_t)((i / Np) % Kp);
+        const uint32_t f = (uint32_t)(i / ((uint64_t)Np * Kp));
+        float2 v = make_float2(0.f, 0.f);
+        if (n < N && k < K) v = src[((uint64_t)k * F + f) * N + n];
+        const uint32_t re_hi = tf32_round(v.x), im_hi = tf32_round(v.y);
+        const uint32_t re_lo = tf32_round(v.x - __uint_as_float(re_hi));
+        const uint32_t im_lo = tf32_round(v.y - __uint_as_float(im_hi));
+        const uint32_t t = n / kTcN, j = n % kTcN;
+        const uint64_t tile = (uint64_t)f * kTcPlanes * plane + ((uint64_t)t * k_tiles + k / kTcStageK) *
+                              (kTcBRows * kTcStageK);
+        const uint64_t w_re = tile + tc_tile_word(j, k % kTcStageK);          // row j: Br (B1), -Bi (B2)
+        const uint64_t w_im = tile + tc_tile_word(j + kTcN, k % kTcStageK);   // row 64 + j: Bi (B1), Br (B2)
+        dst[w_re] = re_hi;
+        dst[w_re + plane] = re_lo;
+        dst[w_im] = im_hi;
+        dst[w_im + plane] = im_lo;
+        dst[w_re + 2 * plane] = im_hi ^ 0x80000000u;
+        dst[w_re + 3 * plane] = im_lo ^ 0x80000000u;
+        dst[w_im + 2 * plane] = re_hi;
+        dst[w_im + 3 * plane] = re_lo;
+    }
+}
+
 __device__ __forceinline__ uint32_t tc_smem(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -153,8 +191,7 @@ __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
 
 // Instruction descriptor: FP32 accumulator, TF32 A and B, both K-major,
 // N = 64 (>> 3 at bit 17), M = 128 (>> 4 at bit 24); bit 13 negates A.
-constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((kTcN >> 3) << 17) | ((kTcM >> 4) << 24);
-constexpr uint32_t kTcIdescNegA = kTcIdesc | (1u << 13);
+constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((kTcBRows >> 3) << 17) | ((kTcM >> 4) << 24);
 
 __device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
     asm volatile(
@@ -249,7 +286,7 @@ qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restri
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = *tmem_slot;
-    const uint64_t a_plane = (uint64_t)Mp * Kp, b_plane = (uint64_t)Np * Kp;
+    const uint64_t a_plane = (uint64_t)Mp * Kp, b_plane = (uint64_t)(Np / kTcN) * kTcBRows * Kp;
     const uint32_t n_tiles = Kp / kTcStageK, n_blocks = Kp / kTcK;
     auto fail_once = [&]() {
         if (s_ok) atomicOr(status, kTcStatusTimeout);
@@ -289,26 +326,22 @@ qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restri
                 }
                 landed = i + 1;
                 asm volatile("tcgen05.fence::after_thread_sync;");
-                // planes: A 0 Ar_hi 1 Ar_lo 2 Ai_hi 3 Ai_lo | B 0 Br_hi 1 Br_lo 2 Bi_hi 3 Bi_lo
+                // planes: A 0 Ar_hi 1 Ar_lo 2 Ai_hi 3 Ai_lo | B 0 B1_hi 1 B1_lo 2 B2_hi 3 B2_lo with
+                // B1 = [Br | Bi] and B2 = [-Bi | Br] along N, so that
+                // Ar B1 + Ai B2 = [Re | Im] in the buffer's 128 columns
                 const uint32_t abase = stage_a(s), bbase = stage_b(s);
-                const uint32_t re = tmem + buf * kTcBufCols, im = re + kTcN;
+                const uint32_t acc = tmem + buf * kTcBufCols;
 #pragma unroll
                 for (uint32_t ks = 0; ks < kTcStageK / 8; ++ks) {
                     auto da = [&](uint32_t q) { return tc_desc(abase + q * kTcAWords * 4u + ks * 256u); };
                     auto db = [&](uint32_t q) { return tc_desc(bbase + q * kTcBWords * 4u + ks * 256u); };
                     const uint32_t first = (block_first && ks == 0) ? 0u : 1u;   // a block starts from zero
-                    tc_mma(re, da(0), db(0), kTcIdesc, first);
-                    tc_mma(re, da(0), db(1), kTcIdesc, 1u);
-                    tc_mma(re, da(1), db(0), kTcIdesc, 1u);
-                    tc_mma(re, da(2), db(2), kTcIdescNegA, 1u);
-                    tc_mma(re, da(2), db(3), kTcIdescNegA, 1u);
-                    tc_mma(re, da(3), db(2), kTcIdescNegA, 1u);
-                    tc_mma(im, da(0), db(2), kTcIdesc, first);
-                    tc_mma(im, da(0), db(3), kTcIdesc, 1u);
-                    tc_mma(im, da(1), db(2), kTcIdesc, 1u);
-                    tc_mma(im, da(2), db(0), kTcIdesc, 1u);
-                    tc_mma(im, da(2), db(1), kTcIdesc, 1u);
-                    tc_mma(im, da(3), db(0), kTcIdesc, 1u);
+                    tc_mma(acc, da(0), db(0), kTcIdesc, first);
+                    tc_mma(acc, da(0), db(1), kTcIdesc, 1u);
+                    tc_mma(acc, da(1), db(0), kTcIdesc, 1u);
+                    tc_mma(acc, da(2), db(2), kTcIdesc, 1u);
+                    tc_mma(acc, da(2), db(3), kTcIdesc, 1u);
+                    tc_mma(acc, da(3), db(2), kTcIdesc, 1u);
                 }
                 tc_commit(empty(s));
                 ++committed[s];
@@ -420,7 +453,7 @@ int qtb_contract_sum_scratch_bytes(int64_t K, int64_t F, int64_t M, int64_t N, i
         return QTB_OK;
     }
     const uint64_t Kp = round_up(K, kTcK), Mp = round_up(M, kTcM), Np = round_up(N, kTcN);
-    *bytes = 256 + (uint64_t)F * kTcPlanes * (Mp + Np) * Kp * 4;
+    *bytes = 256 + (uint64_t)F * kTcPlanes * (Mp + 2 * Np) * Kp * 4;   // B planes hold two rows per column
     return QTB_OK;
 }
 
@@ -454,8 +487,8 @@ int qtb_contract_sum_c64(const void* A, const void* B, void* C, int64_t K, int64
     auto split_blocks = [](uint64_t n) { return (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 32); };
     qtb_tc_split_kernel<<<split_blocks((uint64_t)F * Mp * Kp), 256, 0, st>>>(
         static_cast<const float2*>(A), Ap, (uint32_t)K, (uint32_t)F, (uint32_t)M, (uint32_t)Mp, (uint32_t)Kp, kTcM);
-    qtb_tc_split_kernel<<<split_blocks((uint64_t)F * Np * Kp), 256, 0, st>>>(
-        static_cast<const float2*>(B), Bp, (uint32_t)K, (uint32_t)F, (uint32_t)N, (uint32_t)Np, (uint32_t)Kp, kTcN);
+    qtb_tc_split_b_kernel<<<split_blocks((uint64_t)F * Np * Kp), 256, 0, st>>>(
+        static_cast<const float2*>(B), Bp, (uint32_t)K, (uint32_t)F, (uint32_t)N, (uint32_t)Np, (uint32_t)Kp);
     // per device and cheap: set on every call
     e = cudaFuncSetAttribute(qtb_tc_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kTcSmemBytes);

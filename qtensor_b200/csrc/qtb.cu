@@ -1722,6 +1722,13 @@ static int build_waves(qtb_plan* plan, std::vector<int32_t> wide, int32_t first,
         QTB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qtb_wide_kernel, kWideThreads, 0));
     }
+    // QTB_WIDE_TILES_PER_CTA (1..8, default 2) in the environment sets how
+    // many tiles a step is cut into per resident CTA
+    int tiles_per_cta = 2;
+    if (const char* env = std::getenv("QTB_WIDE_TILES_PER_CTA")) {
+        const int v = std::atoi(env);
+        if (v >= 1 && v <= 8) tiles_per_cta = v;
+    }
     std::vector<WideNet> nets;
     std::vector<WideStep> steps;
     std::vector<WideSeg> segs;
@@ -1771,8 +1778,9 @@ static int build_waves(qtb_plan* plan, std::vector<int32_t> wide, int32_t first,
             st.n_segs = (uint32_t)(segs.size() - rg.seg0) - st.seg_begin;
             st.total_elems = total;
             st.tile_begin = tiles;
-            // about two tiles per resident CTA, within [kWideMinTile, kWideMaxTile]
-            const uint32_t target = total / (uint32_t)(2 * std::max(1, per_sm) * sms) + 1;
+            // about `tiles_per_cta` tiles per resident CTA, within
+            // [kWideMinTile, kWideMaxTile]
+            const uint32_t target = total / (uint32_t)(tiles_per_cta * std::max(1, per_sm) * sms) + 1;
             st.tile_elems = std::min(kWideMaxTile, ((target + kWideMinTile - 1) / kWideMinTile) * kWideMinTile);
             st.n_tiles = std::max(1u, (total + st.tile_elems - 1) / st.tile_elems);
             tiles += st.n_tiles;
