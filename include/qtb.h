@@ -91,8 +91,9 @@ int qtb_bucket_c64(const qtb_bucket_desc* desc, const void* const* inputs,
  *                              C[f,m,n] = sum_k A[k,f,m] * B[k,f,n]
  * The contract-sum runs on the tcgen05 tensor cores (mode 2, or mode 0 when
  * K >= 32 and M, N >= 64): complex products in 3xTF32 (each operand split
- * into TF32 high and low parts), FP32 accumulation in tensor memory, 128 x
- * 128 output tiles; else (mode 1, or mode 0 for smaller shapes) on the CUDA
+ * into TF32 high and low parts), FP32 accumulation in tensor memory per
+ * 32-k block, the blocks summed in FP32 registers with round-to-nearest,
+ * 128 x 64 complex output tiles; else (mode 1, or mode 0 for smaller shapes) on the CUDA
  * cores in FP32.  scratch (qtb_contract_sum_scratch_bytes for the same
  * shape and mode) holds the split operands; its first 4 bytes are a status
  * word, 0 after a good run, 2 when a staging copy or the MMAs did not

@@ -111,14 +111,16 @@ __device__ __forceinline__ uint32_t tf32_round(float x) {
     return r;
 }
 
-// src[k][f][r] (complex64, R rows) -> for every f, planes q = 0..3 of
-// Rp x Kp TF32 words in tiles of `tile_rows` x kTcStageK k, row-tile-major.
+// src[k][f][r] (complex64, R rows) -> TF32 words in tiles of `tile_rows`
+// x kTcStageK k, ordered (f, row tile, k tile), each tile's four planes q
+// = 0..3 consecutive, so that one bulk copy stages all four.
 __global__ void qtb_tc_split_kernel(const float2* __restrict__ src, uint32_t* __restrict__ dst, uint32_t K,
                                     uint32_t F, uint32_t R, uint32_t Rp, uint32_t Kp, uint32_t tile_rows) {
     const uint64_t plane = (uint64_t)Rp * Kp;
     const uint64_t total = (uint64_t)F * plane;
     const uint32_t k_tiles = Kp / kTcStageK;
     const uint32_t tile_words = tile_rows * kTcStageK;
+    const uint32_t row_tiles = Rp / tile_rows;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
          i += (uint64_t)gridDim.x * blockDim.x) {
         // rows fastest, so the source reads are coalesced
@@ -130,26 +132,25 @@ __global__ void qtb_tc_split_kernel(const float2* __restrict__ src, uint32_t* __
         const uint32_t re_hi = tf32_round(v.x), im_hi = tf32_round(v.y);
         const uint32_t re_lo = tf32_round(v.x - __uint_as_float(re_hi));
         const uint32_t im_lo = tf32_round(v.y - __uint_as_float(im_hi));
-        const uint64_t base = (uint64_t)f * kTcPlanes * plane +
-                              ((uint64_t)(r / tile_rows) * k_tiles + k / kTcStageK) * tile_words +
+        const uint64_t base = (((uint64_t)f * row_tiles + r / tile_rows) * k_tiles + k / kTcStageK) *
+                                  (kTcPlanes * tile_words) +
                               tc_tile_word(r % tile_rows, k % kTcStageK);
         dst[base] = re_hi;
-        dst[base + plane] = re_lo;
-        dst[base + 2 * plane] = im_hi;
-        dst[base + 3 * plane] = im_lo;
+        dst[base + tile_words] = re_lo;
+        dst[base + 2 * tile_words] = im_hi;
+        dst[base + 3 * tile_words] = im_lo;
     }
 }
 
-// B[k][f][n] (complex64, N columns) -> for every f, the planes B1_hi,
-// B1_lo, B2_hi, B2_lo of (Np / 64) x 128 rows x Kp TF32 words in tiles of
-// 128 rows x kTcStageK k, row-tile-major: in the rows of output tile t,
+// B[k][f][n] (complex64, N columns) -> the planes B1_hi, B1_lo, B2_hi,
+// B2_lo in tiles of 128 rows x kTcStageK k, ordered (f, output column
+// tile, k tile), each tile's four planes consecutive: in the rows of tile t,
 // B1 holds Br of columns 64 t .. 64 t + 63 then their Bi, and B2 holds -Bi
 // then Br.  The negation is exact in TF32.
 __global__ void qtb_tc_split_b_kernel(const float2* __restrict__ src, uint32_t* __restrict__ dst, uint32_t K,
                                       uint32_t F, uint32_t N, uint32_t Np, uint32_t Kp) {
-    const uint64_t rows = (uint64_t)(Np / kTcN) * kTcBRows;
-    const uint64_t plane = rows * Kp;
-    const uint64_t total = (uint64_t)F * (Np / kTcN) * kTcN * Kp;   // one thread per (f, k, column)
+    const uint32_t col_tiles = Np / kTcN;
+    const uint64_t total = (uint64_t)F * Np * Kp;   // one thread per (f, k, column)
     const uint32_t k_tiles = Kp / kTcStageK;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
          i += (uint64_t)gridDim.x * blockDim.x) {
@@ -162,18 +163,17 @@ __global__ void qtb_tc_split_b_kernel(const float2* __restrict__ src, uint32_t* 
         const uint32_t re_lo = tf32_round(v.x - __uint_as_float(re_hi));
         const uint32_t im_lo = tf32_round(v.y - __uint_as_float(im_hi));
         const uint32_t t = n / kTcN, j = n % kTcN;
-        const uint64_t tile = (uint64_t)f * kTcPlanes * plane + ((uint64_t)t * k_tiles + k / kTcStageK) *
-                              (kTcBRows * kTcStageK);
+        const uint64_t tile = (((uint64_t)f * col_tiles + t) * k_tiles + k / kTcStageK) * (kTcPlanes * kTcBWords);
         const uint64_t w_re = tile + tc_tile_word(j, k % kTcStageK);          // row j: Br (B1), -Bi (B2)
         const uint64_t w_im = tile + tc_tile_word(j + kTcN, k % kTcStageK);   // row 64 + j: Bi (B1), Br (B2)
         dst[w_re] = re_hi;
-        dst[w_re + plane] = re_lo;
+        dst[w_re + kTcBWords] = re_lo;
         dst[w_im] = im_hi;
-        dst[w_im + plane] = im_lo;
-        dst[w_re + 2 * plane] = im_hi ^ 0x80000000u;
-        dst[w_re + 3 * plane] = im_lo ^ 0x80000000u;
-        dst[w_im + 2 * plane] = re_hi;
-        dst[w_im + 3 * plane] = re_lo;
+        dst[w_im + kTcBWords] = im_lo;
+        dst[w_re + 2 * kTcBWords] = im_hi ^ 0x80000000u;
+        dst[w_re + 3 * kTcBWords] = im_lo ^ 0x80000000u;
+        dst[w_im + 2 * kTcBWords] = re_hi;
+        dst[w_im + 3 * kTcBWords] = re_lo;
     }
 }
 
@@ -286,7 +286,6 @@ qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restri
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = *tmem_slot;
-    const uint64_t a_plane = (uint64_t)Mp * Kp, b_plane = (uint64_t)(Np / kTcN) * kTcBRows * Kp;
     const uint32_t n_tiles = Kp / kTcStageK, n_blocks = Kp / kTcK;
     auto fail_once = [&]() {
         if (s_ok) atomicOr(status, kTcStatusTimeout);
@@ -294,8 +293,9 @@ qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restri
     };
     if (warp == kTcEpilogueWarps) {
         if (lane == 0) {
-            const uint32_t* a_f = Ap + (uint64_t)f * kTcPlanes * a_plane + (uint64_t)mt * n_tiles * kTcAWords;
-            const uint32_t* b_f = Bp + (uint64_t)f * kTcPlanes * b_plane + (uint64_t)nt * n_tiles * kTcBWords;
+            // this CTA's tiles: (f, row tile, k tile) of A, (f, column tile, k tile) of B
+            const uint32_t* a_f = Ap + ((uint64_t)f * (Mp / kTcM) + mt) * n_tiles * (kTcPlanes * kTcAWords);
+            const uint32_t* b_f = Bp + ((uint64_t)f * (Np / kTcN) + nt) * n_tiles * (kTcPlanes * kTcBWords);
             auto stage_a = [&](uint32_t s) { return tc_smem(stages + s * kTcStageWords); };
             auto stage_b = [&](uint32_t s) { return tc_smem(stages + s * kTcStageWords + kTcPlanes * kTcAWords); };
             auto load = [&](uint32_t i) {   // tile i into stage i % NS
@@ -303,12 +303,9 @@ qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restri
                 asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full(s)),
                              "r"(kTcStageWords * 4u)
                              : "memory");
-                for (uint32_t q = 0; q < kTcPlanes; ++q) {
-                    tc_bulk(stage_a(s) + q * kTcAWords * 4u, a_f + q * a_plane + (uint64_t)i * kTcAWords,
-                            kTcAWords * 4u, full(s));
-                    tc_bulk(stage_b(s) + q * kTcBWords * 4u, b_f + q * b_plane + (uint64_t)i * kTcBWords,
-                            kTcBWords * 4u, full(s));
-                }
+                // the tile's four planes are consecutive in global memory and in the stage
+                tc_bulk(stage_a(s), a_f + (uint64_t)i * kTcPlanes * kTcAWords, kTcPlanes * kTcAWords * 4u, full(s));
+                tc_bulk(stage_b(s), b_f + (uint64_t)i * kTcPlanes * kTcBWords, kTcPlanes * kTcBWords * 4u, full(s));
             };
             uint32_t loaded = 0, landed = 0;   // tiles whose copies were issued, waited for
             uint32_t committed[NS] = {}, retired[NS] = {};   // empty[s] phases issued, waited for
