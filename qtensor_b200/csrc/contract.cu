@@ -111,70 +111,80 @@ __device__ __forceinline__ uint32_t tf32_round(float x) {
     return r;
 }
 
-// src[k][f][r] (complex64, R rows) -> TF32 words in tiles of `tile_rows`
-// x kTcStageK k, ordered (f, row tile, k tile), each tile's four planes q
-// = 0..3 consecutive, so that one bulk copy stages all four.
-__global__ void qtb_tc_split_kernel(const float2* __restrict__ src, uint32_t* __restrict__ dst, uint32_t K,
-                                    uint32_t F, uint32_t R, uint32_t Rp, uint32_t Kp, uint32_t tile_rows) {
-    const uint64_t plane = (uint64_t)Rp * Kp;
-    const uint64_t total = (uint64_t)F * plane;
-    const uint32_t k_tiles = Kp / kTcStageK;
-    const uint32_t tile_words = tile_rows * kTcStageK;
-    const uint32_t row_tiles = Rp / tile_rows;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        // rows fastest, so the source reads are coalesced
-        const uint32_t r = (uint32_t)(i % Rp);
-        const uint32_t k = (uint32_t)((i / Rp) % Kp);
-        const uint32_t f = (uint32_t)(i / plane);
-        float2 v = make_float2(0.f, 0.f);
-        if (r < R && k < K) v = src[((uint64_t)k * F + f) * R + r];
-        const uint32_t re_hi = tf32_round(v.x), im_hi = tf32_round(v.y);
-        const uint32_t re_lo = tf32_round(v.x - __uint_as_float(re_hi));
-        const uint32_t im_lo = tf32_round(v.y - __uint_as_float(im_hi));
-        const uint64_t base = (((uint64_t)f * row_tiles + r / tile_rows) * k_tiles + k / kTcStageK) *
-                                  (kTcPlanes * tile_words) +
-                              tc_tile_word(r % tile_rows, k % kTcStageK);
-        dst[base] = re_hi;
-        dst[base + tile_words] = re_lo;
-        dst[base + 2 * tile_words] = im_hi;
-        dst[base + 3 * tile_words] = im_lo;
-    }
+// TF32 hi / lo of one component: hi rounded to nearest, lo the rounded remainder.
+__device__ __forceinline__ void tf32_split(float x, uint32_t& hi, uint32_t& lo) {
+    hi = tf32_round(x);
+    lo = tf32_round(x - __uint_as_float(hi));
 }
 
-// B[k][f][n] (complex64, N columns) -> the planes B1_hi, B1_lo, B2_hi,
-// B2_lo in tiles of 128 rows x kTcStageK k, ordered (f, output column
-// tile, k tile), each tile's four planes consecutive: in the rows of tile t,
-// B1 holds Br of columns 64 t .. 64 t + 63 then their Bi, and B2 holds -Bi
-// then Br.  The negation is exact in TF32.
-__global__ void qtb_tc_split_b_kernel(const float2* __restrict__ src, uint32_t* __restrict__ dst, uint32_t K,
-                                      uint32_t F, uint32_t N, uint32_t Np, uint32_t Kp) {
-    const uint32_t col_tiles = Np / kTcN;
-    const uint64_t total = (uint64_t)F * Np * Kp;   // one thread per (f, k, column)
-    const uint32_t k_tiles = Kp / kTcStageK;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t n = (uint32_t)(i % Np);   // columns fastest: coalesced source reads
-        const uint32_t k = (uint32_t)((i / Np) % Kp);
-        const uint32_t f = (uint32_t)(i / ((uint64_t)Np * Kp));
-        float2 v = make_float2(0.f, 0.f);
-        if (n < N && k < K) v = src[((uint64_t)k * F + f) * N + n];
-        const uint32_t re_hi = tf32_round(v.x), im_hi = tf32_round(v.y);
-        const uint32_t re_lo = tf32_round(v.x - __uint_as_float(re_hi));
-        const uint32_t im_lo = tf32_round(v.y - __uint_as_float(im_hi));
-        const uint32_t t = n / kTcN, j = n % kTcN;
-        const uint64_t tile = (((uint64_t)f * col_tiles + t) * k_tiles + k / kTcStageK) * (kTcPlanes * kTcBWords);
-        const uint64_t w_re = tile + tc_tile_word(j, k % kTcStageK);          // row j: Br (B1), -Bi (B2)
-        const uint64_t w_im = tile + tc_tile_word(j + kTcN, k % kTcStageK);   // row 64 + j: Bi (B1), Br (B2)
-        dst[w_re] = re_hi;
-        dst[w_re + kTcBWords] = re_lo;
-        dst[w_im] = im_hi;
-        dst[w_im + kTcBWords] = im_lo;
-        dst[w_re + 2 * kTcBWords] = im_hi ^ 0x80000000u;
-        dst[w_re + 3 * kTcBWords] = im_lo ^ 0x80000000u;
-        dst[w_im + 2 * kTcBWords] = re_hi;
-        dst[w_im + 3 * kTcBWords] = re_lo;
+// Copies a staged tile (`words` 32-bit words) from shared memory to dst, 16 bytes per thread and step.
+__device__ __forceinline__ void tc_write_tile(const uint32_t* s, uint32_t* dst, uint32_t words) {
+    const uint4* in = reinterpret_cast<const uint4*>(s);
+    uint4* out = reinterpret_cast<uint4*>(dst);
+    for (uint32_t i = threadIdx.x; i < words / 4; i += blockDim.x) out[i] = in[i];
+}
+
+// A[k][f][m] (complex64, M rows) -> TF32 planes Ar_hi, Ar_lo, Ai_hi, Ai_lo
+// in tiles of 128 rows x kTcStageK k, ordered (f, row tile, k tile), each
+// tile's four planes consecutive, so that one bulk copy stages all four.
+// One block per tile: coalesced reads of the tile's rows, the split into
+// shared memory in the core-matrix layout, then one contiguous write.
+__global__ void __launch_bounds__(256) qtb_tc_split_kernel(const float2* __restrict__ src,
+                                                           uint32_t* __restrict__ dst, uint32_t K, uint32_t F,
+                                                           uint32_t M, uint32_t Mp, uint32_t Kp) {
+    __shared__ __align__(16) uint32_t s[kTcPlanes * kTcAWords];
+    const uint32_t k_tiles = Kp / kTcStageK, row_tiles = Mp / kTcM;
+    const uint32_t bid = blockIdx.x;
+    const uint32_t kt = bid % k_tiles, rt = (bid / k_tiles) % row_tiles, f = bid / (k_tiles * row_tiles);
+    for (uint32_t e = threadIdx.x; e < kTcM * kTcStageK; e += blockDim.x) {
+        const uint32_t r = e % kTcM, k = e / kTcM;
+        const uint32_t m = rt * kTcM + r, kk = kt * kTcStageK + k;
+        const float2 v = (m < M && kk < K) ? src[((uint64_t)kk * F + f) * M + m] : make_float2(0.f, 0.f);
+        uint32_t rh, rl, ih, il;
+        tf32_split(v.x, rh, rl);
+        tf32_split(v.y, ih, il);
+        const uint32_t w = tc_tile_word(r, k);
+        s[w] = rh;
+        s[kTcAWords + w] = rl;
+        s[2 * kTcAWords + w] = ih;
+        s[3 * kTcAWords + w] = il;
     }
+    __syncthreads();
+    tc_write_tile(s, dst + (uint64_t)bid * kTcPlanes * kTcAWords, kTcPlanes * kTcAWords);
+}
+
+// B[k][f][n] (complex64, N columns) -> TF32 planes B1_hi, B1_lo, B2_hi,
+// B2_lo in tiles of 128 rows x kTcStageK k, ordered (f, output column
+// tile, k tile), each tile's four planes consecutive: in the rows of tile
+// t, B1 holds Br of columns 64 t .. 64 t + 63 then their Bi, and B2 holds
+// -Bi then Br (the negation is exact in TF32).  One block per tile, as for A.
+__global__ void __launch_bounds__(256) qtb_tc_split_b_kernel(const float2* __restrict__ src,
+                                                             uint32_t* __restrict__ dst, uint32_t K, uint32_t F,
+                                                             uint32_t N, uint32_t Np, uint32_t Kp) {
+    __shared__ __align__(16) uint32_t s[kTcPlanes * kTcBWords];
+    const uint32_t k_tiles = Kp / kTcStageK, col_tiles = Np / kTcN;
+    const uint32_t bid = blockIdx.x;
+    const uint32_t kt = bid % k_tiles, t = (bid / k_tiles) % col_tiles, f = bid / (k_tiles * col_tiles);
+    for (uint32_t e = threadIdx.x; e < kTcN * kTcStageK; e += blockDim.x) {
+        const uint32_t j = e % kTcN, k = e / kTcN;
+        const uint32_t n = t * kTcN + j, kk = kt * kTcStageK + k;
+        const float2 v = (n < N && kk < K) ? src[((uint64_t)kk * F + f) * N + n] : make_float2(0.f, 0.f);
+        uint32_t rh, rl, ih, il;
+        tf32_split(v.x, rh, rl);
+        tf32_split(v.y, ih, il);
+        const uint32_t w_re = tc_tile_word(j, k);          // row j: Br (B1), -Bi (B2)
+        const uint32_t w_im = tc_tile_word(j + kTcN, k);   // row 64 + j: Bi (B1), Br (B2)
+        s[w_re] = rh;
+        s[kTcBWords + w_re] = rl;
+        s[w_im] = ih;
+        s[kTcBWords + w_im] = il;
+        s[2 * kTcBWords + w_re] = ih ^ 0x80000000u;
+        s[3 * kTcBWords + w_re] = il ^ 0x80000000u;
+        s[2 * kTcBWords + w_im] = rh;
+        s[3 * kTcBWords + w_im] = rl;
+    }
+    __syncthreads();
+    tc_write_tile(s, dst + (uint64_t)bid * kTcPlanes * kTcBWords, kTcPlanes * kTcBWords);
 }
 
 __device__ __forceinline__ uint32_t tc_smem(const void* p) {
@@ -214,15 +224,24 @@ __device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
     return false;
 }
 
-// Eight 32-bit TMEM columns of this thread's lane.
-__device__ __forceinline__ void tc_ld8(uint32_t taddr, float* out) {
-    uint32_t r[8];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+// Eight 32-bit TMEM columns of this thread's lane at each of two
+// addresses, one wait for both loads; the wait is in the same asm as the
+// loads, so no use of the registers can be scheduled before it.
+__device__ __forceinline__ void tc_ld2x8(uint32_t ta, uint32_t tb, float* a, float* b) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%16];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%8,%9,%10,%11,%12,%13,%14,%15}, [%17];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(ta), "r"(tb)
+        : "memory");
 #pragma unroll
-    for (int j = 0; j < 8; ++j) out[j] = __uint_as_float(r[j]);
+    for (int j = 0; j < 8; ++j) {
+        a[j] = __uint_as_float(r[j]);
+        b[j] = __uint_as_float(r[8 + j]);
+    }
 }
 
 __device__ __forceinline__ void tc_bulk(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
@@ -380,13 +399,13 @@ qtb_tc_contract_kernel(const uint32_t* __restrict__ Ap, const uint32_t* __restri
             asm volatile("tcgen05.fence::after_thread_sync;");
 #pragma unroll
             for (uint32_t c0 = 0; c0 < kTcN; c0 += 8u) {
-                float v[8];
-                tc_ld8(lane_addr + buf * kTcBufCols + c0, v);
+                float vr[8], vi[8];
+                tc_ld2x8(lane_addr + buf * kTcBufCols + c0, lane_addr + buf * kTcBufCols + kTcN + c0, vr, vi);
 #pragma unroll
-                for (uint32_t j = 0; j < 8; ++j) acc_re[c0 + j] += v[j];
-                tc_ld8(lane_addr + buf * kTcBufCols + kTcN + c0, v);
-#pragma unroll
-                for (uint32_t j = 0; j < 8; ++j) acc_im[c0 + j] += v[j];
+                for (uint32_t j = 0; j < 8; ++j) {
+                    acc_re[c0 + j] += vr[j];
+                    acc_im[c0 + j] += vi[j];
+                }
             }
             asm volatile("tcgen05.fence::before_thread_sync;");
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tempty(buf)) : "memory");
@@ -476,15 +495,17 @@ int qtb_contract_sum_c64(const void* A, const void* B, void* C, int64_t K, int64
         return e == cudaSuccess ? QTB_OK : cuda_fail_c(e, "contract_sum launch");
     }
     const uint64_t Kp = round_up(K, kTcK), Mp = round_up(M, kTcM), Np = round_up(N, kTcN);
-    if (Mp / kTcM > 65535 || F > 65535 || Np / kTcN > (1u << 31) || Kp > (1u << 30))
+    if (Mp / kTcM > 65535 || F > 65535 || Np / kTcN > (1u << 31) || Kp > (1u << 30) ||
+        (uint64_t)F * (Mp / kTcM) * (Kp / kTcStageK) >= (1ull << 31) ||
+        (uint64_t)F * (Np / kTcN) * (Kp / kTcStageK) >= (1ull << 31))
         return fail(QTB_ERR_UNSUPPORTED, "contract_sum: shape beyond the tensor-core grid");
     int* status = static_cast<int*>(scratch);
     uint32_t* Ap = reinterpret_cast<uint32_t*>(static_cast<char*>(scratch) + 256);
     uint32_t* Bp = Ap + (uint64_t)F * kTcPlanes * Mp * Kp;
-    auto split_blocks = [](uint64_t n) { return (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 32); };
-    qtb_tc_split_kernel<<<split_blocks((uint64_t)F * Mp * Kp), 256, 0, st>>>(
-        static_cast<const float2*>(A), Ap, (uint32_t)K, (uint32_t)F, (uint32_t)M, (uint32_t)Mp, (uint32_t)Kp, kTcM);
-    qtb_tc_split_b_kernel<<<split_blocks((uint64_t)F * Np * Kp), 256, 0, st>>>(
+    const uint32_t k_tiles = (uint32_t)(Kp / kTcStageK);
+    qtb_tc_split_kernel<<<(unsigned)(F * (Mp / kTcM) * k_tiles), 256, 0, st>>>(
+        static_cast<const float2*>(A), Ap, (uint32_t)K, (uint32_t)F, (uint32_t)M, (uint32_t)Mp, (uint32_t)Kp);
+    qtb_tc_split_b_kernel<<<(unsigned)(F * (Np / kTcN) * k_tiles), 256, 0, st>>>(
         static_cast<const float2*>(B), Bp, (uint32_t)K, (uint32_t)F, (uint32_t)N, (uint32_t)Np, (uint32_t)Kp);
     // per device and cheap: set on every call
     e = cudaFuncSetAttribute(qtb_tc_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
