@@ -928,11 +928,10 @@ constexpr uint32_t kWideSpinLimit = 1u << 23;   // about 1 s of polling
 constexpr int kWideThreads = 256;
 constexpr uint32_t kWideBatchLog = 3;                               // log2 of the elements per thread in flight
 constexpr uint32_t kWideBatch = 1u << kWideBatchLog;
-constexpr uint32_t kWideBatchBits = (kWideBatch - 1u) << 5;          // the bits of j above the lane index
-constexpr uint32_t kWideWarpTile = kWideBatch * 32;                  // 256: smallest tile of one warp
+constexpr uint32_t kWideBatchBits = (kWideBatch - 1u) << 8;          // the bits of j above the thread index
 constexpr uint32_t kWideGroup = 1;                                  // operands per batch of loads
-constexpr uint32_t kWideMinTile = kWideWarpTile;                    // 256: tiles and segments align to it
-constexpr uint32_t kWideMaxTile = 64 * kWideMinTile;
+constexpr uint32_t kWideMinTile = kWideBatch * kWideThreads;         // 2048
+constexpr uint32_t kWideMaxTile = 8 * kWideMinTile;
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
     unsigned int v;
@@ -1018,8 +1017,8 @@ __device__ __forceinline__ void compute_element_wide(const DevOp& op, uint32_t j
     arena[op.dst + j] = op.sum ? make_float2(p0.x + p1.x, p0.y + p1.y) : p0;
 }
 
-// kWideBatch elements j + 32 e of one op at once, with the kWideBatchLog
-// bits of j from bit 5 up zero: they differ from j only in those bits, so
+// kWideBatch elements j + 256 e of one op at once, with the kWideBatchLog
+// bits of j from bit 8 up zero: they differ from j only in those bits, so
 // each operand offset is the gathered offset of j plus the gathered offsets
 // of those bits (one full gather per operand, not kWideBatch), and the
 // loads of kWideGroup operands for all elements are issued together
@@ -1047,11 +1046,11 @@ __device__ __forceinline__ void compute_elements_wide(const DevOp& op, uint32_t 
                 const bool has_sum = op.sum && ((d[t].mask >> w) & 1u);
                 const uint32_t stride_s = has_sum ? 1u << (__popc(d[t].mask) - 1) : 0u;
                 const uint32_t m = d[t].mask & low;
-                // bit 5 + i of j lands at operand bit popc(m below it) when m has it
+                // bit 8 + i of j lands at operand bit popc(m below it) when m has it
                 uint32_t bit_off[kWideBatchLog];
 #pragma unroll
                 for (uint32_t i = 0; i < kWideBatchLog; ++i)
-                    bit_off[i] = ((m >> (5 + i)) & 1u) << __popc(m & ((1u << (5 + i)) - 1u));
+                    bit_off[i] = ((m >> (8 + i)) & 1u) << __popc(m & ((1u << (8 + i)) - 1u));
                 uint32_t off[kWideBatch];
                 off[0] = gather_bits(j, d[t], low);
 #pragma unroll
@@ -1083,7 +1082,7 @@ __device__ __forceinline__ void compute_elements_wide(const DevOp& op, uint32_t 
     }
 #pragma unroll
     for (uint32_t e = 0; e < kWideBatch; ++e)
-        arena[op.dst + j + e * 32u] = op.sum ? make_float2(p0[e].x + p1[e].x, p0[e].y + p1[e].y) : p0[e];
+        arena[op.dst + j + e * 256u] = op.sum ? make_float2(p0[e].x + p1[e].x, p0[e].y + p1[e].y) : p0[e];
 }
 
 __device__ __forceinline__ void prefetch_l1(const void* p) {
@@ -1145,22 +1144,21 @@ __device__ __forceinline__ bool wide_locate(const WideArgs& w, const RunArgs& a,
     return true;
 }
 
-// The unit of work is one warp: a warp claims tiles in order from one
-// counter, claims its next tile as soon as it starts waiting on the
-// current one, and locates its lanes' first elements (segment, network,
-// phase, op, operand descriptors: plan data, which no tile writes) before
-// lane 0 waits for the previous step's tiles.  No CTA barrier is involved,
-// so a warp never waits for the slower warps of its CTA.  A claimed tile
-// is processed after the warp's current one, and a tile waits only on
-// tiles claimed before it, so the scheme cannot deadlock and needs no
-// co-residency.
+// Tiles are claimed in order from one counter; a CTA claims its next tile
+// as soon as it starts waiting on the current one, and every thread
+// locates its first element of the tile (segment, network, phase, op,
+// operand descriptors: plan data, which no tile writes) before the wait on
+// the previous step, so that a step's tiles start with their loads of the
+// previous step's results instead of a chain of dependent lookups.  A
+// claimed tile is processed after the CTA's current one, and a tile waits
+// only on tiles claimed before it, so the scheme still cannot deadlock.
 __global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArgs w, const RunArgs a) {
-    const uint32_t lane = threadIdx.x & 31u;
-    constexpr unsigned kAll = 0xffffffffu;
-    uint32_t t = 0;
-    if (lane == 0) t = atomicAdd(w.counters, 1u);
-    t = __shfl_sync(kAll, t, 0);
+    __shared__ uint32_t s_tile;
+    __shared__ int s_ok, s_last;
+    if (threadIdx.x == 0) s_tile = atomicAdd(w.counters, 1u);
     for (;;) {
+        __syncthreads();   // s_tile holds this CTA's next tile
+        const uint32_t t = s_tile;
         if (t > w.n_tiles) break;
         uint32_t s = w.n_steps;   // the result tile follows the last step
         if (t < w.n_tiles) {
@@ -1179,70 +1177,71 @@ __global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArg
             st = w.steps[s];
             e0 = (t - st.tile_begin) * st.tile_elems;
             e1 = min(e0 + st.tile_elems, st.total_elems);
-            const uint32_t g0 = e0 + lane;
+            const uint32_t g0 = e0 + threadIdx.x;
             if (g0 < e1 && wide_locate(w, a, st, s, g0, pl)) prefetch_l1(pl.ins + pl.op.in_begin);
         }
-        uint32_t next = 0;
-        int ok = 1;
-        if (lane == 0) {
-            if (t < w.n_tiles) next = atomicAdd(w.counters, 1u);
-            if (s > 0 && !wait_counter(w.counters + s, __ldg(&w.steps[s - 1].n_tiles), kWideSpinLimit, a.status,
-                                       kStatusWideTimeout))
-                ok = 0;
+        __syncthreads();   // every thread has read s_tile
+        if (threadIdx.x == 0) {
+            if (t < w.n_tiles) s_tile = atomicAdd(w.counters, 1u);
+            s_ok = 1;
+            if (s > 0 && !wait_counter(w.counters + s, __ldg(&w.steps[s - 1].n_tiles), kWideSpinLimit,
+                                       a.status, kStatusWideTimeout))
+                s_ok = 0;
             __threadfence();
         }
-        ok = __shfl_sync(kAll, ok, 0);
-        next = __shfl_sync(kAll, next, 0);
-        if (!ok) return;
+        __syncthreads();
+        if (!s_ok) return;
         if (t == w.n_tiles) {
             // every step is done: the wave's terms, then the run's energy if
             // this wave finished the run's last networks
-            for (uint32_t n = lane; n < w.n_nets; n += 32u) {
+            for (uint32_t n = threadIdx.x; n < w.n_nets; n += blockDim.x) {
                 const WideNet wn = w.nets[n];
                 const DevNetRun net = *wn.run;
                 const float2* arena = w.arenas + wn.arena_off;
                 *wn.term = (net.result_src & kSrcTable) ? __ldg(a.gtable + (net.result_src & ~kSrcTable))
                                                         : __ldcg(arena + net.result_src);
             }
-            __syncwarp();
-            uint32_t last = 0;
-            if (lane == 0 && a.energy) {
-                __threadfence();
-                last = atomicAdd(a.done, w.n_nets) == a.total_jobs - w.n_nets;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                s_last = 0;
+                if (a.energy) {
+                    __threadfence();
+                    s_last = atomicAdd(a.done, w.n_nets) == a.total_jobs - w.n_nets;
+                }
             }
-            last = __shfl_sync(kAll, last, 0);
-            if (last) {
+            __syncthreads();
+            if (s_last) {
                 __threadfence();
-                reduce_energy_warp(a.terms, a.total_jobs, a.energy_groups, a.energy);
-                if (lane == 0) *a.done = 0u;
+                reduce_energy(a.terms, a.total_jobs, a.energy_groups, a.energy);
+                if (threadIdx.x == 0) *a.done = 0u;
             }
             break;
         }
-        for (uint32_t g = e0 + lane; g < e1;) {
+        const uint32_t bd = blockDim.x;
+        for (uint32_t g = e0 + threadIdx.x; g < e1;) {
             if (!wide_locate(w, a, st, s, g, pl)) {   // padding between segments
-                g += 32u;
+                g += bd;
                 continue;
             }
             // kWideBatch elements of the same op that differ only in the bits
-            // from bit 5 up of the op index (the common case in wide phases:
-            // tiles, segments and ops start at multiples of kWideWarpTile)
+            // from bit 8 up of the op index (the common case in wide phases:
+            // tiles, segments and ops start at multiples of kWideMinTile)
             const uint32_t l = g - pl.seg_lo;
             const uint32_t j = l - pl.op.elem_begin;
-            if ((j & kWideBatchBits) == 0u && g + (kWideBatch - 1) * 32u < min(e1, pl.seg_hi) &&
-                l + (kWideBatch - 1) * 32u < pl.op_hi) {
+            if (bd == 256u && (j & kWideBatchBits) == 0u && g + (kWideBatch - 1) * bd < min(e1, pl.seg_hi) &&
+                l + (kWideBatch - 1) * bd < pl.op_hi) {
                 compute_elements_wide(pl.op, j, pl.ins, a.gtable, pl.arena);
-                g += kWideBatch * 32u;
+                g += kWideBatch * bd;
             } else {
                 compute_element_wide(pl.op, j, pl.ins, a.gtable, pl.arena);
-                g += 32u;
+                g += bd;
             }
         }
-        __syncwarp();
-        if (lane == 0) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
             __threadfence();
             atomicAdd(w.counters + 1 + s, 1u);
         }
-        t = next;
     }
 }
 
@@ -1730,12 +1729,12 @@ static int build_waves(qtb_plan* plan, std::vector<int32_t> wide, int32_t first,
         QTB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qtb_wide_kernel, kWideThreads, 0));
     }
-    // QTB_WIDE_TILES_PER_WARP (1..8, default 2) in the environment sets how
-    // many tiles a step is cut into per resident warp
-    int tiles_per_warp = 2;
-    if (const char* env = std::getenv("QTB_WIDE_TILES_PER_WARP")) {
+    // QTB_WIDE_TILES_PER_CTA (1..8, default 2) in the environment sets how
+    // many tiles a step is cut into per resident CTA
+    int tiles_per_cta = 2;
+    if (const char* env = std::getenv("QTB_WIDE_TILES_PER_CTA")) {
         const int v = std::atoi(env);
-        if (v >= 1 && v <= 8) tiles_per_warp = v;
+        if (v >= 1 && v <= 8) tiles_per_cta = v;
     }
     std::vector<WideNet> nets;
     std::vector<WideStep> steps;
@@ -1777,8 +1776,8 @@ static int build_waves(qtb_plan* plan, std::vector<int32_t> wide, int32_t first,
                 const Network& n = plan->nets[wide[k]];
                 if (ph >= n.phases.size()) continue;
                 // segments start at multiples of kWideMinTile, so that with the
-                // ops of a phase sorted widest first the elements a lane
-                // batches differ only in bits 5 to 7 of their op index
+                // ops of a phase sorted widest first the elements a thread
+                // batches differ only in bits 8 and 9 of their op index
                 total = (total + kWideMinTile - 1) & ~(kWideMinTile - 1);
                 segs.push_back(WideSeg{(uint32_t)(k - pos), total});
                 total += n.phases[ph].total_elems;
@@ -1786,10 +1785,9 @@ static int build_waves(qtb_plan* plan, std::vector<int32_t> wide, int32_t first,
             st.n_segs = (uint32_t)(segs.size() - rg.seg0) - st.seg_begin;
             st.total_elems = total;
             st.tile_begin = tiles;
-            // about `tiles_per_warp` tiles per resident warp, within
+            // about `tiles_per_cta` tiles per resident CTA, within
             // [kWideMinTile, kWideMaxTile]
-            const uint32_t warps = (uint32_t)(std::max(1, per_sm) * sms * (kWideThreads / 32));
-            const uint32_t target = total / (uint32_t)(tiles_per_warp * warps) + 1;
+            const uint32_t target = total / (uint32_t)(tiles_per_cta * std::max(1, per_sm) * sms) + 1;
             st.tile_elems = std::min(kWideMaxTile, ((target + kWideMinTile - 1) / kWideMinTile) * kWideMinTile);
             st.n_tiles = std::max(1u, (total + st.tile_elems - 1) / st.tile_elems);
             tiles += st.n_tiles;
@@ -1797,8 +1795,7 @@ static int build_waves(qtb_plan* plan, std::vector<int32_t> wide, int32_t first,
         }
         wv.n_steps = max_phases;
         wv.n_tiles = tiles;
-        wv.grid = std::max(1, std::min<int>(((int)tiles + 1 + kWideThreads / 32 - 1) / (kWideThreads / 32),
-                                            std::max(1, per_sm) * sms));
+        wv.grid = std::max(1, std::min<int>((int)tiles + 1, std::max(1, per_sm) * sms));
         rc->waves.push_back(wv);
         ranges.push_back(rg);
         pos = end;
