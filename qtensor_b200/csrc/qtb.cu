@@ -679,37 +679,30 @@ __global__ void __launch_bounds__(kLean == 2 ? 96 : kLean ? 128 : (kPersistent ?
         blob + a.blob_capacity + (kSmemTable ? ((a.table_elems * 8u + 15u) & ~15u) : 0u);
     float2* arena = kSmemArena ? reinterpret_cast<float2*>(after_table)
                                : a.gscratch + (size_t)blockIdx.x * a.arena_capacity;
-    // a persistent CTA claims its next network while contracting the
-    // current one (two slots, read and written in alternate iterations), so
-    // the queue's round trip is off the critical path
-    __shared__ unsigned int s_job[2], is_last;
+    __shared__ unsigned int s_job, is_last;
     __shared__ uint2 s_head[kSmemArena && kSmemTable ? kRecHeadSmem : 1];
     if (kPersistent && a.queue == nullptr) {   // a persistent launch needs its queue
         if (threadIdx.x == 0) atomicOr(a.status, kStatusQueue);
         return;
     }
     if (threadIdx.x == 0) {
-        if (kPersistent) s_job[0] = atomicAdd(a.queue, 1u);
         l2_prefetch_part(a.recs, a.recs_bytes, blockIdx.x, gridDim.x);
         l2_prefetch_part(a.runs, a.runs_bytes, blockIdx.x, gridDim.x);
         l2_prefetch_part(jobs, a.n_jobs * (uint32_t)sizeof(Job), blockIdx.x, gridDim.x);
     }
-    mbar_init(bar);   // (its barrier also publishes s_job[0])
+    mbar_init(bar);
     uint32_t parity = 0;
     const float2* __restrict__ table = kSmemTable ? stable : a.gtable;
     bool table_ready = !kSmemTable;
     for (uint32_t iter = 0;; ++iter) {
-        uint32_t cur = blockIdx.x;
         if (kPersistent) {
-            // s_job[iter & 1] was written before the previous iteration's
-            // last barrier; s_job[(iter + 1) & 1] was last read before it
-            cur = s_job[iter & 1u];
-            if (cur >= a.n_jobs) break;
-            if (threadIdx.x == 0) s_job[(iter + 1u) & 1u] = atomicAdd(a.queue, 1u);
+            if (threadIdx.x == 0) s_job = atomicAdd(a.queue, 1u);
+            __syncthreads();
+            if (s_job >= a.n_jobs) break;
         } else if (iter > 0) {
             break;
         }
-        const Job job = jobs[cur];
+        const Job job = jobs[kPersistent ? s_job : blockIdx.x];
         const DevNetRun net = *job.net;
         // a network with element records needs no blob (shared table and
         // arena only); otherwise blob_capacity 0: the launch reads plan
