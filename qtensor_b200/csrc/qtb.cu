@@ -446,6 +446,13 @@ __device__ void build_table(const unsigned char* common, const RunArgs& a, float
     __syncthreads();
 }
 
+// Thread 32 claims the CTA's next network when the current one reaches its
+// tail (phases of at most 32 elements, run by warp 0 alone): the other
+// warps are idle by then, and the queue's round trip overlaps the tail.
+__device__ __forceinline__ void claim_next(unsigned int* slot, unsigned int* queue) {
+    if (threadIdx.x == 32 && slot != nullptr) *slot = atomicAdd(queue, 1u);
+}
+
 // The phases of one staged network; its scalar result is returned to thread 0.
 template <bool kSmemTable>
 __device__ float2 contract_network(const DevNetRun& net, const unsigned char* blob,
@@ -493,13 +500,6 @@ __device__ float2 contract_network(const DevNetRun& net, const unsigned char* bl
     if (threadIdx.x == 0)
         result = (net.result_src & kSrcTable) ? table[net.result_src & ~kSrcTable] : arena[net.result_src];
     return result;
-}
-
-// Thread 32 claims the CTA's next network when the current one reaches its
-// tail (phases of at most 32 elements, run by warp 0 alone): the other
-// warps are idle by then, and the queue's round trip overlaps the tail.
-__device__ __forceinline__ void claim_next(unsigned int* slot, unsigned int* queue) {
-    if (threadIdx.x == 32 && slot != nullptr) *slot = atomicAdd(queue, 1u);
 }
 
 // ------------------------------------------- element records (see plan.h)
