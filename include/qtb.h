@@ -347,12 +347,15 @@ int qtb_plan_device_status(qtb_plan* plan, int32_t* status);
  * word returned in *status_out.  Synchronous; the device stays usable.    */
 int qtb_selftest_wait_timeout(int32_t spin_limit, int32_t* status_out);
 
-/* Device pointer of pinned host memory (cudaHostGetDevicePointer): passed
- * as qtb_plan_run's params_dev and energy_dev, the executor reads a
- * caller's pinned angles and writes its pinned energy directly, so that a
- * captured call needs no host<->device copy nodes.  No counterpart in the
- * reference.                                                             */
+/* Device pointer of pinned host memory (cudaHostGetDevicePointer), so that
+ * kernels read a caller's pinned angles and write its pinned energy
+ * directly: a captured call then needs no host<->device copy nodes.  No
+ * counterpart in the reference.                                          */
 int qtb_host_device_pointer(void* host, void** dev);
+/* Copy of `bytes` (a multiple of 8) between device-accessible buffers by a
+ * kernel (device memory, or pinned host memory through its device
+ * pointer), asynchronous on stream.                                      */
+int qtb_copy_c(void* dst, const void* src, size_t bytes, void* stream);
 
 /* CUDA-event timing of the network-executor launches of qtb_plan_run, on
  * the run's stream.  set_timing resets the totals; collect_timing waits for

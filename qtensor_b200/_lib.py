@@ -36,7 +36,7 @@ EXPORTS = (
     'qtb_plan_scratch_bytes', 'qtb_plan_run', 'qtb_plan_plain_scratch_bytes',
     'qtb_plan_run_plain', 'qtb_plan_set_autotune',
     'qtb_plan_last_launch_config', 'qtb_plan_device_bytes', 'qtb_plan_device_status',
-    'qtb_selftest_wait_timeout', 'qtb_host_device_pointer',
+    'qtb_selftest_wait_timeout', 'qtb_host_device_pointer', 'qtb_copy_c',
     'qtb_plan_set_timing', 'qtb_plan_collect_timing', 'qtb_plan_run_noalloc',
 )
 NOALLOC_SCRATCH_BYTES = 64 << 20
@@ -146,6 +146,7 @@ def _declare(lib):
         'qtb_plan_device_status': (c.c_int, [P, c.POINTER(c.c_int32)]),
         'qtb_selftest_wait_timeout': (c.c_int, [c.c_int32, c.POINTER(c.c_int32)]),
         'qtb_host_device_pointer': (c.c_int, [c.c_void_p, c.POINTER(c.c_void_p)]),
+        'qtb_copy_c': (c.c_int, [c.c_void_p, c.c_void_p, c.c_size_t, c.c_void_p]),
         'qtb_plan_set_timing': (c.c_int, [P, c.c_int32]),
         'qtb_plan_collect_timing': (c.c_int, [P, c.POINTER(c.c_double), c.POINTER(c.c_int64)]),
         'qtb_plan_run_noalloc': (c.c_int, [P, c.c_int32, c.c_int32, P, P, P, P]),

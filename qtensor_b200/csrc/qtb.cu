@@ -435,9 +435,7 @@ __device__ void build_table(const unsigned char* common, const RunArgs& a, float
         const DevEntry en = entries[lo];
         double alpha = 0.0;
         for (int t = 0; t < en.expr_count; ++t)
-            // plain loads: the angles may be a caller's pinned host buffer
-            // read through its device mapping
-            alpha += terms[en.expr_begin + t].coef * a.params[terms[en.expr_begin + t].param];
+            alpha += terms[en.expr_begin + t].coef * __ldg(a.params + terms[en.expr_begin + t].param);
         const int o = (int)(i - en.off);
         uint32_t ixb = en.sliced_value;   // sliced axes at their values
         for (int ax = 0; ax < en.rank_out; ++ax)
@@ -2734,9 +2732,30 @@ __global__ void qtb_selftest_wait_kernel(const unsigned int* counter, uint32_t l
 
 extern "C" {
 
+namespace qtb {
+// 8-byte words from src to dst, both device-accessible (device memory, or
+// pinned host memory through its device mapping).
+__global__ void qtb_copy_kernel(const unsigned long long* __restrict__ src, unsigned long long* __restrict__ dst,
+                                size_t words) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < words; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+}  // namespace qtb
+
 int qtb_host_device_pointer(void* host, void** dev) {
     if (!host || !dev) return fail(QTB_ERR_ARG, "host_device_pointer: null argument");
     QTB_CUDA(cudaHostGetDevicePointer(dev, host, 0));
+    return QTB_OK;
+}
+
+int qtb_copy_c(void* dst, const void* src, size_t bytes, void* stream) {
+    if (!dst || !src || bytes % 8 != 0) return fail(QTB_ERR_ARG, "copy: null pointer or size not a multiple of 8");
+    if (bytes == 0) return QTB_OK;
+    const size_t words = bytes / 8;
+    const unsigned blocks = (unsigned)std::min<size_t>((words + 255) / 256, 1024);
+    qtb_copy_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const unsigned long long*>(src), static_cast<unsigned long long*>(dst), words);
+    QTB_CUDA(cudaGetLastError());
     return QTB_OK;
 }
 

@@ -121,13 +121,14 @@ class CompiledGraph:
         return dev.value
 
     def _capture(self):
-        """CUDA graph of one call: gate table from the pinned angles,
-        executor classes (forked streams), energy -> pinned host.  The
-        executor reads the angles from the pinned buffer and writes the
-        energy into the pinned result buffer, both through their device
-        mappings: a graph without copy nodes (each cost several microseconds
-        of a call of about fifty).  Without a mapping, copy nodes do the
-        same."""
+        """CUDA graph of one call: pinned angles -> device, gate table,
+        executor classes (forked streams), energy -> pinned host.  The angles
+        are copied by a kernel that reads the pinned buffer through its
+        device mapping, and the energy is written by the executor straight
+        into the pinned result buffer: a graph without copy nodes (each cost
+        several microseconds of a call of about fifty).  Without a mapping,
+        copy nodes do the same."""
+        lib = _lib.lib()
         with torch.cuda.device(self.device):
             self.launch()                      # builds the run's job arrays outside capture
             torch.cuda.synchronize(self.device)
@@ -136,7 +137,9 @@ class CompiledGraph:
             with torch.cuda.graph(graph):
                 stream = torch.cuda.current_stream(self.device)
                 if h_params is not None and h_energy is not None:
-                    self.plan.run(0, self.n_networks, h_params, self.terms, h_energy,
+                    _lib.check(lib.qtb_copy_c(ctypes.c_void_p(self.params.data_ptr()), ctypes.c_void_p(h_params),
+                                              8 * self.params.numel(), ctypes.c_void_p(stream.cuda_stream)))
+                    self.plan.run(0, self.n_networks, self.params, self.terms, h_energy,
                                   self.scratch, stream.cuda_stream)
                 else:
                     self.params.copy_(self.host_params, non_blocking=True)
