@@ -600,24 +600,28 @@ __device__ float2 contract_records(const DevNetRun& net, const uint32_t* __restr
 
 // One output element from its compact record (kRecCompact): the same
 // products, in the same operand order, as compute_element.  The operand
-// fields after the first are taken from a queue shifted 16 bits per
-// operand, so an element costs its own operand count (a warp: the largest
-// of its lanes'), not the format's seven slots.
+// fields after the first come two per 32-bit word, taken a word per loop
+// step, so an element costs its own operand count (a warp: the largest of
+// its lanes'), not the format's seven slots, and the two operands of a
+// word load together.
+__device__ __forceinline__ void rec_operand(uint32_t f, const float2* __restrict__ S, float2& p0, float2& p1) {
+    const uint32_t o = f & 0xfffu;
+    p0 = cmul(p0, S[o]);
+    p1 = cmul(p1, S[o + ((1u << (f >> 12)) >> 1)]);
+}
+
 __device__ __forceinline__ void rec_element_compact(const uint4 r, float2* __restrict__ S) {
     const uint32_t h = r.x & 0xffffu, k = ((h >> 12) & 7u) + 1u;
-    uint32_t f = r.x >> 16;
-    uint32_t o = f & 0xfffu;
+    const uint32_t f = r.x >> 16;
+    const uint32_t o = f & 0xfffu;
     float2 p0 = S[o], p1 = S[o + ((1u << (f >> 12)) >> 1)];
-    uint32_t q0 = r.y, q1 = r.z, q2 = r.w;
+    uint32_t q0 = r.y, q1 = r.z, q2 = r.w;   // operands 1-2, 3-4, 5-6
 #pragma unroll 1
-    for (uint32_t t = 1; t < k; ++t) {
-        f = q0 & 0xffffu;
-        q0 = __funnelshift_r(q0, q1, 16);
-        q1 = __funnelshift_r(q1, q2, 16);
-        q2 >>= 16;
-        o = f & 0xfffu;
-        p0 = cmul(p0, S[o]);
-        p1 = cmul(p1, S[o + ((1u << (f >> 12)) >> 1)]);
+    for (uint32_t t = 1; t < k; t += 2) {
+        rec_operand(q0 & 0xffffu, S, p0, p1);
+        if (t + 1 < k) rec_operand(q0 >> 16, S, p0, p1);
+        q0 = q1;
+        q1 = q2;
     }
     S[h & 0xfffu] = (h >> 15) ? make_float2(p0.x + p1.x, p0.y + p1.y) : p0;
 }
