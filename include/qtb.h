@@ -316,6 +316,11 @@ int qtb_plan_run_plain(qtb_plan* plan, int32_t first, int32_t count, const doubl
  * runs reuse the choice.
  * QTB_AUTOTUNE=0 in the environment keeps the default block sizes.        */
 int qtb_plan_set_autotune(qtb_plan* plan, int32_t enable);
+/* Resident CTAs per SM of the plan's wide waves (0, the default: as many
+ * as fit, two).  A wave keeps its CTAs for its whole run; with 1, half of
+ * every SM stays free for other streams' kernels (a server's concurrent
+ * requests) while a wide request runs.  Set before a range's first run.  */
+int qtb_plan_set_wave_ctas_per_sm(qtb_plan* plan, int32_t ctas);
 /* Launch classes of the plan's most recent run: 4 ints per class (networks,
  * threads per CTA, dynamic shared memory bytes, flags: 1 = shared-memory
  * arena, 2 = persistent launch taking networks from a queue, 4 = a wave of

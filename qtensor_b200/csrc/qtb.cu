@@ -1760,6 +1760,7 @@ static int build_waves(qtb_plan* plan, std::vector<int32_t> wide, int32_t first,
         QTB_CUDA(cudaGetDevice(&dev));
         QTB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qtb_wide_kernel, kWideThreads, 0));
+        if (plan->wave_ctas_per_sm > 0) per_sm = std::min(per_sm, (int)plan->wave_ctas_per_sm);
     }
     // QTB_WIDE_TILES_PER_CTA (1..8, default 2) in the environment sets how
     // many tiles a step is cut into per resident CTA
@@ -2910,6 +2911,12 @@ int qtb_plan_run_noalloc(qtb_plan* plan, int32_t first, int32_t count, const dou
     else
         qtb_network_kernel<false, false, false><<<count, threads, smem_bytes, st>>>(jobs, a);
     QTB_CUDA(cudaGetLastError());
+    return QTB_OK;
+}
+
+int qtb_plan_set_wave_ctas_per_sm(qtb_plan* plan, int32_t ctas) {
+    if (!plan || ctas < 0) return fail(QTB_ERR_ARG, "plan_set_wave_ctas_per_sm: bad arguments");
+    plan->wave_ctas_per_sm = ctas;
     return QTB_OK;
 }
 

@@ -186,6 +186,11 @@ class NetworkPlan:
                                            ptr(terms_dev), ptr(energy_dev), ptr(scratch_dev),
                                            nbytes, ctypes.c_void_p(int(stream))))
 
+    def set_wave_ctas_per_sm(self, ctas):
+        """Resident CTAs per SM of the wide waves (0: as many as fit); set
+        before the first run."""
+        check(self._lib.qtb_plan_set_wave_ctas_per_sm(self._h, int(ctas)))
+
     def set_autotune(self, enable):
         """Time every launch class with 64..1024 threads per CTA on the first
         run of a range and keep the fastest."""

@@ -120,11 +120,14 @@ class QAOAServer:
     candidates they bring), fewer than the engine's 16 because a request's
     compile is on its latency path.  compile_workers: host threads compiling
     requests concurrently, each with compile_threads C++ threads (default:
-    its share of the CPUs the process may use)."""
+    its share of the CPUs the process may use).  wave_ctas_per_sm: resident
+    CTAs per SM of a wide request's whole-GPU waves (1 leaves half of every
+    SM to the other requests' kernels while a wide request runs; 0 lets
+    the waves take whole SMs)."""
 
     def __init__(self, device=None, n_streams=4, memory_budget=None, max_width=29,
                  max_slices=1024, composer='default', order_trials=4, compile_workers=2,
-                 compile_threads=0, max_request_bytes=None):
+                 compile_threads=0, max_request_bytes=None, wave_ctas_per_sm=1):
         if not torch.cuda.is_available():
             raise RuntimeError('QAOAServer needs a CUDA device; there is no CPU fallback')
         self.device = torch.device('cuda', torch.cuda.current_device() if device is None else device)
@@ -134,6 +137,7 @@ class QAOAServer:
         self.order_trials = order_trials
         # the compile workers share the CPUs the process may use
         self.compile_threads = compile_threads or max(1, _lib.available_cpus() // max(1, compile_workers))
+        self.wave_ctas_per_sm = wave_ctas_per_sm
         self.max_request_bytes = max_request_bytes
         _lib.check(_lib.lib().qtb_init(self.device.index))
         if memory_budget is None:
@@ -192,6 +196,7 @@ class QAOAServer:
             plan = NetworkPlan(2 * p)
             plan.set_order_trials(self.order_trials)
             plan.set_max_width(self.max_width, self.max_slices)
+            plan.set_wave_ctas_per_sm(self.wave_ctas_per_sm)
             plan.add_lightcones(csr, edges, p, self.cid, params, self.compile_threads)
             if self.max_request_bytes is not None:
                 work = sum(plan.info(i)['alg_bytes'] for i in range(len(plan)))
