@@ -446,18 +446,10 @@ __device__ void build_table(const unsigned char* common, const RunArgs& a, float
     __syncthreads();
 }
 
-// Thread 32 claims the CTA's next network when the current one reaches its
-// tail (phases of at most 32 elements, run by warp 0 alone): the other
-// warps are idle by then, and the queue's round trip overlaps the tail.
-__device__ __forceinline__ void claim_next(unsigned int* slot, unsigned int* queue) {
-    if (threadIdx.x == 32 && slot != nullptr) *slot = atomicAdd(queue, 1u);
-}
-
 // The phases of one staged network; its scalar result is returned to thread 0.
 template <bool kSmemTable>
 __device__ float2 contract_network(const DevNetRun& net, const unsigned char* blob,
-                                   const float2* __restrict__ table, float2* __restrict__ arena,
-                                   unsigned int* claim_slot, unsigned int* queue) {
+                                   const float2* __restrict__ table, float2* __restrict__ arena) {
     const DevPhase* phases = reinterpret_cast<const DevPhase*>(blob);
     const DevOp* ops = reinterpret_cast<const DevOp*>(blob + net.n_phases * sizeof(DevPhase));
     const DevIn* ins = reinterpret_cast<const DevIn*>(blob + net.ins_off);
@@ -483,7 +475,6 @@ __device__ float2 contract_network(const DevNetRun& net, const unsigned char* bl
         __syncthreads();
     }
     // the tail (every phase <= 32 elements): warp 0 alone, warp barriers
-    if (net.tail_start < net.n_phases) claim_next(claim_slot, queue);
     if (threadIdx.x < 32) {
         for (uint32_t p = net.tail_start; p < net.n_phases; ++p) {
             const DevPhase ph = phases[p];
@@ -563,8 +554,7 @@ __device__ __forceinline__ void rec_element(const uint32_t (&w)[kRecMaxK + 1], f
 // contract_network: phases of more than 32 elements on every thread with
 // block barriers, the tail on warp 0 with warp barriers.
 __device__ float2 contract_records(const DevNetRun& net, const uint32_t* __restrict__ rec,
-                                   float2* __restrict__ S, const float2* __restrict__ arena,
-                                   unsigned int* claim_slot, unsigned int* queue) {
+                                   float2* __restrict__ S, const float2* __restrict__ arena) {
     const uint32_t tid = threadIdx.x;
     RecHead h = rec_head(rec, 0, net.n_phases);
     RecHead h1 = rec_head(rec, 1, net.n_phases);
@@ -572,10 +562,7 @@ __device__ float2 contract_records(const DevNetRun& net, const uint32_t* __restr
     rec_load(h, tid, cur);
     for (uint32_t p = 0; p < net.n_phases; ++p) {
         const bool tail = p >= net.tail_start;
-        if (tail && tid >= 32) {
-            claim_next(claim_slot, queue);
-            break;
-        }
+        if (tail && tid >= 32) break;
         uint32_t nxt[kRecMaxK + 1];
         rec_load(h1, tid, nxt);
         const RecHead h2 = rec_head(rec, p + 2, net.n_phases);
@@ -637,8 +624,7 @@ constexpr uint32_t kRecHeadSmem = 64;
 // phase split as contract_network.
 __device__ float2 contract_records_compact(const DevNetRun& net, const uint32_t* __restrict__ rec,
                                            float2* __restrict__ S, const float2* __restrict__ arena,
-                                           uint2* __restrict__ s_head, unsigned int* claim_slot,
-                                           unsigned int* queue) {
+                                           uint2* __restrict__ s_head) {
     const uint32_t tid = threadIdx.x, np = net.n_phases;
     const uint2* ghead = reinterpret_cast<const uint2*>(rec);
     const bool staged = np <= kRecHeadSmem;
@@ -656,10 +642,7 @@ __device__ float2 contract_records_compact(const DevNetRun& net, const uint32_t*
     uint4 r0 = first(0), r1 = first(1), r2 = first(2);
     for (uint32_t p = 0; p < np; ++p) {
         const bool tail = p >= net.tail_start;
-        if (tail && tid >= 32) {
-            claim_next(claim_slot, queue);
-            break;
-        }
+        if (tail && tid >= 32) break;
         const uint4 r3 = first(p + 3);
         const uint2 h = head(p);
         const uint32_t total = h.y & 0xffffffu;
@@ -705,10 +688,7 @@ __global__ void __launch_bounds__(kLean == 2 ? 96 : kLean ? 128 : (kPersistent ?
         blob + a.blob_capacity + (kSmemTable ? ((a.table_elems * 8u + 15u) & ~15u) : 0u);
     float2* arena = kSmemArena ? reinterpret_cast<float2*>(after_table)
                                : a.gscratch + (size_t)blockIdx.x * a.arena_capacity;
-    // a persistent CTA's network: claimed at the top of an iteration, or by
-    // the previous network's tail (claim_next); two slots, read and written
-    // in alternate iterations
-    __shared__ unsigned int s_job[2], is_last;
+    __shared__ unsigned int s_job, is_last;
     __shared__ uint2 s_head[kSmemArena && kSmemTable ? kRecHeadSmem : 1];
     if (kPersistent && a.queue == nullptr) {   // a persistent launch needs its queue
         if (threadIdx.x == 0) atomicOr(a.status, kStatusQueue);
@@ -723,20 +703,15 @@ __global__ void __launch_bounds__(kLean == 2 ? 96 : kLean ? 128 : (kPersistent ?
     uint32_t parity = 0;
     const float2* __restrict__ table = kSmemTable ? stable : a.gtable;
     bool table_ready = !kSmemTable;
-    bool claimed = false;   // the current slot was filled by the previous network's tail
     for (uint32_t iter = 0;; ++iter) {
-        uint32_t cur = blockIdx.x;
         if (kPersistent) {
-            if (!claimed) {
-                if (threadIdx.x == 0) s_job[iter & 1u] = atomicAdd(a.queue, 1u);
-                __syncthreads();
-            }
-            cur = s_job[iter & 1u];
-            if (cur >= a.n_jobs) break;
+            if (threadIdx.x == 0) s_job = atomicAdd(a.queue, 1u);
+            __syncthreads();
+            if (s_job >= a.n_jobs) break;
         } else if (iter > 0) {
             break;
         }
-        const Job job = jobs[cur];
+        const Job job = jobs[kPersistent ? s_job : blockIdx.x];
         const DevNetRun net = *job.net;
         // a network with element records needs no blob (shared table and
         // arena only); otherwise blob_capacity 0: the launch reads plan
@@ -764,16 +739,11 @@ __global__ void __launch_bounds__(kLean == 2 ? 96 : kLean ? 128 : (kPersistent ?
         }
         const unsigned char* nblob =
             staged ? blob : reinterpret_cast<const unsigned char*>(a.blobs + net.blob_off16);
-        // the next network is claimed in this one's tail when it has one
-        // (uniform over the CTA: the tail is the same for every thread)
-        const bool tail_claim = kPersistent && net.tail_start < net.n_phases && blockDim.x > 32;
-        unsigned int* slot = tail_claim ? &s_job[(iter + 1u) & 1u] : nullptr;
         float2 term;
-        if (!records) term = contract_network<kSmemTable>(net, nblob, table, arena, slot, a.queue);
+        if (!records) term = contract_network<kSmemTable>(net, nblob, table, arena);
         else if (net.rec_format == kRecCompact)
-            term = contract_records_compact(net, a.recs + net.rec_off, stable, arena, s_head, slot, a.queue);
-        else term = contract_records(net, a.recs + net.rec_off, stable, arena, slot, a.queue);
-        claimed = tail_claim;
+            term = contract_records_compact(net, a.recs + net.rec_off, stable, arena, s_head);
+        else term = contract_records(net, a.recs + net.rec_off, stable, arena);
         if (threadIdx.x == 0) {
             *job.term = term;
             if (a.energy) {
