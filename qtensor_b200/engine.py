@@ -193,11 +193,13 @@ class QAOAEnergyEngine:
     records: resolve every output element's operand offsets on the host, so
     that the shared-memory executor only loads and multiplies (same
     products, same order; off: the executor decodes the plan blobs).
+    wave_ctas_per_sm: resident CTAs per SM of the wide networks' whole-GPU
+    waves (0: as many as fit).
     """
 
     def __init__(self, composer='default', ordering='native', device=None, threads=0,
                  cache_size=16, order_trials=16, autotune=True, max_width=29,
-                 max_slices=1024, slicing='greedy', records=True):
+                 max_slices=1024, slicing='greedy', records=True, wave_ctas_per_sm=0):
         _require_cuda()
         if ordering not in ('native', 'reference'):
             raise ValueError('ordering must be "native" or "reference"')
@@ -213,6 +215,7 @@ class QAOAEnergyEngine:
         self.max_slices = max_slices
         self.slicing = slicing
         self.records = records
+        self.wave_ctas_per_sm = wave_ctas_per_sm
         self._cache = {}
         self._by_id = {}        # id(G) -> (weakref, nodes, p, key, edge count)
         self._edge_digests = {}  # id(edge subset) -> (subset, tuple, digest, length)
@@ -247,6 +250,7 @@ class QAOAEnergyEngine:
         plan.set_max_width(self.max_width, self.max_slices)
         plan.set_slicing(self.slicing)
         plan.set_records(self.records)
+        plan.set_wave_ctas_per_sm(self.wave_ctas_per_sm)
         if self.ordering == 'native':
             csr = graph_csr(G)
             index = {v: i for i, v in enumerate(csr[0])}
