@@ -377,9 +377,12 @@ def run_serving(n_requests, rate, device_index, plain_budget_s=20.0):
         stream, wall_stream = poisson(srv)
     # the same arrivals through a plain FIFO queue: one compile worker, one
     # request on the GPU at a time
-    with QAOAServer(device=device_index, n_streams=1, compile_workers=1, max_request_bytes=budget) as srv:
+    # one request at a time on the GPU: its wide waves may take whole SMs
+    with QAOAServer(device=device_index, n_streams=1, compile_workers=1, max_request_bytes=budget,
+                    wave_ctas_per_sm=0) as srv:
         fifo, wall_fifo = poisson(srv)
-    with QAOAServer(device=device_index, n_streams=1, compile_workers=1, max_request_bytes=budget) as srv:
+    with QAOAServer(device=device_index, n_streams=1, compile_workers=1, max_request_bytes=budget,
+                    wave_ctas_per_sm=0) as srv:
         t0 = time.perf_counter()
         alone = []
         for r in reqs:
