@@ -639,21 +639,29 @@ __device__ float2 contract_records_compact(const DevNetRun& net, const uint32_t*
         return tid < (h.y & 0xffffffu) ? __ldg(reinterpret_cast<const uint4*>(rec + h.x) + tid)
                                        : make_uint4(0u, 0u, 0u, 0u);
     };
-    uint4 r0 = first(0), r1 = first(1), r2 = first(2);
-    for (uint32_t p = 0; p < np; ++p) {
-        const bool tail = p >= net.tail_start;
-        if (tail && tid >= 32) break;
-        const uint4 r3 = first(p + 3);
-        const uint2 h = head(p);
+    // phase q contracts from `cur` and loads phase q + 3's record into
+    // `ahead`; four register slots rotate through an unrolled loop, so no
+    // record is moved between registers
+    auto phase = [&](uint32_t q, const uint4& cur, uint4& ahead) -> bool {
+        if (q >= np) return false;
+        const bool tail = q >= net.tail_start;
+        if (tail && tid >= 32) return false;
+        ahead = first(q + 3);
+        const uint2 h = head(q);
         const uint32_t total = h.y & 0xffffffu;
-        if (tid < total) rec_element_compact(r0, S);
+        if (tid < total) rec_element_compact(cur, S);
         for (uint32_t g = tid + blockDim.x; g < total; g += blockDim.x)
             rec_element_compact(__ldg(reinterpret_cast<const uint4*>(rec + h.x) + g), S);
         if (tail) __syncwarp();
         else __syncthreads();
-        r0 = r1;
-        r1 = r2;
-        r2 = r3;
+        return true;
+    };
+    uint4 ra = first(0), rb = first(1), rc = first(2), rd;
+    for (uint32_t p = 0;; p += 4) {
+        if (!phase(p, ra, rd)) break;
+        if (!phase(p + 1, rb, ra)) break;
+        if (!phase(p + 2, rc, rb)) break;
+        if (!phase(p + 3, rd, rc)) break;
     }
     float2 result = make_float2(0.f, 0.f);
     if (tid == 0)
