@@ -634,29 +634,35 @@ __device__ float2 contract_records_compact(const DevNetRun& net, const uint32_t*
     auto head = [&](uint32_t p) {
         return p >= np ? make_uint2(0u, 0u) : staged ? s_head[p] : __ldg(ghead + p);
     };
-    auto first = [&](uint32_t p) {
-        const uint2 h = head(p);
-        return tid < (h.y & 0xffffffu) ? __ldg(reinterpret_cast<const uint4*>(rec + h.x) + tid)
-                                       : make_uint4(0u, 0u, 0u, 0u);
+    // a phase's header and this thread's record of its first element
+    struct Ahead {
+        uint2 h;
+        uint4 r;
     };
-    // phase q contracts from `cur` and loads phase q + 3's record into
-    // `ahead`; four register slots rotate through an unrolled loop, so no
-    // record is moved between registers
-    auto phase = [&](uint32_t q, const uint4& cur, uint4& ahead) -> bool {
+    auto first = [&](uint32_t p) {
+        Ahead a;
+        a.h = head(p);
+        a.r = tid < (a.h.y & 0xffffffu) ? __ldg(reinterpret_cast<const uint4*>(rec + a.h.x) + tid)
+                                         : make_uint4(0u, 0u, 0u, 0u);
+        return a;
+    };
+    // phase q contracts from `cur` and loads phase q + 3's header and record
+    // into `ahead`; four register slots rotate through an unrolled loop, so
+    // nothing is moved between registers
+    auto phase = [&](uint32_t q, const Ahead& cur, Ahead& ahead) -> bool {
         if (q >= np) return false;
         const bool tail = q >= net.tail_start;
         if (tail && tid >= 32) return false;
         ahead = first(q + 3);
-        const uint2 h = head(q);
-        const uint32_t total = h.y & 0xffffffu;
-        if (tid < total) rec_element_compact(cur, S);
+        const uint32_t total = cur.h.y & 0xffffffu;
+        if (tid < total) rec_element_compact(cur.r, S);
         for (uint32_t g = tid + blockDim.x; g < total; g += blockDim.x)
-            rec_element_compact(__ldg(reinterpret_cast<const uint4*>(rec + h.x) + g), S);
+            rec_element_compact(__ldg(reinterpret_cast<const uint4*>(rec + cur.h.x) + g), S);
         if (tail) __syncwarp();
         else __syncthreads();
         return true;
     };
-    uint4 ra = first(0), rb = first(1), rc = first(2), rd;
+    Ahead ra = first(0), rb = first(1), rc = first(2), rd;
     for (uint32_t p = 0;; p += 4) {
         if (!phase(p, ra, rd)) break;
         if (!phase(p + 1, rb, ra)) break;
