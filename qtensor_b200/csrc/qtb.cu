@@ -948,7 +948,6 @@ constexpr uint32_t kWideBatchBits = (kWideBatch - 1u) << 8;          // the bits
 constexpr uint32_t kWideGroup = 1;                                  // operands per batch of loads
 constexpr uint32_t kWideMinTile = kWideBatch * kWideThreads;         // 2048
 constexpr uint32_t kWideMaxTile = 8 * kWideMinTile;
-constexpr uint64_t kWideTailElems = 32768;   // steps this small go to the per-network tail
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
     unsigned int v;
@@ -1161,35 +1160,6 @@ __device__ __forceinline__ bool wide_locate(const WideArgs& w, const RunArgs& a,
     return true;
 }
 
-// A tail tile: one network's phases from `first` to its last, by one CTA,
-// phases separated by CTA barriers (the arena is read through L2 with
-// ld.cg, so the CTA's own writes of a phase are seen after the barrier).
-__device__ __noinline__ void wide_tail(const WideArgs& w, const RunArgs& a, const WideStep& st, uint32_t first,
-                                       uint32_t idx) {
-    const WideSeg sg = w.segs[st.seg_begin + idx];
-    const WideNet wn = w.nets[sg.net];
-    const DevNetRun net = *wn.run;
-    const unsigned char* blob = reinterpret_cast<const unsigned char*>(a.blobs + net.blob_off16);
-    const DevOp* ops = reinterpret_cast<const DevOp*>(blob + net.n_phases * sizeof(DevPhase));
-    const DevIn* ins = reinterpret_cast<const DevIn*>(blob + net.ins_off);
-    float2* arena = w.arenas + wn.arena_off;
-    for (uint32_t p = first; p < net.n_phases; ++p) {
-        const uint4 pv = __ldg(reinterpret_cast<const uint4*>(blob) + p);   // DevPhase
-        const uint32_t op_first = pv.x, op_last = pv.x + pv.y - 1u, total = pv.z;
-        uint32_t op_lo = 1u, op_hi = 0u;
-        DevOp op{};
-        for (uint32_t g = threadIdx.x; g < total; g += blockDim.x) {
-            if (g < op_lo || g >= op_hi) {
-                op = ldg_op(ops + search_op<true>(ops, op_first, op_last, g));
-                op_lo = op.elem_begin;
-                op_hi = op.elem_begin + (1u << (op.u - op.sum));
-            }
-            compute_element_wide(op, g - op.elem_begin, ins, a.gtable, arena);
-        }
-        __syncthreads();
-    }
-}
-
 // Tiles are claimed in order from one counter; a CTA claims its next tile
 // as soon as it starts waiting on the current one, and every thread
 // locates its first element of the tile (segment, network, phase, op,
@@ -1224,7 +1194,7 @@ __global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArg
             e0 = (t - st.tile_begin) * st.tile_elems;
             e1 = min(e0 + st.tile_elems, st.total_elems);
             const uint32_t g0 = e0 + threadIdx.x;
-            if (st.tile_elems && g0 < e1 && wide_locate(w, a, st, s, g0, pl)) prefetch_l1(pl.ins + pl.op.in_begin);
+            if (g0 < e1 && wide_locate(w, a, st, s, g0, pl)) prefetch_l1(pl.ins + pl.op.in_begin);
         }
         __syncthreads();   // every thread has read s_tile
         if (threadIdx.x == 0) {
@@ -1263,28 +1233,24 @@ __global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArg
             }
             break;
         }
-        if (st.tile_elems == 0) {
-            wide_tail(w, a, st, s, t - st.tile_begin);
-        } else {
-            const uint32_t bd = blockDim.x;
-            for (uint32_t g = e0 + threadIdx.x; g < e1;) {
-                if (!wide_locate(w, a, st, s, g, pl)) {   // padding between segments
-                    g += bd;
-                    continue;
-                }
-                // kWideBatch elements of the same op that differ only in the bits
-                // from bit 8 up of the op index (the common case in wide phases:
-                // tiles, segments and ops start at multiples of kWideMinTile)
-                const uint32_t l = g - pl.seg_lo;
-                const uint32_t j = l - pl.op.elem_begin;
-                if (bd == 256u && (j & kWideBatchBits) == 0u && g + (kWideBatch - 1) * bd < min(e1, pl.seg_hi) &&
-                    l + (kWideBatch - 1) * bd < pl.op_hi) {
-                    compute_elements_wide(pl.op, j, pl.ins, a.gtable, pl.arena);
-                    g += kWideBatch * bd;
-                } else {
-                    compute_element_wide(pl.op, j, pl.ins, a.gtable, pl.arena);
-                    g += bd;
-                }
+        const uint32_t bd = blockDim.x;
+        for (uint32_t g = e0 + threadIdx.x; g < e1;) {
+            if (!wide_locate(w, a, st, s, g, pl)) {   // padding between segments
+                g += bd;
+                continue;
+            }
+            // kWideBatch elements of the same op that differ only in the bits
+            // from bit 8 up of the op index (the common case in wide phases:
+            // tiles, segments and ops start at multiples of kWideMinTile)
+            const uint32_t l = g - pl.seg_lo;
+            const uint32_t j = l - pl.op.elem_begin;
+            if (bd == 256u && (j & kWideBatchBits) == 0u && g + (kWideBatch - 1) * bd < min(e1, pl.seg_hi) &&
+                l + (kWideBatch - 1) * bd < pl.op_hi) {
+                compute_elements_wide(pl.op, j, pl.ins, a.gtable, pl.arena);
+                g += kWideBatch * bd;
+            } else {
+                compute_element_wide(pl.op, j, pl.ins, a.gtable, pl.arena);
+                g += bd;
             }
         }
         __syncthreads();
@@ -1787,10 +1753,6 @@ static int build_waves(qtb_plan* plan, std::vector<int32_t> wide, int32_t first,
         const int v = std::atoi(env);
         if (v >= 1 && v <= 8) tiles_per_cta = v;
     }
-    // QTB_WIDE_TAIL_ELEMS sets the largest step (elements over the wave)
-    // that the tail takes over (0: no tail)
-    uint64_t tail_elems = kWideTailElems;
-    if (const char* env = std::getenv("QTB_WIDE_TAIL_ELEMS")) tail_elems = std::strtoull(env, nullptr, 10);
     std::vector<WideNet> nets;
     std::vector<WideStep> steps;
     std::vector<WideSeg> segs;
@@ -1822,22 +1784,8 @@ static int build_waves(qtb_plan* plan, std::vector<int32_t> wide, int32_t first,
             max_phases = std::max(max_phases, plan->druns[i].n_phases);
         }
         rc->scratch_elems = std::max(rc->scratch_elems, off);
-        // the tail: from the first phase after which every step is small,
-        // one CTA per network finishes the network's remaining phases with
-        // CTA barriers (a step of its own whose tiles are whole networks),
-        // instead of one grid-wide step per phase
-        uint32_t tail = max_phases;
-        while (tail > 0) {
-            uint64_t total = 0;
-            for (size_t k = pos; k < end; ++k) {
-                const Network& n = plan->nets[wide[k]];
-                if (tail - 1 < n.phases.size()) total += n.phases[tail - 1].total_elems;
-            }
-            if (total > tail_elems) break;
-            --tail;
-        }
         uint32_t tiles = 0;
-        for (uint32_t ph = 0; ph < tail; ++ph) {
+        for (uint32_t ph = 0; ph < max_phases; ++ph) {
             WideStep st{};
             st.seg_begin = (uint32_t)(segs.size() - rg.seg0);
             uint32_t total = 0;
@@ -1862,18 +1810,7 @@ static int build_waves(qtb_plan* plan, std::vector<int32_t> wide, int32_t first,
             tiles += st.n_tiles;
             steps.push_back(st);
         }
-        if (tail < max_phases) {
-            WideStep st{};   // tile_elems 0: one tile per network, its phases from `tail` on
-            st.seg_begin = (uint32_t)(segs.size() - rg.seg0);
-            for (size_t k = pos; k < end; ++k)
-                if (tail < plan->nets[wide[k]].phases.size()) segs.push_back(WideSeg{(uint32_t)(k - pos), 0u});
-            st.n_segs = (uint32_t)(segs.size() - rg.seg0) - st.seg_begin;
-            st.tile_begin = tiles;
-            st.n_tiles = st.n_segs;
-            tiles += st.n_tiles;
-            steps.push_back(st);
-        }
-        wv.n_steps = tail < max_phases ? tail + 1 : max_phases;
+        wv.n_steps = max_phases;
         wv.n_tiles = tiles;
         wv.grid = std::max(1, std::min<int>((int)tiles + 1, std::max(1, per_sm) * sms));
         rc->waves.push_back(wv);
