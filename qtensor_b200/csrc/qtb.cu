@@ -1101,79 +1101,12 @@ __device__ __forceinline__ void compute_elements_wide(const DevOp& op, uint32_t 
         arena[op.dst + j + e * 256u] = op.sum ? make_float2(p0[e].x + p1[e].x, p0[e].y + p1[e].y) : p0[e];
 }
 
-__device__ __forceinline__ void prefetch_l1(const void* p) {
-    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
-}
-
-// Per-thread place in a step: the segment (network) and the op of the
-// element last located, cached across the elements a thread takes.
-struct WidePlace {
-    uint32_t seg_lo = 1u, seg_hi = 0u, op_lo = 1u, op_hi = 0u, ph_total = 0u;
-    uint32_t op_first = 0u, op_last = 0u;
-    const DevIn* ins = nullptr;
-    const DevOp* ops = nullptr;
-    const uint16_t* chunk = nullptr;
-    float2* arena = nullptr;
-    DevOp op{};
-};
-
-// Locates element g of step s (plan data only: nothing another tile
-// writes).  Returns false for padding between segments.
-__device__ __forceinline__ bool wide_locate(const WideArgs& w, const RunArgs& a, const WideStep& st, uint32_t s,
-                                            uint32_t g, WidePlace& pl) {
-    if (g < pl.seg_lo || g >= pl.seg_hi) {
-        uint32_t lo = st.seg_begin, hi = st.seg_begin + st.n_segs - 1u;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi + 1u) >> 1;
-            if (__ldg(&w.segs[mid].elem_begin) <= g) lo = mid;
-            else hi = mid - 1u;
-        }
-        const WideSeg sg = w.segs[lo];
-        pl.seg_lo = sg.elem_begin;
-        pl.seg_hi = lo + 1u < st.seg_begin + st.n_segs ? __ldg(&w.segs[lo + 1u].elem_begin) : st.total_elems;
-        const WideNet wn = w.nets[sg.net];
-        const DevNetRun net = *wn.run;
-        const unsigned char* blob = reinterpret_cast<const unsigned char*>(a.blobs + net.blob_off16);
-        const DevPhase ph = reinterpret_cast<const DevPhase*>(blob)[s];
-        pl.ph_total = ph.total_elems;
-        pl.ops = reinterpret_cast<const DevOp*>(blob + net.n_phases * sizeof(DevPhase));
-        pl.ins = reinterpret_cast<const DevIn*>(blob + net.ins_off);
-        pl.chunk = ph.chunk_off ? reinterpret_cast<const uint16_t*>(blob + ph.chunk_off) : nullptr;
-        pl.arena = w.arenas + wn.arena_off;
-        pl.op_first = ph.op_first;
-        pl.op_last = ph.op_first + ph.op_count - 1u;
-        pl.op_lo = 1u;
-        pl.op_hi = 0u;
-    }
-    const uint32_t l = g - pl.seg_lo;
-    if (l >= pl.ph_total) return false;
-    if (l < pl.op_lo || l >= pl.op_hi) {
-        const uint32_t oi =
-            pl.chunk ? __ldg(pl.chunk + l / kChunkElems) : search_op<true>(pl.ops, pl.op_first, pl.op_last, l);
-        pl.op = ldg_op(pl.ops + oi);
-        const DevOp* ops = pl.ops;
-        const uint32_t last = pl.op_last;
-        find_op(l, oi, pl.op, [&](uint32_t i) { return ldg_op(ops + min(i, last)); });
-        pl.op_lo = pl.op.elem_begin;
-        pl.op_hi = pl.op.elem_begin + (1u << (pl.op.u - pl.op.sum));
-    }
-    return true;
-}
-
-// Tiles are claimed in order from one counter; a CTA claims its next tile
-// as soon as it starts waiting on the current one, and every thread
-// locates its first element of the tile (segment, network, phase, op,
-// operand descriptors: plan data, which no tile writes) before the wait on
-// the previous step, so that a step's tiles start with their loads of the
-// previous step's results instead of a chain of dependent lookups.  A
-// claimed tile is processed after the CTA's current one, and a tile waits
-// only on tiles claimed before it, so the scheme still cannot deadlock.
 __global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArgs w, const RunArgs a) {
     __shared__ uint32_t s_tile;
     __shared__ int s_ok, s_last;
-    if (threadIdx.x == 0) s_tile = atomicAdd(w.counters, 1u);
     for (;;) {
-        __syncthreads();   // s_tile holds this CTA's next tile
+        if (threadIdx.x == 0) s_tile = atomicAdd(w.counters, 1u);
+        __syncthreads();
         const uint32_t t = s_tile;
         if (t > w.n_tiles) break;
         uint32_t s = w.n_steps;   // the result tile follows the last step
@@ -1186,19 +1119,7 @@ __global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArg
             }
             s = lo;
         }
-        WideStep st{};
-        uint32_t e0 = 0, e1 = 0;
-        WidePlace pl;
-        if (t < w.n_tiles) {
-            st = w.steps[s];
-            e0 = (t - st.tile_begin) * st.tile_elems;
-            e1 = min(e0 + st.tile_elems, st.total_elems);
-            const uint32_t g0 = e0 + threadIdx.x;
-            if (g0 < e1 && wide_locate(w, a, st, s, g0, pl)) prefetch_l1(pl.ins + pl.op.in_begin);
-        }
-        __syncthreads();   // every thread has read s_tile
         if (threadIdx.x == 0) {
-            if (t < w.n_tiles) s_tile = atomicAdd(w.counters, 1u);
             s_ok = 1;
             if (s > 0 && !wait_counter(w.counters + s, __ldg(&w.steps[s - 1].n_tiles), kWideSpinLimit,
                                        a.status, kStatusWideTimeout))
@@ -1233,23 +1154,66 @@ __global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArg
             }
             break;
         }
+        const WideStep st = w.steps[s];
+        const uint32_t e0 = (t - st.tile_begin) * st.tile_elems;
+        const uint32_t e1 = min(e0 + st.tile_elems, st.total_elems);
+        // per-thread cache of the current segment and op
+        uint32_t seg_lo = 1u, seg_hi = 0u, op_lo = 1u, op_hi = 0u, ph_total = 0u;
+        const unsigned char* blob = nullptr;
+        const DevIn* ins = nullptr;
+        const DevOp* ops = nullptr;
+        const uint16_t* chunk = nullptr;
+        float2* arena = nullptr;
+        DevOp op{};
+        uint32_t op_first = 0, op_last = 0;
         const uint32_t bd = blockDim.x;
         for (uint32_t g = e0 + threadIdx.x; g < e1;) {
-            if (!wide_locate(w, a, st, s, g, pl)) {   // padding between segments
+            if (g < seg_lo || g >= seg_hi) {
+                uint32_t lo = st.seg_begin, hi = st.seg_begin + st.n_segs - 1u;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi + 1u) >> 1;
+                    if (__ldg(&w.segs[mid].elem_begin) <= g) lo = mid;
+                    else hi = mid - 1u;
+                }
+                const WideSeg sg = w.segs[lo];
+                seg_lo = sg.elem_begin;
+                seg_hi = lo + 1u < st.seg_begin + st.n_segs ? __ldg(&w.segs[lo + 1u].elem_begin) : st.total_elems;
+                const WideNet wn = w.nets[sg.net];
+                const DevNetRun net = *wn.run;
+                blob = reinterpret_cast<const unsigned char*>(a.blobs + net.blob_off16);
+                const DevPhase ph = reinterpret_cast<const DevPhase*>(blob)[s];
+                ph_total = ph.total_elems;
+                ops = reinterpret_cast<const DevOp*>(blob + net.n_phases * sizeof(DevPhase));
+                ins = reinterpret_cast<const DevIn*>(blob + net.ins_off);
+                chunk = ph.chunk_off ? reinterpret_cast<const uint16_t*>(blob + ph.chunk_off) : nullptr;
+                arena = w.arenas + wn.arena_off;
+                op_first = ph.op_first;
+                op_last = ph.op_first + ph.op_count - 1u;
+                op_lo = 1u;
+                op_hi = 0u;
+            }
+            const uint32_t l = g - seg_lo;
+            if (l >= ph_total) {   // padding between segments
                 g += bd;
                 continue;
+            }
+            if (l < op_lo || l >= op_hi) {
+                const uint32_t oi = chunk ? __ldg(chunk + l / kChunkElems) : search_op<true>(ops, op_first, op_last, l);
+                op = ldg_op(ops + oi);
+                find_op(l, oi, op, [&](uint32_t i) { return ldg_op(ops + min(i, op_last)); });
+                op_lo = op.elem_begin;
+                op_hi = op.elem_begin + (1u << (op.u - op.sum));
             }
             // kWideBatch elements of the same op that differ only in the bits
             // from bit 8 up of the op index (the common case in wide phases:
             // tiles, segments and ops start at multiples of kWideMinTile)
-            const uint32_t l = g - pl.seg_lo;
-            const uint32_t j = l - pl.op.elem_begin;
-            if (bd == 256u && (j & kWideBatchBits) == 0u && g + (kWideBatch - 1) * bd < min(e1, pl.seg_hi) &&
-                l + (kWideBatch - 1) * bd < pl.op_hi) {
-                compute_elements_wide(pl.op, j, pl.ins, a.gtable, pl.arena);
+            const uint32_t j = l - op.elem_begin;
+            if (bd == 256u && (j & kWideBatchBits) == 0u && g + (kWideBatch - 1) * bd < min(e1, seg_hi) &&
+                l + (kWideBatch - 1) * bd < op_hi) {
+                compute_elements_wide(op, j, ins, a.gtable, arena);
                 g += kWideBatch * bd;
             } else {
-                compute_element_wide(pl.op, j, pl.ins, a.gtable, pl.arena);
+                compute_element_wide(op, j, ins, a.gtable, arena);
                 g += bd;
             }
         }
