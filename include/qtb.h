@@ -311,10 +311,14 @@ int qtb_plan_run_plain(qtb_plan* plan, int32_t first, int32_t count, const doubl
  * of a network range (outside stream capture) times every launch class of
  * the class schedule (one CTA per network, networks grouped by shared
  * memory, classes concurrent) with 64..1024 threads per CTA, then the whole
- * class schedule against the persistent schedule (CTAs resident on every
- * SM take networks widest-first from a queue), and keeps the faster; later
- * runs reuse the choice.
- * QTB_AUTOTUNE=0 in the environment keeps the default block sizes.        */
+ * class schedule against the persistent, hybrid (large networks as
+ * classes + a lean persistent queue) and warp-per-network schedules, and
+ * keeps the fastest; with wide networks it then times the wave kernel with
+ * 8 and with 4 elements per thread in flight and keeps the faster; later
+ * runs reuse the choices.
+ * QTB_AUTOTUNE=0 in the environment keeps the default block sizes;
+ * QTB_SCHEDULE and QTB_WIDE_BATCH (2 or 3) fix the schedule and the wave
+ * variant.                                                               */
 int qtb_plan_set_autotune(qtb_plan* plan, int32_t enable);
 /* Resident CTAs per SM of the plan's wide waves (0, the default: as many
  * as fit, two).  A wave keeps its CTAs for its whole run; with 1, half of

@@ -942,9 +942,12 @@ static_assert(sizeof(WideNet) == 32, "WideNet layout");
 static_assert(sizeof(WideStep) == 32, "WideStep layout");
 constexpr uint32_t kWideSpinLimit = 1u << 23;   // about 1 s of polling
 constexpr int kWideThreads = 256;
-constexpr uint32_t kWideBatchLog = 3;                               // log2 of the elements per thread in flight
+// log2 of the elements a thread has in flight: the wave kernel comes in
+// two variants, 8 (3) and 4 (2) elements, chosen per plan by the autotuner
+// (the smaller batch needs fewer registers and won on N=256 p=4, the larger
+// on Erdos-Renyi N=400 p=3)
+constexpr uint32_t kWideBatchLog = 3;
 constexpr uint32_t kWideBatch = 1u << kWideBatchLog;
-constexpr uint32_t kWideBatchBits = (kWideBatch - 1u) << 8;          // the bits of j above the thread index
 constexpr uint32_t kWideGroup = 1;                                  // operands per batch of loads
 constexpr uint32_t kWideMinTile = kWideBatch * kWideThreads;         // 2048
 constexpr uint32_t kWideMaxTile = 8 * kWideMinTile;
@@ -1033,27 +1036,29 @@ __device__ __forceinline__ void compute_element_wide(const DevOp& op, uint32_t j
     arena[op.dst + j] = op.sum ? make_float2(p0.x + p1.x, p0.y + p1.y) : p0;
 }
 
-// kWideBatch elements j + 256 e of one op at once, with the kWideBatchLog
+// 2^kBatchLog elements j + 256 e of one op at once, with the kBatchLog
 // bits of j from bit 8 up zero: they differ from j only in those bits, so
 // each operand offset is the gathered offset of j plus the gathered offsets
-// of those bits (one full gather per operand, not kWideBatch), and the
+// of those bits (one full gather per operand, not one per element), and the
 // loads of kWideGroup operands for all elements are issued together
-// (2 kWideBatch L2 requests in flight per thread and operand).
+// (2^(kBatchLog + 1) L2 requests in flight per thread and operand).
+template <uint32_t kBatchLog>
 __device__ __forceinline__ void compute_elements_wide(const DevOp& op, uint32_t j, const DevIn* ins,
                                                        const float2* __restrict__ table,
                                                        float2* __restrict__ arena) {
+    constexpr uint32_t kB = 1u << kBatchLog;
     const uint32_t w = op.u - op.sum;
     const uint32_t low = (1u << w) - 1u;
     const DevIn* in = ins + op.in_begin;
-    float2 p0[kWideBatch], p1[kWideBatch];
+    float2 p0[kB], p1[kB];
 #pragma unroll
-    for (uint32_t e = 0; e < kWideBatch; ++e) p0[e] = p1[e] = make_float2(1.f, 0.f);
+    for (uint32_t e = 0; e < kB; ++e) p0[e] = p1[e] = make_float2(1.f, 0.f);
     for (uint32_t t0 = 0; t0 < op.k; t0 += kWideGroup) {
         DevIn d[kWideGroup];
 #pragma unroll
         for (int t = 0; t < kWideGroup; ++t)
             if (t0 + t < op.k) d[t] = ldg_in(in + t0 + t);
-        float2 x0[kWideGroup][kWideBatch], x1[kWideGroup][kWideBatch];
+        float2 x0[kWideGroup][kB], x1[kWideGroup][kB];
 #pragma unroll
         for (int t = 0; t < kWideGroup; ++t) {
             if (t0 + t < op.k) {
@@ -1063,22 +1068,22 @@ __device__ __forceinline__ void compute_elements_wide(const DevOp& op, uint32_t 
                 const uint32_t stride_s = has_sum ? 1u << (__popc(d[t].mask) - 1) : 0u;
                 const uint32_t m = d[t].mask & low;
                 // bit 8 + i of j lands at operand bit popc(m below it) when m has it
-                uint32_t bit_off[kWideBatchLog];
+                uint32_t bit_off[kBatchLog];
 #pragma unroll
-                for (uint32_t i = 0; i < kWideBatchLog; ++i)
+                for (uint32_t i = 0; i < kBatchLog; ++i)
                     bit_off[i] = ((m >> (8 + i)) & 1u) << __popc(m & ((1u << (8 + i)) - 1u));
-                uint32_t off[kWideBatch];
+                uint32_t off[kB];
                 off[0] = gather_bits(j, d[t], low);
 #pragma unroll
-                for (uint32_t e = 1; e < kWideBatch; ++e) {
+                for (uint32_t e = 1; e < kB; ++e) {
                     uint32_t o = off[0];
 #pragma unroll
-                    for (uint32_t i = 0; i < kWideBatchLog; ++i)
+                    for (uint32_t i = 0; i < kBatchLog; ++i)
                         if ((e >> i) & 1u) o += bit_off[i];
                     off[e] = o;
                 }
 #pragma unroll
-                for (uint32_t e = 0; e < kWideBatch; ++e) {
+                for (uint32_t e = 0; e < kB; ++e) {
                     x0[t][e] = tab ? __ldg(base + off[e]) : __ldcg(base + off[e]);
                     x1[t][e] = has_sum ? (tab ? __ldg(base + off[e] + stride_s) : __ldcg(base + off[e] + stride_s))
                                        : x0[t][e];
@@ -1089,7 +1094,7 @@ __device__ __forceinline__ void compute_elements_wide(const DevOp& op, uint32_t 
         for (int t = 0; t < kWideGroup; ++t) {
             if (t0 + t < op.k) {
 #pragma unroll
-                for (uint32_t e = 0; e < kWideBatch; ++e) {
+                for (uint32_t e = 0; e < kB; ++e) {
                     p0[e] = cmul(p0[e], x0[t][e]);
                     p1[e] = cmul(p1[e], x1[t][e]);
                 }
@@ -1097,11 +1102,14 @@ __device__ __forceinline__ void compute_elements_wide(const DevOp& op, uint32_t 
         }
     }
 #pragma unroll
-    for (uint32_t e = 0; e < kWideBatch; ++e)
+    for (uint32_t e = 0; e < kB; ++e)
         arena[op.dst + j + e * 256u] = op.sum ? make_float2(p0[e].x + p1[e].x, p0[e].y + p1[e].y) : p0[e];
 }
 
+template <uint32_t kBatchLog>
 __global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArgs w, const RunArgs a) {
+    constexpr uint32_t kB = 1u << kBatchLog;
+    constexpr uint32_t kBatchBits = (kB - 1u) << 8;   // the bits of j above the thread index
     __shared__ uint32_t s_tile;
     __shared__ int s_ok, s_last;
     for (;;) {
@@ -1204,14 +1212,14 @@ __global__ void __launch_bounds__(kWideThreads, 2) qtb_wide_kernel(const WideArg
                 op_lo = op.elem_begin;
                 op_hi = op.elem_begin + (1u << (op.u - op.sum));
             }
-            // kWideBatch elements of the same op that differ only in the bits
+            // 2^kBatchLog elements of the same op that differ only in the bits
             // from bit 8 up of the op index (the common case in wide phases:
             // tiles, segments and ops start at multiples of kWideMinTile)
             const uint32_t j = l - op.elem_begin;
-            if (bd == 256u && (j & kWideBatchBits) == 0u && g + (kWideBatch - 1) * bd < min(e1, seg_hi) &&
-                l + (kWideBatch - 1) * bd < op_hi) {
-                compute_elements_wide(op, j, ins, a.gtable, arena);
-                g += kWideBatch * bd;
+            if (bd == 256u && (j & kBatchBits) == 0u && g + (kB - 1) * bd < min(e1, seg_hi) &&
+                l + (kB - 1) * bd < op_hi) {
+                compute_elements_wide<kBatchLog>(op, j, ins, a.gtable, arena);
+                g += kB * bd;
             } else {
                 compute_element_wide(op, j, ins, a.gtable, arena);
                 g += bd;
@@ -1273,7 +1281,7 @@ __global__ void __launch_bounds__(kClusterThreads) qtb_cluster_kernel(const Clus
             const uint32_t size = 1u << (op.u - op.sum);
             if (size >= kClusterChunk && base + kClusterChunk <= total) {
                 // the whole chunk lies in this op (ops start at multiples of their size)
-                compute_elements_wide(op, base + t - op.elem_begin, ins, a.gtable, arena);
+                compute_elements_wide<kWideBatchLog>(op, base + t - op.elem_begin, ins, a.gtable, arena);
             } else {
                 uint32_t op_hi = op.elem_begin + size;
 #pragma unroll 1
@@ -1391,6 +1399,7 @@ struct RunCache {
     std::vector<LaunchClass> h12classes;  // the same with the 96-thread lean queue (12 CTAs per SM)
     std::vector<LaunchClass> wclasses;  // warp schedule: large networks as classes + warp queue
     std::vector<WideWave> waves;        // wide networks (both schedules), run one after another
+    int wide_batch_log = kWideBatchLog; // wave kernel variant: 2^this elements per thread in flight
     void* wide_buf = nullptr;
     size_t counters_bytes = 0;          // counters of all waves, zeroed before a run
     size_t scratch_elems = 0;           // arenas of the largest wave, then the cluster arenas
@@ -1707,7 +1716,8 @@ static int build_waves(qtb_plan* plan, std::vector<int32_t> wide, int32_t first,
     if (device) {
         QTB_CUDA(cudaGetDevice(&dev));
         QTB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qtb_wide_kernel, kWideThreads, 0));
+        QTB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qtb_wide_kernel<kWideBatchLog>,
+                                                               kWideThreads, 0));
         if (plan->wave_ctas_per_sm > 0) per_sm = std::min(per_sm, (int)plan->wave_ctas_per_sm);
     }
     // QTB_WIDE_TILES_PER_CTA (1..8, default 2) in the environment sets how
@@ -1998,6 +2008,12 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
     if (const char* env = std::getenv("QTB_CLUSTER_MAX_ELEMS")) cl_max = std::strtoull(env, nullptr, 10);
     for (int32_t i : members[kSmemClasses])
         (plan->druns[i].arena_elems <= cl_max ? cl_nets : wave_nets).push_back(i);
+    // QTB_WIDE_BATCH=2 or 3 in the environment fixes the wave kernel variant
+    // (2^this elements per thread in flight) instead of the autotuner
+    if (const char* env = std::getenv("QTB_WIDE_BATCH")) {
+        const int v = std::atoi(env);
+        if (v == 2 || v == 3) rc->wide_batch_log = v;
+    }
     // QTB_CLUSTER_CTAS (2, 4, 8 or 16) sets the CTAs per cluster
     rc->cl_ctas = kClusterCtas;
     if (const char* env = std::getenv("QTB_CLUSTER_CTAS")) {
@@ -2204,7 +2220,8 @@ static int launch_waves(const RunCache* rc, const RunArgs& base, void* scratch_d
         w.n_nets = wv.n_nets;
         w.n_steps = wv.n_steps;
         w.n_tiles = wv.n_tiles;
-        qtb_wide_kernel<<<wv.grid, kWideThreads, 0, st>>>(w, base);
+        if (rc->wide_batch_log == 2) qtb_wide_kernel<2><<<wv.grid, kWideThreads, 0, st>>>(w, base);
+        else qtb_wide_kernel<kWideBatchLog><<<wv.grid, kWideThreads, 0, st>>>(w, base);
         QTB_CUDA(cudaGetLastError());
     }
     return QTB_OK;
@@ -2435,6 +2452,21 @@ static int autotune_run(qtb_plan_device* s, RunCache* rc, const RunArgs& base, v
                      : rc->schedule == kSchedHybrid   ? "hybrid"
                      : rc->schedule == kSchedPersistent ? "persistent"
                                                       : "classes");
+    // the wave kernel variant (8 or 4 elements per thread in flight), timed
+    // with the chosen schedule unless QTB_WIDE_BATCH fixes it
+    if (!rc->waves.empty() && !std::getenv("QTB_WIDE_BATCH")) {
+        float wave_ms[2] = {1e30f, 1e30f};
+        for (int v = 0; v < 2; ++v) {
+            rc->wide_batch_log = v == 0 ? (int)kWideBatchLog : 2;
+            if ((r = time_it([&] { return launch_schedule(s, rc, schedule_of(rc), a, scratch_dev, st); },
+                             &wave_ms[v])))
+                return r;
+        }
+        rc->wide_batch_log = wave_ms[1] < wave_ms[0] ? 2 : (int)kWideBatchLog;
+        if (log)
+            std::fprintf(stderr, "qtb autotune: waves with 8 elements per thread %.1f us, 4 elements %.1f us\n",
+                         1e3 * wave_ms[0], 1e3 * wave_ms[1]);
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     rc->tuned = true;

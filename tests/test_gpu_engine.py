@@ -159,19 +159,22 @@ def test_plain_path_matches_batched_and_reference(cuda_device, name, max_width):
     assert eng.compile(G, len(w['gamma']), w['gamma'], w['beta']).plan.device_status() == 0
 
 
-@pytest.mark.parametrize('cluster_max', [None, str(1 << 22)])
-def test_wide_networks_match_plain_path(cuda_device, monkeypatch, cluster_max):
+@pytest.mark.parametrize('cluster_max,wide_batch', [(None, '3'), (None, '2'), (str(1 << 22), None)])
+def test_wide_networks_match_plain_path(cuda_device, monkeypatch, cluster_max, wide_batch):
     """Erdos-Renyi N=400 p=3 (seed 24323709) with the reference's greedy rule
     alone (order_trials=0, slicing from width 22): 247 networks too large
     for shared memory (3.5 GB of arenas) run beside the shared-memory
     classes, by default in whole-GPU waves (K4), and with
     QTB_CLUSTER_MAX_ELEMS=2^22 as one thread-block cluster each when their
-    arena is at most 32 MB (K5) and in waves above; either way every edge
-    term equals the plain per-bucket path's (an independent execution of
-    the same plans) and the energies agree."""
+    arena is at most 32 MB (K5) and in waves above; the wave kernel with 8
+    and with 4 elements per thread in flight (QTB_WIDE_BATCH); either way
+    every edge term equals the plain per-bucket path's (an independent
+    execution of the same plans) and the energies agree."""
     import networkx as nx
     if cluster_max is not None:
         monkeypatch.setenv('QTB_CLUSTER_MAX_ELEMS', cluster_max)
+    if wide_batch is not None:                 # the wave kernel with 8 or 4 elements per thread
+        monkeypatch.setenv('QTB_WIDE_BATCH', wide_batch)
     G = nx.erdos_renyi_graph(400, 3 / 399, seed=24323709)
     gamma, beta = graphs.angles(3, seed=1)
     eng = _engine(max_width=22, order_trials=0)
