@@ -2442,16 +2442,26 @@ static int autotune_run(qtb_plan_device* s, RunCache* rc, const RunArgs& base, v
         best_ms = warp_ms;
     }
     if (hyb12_ms < best_ms) rc->schedule = kSchedHybrid12;
-    if (log)
+    if (log) {
+        // a schedule that does not apply to the plan keeps its 1e30 sentinel
+        auto us = [](float ms, char* buf) {
+            if (ms >= 1e29f)
+                std::snprintf(buf, 24, "n/a");
+            else
+                std::snprintf(buf, 24, "%.1f us", 1e3 * ms);
+            return buf;
+        };
+        char b0[24], b1[24], b2[24], b3[24], b4[24];
         std::fprintf(stderr,
-                     "qtb autotune: class schedule %.1f us, persistent %.1f us, hybrid %.1f us, hybrid "
-                     "(96-thread lean) %.1f us, warp %.1f us -> %s\n",
-                     1e3 * class_ms, 1e3 * pers_ms, 1e3 * hyb_ms, 1e3 * hyb12_ms, 1e3 * warp_ms,
+                     "qtb autotune: class schedule %s, persistent %s, hybrid %s, hybrid "
+                     "(96-thread lean) %s, warp %s -> %s\n",
+                     us(class_ms, b0), us(pers_ms, b1), us(hyb_ms, b2), us(hyb12_ms, b3), us(warp_ms, b4),
                      rc->schedule == kSchedWarp       ? "warp"
                      : rc->schedule == kSchedHybrid12 ? "hybrid12"
                      : rc->schedule == kSchedHybrid   ? "hybrid"
                      : rc->schedule == kSchedPersistent ? "persistent"
                                                       : "classes");
+    }
     // the wave kernel variant (8 or 4 elements per thread in flight), timed
     // with the chosen schedule unless QTB_WIDE_BATCH fixes it
     if (!rc->waves.empty() && !std::getenv("QTB_WIDE_BATCH")) {
