@@ -262,7 +262,7 @@ struct RunArgs {
     uint32_t blob_capacity;       // bytes per CTA
     int* status;
     unsigned int* done;           // networks finished in this run (reset by the last one)
-    unsigned int* queue;          // next job of a persistent launch (zeroed before it)
+    unsigned int* queue;          // claims of a persistent launch past its first jobs (zeroed before it)
     uint32_t n_jobs;              // jobs of this launch
     uint32_t total_jobs;          // networks of the run over all its launches
     const float2* terms;          // the run's edge terms, [total_jobs]
@@ -298,17 +298,20 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar) {
 
 // Bulk (TMA) copies global -> shared completing on the mbarrier's current
 // phase (`parity`); every thread waits with a bounded spin.  Returns false
-// (status word set) if the copies did not land.
-__device__ bool stage(void* dst0, const void* src0, uint32_t bytes0, void* dst1, const void* src1,
-                      uint32_t bytes1, uint64_t* bar, uint32_t parity, int* status) {
+// (status word set) if the copies did not land.  stage_issue (one thread)
+// starts the copies, stage_wait (every thread) waits for them, stage does
+// both.
+__device__ __forceinline__ void stage_issue(void* dst0, const void* src0, uint32_t bytes0, void* dst1,
+                                            const void* src1, uint32_t bytes1, uint64_t* bar) {
     const uint32_t bar_a = smem_addr(bar);
-    if (threadIdx.x == 0) {
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a),
-                     "r"(bytes0 + bytes1)
-                     : "memory");
-        if (bytes0) bulk_copy(dst0, src0, bytes0, bar_a);
-        if (bytes1) bulk_copy(dst1, src1, bytes1, bar_a);
-    }
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes0 + bytes1)
+                 : "memory");
+    if (bytes0) bulk_copy(dst0, src0, bytes0, bar_a);
+    if (bytes1) bulk_copy(dst1, src1, bytes1, bar_a);
+}
+
+__device__ bool stage_wait(uint64_t* bar, uint32_t parity, int* status) {
+    const uint32_t bar_a = smem_addr(bar);
     uint32_t done = 0;
     for (uint32_t it = 0; it < kStageSpinLimit; ++it) {
         asm volatile(
@@ -319,6 +322,12 @@ __device__ bool stage(void* dst0, const void* src0, uint32_t bytes0, void* dst1,
     }
     if (!done && threadIdx.x == 0) atomicOr(status, kStatusStageTimeout);
     return __syncthreads_and(done) != 0;
+}
+
+__device__ bool stage(void* dst0, const void* src0, uint32_t bytes0, void* dst1, const void* src1,
+                      uint32_t bytes1, uint64_t* bar, uint32_t parity, int* status) {
+    if (threadIdx.x == 0) stage_issue(dst0, src0, bytes0, dst1, src1, bytes1, bar);
+    return stage_wait(bar, parity, status);
 }
 
 __device__ __forceinline__ void neumaier_add(double& sum, double& comp, double x) {
@@ -332,9 +341,17 @@ __device__ __forceinline__ void neumaier_add(double& sum, double& comp, double x
 // then energy = (n_groups - sum) / 2.  The order does not depend on the
 // launch shape, so every schedule gives the same energy for the same terms.
 __device__ void reduce_energy_warp(const float2* terms, uint32_t n, double n_groups, double* energy) {
+    constexpr uint32_t kBatch = 16;   // loads in flight per lane: one L2 round trip per 16 terms
     const uint32_t lane = threadIdx.x & 31u;
     double s = 0.0, c = 0.0;
-    for (uint32_t i = lane; i < n; i += 32u) neumaier_add(s, c, (double)__ldcg(terms + i).x);
+    for (uint32_t base = lane; base < n; base += 32u * kBatch) {
+        float x[kBatch];
+#pragma unroll
+        for (uint32_t j = 0; j < kBatch; ++j) x[j] = base + 32u * j < n ? __ldcg(&terms[base + 32u * j].x) : 0.f;
+#pragma unroll
+        for (uint32_t j = 0; j < kBatch; ++j)
+            if (base + 32u * j < n) neumaier_add(s, c, (double)x[j]);
+    }
     for (int off = 16; off > 0; off >>= 1) {
         const double os = __shfl_xor_sync(0xffffffffu, s, off);
         const double oc = __shfl_xor_sync(0xffffffffu, c, off);
@@ -717,15 +734,27 @@ __global__ void __launch_bounds__(kLean == 2 ? 96 : kLean ? 128 : (kPersistent ?
     uint32_t parity = 0;
     const float2* __restrict__ table = kSmemTable ? stable : a.gtable;
     bool table_ready = !kSmemTable;
+    // The plan-wide gate entries are staged once per CTA.  Their copy starts
+    // before the first network is located, so that the two overlap.
+    if (kSmemTable && threadIdx.x == 0) stage_issue(common, a.common, a.common_bytes, nullptr, nullptr, 0u, bar);
     for (uint32_t iter = 0;; ++iter) {
-        if (kPersistent) {
-            if (threadIdx.x == 0) s_job = atomicAdd(a.queue, 1u);
+        // A persistent CTA's first network is job blockIdx.x (every CTA of
+        // the grid is resident, so the widest jobs start at once without a
+        // queue round trip); later ones come from the queue, which counts
+        // the claims past the first gridDim.x jobs.
+        uint32_t job_i = blockIdx.x;
+        if (kPersistent && iter > 0) {
+            if (threadIdx.x == 0) s_job = gridDim.x + atomicAdd(a.queue, 1u);
             __syncthreads();
-            if (s_job >= a.n_jobs) break;
-        } else if (iter > 0) {
+            job_i = s_job;
+        } else if (!kPersistent && iter > 0) {
             break;
         }
-        const Job job = jobs[kPersistent ? s_job : blockIdx.x];
+        if (job_i >= a.n_jobs) {
+            if (!table_ready) stage_wait(bar, parity, a.status);   // no copy left in flight
+            break;
+        }
+        const Job job = jobs[job_i];
         const DevNetRun net = *job.net;
         // a network with element records needs no blob (shared table and
         // arena only); otherwise blob_capacity 0: the launch reads plan
@@ -735,21 +764,19 @@ __global__ void __launch_bounds__(kLean == 2 ? 96 : kLean ? 128 : (kPersistent ?
         if (net.arena_elems > a.arena_capacity || (staged && net.blob_bytes > a.blob_capacity)) {
             if (threadIdx.x == 0)
                 atomicOr(a.status, net.arena_elems > a.arena_capacity ? kStatusArena : kStatusBlob);
+            if (!table_ready) stage_wait(bar, parity, a.status);
             return;
         }
-        // the first staging of a CTA also brings the plan-wide gate entries
-        const bool with_common = kSmemTable && !table_ready;
-        const uint32_t blob_bytes = staged ? net.blob_bytes : 0u;
-        const uint32_t common_bytes = with_common ? a.common_bytes : 0u;
-        if (blob_bytes + common_bytes) {
-            if (!stage(blob, a.blobs + net.blob_off16, blob_bytes, common, a.common, common_bytes, bar, parity,
-                       a.status))
-                return;
-            parity ^= 1u;
-        }
         if (!table_ready) {
+            if (!stage_wait(bar, parity, a.status)) return;
+            parity ^= 1u;
             build_table(common, a, stable);
             table_ready = true;
+        }
+        if (staged) {
+            if (!stage(blob, a.blobs + net.blob_off16, net.blob_bytes, nullptr, nullptr, 0u, bar, parity, a.status))
+                return;
+            parity ^= 1u;
         }
         const unsigned char* nblob =
             staged ? blob : reinterpret_cast<const unsigned char*>(a.blobs + net.blob_off16);
