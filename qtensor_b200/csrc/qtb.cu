@@ -238,10 +238,14 @@ __global__ void qtb_table_kernel(const DevEntry* entries, int n_entries, const D
 }
 
 // ----------------------------------------------------------------- K3
+// A network of a launch: its run descriptor inline (one load locates
+// everything the executor needs) and where its edge term goes.
 struct Job {
-    const DevNetRun* net;
+    DevNetRun net;
     float2* term;
+    uint64_t pad;
 };
+static_assert(sizeof(Job) == 64, "Job layout");
 
 // Arguments shared by every CTA of one run (all size classes).
 struct RunArgs {
@@ -645,6 +649,14 @@ __device__ float2 contract_records_compact(const DevNetRun& net, const uint32_t*
     const uint32_t tid = threadIdx.x, np = net.n_phases;
     const uint2* ghead = reinterpret_cast<const uint2*>(rec);
     const bool staged = np <= kRecHeadSmem;
+    // Phase 0's records follow the headers (rounded up to 16 bytes), so this
+    // thread's first record is loaded together with the headers instead of
+    // after them; the load stays inside the network's records, and the
+    // record is used only if the thread has an element in phase 0.
+    const uint32_t first_word = (2u * np + 3u) & ~3u;
+    const uint4 r0 = first_word + 4u * (tid + 1u) <= net.rec_words
+                         ? __ldg(reinterpret_cast<const uint4*>(rec + first_word) + tid)
+                         : make_uint4(0u, 0u, 0u, 0u);
     if (staged)
         for (uint32_t i = tid; i < np; i += blockDim.x) s_head[i] = __ldg(ghead + i);
     __syncthreads();
@@ -679,7 +691,7 @@ __device__ float2 contract_records_compact(const DevNetRun& net, const uint32_t*
         else __syncthreads();
         return true;
     };
-    Ahead ra = first(0), rb = first(1), rc = first(2), rd;
+    Ahead ra{head(0), r0}, rb = first(1), rc = first(2), rd;
     for (uint32_t p = 0;; p += 4) {
         if (!phase(p, ra, rd)) break;
         if (!phase(p + 1, rb, ra)) break;
@@ -755,7 +767,7 @@ __global__ void __launch_bounds__(kLean == 2 ? 96 : kLean ? 128 : (kPersistent ?
             break;
         }
         const Job job = jobs[job_i];
-        const DevNetRun net = *job.net;
+        const DevNetRun& net = job.net;
         // a network with element records needs no blob (shared table and
         // arena only); otherwise blob_capacity 0: the launch reads plan
         // blobs from global memory
@@ -870,7 +882,7 @@ __global__ void __launch_bounds__(kWarpMaxThreads) qtb_warp_network_kernel(const
         job = __shfl_sync(0xffffffffu, job, 0);
         if (job >= a.n_jobs) break;
         const Job jb = jobs[job];
-        const DevNetRun net = *jb.net;
+        const DevNetRun& net = jb.net;
         if (net.arena_elems > a.arena_capacity || net.blob_bytes > a.blob_capacity) {
             if (lane == 0) atomicOr(a.status, net.arena_elems > a.arena_capacity ? kStatusArena : kStatusBlob);
             return;
@@ -1910,8 +1922,8 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
             cap = std::max(cap, plan->druns[i].arena_elems);
             blob = std::max(blob, staged_blob(plan->druns[i], lc.records));
             maxe = std::max(maxe, plan->druns[i].max_elems);
-            Job j;
-            j.net = runs ? runs + i : nullptr;    // null in a size-only build
+            Job j{};
+            j.net = plan->druns[i];
             j.term = terms + (i - first);
             jobs.push_back(j);
         }
@@ -2820,8 +2832,9 @@ __global__ void qtb_noalloc_jobs_kernel(Job* jobs, const DevNetRun* runs, int32_
                                         int32_t count, float2* terms) {
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < count) {
-        jobs[i].net = runs + first + i;
+        jobs[i].net = runs[first + i];
         jobs[i].term = terms + i;
+        jobs[i].pad = 0;
     }
 }
 
