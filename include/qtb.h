@@ -389,7 +389,7 @@ int qtb_plan_collect_timing(qtb_plan* plan, double* total_ms, int64_t* launches)
  * shared memory are read from global memory), so a network too wide for
  * shared memory, which qtb_plan_run would contract with the whole GPU, runs
  * far slower here.  Results equal qtb_plan_run's.  Requests needing more than
- * the array (16 B per network plus count x the largest arena of the range x
+ * the array (64 B per network plus count x the largest arena of the range x
  * 8 B, plus 512 B) fail with QTB_ERR_UNSUPPORTED and a message; split the
  * range.  The first call on a device looks up the array's device address
  * (once per device, that device current) and should come before any stream
