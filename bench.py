@@ -364,7 +364,17 @@ def run_serving(n_requests, rate, device_index, plain_budget_s=20.0):
                 out.append(exc)
         return out
 
+    warm_reqs = serving_requests(6, seed=7)
+
+    def warm(srv):
+        """Untimed, before a server's timed requests: a few requests of the
+        same distribution (another seed), so that one-time costs (kernel
+        modules loaded on first launch, allocator pools, worker start-up)
+        fall outside every policy's numbers alike."""
+        collect([srv.submit(*r) for r in warm_reqs])
+
     def poisson(srv):
+        warm(srv)
         t0 = time.perf_counter()
         futs = []
         for (G, gamma, beta), gap in zip(reqs, gaps):
@@ -383,6 +393,7 @@ def run_serving(n_requests, rate, device_index, plain_budget_s=20.0):
         fifo, wall_fifo = poisson(srv)
     with QAOAServer(device=device_index, n_streams=1, compile_workers=1, max_request_bytes=budget,
                     wave_ctas_per_sm=0) as srv:
+        warm(srv)
         t0 = time.perf_counter()
         alone = []
         for r in reqs:
@@ -422,7 +433,8 @@ def run_serving(n_requests, rate, device_index, plain_budget_s=20.0):
             'workload': '{} requests: 3-regular or Erdos-Renyi (mean degree 3), N U[16,500], '
                         'p U[1,4], angles U[0,pi) (seed 0); Poisson arrivals at {} req/s '
                         '(seed 1); slicing from width 29, at most 1024 slices per edge, at most '
-                        '{:.0e} algorithmic bytes per request'.format(len(reqs), rate, budget),
+                        '{:.0e} algorithmic bytes per request; each server first answers 6 untimed '
+                        'requests of the same distribution (seed 7)'.format(len(reqs), rate, budget),
             'continuous_batching': summarize(stream, wall_stream),
             'fifo_queue': summarize(fifo, wall_fifo),
             'batched_one_at_a_time': summarize(alone, wall_alone),

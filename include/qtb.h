@@ -325,6 +325,15 @@ int qtb_plan_set_autotune(qtb_plan* plan, int32_t enable);
  * every SM stays free for other streams' kernels (a server's concurrent
  * requests) while a wide request runs.  Set before a range's first run.  */
 int qtb_plan_set_wave_ctas_per_sm(qtb_plan* plan, int32_t ctas);
+/* How the CTAs of a persistent launch take networks.  0 (the default): a
+ * CTA's first network is the job of its own index, later ones come from
+ * the launch's queue; on a GPU the run has to itself every CTA is resident
+ * at once, and the first networks start without a queue round trip.  1:
+ * every network comes from the queue, so that where other streams' kernels
+ * hold part of the GPU (a server's concurrent requests) and some CTAs start
+ * late, the CTAs that run take the widest networks first.  Results are the
+ * same either way.                                                        */
+int qtb_plan_set_dynamic_claims(qtb_plan* plan, int32_t enable);
 /* Launch classes of the plan's most recent run: 4 ints per class (networks,
  * threads per CTA, dynamic shared memory bytes, flags: 1 = shared-memory
  * arena, 2 = persistent launch taking networks from a queue, 4 = a wave of

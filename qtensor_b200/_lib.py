@@ -35,6 +35,7 @@ EXPORTS = (
     'qtb_plan_export', 'qtb_plan_table_elems', 'qtb_plan_upload',
     'qtb_plan_scratch_bytes', 'qtb_plan_run', 'qtb_plan_plain_scratch_bytes',
     'qtb_plan_run_plain', 'qtb_plan_set_autotune', 'qtb_plan_set_wave_ctas_per_sm',
+    'qtb_plan_set_dynamic_claims',
     'qtb_plan_last_launch_config', 'qtb_plan_device_bytes', 'qtb_plan_device_status',
     'qtb_selftest_wait_timeout', 'qtb_host_device_pointer', 'qtb_copy_c',
     'qtb_plan_set_timing', 'qtb_plan_collect_timing', 'qtb_plan_run_noalloc',
@@ -142,6 +143,7 @@ def _declare(lib):
         'qtb_plan_run': (c.c_int, [P, c.c_int32, c.c_int32, P, P, P, P, P]),
         'qtb_plan_set_autotune': (c.c_int, [P, c.c_int32]),
         'qtb_plan_set_wave_ctas_per_sm': (c.c_int, [P, c.c_int32]),
+        'qtb_plan_set_dynamic_claims': (c.c_int, [P, c.c_int32]),
         'qtb_plan_last_launch_config': (c.c_int, [P, P, c.c_int32, c.POINTER(c.c_int32)]),
         'qtb_plan_device_bytes': (c.c_int, [P, c.POINTER(c.c_size_t)]),
         'qtb_plan_device_status': (c.c_int, [P, c.POINTER(c.c_int32)]),

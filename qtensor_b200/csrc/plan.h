@@ -210,6 +210,7 @@ struct qtb_plan {
     int32_t max_slices = 256;   // networks one sliced circuit may become
     int32_t slicing = QTB_SLICE_GREEDY;   // how sliced variables are chosen
     int32_t wave_ctas_per_sm = 0;   // resident CTAs per SM of a wide wave (0: as many as fit)
+    bool dynamic_claims = false;    // persistent CTAs claim their first network from the queue too
     int32_t n_groups = 0;       // circuits added (networks of a circuit share a group)
     std::vector<qtb::Network> nets;
     // global gate table, built from the networks' local entries

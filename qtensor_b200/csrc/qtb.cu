@@ -266,7 +266,8 @@ struct RunArgs {
     uint32_t blob_capacity;       // bytes per CTA
     int* status;
     unsigned int* done;           // networks finished in this run (reset by the last one)
-    unsigned int* queue;          // claims of a persistent launch past its first jobs (zeroed before it)
+    unsigned int* queue;          // claims of a persistent launch (zeroed before it)
+    uint32_t static_first;        // 1: a persistent CTA's first network is job blockIdx.x
     uint32_t n_jobs;              // jobs of this launch
     uint32_t total_jobs;          // networks of the run over all its launches
     const float2* terms;          // the run's edge terms, [total_jobs]
@@ -750,13 +751,16 @@ __global__ void __launch_bounds__(kLean == 2 ? 96 : kLean ? 128 : (kPersistent ?
     // before the first network is located, so that the two overlap.
     if (kSmemTable && threadIdx.x == 0) stage_issue(common, a.common, a.common_bytes, nullptr, nullptr, 0u, bar);
     for (uint32_t iter = 0;; ++iter) {
-        // A persistent CTA's first network is job blockIdx.x (every CTA of
-        // the grid is resident, so the widest jobs start at once without a
-        // queue round trip); later ones come from the queue, which counts
-        // the claims past the first gridDim.x jobs.
+        // With static_first, a persistent CTA's first network is job
+        // blockIdx.x (on a GPU of its own every CTA of the grid is resident
+        // at once, so the widest jobs start together without a queue round
+        // trip) and the queue counts the claims past the first gridDim.x
+        // jobs.  Without it every network is claimed from the queue: where
+        // other kernels share the GPU and some CTAs start late, the CTAs
+        // that start first take the widest networks.
         uint32_t job_i = blockIdx.x;
-        if (kPersistent && iter > 0) {
-            if (threadIdx.x == 0) s_job = gridDim.x + atomicAdd(a.queue, 1u);
+        if (kPersistent && (iter > 0 || !a.static_first)) {
+            if (threadIdx.x == 0) s_job = (a.static_first ? gridDim.x : 0u) + atomicAdd(a.queue, 1u);
             __syncthreads();
             job_i = s_job;
         } else if (!kPersistent && iter > 0) {
@@ -2602,6 +2606,7 @@ int qtb_plan_run(qtb_plan* plan, int32_t first, int32_t count, const double* par
     a.terms_off = plan->common_terms_off;
     a.table_elems = plan->table_elems;
     a.params = params_dev;
+    a.static_first = plan->dynamic_claims ? 0u : 1u;
     a.recs = static_cast<const uint32_t*>(plan->dev.recs);
     a.recs_bytes = (uint32_t)(plan->drecs.size() * sizeof(uint32_t));
     a.runs = static_cast<const DevNetRun*>(plan->dev.runs);
@@ -2921,6 +2926,7 @@ int qtb_plan_run_noalloc(qtb_plan* plan, int32_t first, int32_t count, const dou
     a.terms_off = plan->common_terms_off;
     a.table_elems = plan->table_elems;
     a.params = params_dev;
+    a.static_first = plan->dynamic_claims ? 0u : 1u;
     a.gtable = static_cast<const float2*>(plan->dev.table);
     a.gscratch = arenas;
     a.arena_capacity = cap;
@@ -2947,6 +2953,12 @@ int qtb_plan_run_noalloc(qtb_plan* plan, int32_t first, int32_t count, const dou
 int qtb_plan_set_wave_ctas_per_sm(qtb_plan* plan, int32_t ctas) {
     if (!plan || ctas < 0) return fail(QTB_ERR_ARG, "plan_set_wave_ctas_per_sm: bad arguments");
     plan->wave_ctas_per_sm = ctas;
+    return QTB_OK;
+}
+
+int qtb_plan_set_dynamic_claims(qtb_plan* plan, int32_t enable) {
+    if (!plan) return fail(QTB_ERR_ARG, "plan_set_dynamic_claims: bad arguments");
+    plan->dynamic_claims = enable != 0;
     return QTB_OK;
 }
 

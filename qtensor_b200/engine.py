@@ -195,11 +195,16 @@ class QAOAEnergyEngine:
     products, same order; off: the executor decodes the plan blobs).
     wave_ctas_per_sm: resident CTAs per SM of the wide networks' whole-GPU
     waves (0: as many as fit).
+    dynamic_claims: persistent launches claim every network from their
+    queue (for a GPU shared with other streams' kernels; off: each CTA starts
+    on the job of its own index, which saves a queue round trip when the
+    run has the GPU to itself).
     """
 
     def __init__(self, composer='default', ordering='native', device=None, threads=0,
                  cache_size=16, order_trials=16, autotune=True, max_width=29,
-                 max_slices=1024, slicing='greedy', records=True, wave_ctas_per_sm=0):
+                 max_slices=1024, slicing='greedy', records=True, wave_ctas_per_sm=0,
+                 dynamic_claims=False):
         _require_cuda()
         if ordering not in ('native', 'reference'):
             raise ValueError('ordering must be "native" or "reference"')
@@ -216,6 +221,7 @@ class QAOAEnergyEngine:
         self.slicing = slicing
         self.records = records
         self.wave_ctas_per_sm = wave_ctas_per_sm
+        self.dynamic_claims = dynamic_claims
         self._cache = {}
         self._by_id = {}        # id(G) -> (weakref, nodes, p, key, edge count)
         self._edge_digests = {}  # id(edge subset) -> (subset, tuple, digest, length)
@@ -251,6 +257,7 @@ class QAOAEnergyEngine:
         plan.set_slicing(self.slicing)
         plan.set_records(self.records)
         plan.set_wave_ctas_per_sm(self.wave_ctas_per_sm)
+        plan.set_dynamic_claims(self.dynamic_claims)
         if self.ordering == 'native':
             csr = graph_csr(G)
             index = {v: i for i, v in enumerate(csr[0])}

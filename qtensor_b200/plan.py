@@ -191,6 +191,12 @@ class NetworkPlan:
         before the first run."""
         check(self._lib.qtb_plan_set_wave_ctas_per_sm(self._h, int(ctas)))
 
+    def set_dynamic_claims(self, enable):
+        """Persistent launches claim every network from their queue (for a
+        GPU shared with other streams' kernels) instead of starting each CTA
+        on the job of its own index; results are the same."""
+        check(self._lib.qtb_plan_set_dynamic_claims(self._h, int(bool(enable))))
+
     def set_autotune(self, enable):
         """Time every launch class with 64..1024 threads per CTA on the first
         run of a range and keep the fastest."""

@@ -123,7 +123,10 @@ class QAOAServer:
     its share of the CPUs the process may use).  wave_ctas_per_sm: resident
     CTAs per SM of a wide request's whole-GPU waves (1 leaves half of every
     SM to the other requests' kernels while a wide request runs; 0 lets
-    the waves take whole SMs)."""
+    the waves take whole SMs).  Every request's persistent launches claim
+    all their networks from their queues (the engine's dynamic_claims): with
+    concurrent requests holding SMs, a CTA that starts late takes whatever
+    network is left rather than one fixed in advance."""
 
     def __init__(self, device=None, n_streams=4, memory_budget=None, max_width=29,
                  max_slices=1024, composer='default', order_trials=4, compile_workers=2,
@@ -197,6 +200,7 @@ class QAOAServer:
             plan.set_order_trials(self.order_trials)
             plan.set_max_width(self.max_width, self.max_slices)
             plan.set_wave_ctas_per_sm(self.wave_ctas_per_sm)
+            plan.set_dynamic_claims(True)
             plan.add_lightcones(csr, edges, p, self.cid, params, self.compile_threads)
             if self.max_request_bytes is not None:
                 work = sum(plan.info(i)['alg_bytes'] for i in range(len(plan)))

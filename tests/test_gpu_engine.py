@@ -223,6 +223,20 @@ def test_every_schedule_matches_reference(cuda_device, monkeypatch, schedule):
         assert len(cfg) == 1 and cfg[0][3] & 2 and cfg[0][1] == 256
 
 
+@pytest.mark.parametrize('schedule', ['persistent:128', 'hybrid:512', 'hybrid12:1024'])
+def test_dynamic_claims_match_reference(cuda_device, monkeypatch, schedule):
+    """Persistent launches that claim every network from their queue (the
+    server's setting) give the same edge terms as the default, where a CTA
+    starts on the job of its own index, and the reference's within TOL."""
+    monkeypatch.setenv('QTB_SCHEDULE', schedule)
+    G, w = golden_graph('cfg3')
+    ref = np.array([complex(*t) for t in w['terms']])
+    static = _engine().edge_terms(G, w['gamma'], w['beta'])
+    dynamic = _engine(dynamic_claims=True).edge_terms(G, w['gamma'], w['beta'])
+    assert np.max(np.abs(dynamic - ref)) < TOL
+    assert np.array_equal(dynamic, static)   # same products in the same order
+
+
 @pytest.mark.parametrize('name,p,max_width', [('cfg3', 3, 29), ('cfg4', 4, 29), ('cfg2', 3, 11)])
 def test_element_records_match_blob_path(cuda_device, name, p, max_width):
     """The shared-memory executor contracting from element records gives the
