@@ -848,6 +848,68 @@ __device__ __forceinline__ void warp_bar_wait(uint64_t* bar, uint32_t parity, in
     *ok = __all_sync(0xffffffffu, done != 0);
 }
 
+// The phases of one network from its compact element records, contracted by
+// one warp: lane l takes elements l, l + 32, ... of a phase, and phases are
+// separated by warp barriers only.  S is the warp's window [gate table]
+// [arena], the layout the records address.  Each lane's record of its first
+// element in the next three phases is in flight while the current phase
+// computes (a four-slot rotation through an unrolled loop, as in
+// contract_records_compact), and within a phase the next record loads while
+// the current element computes.  Networks of at most 32 phases keep their
+// phase headers one per lane.
+__device__ void warp_records_compact(const DevNetRun& net, const uint32_t* __restrict__ rec,
+                                     float2* __restrict__ S, uint32_t lane) {
+    const uint32_t np = net.n_phases;
+    const uint2* ghead = reinterpret_cast<const uint2*>(rec);
+    const uint2 mine = lane < np ? __ldg(ghead + lane) : make_uint2(0u, 0u);
+    auto head = [&](uint32_t p) -> uint2 {
+        if (np <= 32u) {
+            uint2 h;
+            h.x = __shfl_sync(0xffffffffu, mine.x, p & 31u);
+            h.y = __shfl_sync(0xffffffffu, mine.y, p & 31u);
+            return p < np ? h : make_uint2(0u, 0u);
+        }
+        return p < np ? __ldg(ghead + p) : make_uint2(0u, 0u);
+    };
+    struct Ahead {
+        uint2 h;
+        uint4 r;
+    };
+    auto first = [&](uint32_t p) {
+        Ahead x;
+        x.h = head(p);
+        x.r = lane < (x.h.y & 0xffffffu) ? __ldg(reinterpret_cast<const uint4*>(rec + x.h.x) + lane)
+                                          : make_uint4(0u, 0u, 0u, 0u);
+        return x;
+    };
+    auto phase = [&](uint32_t q, const Ahead& cur, Ahead& ahead) -> bool {
+        if (q >= np) return false;
+        ahead = first(q + 3);
+        const uint32_t total = cur.h.y & 0xffffffu;
+        const uint4* prec = reinterpret_cast<const uint4*>(rec + cur.h.x);
+        uint4 r = cur.r;
+        for (uint32_t g = lane; g < total; g += 32u) {
+            const uint4 nx = g + 32u < total ? __ldg(prec + g + 32u) : r;
+            rec_element_compact(r, S);
+            r = nx;
+        }
+        __syncwarp();
+        return true;
+    };
+    Ahead ra = first(0), rb = first(1), rc = first(2), rd;
+    for (uint32_t p = 0;; p += 4) {
+        if (!phase(p, ra, rd)) break;
+        if (!phase(p + 1, rb, ra)) break;
+        if (!phase(p + 2, rc, rb)) break;
+        if (!phase(p + 3, rd, rc)) break;
+    }
+}
+
+// With a.recs set (a launch whose every network has compact element
+// records, kSmemTable), a warp's slot is [mbarrier][blob_capacity][copy of
+// the gate table][arena]: the records address one window [table][arena],
+// so every warp keeps its own copy of the table right before its arena and
+// contracts without staging the blob.
 template <bool kSmemTable>
 __global__ void __launch_bounds__(kWarpMaxThreads) qtb_warp_network_kernel(const Job* __restrict__ jobs,
                                                                           const RunArgs a) {
@@ -860,11 +922,14 @@ __global__ void __launch_bounds__(kWarpMaxThreads) qtb_warp_network_kernel(const
     unsigned char* common = smem;
     float2* stable = reinterpret_cast<float2*>(smem + (kSmemTable ? a.common_bytes : 0u));
     const uint32_t table_bytes = kSmemTable ? ((a.table_elems * 8u + 15u) & ~15u) : 0u;
-    const uint32_t slot_bytes = 16u + a.blob_capacity + 8u * a.arena_capacity;
+    const bool rec_slots = kSmemTable && a.recs != nullptr;
+    const uint32_t copy_bytes = rec_slots ? table_bytes : 0u;
+    const uint32_t slot_bytes = 16u + a.blob_capacity + copy_bytes + 8u * a.arena_capacity;
     unsigned char* slot = smem + (kSmemTable ? a.common_bytes : 0u) + table_bytes + warp * slot_bytes;
     uint64_t* bar = reinterpret_cast<uint64_t*>(slot);
     unsigned char* blob = slot + 16;
-    float2* arena = reinterpret_cast<float2*>(blob + a.blob_capacity);
+    float2* window = reinterpret_cast<float2*>(blob + a.blob_capacity);   // the table copy (rec_slots)
+    float2* arena = reinterpret_cast<float2*>(blob + a.blob_capacity + copy_bytes);
     if (kSmemTable) {
         // plan-wide gate entries and angle terms (tiny), then the table
         const uint4* src = a.common;
@@ -872,6 +937,8 @@ __global__ void __launch_bounds__(kWarpMaxThreads) qtb_warp_network_kernel(const
         for (uint32_t i = threadIdx.x; i < a.common_bytes / 16u; i += blockDim.x) dst[i] = __ldg(src + i);
         __syncthreads();
         build_table(common, a, stable);
+        if (rec_slots)
+            for (uint32_t i = threadIdx.x & 31u; i < a.table_elems; i += 32u) window[i] = stable[i];
     }
     const float2* __restrict__ table = kSmemTable ? stable : a.gtable;
     if (lane == 0) {
@@ -887,39 +954,44 @@ __global__ void __launch_bounds__(kWarpMaxThreads) qtb_warp_network_kernel(const
         if (job >= a.n_jobs) break;
         const Job jb = jobs[job];
         const DevNetRun& net = jb.net;
-        if (net.arena_elems > a.arena_capacity || net.blob_bytes > a.blob_capacity) {
+        const bool use_recs = rec_slots && net.rec_words != 0 && net.rec_format == kRecCompact;
+        if (net.arena_elems > a.arena_capacity || (!use_recs && net.blob_bytes > a.blob_capacity)) {
             if (lane == 0) atomicOr(a.status, net.arena_elems > a.arena_capacity ? kStatusArena : kStatusBlob);
             return;
         }
-        if (lane == 0) {
-            // the slot was last read by this warp's generic loads
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            const uint32_t bar_a = smem_addr(bar);
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(net.blob_bytes)
-                         : "memory");
-            bulk_copy(blob, a.blobs + net.blob_off16, net.blob_bytes, bar_a);
-        }
-        bool ok = false;
-        warp_bar_wait(bar, parity, a.status, &ok);
-        if (!ok) return;
-        parity ^= 1u;
-        const DevPhase* phases = reinterpret_cast<const DevPhase*>(blob);
-        const DevOp* ops = reinterpret_cast<const DevOp*>(blob + net.n_phases * sizeof(DevPhase));
-        const DevIn* ins = reinterpret_cast<const DevIn*>(blob + net.ins_off);
-        for (uint32_t p = 0; p < net.n_phases; ++p) {
-            const DevPhase ph = phases[p];
-            const uint16_t* chunk = reinterpret_cast<const uint16_t*>(blob + ph.chunk_off);
-            for (uint32_t r = 0; r * 32u < ph.total_elems; ++r) {
-                const uint32_t g = r * 32u + lane;
-                if (g < ph.total_elems) {
-                    uint32_t oi = ph.chunk_off ? chunk[r]
-                                               : search_op<false>(ops, ph.op_first, ph.op_first + ph.op_count - 1u, g);
-                    DevOp op = ops[oi];
-                    find_op(g, oi, op, [&](uint32_t i) { return ops[i]; });
-                    compute_element<kSmemTable>(op, g - op.elem_begin, ins, table, arena);
-                }
+        if (use_recs) {
+            warp_records_compact(net, a.recs + net.rec_off, window, lane);
+        } else {
+            if (lane == 0) {
+                // the slot was last read by this warp's generic loads
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                const uint32_t bar_a = smem_addr(bar);
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(net.blob_bytes)
+                             : "memory");
+                bulk_copy(blob, a.blobs + net.blob_off16, net.blob_bytes, bar_a);
             }
-            __syncwarp();
+            bool ok = false;
+            warp_bar_wait(bar, parity, a.status, &ok);
+            if (!ok) return;
+            parity ^= 1u;
+            const DevPhase* phases = reinterpret_cast<const DevPhase*>(blob);
+            const DevOp* ops = reinterpret_cast<const DevOp*>(blob + net.n_phases * sizeof(DevPhase));
+            const DevIn* ins = reinterpret_cast<const DevIn*>(blob + net.ins_off);
+            for (uint32_t p = 0; p < net.n_phases; ++p) {
+                const DevPhase ph = phases[p];
+                const uint16_t* chunk = reinterpret_cast<const uint16_t*>(blob + ph.chunk_off);
+                for (uint32_t r = 0; r * 32u < ph.total_elems; ++r) {
+                    const uint32_t g = r * 32u + lane;
+                    if (g < ph.total_elems) {
+                        uint32_t oi = ph.chunk_off ? chunk[r]
+                                                   : search_op<false>(ops, ph.op_first, ph.op_first + ph.op_count - 1u, g);
+                        DevOp op = ops[oi];
+                        find_op(g, oi, op, [&](uint32_t i) { return ops[i]; });
+                        compute_element<kSmemTable>(op, g - op.elem_begin, ins, table, arena);
+                    }
+                }
+                __syncwarp();
+            }
         }
         uint32_t last = 0;
         if (lane == 0) {
@@ -1400,6 +1472,7 @@ struct LaunchClass {
     size_t job_offset;      // into the job buffer
     size_t scratch_offset;  // elements into scratch (classes without a shared arena)
     size_t smem_bytes;
+    uint32_t slot_table;    // warp queue over element records: bytes of each warp's gate-table copy
 };
 
 // Plan-wide staging image: gate entries, padded to 16 bytes, then the angle
@@ -1650,7 +1723,7 @@ static int hybrid_lean_grid(std::vector<LaunchClass>& sched, bool smem_table) {
 // Shared memory of a warp-queue launch class of `threads` threads: the
 // fixed part, then one slot (mbarrier, blob, arena) per warp.
 static size_t warp_slot(const LaunchClass& lc) {
-    return 16 + (size_t)lc.blob_capacity + 8 * (size_t)lc.capacity;
+    return 16 + (size_t)lc.blob_capacity + lc.slot_table + 8 * (size_t)lc.capacity;
 }
 static size_t warp_smem(const LaunchClass& lc, size_t fixed, int threads) {
     return fixed + (size_t)(threads / 32) * warp_slot(lc);
@@ -2010,11 +2083,19 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
     // warp schedule: the networks whose warp slot (blob + arena) is at most
     // the 95th percentile of the run's slots go to one warp queue (every
     // warp contracts its own network), the others run as class launches,
-    // started first
+    // started first.  Networks with compact element records need no blob in
+    // the slot, only a copy of the gate table before the arena; when every
+    // network of the queue has them, the queue contracts from the records.
     rc->wclasses.clear();
     if (!all.empty()) {
+        const size_t table_copy = ((size_t)plan->table_elems * 8 + 15) & ~size_t(15);
+        auto compact = [&](int32_t i) {
+            const DevNetRun& r = plan->druns[i];
+            return recs && r.rec_words != 0 && r.rec_format == kRecCompact;
+        };
         auto slot_of = [&](int32_t i) {
-            return 16 + (size_t)plan->druns[i].blob_bytes + 8 * (size_t)((plan->druns[i].arena_elems + 3u) & ~3u);
+            return 16 + (compact(i) ? table_copy : (size_t)plan->druns[i].blob_bytes) +
+                   8 * (size_t)((plan->druns[i].arena_elems + 3u) & ~3u);
         };
         std::vector<size_t> slots;
         for (int32_t i : all) slots.push_back(slot_of(i));
@@ -2033,8 +2114,10 @@ static int build_run(qtb_plan* plan, int32_t first, int32_t count, float2* terms
                     if (class_of[i - first] == c) m.push_back(i);
                 if (!m.empty()) rc->wclasses.push_back(make_class(m, true, false));
             }
-            LaunchClass lc = make_class(small, true, true, false);
+            const bool all_compact = std::all_of(small.begin(), small.end(), compact);
+            LaunchClass lc = make_class(small, true, true, all_compact);
             lc.warp = true;
+            lc.slot_table = lc.records ? (uint32_t)table_copy : 0u;
             lc.threads = kWarpDefaultThreads;
             while (lc.threads > 32 && warp_smem(lc, fixed, lc.threads) > kSmemLimitBytes) lc.threads /= 2;
             lc.smem_bytes = warp_smem(lc, fixed, lc.threads);

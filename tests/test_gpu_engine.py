@@ -256,6 +256,35 @@ def test_element_records_match_blob_path(cuda_device, name, p, max_width):
     assert np.max(np.abs(out[0] - out[1])) < 1e-6
 
 
+@pytest.mark.parametrize('name,p,max_width', [('cfg3', 3, 29), ('cfg4', 4, 29), ('cfg2', 3, 11)])
+def test_warp_queue_records_match_blob_path(cuda_device, monkeypatch, name, p, max_width):
+    """The warp-per-network queue contracting from compact element records
+    (each warp's own gate-table copy before its arena) gives the reference's
+    edge terms and the terms of the same queue staging plan blobs (records
+    off): N=1000 p=3 (every network has compact records, so the queue runs
+    on them), N=256 p=4 (wide networks beside it in waves; its queue also
+    holds networks with wide-format records, so it stages blobs either
+    way), N=100 p=3 sliced below its width."""
+    monkeypatch.setenv('QTB_SCHEDULE', 'warp:64')   # two warp slots fit a CTA on every workload
+    G, w = golden_graph(name)
+    ref = np.array([complex(*t) for t in w['terms']])
+    out = []
+    for records in (True, False):
+        eng = _engine(max_width=max_width, records=records)
+        terms = eng.edge_terms(G, w['gamma'], w['beta'])
+        assert np.max(np.abs(terms - ref)) < TOL
+        cg = eng.compile(G, p, w['gamma'], w['beta'])
+        warp = [c for c in cg.plan.last_launch_config() if c[3] & 16]
+        assert len(warp) == 1
+        if not records or name == 'cfg3':
+            assert bool(warp[0][3] & 128) == records
+        E = eng.energy_expectation(G, w['gamma'], w['beta'])
+        assert abs(E - w['energy']) <= TOL * abs(w['energy'])
+        assert cg.plan.device_status() == 0
+        out.append(terms)
+    assert np.max(np.abs(out[0] - out[1])) < 1e-6
+
+
 def test_reference_named_simulator(cuda_device):
     """QAOAQtreeSimulator under the reference's method names, returning the
     reference's result shape: a one-element float64 array for a graph with
