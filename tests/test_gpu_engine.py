@@ -57,6 +57,26 @@ def test_engine_full_size_p1_closed_form(cuda_device):
     assert np.max(np.abs(terms - exact)) < TOL
 
 
+@pytest.mark.parametrize('name,p,seeds,stride', [('cfg3', 3, range(100, 105), 60),
+                                                  ('cfg4', 4, range(400, 403), 48)])
+def test_engine_benchmark_angle_sets_against_oracle(cuda_device, name, p, seeds, stride):
+    """The angle sets the benchmark times (N=1000 p=3: seeds 100 + i; N=256
+    p=4: seeds 400 + i), contracted on one cached plan: every sampled edge
+    term equals the complex128 oracle port's (QAOASimulator._get_edge_energy
+    restated), so the timed steps compute the reference's values and not
+    only the fixture's angles do."""
+    import qtensor_port as port
+    G, _ = golden_graph(name)
+    edges = list(G.edges())
+    eng = _engine()
+    for seed in seeds:
+        gamma, beta = graphs.angles(p, seed=seed)
+        terms = eng.edge_terms(G, gamma, beta)
+        for k in range(0, len(edges), stride):
+            ref = complex(port.edge_energy(G, gamma, beta, edges[k]))
+            assert abs(terms[k] - ref) < TOL, (seed, edges[k], terms[k], ref)
+
+
 def test_engine_plan_reuse_across_angles(cuda_device):
     """A cached plan with new angles equals a fresh compile with those angles."""
     G = graphs.regular(100)
