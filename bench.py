@@ -543,15 +543,34 @@ def measured_peak_hbm():
         return 6650.0, 'fallback'
 
 
-def profiled_traffic():
-    """DRAM bytes of the executor's launches per step, from the committed
-    ncu summary, if any."""
+def profiled_traffic(key='dram_bytes_per_step'):
+    """DRAM bytes (or, with key='warp_instructions_per_step', the executed
+    warp-instructions) of the executor's launches per step, from the
+    committed ncu summary, if any."""
     path = os.path.join(ROOT, 'profiles', 'network_kernel_cfg3.json')
     try:
         with open(path) as f:
-            return json.load(f).get('dram_bytes_per_step')
+            return json.load(f).get(key)
     except (OSError, ValueError):
         return None
+
+
+def issue_roofline(kernel_ms, clk, device_index):
+    """The executor's instruction-issue rate: ncu's warp-instructions per
+    step over the live executor span, per SM and SM cycle at the median
+    clock sampled during the timed region, against the 4 instructions an
+    SM can issue per cycle (one per scheduler).  The executor keeps its
+    intermediates in shared memory, so this, not HBM, is what bounds it."""
+    import torch
+    instr = profiled_traffic('warp_instructions_per_step')
+    mhz = (clk or {}).get('sm_mhz')
+    if not instr or not mhz or not kernel_ms:
+        return None
+    sms = torch.cuda.get_device_properties(device_index).multi_processor_count
+    achieved = instr / (kernel_ms * 1e-3 * sms * mhz * 1e6)
+    return {'achieved': achieved, 'peak': 4.0, 'unit': 'warp-instructions issued per SM cycle',
+            'frac': achieved / 4.0, 'warp_instructions_per_step': instr, 'sms': sms, 'sm_mhz': mhz,
+            'source': 'instruction count from ncu (profiles/network_kernel_cfg3.json), time live'}
 
 
 def device_steps(eng, cg, G, p, angle_sets, flush, stream, warmup, steps):
@@ -962,7 +981,8 @@ def run_b200(args):
                          'kernel': 'qtb_network_kernel / qtb_warp_network_kernel', 'peak_source': peak_kind,
                          'kernel_ms_per_step': kernel_step_ms,
                          'class_launches_per_step': launches_per_step,
-                         'alg_bytes_per_step': stats['alg_bytes']},
+                         'alg_bytes_per_step': stats['alg_bytes'],
+                         'issue': issue_roofline(kernel_step_ms, clk, local)},
             'cpu_baseline': cpu,
             'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': 8 * 2 * p,
                     'd2h_bytes_per_step': 8, 'ms_per_step': e2e_total / args.steps},
